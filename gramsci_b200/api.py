@@ -1,0 +1,181 @@
+"""Python front end of the B200 N-point correlation library.
+
+Mirrors the reference program's flow (src/gramsci.F90:55-224): a catalogue of
+galaxies then randoms with signed normalised weights, a binning (rmin, rmax,
+nbins, nmu, log), then one query (2PCF, 3PCF or 4PCF) whose results have the
+reference's array shapes:
+
+    2PCF  N2, N3 (nbins, nmu)                       query_graph_2pcf
+    3PCF  N2, N3 (ncfg3, nmu)                       query_graph_3pcf_all
+    4PCF  N2, N3 (ncfg4, nbins, nbins),
+          discN, discR (ncfg4, nbins, nbins, 6)     query_4pcf_all2
+
+plus integer counts by galaxy/random category.  Inputs may be numpy arrays
+(host) or CUDA torch tensors (device-resident; no host copy is made).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _native
+from ._native import GramsciError  # noqa: F401
+
+
+def ncfg3(nbins):
+    return nbins * (nbins + 1) * (nbins + 2) // 6
+
+
+def ncfg4(nbins):
+    return nbins * (nbins + 1) * (nbins + 2) * (nbins + 3) // 24
+
+
+def _fortran(a, *shape):
+    """View a flat Fortran-ordered buffer with the given shape."""
+    return np.asarray(a).reshape(shape[::-1]).transpose()
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def _is_torch_cuda(x):
+    return hasattr(x, "is_cuda") and hasattr(x, "data_ptr") and x.is_cuda
+
+
+class Context:
+    """One library context (device state, catalogue, binning)."""
+
+    def __init__(self, device=0):
+        self._lib = _native.load()
+        h = ctypes.c_void_p()
+        rc = self._lib.gr_create(ctypes.byref(h), int(device))
+        if rc != 0:
+            raise GramsciError(rc, "gr_create failed (no CUDA device?)")
+        self._h = h
+        self.device = device
+        self.nbins = self.nmu = None
+        self.n = None
+        self._keep = None
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.gr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc):
+        return _native.check(self._lib, self._h, rc)
+
+    # -- state -----------------------------------------------------------
+    def set_stream(self, stream):
+        """Run on a caller-owned CUDA stream (torch.cuda.Stream or raw handle)."""
+        handle = getattr(stream, "cuda_stream", stream)
+        self._check(self._lib.gr_set_stream(self._h, ctypes.c_void_p(handle or 0)))
+
+    def set_catalog(self, xyz, w, n_data, buffer=None):
+        """xyz (N,3) FP64, w (N,) signed normalised FP64 weights, galaxies
+        first (n_data of them), buffer (N,) 0/1 or None."""
+        if _is_torch_cuda(xyz):
+            import torch
+
+            xyz = xyz.detach().to(torch.float64).contiguous()
+            w = w.detach().to(torch.float64).contiguous()
+            buf = None if buffer is None else buffer.detach().to(torch.int32).contiguous()
+            n = xyz.shape[0]
+            self._keep = (xyz, w, buf)
+            self.n = int(n)
+            self._check(self._lib.gr_set_catalog_dev(
+                self._h, ctypes.c_void_p(xyz.data_ptr()), ctypes.c_void_p(w.data_ptr()),
+                ctypes.c_void_p(buf.data_ptr()) if buf is not None else None,
+                int(n_data), int(n - n_data)))
+            return
+        xyz = np.ascontiguousarray(xyz, np.float64).reshape(-1, 3)
+        w = np.ascontiguousarray(w, np.float64)
+        n = xyz.shape[0]
+        if w.shape[0] != n:
+            raise ValueError("w must have one entry per point")
+        buf = None if buffer is None else np.ascontiguousarray(buffer, np.int32)
+        self.n = int(n)
+        self._check(self._lib.gr_set_catalog(self._h, _ptr(xyz), _ptr(w), _ptr(buf),
+                                             int(n_data), int(n - n_data)))
+
+    def set_bins(self, rmin, rmax, nbins, nmu=1, logbins=False):
+        self._check(self._lib.gr_set_bins(self._h, float(rmin), float(rmax), int(nbins),
+                                          int(nmu), int(bool(logbins))))
+        self.nbins, self.nmu = int(nbins), int(nmu)
+
+    def set_precision(self, mode):
+        """'f32' (FP32 separations + FP64 guard band, default) or 'f64'."""
+        v = {"f32": 0, "f64": 1}[mode]
+        self._check(self._lib.gr_set_option(self._h, _native.GR_OPT_PRECISION, v))
+
+    def stats(self):
+        s = _native.GrStats()
+        self._check(self._lib.gr_get_stats(self._h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in s._fields_}
+
+    # -- queries ---------------------------------------------------------
+    def count_2pcf(self):
+        nb, nm = self.nbins, self.nmu
+        N2, N3 = np.zeros(nb * nm), np.zeros(nb * nm)
+        counts = np.zeros(nb * nm * 4, np.int64)
+        catsum = np.zeros(nb * nm * 4)
+        self._check(self._lib.gr_count_2pcf(self._h, _ptr(N2), _ptr(N3), _ptr(counts), _ptr(catsum)))
+        return dict(N2=_fortran(N2, nb, nm), N3=_fortran(N3, nb, nm),
+                    counts=_fortran(counts, nb, nm, 4), catsum=_fortran(catsum, nb, nm, 4))
+
+    def count_3pcf(self):
+        nb, nm = self.nbins, self.nmu
+        nc = ncfg3(nb)
+        N2, N3 = np.zeros(nc * nm), np.zeros(nc * nm)
+        counts = np.zeros(nc * nm * 4, np.int64)
+        catsum = np.zeros(nc * nm * 4)
+        self._check(self._lib.gr_count_3pcf(self._h, _ptr(N2), _ptr(N3), _ptr(counts), _ptr(catsum)))
+        return dict(N2=_fortran(N2, nc, nm), N3=_fortran(N3, nc, nm),
+                    counts=_fortran(counts, nc, nm, 4), catsum=_fortran(catsum, nc, nm, 4))
+
+    def count_4pcf(self):
+        nb = self.nbins
+        nc = ncfg4(nb)
+        nbin = nc * nb * nb
+        N2, N3 = np.zeros(nbin), np.zeros(nbin)
+        dN, dR = np.zeros(nbin * 6), np.zeros(nbin * 6)
+        counts = np.zeros(nbin * 5, np.int64)
+        catsum = np.zeros(nbin * 5)
+        dcount = np.zeros(nbin * 24, np.int64)
+        dsum = np.zeros(nbin * 24)
+        self._check(self._lib.gr_count_4pcf(self._h, _ptr(N2), _ptr(N3), _ptr(dN), _ptr(dR),
+                                            _ptr(counts), _ptr(catsum), _ptr(dcount), _ptr(dsum)))
+        return dict(N2=_fortran(N2, nc, nb, nb), N3=_fortran(N3, nc, nb, nb),
+                    discN=_fortran(dN, nc, nb, nb, 6), discR=_fortran(dR, nc, nb, nb, 6),
+                    counts=_fortran(counts, nc, nb, nb, 5), catsum=_fortran(catsum, nc, nb, nb, 5),
+                    dcount=_fortran(dcount, nc, nb, nb, 6, 4), dsum=_fortran(dsum, nc, nb, nb, 6, 4))
+
+    def graph(self):
+        """The (rmin, rmax) neighbour graph in the reference's layout: rows in
+        catalogue order, ids sorted, radial bin and mu bin per edge."""
+        self._check(self._lib.gr_graph_build(self._h))
+        E = ctypes.c_int64()
+        self._check(self._lib.gr_graph_nedges(self._h, ctypes.byref(E)))
+        n = self.n
+        row_ptr = np.zeros(n + 1, np.int64)
+        col = np.zeros(E.value, np.int32)
+        b = np.zeros(E.value, np.uint8)
+        mu = np.zeros(E.value, np.uint8)
+        self._check(self._lib.gr_graph_export(self._h, _ptr(row_ptr), _ptr(col), _ptr(b), _ptr(mu)))
+        return row_ptr, col, b, mu
+
+
+def version():
+    return _native.load().gr_version().decode()

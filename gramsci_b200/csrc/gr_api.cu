@@ -1,0 +1,700 @@
+// C ABI of libgramsci_cuda.so (include/gramsci_cuda.h): context, catalogue
+// and binning state, and the count entry points that chain the cell index,
+// the CSR build and the counting kernels.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/gramsci_cuda.h"
+#include "gr_kernels.cuh"
+
+using namespace gr;
+
+struct gr_ctx {
+  int device = 0;
+  cudaStream_t own = nullptr;
+  cudaStream_t user = nullptr;
+  std::string err;
+  // catalogue, catalogue order
+  DevBuf<double> xyz, w;
+  DevBuf<int> buffer;
+  bool has_buffer = false;
+  bool cat_set = false;
+  int64_t n = 0, n_data = 0, n_rand = 0;
+  bool uniform = false;
+  double w_gal = 0.0, w_ran = 0.0;
+  // binning
+  bool bins_set = false;
+  double rmin = 0, rmax = 0;
+  int nbins = 0, nmu = 1, logbins = 0;
+  int precision = 0;
+  int64_t timeout_ms = 1000;
+  // derived state
+  CellIndex index;
+  UpperCSR csr;
+  bool csr_valid = false;
+  PairParams P{};
+  DevBuf<uint8_t> normal_dev;
+  DevBuf<unsigned long long> hcnt, dcnt, stats;
+  DevBuf<double> hsum, dsum;
+  DevBuf<unsigned char> uniform_flag;
+  gr_stats st{};
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+
+  cudaStream_t stream() const { return user ? user : own; }
+};
+
+namespace gr {
+
+// ---------------------------------------------------------------- params ----
+void make_pair_params(PairParams& P, double rmin, double rmax, int nbins, int nmu, int logbins,
+                      double X, int force_fp64) {
+  std::memset(&P, 0, sizeof(P));
+  P.rmin = rmin;
+  P.rmax = rmax;
+  P.rmin2 = rmin * rmin;
+  P.rmax2 = rmax * rmax;
+  P.nbins = nbins;
+  P.nmu = nmu;
+  P.logbins = logbins;
+  P.rsd = nmu >= 2;
+  if (logbins) {
+    P.inv_dr = 1.0 / ((std::log10(rmax) - std::log10(rmin)) / (double)nbins);
+    P.log_rmin = std::log10(rmin);
+  } else {
+    P.inv_dr = 1.0 / ((rmax - rmin) / (double)nbins);
+    P.log_rmin = 0.0;
+  }
+  P.mu_scale = (double)(0.5f * (float)nmu);
+  // FP32 fast path: error bounds for coordinates rounded to float.
+  //   coordinate error            <= X u            (u = 2^-24)
+  //   separation component error  <= e1 = 2 X u + R u
+  //   |d_f - d|                   <= sqrt(3) e1 + 2.5 u R
+  // doubled for safety.
+  const double u = std::ldexp(1.0, -24);
+  const double R = rmax * 1.01 + 1e-30;
+  const double e1 = 2.0 * X * u + R * u;
+  const double d0 = 2.0 * (std::sqrt(3.0) * e1 + 2.5 * u * R);
+  P.d0 = (float)(d0 * (1.0 + 1e-6));
+  double hi = rmax + 2.0 * d0;
+  hi = hi * hi * (1.0 + 16.0 * u);
+  P.rmax2_hi = std::nextafter((float)hi, std::numeric_limits<float>::infinity());
+  double lo = rmin - 2.0 * d0;
+  if (lo > 0.0) {
+    lo = lo * lo * (1.0 - 16.0 * u);
+    P.rmin2_lo = std::nextafter((float)lo, -std::numeric_limits<float>::infinity());
+  } else {
+    P.rmin2_lo = -1.0f;
+  }
+  P.f_rmin = (float)rmin;
+  P.f_inv_dr = (float)P.inv_dr;
+  P.f_mu_scale = (float)P.mu_scale;
+  P.f_nmu = (float)nmu;
+  const double tmax = nbins + 1.0;
+  double tg = (d0 + u * std::fabs(rmin) + u * R) * P.inv_dr + 4.0 * u * tmax;
+  tg = 2.0 * tg + 1e-9 * tmax;
+  P.tguard = (float)tg;
+  // line-of-sight cosine: (pi/2)(|ds|/|s| + |dm|/|m|) + arithmetic, doubled
+  const double pi = 3.14159265358979323846;
+  P.eA = (float)(pi * std::sqrt(3.0) * e1);
+  P.mB = (float)(8.0 * X * u + 1e-30);
+  P.eB = (float)(pi * 2.0 * std::sqrt(3.0) * X * u);
+  P.eC = (float)(64.0 * u);
+  P.f32 = (!force_fp64 && !logbins && std::isfinite(tg) && tg < 0.05 && std::isfinite(X)) ? 1 : 0;
+}
+
+static int64_t multiset(int64_t m, int r) {
+  if (r == 0) return 1;
+  if (m <= 0) return 0;
+  int64_t num = 1, den = 1;
+  for (int i = 0; i < r; ++i) {
+    num *= (m + i);
+    den *= (i + 1);
+  }
+  return num / den;
+}
+
+void make_rank_tables(RankTables& T, int n, int k) {
+  std::memset(&T, 0, sizeof(T));
+  T.n = n;
+  T.k = k;
+  for (int j = 0; j < k; ++j) {
+    int r = k - j - 1;
+    T.F[j][0] = 0;
+    T.F[j][1] = 0;
+    for (int v = 1; v <= n; ++v) T.F[j][v + 1] = T.F[j][v] + (int)multiset(n - v + 1, r);
+  }
+}
+
+}  // namespace gr
+
+namespace {
+
+// find_normal (src/gramsci.F90:1611-1625) for every (mu1, mu2): single
+// precision, operations in source order, no contraction.  A negative
+// radicand gives NaN and bin 1.
+void normal_table(int nmu, std::vector<uint8_t>& out) {
+  out.assign((size_t)nmu * nmu, 1);
+  const double mu_scale = (double)(0.5f * (float)nmu);
+  for (int b = 1; b <= nmu; ++b)
+    for (int a = 1; a <= nmu; ++a) {
+      volatile float m1 = (float)((double)((float)a - 0.5f) / mu_scale - 1.0);
+      volatile float m2 = (float)((double)((float)b - 0.5f) / mu_scale - 1.0);
+      volatile float t1 = m1 * m1;
+      volatile float s1 = 0.75f - t1;
+      volatile float t2 = m2 * m2;
+      volatile float s2 = s1 - t2;
+      volatile float t3 = m1 * m2;
+      volatile float r = s2 + t3;
+      volatile float sq = std::sqrt((float)r);
+      volatile float v = 1.1547f * sq;
+      volatile float v2 = v * (float)nmu;
+      int m = 1;
+      if (v2 == v2) {
+        float f = std::floor((float)v2);
+        m = (int)f + 1;
+        if (m < 1) m = 1;
+        if (m > nmu) m = nmu;
+      }
+      out[(size_t)(a - 1) + (size_t)nmu * (b - 1)] = (uint8_t)m;
+    }
+}
+
+int set_err(gr_ctx* c, int code, const std::string& m) {
+  if (c) c->err = m;
+  return code;
+}
+
+#define GR_API_BEGIN(ctx)                          \
+  if (!(ctx)) return GR_E_ARG;                     \
+  try {                                            \
+    GR_CUDA_TRY(cudaSetDevice((ctx)->device));
+
+#define GR_API_END(ctx)                            \
+  }                                                \
+  catch (const gr::Error& e) {                     \
+    return set_err((ctx), e.code, e.msg);          \
+  }                                                \
+  catch (const std::bad_alloc&) {                  \
+    return set_err((ctx), GR_E_CAPACITY, "host allocation failed"); \
+  }                                                \
+  catch (...) {                                    \
+    return set_err((ctx), GR_E_CUDA, "unknown error"); \
+  }                                                \
+  return GR_OK;
+
+__global__ void uniform_check_kernel(const double* __restrict__ w, int64_t n_data, int64_t n,
+                                     unsigned char* flag) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double ref = i < n_data ? w[0] : w[n_data];
+    if (__double_as_longlong(w[i]) != __double_as_longlong(ref)) *flag = 0;
+  }
+}
+
+void require_ready(gr_ctx* c) {
+  if (!c->cat_set) throw gr::Error{GR_E_ARG, "catalogue not set (gr_set_catalog)"};
+  if (!c->bins_set) throw gr::Error{GR_E_ARG, "bins not set (gr_set_bins)"};
+}
+
+void ensure_events(gr_ctx* c) {
+  for (int k = 0; k < 4; ++k)
+    if (!c->ev[k]) GR_CUDA_TRY(cudaEventCreate(&c->ev[k]));
+}
+
+float ev_ms(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  return ms;
+}
+
+// Index build + pair parameters (shared by every query).
+void build_index(gr_ctx* c) {
+  cudaStream_t s = c->stream();
+  c->index.build(c->xyz.p, c->w.p, c->has_buffer ? c->buffer.p : nullptr, c->n, c->n_data, c->rmax, s);
+  make_pair_params(c->P, c->rmin, c->rmax, c->nbins, c->nmu, c->logbins, c->index.coord_max,
+                   c->precision == 1);
+  c->csr_valid = false;
+}
+
+void build_csr(gr_ctx* c) {
+  c->csr.build(c->index.view(), c->P, c->stream());
+  c->csr_valid = true;
+}
+
+int round_cap(int64_t maxdeg, int lo, int hi) {
+  int64_t c = ((maxdeg + 31) / 32) * 32;
+  if (c < lo) c = lo;
+  if (c > hi) c = hi;
+  return (int)c;
+}
+
+// product of `ng` galaxy weights and `nr` random weights, left to right
+double uniform_product(double wg, double wr, int ng, int nr) {
+  double p = 1.0;
+  bool first = true;
+  for (int k = 0; k < ng; ++k) {
+    p = first ? wg : p * wg;
+    first = false;
+  }
+  for (int k = 0; k < nr; ++k) {
+    p = first ? wr : p * wr;
+    first = false;
+  }
+  return p;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* gr_version(void) { return "gramsci_b200 0.1 (sm_100a)"; }
+
+int gr_create(gr_ctx** out, int device) {
+  if (!out) return GR_E_ARG;
+  *out = nullptr;
+  gr_ctx* c = nullptr;
+  try {
+    c = new gr_ctx();
+    c->device = device;
+    GR_CUDA_TRY(cudaSetDevice(device));
+    GR_CUDA_TRY(cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking));
+  } catch (const gr::Error& e) {
+    delete c;
+    return e.code;
+  } catch (...) {
+    delete c;
+    return GR_E_CAPACITY;
+  }
+  *out = c;
+  return GR_OK;
+}
+
+int gr_destroy(gr_ctx* c) {
+  if (!c) return GR_E_ARG;
+  cudaSetDevice(c->device);
+  if (c->own) cudaStreamSynchronize(c->own);
+  for (int k = 0; k < 4; ++k)
+    if (c->ev[k]) cudaEventDestroy(c->ev[k]);
+  if (c->own) cudaStreamDestroy(c->own);
+  delete c;
+  return GR_OK;
+}
+
+const char* gr_last_error(const gr_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int gr_set_stream(gr_ctx* c, void* stream) {
+  GR_API_BEGIN(c)
+  c->user = reinterpret_cast<cudaStream_t>(stream);
+  GR_API_END(c)
+}
+
+static int set_catalog_impl(gr_ctx* c, const double* xyz, const double* w, const int32_t* buffer,
+                            int64_t n_data, int64_t n_rand, cudaMemcpyKind kind) {
+  GR_API_BEGIN(c)
+  if (n_data < 0 || n_rand < 0) return set_err(c, GR_E_ARG, "negative catalogue size");
+  int64_t n = n_data + n_rand;
+  if (n >= (int64_t)1 << 31) return set_err(c, GR_E_CAPACITY, "catalogue larger than 2^31-1 points");
+  if (n > 0 && (!xyz || !w)) return set_err(c, GR_E_ARG, "null xyz or w");
+  cudaStream_t s = c->stream();
+  c->xyz.reserve(3 * n + 1);
+  c->w.reserve(n + 1);
+  if (n > 0) {
+    GR_CUDA_TRY(cudaMemcpyAsync(c->xyz.p, xyz, sizeof(double) * 3 * n, kind, s));
+    GR_CUDA_TRY(cudaMemcpyAsync(c->w.p, w, sizeof(double) * n, kind, s));
+  }
+  c->has_buffer = buffer != nullptr;
+  if (buffer) {
+    c->buffer.reserve(n + 1);
+    GR_CUDA_TRY(cudaMemcpyAsync(c->buffer.p, buffer, sizeof(int32_t) * n, kind, s));
+  }
+  c->n = n;
+  c->n_data = n_data;
+  c->n_rand = n_rand;
+  // Uniform weights (all galaxies equal, all randoms equal) let the kernels
+  // keep integer counts only; sums are then count x product.
+  c->uniform_flag.reserve(1);
+  unsigned char one = 1, flag = 1;
+  GR_CUDA_TRY(cudaMemcpyAsync(c->uniform_flag.p, &one, 1, cudaMemcpyHostToDevice, s));
+  if (n > 0) {
+    int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
+    uniform_check_kernel<<<blocks, 256, 0, s>>>(c->w.p, n_data, n, c->uniform_flag.p);
+    GR_CHECK_LAUNCH();
+  }
+  GR_CUDA_TRY(cudaMemcpyAsync(&flag, c->uniform_flag.p, 1, cudaMemcpyDeviceToHost, s));
+  double wg = 0.0, wr = 0.0;
+  if (n_data > 0) GR_CUDA_TRY(cudaMemcpyAsync(&wg, c->w.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (n_rand > 0)
+    GR_CUDA_TRY(cudaMemcpyAsync(&wr, c->w.p + n_data, sizeof(double), cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaStreamSynchronize(s));
+  c->uniform = flag != 0;
+  c->w_gal = wg;
+  c->w_ran = wr;
+  c->cat_set = true;
+  c->csr_valid = false;
+  GR_API_END(c)
+}
+
+int gr_set_catalog(gr_ctx* c, const double* xyz, const double* w, const int32_t* buffer,
+                   int64_t n_data, int64_t n_rand) {
+  return set_catalog_impl(c, xyz, w, buffer, n_data, n_rand, cudaMemcpyHostToDevice);
+}
+
+int gr_set_catalog_dev(gr_ctx* c, const double* xyz, const double* w, const int32_t* buffer,
+                       int64_t n_data, int64_t n_rand) {
+  return set_catalog_impl(c, xyz, w, buffer, n_data, n_rand, cudaMemcpyDeviceToDevice);
+}
+
+int gr_set_bins(gr_ctx* c, double rmin, double rmax, int32_t nbins, int32_t nmu, int32_t logbins) {
+  GR_API_BEGIN(c)
+  if (nbins < 1 || nbins > kMaxBins) return set_err(c, GR_E_ARG, "nbins must be in 1..127");
+  if (nmu < 1 || nmu > kMaxBins) return set_err(c, GR_E_ARG, "nmu must be in 1..127");
+  if (!(rmax > rmin) || !(rmin >= 0.0) || !std::isfinite(rmax))
+    return set_err(c, GR_E_ARG, "need 0 <= rmin < rmax");
+  if (logbins && !(rmin > 0.0)) return set_err(c, GR_E_ARG, "log bins need rmin > 0");
+  c->rmin = rmin;
+  c->rmax = rmax;
+  c->nbins = nbins;
+  c->nmu = nmu;
+  c->logbins = logbins ? 1 : 0;
+  c->bins_set = true;
+  c->csr_valid = false;
+  GR_API_END(c)
+}
+
+int gr_set_option(gr_ctx* c, int32_t key, int64_t value) {
+  GR_API_BEGIN(c)
+  if (key == GR_OPT_PRECISION) {
+    if (value != 0 && value != 1) return set_err(c, GR_E_ARG, "precision must be 0 or 1");
+    c->precision = (int)value;
+  } else if (key == GR_OPT_TIMEOUT_MS) {
+    if (value <= 0) return set_err(c, GR_E_ARG, "timeout must be positive");
+    c->timeout_ms = value;
+  } else {
+    return set_err(c, GR_E_UNSUPPORTED, "unknown option");
+  }
+  GR_API_END(c)
+}
+
+int gr_count_2pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* catsum) {
+  GR_API_BEGIN(c)
+  require_ready(c);
+  ensure_events(c);
+  cudaStream_t s = c->stream();
+  const int nbm = c->nbins * c->nmu, nh = nbm * 4;
+  const bool weighted = !c->uniform;
+  c->hcnt.reserve(nh);
+  c->hsum.reserve(nh);
+  c->stats.reserve(8);
+  GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
+  build_index(c);
+  GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nh, s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->hsum.p, 0, sizeof(double) * nh, s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
+  launch_pair2(c->index.view(), c->P, weighted, c->hcnt.p, c->hsum.p, c->stats.p, s);
+  GR_CUDA_TRY(cudaEventRecord(c->ev[2], s));
+  std::vector<unsigned long long> hc(nh);
+  std::vector<double> hs(nh, 0.0);
+  unsigned long long st[8];
+  GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
+  if (weighted)
+    GR_CUDA_TRY(cudaMemcpyAsync(hs.data(), c->hsum.p, sizeof(double) * nh, cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
+  GR_CUDA_TRY(cudaStreamSynchronize(s));
+  if (!weighted) {
+    for (int cat = 0; cat < 4; ++cat) {
+      double prod = uniform_product(c->w_gal, c->w_ran, 2 - ((cat >> 1) + (cat & 1)),
+                                    (cat >> 1) + (cat & 1));
+      for (int k = 0; k < nbm; ++k) hs[k + nbm * cat] = (double)hc[k + nbm * cat] * prod;
+    }
+  }
+  int64_t rooted = 0;
+  for (int k = 0; k < nh; ++k) rooted += (int64_t)hc[k];
+  for (int k = 0; k < nbm; ++k) {
+    if (N2) N2[k] = ((hs[k] + hs[k + nbm]) + hs[k + 2 * nbm]) + hs[k + 3 * nbm];
+    if (N3) N3[k] = hs[k + 3 * nbm];
+  }
+  if (counts)
+    for (int k = 0; k < nh; ++k) counts[k] = (int64_t)hc[k];
+  if (catsum)
+    for (int k = 0; k < nh; ++k) catsum[k] = hs[k];
+  std::memset(&c->st, 0, sizeof(c->st));
+  c->st.ms_index = ev_ms(c->ev[0], c->ev[1]);
+  c->st.ms_graph = 0.0;
+  c->st.ms_query = ev_ms(c->ev[1], c->ev[2]);
+  c->st.ms_total = ev_ms(c->ev[0], c->ev[2]);
+  c->st.n_points = c->n;
+  c->st.n_edges = 2 * (int64_t)st[2];
+  c->st.tuples = (int64_t)st[2];
+  c->st.rooted = rooted;
+  c->st.fp64_rechecks = (int64_t)st[0];
+  c->st.candidates = (int64_t)st[1];
+  c->st.kernel_launches = c->index.launches + 1;
+  GR_API_END(c)
+}
+
+int gr_count_3pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* catsum) {
+  GR_API_BEGIN(c)
+  require_ready(c);
+  ensure_events(c);
+  cudaStream_t s = c->stream();
+  const int nmu = c->nmu;
+  const int ncfg = (int)(((int64_t)c->nbins * (c->nbins + 1) * (c->nbins + 2)) / 6);
+  const int nbin = ncfg * nmu, nh = nbin * 4;
+  const bool weighted = !c->uniform;
+  c->hcnt.reserve(nh);
+  c->hsum.reserve(nh);
+  c->stats.reserve(8);
+  std::vector<uint8_t> nt;
+  normal_table(nmu, nt);
+  c->normal_dev.reserve(nt.size());
+  GR_CUDA_TRY(cudaMemcpyAsync(c->normal_dev.p, nt.data(), nt.size(), cudaMemcpyHostToDevice, s));
+  GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
+  build_index(c);
+  GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+  build_csr(c);
+  GR_CUDA_TRY(cudaEventRecord(c->ev[2], s));
+  unsigned long long gst[4];
+  GR_CUDA_TRY(cudaMemcpyAsync(gst, c->csr.stats.p, sizeof(gst), cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nh, s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->hsum.p, 0, sizeof(double) * nh, s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
+  GR_CUDA_TRY(cudaStreamSynchronize(s));
+  TriParams T;
+  T.nbins = c->nbins;
+  T.nmu = nmu;
+  T.ncfg = ncfg;
+  T.rsd = nmu >= 2;
+  T.cap = round_cap((int64_t)gst[2], 32, 256);
+  T.normal = c->normal_dev.p;
+  make_rank_tables(T.rank, c->nbins, 3);
+  CSRView G{c->csr.row_ptr.p, c->csr.col.p, c->csr.meta.p, c->csr.deg_full.p};
+  cudaEvent_t q0;
+  GR_CUDA_TRY(cudaEventCreate(&q0));
+  GR_CUDA_TRY(cudaEventRecord(q0, s));
+  launch_tri3(c->index.view(), G, T, weighted, c->hcnt.p, c->hsum.p, c->stats.p, s);
+  GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
+  std::vector<unsigned long long> hc(nh);
+  std::vector<double> hs(nh, 0.0);
+  unsigned long long st[8];
+  GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
+  if (weighted)
+    GR_CUDA_TRY(cudaMemcpyAsync(hs.data(), c->hsum.p, sizeof(double) * nh, cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaStreamSynchronize(s));
+  if (!weighted) {
+    for (int nr = 0; nr < 4; ++nr) {
+      double prod = uniform_product(c->w_gal, c->w_ran, 3 - nr, nr);
+      for (int k = 0; k < nbin; ++k) hs[k + nbin * nr] = (double)hc[k + nbin * nr] * prod;
+    }
+  }
+  for (int k = 0; k < nbin; ++k) {
+    if (N2) N2[k] = ((hs[k] + hs[k + nbin]) + hs[k + 2 * nbin]) + hs[k + 3 * nbin];
+    if (N3) N3[k] = -hs[k + 3 * nbin];
+  }
+  if (counts)
+    for (int k = 0; k < nh; ++k) counts[k] = (int64_t)hc[k];
+  if (catsum)
+    for (int k = 0; k < nh; ++k) catsum[k] = hs[k];
+  std::memset(&c->st, 0, sizeof(c->st));
+  c->st.ms_index = ev_ms(c->ev[0], c->ev[1]);
+  c->st.ms_graph = ev_ms(c->ev[1], c->ev[2]);
+  c->st.ms_query = ev_ms(q0, c->ev[3]);
+  c->st.ms_total = c->st.ms_index + c->st.ms_graph + c->st.ms_query;
+  cudaEventDestroy(q0);
+  c->st.n_points = c->n;
+  c->st.n_edges = 2 * c->csr.n_edges;
+  c->st.tuples = (int64_t)st[0];
+  c->st.rooted = (int64_t)st[1];
+  c->st.fp64_rechecks = (int64_t)gst[0];
+  c->st.candidates = (int64_t)gst[1];
+  c->st.kernel_launches = c->index.launches + c->csr.launches + 1;
+  GR_API_END(c)
+}
+
+int gr_count_4pcf(gr_ctx* c, double* N2, double* N3, double* discN, double* discR,
+                  int64_t* counts, double* catsum, int64_t* dcount, double* dsum) {
+  GR_API_BEGIN(c)
+  require_ready(c);
+  ensure_events(c);
+  cudaStream_t s = c->stream();
+  const int nb = c->nbins;
+  const int64_t ncfg64 = ((int64_t)nb * (nb + 1) * (nb + 2) * (nb + 3)) / 24;
+  const int64_t nbin64 = ncfg64 * nb * nb;
+  if (nbin64 * 29 > ((int64_t)1 << 31)) return set_err(c, GR_E_CAPACITY, "4PCF histogram too large");
+  const int ncfg = (int)ncfg64, nbin = (int)nbin64;
+  const int nh = nbin * 5, nd = nbin * 24;
+  const bool weighted = !c->uniform;
+  c->hcnt.reserve(nh);
+  c->hsum.reserve(nh);
+  c->dcnt.reserve(nd);
+  c->dsum.reserve(nd);
+  c->stats.reserve(8);
+  GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
+  build_index(c);
+  GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+  build_csr(c);
+  GR_CUDA_TRY(cudaEventRecord(c->ev[2], s));
+  unsigned long long gst[4];
+  GR_CUDA_TRY(cudaMemcpyAsync(gst, c->csr.stats.p, sizeof(gst), cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nh, s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->hsum.p, 0, sizeof(double) * nh, s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->dcnt.p, 0, sizeof(unsigned long long) * nd, s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->dsum.p, 0, sizeof(double) * nd, s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
+  GR_CUDA_TRY(cudaStreamSynchronize(s));
+  if ((int64_t)gst[2] > 1024)
+    return set_err(c, GR_E_CAPACITY, "4PCF: a point has more than 1024 larger-label neighbours");
+  QuadParams Q;
+  Q.nbins = nb;
+  Q.ncfg = ncfg;
+  Q.cap = round_cap((int64_t)gst[2], 32, 1024);
+  make_rank_tables(Q.rank, nb, 4);
+  CSRView G{c->csr.row_ptr.p, c->csr.col.p, c->csr.meta.p, c->csr.deg_full.p};
+  cudaEvent_t q0;
+  GR_CUDA_TRY(cudaEventCreate(&q0));
+  GR_CUDA_TRY(cudaEventRecord(q0, s));
+  launch_quad4(c->index.view(), G, Q, weighted, c->hcnt.p, c->hsum.p, c->dcnt.p, c->dsum.p,
+               c->stats.p, s);
+  GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
+  std::vector<unsigned long long> hc(nh), dc(nd);
+  std::vector<double> hs(nh, 0.0), ds(nd, 0.0);
+  unsigned long long st[8];
+  GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaMemcpyAsync(dc.data(), c->dcnt.p, sizeof(unsigned long long) * nd, cudaMemcpyDeviceToHost, s));
+  if (weighted) {
+    GR_CUDA_TRY(cudaMemcpyAsync(hs.data(), c->hsum.p, sizeof(double) * nh, cudaMemcpyDeviceToHost, s));
+    GR_CUDA_TRY(cudaMemcpyAsync(ds.data(), c->dsum.p, sizeof(double) * nd, cudaMemcpyDeviceToHost, s));
+  }
+  GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaStreamSynchronize(s));
+  if (!weighted) {
+    for (int nr = 0; nr < 5; ++nr) {
+      double prod = uniform_product(c->w_gal, c->w_ran, 4 - nr, nr);
+      for (int k = 0; k < nbin; ++k) hs[k + (size_t)nbin * nr] = (double)hc[k + (size_t)nbin * nr] * prod;
+    }
+    for (int cat = 0; cat < 4; ++cat) {
+      int npr = cat == 3 ? 2 : cat;
+      double prod = uniform_product(c->w_gal, c->w_ran, 2 - npr, npr);
+      for (int k = 0; k < nbin * 6; ++k)
+        ds[k + (size_t)nbin * 6 * cat] = (double)dc[k + (size_t)nbin * 6 * cat] * prod;
+    }
+  }
+  for (int k = 0; k < nbin; ++k) {
+    double acc = 0.0;
+    for (int nr = 0; nr < 5; ++nr) acc += hs[k + (size_t)nbin * nr];
+    if (N2) N2[k] = acc;
+    if (N3) N3[k] = hs[k + (size_t)nbin * 4];
+  }
+  for (int k = 0; k < nbin * 6; ++k) {
+    if (discN) discN[k] = (ds[k] + ds[k + (size_t)nbin * 6]) + ds[k + (size_t)nbin * 12];
+    if (discR) discR[k] = ds[k + (size_t)nbin * 18];
+  }
+  if (counts)
+    for (int k = 0; k < nh; ++k) counts[k] = (int64_t)hc[k];
+  if (catsum)
+    for (int k = 0; k < nh; ++k) catsum[k] = hs[k];
+  if (dcount)
+    for (int k = 0; k < nd; ++k) dcount[k] = (int64_t)dc[k];
+  if (dsum)
+    for (int k = 0; k < nd; ++k) dsum[k] = ds[k];
+  std::memset(&c->st, 0, sizeof(c->st));
+  c->st.ms_index = ev_ms(c->ev[0], c->ev[1]);
+  c->st.ms_graph = ev_ms(c->ev[1], c->ev[2]);
+  c->st.ms_query = ev_ms(q0, c->ev[3]);
+  c->st.ms_total = c->st.ms_index + c->st.ms_graph + c->st.ms_query;
+  cudaEventDestroy(q0);
+  c->st.n_points = c->n;
+  c->st.n_edges = 2 * c->csr.n_edges;
+  c->st.tuples = (int64_t)st[0];
+  c->st.rooted = (int64_t)st[1];
+  c->st.fp64_rechecks = (int64_t)gst[0];
+  c->st.candidates = (int64_t)gst[1];
+  c->st.kernel_launches = c->index.launches + c->csr.launches + 1;
+  GR_API_END(c)
+}
+
+int gr_graph_build(gr_ctx* c) {
+  GR_API_BEGIN(c)
+  require_ready(c);
+  build_index(c);
+  build_csr(c);
+  GR_CUDA_TRY(cudaStreamSynchronize(c->stream()));
+  GR_API_END(c)
+}
+
+int gr_graph_nedges(gr_ctx* c, int64_t* n_edges) {
+  GR_API_BEGIN(c)
+  if (!n_edges) return set_err(c, GR_E_ARG, "null output");
+  if (!c->csr_valid) {
+    require_ready(c);
+    build_index(c);
+    build_csr(c);
+  }
+  *n_edges = 2 * c->csr.n_edges;
+  GR_API_END(c)
+}
+
+int gr_graph_export(gr_ctx* c, int64_t* row_ptr, int32_t* col, uint8_t* bin, uint8_t* mu) {
+  GR_API_BEGIN(c)
+  if (!c->csr_valid) {
+    require_ready(c);
+    build_index(c);
+    build_csr(c);
+  }
+  cudaStream_t s = c->stream();
+  const int64_t n = c->n, E = c->csr.n_edges;
+  std::vector<int64_t> rp(n + 1);
+  std::vector<int> cl(E), orig(n);
+  std::vector<uint32_t> mt(E);
+  GR_CUDA_TRY(cudaMemcpyAsync(rp.data(), c->csr.row_ptr.p, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, s));
+  if (E > 0) {
+    GR_CUDA_TRY(cudaMemcpyAsync(cl.data(), c->csr.col.p, sizeof(int) * E, cudaMemcpyDeviceToHost, s));
+    GR_CUDA_TRY(cudaMemcpyAsync(mt.data(), c->csr.meta.p, sizeof(uint32_t) * E, cudaMemcpyDeviceToHost, s));
+  }
+  if (n > 0)
+    GR_CUDA_TRY(cudaMemcpyAsync(orig.data(), c->index.orig.p, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaStreamSynchronize(s));
+  // expand the upper rows into the reference's symmetric, id-sorted rows
+  std::vector<int64_t> deg(n + 1, 0);
+  for (int64_t p = 0; p < n; ++p)
+    for (int64_t e = rp[p]; e < rp[p + 1]; ++e) {
+      deg[orig[p]]++;
+      deg[orig[cl[e]]]++;
+    }
+  std::vector<int64_t> out_ptr(n + 1, 0);
+  for (int64_t i = 0; i < n; ++i) out_ptr[i + 1] = out_ptr[i] + deg[i];
+  std::vector<int64_t> fill(out_ptr.begin(), out_ptr.end() - 1);
+  std::vector<uint64_t> ent(2 * E);
+  for (int64_t p = 0; p < n; ++p)
+    for (int64_t e = rp[p]; e < rp[p + 1]; ++e) {
+      int i = orig[p], j = orig[cl[e]];
+      uint32_t m = mt[e];
+      uint64_t b = m & 0xff, mf = (m >> 8) & 0xff, mr = (m >> 16) & 0xff;
+      ent[fill[i]++] = ((uint64_t)j << 16) | (b << 8) | mf;
+      ent[fill[j]++] = ((uint64_t)i << 16) | (b << 8) | mr;
+    }
+  for (int64_t i = 0; i < n; ++i) std::sort(ent.begin() + out_ptr[i], ent.begin() + out_ptr[i + 1]);
+  if (row_ptr) std::copy(out_ptr.begin(), out_ptr.end(), row_ptr);
+  for (int64_t k = 0; k < 2 * E; ++k) {
+    if (col) col[k] = (int32_t)(ent[k] >> 16);
+    if (bin) bin[k] = (uint8_t)((ent[k] >> 8) & 0xff);
+    if (mu) mu[k] = (uint8_t)(ent[k] & 0xff);
+  }
+  GR_API_END(c)
+}
+
+int gr_get_stats(gr_ctx* c, gr_stats* out) {
+  if (!c || !out) return GR_E_ARG;
+  *out = c->st;
+  return GR_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,54 @@
+// Device cell index and upper-triangular CSR adjacency.
+#pragma once
+
+#include <algorithm>
+#include <cstring>
+
+#include "gr_internal.cuh"
+
+namespace gr {
+
+// Uniform-grid index over the catalogue, points laid out in cell order.
+struct CellIndex {
+  int64_t n = 0, n_data = 0;
+  double coord_max = 0.0;  // max |coordinate|, bounds the FP32 rounding error
+  GridParams grid{};
+  int launches = 0;
+  DevBuf<unsigned long long> bbox_raw;
+  DevBuf<int> cell_count, key_orig, slot, tmp_perm, perm, cell_start, orig, cell_key;
+  DevBuf<int64_t> cell_start64, scan_tmp;
+  DevBuf<float4> pos4;
+  DevBuf<double4> posd;
+  DevBuf<double> w;
+  DevBuf<uint8_t> flags;
+
+  void build(const double* d_xyz, const double* d_w, const int* d_buffer, int64_t n, int64_t n_data,
+             double rmax, cudaStream_t s);
+  DevCatalog view() const;
+};
+
+void narrow_kernel_launch(const int64_t* in, int* out, int64_t n, cudaStream_t s);
+
+// Upper adjacency: row p lists the neighbours q > p (internal labels) of the
+// (rmin, rmax) graph in increasing label order, with packed bin / mu
+// metadata.  deg_full[p] is the full degree (the reference's row length nn).
+struct UpperCSR {
+  int64_t n = 0, n_edges = 0;  // n_edges counts upper (undirected) edges
+  int launches = 0;
+  DevBuf<int> deg_up, deg_full;
+  DevBuf<int64_t> row_ptr, scan_tmp;
+  DevBuf<int> col;
+  DevBuf<uint32_t> meta;
+  DevBuf<unsigned long long> stats;  // [0] FP64 rechecks, [1] candidates
+
+  void build(const DevCatalog& C, const PairParams& P, cudaStream_t s);
+};
+
+struct CSRView {
+  const int64_t* row_ptr;
+  const int* col;
+  const uint32_t* meta;
+  const int* deg_full;
+};
+
+}  // namespace gr

@@ -1,0 +1,313 @@
+// Internal declarations shared by the CUDA translation units of
+// libgramsci_cuda.so: the pair predicate (FP32 fast path with an FP64 guard
+// band, and the exact FP64 reference form), cell-grid helpers, tuple-rank
+// tables and small device utilities.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <string>
+#include <vector>
+
+namespace gr {
+
+// ------------------------------------------------------------------ errors --
+struct Error {
+  int code;
+  std::string msg;
+};
+
+#define GR_CUDA_TRY(call)                                                     \
+  do {                                                                        \
+    cudaError_t _e = (call);                                                  \
+    if (_e != cudaSuccess)                                                    \
+      throw ::gr::Error{-3, std::string(#call) + ": " + cudaGetErrorString(_e)}; \
+  } while (0)
+
+#define GR_CHECK_LAUNCH() GR_CUDA_TRY(cudaGetLastError())
+
+// ------------------------------------------------------------ device buffer --
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;  // capacity in elements
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  // Grow to at least `count` elements (contents are not preserved).
+  void reserve(size_t count) {
+    if (count <= n && p) return;
+    release();
+    size_t c = count > 0 ? count : 1;
+    GR_CUDA_TRY(cudaMalloc(&p, c * sizeof(T)));
+    n = c;
+  }
+};
+
+// ------------------------------------------------------------ pair predicate --
+// Everything a kernel needs to decide whether (i, j) is an edge of the
+// reference graph and which radial / mu bins it falls in.
+struct PairParams {
+  // exact FP64 form (src/gramsci.F90:136-147, 295-340)
+  double rmin, rmax, rmin2, rmax2, inv_dr, log_rmin, mu_scale;
+  int nbins, nmu, logbins, rsd;
+  // FP32 fast path with guard band
+  int f32;           // 1 = FP32 path enabled
+  float f_rmin, f_inv_dr, f_mu_scale;
+  float rmax2_hi;    // d2 >= rmax2_hi: certainly d >= rmax
+  float rmin2_lo;    // d2 <= rmin2_lo: certainly d <= rmin (or -1)
+  float tguard;      // |t - nearest integer| below this -> FP64
+  float d0;          // bound on |d_f - d_true|
+  float eA, eB, mB, eC;  // cosine error model eA/(d-d0) + eB/(|m|-mB) + eC
+  float f_nmu;
+};
+
+// Host: fill PairParams.  coord_max bounds |x|,|y|,|z| over the catalogue.
+void make_pair_params(PairParams& P, double rmin, double rmax, int nbins, int nmu, int logbins,
+                      double coord_max, int force_fp64);
+
+__device__ __forceinline__ int mu_bin_f64(double th, const PairParams& P) {
+  double v = __dmul_rn(__dadd_rn(th, 1.0), P.mu_scale);
+  if (!(v == v)) return 1;
+  double f = floor(v);
+  if (f < -1.0e9) return 1;
+  if (f > 1.0e9) return P.nmu;
+  int m = (int)f + 1;
+  m = m < 1 ? 1 : m;
+  m = m > P.nmu ? P.nmu : m;
+  return m;
+}
+
+// Exact reference predicate in FP64 (separate IEEE multiply / add, no FMA),
+// root pi, neighbour pj.  Identical arithmetic to the CPU oracle.
+__device__ __forceinline__ bool edge_f64(const double4 pi, const double4 pj, const PairParams& P,
+                                         int& bin, int& muf, int& mur) {
+  double dx = __dsub_rn(pj.x, pi.x);
+  double dy = __dsub_rn(pj.y, pi.y);
+  double dz = __dsub_rn(pj.z, pi.z);
+  double sd = __dmul_rn(dx, dx);
+  sd = __dadd_rn(sd, __dmul_rn(dy, dy));
+  sd = __dadd_rn(sd, __dmul_rn(dz, dz));
+  if (sd > P.rmax2) return false;
+  if (P.rmin > 0.0 && sd <= P.rmin2) return false;
+  double d = __dsqrt_rn(sd);
+  if (d <= P.rmin || d >= P.rmax) return false;
+  double t;
+  if (P.logbins)
+    t = __dmul_rn(__dsub_rn(log10(d), P.log_rmin), P.inv_dr);
+  else
+    t = __dmul_rn(__dsub_rn(d, P.rmin), P.inv_dr);
+  int b = (int)floor(t) + 1;
+  b = b > P.nbins ? P.nbins : b;
+  b = b < 1 ? 1 : b;
+  bin = b;
+  if (P.rsd) {
+    double m0 = __dmul_rn(0.5, __dadd_rn(pi.x, pj.x));
+    double m1 = __dmul_rn(0.5, __dadd_rn(pi.y, pj.y));
+    double m2 = __dmul_rn(0.5, __dadd_rn(pi.z, pj.z));
+    double s0 = __dsub_rn(pi.x, pj.x);
+    double s1 = __dsub_rn(pi.y, pj.y);
+    double s2 = __dsub_rn(pi.z, pj.z);
+    double th = __dmul_rn(m0, s0);
+    th = __dadd_rn(th, __dmul_rn(m1, s1));
+    th = __dadd_rn(th, __dmul_rn(m2, s2));
+    double nm = __dmul_rn(m0, m0);
+    nm = __dadd_rn(nm, __dmul_rn(m1, m1));
+    nm = __dadd_rn(nm, __dmul_rn(m2, m2));
+    double ns = __dmul_rn(s0, s0);
+    ns = __dadd_rn(ns, __dmul_rn(s1, s1));
+    ns = __dadd_rn(ns, __dmul_rn(s2, s2));
+    th = __ddiv_rn(th, __dmul_rn(__dsqrt_rn(nm), __dsqrt_rn(ns)));
+    muf = mu_bin_f64(th, P);
+    mur = mu_bin_f64(-th, P);
+  } else {
+    muf = 1;
+    mur = 1;
+  }
+  return true;
+}
+
+// FP32 classification.  Returns 0: certainly not an edge; 1: edge with the
+// bins written; 2: inside the guard band, re-evaluate with edge_f64.
+// NEED_BINS=false only decides membership (guards only at rmin and rmax).
+template <bool NEED_BINS>
+__device__ __forceinline__ int classify_f32(const float4 pi, const float4 pj, const PairParams& P,
+                                            int& bin, int& muf, int& mur) {
+  float dx = pj.x - pi.x;
+  float dy = pj.y - pi.y;
+  float dz = pj.z - pi.z;
+  float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+  if (d2 >= P.rmax2_hi || d2 <= P.rmin2_lo) return 0;
+  float d = __fsqrt_rn(d2);
+  float t = (d - P.f_rmin) * P.f_inv_dr;
+  float tn = rintf(t);
+  if (NEED_BINS) {
+    if (fabsf(t - tn) < P.tguard) return 2;
+  } else {
+    if ((tn == 0.0f || tn == (float)P.nbins) && fabsf(t - tn) < P.tguard) return 2;
+  }
+  if (t <= 0.0f || t >= (float)P.nbins) return 0;
+  if (!NEED_BINS) return 1;
+  bin = (int)t + 1;
+  if (P.rsd) {
+    float dd = d - P.d0;
+    float mx = 0.5f * (pi.x + pj.x);
+    float my = 0.5f * (pi.y + pj.y);
+    float mz = 0.5f * (pi.z + pj.z);
+    float mm = __fsqrt_rn(fmaf(mz, mz, fmaf(my, my, mx * mx)));
+    float mmm = mm - P.mB;
+    if (dd <= 0.0f || mmm <= 0.0f) return 2;
+    float dot = fmaf(mz, -dz, fmaf(my, -dy, mx * -dx));
+    float th = dot / (mm * d);
+    float eth = P.eA / dd + P.eB / mmm + P.eC;
+    float ug = eth * P.f_mu_scale + 8.0f * 5.96046448e-8f * P.f_nmu;
+    float u1 = (th + 1.0f) * P.f_mu_scale;
+    float u2 = (1.0f - th) * P.f_mu_scale;
+    float k1 = rintf(u1), k2 = rintf(u2);
+    if (k1 >= 1.0f && k1 <= P.f_nmu - 1.0f && fabsf(u1 - k1) < ug) return 2;
+    if (k2 >= 1.0f && k2 <= P.f_nmu - 1.0f && fabsf(u2 - k2) < ug) return 2;
+    int a = (int)floorf(u1) + 1;
+    int b = (int)floorf(u2) + 1;
+    muf = a < 1 ? 1 : (a > P.nmu ? P.nmu : a);
+    mur = b < 1 ? 1 : (b > P.nmu ? P.nmu : b);
+  } else {
+    muf = 1;
+    mur = 1;
+  }
+  return 1;
+}
+
+// ---------------------------------------------------------------- cell grid --
+struct GridParams {
+  int nx, ny, nz;
+  int64_t ncell;
+};
+
+// Forward (half-stencil) candidate ranges of a root at internal label p in
+// cell `key`: labels q > p in the root's own cell and the 13 neighbouring
+// cells that follow it in key order, as at most 5 contiguous label ranges in
+// increasing order.
+struct Ranges {
+  int n;
+  int beg[5], end[5];
+};
+
+__device__ __forceinline__ void forward_ranges(int p, int key, const GridParams& g,
+                                               const int* __restrict__ cell_start, Ranges& R) {
+  int cx = key % g.nx;
+  int cy = (key / g.nx) % g.ny;
+  int cz = key / (g.nx * g.ny);
+  int x0 = cx > 0 ? cx - 1 : 0;
+  int x1 = cx + 1 < g.nx ? cx + 1 : cx;
+  R.n = 0;
+  {
+    int e = cell_start[key + (cx + 1 < g.nx ? 2 : 1)];
+    if (e > p + 1) {
+      R.beg[R.n] = p + 1;
+      R.end[R.n] = e;
+      R.n++;
+    }
+  }
+  if (cy + 1 < g.ny) {
+    int kb = (cz * g.ny + cy + 1) * g.nx;
+    int b = cell_start[kb + x0], e = cell_start[kb + x1 + 1];
+    if (e > b) {
+      R.beg[R.n] = b;
+      R.end[R.n] = e;
+      R.n++;
+    }
+  }
+  if (cz + 1 < g.nz) {
+    for (int dy = -1; dy <= 1; ++dy) {
+      int y = cy + dy;
+      if (y < 0 || y >= g.ny) continue;
+      int kb = ((cz + 1) * g.ny + y) * g.nx;
+      int b = cell_start[kb + x0], e = cell_start[kb + x1 + 1];
+      if (e > b) {
+        R.beg[R.n] = b;
+        R.end[R.n] = e;
+        R.n++;
+      }
+    }
+  }
+}
+
+// Map flattened candidate index f (0 <= f < total) to a label.
+__device__ __forceinline__ int range_label(const Ranges& R, const int* pre, int f) {
+  int r = 0;
+#pragma unroll
+  for (int k = 1; k < 5; ++k)
+    if (k < R.n && f >= pre[k]) r = k;
+  return R.beg[r] + (f - pre[r]);
+}
+
+// --------------------------------------------------------- tuple rank tables --
+// Rank (1-based) of a non-decreasing k-tuple over [1, n] in lexicographic
+// order, as create_binlookup numbers configurations
+// (src/gramsci.F90:1398-1477).  F[j][v] = sum_{u<v} C(n-u+1 + (k-j-1) - 1, k-j-1)
+// so rank = 1 + sum_j (F[j][x_j] - F[j][x_{j-1}]).
+constexpr int kMaxBins = 127;
+struct RankTables {
+  int n;
+  int k;
+  int F[4][kMaxBins + 2];
+};
+void make_rank_tables(RankTables& T, int n, int k);
+
+__device__ __forceinline__ int rank_sorted3(const RankTables& T, int a, int b, int c) {
+  // a <= b <= c, 1-based
+  return 1 + (T.F[0][a] - T.F[0][1]) + (T.F[1][b] - T.F[1][a]) + (T.F[2][c] - T.F[2][b]);
+}
+
+__device__ __forceinline__ int rank_sorted4(const RankTables& T, int a, int b, int c, int d) {
+  return 1 + (T.F[0][a] - T.F[0][1]) + (T.F[1][b] - T.F[1][a]) + (T.F[2][c] - T.F[2][b]) +
+         (T.F[3][d] - T.F[3][c]);
+}
+
+__device__ __forceinline__ void sort3i(int& a, int& b, int& c) {
+  int t;
+  if (a > b) { t = a; a = b; b = t; }
+  if (b > c) { t = b; b = c; c = t; }
+  if (a > b) { t = a; a = b; b = t; }
+}
+
+// Packed edge metadata of the upper CSR: radial bin, mu seen from the row's
+// point, mu seen from the neighbour.
+__device__ __forceinline__ uint32_t pack_meta(int bin, int muf, int mur) {
+  return (uint32_t)bin | ((uint32_t)muf << 8) | ((uint32_t)mur << 16);
+}
+__device__ __forceinline__ int meta_bin(uint32_t m) { return (int)(m & 0xff); }
+__device__ __forceinline__ int meta_muf(uint32_t m) { return (int)((m >> 8) & 0xff); }
+__device__ __forceinline__ int meta_mur(uint32_t m) { return (int)((m >> 16) & 0xff); }
+
+// ---------------------------------------------------------- device catalogue --
+// Points in cell order ("internal labels").  orig[p] is the position in the
+// reference's catalogue order; random = orig >= n_data.
+struct DevCatalog {
+  const float4* pos4;    // float x, y, z, (unused)
+  const double4* posd;   // double x, y, z, w
+  const double* w;       // weight
+  const int* orig;       // original index
+  const uint8_t* flags;  // bit0 random, bit1 buffer
+  const int* cell_key;   // cell of each point
+  const int* cell_start; // ncell + 1
+  int n;
+  int n_data;
+  GridParams grid;
+};
+
+enum : uint8_t { FLAG_RANDOM = 1, FLAG_BUFFER = 2 };
+
+// -------------------------------------------------------------- host launch --
+// Exclusive scan of n int32 values into n+1 int64 values (out[n] = total).
+void scan_i32_to_i64(const int* in, int64_t* out, int64_t n, cudaStream_t s, DevBuf<int64_t>& tmp);
+
+}  // namespace gr

@@ -1,0 +1,139 @@
+/*
+ * gramsci_cuda.h -- C ABI of the B200 N-point correlation library
+ * (libgramsci_cuda.so).
+ *
+ * The reference program (csabiu/Gramsci, Fortran 90) has no plugin or FFI
+ * layer: its hot path is a chain of internal subroutines that share module
+ * globals.  Each entry point below replaces one of those seams, so a host
+ * program (the Fortran driver through iso_c_binding, the C++ `gramsci` CLI,
+ * or Python through ctypes) can swap the CPU code for this library without
+ * changing the program's inputs, outputs or CLI.
+ *
+ * Conventions
+ *  - Every function returns a status: GR_OK (0) or a negative GR_E_* code;
+ *    gr_last_error() gives the message.  No C++ exception crosses the ABI.
+ *  - Point ids are positions in the catalogue as the reference orders it:
+ *    galaxies first (0 .. n_data-1), then randoms.  Ids in exported graphs are
+ *    0-based (the Fortran host adds 1).
+ *  - Output arrays are caller-allocated HOST memory in Fortran (column-major)
+ *    order with the shapes documented per function.  A NULL output pointer
+ *    means "not wanted".
+ *  - One context per host thread.  Calls are synchronous: they return after
+ *    the work on the context's stream has finished.
+ *  - Radial bins are 1..nbins and mu bins 1..nmu as in the reference; both
+ *    must be <= 127 because the reference stores them as int8
+ *    (src/node_module.F90:7).
+ */
+#ifndef GRAMSCI_CUDA_H
+#define GRAMSCI_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GR_OK 0
+#define GR_E_ARG (-1)         /* invalid argument or call order            */
+#define GR_E_CAPACITY (-2)    /* a size exceeds what the library supports  */
+#define GR_E_CUDA (-3)        /* CUDA runtime error                        */
+#define GR_E_TIMEOUT (-4)     /* a bounded device wait ran out             */
+#define GR_E_UNSUPPORTED (-5) /* option not available                      */
+
+typedef struct gr_ctx gr_ctx;
+
+/* Options for gr_set_option. */
+#define GR_OPT_PRECISION 1 /* 0: FP32 separations + FP64 guard band (default); 1: FP64 throughout */
+#define GR_OPT_TIMEOUT_MS 2 /* bound on device-side waits in the persistent batched kernel */
+
+/* Run statistics of the last count call (gr_get_stats). */
+typedef struct gr_stats {
+  double ms_index;        /* cell index build (device time)                     */
+  double ms_graph;        /* CSR adjacency build (device time), 0 for 2PCF      */
+  double ms_query;        /* counting kernel(s) (device time)                   */
+  double ms_total;        /* whole call on the device                           */
+  int64_t n_points;
+  int64_t n_edges;        /* directed edges of the (rmin, rmax) graph            */
+  int64_t tuples;         /* distinct pairs / triangles / 4-cliques binned       */
+  int64_t rooted;         /* rooted incidences (the reference's loop count)      */
+  int64_t fp64_rechecks;  /* pairs re-evaluated in FP64 inside the guard band    */
+  int64_t candidates;     /* candidate pairs tested                              */
+  int64_t kernel_launches;/* kernels launched by the call                        */
+} gr_stats;
+
+/* Library version string. */
+const char* gr_version(void);
+
+/* Context lifetime.  Replaces the program-global state of Ngramsci
+ * (src/gramsci.F90:13-38). */
+int gr_create(gr_ctx** out, int device);
+int gr_destroy(gr_ctx* ctx);
+const char* gr_last_error(const gr_ctx* ctx);
+
+/* Use a caller-owned CUDA stream (cudaStream_t passed as void*); NULL
+ * restores the context's own stream. */
+int gr_set_stream(gr_ctx* ctx, void* stream);
+
+/* Catalogue.  Replaces read_files_2's result (src/gramsci.F90:1364-1396):
+ *   xyz    points(3,N) in Fortran order, i.e. x,y,z interleaved, N = n_data+n_rand
+ *   w      signed normalised weights exactly as after gramsci.F90:1390-1391
+ *   buffer 0/1 per point (1 = buffer point, never a root; gramsci.F90:363) or NULL
+ * gr_set_catalog copies from host memory; gr_set_catalog_dev takes device
+ * pointers (device-resident inputs) and copies them device-to-device. */
+int gr_set_catalog(gr_ctx* ctx, const double* xyz, const double* w, const int32_t* buffer,
+                   int64_t n_data, int64_t n_rand);
+int gr_set_catalog_dev(gr_ctx* ctx, const double* xyz, const double* w, const int32_t* buffer,
+                       int64_t n_data, int64_t n_rand);
+
+/* Binning.  Replaces the CLI values rmin/rmax/nbins/nmu/-log and the derived
+ * delta_r, inv_delta_r, mu_scale (src/gramsci.F90:136-147, 1216-1223).
+ * RSD (line-of-sight binning) is on when nmu >= 2. */
+int gr_set_bins(gr_ctx* ctx, double rmin, double rmax, int32_t nbins, int32_t nmu, int32_t logbins);
+int gr_set_option(gr_ctx* ctx, int32_t key, int64_t value);
+
+/* 2PCF.  Replaces create_graph + query_graph_2pcf (src/gramsci.F90:288-379):
+ *   N2      (nbins, nmu)     sum over rooted pairs of w_i w_j          (N2(:,:,3))
+ *   N3      (nbins, nmu)     the same restricted to random-random pairs (N3(:,:,3))
+ *   counts  (nbins, nmu, 4)  rooted pairs by category 2*random(root)+random(neighbour)
+ *   catsum  (nbins, nmu, 4)  sum of w_i w_j per category
+ * The graph is not materialised: pairs are binned straight from the cell
+ * sweep. */
+int gr_count_2pcf(gr_ctx* ctx, double* N2, double* N3, int64_t* counts, double* catsum);
+
+/* 3PCF.  Replaces create_graph + query_graph_3pcf_all (src/gramsci.F90:463-510)
+ * including find_dist (:1579-1609), find_normal (:1611-1625) and the symmetric
+ * bin table (:1459-1474).  ncfg = nbins(nbins+1)(nbins+2)/6:
+ *   N2, N3  (ncfg, nmu)      N3 as the reference forms it (minus the sum over
+ *                            all-random triangles)
+ *   counts  (ncfg, nmu, 4)   rooted triangles by number of randoms (0..3)
+ *   catsum  (ncfg, nmu, 4)   sum of w_i w_a w_b by number of randoms */
+int gr_count_3pcf(gr_ctx* ctx, double* N2, double* N3, int64_t* counts, double* catsum);
+
+/* 4PCF.  Replaces create_graph + query_4pcf_all2 (src/gramsci.F90:662-825).
+ * ncfg = nbins(nbins+1)(nbins+2)(nbins+3)/24 canonical perimeters:
+ *   N2, N3        (ncfg, nbins, nbins)     indexed (cfg, bin(i,b), bin(a,c))
+ *   discN, discR  (ncfg, nbins, nbins, 6)  the six disconnected pair terms
+ *   counts        (ncfg, nbins, nbins, 5)  rooted 4-cliques by number of randoms
+ *   catsum        (ncfg, nbins, nbins, 5)
+ *   dcount, dsum  (ncfg, nbins, nbins, 6, 4) disc terms by category: 0..2 =
+ *                 discN by number of randoms in the pair, 3 = discR */
+int gr_count_4pcf(gr_ctx* ctx, double* N2, double* N3, double* discN, double* discR,
+                  int64_t* counts, double* catsum, int64_t* dcount, double* dsum);
+
+/* Graph access (parity tests, graph reuse).  Builds the (rmin, rmax) graph
+ * of create_graph (src/gramsci.F90:288-348) if needed.  Export gives the
+ * reference's layout: rows in point order, each row sorted by id (as
+ * sort2 leaves it, src/sorting_module.F90:36-47), with the radial bin and the
+ * mu bin seen from the row's point.  row_ptr has N+1 entries. */
+int gr_graph_build(gr_ctx* ctx);
+int gr_graph_nedges(gr_ctx* ctx, int64_t* n_edges);
+int gr_graph_export(gr_ctx* ctx, int64_t* row_ptr, int32_t* col, uint8_t* bin, uint8_t* mu);
+
+/* Statistics of the last count call. */
+int gr_get_stats(gr_ctx* ctx, gr_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GRAMSCI_CUDA_H */

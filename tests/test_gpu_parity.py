@@ -1,0 +1,137 @@
+"""GPU parity: the CUDA library (through its C ABI) against the CPU oracle.
+
+Integer work is compared bit-exactly: the graph edge set with its bins, and
+the rooted pair / triangle / 4-clique counts per bin and category.  Weighted
+sums are FP64 on both sides but summed in different orders; each category
+sum has a single sign, so they are compared with a relative tolerance of
+1e-12.  N2 mixes signs (DD - 2DR + RR), so it is compared against the sum of
+absolute category sums: |N2_gpu - N2_oracle| <= 1e-12 * sum_c |catsum_c|.
+"""
+import numpy as np
+import pytest
+
+from gramsci_b200 import catalogs
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-12
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    den = np.maximum(np.abs(b), 1e-300)
+    d = np.abs(a - b) / den
+    d[(a == 0) & (b == 0)] = 0.0
+    return float(d.max()) if d.size else 0.0
+
+
+def _check_sums(got, ref, ncat_axis=-1):
+    assert np.array_equal(got["counts"], ref["counts"])
+    assert _rel(got["catsum"], ref["catsum"]) < RTOL
+    scale = np.abs(ref["catsum"]).sum(axis=ncat_axis)
+    assert np.all(np.abs(got["N2"] - ref["N2"]) <= RTOL * scale + 1e-300)
+
+
+def _cat(name, scale, seed=None):
+    cat = catalogs.make(name, scale=scale, seed=seed)
+    w = catalogs.normalise(cat.w, cat.n_data, cat.n_rand)
+    return cat, w, catalogs.WORKLOADS[name]
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+@pytest.mark.parametrize("name,scale", [("c1_2pcf", 0.05), ("c2_3pcf", 0.01), ("c3_4pcf", 0.05)])
+def test_graph_edges_equal(gpu_ctx, oracle, name, scale, precision):
+    cat, w, sp = _cat(name, scale)
+    gpu_ctx.set_precision(precision)
+    gpu_ctx.set_catalog(cat.xyz, w, cat.n_data)
+    gpu_ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
+    rp, col, b, mu = gpu_ctx.graph()
+    G = oracle.Graph(cat.xyz, sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
+    orp, ocol, ob, omu = G.csr()
+    assert np.array_equal(rp, orp)
+    assert np.array_equal(col, ocol)
+    assert np.array_equal(b, ob)
+    assert np.array_equal(mu, omu)
+    gpu_ctx.set_precision("f32")
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+@pytest.mark.parametrize("name,scale,nmu", [("c1_2pcf", 0.1, 1), ("c1_2pcf", 0.1, 7),
+                                            ("c5_adjoint_2pcf", 0.003, 4)])
+def test_2pcf(gpu_ctx, oracle, name, scale, nmu, precision):
+    cat, w, sp = _cat(name, scale)
+    gpu_ctx.set_precision(precision)
+    gpu_ctx.set_catalog(cat.xyz, w, cat.n_data)
+    gpu_ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], nmu)
+    got = gpu_ctx.count_2pcf()
+    ref = oracle.Graph(cat.xyz, sp["rmin"], sp["rmax"], sp["nbins"], nmu).pcf2(w, cat.n_data)
+    _check_sums(got, ref)
+    assert np.all(np.abs(got["N3"] - ref["N3"]) <= RTOL * np.abs(ref["N3"]) + 1e-300)
+    gpu_ctx.set_precision("f32")
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_3pcf_c2(gpu_ctx, oracle, precision):
+    cat, w, sp = _cat("c2_3pcf", 0.02)
+    gpu_ctx.set_precision(precision)
+    gpu_ctx.set_catalog(cat.xyz, w, cat.n_data)
+    gpu_ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
+    got = gpu_ctx.count_3pcf()
+    ref = oracle.Graph(cat.xyz, sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"]).pcf3(w, cat.n_data)
+    _check_sums(got, ref)
+    st = gpu_ctx.stats()
+    assert st["rooted"] == int(ref["counts"].sum())
+    gpu_ctx.set_precision("f32")
+
+
+def test_3pcf_unit_weights(gpu_ctx, oracle):
+    cat, w, sp = _cat("c5_adjoint_3pcf", 0.002)
+    w = catalogs.normalise(np.ones(cat.n), cat.n_data, cat.n_rand)
+    gpu_ctx.set_catalog(cat.xyz, w, cat.n_data)
+    gpu_ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
+    got = gpu_ctx.count_3pcf()
+    ref = oracle.Graph(cat.xyz, sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"]).pcf3(w, cat.n_data)
+    _check_sums(got, ref)
+
+
+def test_4pcf_c3(gpu_ctx, oracle):
+    cat, w, sp = _cat("c3_4pcf", 0.1)
+    gpu_ctx.set_catalog(cat.xyz, w, cat.n_data)
+    gpu_ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
+    got = gpu_ctx.count_4pcf()
+    ref = oracle.Graph(cat.xyz, sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"]).pcf4(w, cat.n_data)
+    assert np.array_equal(got["counts"], ref["counts"])
+    assert np.array_equal(got["dcount"], ref["dcount"])
+    assert _rel(got["catsum"], ref["catsum"]) < RTOL
+    assert _rel(got["dsum"], ref["dsum"]) < RTOL
+    assert _rel(got["discR"], ref["discR"]) < RTOL
+
+
+def test_4pcf_weighted_buffer(gpu_ctx, oracle):
+    cat, w, sp = _cat("c3_4pcf", 0.05)
+    rng = np.random.default_rng(11)
+    w = catalogs.normalise(rng.lognormal(0, 0.3, cat.n), cat.n_data, cat.n_rand)
+    buf = (rng.random(cat.n) < 0.2).astype(np.int32)
+    gpu_ctx.set_catalog(cat.xyz, w, cat.n_data, buffer=buf)
+    gpu_ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
+    got = gpu_ctx.count_4pcf()
+    ref = oracle.Graph(cat.xyz, sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"]).pcf4(
+        w, cat.n_data, buffer=buf)
+    assert np.array_equal(got["counts"], ref["counts"])
+    assert np.array_equal(got["dcount"], ref["dcount"])
+    assert _rel(got["catsum"], ref["catsum"]) < RTOL
+    assert _rel(got["dsum"], ref["dsum"]) < RTOL
+
+
+@pytest.mark.parametrize("query", ["2pcf", "3pcf"])
+def test_buffer_points(gpu_ctx, oracle, query):
+    cat, w, sp = _cat("c2_3pcf", 0.01)
+    buf = (np.random.default_rng(5).random(cat.n) < 0.3).astype(np.int32)
+    gpu_ctx.set_catalog(cat.xyz, w, cat.n_data, buffer=buf)
+    gpu_ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
+    G = oracle.Graph(cat.xyz, sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
+    if query == "2pcf":
+        got, ref = gpu_ctx.count_2pcf(), G.pcf2(w, cat.n_data, buffer=buf)
+    else:
+        got, ref = gpu_ctx.count_3pcf(), G.pcf3(w, cat.n_data, buffer=buf)
+    _check_sums(got, ref)
