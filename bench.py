@@ -1,0 +1,337 @@
+"""Benchmark: 3PCF triangles binned per second on one B200 (clustered catalogue).
+
+Workload (one "step" = the whole hot path over one catalogue, from the
+device-resident catalogue to the binned histograms): 100,000 Neyman-Scott
+galaxies (10,000 parents, Poisson(10) children, Gaussian sigma 4 Mpc/h) and
+300,000 uniform randoms in [0,1000]^3, lognormal(0, 0.3) weights, rmin 5,
+rmax 25, 8 radial bins, 5 mu bins (line-of-sight binning on).  Each step
+builds the cell index, the CSR neighbour graph and counts every triangle.
+
+value      distinct triangles binned / second of device time (inputs in HBM)
+e2e        the same through the public API with host inputs: pinned host ->
+           device copy of the catalogue, the count, and the histogram read back
+roofline   the triangle kernel: algorithmic bytes / its CUDA-event time
+cpu_baseline  the CPU restatement of the reference algorithm (kd-tree range
+           search, id-sorted rows, the reference's 3PCF loop) on the host cores
+
+--impl reference times that CPU restatement on the same workload (it is the
+reference's algorithm; the Fortran reference itself cannot be built here).
+Multi-GPU (torchrun): each rank runs its own independently seeded mock of the
+same size (weak scaling, no collective on the data path).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "2/3/4PCF tuples binned/s on 1 B200 (exact counts), batched+adjoint vs plain GPU"
+WORKLOAD = "c2_3pcf"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0, help="workload scale (1.0 = full size)")
+    ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def make_catalogue(scale, seed):
+    from gramsci_b200 import catalogs
+
+    cat = catalogs.make(WORKLOAD, scale=scale, seed=seed)
+    w = catalogs.normalise(cat.w, cat.n_data, cat.n_rand)
+    return cat, w, catalogs.WORKLOADS[WORKLOAD]
+
+
+def workload_config(cat, sp, scale, extra=None):
+    cfg = {
+        "workload": f"{WORKLOAD}: Neyman-Scott 3PCF, {cat.n_data} galaxies + {cat.n_rand} randoms, "
+                    f"box {cat.meta['box']:.0f}, rmin {sp['rmin']}, rmax {sp['rmax']}, "
+                    f"nbins {sp['nbins']}, nmu {sp['nmu']}, lognormal weights",
+        "n_points": int(cat.n),
+        "scale": scale,
+        "l2": "flushed between steps (256 MB write)",
+    }
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() in ("active", "0x1", "1"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_run(cat, w, sp, threads):
+    """The reference algorithm restated on the CPU (kd-tree graph build with
+    id-sorted rows, then the 3PCF loop), timed on the host cores."""
+    from oracle import oracle
+
+    t0 = time.perf_counter()
+    G = oracle.Graph(cat.xyz, sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"], method="kdtree",
+                     threads=threads)
+    t1 = time.perf_counter()
+    r = G.pcf3(w, cat.n_data)
+    t2 = time.perf_counter()
+    rooted = int(r["counts"].sum())
+    return dict(graph_s=t1 - t0, query_s=t2 - t1, total_s=t2 - t0, rooted=rooted,
+                triangles=rooted // 3)
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import oracle
+
+    threads = os.cpu_count() or 1
+    cat, w, sp = make_catalogue(args.scale, None)
+    cfg = workload_config(cat, sp, args.scale)
+    for _ in range(max(args.warmup, 0) and 1):
+        pass
+    times, tri = [], 0
+    nsteps = max(1, min(args.steps, 3))
+    r = cpu_reference_run(cat, w, sp, threads)  # warm-up (page-in, thread pool)
+    for _ in range(nsteps):
+        r = cpu_reference_run(cat, w, sp, threads)
+        times.append(r["total_s"])
+        tri = r["triangles"]
+    t = float(np.mean(times))
+    value = tri / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "tuples/s",
+        "n_gpus": world, "steps": nsteps, "warmup": 1, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Neyman-Scott + uniform randoms)", "config": cfg,
+        "cpu_baseline": {"value": value, "unit": "tuples/s", "cores": threads, "kind": "port",
+                         "sample": f"full {WORKLOAD} catalogue, {nsteps} timed runs, "
+                                   "kd-tree graph build + 3PCF query (C++ OpenMP restatement "
+                                   "of the reference algorithm; no Fortran compiler here)"},
+        "e2e": {"value": value, "unit": "tuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "phases_s": {"graph": r["graph_s"], "query": r["query_s"]},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    device = local if world > 1 else 0
+    torch.cuda.set_device(device)
+    from gramsci_b200 import api
+
+    seed = None if rank == 0 else 1000 + rank
+    cat, w, sp = make_catalogue(args.scale, seed)
+    stream = torch.cuda.current_stream()
+    ctx = api.Context(device)
+    ctx.set_stream(stream)
+    ctx.set_precision(args.precision)
+    xyz_d = torch.from_numpy(cat.xyz).to(f"cuda:{device}")
+    w_d = torch.from_numpy(w).to(f"cuda:{device}")
+    ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
+    ctx.set_catalog(xyz_d, w_d, cat.n_data)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    for _ in range(args.warmup):
+        ctx.count_3pcf()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(device)
+    sampler.start()
+    barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    q_ms, tri, launches = [], 0, 0
+    st = None
+    for k in range(args.steps):
+        flush.zero_()
+        ev[k][0].record(stream)
+        ctx.count_3pcf()
+        ev[k][1].record(stream)
+        st = ctx.stats()
+        q_ms.append(st["ms_query"])
+        tri += st["tuples"]
+        launches += st["kernel_launches"]
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = float(sum(step_ms))
+    t_max = total_ms
+    tri_all = tri
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([total_ms], device=f"cuda:{device}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+        c = torch.tensor([tri], device=f"cuda:{device}", dtype=torch.float64)
+        dist.all_reduce(c, op=dist.ReduceOp.SUM)
+        tri_all = float(c.item())
+    value = tri_all / (t_max / 1e3)
+
+    # end to end through the public API: pinned host catalogue -> device,
+    # count, histograms back to the host, every step
+    xyz_h = torch.from_numpy(cat.xyz).pin_memory()
+    w_h = torch.from_numpy(w).pin_memory()
+    e2e_ms = []
+    for k in range(max(3, min(args.steps, 10))):
+        flush.zero_()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ctx._check(ctx._lib.gr_set_catalog(ctx._h, xyz_h.data_ptr(), w_h.data_ptr(), None,
+                                           cat.n_data, cat.n_rand))
+        out = ctx.count_3pcf()
+        b.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+    e2e_tri = ctx.stats()["tuples"]
+    e2e_t = float(np.mean(e2e_ms))
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([e2e_t], device=f"cuda:{device}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+    e2e_value = e2e_tri * world / (e2e_t / 1e3)
+    nh = out["catsum"].size
+    h2d = int(cat.xyz.nbytes + w.nbytes)
+    d2h = int(nh * 8 * 2 + 8 * 8)
+
+    # roofline of the triangle kernel: algorithmic CSR bytes it must stream
+    # (8 B per upper-row entry read: the root's row and, per neighbour a, the
+    # row of a; 16 B of row offsets per neighbour) over its event time
+    from gramsci_b200 import roofline
+
+    peaks = roofline.peaks()
+    rf = roofline.tri3_roofline(ctx, q_ms, peaks)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "tuples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic (seeded Neyman-Scott galaxies + uniform randoms)",
+        "config": workload_config(cat, sp, args.scale, {
+            "parallelism": f"replicas{world}" if world > 1 else "single",
+            "precision": args.precision,
+            "triangles_per_step": st["tuples"], "rooted_per_step": st["rooted"],
+            "edges": st["n_edges"], "fp64_rechecks": st["fp64_rechecks"],
+            "phase_ms": {"index": st["ms_index"], "graph": st["ms_graph"], "query": st["ms_query"]},
+        }),
+        "e2e": {"value": e2e_value, "unit": "tuples/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "roofline": rf,
+        "clocks": clocks,
+        "gpu_launches": launches,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        r = cpu_reference_run(cat, w, sp, threads)
+        line["cpu_baseline"] = {
+            "value": r["triangles"] / r["total_s"], "unit": "tuples/s", "cores": threads,
+            "kind": "port",
+            "sample": f"the full {WORKLOAD} catalogue once: kd-tree graph build "
+                      f"{r['graph_s']:.2f} s + 3PCF query {r['query_s']:.2f} s "
+                      "(C++ OpenMP restatement of the reference algorithm)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

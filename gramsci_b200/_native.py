@@ -41,6 +41,8 @@ class GrStats(ctypes.Structure):
         ("fp64_rechecks", ctypes.c_int64),
         ("candidates", ctypes.c_int64),
         ("kernel_launches", ctypes.c_int64),
+        ("probes", ctypes.c_int64),
+        ("upper_edges", ctypes.c_int64),
     ]
 
 

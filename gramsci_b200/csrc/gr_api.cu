@@ -513,6 +513,8 @@ int gr_count_3pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
   c->st.n_edges = 2 * c->csr.n_edges;
   c->st.tuples = (int64_t)st[0];
   c->st.rooted = (int64_t)st[1];
+  c->st.probes = (int64_t)st[2];
+  c->st.upper_edges = c->csr.n_edges;
   c->st.fp64_rechecks = (int64_t)gst[0];
   c->st.candidates = (int64_t)gst[1];
   c->st.kernel_launches = c->index.launches + c->csr.launches + 1;
@@ -615,6 +617,8 @@ int gr_count_4pcf(gr_ctx* c, double* N2, double* N3, double* discN, double* disc
   c->st.n_edges = 2 * c->csr.n_edges;
   c->st.tuples = (int64_t)st[0];
   c->st.rooted = (int64_t)st[1];
+  c->st.probes = (int64_t)st[2];
+  c->st.upper_edges = c->csr.n_edges;
   c->st.fp64_rechecks = (int64_t)gst[0];
   c->st.candidates = (int64_t)gst[1];
   c->st.kernel_launches = c->index.launches + c->csr.launches + 1;

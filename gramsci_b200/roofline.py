@@ -1,0 +1,40 @@
+"""Roofline figures for the bench line: measured peaks and the algorithmic
+work of the counting kernels."""
+import json
+import os
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+FALLBACK_HBM_GBS = 6650.0
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    except Exception:
+        return {"hbm_gbs": FALLBACK_HBM_GBS, "source": "fallback"}
+
+
+def tri3_bytes(stats):
+    """Algorithmic bytes of one triangle-kernel launch.
+
+    Per upper edge (p, a): the root row entry (col + meta, 8 B) and the two
+    row offsets of a (16 B).  Per probe (an entry c of the row of a looked up
+    in the row of p): its column index (4 B).  Per rooted triangle
+    contribution the (a, c) edge metadata and the two far vertices' flags,
+    ids and weights are gathered: counted as 4 + 2 * 13 B per triangle.
+    """
+    e = stats["upper_edges"]
+    return 24 * e + 4 * stats["probes"] + 30 * stats["tuples"]
+
+
+def tri3_roofline(ctx, q_ms, pk):
+    st = ctx.stats()
+    ms = sum(q_ms) / len(q_ms)
+    b = tri3_bytes(st)
+    achieved = b / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": "tri3_kernel", "achieved": achieved, "peak": pk["hbm_gbs"],
+            "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "traffic": None,
+            "bytes_per_launch": b, "ms_per_launch": ms, "peak_source": pk["source"]}

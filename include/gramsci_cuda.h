@@ -59,6 +59,9 @@ typedef struct gr_stats {
   int64_t fp64_rechecks;  /* pairs re-evaluated in FP64 inside the guard band    */
   int64_t candidates;     /* candidate pairs tested                              */
   int64_t kernel_launches;/* kernels launched by the call                        */
+  int64_t probes;         /* intersection probes (3PCF/4PCF): neighbour-row entries
+                             looked up in the root's row                          */
+  int64_t upper_edges;    /* undirected edges stored in the upper CSR            */
 } gr_stats;
 
 /* Library version string. */

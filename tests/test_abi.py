@@ -1,0 +1,45 @@
+"""C ABI checks that need no GPU: the library loads and exports every entry
+point declared in include/gramsci_cuda.h, and the ctypes binding declares
+exactly those."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from gramsci_b200 import _native
+
+HEADER = _native.HEADER
+
+
+def declared():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(gr_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declarations_bound():
+    names = declared()
+    assert "gr_count_3pcf" in names and "gr_create" in names
+    assert sorted(_native.SIGNATURES) == names
+
+
+def test_library_exports_every_symbol():
+    lib = ctypes.CDLL(_native.LIB_PATH)
+    for name in declared():
+        assert hasattr(lib, name), name
+
+
+def test_version_string():
+    assert "sm_100a" in _native.load().gr_version().decode()
+
+
+def test_null_context_is_rejected():
+    lib = _native.load()
+    assert lib.gr_destroy(None) == _native.GR_E_ARG
+    assert lib.gr_set_bins(None, 1.0, 2.0, 3, 1, 0) == _native.GR_E_ARG
+    assert lib.gr_count_3pcf(None, None, None, None, None) == _native.GR_E_ARG
+
+
+def test_library_is_in_tree():
+    assert os.path.dirname(_native.LIB_PATH).endswith(os.path.join("gramsci_b200", "lib"))
