@@ -41,8 +41,10 @@ struct gr_ctx {
   PairParams P{};
   DevBuf<uint8_t> normal_dev;
   DevBuf<unsigned long long> hcnt, dcnt, stats;
-  DevBuf<double> hsum, dsum;
+  DevBuf<unsigned long long> hfix, dfix;  // fixed-point sums (lo words, then hi words)
+  double wmax = 0.0;                      // max |w| over the catalogue
   DevBuf<unsigned char> uniform_flag;
+  DevBuf<int> work;
   gr_stats st{};
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
@@ -131,6 +133,19 @@ void make_rank_tables(RankTables& T, int n, int k) {
   }
 }
 
+double fix_scale(double pmax) {
+  // 4 * pmax * scale <= 2^62, so a sum of up to four products fits in 63 bits
+  if (!(pmax > 0.0) || !std::isfinite(pmax)) return 1.0;
+  int e;
+  std::frexp(pmax * (1.0 + 1e-9), &e);  // pmax < 2^e
+  return std::ldexp(1.0, 60 - e);
+}
+
+double fix_value(unsigned long long lo, unsigned long long hi, double scale) {
+  const long double v = (long double)(long long)hi * 18446744073709551616.0L + (long double)lo;
+  return (double)(v / (long double)scale);
+}
+
 }  // namespace gr
 
 namespace {
@@ -188,13 +203,23 @@ int set_err(gr_ctx* c, int code, const std::string& m) {
   }                                                \
   return GR_OK;
 
+// Clears *flag unless all galaxy weights are equal and all random weights are
+// equal; writes max |w| (as the bits of a non-negative double) to *wmax.
 __global__ void uniform_check_kernel(const double* __restrict__ w, int64_t n_data, int64_t n,
-                                     unsigned char* flag) {
+                                     unsigned char* flag, unsigned long long* wmax) {
+  unsigned long long m = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     double ref = i < n_data ? w[0] : w[n_data];
     if (__double_as_longlong(w[i]) != __double_as_longlong(ref)) *flag = 0;
+    unsigned long long a = (unsigned long long)__double_as_longlong(fabs(w[i]));
+    m = a > m ? a : m;
   }
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long u = __shfl_xor_sync(0xffffffffu, m, o);
+    m = u > m ? u : m;
+  }
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(wmax, m);
 }
 
 void require_ready(gr_ctx* c) {
@@ -318,20 +343,25 @@ static int set_catalog_impl(gr_ctx* c, const double* xyz, const double* w, const
   c->n_rand = n_rand;
   // Uniform weights (all galaxies equal, all randoms equal) let the kernels
   // keep integer counts only; sums are then count x product.
-  c->uniform_flag.reserve(1);
-  unsigned char one = 1, flag = 1;
-  GR_CUDA_TRY(cudaMemcpyAsync(c->uniform_flag.p, &one, 1, cudaMemcpyHostToDevice, s));
+  c->uniform_flag.reserve(16);
+  unsigned char init[16] = {1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  unsigned char out[16];
+  GR_CUDA_TRY(cudaMemcpyAsync(c->uniform_flag.p, init, 16, cudaMemcpyHostToDevice, s));
+  unsigned long long* d_wmax = reinterpret_cast<unsigned long long*>(c->uniform_flag.p + 8);
   if (n > 0) {
     int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
-    uniform_check_kernel<<<blocks, 256, 0, s>>>(c->w.p, n_data, n, c->uniform_flag.p);
+    uniform_check_kernel<<<blocks, 256, 0, s>>>(c->w.p, n_data, n, c->uniform_flag.p, d_wmax);
     GR_CHECK_LAUNCH();
   }
-  GR_CUDA_TRY(cudaMemcpyAsync(&flag, c->uniform_flag.p, 1, cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaMemcpyAsync(out, c->uniform_flag.p, 16, cudaMemcpyDeviceToHost, s));
   double wg = 0.0, wr = 0.0;
   if (n_data > 0) GR_CUDA_TRY(cudaMemcpyAsync(&wg, c->w.p, sizeof(double), cudaMemcpyDeviceToHost, s));
   if (n_rand > 0)
     GR_CUDA_TRY(cudaMemcpyAsync(&wr, c->w.p + n_data, sizeof(double), cudaMemcpyDeviceToHost, s));
   GR_CUDA_TRY(cudaStreamSynchronize(s));
+  unsigned char flag = out[0];
+  std::memcpy(&c->wmax, out + 8, 8);
+  if (!std::isfinite(c->wmax)) return set_err(c, GR_E_ARG, "non-finite weights");
   c->uniform = flag != 0;
   c->w_gal = wg;
   c->w_ran = wr;
@@ -388,26 +418,31 @@ int gr_count_2pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
   cudaStream_t s = c->stream();
   const int nbm = c->nbins * c->nmu, nh = nbm * 4;
   const bool weighted = !c->uniform;
+  const double fscale = fix_scale(c->wmax * c->wmax);
   c->hcnt.reserve(nh);
-  c->hsum.reserve(nh);
+  c->hfix.reserve(2 * nh);
   c->stats.reserve(8);
   GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
   build_index(c);
   GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
   GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nh, s));
-  GR_CUDA_TRY(cudaMemsetAsync(c->hsum.p, 0, sizeof(double) * nh, s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->hfix.p, 0, sizeof(unsigned long long) * 2 * nh, s));
   GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
-  launch_pair2(c->index.view(), c->P, weighted, c->hcnt.p, c->hsum.p, c->stats.p, s);
+  c->work.reserve(4);
+  launch_pair2(c->index.view(), c->P, weighted, c->hcnt.p, c->hfix.p, fscale, c->stats.p,
+               c->work.p, s);
   GR_CUDA_TRY(cudaEventRecord(c->ev[2], s));
-  std::vector<unsigned long long> hc(nh);
+  std::vector<unsigned long long> hc(nh), hf(2 * nh, 0ull);
   std::vector<double> hs(nh, 0.0);
   unsigned long long st[8];
   GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
   if (weighted)
-    GR_CUDA_TRY(cudaMemcpyAsync(hs.data(), c->hsum.p, sizeof(double) * nh, cudaMemcpyDeviceToHost, s));
+    GR_CUDA_TRY(cudaMemcpyAsync(hf.data(), c->hfix.p, sizeof(unsigned long long) * 2 * nh, cudaMemcpyDeviceToHost, s));
   GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
   GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
   GR_CUDA_TRY(cudaStreamSynchronize(s));
+  if (weighted)
+    for (int k = 0; k < nh; ++k) hs[k] = fix_value(hf[k], hf[nh + k], fscale);
   if (!weighted) {
     for (int cat = 0; cat < 4; ++cat) {
       double prod = uniform_product(c->w_gal, c->w_ran, 2 - ((cat >> 1) + (cat & 1)),
@@ -449,8 +484,9 @@ int gr_count_3pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
   const int ncfg = (int)(((int64_t)c->nbins * (c->nbins + 1) * (c->nbins + 2)) / 6);
   const int nbin = ncfg * nmu, nh = nbin * 4;
   const bool weighted = !c->uniform;
+  const double fscale = fix_scale(c->wmax * c->wmax * c->wmax);
   c->hcnt.reserve(nh);
-  c->hsum.reserve(nh);
+  c->hfix.reserve(2 * nh);
   c->stats.reserve(8);
   std::vector<uint8_t> nt;
   normal_table(nmu, nt);
@@ -464,7 +500,7 @@ int gr_count_3pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
   unsigned long long gst[4];
   GR_CUDA_TRY(cudaMemcpyAsync(gst, c->csr.stats.p, sizeof(gst), cudaMemcpyDeviceToHost, s));
   GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nh, s));
-  GR_CUDA_TRY(cudaMemsetAsync(c->hsum.p, 0, sizeof(double) * nh, s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->hfix.p, 0, sizeof(unsigned long long) * 2 * nh, s));
   GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
   GR_CUDA_TRY(cudaStreamSynchronize(s));
   TriParams T;
@@ -475,20 +511,24 @@ int gr_count_3pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
   T.cap = round_cap((int64_t)gst[2], 32, 256);
   T.normal = c->normal_dev.p;
   make_rank_tables(T.rank, c->nbins, 3);
-  CSRView G{c->csr.row_ptr.p, c->csr.col.p, c->csr.meta.p, c->csr.deg_full.p};
+  CSRView G{c->csr.row_ptr.p, c->csr.rec.p, c->csr.deg_full.p};
   cudaEvent_t q0;
   GR_CUDA_TRY(cudaEventCreate(&q0));
   GR_CUDA_TRY(cudaEventRecord(q0, s));
-  launch_tri3(c->index.view(), G, T, weighted, c->hcnt.p, c->hsum.p, c->stats.p, s);
+  c->work.reserve(4);
+  launch_tri3(c->index.view(), G, T, weighted, c->hcnt.p, c->hfix.p, fscale, c->stats.p,
+              c->work.p, s);
   GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
-  std::vector<unsigned long long> hc(nh);
+  std::vector<unsigned long long> hc(nh), hf(2 * nh, 0ull);
   std::vector<double> hs(nh, 0.0);
   unsigned long long st[8];
   GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
   if (weighted)
-    GR_CUDA_TRY(cudaMemcpyAsync(hs.data(), c->hsum.p, sizeof(double) * nh, cudaMemcpyDeviceToHost, s));
+    GR_CUDA_TRY(cudaMemcpyAsync(hf.data(), c->hfix.p, sizeof(unsigned long long) * 2 * nh, cudaMemcpyDeviceToHost, s));
   GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
   GR_CUDA_TRY(cudaStreamSynchronize(s));
+  if (weighted)
+    for (int k = 0; k < nh; ++k) hs[k] = fix_value(hf[k], hf[nh + k], fscale);
   if (!weighted) {
     for (int nr = 0; nr < 4; ++nr) {
       double prod = uniform_product(c->w_gal, c->w_ran, 3 - nr, nr);
@@ -534,10 +574,12 @@ int gr_count_4pcf(gr_ctx* c, double* N2, double* N3, double* discN, double* disc
   const int ncfg = (int)ncfg64, nbin = (int)nbin64;
   const int nh = nbin * 5, nd = nbin * 24;
   const bool weighted = !c->uniform;
+  const double fscale = fix_scale(c->wmax * c->wmax * c->wmax * c->wmax);
+  const double dscale = fix_scale(c->wmax * c->wmax);
   c->hcnt.reserve(nh);
-  c->hsum.reserve(nh);
+  c->hfix.reserve(2 * nh);
   c->dcnt.reserve(nd);
-  c->dsum.reserve(nd);
+  c->dfix.reserve(2 * nd);
   c->stats.reserve(8);
   GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
   build_index(c);
@@ -547,9 +589,9 @@ int gr_count_4pcf(gr_ctx* c, double* N2, double* N3, double* discN, double* disc
   unsigned long long gst[4];
   GR_CUDA_TRY(cudaMemcpyAsync(gst, c->csr.stats.p, sizeof(gst), cudaMemcpyDeviceToHost, s));
   GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nh, s));
-  GR_CUDA_TRY(cudaMemsetAsync(c->hsum.p, 0, sizeof(double) * nh, s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->hfix.p, 0, sizeof(unsigned long long) * 2 * nh, s));
   GR_CUDA_TRY(cudaMemsetAsync(c->dcnt.p, 0, sizeof(unsigned long long) * nd, s));
-  GR_CUDA_TRY(cudaMemsetAsync(c->dsum.p, 0, sizeof(double) * nd, s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->dfix.p, 0, sizeof(unsigned long long) * 2 * nd, s));
   GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
   GR_CUDA_TRY(cudaStreamSynchronize(s));
   if ((int64_t)gst[2] > 1024)
@@ -559,24 +601,30 @@ int gr_count_4pcf(gr_ctx* c, double* N2, double* N3, double* discN, double* disc
   Q.ncfg = ncfg;
   Q.cap = round_cap((int64_t)gst[2], 32, 1024);
   make_rank_tables(Q.rank, nb, 4);
-  CSRView G{c->csr.row_ptr.p, c->csr.col.p, c->csr.meta.p, c->csr.deg_full.p};
+  CSRView G{c->csr.row_ptr.p, c->csr.rec.p, c->csr.deg_full.p};
   cudaEvent_t q0;
   GR_CUDA_TRY(cudaEventCreate(&q0));
   GR_CUDA_TRY(cudaEventRecord(q0, s));
-  launch_quad4(c->index.view(), G, Q, weighted, c->hcnt.p, c->hsum.p, c->dcnt.p, c->dsum.p,
-               c->stats.p, s);
+  launch_quad4(c->index.view(), G, Q, weighted, c->hcnt.p, c->hfix.p, c->dcnt.p, c->dfix.p,
+               fscale, dscale, c->stats.p, s);
   GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
-  std::vector<unsigned long long> hc(nh), dc(nd);
+  std::vector<unsigned long long> hc(nh), dc(nd), hf, df;
   std::vector<double> hs(nh, 0.0), ds(nd, 0.0);
   unsigned long long st[8];
   GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
   GR_CUDA_TRY(cudaMemcpyAsync(dc.data(), c->dcnt.p, sizeof(unsigned long long) * nd, cudaMemcpyDeviceToHost, s));
   if (weighted) {
-    GR_CUDA_TRY(cudaMemcpyAsync(hs.data(), c->hsum.p, sizeof(double) * nh, cudaMemcpyDeviceToHost, s));
-    GR_CUDA_TRY(cudaMemcpyAsync(ds.data(), c->dsum.p, sizeof(double) * nd, cudaMemcpyDeviceToHost, s));
+    hf.resize(2 * (size_t)nh);
+    df.resize(2 * (size_t)nd);
+    GR_CUDA_TRY(cudaMemcpyAsync(hf.data(), c->hfix.p, sizeof(unsigned long long) * 2 * nh, cudaMemcpyDeviceToHost, s));
+    GR_CUDA_TRY(cudaMemcpyAsync(df.data(), c->dfix.p, sizeof(unsigned long long) * 2 * nd, cudaMemcpyDeviceToHost, s));
   }
   GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
   GR_CUDA_TRY(cudaStreamSynchronize(s));
+  if (weighted) {
+    for (int k = 0; k < nh; ++k) hs[k] = fix_value(hf[k], hf[(size_t)nh + k], fscale);
+    for (int k = 0; k < nd; ++k) ds[k] = fix_value(df[k], df[(size_t)nd + k], dscale);
+  }
   if (!weighted) {
     for (int nr = 0; nr < 5; ++nr) {
       double prod = uniform_product(c->w_gal, c->w_ran, 4 - nr, nr);
@@ -656,13 +704,11 @@ int gr_graph_export(gr_ctx* c, int64_t* row_ptr, int32_t* col, uint8_t* bin, uin
   cudaStream_t s = c->stream();
   const int64_t n = c->n, E = c->csr.n_edges;
   std::vector<int64_t> rp(n + 1);
-  std::vector<int> cl(E), orig(n);
-  std::vector<uint32_t> mt(E);
+  std::vector<int> orig(n);
+  std::vector<unsigned long long> rc(E);
   GR_CUDA_TRY(cudaMemcpyAsync(rp.data(), c->csr.row_ptr.p, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, s));
-  if (E > 0) {
-    GR_CUDA_TRY(cudaMemcpyAsync(cl.data(), c->csr.col.p, sizeof(int) * E, cudaMemcpyDeviceToHost, s));
-    GR_CUDA_TRY(cudaMemcpyAsync(mt.data(), c->csr.meta.p, sizeof(uint32_t) * E, cudaMemcpyDeviceToHost, s));
-  }
+  if (E > 0)
+    GR_CUDA_TRY(cudaMemcpyAsync(rc.data(), c->csr.rec.p, sizeof(unsigned long long) * E, cudaMemcpyDeviceToHost, s));
   if (n > 0)
     GR_CUDA_TRY(cudaMemcpyAsync(orig.data(), c->index.orig.p, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
   GR_CUDA_TRY(cudaStreamSynchronize(s));
@@ -671,7 +717,7 @@ int gr_graph_export(gr_ctx* c, int64_t* row_ptr, int32_t* col, uint8_t* bin, uin
   for (int64_t p = 0; p < n; ++p)
     for (int64_t e = rp[p]; e < rp[p + 1]; ++e) {
       deg[orig[p]]++;
-      deg[orig[cl[e]]]++;
+      deg[orig[(int)(uint32_t)rc[e]]]++;
     }
   std::vector<int64_t> out_ptr(n + 1, 0);
   for (int64_t i = 0; i < n; ++i) out_ptr[i + 1] = out_ptr[i] + deg[i];
@@ -679,8 +725,8 @@ int gr_graph_export(gr_ctx* c, int64_t* row_ptr, int32_t* col, uint8_t* bin, uin
   std::vector<uint64_t> ent(2 * E);
   for (int64_t p = 0; p < n; ++p)
     for (int64_t e = rp[p]; e < rp[p + 1]; ++e) {
-      int i = orig[p], j = orig[cl[e]];
-      uint32_t m = mt[e];
+      int i = orig[p], j = orig[(int)(uint32_t)rc[e]];
+      uint32_t m = (uint32_t)(rc[e] >> 32);
       uint64_t b = m & 0xff, mf = (m >> 8) & 0xff, mr = (m >> 16) & 0xff;
       ent[fill[i]++] = ((uint64_t)j << 16) | (b << 8) | mf;
       ent[fill[j]++] = ((uint64_t)i << 16) | (b << 8) | mr;

@@ -43,13 +43,29 @@ __global__ void bbox_kernel(const double* __restrict__ xyz, int64_t n, unsigned 
     unsigned long long c = __shfl_xor_sync(0xffffffffu, ab, o);
     ab = c > ab ? c : ab;
   }
+  // block reduction, then one set of atomics per block
+  __shared__ unsigned long long red[32][7];
+  const int wid = threadIdx.x >> 5;
   if ((threadIdx.x & 31) == 0) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      atomicMin(&out[d], mn[d]);
-      atomicMax(&out[3 + d], mx[d]);
+      red[wid][d] = mn[d];
+      red[wid][3 + d] = mx[d];
     }
-    atomicMax(&out[6], ab);
+    red[wid][6] = ab;
+  }
+  __syncthreads();
+  if (threadIdx.x < 7) {
+    const int t = threadIdx.x;
+    unsigned long long v = red[0][t];
+    for (int k = 1; k < (int)(blockDim.x >> 5); ++k) {
+      const unsigned long long u = red[k][t];
+      v = (t < 3) ? (u < v ? u : v) : (u > v ? u : v);
+    }
+    if (t < 3)
+      atomicMin(&out[t], v);
+    else
+      atomicMax(&out[t], v);
   }
 }
 
@@ -164,7 +180,7 @@ void CellIndex::build(const double* d_xyz, const double* d_w, const int* d_buffe
   init_bbox_kernel<<<1, 32, 0, s>>>(bbox_raw.p);
   launches++;
   if (n > 0) {
-    bbox_kernel<<<blocks_for(n, 256), 256, 0, s>>>(d_xyz, n, bbox_raw.p);
+    bbox_kernel<<<blocks_for(n, 256, 296), 256, 0, s>>>(d_xyz, n, bbox_raw.p);
     launches++;
   }
   GR_CHECK_LAUNCH();

@@ -1,6 +1,9 @@
 // Device cell index and upper-triangular CSR adjacency.
 #pragma once
 
+// candidates staged per warp and tile by the cell sweeps
+#define kCellTile 256
+
 #include <algorithm>
 #include <cstring>
 
@@ -35,20 +38,21 @@ void narrow_kernel_launch(const int64_t* in, int* out, int64_t n, cudaStream_t s
 struct UpperCSR {
   int64_t n = 0, n_edges = 0;  // n_edges counts upper (undirected) edges
   int launches = 0;
-  DevBuf<int> deg_up, deg_full;
+  DevBuf<int> deg_up, deg_full, cursor, work;
   DevBuf<int64_t> row_ptr, scan_tmp;
-  DevBuf<int> col;
-  DevBuf<uint32_t> meta;
-  DevBuf<unsigned long long> stats;  // [0] FP64 rechecks, [1] candidates
+  DevBuf<unsigned long long> rec;    // (meta << 32) | neighbour label
+  DevBuf<unsigned long long> stats;  // [0] FP64 rechecks, [1] candidates, [2] max upper degree
 
   void build(const DevCatalog& C, const PairParams& P, cudaStream_t s);
 };
 
 struct CSRView {
   const int64_t* row_ptr;
-  const int* col;
-  const uint32_t* meta;
+  const unsigned long long* rec;  // (meta << 32) | neighbour label
   const int* deg_full;
 };
+
+__device__ __forceinline__ int rec_col(unsigned long long r) { return (int)(uint32_t)r; }
+__device__ __forceinline__ uint32_t rec_meta(unsigned long long r) { return (uint32_t)(r >> 32); }
 
 }  // namespace gr

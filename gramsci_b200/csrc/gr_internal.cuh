@@ -306,6 +306,36 @@ struct DevCatalog {
 
 enum : uint8_t { FLAG_RANDOM = 1, FLAG_BUFFER = 2 };
 
+// ------------------------------------------------------- fixed-point sums --
+// Weighted sums are accumulated as signed 128-bit fixed-point integers with
+// 64-bit integer atomics: a product x becomes V = round(x * 2^e) (|V| < 2^63,
+// e chosen per launch from the largest possible |product|) and is added in
+// two's complement to a (lo, hi) pair.  Integer addition is exact and
+// order-independent, so the sums are deterministic; the only rounding is the
+// quantisation of each product, at most 2^-(e+1) absolute.
+__device__ __forceinline__ void fix_add(unsigned long long* lo, unsigned long long* hi, double x,
+                                        double scale) {
+  const long long v = __double2ll_rn(x * scale);
+  const unsigned long long add = (unsigned long long)v;
+  const unsigned long long old = atomicAdd(lo, add);
+  const unsigned long long carry = (old + add < old) ? 1ull : 0ull;
+  const unsigned long long d = (v < 0 ? ~0ull : 0ull) + carry;
+  if (d) atomicAdd(hi, d);
+}
+
+// merge a partial (lo, hi) pair into another with atomics
+__device__ __forceinline__ void fix_merge(unsigned long long* lo, unsigned long long* hi,
+                                          unsigned long long plo, unsigned long long phi) {
+  const unsigned long long old = atomicAdd(lo, plo);
+  const unsigned long long d = phi + ((old + plo < old) ? 1ull : 0ull);
+  if (d) atomicAdd(hi, d);
+}
+
+// Host: scale 2^e with max_abs_product * 2^e < 2^62.
+double fix_scale(double max_abs_product);
+// Host: value of a (lo, hi) pair.
+double fix_value(unsigned long long lo, unsigned long long hi, double scale);
+
 // -------------------------------------------------------------- host launch --
 // Exclusive scan of n int32 values into n+1 int64 values (out[n] = total).
 void scan_i32_to_i64(const int* in, int64_t* out, int64_t n, cudaStream_t s, DevBuf<int64_t>& tmp);

@@ -7,15 +7,18 @@ namespace gr {
 
 // Shared-memory budget for a privatised histogram; larger histograms are
 // accumulated with global atomics instead.
-constexpr size_t kMaxHistSmem = 96 * 1024;
+constexpr size_t kMaxHistSmem = 120 * 1024;
+
+// Weighted sums (g_fix / d_fix below) are fixed-point (lo, hi) pairs: the
+// nh lo words followed by the nh hi words, scale fscale (fix_add).
 
 // 2PCF: pairs binned straight from the half-stencil cell sweep.
-// g_cnt (nbins*nmu*4) and g_sum (same, weighted only) must be zeroed.
+// g_cnt (nh = nbins*nmu*4) and g_fix (2*nh, weighted only) must be zeroed.
 // stats: [0] FP64 rechecks, [1] candidates, [2] binned unordered pairs.
 size_t pair2_smem_bytes(const PairParams& P, bool weighted);
 void launch_pair2(const DevCatalog& C, const PairParams& P, bool weighted,
-                  unsigned long long* g_cnt, double* g_sum, unsigned long long* stats,
-                  cudaStream_t s);
+                  unsigned long long* g_cnt, unsigned long long* g_fix, double fscale,
+                  unsigned long long* stats, int* work, cudaStream_t s);
 
 struct TriParams {
   int nbins, nmu, ncfg, rsd;
@@ -26,11 +29,13 @@ struct TriParams {
 
 // 3PCF: triangles p < a < c enumerated once over the upper CSR; each adds to
 // the rooted histogram of every non-buffer vertex.  g_cnt / g_sum have
-// ncfg*nmu*4 entries.  stats: [0] distinct triangles binned, [1] rooted
+// nh = ncfg*nmu*4 entries (g_fix 2*nh).  stats: [0] distinct triangles binned, [1] rooted
 // incidences, [2] intersection probes.
+// work: one device int used as the dynamic root counter (reset by the launch).
+size_t tri3_smem_bytes(const TriParams& T, bool weighted);
 void launch_tri3(const DevCatalog& C, const CSRView& G, const TriParams& T, bool weighted,
-                 unsigned long long* g_cnt, double* g_sum, unsigned long long* stats,
-                 cudaStream_t s);
+                 unsigned long long* g_cnt, unsigned long long* g_fix, double fscale,
+                 unsigned long long* stats, int* work, cudaStream_t s);
 
 struct QuadParams {
   int nbins, ncfg;
@@ -40,10 +45,11 @@ struct QuadParams {
 
 // 4PCF: 4-cliques p < a < b < c enumerated once; each adds to the rooted
 // histograms of its non-buffer vertices whose perimeter is canonical.
-// g_cnt/g_sum: ncfg*nbins*nbins*5; d_cnt/d_sum: ncfg*nbins*nbins*24.
+// g_cnt: nh = ncfg*nbins*nbins*5 (g_fix 2*nh); d_cnt: nd = ncfg*nbins*nbins*24 (d_fix 2*nd).
 // stats: [0] distinct 4-cliques binned, [1] rooted incidences, [2] probes.
 void launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bool weighted,
-                  unsigned long long* g_cnt, double* g_sum, unsigned long long* d_cnt,
-                  double* d_sum, unsigned long long* stats, cudaStream_t s);
+                  unsigned long long* g_cnt, unsigned long long* g_fix, unsigned long long* d_cnt,
+                  unsigned long long* d_fix, double fscale, double dscale,
+                  unsigned long long* stats, cudaStream_t s);
 
 }  // namespace gr

@@ -6,87 +6,119 @@
 // mu(q->p) if q is not.
 //
 // Histograms are privatised per block in shared memory: 64-bit counts per
-// (bin, mu, category) and, for weighted catalogues, FP64 sums of w_i w_j per
-// category (each category sum has a single sign, so it is well conditioned).
+// (bin, mu, category) and, for weighted catalogues, 128-bit fixed-point sums
+// of w_i w_j per category (see fix_add).
 #include "gr_kernels.cuh"
 
 namespace gr {
 
 namespace {
 
-constexpr int kPairThreads = 256;
+constexpr int kPairWarps = 8;
+constexpr int kPairThreads = kPairWarps * 32;
 
 // SHIST: histogram privatised in shared memory (false: atomics straight to
 // the global histogram, for bin counts too large for shared memory).
+// Warp per cell: the forward candidates of a cell are computed once and
+// staged in shared memory (tiles of kCellTile), then every root of the cell
+// is tested against the staged candidates with larger labels.
 template <bool F32, bool WEIGHTED, bool SHIST>
 __global__ void __launch_bounds__(kPairThreads) pair2_kernel(DevCatalog C, PairParams P,
                                                              unsigned long long* __restrict__ g_cnt,
-                                                             double* __restrict__ g_sum,
-                                                             unsigned long long* __restrict__ stats) {
+                                                             unsigned long long* __restrict__ g_fix,
+                                                             double fscale,
+                                                             unsigned long long* __restrict__ stats,
+                                                             int* __restrict__ work) {
   extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ float4 s_pos[kPairWarps][kCellTile];
+  __shared__ int s_lab[kPairWarps][kCellTile];
   const int nbm = P.nbins * P.nmu;
   const int nh = nbm * 4;
   unsigned long long* s_cnt = SHIST ? reinterpret_cast<unsigned long long*>(smem) : g_cnt;
-  double* s_sum = SHIST ? reinterpret_cast<double*>(smem + sizeof(unsigned long long) * nh) : g_sum;
+  unsigned long long* s_lo = SHIST ? s_cnt + nh : g_fix;
+  unsigned long long* s_hi = s_lo + nh;
   if (SHIST) {
     for (int k = threadIdx.x; k < nh; k += blockDim.x) {
       s_cnt[k] = 0ull;
-      if (WEIGHTED) s_sum[k] = 0.0;
+      if (WEIGHTED) {
+        s_lo[k] = 0ull;
+        s_hi[k] = 0ull;
+      }
     }
     __syncthreads();
   }
 
   const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int wib = threadIdx.x >> 5;
+  const int ncell = (int)C.grid.ncell;
   unsigned long long rechecks = 0, cands = 0, pairs = 0;
-  for (int p = warp; p < C.n; p += nwarps) {
+  for (;;) {
+    int cell = 0;
+    if (lane == 0) cell = atomicAdd(work, 1);
+    cell = __shfl_sync(0xffffffffu, cell, 0);
+    if (cell >= ncell) break;
+    const int cb = C.cell_start[cell], ce = C.cell_start[cell + 1];
+    if (cb == ce) continue;
     Ranges R;
-    forward_ranges(p, C.cell_key[p], C.grid, C.cell_start, R);
+    forward_ranges(cb - 1, cell, C.grid, C.cell_start, R);
     int pre[5], total = 0;
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
       pre[k] = total;
       if (k < R.n) total += R.end[k] - R.beg[k];
     }
-    const float4 pi = C.pos4[p];
-    const uint8_t fp = C.flags[p];
-    const bool root_p = !(fp & FLAG_BUFFER);
-    const int rp = fp & FLAG_RANDOM;
-    const double wp = WEIGHTED ? C.w[p] : 0.0;
-    for (int f = lane; f < total; f += 32) {
-      int q = range_label(R, pre, f);
-      int b, mf, mr;
-      bool e;
-      if (F32) {
-        int r = classify_f32<true>(pi, C.pos4[q], P, b, mf, mr);
-        if (r == 2) {
-          rechecks++;
-          e = edge_f64(C.posd[p], C.posd[q], P, b, mf, mr);
-        } else {
-          e = r == 1;
+    for (int t0 = 0; t0 < total; t0 += kCellTile) {
+      const int tn = min(kCellTile, total - t0);
+      __syncwarp();
+      for (int f = lane; f < tn; f += 32) {
+        const int q = range_label(R, pre, t0 + f);
+        s_lab[wib][f] = q;
+        s_pos[wib][f] = C.pos4[q];
+      }
+      __syncwarp();
+      for (int p = cb; p < ce; ++p) {
+        const int fstart = max(0, p - cb + 1 - t0);
+        if (fstart >= tn) continue;
+        const float4 pi = C.pos4[p];
+        const uint8_t fp = C.flags[p];
+        const bool root_p = !(fp & FLAG_BUFFER);
+        const int rp = fp & FLAG_RANDOM;
+        const double wp = WEIGHTED ? C.w[p] : 0.0;
+        for (int f = fstart + lane; f < tn; f += 32) {
+          const int q = s_lab[wib][f];
+          int b, mf, mr;
+          bool e;
+          if (F32) {
+            const int r = classify_f32<true>(pi, s_pos[wib][f], P, b, mf, mr);
+            if (r == 2) {
+              rechecks++;
+              e = edge_f64(C.posd[p], C.posd[q], P, b, mf, mr);
+            } else {
+              e = r == 1;
+            }
+          } else {
+            e = edge_f64(C.posd[p], C.posd[q], P, b, mf, mr);
+          }
+          if (!e) continue;
+          const uint8_t fq = C.flags[q];
+          const int rq = fq & FLAG_RANDOM;
+          pairs += (root_p || !(fq & FLAG_BUFFER)) ? 1 : 0;
+          double prod = 0.0;
+          if (WEIGHTED) prod = wp * C.w[q];
+          if (root_p) {
+            const int k = (b - 1) + P.nbins * (mf - 1) + nbm * (2 * rp + rq);
+            atomicAdd(&s_cnt[k], 1ull);
+            if (WEIGHTED) fix_add(&s_lo[k], &s_hi[k], prod, fscale);
+          }
+          if (!(fq & FLAG_BUFFER)) {
+            const int k = (b - 1) + P.nbins * (mr - 1) + nbm * (2 * rq + rp);
+            atomicAdd(&s_cnt[k], 1ull);
+            if (WEIGHTED) fix_add(&s_lo[k], &s_hi[k], prod, fscale);
+          }
         }
-      } else {
-        e = edge_f64(C.posd[p], C.posd[q], P, b, mf, mr);
-      }
-      if (!e) continue;
-      const uint8_t fq = C.flags[q];
-      pairs += (root_p || !(fq & FLAG_BUFFER)) ? 1 : 0;
-      const int rq = fq & FLAG_RANDOM;
-      double prod = 0.0;
-      if (WEIGHTED) prod = wp * C.w[q];
-      if (root_p) {
-        int k = (b - 1) + P.nbins * (mf - 1) + nbm * (2 * rp + rq);
-        atomicAdd(&s_cnt[k], 1ull);
-        if (WEIGHTED) atomicAdd(&s_sum[k], prod);
-      }
-      if (!(fq & FLAG_BUFFER)) {
-        int k = (b - 1) + P.nbins * (mr - 1) + nbm * (2 * rq + rp);
-        atomicAdd(&s_cnt[k], 1ull);
-        if (WEIGHTED) atomicAdd(&s_sum[k], prod);
+        if (lane == 0) cands += (unsigned long long)(tn - fstart);
       }
     }
-    if (lane == 0) cands += (unsigned long long)total;
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -101,8 +133,10 @@ __global__ void __launch_bounds__(kPairThreads) pair2_kernel(DevCatalog C, PairP
   if (SHIST) {
     __syncthreads();
     for (int k = threadIdx.x; k < nh; k += blockDim.x) {
-      if (s_cnt[k]) atomicAdd(&g_cnt[k], s_cnt[k]);
-      if (WEIGHTED && s_sum[k] != 0.0) atomicAdd(&g_sum[k], s_sum[k]);
+      if (s_cnt[k]) {
+        atomicAdd(&g_cnt[k], s_cnt[k]);
+        if (WEIGHTED) fix_merge(&g_fix[k], &g_fix[nh + k], s_lo[k], s_hi[k]);
+      }
     }
   }
 }
@@ -111,26 +145,26 @@ __global__ void __launch_bounds__(kPairThreads) pair2_kernel(DevCatalog C, PairP
 
 size_t pair2_smem_bytes(const PairParams& P, bool weighted) {
   size_t nh = (size_t)P.nbins * P.nmu * 4;
-  return nh * sizeof(unsigned long long) + (weighted ? nh * sizeof(double) : 0);
+  return nh * sizeof(unsigned long long) * (weighted ? 3 : 1);
 }
 
 void launch_pair2(const DevCatalog& C, const PairParams& P, bool weighted,
-                  unsigned long long* g_cnt, double* g_sum, unsigned long long* stats,
-                  cudaStream_t s) {
+                  unsigned long long* g_cnt, unsigned long long* g_fix, double fscale,
+                  unsigned long long* stats, int* work, cudaStream_t s) {
   if (C.n <= 0) return;
   size_t smem = pair2_smem_bytes(P, weighted);
   const bool shist = smem <= kMaxHistSmem;
   if (!shist) smem = 0;
-  int64_t warps = C.n;
-  int64_t blocks = (warps * 32 + kPairThreads - 1) / kPairThreads;
-  if (blocks > 148 * 8) blocks = 148 * 8;
+  GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));
+  int64_t blocks = (C.grid.ncell + kPairWarps - 1) / kPairWarps;
+  if (blocks > 148 * 4) blocks = 148 * 4;
   if (blocks < 1) blocks = 1;
 #define GR_PAIR_LAUNCH(F, W, S)                                                          \
   do {                                                                                   \
     auto k = pair2_kernel<F, W, S>;                                                      \
     GR_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
                                      (int)smem));                                        \
-    k<<<(unsigned)blocks, kPairThreads, smem, s>>>(C, P, g_cnt, g_sum, stats);           \
+    k<<<(unsigned)blocks, kPairThreads, smem, s>>>(C, P, g_cnt, g_fix, fscale, stats, work);           \
   } while (0)
 #define GR_PAIR_LAUNCH_W(F, S)                                                           \
   do {                                                                                   \

@@ -54,7 +54,9 @@ struct QuadCtx {
   const int* F;  // 4 x (nbins+2)
   int nbins, ncfg, nbin;
   unsigned long long *cnt, *dcnt;
-  double *sum, *dsum;
+  unsigned long long *fix, *dfix;  // fixed-point (lo, hi) sums, hi at +5*nbin / +24*nbin
+  double fscale;  // scale of the 4-point products
+  double dscale;  // scale of the pair products of the disconnected terms
 };
 
 // disc term t: gate role and pair roles (0 = root i, 1 = a, 2 = b, 3 = c),
@@ -109,7 +111,9 @@ __device__ __forceinline__ int quad_contrib(const DevCatalog& C, const CSRView& 
     const int d1 = B[r][o[1]], d2 = B[o[0]][o[2]];
     const int kk = (cfg - 1) + X.ncfg * ((d1 - 1) + X.nbins * (d2 - 1));
     atomicAdd(&X.cnt[kk + X.nbin * nr], 1ull);
-    if (WEIGHTED) atomicAdd(&X.sum[kk + X.nbin * nr], ((w[r] * w[o[0]]) * w[o[1]]) * w[o[2]]);
+    if (WEIGHTED)
+      fix_add(&X.fix[kk + X.nbin * nr], &X.fix[kk + X.nbin * (nr + 5)],
+              ((w[r] * w[o[0]]) * w[o[1]]) * w[o[2]], X.fscale);
     const int role[4] = {r, o[0], o[1], o[2]};
 #pragma unroll
     for (int tt = 0; tt < 6; ++tt) {
@@ -117,11 +121,13 @@ __device__ __forceinline__ int quad_contrib(const DevCatalog& C, const CSRView& 
       const int u = role[kPu[tt]], vv = role[kPv[tt]];
       const int npr = (int)rnd[u] + (int)rnd[vv];
       const int kt = kk + X.nbin * tt;
+      const double q = WEIGHTED ? w[u] * w[vv] : 0.0;
       atomicAdd(&X.dcnt[kt + X.nbin * 6 * npr], 1ull);
-      if (WEIGHTED) atomicAdd(&X.dsum[kt + X.nbin * 6 * npr], w[u] * w[vv]);
+      if (WEIGHTED)
+        fix_add(&X.dfix[kt + X.nbin * 6 * npr], &X.dfix[kt + X.nbin * (6 * npr + 24)], q, X.dscale);
       if (npr == 2) {
         atomicAdd(&X.dcnt[kt + X.nbin * 18], 1ull);
-        if (WEIGHTED) atomicAdd(&X.dsum[kt + X.nbin * 18], w[u] * w[vv]);
+        if (WEIGHTED) fix_add(&X.dfix[kt + X.nbin * 18], &X.dfix[kt + X.nbin * 42], q, X.dscale);
       }
     }
     n++;
@@ -132,9 +138,10 @@ __device__ __forceinline__ int quad_contrib(const DevCatalog& C, const CSRView& 
 template <bool WEIGHTED>
 __global__ void __launch_bounds__(kQuadThreads) quad4_kernel(DevCatalog C, CSRView G, QuadParams Q,
                                                              unsigned long long* __restrict__ g_cnt,
-                                                             double* __restrict__ g_sum,
+                                                             unsigned long long* __restrict__ g_fix,
                                                              unsigned long long* __restrict__ d_cnt,
-                                                             double* __restrict__ d_sum,
+                                                             unsigned long long* __restrict__ d_fix,
+                                                             double fscale, double dscale,
                                                              unsigned long long* __restrict__ stats) {
   extern __shared__ __align__(16) unsigned char smem[];
   const QuadLayout L = quad_layout(Q.nbins, Q.cap);
@@ -148,9 +155,11 @@ __global__ void __launch_bounds__(kQuadThreads) quad4_kernel(DevCatalog C, CSRVi
   X.ncfg = Q.ncfg;
   X.nbin = Q.ncfg * Q.nbins * Q.nbins;
   X.cnt = g_cnt;
-  X.sum = g_sum;
+  X.fix = g_fix;
   X.dcnt = d_cnt;
-  X.dsum = d_sum;
+  X.dfix = d_fix;
+  X.fscale = fscale;
+  X.dscale = dscale;
 
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
@@ -177,9 +186,10 @@ __global__ void __launch_bounds__(kQuadThreads) quad4_kernel(DevCatalog C, CSRVi
     if (k < 3 || k > cap) continue;  // rows longer than cap are rejected on the host
     __syncwarp();
     for (int x = lane; x < k; x += 32) {
-      int a = G.col[b0 + x];
+      const unsigned long long rr = G.rec[b0 + x];
+      int a = rec_col(rr);
       r_col[x] = a;
-      r_meta[x] = G.meta[b0 + x];
+      r_meta[x] = rec_meta(rr);
       long long rs = G.row_ptr[a];
       r_start[x] = rs;
       r_len[x] = (int)(G.row_ptr[a + 1] - rs);
@@ -195,8 +205,10 @@ __global__ void __launch_bounds__(kQuadThreads) quad4_kernel(DevCatalog C, CSRVi
         int j = j0 + lane;
         bool found = false;
         int c = 0, y = 0;
+        unsigned long long rr = 0;
         if (j < ka) {
-          c = G.col[ra + j];
+          rr = G.rec[ra + j];
+          c = rec_col(rr);
           y = x + 1 + qlower_bound(r_col + x + 1, k - x - 1, c);
           found = y < k && r_col[y] == c;
         }
@@ -205,7 +217,7 @@ __global__ void __launch_bounds__(kQuadThreads) quad4_kernel(DevCatalog C, CSRVi
           int pos = nx + __popc(msk & lt);
           x_c[pos] = c;
           x_y[pos] = y;
-          x_m[pos] = G.meta[ra + j];
+          x_m[pos] = rec_meta(rr);
           long long cs = G.row_ptr[c];
           x_start[pos] = cs;
         }
@@ -246,12 +258,13 @@ __global__ void __launch_bounds__(kQuadThreads) quad4_kernel(DevCatalog C, CSRVi
         }
         const int z = lo;
         const int64_t e = x_start[z] + (f - x_pre[z]);
-        const int d = G.col[e];
+        const unsigned long long rr = G.rec[e];
+        const int d = rec_col(rr);
         const int z2 = z + 1 + qlower_bound(x_c + z + 1, nx - z - 1, d);
         if (z2 < nx && x_c[z2] == d) {
           const int v[4] = {p, a, x_c[z], d};
           const uint32_t m[6] = {r_meta[x], r_meta[x_y[z]], r_meta[x_y[z2]],
-                                 x_m[z],    x_m[z2],        G.meta[e]};
+                                 x_m[z],    x_m[z2],        rec_meta(rr)};
           int nroot = quad_contrib<WEIGHTED>(C, G, X, v, m);
           quads += nroot > 0;
           rooted += nroot;
@@ -276,8 +289,9 @@ __global__ void __launch_bounds__(kQuadThreads) quad4_kernel(DevCatalog C, CSRVi
 }  // namespace
 
 void launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bool weighted,
-                  unsigned long long* g_cnt, double* g_sum, unsigned long long* d_cnt,
-                  double* d_sum, unsigned long long* stats, cudaStream_t s) {
+                  unsigned long long* g_cnt, unsigned long long* g_fix, unsigned long long* d_cnt,
+                  unsigned long long* d_fix, double fscale, double dscale,
+                  unsigned long long* stats, cudaStream_t s) {
   if (C.n <= 0) return;
   QuadLayout L = quad_layout(Q.nbins, Q.cap);
   size_t smem = L.total;
@@ -292,7 +306,7 @@ void launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bo
     int64_t blocks = (int64_t)per_sm * 148;                                                   \
     int64_t need = ((int64_t)C.n + kQuadWarps - 1) / kQuadWarps;                              \
     if (blocks > need) blocks = need;                                                         \
-    kfn<<<(unsigned)blocks, kQuadThreads, smem, s>>>(C, G, Q, g_cnt, g_sum, d_cnt, d_sum, stats); \
+    kfn<<<(unsigned)blocks, kQuadThreads, smem, s>>>(C, G, Q, g_cnt, g_fix, d_cnt, d_fix, fscale, dscale, stats); \
   } while (0)
   if (weighted) GR_QUAD_LAUNCH(true); else GR_QUAD_LAUNCH(false);
 #undef GR_QUAD_LAUNCH

@@ -3,119 +3,149 @@
 // edge with a binary search into another vertex's row (find_dist,
 // :1579-1609).
 //
-// Here every triangle is enumerated exactly once, from its smallest internal
-// label p: for each a in R+(p) and each c in R+(a), c is looked up in R+(p),
-// which sits in shared memory.  The (a, c) work items of one root are
-// flattened over the warp's lanes through a prefix sum of |R+(a)|, so short
-// and long rows keep all lanes busy.  A found triangle contributes to the
-// rooted histogram of each non-buffer vertex r, with the bins of its three
-// edges, the find_normal mu bin of r's two edges taken in catalogue-id order
-// (as k1 < k2 in the reference's id-sorted row), and the product
-// (w_r w_first) w_second.
+// Every triangle is enumerated exactly once, from its smallest internal
+// label p.  A warp takes a root p and stages its upper row R+(p) in shared
+// memory together with the flags, catalogue ids and weights of those
+// neighbours, a small open-addressing hash table (label -> row position) and
+// an owner table mapping each flattened work item f to the neighbour a whose
+// row it reads.  The work items (a, c) for c in R+(a) are spread over the
+// lanes; each lane loads one 8-byte CSR record and probes the hash table for
+// c.  Hits (triangles p < a < c) are pushed to a per-warp queue that is
+// drained 32 at a time, so the binning work runs with every lane busy.
+//
+// A triangle contributes to the rooted histogram of each non-buffer vertex r
+// with the bins of its three edges (symmetric bin table), the find_normal mu
+// bin of r's two edges taken in catalogue-id order (k1 < k2 in the
+// reference's id-sorted row) and the product (w_r w_first) w_second.
 #include "gr_kernels.cuh"
 
 namespace gr {
 
 namespace {
 
-constexpr int kTriWarps = 8;
-constexpr int kTriThreads = kTriWarps * 32;
-
-struct TriLayout {
-  size_t off_cnt, off_sum, off_norm, off_rank, off_warp, warp_bytes, total;
-};
+constexpr int kTriMaxWarps = 32;  // block size is chosen at launch to fit shared memory
+constexpr size_t kSmemLimit = 227 * 1024;
+constexpr int kOwn = 512;    // flattened work items per owner-table chunk
+constexpr int kQueue = 64;   // hit queue entries per warp
+constexpr int kChunk = 4;    // roots taken per work-counter increment
 
 __host__ __device__ inline size_t align8(size_t x) { return (x + 7) & ~(size_t)7; }
+__host__ __device__ inline int hash_size(int cap) {
+  int h = 32;
+  while (h < 2 * cap) h <<= 1;
+  return h;
+}
+
+struct TriLayout {
+  size_t off_cnt, off_fix, off_norm, off_rank, off_warp, warp_bytes, total;
+  // per-warp sub-offsets
+  size_t o_rs, o_w, o_col, o_meta, o_orig, o_pre, o_hkey, o_qm, o_qxy, o_flag, o_hval, o_own;
+};
 
 __host__ __device__ inline TriLayout tri_layout(int nh, int nmu, int nbins, int cap, bool shist,
-                                                bool weighted) {
+                                                bool weighted, int nwarps) {
   TriLayout L;
   size_t o = 0;
   L.off_cnt = o;
   if (shist) o += (size_t)nh * 8;
-  L.off_sum = o;
-  if (shist && weighted) o += (size_t)nh * 8;
+  L.off_fix = o;
+  if (shist && weighted) o += (size_t)nh * 16;
   L.off_norm = o;
   o = align8(o + (size_t)nmu * nmu);
   L.off_rank = o;
   o = align8(o + sizeof(int) * 3 * (size_t)(nbins + 2));
   L.off_warp = o;
-  L.warp_bytes = align8((size_t)cap * (8 + 4 + 4) + (size_t)(cap + 1) * 4);
-  L.total = o + L.warp_bytes * kTriWarps;
+  const int hs = hash_size(cap);
+  size_t w = 0;
+  L.o_rs = w;   w += (size_t)cap * 8;
+  L.o_w = w;    w += (size_t)cap * 8;
+  L.o_col = w;  w += (size_t)cap * 4;
+  L.o_meta = w; w += (size_t)cap * 4;
+  L.o_orig = w; w += (size_t)cap * 4;
+  L.o_pre = w;  w += (size_t)(cap + 1) * 4;
+  L.o_hkey = w; w += (size_t)hs * 4;
+  L.o_qm = w;   w += (size_t)kQueue * 4;
+  L.o_qxy = w;  w += (size_t)kQueue * 2;
+  L.o_flag = w; w += (size_t)cap;
+  L.o_hval = w; w += (size_t)hs;
+  L.o_own = w;  w += (size_t)kOwn;
+  L.warp_bytes = align8(w);
+  L.total = o + L.warp_bytes * nwarps;
   return L;
 }
 
 struct TriCtx {
   const uint8_t* norm;
   const int* F;  // 3 x (nbins+2)
-  int nbins, nmu, ncfg, rsd;
+  int nbins, nmu, ncfg, rsd, nh;
   unsigned long long* cnt;
-  double* sum;
+  unsigned long long* lo;  // fixed-point sums: lo[k], lo[nh + k] = hi[k]
+  double fscale;
 };
 
 __device__ __forceinline__ int rank3_s(const int* F, int nb2, int a, int b, int c) {
   return 1 + (F[a] - F[1]) + (F[nb2 + b] - F[nb2 + a]) + (F[2 * nb2 + c] - F[2 * nb2 + b]);
 }
 
-template <bool WEIGHTED>
-__device__ __forceinline__ void tri_add(const TriCtx& X, int cfg, int mu1, int mu2, bool first_is_1,
-                                        int nr, double prod) {
-  int m = 1;
-  if (X.rsd) m = first_is_1 ? X.norm[(mu1 - 1) + X.nmu * (mu2 - 1)]
-                            : X.norm[(mu2 - 1) + X.nmu * (mu1 - 1)];
-  int k = (cfg - 1) + X.ncfg * ((m - 1) + X.nmu * nr);
-  atomicAdd(&X.cnt[k], 1ull);
-  if (WEIGHTED) atomicAdd(&X.sum[k], prod);
+__device__ __forceinline__ int normal_bin(const TriCtx& X, int mu1, int mu2, bool first_is_1) {
+  if (!X.rsd) return 1;
+  return first_is_1 ? X.norm[(mu1 - 1) + X.nmu * (mu2 - 1)] : X.norm[(mu2 - 1) + X.nmu * (mu1 - 1)];
 }
 
-// Triangle (p, a, c), p < a < c in labels, with edge metadata (p,a), (p,c),
-// (a,c).  Returns the number of rooted contributions.
+// One triangle (p, a, c) with p < a < c in labels.  Per-vertex data are
+// passed in; contributions that land in the same bin are merged before the
+// shared-memory atomics.  Returns the number of rooted contributions.
 template <bool WEIGHTED>
-__device__ __forceinline__ int tri_contrib(const DevCatalog& C, const TriCtx& X, uint8_t fp, int op,
-                                           double wp, int a, int c, uint32_t mpa, uint32_t mpc,
-                                           uint32_t mac) {
-  const uint8_t fa = C.flags[a], fc = C.flags[c];
-  const int oa = C.orig[a], oc = C.orig[c];
-  double wa = 0.0, wc = 0.0;
-  if (WEIGHTED) {
-    wa = C.w[a];
-    wc = C.w[c];
-  }
+__device__ __forceinline__ int tri_bin(const TriCtx& X, uint8_t fp, int op, double wp, uint8_t fa,
+                                       int oa, double wa, uint8_t fc, int oc, double wc,
+                                       uint32_t mpa, uint32_t mpc, uint32_t mac) {
   int s1 = meta_bin(mpa), s2 = meta_bin(mpc), s3 = meta_bin(mac);
   sort3i(s1, s2, s3);
   const int cfg = rank3_s(X.F, X.nbins + 2, s1, s2, s3);
   const int nr = (fp & FLAG_RANDOM) + (fa & FLAG_RANDOM) + (fc & FLAG_RANDOM);
-  int n = 0;
+  int m[3] = {-1, -1, -1};
+  double pr[3] = {0.0, 0.0, 0.0};
+  int cnt[3] = {0, 0, 0};
   if (!(fp & FLAG_BUFFER)) {  // root p: neighbours a, c
-    bool ac = oa < oc;
-    double pr = 0.0;
-    if (WEIGHTED) pr = ac ? (wp * wa) * wc : (wp * wc) * wa;
-    tri_add<WEIGHTED>(X, cfg, meta_muf(mpa), meta_muf(mpc), ac, nr, pr);
-    n++;
+    const bool ac = oa < oc;
+    m[0] = normal_bin(X, meta_muf(mpa), meta_muf(mpc), ac);
+    if (WEIGHTED) pr[0] = ac ? (wp * wa) * wc : (wp * wc) * wa;
+    cnt[0] = 1;
   }
   if (!(fa & FLAG_BUFFER)) {  // root a: neighbours p, c
-    bool pc = op < oc;
-    double pr = 0.0;
-    if (WEIGHTED) pr = pc ? (wa * wp) * wc : (wa * wc) * wp;
-    tri_add<WEIGHTED>(X, cfg, meta_mur(mpa), meta_muf(mac), pc, nr, pr);
-    n++;
+    const bool pc = op < oc;
+    m[1] = normal_bin(X, meta_mur(mpa), meta_muf(mac), pc);
+    if (WEIGHTED) pr[1] = pc ? (wa * wp) * wc : (wa * wc) * wp;
+    cnt[1] = 1;
   }
   if (!(fc & FLAG_BUFFER)) {  // root c: neighbours p, a
-    bool pa = op < oa;
-    double pr = 0.0;
-    if (WEIGHTED) pr = pa ? (wc * wp) * wa : (wc * wa) * wp;
-    tri_add<WEIGHTED>(X, cfg, meta_mur(mpc), meta_mur(mac), pa, nr, pr);
-    n++;
+    const bool pa = op < oa;
+    m[2] = normal_bin(X, meta_mur(mpc), meta_mur(mac), pa);
+    if (WEIGHTED) pr[2] = pa ? (wc * wp) * wa : (wc * wa) * wp;
+    cnt[2] = 1;
   }
-  return n;
+  const int total = cnt[0] + cnt[1] + cnt[2];
+  // merge equal bins
+  if (m[1] >= 0 && m[1] == m[0]) { cnt[0] += cnt[1]; pr[0] += pr[1]; cnt[1] = 0; }
+  if (m[2] >= 0 && m[2] == m[0]) { cnt[0] += cnt[2]; pr[0] += pr[2]; cnt[2] = 0; }
+  else if (m[2] >= 0 && m[2] == m[1] && cnt[1]) { cnt[1] += cnt[2]; pr[1] += pr[2]; cnt[2] = 0; }
+  const int base = (cfg - 1) + X.ncfg * X.nmu * nr;
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    if (cnt[r] == 0) continue;
+    const int k = base + X.ncfg * (m[r] - 1);
+    atomicAdd(&X.cnt[k], (unsigned long long)cnt[r]);
+    if (WEIGHTED) fix_add(&X.lo[k], &X.lo[X.nh + k], pr[r], X.fscale);
+  }
+  return total;
 }
 
 // first index in sorted a[0..n) with a[i] >= v
-__device__ __forceinline__ int lower_bound_i(const int* a, int n, int v) {
+__device__ __forceinline__ int lower_bound_g(const unsigned long long* a, int n, int v) {
   int lo = 0, hi = n;
   while (lo < hi) {
     int mid = (lo + hi) >> 1;
-    if (a[mid] < v)
+    if (rec_col(a[mid]) < v)
       lo = mid + 1;
     else
       hi = mid;
@@ -123,21 +153,29 @@ __device__ __forceinline__ int lower_bound_i(const int* a, int n, int v) {
   return lo;
 }
 
+__device__ __forceinline__ uint32_t hash_slot(int key, int hmask) {
+  return ((uint32_t)key * 2654435761u) & (uint32_t)hmask;
+}
+
 template <bool WEIGHTED, bool SHIST>
-__global__ void __launch_bounds__(kTriThreads) tri3_kernel(DevCatalog C, CSRView G, TriParams T,
+__global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, CSRView G, TriParams T,
                                                            unsigned long long* __restrict__ g_cnt,
-                                                           double* __restrict__ g_sum,
-                                                           unsigned long long* __restrict__ stats) {
+                                                           unsigned long long* __restrict__ g_fix,
+                                                           double fscale,
+                                                           unsigned long long* __restrict__ stats,
+                                                           int* __restrict__ work) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int nh = T.ncfg * T.nmu * 4;
-  const TriLayout L = tri_layout(nh, T.nmu, T.nbins, T.cap, SHIST, WEIGHTED);
+  const TriLayout L = tri_layout(nh, T.nmu, T.nbins, T.cap, SHIST, WEIGHTED, blockDim.x >> 5);
   TriCtx X;
   X.nbins = T.nbins;
   X.nmu = T.nmu;
   X.ncfg = T.ncfg;
   X.rsd = T.rsd;
+  X.nh = nh;
+  X.fscale = fscale;
   X.cnt = SHIST ? reinterpret_cast<unsigned long long*>(smem + L.off_cnt) : g_cnt;
-  X.sum = SHIST ? reinterpret_cast<double*>(smem + L.off_sum) : g_sum;
+  X.lo = SHIST ? reinterpret_cast<unsigned long long*>(smem + L.off_fix) : g_fix;
   uint8_t* s_norm = smem + L.off_norm;
   int* s_F = reinterpret_cast<int*>(smem + L.off_rank);
   X.norm = s_norm;
@@ -145,7 +183,10 @@ __global__ void __launch_bounds__(kTriThreads) tri3_kernel(DevCatalog C, CSRView
   if (SHIST) {
     for (int k = threadIdx.x; k < nh; k += blockDim.x) {
       X.cnt[k] = 0ull;
-      if (WEIGHTED) X.sum[k] = 0.0;
+      if (WEIGHTED) {
+        X.lo[k] = 0ull;
+        X.lo[nh + k] = 0ull;
+      }
     }
   }
   for (int k = threadIdx.x; k < T.nmu * T.nmu; k += blockDim.x) s_norm[k] = T.rsd ? T.normal[k] : 1;
@@ -154,91 +195,169 @@ __global__ void __launch_bounds__(kTriThreads) tri3_kernel(DevCatalog C, CSRView
   __syncthreads();
 
   const int lane = threadIdx.x & 31;
-  const int wib = threadIdx.x >> 5;
-  unsigned char* wbase = smem + L.off_warp + L.warp_bytes * wib;
-  long long* s_rstart = reinterpret_cast<long long*>(wbase);
-  int* s_col = reinterpret_cast<int*>(wbase + (size_t)T.cap * 8);
-  uint32_t* s_meta = reinterpret_cast<uint32_t*>(wbase + (size_t)T.cap * 12);
-  int* s_pre = reinterpret_cast<int*>(wbase + (size_t)T.cap * 16);
+  const unsigned lt = (1u << lane) - 1u;
+  unsigned char* wb = smem + L.off_warp + L.warp_bytes * (threadIdx.x >> 5);
+  long long* s_rs = reinterpret_cast<long long*>(wb + L.o_rs);
+  double* s_w = reinterpret_cast<double*>(wb + L.o_w);
+  int* s_col = reinterpret_cast<int*>(wb + L.o_col);
+  uint32_t* s_meta = reinterpret_cast<uint32_t*>(wb + L.o_meta);
+  int* s_orig = reinterpret_cast<int*>(wb + L.o_orig);
+  int* s_pre = reinterpret_cast<int*>(wb + L.o_pre);
+  int* s_hkey = reinterpret_cast<int*>(wb + L.o_hkey);
+  uint32_t* s_qm = reinterpret_cast<uint32_t*>(wb + L.o_qm);
+  uint16_t* s_qxy = reinterpret_cast<uint16_t*>(wb + L.o_qxy);
+  uint8_t* s_flag = wb + L.o_flag;
+  uint8_t* s_hval = wb + L.o_hval;
+  uint8_t* s_own = wb + L.o_own;
+  const int hs = hash_size(T.cap);
+  const int hmask = hs - 1;
 
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
   unsigned long long tris = 0, rooted = 0, probes = 0;
 
-  for (int p = warp; p < C.n; p += nwarps) {
-    const int64_t b0 = G.row_ptr[p];
-    const int k = (int)(G.row_ptr[p + 1] - b0);
-    if (k < 2) continue;
-    const uint8_t fp = C.flags[p];
-    const int op = C.orig[p];
-    const double wp = WEIGHTED ? C.w[p] : 0.0;
-    if (k <= T.cap) {
-      __syncwarp();
-      int carry = 0;
-      for (int xb = 0; xb < k; xb += 32) {
-        int x = xb + lane;
-        int len = 0;
-        if (x < k) {
-          int a = G.col[b0 + x];
-          s_col[x] = a;
-          s_meta[x] = G.meta[b0 + x];
-          long long rs = G.row_ptr[a];
-          s_rstart[x] = rs;
-          len = (int)(G.row_ptr[a + 1] - rs);
-        }
-        int incl = len;
+  for (;;) {
+    int base_root = 0;
+    if (lane == 0) base_root = atomicAdd(work, kChunk);
+    base_root = __shfl_sync(0xffffffffu, base_root, 0);
+    if (base_root >= C.n) break;
+    const int end_root = min(base_root + kChunk, C.n);
+    for (int p = base_root; p < end_root; ++p) {
+      const int64_t b0 = G.row_ptr[p];
+      const int k = (int)(G.row_ptr[p + 1] - b0);
+      if (k < 2) continue;
+      const uint8_t fp = C.flags[p];
+      const int op = C.orig[p];
+      const double wp = WEIGHTED ? C.w[p] : 0.0;
+      if (k <= T.cap) {
+        __syncwarp();
+        for (int h = lane; h < hs; h += 32) s_hkey[h] = -1;
+        __syncwarp();
+        // stage R+(p) and the data of its vertices; insert into the hash table
+        int carry = 0;
+        for (int xb = 0; xb < k; xb += 32) {
+          const int x = xb + lane;
+          int len = 0;
+          if (x < k) {
+            const unsigned long long r = G.rec[b0 + x];
+            const int a = rec_col(r);
+            s_col[x] = a;
+            s_meta[x] = rec_meta(r);
+            const long long rs = G.row_ptr[a];
+            s_rs[x] = rs;
+            len = (int)(G.row_ptr[a + 1] - rs);
+            s_flag[x] = C.flags[a];
+            s_orig[x] = C.orig[a];
+            if (WEIGHTED) s_w[x] = C.w[a];
+            uint32_t h = hash_slot(a, hmask);
+            for (int t = 0; t < hs; ++t) {
+              if (atomicCAS(&s_hkey[h], -1, a) == -1) {
+                s_hval[h] = (uint8_t)x;
+                break;
+              }
+              h = (h + 1) & hmask;
+            }
+          }
+          int incl = len;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          int y = __shfl_up_sync(0xffffffffu, incl, o);
-          if (lane >= o) incl += y;
+          for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+          }
+          if (x < k) s_pre[x + 1] = carry + incl;
+          carry += __shfl_sync(0xffffffffu, incl, 31);
         }
-        if (x < k) s_pre[x + 1] = carry + incl;
-        carry += __shfl_sync(0xffffffffu, incl, 31);
-      }
-      if (lane == 0) s_pre[0] = 0;
-      __syncwarp();
-      const int W = carry;
-      probes += (lane == 0) ? (unsigned long long)W : 0ull;
-      for (int base = 0; base < W; base += 32) {
-        int f = base + lane;
-        if (f >= W) break;
-        // last x with pre[x] <= f
-        int lo = 0, hi = k - 1;
-        while (lo < hi) {
-          int mid = (lo + hi + 1) >> 1;
-          if (s_pre[mid] <= f)
-            lo = mid;
-          else
-            hi = mid - 1;
+        if (lane == 0) s_pre[0] = 0;
+        const int W = carry;
+        if (lane == 0) probes += (unsigned long long)W;
+        int qn = 0;
+        int x0 = 0;  // first row overlapping the current owner chunk
+        for (int fb = 0; fb < W; fb += kOwn) {
+          const int fe = min(W, fb + kOwn);
+          __syncwarp();
+          // owner table for work items [fb, fe)
+          while (x0 < k && s_pre[x0 + 1] <= fb) ++x0;
+          for (int x = x0; x < k && s_pre[x] < fe; ++x) {
+            const int lo = max(s_pre[x], fb), hi = min(s_pre[x + 1], fe);
+            for (int f = lo + lane; f < hi; f += 32) s_own[f - fb] = (uint8_t)x;
+          }
+          __syncwarp();
+          for (int f0 = fb; f0 < fe; f0 += 32) {
+            const int f = f0 + lane;
+            bool hit = false;
+            int x = 0, y = 0;
+            uint32_t mac = 0;
+            if (f < fe) {
+              x = s_own[f - fb];
+              const unsigned long long r = G.rec[s_rs[x] + (f - s_pre[x])];
+              const int c = rec_col(r);
+              mac = rec_meta(r);
+              uint32_t h = hash_slot(c, hmask);
+              for (int t = 0; t < hs; ++t) {
+                const int key = s_hkey[h];
+                if (key == c) {
+                  hit = true;
+                  y = s_hval[h];
+                  break;
+                }
+                if (key < 0) break;
+                h = (h + 1) & hmask;
+              }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (hit) {
+              const int pos = qn + __popc(m & lt);
+              s_qm[pos] = mac;
+              s_qxy[pos] = (uint16_t)(x | (y << 8));
+            }
+            qn += __popc(m);
+            if (qn >= 32) {
+              __syncwarp();
+              const int e = qn - 32 + lane;
+              const uint16_t xy = s_qxy[e];
+              const int qx = xy & 0xff, qy = xy >> 8;
+              const int nroot = tri_bin<WEIGHTED>(
+                  X, fp, op, wp, s_flag[qx], s_orig[qx], WEIGHTED ? s_w[qx] : 0.0, s_flag[qy],
+                  s_orig[qy], WEIGHTED ? s_w[qy] : 0.0, s_meta[qx], s_meta[qy], s_qm[e]);
+              tris += nroot > 0;
+              rooted += nroot;
+              qn -= 32;
+              __syncwarp();
+            }
+          }
         }
-        const int x = lo;
-        const int64_t e = s_rstart[x] + (f - s_pre[x]);
-        const int c = G.col[e];
-        const int y = lower_bound_i(s_col, k, c);
-        if (y < k && s_col[y] == c) {
-          int nroot = tri_contrib<WEIGHTED>(C, X, fp, op, wp, s_col[x], c, s_meta[x], s_meta[y],
-                                            G.meta[e]);
+        __syncwarp();
+        if (lane < qn) {
+          const uint16_t xy = s_qxy[lane];
+          const int qx = xy & 0xff, qy = xy >> 8;
+          const int nroot = tri_bin<WEIGHTED>(
+              X, fp, op, wp, s_flag[qx], s_orig[qx], WEIGHTED ? s_w[qx] : 0.0, s_flag[qy],
+              s_orig[qy], WEIGHTED ? s_w[qy] : 0.0, s_meta[qx], s_meta[qy], s_qm[lane]);
           tris += nroot > 0;
           rooted += nroot;
         }
-      }
-    } else {
-      // Long row: the same enumeration with the row read from global memory.
-      const int* rowc = G.col + b0;
-      for (int x = 0; x < k - 1; ++x) {
-        const int a = rowc[x];
-        const uint32_t mpa = G.meta[b0 + x];
-        const int64_t ra = G.row_ptr[a];
-        const int ka = (int)(G.row_ptr[a + 1] - ra);
-        if (lane == 0) probes += (unsigned long long)ka;
-        for (int j = lane; j < ka; j += 32) {
-          const int c = G.col[ra + j];
-          const int y = lower_bound_i(rowc, k, c);
-          if (y < k && rowc[y] == c) {
-            int nroot = tri_contrib<WEIGHTED>(C, X, fp, op, wp, a, c, mpa, G.meta[b0 + y],
-                                              G.meta[ra + j]);
-            tris += nroot > 0;
-            rooted += nroot;
+      } else {
+        // Long row: the same enumeration reading the row from global memory.
+        const unsigned long long* rowp = G.rec + b0;
+        for (int x = 0; x < k - 1; ++x) {
+          const unsigned long long ra_rec = rowp[x];
+          const int a = rec_col(ra_rec);
+          const uint32_t mpa = rec_meta(ra_rec);
+          const int64_t ra = G.row_ptr[a];
+          const int ka = (int)(G.row_ptr[a + 1] - ra);
+          const uint8_t fa = C.flags[a];
+          const int oa = C.orig[a];
+          const double wa = WEIGHTED ? C.w[a] : 0.0;
+          if (lane == 0) probes += (unsigned long long)ka;
+          for (int j = lane; j < ka; j += 32) {
+            const unsigned long long r = G.rec[ra + j];
+            const int c = rec_col(r);
+            const int y = x + 1 + lower_bound_g(rowp + x + 1, k - x - 1, c);
+            if (y < k && rec_col(rowp[y]) == c) {
+              const int nroot = tri_bin<WEIGHTED>(X, fp, op, wp, fa, oa, wa, C.flags[c], C.orig[c],
+                                                  WEIGHTED ? C.w[c] : 0.0, mpa, rec_meta(rowp[y]),
+                                                  rec_meta(r));
+              tris += nroot > 0;
+              rooted += nroot;
+            }
           }
         }
       }
@@ -258,10 +377,10 @@ __global__ void __launch_bounds__(kTriThreads) tri3_kernel(DevCatalog C, CSRView
   if (SHIST) {
     __syncthreads();
     for (int k = threadIdx.x; k < nh; k += blockDim.x) {
-      unsigned long long v = X.cnt[k];
+      const unsigned long long v = X.cnt[k];
       if (v) {
         atomicAdd(&g_cnt[k], v);
-        if (WEIGHTED) atomicAdd(&g_sum[k], X.sum[k]);
+        if (WEIGHTED) fix_merge(&g_fix[k], &g_fix[nh + k], X.lo[k], X.lo[nh + k]);
       }
     }
   }
@@ -269,27 +388,44 @@ __global__ void __launch_bounds__(kTriThreads) tri3_kernel(DevCatalog C, CSRView
 
 }  // namespace
 
+// Warps per block: as many as fit in shared memory (at most 32).
+static int tri3_warps(const TriParams& T, bool weighted, bool shist) {
+  const int nh = T.ncfg * T.nmu * 4;
+  int nw = kTriMaxWarps;
+  while (nw > 1 && tri_layout(nh, T.nmu, T.nbins, T.cap, shist, weighted, nw).total > kSmemLimit)
+    nw >>= 1;
+  return nw;
+}
+
+size_t tri3_smem_bytes(const TriParams& T, bool weighted) {
+  const int nh = T.ncfg * T.nmu * 4;
+  const bool shist = (size_t)nh * 8 * (weighted ? 3 : 1) <= kMaxHistSmem;
+  return tri_layout(nh, T.nmu, T.nbins, T.cap, shist, weighted, tri3_warps(T, weighted, shist)).total;
+}
+
 void launch_tri3(const DevCatalog& C, const CSRView& G, const TriParams& T, bool weighted,
-                 unsigned long long* g_cnt, double* g_sum, unsigned long long* stats,
-                 cudaStream_t s) {
+                 unsigned long long* g_cnt, unsigned long long* g_fix, double fscale,
+                 unsigned long long* stats, int* work, cudaStream_t s) {
   if (C.n <= 0) return;
   const int nh = T.ncfg * T.nmu * 4;
-  size_t hist_bytes = (size_t)nh * 8 * (weighted ? 2 : 1);
-  const bool shist = hist_bytes <= kMaxHistSmem;
-  TriLayout L = tri_layout(nh, T.nmu, T.nbins, T.cap, shist, weighted);
-  size_t smem = L.total;
+  const bool shist = (size_t)nh * 8 * (weighted ? 3 : 1) <= kMaxHistSmem;
+  const int nw = tri3_warps(T, weighted, shist);
+  const TriLayout L = tri_layout(nh, T.nmu, T.nbins, T.cap, shist, weighted, nw);
+  const size_t smem = L.total;
+  if (smem > kSmemLimit) throw Error{-2, "3PCF: per-warp shared memory exceeds the SM limit"};
+  GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));
 #define GR_TRI_LAUNCH(W, S)                                                                   \
   do {                                                                                        \
     auto kfn = tri3_kernel<W, S>;                                                             \
     GR_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
                                      (int)smem));                                             \
     int per_sm = 0;                                                                           \
-    GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kTriThreads, smem)); \
+    GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nw * 32, smem));   \
     if (per_sm < 1) per_sm = 1;                                                               \
     int64_t blocks = (int64_t)per_sm * 148;                                                   \
-    int64_t need = ((int64_t)C.n + kTriWarps - 1) / kTriWarps;                                \
+    const int64_t need = ((int64_t)C.n + nw * kChunk - 1) / (nw * kChunk);                    \
     if (blocks > need) blocks = need;                                                         \
-    kfn<<<(unsigned)blocks, kTriThreads, smem, s>>>(C, G, T, g_cnt, g_sum, stats);            \
+    kfn<<<(unsigned)blocks, nw * 32, smem, s>>>(C, G, T, g_cnt, g_fix, fscale, stats, work);   \
   } while (0)
   if (weighted) {
     if (shist) GR_TRI_LAUNCH(true, true); else GR_TRI_LAUNCH(true, false);
