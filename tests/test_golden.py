@@ -1,0 +1,74 @@
+"""Known-answer configurations (tests/golden/known_answers.json, made by
+tests/golden/make_golden.py from geometry alone) against the oracle (CPU)
+and against the CUDA library (GPU)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from gramsci_b200 import catalogs
+
+CASES = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "known_answers.json")))
+
+
+def _prep(c):
+    xyz = np.array(c["xyz"], np.float64)
+    n = len(xyz)
+    w = catalogs.normalise(np.array(c["w"], np.float64), c["n_data"], n - c["n_data"])
+    return xyz, w
+
+
+def _check(c, counts2, counts3=None, N2_3=None):
+    exp2 = np.zeros_like(counts2)
+    for k, v in c["counts2"].items():
+        b, m, cat = map(int, k.split(","))
+        exp2[b - 1, m - 1, cat] = v
+    assert np.array_equal(counts2, exp2), c["name"]
+    if counts3 is not None and "counts3" in c:
+        exp3 = np.zeros_like(counts3)
+        for k, v in c["counts3"].items():
+            cfg, m, nr = map(int, k.split(","))
+            exp3[cfg - 1, m - 1, nr] = v
+        assert np.array_equal(counts3, exp3), c["name"]
+    if N2_3 is not None and "N2_3" in c:
+        for k, v in c["N2_3"].items():
+            cfg, m = map(int, k.split(","))
+            assert abs(N2_3[cfg - 1, m - 1] - v) <= 1e-15 * abs(v)
+
+
+@pytest.mark.parametrize("c", CASES, ids=[c["name"] for c in CASES])
+def test_oracle_known_answers(oracle, c):
+    xyz, w = _prep(c)
+    G = oracle.Graph(xyz, c["rmin"], c["rmax"], c["nbins"], c["nmu"])
+    r2 = G.pcf2(w, c["n_data"])
+    r3 = G.pcf3(w, c["n_data"]) if c["n_data"] >= 3 else None
+    _check(c, r2["counts"], r3["counts"] if r3 else None, r3["N2"] if r3 else None)
+    if "edges" in c:
+        rp, col, b, mu = G.csr()
+        for k, (eb, em) in c["edges"].items():
+            i, j = map(int, k.split(","))
+            row = list(col[rp[i]:rp[i + 1]])
+            e = rp[i] + row.index(j)
+            assert (b[e], mu[e]) == (eb, em), k
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+@pytest.mark.parametrize("c", CASES, ids=[c["name"] for c in CASES])
+def test_gpu_known_answers(gpu_ctx, c, precision):
+    xyz, w = _prep(c)
+    gpu_ctx.set_precision(precision)
+    gpu_ctx.set_catalog(xyz, w, c["n_data"])
+    gpu_ctx.set_bins(c["rmin"], c["rmax"], c["nbins"], c["nmu"])
+    r2 = gpu_ctx.count_2pcf()
+    r3 = gpu_ctx.count_3pcf()
+    _check(c, r2["counts"], r3["counts"], r3["N2"])
+    if "edges" in c:
+        rp, col, b, mu = gpu_ctx.graph()
+        for k, (eb, em) in c["edges"].items():
+            i, j = map(int, k.split(","))
+            row = list(col[rp[i]:rp[i + 1]])
+            e = rp[i] + row.index(j)
+            assert (b[e], mu[e]) == (eb, em), k
+    gpu_ctx.set_precision("f32")
