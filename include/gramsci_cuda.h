@@ -135,6 +135,28 @@ int gr_graph_export(gr_ctx* ctx, int64_t* row_ptr, int32_t* col, uint8_t* bin, u
 /* Statistics of the last count call. */
 int gr_get_stats(gr_ctx* ctx, gr_stats* out);
 
+/* 2PCF without any device allocation.  This entry point has no counterpart
+ * in the reference; it exists for callers that cannot call cudaMalloc (code
+ * running inside another framework's memory pool or under a fixed memory
+ * budget, plugins limited to the buffers their host gives them).  It takes
+ * DEVICE pointers: the catalogue (xyz interleaved, signed normalised w,
+ * galaxies first; no buffer points) and the outputs, any of which may be
+ * NULL: counts (nbins, nmu, 4) int64, catsum (nbins, nmu, 4), N2 and N3
+ * (nbins, nmu), the same quantities as gr_count_2pcf.  All intermediate data
+ * live in one fixed device array inside the library (about 4.3 MB per GPU,
+ * held until the process exits).  At most GR_NOALLOC_MAX_POINTS points and
+ * nbins*nmu <= GR_NOALLOC_MAX_BINS; larger inputs return GR_E_CAPACITY and
+ * run nothing.  Work is queued on `stream` (cudaStream_t, NULL = default
+ * stream) on the current device; the outputs are ready when it completes.
+ * The first call on a device looks up the array's device address, so make it
+ * before any stream capture.  All calls share the array: calls whose work
+ * overlaps on the GPU race and must be serialised by the caller. */
+#define GR_NOALLOC_MAX_POINTS 32768
+#define GR_NOALLOC_MAX_BINS 4096
+int gr_count_2pcf_noalloc(const double* d_xyz, const double* d_w, int64_t n_data, int64_t n_rand,
+                          double rmin, double rmax, int32_t nbins, int32_t nmu, int64_t* d_counts,
+                          double* d_catsum, double* d_N2, double* d_N3, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
