@@ -1,0 +1,117 @@
+"""CPU tests of the `gramsci` driver's host side (libgramsci_host.so):
+option parsing as the reference's parseOptions does it, list-directed
+catalogue reading, weight normalisation, radial bin edges and the E14.7
+output records."""
+import os
+
+import numpy as np
+import pytest
+
+from gramsci_b200 import catalogs, host
+
+
+@pytest.mark.parametrize("v,s", [
+    (1.0, " 0.1000000E+01"), (-0.5, "-0.5000000E+00"), (0.0, " 0.0000000E+00"),
+    (123456789.0, " 0.1234568E+09"), (9.99999996, " 0.1000000E+02"), (0.1, " 0.1000000E+00"),
+    (1e-300, " 0.1000000-299"), (1e100, " 0.1000000+101"), (float("nan"), "           NaN"),
+    (float("inf"), "      Infinity"), (-float("inf"), "     -Infinity"),
+    (-2.124343822e-07, "-0.2124344E-06"),
+])
+def test_e14_7(v, s):
+    assert host.format_e14_7(v) == s
+
+
+def test_options_defaults_and_six_character_match():
+    o = host.parse_args(["-gal", "g", "-ran", "r", "-rmin", "1d1", "-rmax", "5.0E1", "-nbins_x",
+                         "10", "-nmu", "4", "-2pcf", "-3pcf"])
+    assert o.error == 0 and not o.help
+    assert (o.gal, o.ran, o.out) == (b"g", b"r", b"result.txt")
+    assert (o.rmin, o.rmax, o.nbins, o.nmu, o.rsd) == (10.0, 50.0, 10, 4, 1)
+    assert (o.two_pcf, o.three_pcf, o.four_pcf, o.rancat) == (1, 1, 0, 1)
+
+
+def test_options_errors():
+    assert host.parse_args(["-gal", "g", "-rmin", "1"]).help == 1  # fewer than 6 arguments
+    o = host.parse_args(["-gal", "g", "-ran", "r", "-rmin", "1", "-bogus", "-2pcf"])
+    assert o.error == 1 and b"unknown option -bogus ignored" in o.message
+    o = host.parse_args(["-gal", "g", "-ran", "r", "-rmin", "one", "-2pcf"])
+    assert o.error == 2
+    o = host.parse_args(["-gal", "g", "-ran", "r", "-nbins", "2.5", "-2pcf"])
+    assert o.error == 2
+    o = host.parse_args(["-cut", "3.loadnodes", "-rmin", "1", "-rmax", "2", "-2pcf"])
+    assert o.cut_mode == 1 and o.out == b"3.loadnodes"
+
+
+def test_read_catalogue_list_directed(tmp_path):
+    g = tmp_path / "g.txt"
+    g.write_text("1 2 3 1.0\n4.0d0, 5, 6, 2\n\n7 8\n9 3 extra ignored\n")
+    r = tmp_path / "r.txt"
+    r.write_text("0 0 0 1\n1 1 1 1\n")
+    xyz, w, nd, nr = host.read_catalogue(str(g), str(r))
+    # the blank line and the split record count as one value-read each, as
+    # gfortran's list-directed count loop sees them
+    assert (nd, nr) == (4, 2)
+    assert np.array_equal(xyz[:3], [[1, 2, 3], [4, 5, 6], [7, 8, 9]])
+    assert np.array_equal(w[:3], [1.0, 2.0, 3.0])
+    assert np.array_equal(xyz[4:], [[0, 0, 0], [1, 1, 1]])
+
+
+def test_read_catalogue_roundtrip(tmp_path):
+    cat = catalogs.make("c1_2pcf", scale=0.01)
+    gp, rp = tmp_path / "g", tmp_path / "r"
+    catalogs.write_ascii(gp, cat.xyz[:cat.n_data], cat.w[:cat.n_data])
+    catalogs.write_ascii(rp, cat.xyz[cat.n_data:], cat.w[cat.n_data:])
+    xyz, w, nd, nr = host.read_catalogue(str(gp), str(rp))
+    assert (nd, nr) == (cat.n_data, cat.n_rand)
+    assert np.array_equal(xyz, cat.xyz) and np.array_equal(w, cat.w)
+
+
+def test_radial_bins():
+    e = host.radial_bins(10.0, 50.0, 10)
+    assert np.array_equal(e, 10.0 + np.arange(11) * 40.0 / 10)
+    el = host.radial_bins(1.0, 100.0, 2, logbins=True)
+    assert np.allclose(el, [1.0, 10.0, 100.0], rtol=1e-15)
+
+
+def test_writers_layout(tmp_path):
+    nb, nm = 3, 2
+    e = host.radial_bins(1.0, 10.0, nb)
+    N2 = np.arange(nb * nm, dtype=float).reshape(nb, nm, order="F") + 1
+    N3 = np.full((nb, nm), 2.0)
+    p = tmp_path / "o2"
+    assert host.write_2pcf(str(p), e, nb, nm, N2, N3) == 0
+    lines = p.read_text().splitlines()
+    assert lines[0] == " r1 min, r1 max, r2 min, r2 max, NN, RR, 2pcf (xi)"
+    assert len(lines) == 1 + nb * nm
+    # row order: radial bin outer, mu bin inner; columns 15 characters apart
+    assert lines[1] == " ".join(host.format_e14_7(v) for v in
+                                [1.0, 4.0, -1.0, 0.0, N2[0, 0], 2.0, N2[0, 0] / 2.0])
+    assert lines[2].split()[2:4] == [host.format_e14_7(0.0).strip(), host.format_e14_7(1.0).strip()]
+    nc = nb * (nb + 1) * (nb + 2) // 6
+    p3 = tmp_path / "o3"
+    assert host.write_3pcf(str(p3), e, nb, 1, np.ones((nc, 1)), np.ones((nc, 1))) == 0
+    l3 = p3.read_text().splitlines()
+    assert len(l3) == 1 + nc and len(l3[1].split()) == 9
+    p3m = tmp_path / "o3m"
+    assert host.write_3pcf(str(p3m), e, nb, nm, np.ones((nc, nm)), np.ones((nc, nm))) == 0
+    l3m = p3m.read_text().splitlines()
+    assert len(l3m) == 1 + nc * nm and len(l3m[1].split()) == 11
+    nc4 = nb * (nb + 1) * (nb + 2) * (nb + 3) // 24
+    p4 = tmp_path / "o4"
+    z = np.ones((nc4, nb, nb))
+    assert host.write_4pcf(str(p4), e, nb, z, z, np.ones((nc4, nb, nb, 6)), np.ones((nc4, nb, nb, 6))) == 0
+    l4 = p4.read_text().splitlines()
+    assert len(l4) == 1 + nc4 * nb * nb and len(l4[1].split()) == 14
+
+
+def test_cli_help_and_unknown_option():
+    import subprocess
+
+    r = subprocess.run([host.CLI_PATH, "-help"], capture_output=True, text=True)
+    assert r.returncode == 0 and "usage" in r.stdout
+    r = subprocess.run([host.CLI_PATH, "-gal", "a", "-ran", "b", "-rmin", "1", "-what", "-2pcf"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0 and "unknown option -what ignored" in r.stdout
+    r = subprocess.run([host.CLI_PATH, "-gal", "a", "-ran", "b", "-rmin", "x", "-rmax", "2"],
+                       capture_output=True, text=True)
+    assert r.returncode == 2
