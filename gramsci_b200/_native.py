@@ -72,6 +72,8 @@ SIGNATURES = {
     "gr_graph_nedges": (ctypes.c_int, [_ctx, _i64]),
     "gr_graph_export": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp]),
     "gr_get_stats": (ctypes.c_int, [_ctx, ctypes.POINTER(GrStats)]),
+    "gr_adjoint_2pcf": (ctypes.c_int, [_ctx, _vp, _vp, _vp]),
+    "gr_adjoint_3pcf": (ctypes.c_int, [_ctx, _vp, _vp, _vp]),
     "gr_count_2pcf_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.c_int64,
                                              ctypes.c_double, ctypes.c_double, ctypes.c_int32,
                                              ctypes.c_int32, _vp, _vp, _vp, _vp, _vp]),

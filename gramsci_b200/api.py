@@ -162,6 +162,24 @@ class Context:
                     counts=_fortran(counts, nc, nb, nb, 5), catsum=_fortran(catsum, nc, nb, nb, 5),
                     dcount=_fortran(dcount, nc, nb, nb, 6, 4), dsum=_fortran(dsum, nc, nb, nb, 6, 4))
 
+    def _adjoint(self, fn, cot2, cot3, shape):
+        c2 = np.ascontiguousarray(np.asarray(cot2, np.float64).reshape(shape).T.ravel())
+        c3 = None if cot3 is None else np.ascontiguousarray(
+            np.asarray(cot3, np.float64).reshape(shape).T.ravel())
+        g = np.zeros(self.n)
+        self._check(fn(self._h, _ptr(c2), _ptr(c3), _ptr(g)))
+        return g
+
+    def adjoint_2pcf(self, cot2, cot3=None):
+        """Gradient of sum(cot2*N2) + sum(cot3*N3) of the 2PCF with respect to
+        the weights (catalogue order)."""
+        return self._adjoint(self._lib.gr_adjoint_2pcf, cot2, cot3, (self.nbins, self.nmu))
+
+    def adjoint_3pcf(self, cot2, cot3=None):
+        """Gradient of sum(cot2*N2) + sum(cot3*N3) of the 3PCF with respect to
+        the weights (catalogue order)."""
+        return self._adjoint(self._lib.gr_adjoint_3pcf, cot2, cot3, (ncfg3(self.nbins), self.nmu))
+
     def graph(self):
         """The (rmin, rmax) neighbour graph in the reference's layout: rows in
         catalogue order, ids sorted, radial bin and mu bin per edge."""

@@ -45,6 +45,8 @@ struct gr_ctx {
   double wmax = 0.0;                      // max |w| over the catalogue
   DevBuf<unsigned char> uniform_flag;
   DevBuf<int> work;
+  DevBuf<double> cot, grad;              // adjoint inputs / output
+  DevBuf<unsigned long long> gfix;       // adjoint fixed-point gradients (lo[n], hi[n])
   gr_stats st{};
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
@@ -508,7 +510,7 @@ int gr_count_3pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
   T.nmu = nmu;
   T.ncfg = ncfg;
   T.rsd = nmu >= 2;
-  T.cap = round_cap((int64_t)gst[2], 32, 256);
+  T.cap = round_cap(c->csr.max_deg, 32, 256);
   T.normal = c->normal_dev.p;
   make_rank_tables(T.rank, c->nbins, 3);
   CSRView G{c->csr.row_ptr.p, c->csr.rec.p, c->csr.deg_full.p};
@@ -738,6 +740,110 @@ int gr_graph_export(gr_ctx* c, int64_t* row_ptr, int32_t* col, uint8_t* bin, uin
     if (bin) bin[k] = (uint8_t)((ent[k] >> 8) & 0xff);
     if (mu) mu[k] = (uint8_t)(ent[k] & 0xff);
   }
+  GR_API_END(c)
+}
+
+// ---------------------------------------------------------------- adjoints --
+static double max_abs(const double* a, int64_t n) {
+  double m = 0.0;
+  if (a)
+    for (int64_t i = 0; i < n; ++i) m = std::max(m, std::fabs(a[i]));
+  return m;
+}
+
+static void finish_grad(gr_ctx* c, double gscale, double* grad_w, cudaEvent_t q0) {
+  cudaStream_t s = c->stream();
+  const int64_t n = c->n;
+  c->grad.reserve(n + 1);
+  launch_grad_finish((int)n, c->index.orig.p, c->gfix.p, c->gfix.p + n, gscale, c->grad.p, s);
+  GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
+  if (n > 0) GR_CUDA_TRY(cudaMemcpyAsync(grad_w, c->grad.p, sizeof(double) * n, cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaStreamSynchronize(s));
+  c->st.ms_query = ev_ms(q0, c->ev[3]);
+}
+
+int gr_adjoint_2pcf(gr_ctx* c, const double* cot2, const double* cot3, double* grad_w) {
+  GR_API_BEGIN(c)
+  require_ready(c);
+  if (!cot2 || !grad_w) return set_err(c, GR_E_ARG, "null cot2 or grad_w");
+  ensure_events(c);
+  cudaStream_t s = c->stream();
+  const int nbm = c->nbins * c->nmu;
+  const int64_t n = c->n;
+  const double cmax = max_abs(cot2, nbm) + max_abs(cot3, nbm);
+  const double gscale = fix_scale(2.0 * cmax * c->wmax);
+  c->cot.reserve(2 * nbm);
+  c->gfix.reserve(2 * n + 2);
+  c->work.reserve(4);
+  GR_CUDA_TRY(cudaMemcpyAsync(c->cot.p, cot2, sizeof(double) * nbm, cudaMemcpyHostToDevice, s));
+  if (cot3)
+    GR_CUDA_TRY(cudaMemcpyAsync(c->cot.p + nbm, cot3, sizeof(double) * nbm, cudaMemcpyHostToDevice, s));
+  GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
+  build_index(c);
+  GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->gfix.p, 0, sizeof(unsigned long long) * (2 * n + 2), s));
+  std::memset(&c->st, 0, sizeof(c->st));
+  launch_adj2(c->index.view(), c->P, c->cot.p, cot3 ? c->cot.p + nbm : nullptr, gscale, c->gfix.p,
+              c->gfix.p + n, c->work.p, s);
+  finish_grad(c, gscale, grad_w, c->ev[1]);
+  c->st.ms_index = ev_ms(c->ev[0], c->ev[1]);
+  c->st.ms_total = c->st.ms_index + c->st.ms_query;
+  c->st.n_points = n;
+  c->st.kernel_launches = c->index.launches + 2;
+  GR_API_END(c)
+}
+
+int gr_adjoint_3pcf(gr_ctx* c, const double* cot2, const double* cot3, double* grad_w) {
+  GR_API_BEGIN(c)
+  require_ready(c);
+  if (!cot2 || !grad_w) return set_err(c, GR_E_ARG, "null cot2 or grad_w");
+  ensure_events(c);
+  cudaStream_t s = c->stream();
+  const int nmu = c->nmu;
+  const int ncfg = (int)(((int64_t)c->nbins * (c->nbins + 1) * (c->nbins + 2)) / 6);
+  const int nc = ncfg * nmu;
+  const int64_t n = c->n;
+  const double cmax = max_abs(cot2, nc) + max_abs(cot3, nc);
+  const double gscale = fix_scale(3.0 * cmax * c->wmax * c->wmax);
+  std::vector<uint8_t> nt;
+  normal_table(nmu, nt);
+  c->normal_dev.reserve(nt.size());
+  c->cot.reserve(2 * nc);
+  c->gfix.reserve(2 * n + 2);
+  c->work.reserve(4);
+  c->stats.reserve(8);
+  GR_CUDA_TRY(cudaMemcpyAsync(c->normal_dev.p, nt.data(), nt.size(), cudaMemcpyHostToDevice, s));
+  GR_CUDA_TRY(cudaMemcpyAsync(c->cot.p, cot2, sizeof(double) * nc, cudaMemcpyHostToDevice, s));
+  if (cot3)
+    GR_CUDA_TRY(cudaMemcpyAsync(c->cot.p + nc, cot3, sizeof(double) * nc, cudaMemcpyHostToDevice, s));
+  GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
+  const bool rebuilt = !c->csr_valid;
+  if (rebuilt) {
+    build_index(c);
+    build_csr(c);
+  }
+  GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->gfix.p, 0, sizeof(unsigned long long) * (2 * n + 2), s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
+  TriParams T;
+  T.nbins = c->nbins;
+  T.nmu = nmu;
+  T.ncfg = ncfg;
+  T.rsd = nmu >= 2;
+  T.cap = round_cap(c->csr.max_deg, 32, 256);
+  T.normal = c->normal_dev.p;
+  make_rank_tables(T.rank, c->nbins, 3);
+  CSRView G{c->csr.row_ptr.p, c->csr.rec.p, c->csr.deg_full.p};
+  std::memset(&c->st, 0, sizeof(c->st));
+  launch_adj3(c->index.view(), G, T, c->cot.p, cot3 ? c->cot.p + nc : nullptr, gscale, c->gfix.p,
+              c->gfix.p + n, c->stats.p, c->work.p, s);
+  finish_grad(c, gscale, grad_w, c->ev[1]);
+  c->st.ms_graph = rebuilt ? ev_ms(c->ev[0], c->ev[1]) : 0.0;
+  c->st.ms_total = c->st.ms_graph + c->st.ms_query;
+  c->st.n_points = n;
+  c->st.n_edges = 2 * c->csr.n_edges;
+  c->st.upper_edges = c->csr.n_edges;
+  c->st.kernel_launches = (rebuilt ? c->index.launches + c->csr.launches : 0) + 2;
   GR_API_END(c)
 }
 

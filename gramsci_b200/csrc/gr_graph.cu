@@ -170,7 +170,12 @@ void UpperCSR::build(const DevCatalog& C, const PairParams& P, cudaStream_t s) {
   scan_i32_to_i64(deg_up.p, row_ptr.p, n, s, scan_tmp);
   launches += 3;
   GR_CUDA_TRY(cudaMemcpyAsync(&n_edges, row_ptr.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  unsigned long long hs[3] = {0, 0, 0};
+  GR_CUDA_TRY(cudaMemcpyAsync(hs, stats.p, sizeof(hs), cudaMemcpyDeviceToHost, s));
   GR_CUDA_TRY(cudaStreamSynchronize(s));
+  rechecks = (int64_t)hs[0];
+  candidates = (int64_t)hs[1];
+  max_deg = (int64_t)hs[2];
   rec.reserve(n_edges);
   if (n > 0 && n_edges > 0) {
     if (P.f32)

@@ -37,6 +37,8 @@ void narrow_kernel_launch(const int64_t* in, int* out, int64_t n, cudaStream_t s
 // metadata.  deg_full[p] is the full degree (the reference's row length nn).
 struct UpperCSR {
   int64_t n = 0, n_edges = 0;  // n_edges counts upper (undirected) edges
+  int64_t max_deg = 0;         // largest upper degree
+  int64_t rechecks = 0, candidates = 0;
   int launches = 0;
   DevBuf<int> deg_up, deg_full, cursor, work;
   DevBuf<int64_t> row_ptr, scan_tmp;

@@ -331,6 +331,44 @@ __device__ __forceinline__ void fix_merge(unsigned long long* lo, unsigned long 
   if (d) atomicAdd(hi, d);
 }
 
+// A 128-bit fixed-point accumulator held in registers.
+struct Fix128 {
+  unsigned long long lo, hi;
+};
+
+__device__ __forceinline__ void fix_acc(Fix128& a, double x, double scale) {
+  const long long v = __double2ll_rn(x * scale);
+  const unsigned long long add = (unsigned long long)v;
+  const unsigned long long old = a.lo;
+  a.lo += add;
+  a.hi += (v < 0 ? ~0ull : 0ull) + (a.lo < old ? 1ull : 0ull);
+}
+
+// Exact warp sum of 128-bit accumulators (every lane gets the total).
+__device__ __forceinline__ Fix128 fix_warp_sum(Fix128 a) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long l2 = __shfl_xor_sync(0xffffffffu, a.lo, o);
+    const unsigned long long h2 = __shfl_xor_sync(0xffffffffu, a.hi, o);
+    const unsigned long long s = a.lo + l2;
+    a.hi = a.hi + h2 + (s < a.lo ? 1ull : 0ull);
+    a.lo = s;
+  }
+  return a;
+}
+
+// Device: value of a signed 128-bit (lo, hi) pair divided by scale.
+__device__ __forceinline__ double fix_to_double(unsigned long long lo, unsigned long long hi,
+                                                double inv_scale) {
+  const bool neg = (long long)hi < 0;
+  if (neg) {
+    lo = ~lo + 1ull;
+    hi = ~hi + (lo == 0ull ? 1ull : 0ull);
+  }
+  const double mag = (double)hi * 18446744073709551616.0 + (double)lo;
+  return (neg ? -mag : mag) * inv_scale;
+}
+
 // Host: scale 2^e with max_abs_product * 2^e < 2^62.
 double fix_scale(double max_abs_product);
 // Host: value of a (lo, hi) pair.

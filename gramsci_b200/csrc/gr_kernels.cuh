@@ -37,6 +37,20 @@ void launch_tri3(const DevCatalog& C, const CSRView& G, const TriParams& T, bool
                  unsigned long long* g_cnt, unsigned long long* g_fix, double fscale,
                  unsigned long long* stats, int* work, cudaStream_t s);
 
+// Weight adjoints: gradient of sum(cot2 * N2) + sum(cot3 * N3) with respect
+// to the weights, as 128-bit fixed-point sums (g_lo, g_hi, label order,
+// zeroed by the caller) of scale gscale; launch_grad_finish converts them to
+// FP64 in catalogue order.  cot3 may be NULL.
+void launch_adj2(const DevCatalog& C, const PairParams& P, const double* cot2, const double* cot3,
+                 double gscale, unsigned long long* g_lo, unsigned long long* g_hi, int* work,
+                 cudaStream_t s);
+void launch_adj3(const DevCatalog& C, const CSRView& G, const TriParams& T, const double* cot2,
+                 const double* cot3, double gscale, unsigned long long* g_lo,
+                 unsigned long long* g_hi, unsigned long long* stats, int* work, cudaStream_t s);
+void launch_grad_finish(int n, const int* orig, const unsigned long long* g_lo,
+                        const unsigned long long* g_hi, double gscale, double* grad,
+                        cudaStream_t s);
+
 struct QuadParams {
   int nbins, ncfg;
   int cap;

@@ -37,19 +37,23 @@ __host__ __device__ inline int hash_size(int cap) {
 }
 
 struct TriLayout {
-  size_t off_cnt, off_fix, off_norm, off_rank, off_warp, warp_bytes, total;
+  size_t off_cnt, off_fix, off_cot, off_norm, off_rank, off_warp, warp_bytes, total;
   // per-warp sub-offsets
-  size_t o_rs, o_w, o_col, o_meta, o_orig, o_pre, o_hkey, o_qm, o_qxy, o_flag, o_hval, o_own;
+  size_t o_rs, o_w, o_g, o_col, o_meta, o_orig, o_pre, o_hkey, o_qm, o_qxy, o_flag, o_hval, o_own;
 };
 
+// adj: the adjoint variant (cotangent tables, per-neighbour gradient
+// accumulators) instead of histograms.
 __host__ __device__ inline TriLayout tri_layout(int nh, int nmu, int nbins, int cap, bool shist,
-                                                bool weighted, int nwarps) {
+                                                bool weighted, int nwarps, bool adj = false) {
   TriLayout L;
   size_t o = 0;
   L.off_cnt = o;
   if (shist) o += (size_t)nh * 8;
   L.off_fix = o;
   if (shist && weighted) o += (size_t)nh * 16;
+  L.off_cot = o;
+  if (adj) o += (size_t)nh / 4 * 2 * 8;  // cot2, cot3: ncfg * nmu doubles each
   L.off_norm = o;
   o = align8(o + (size_t)nmu * nmu);
   L.off_rank = o;
@@ -59,6 +63,7 @@ __host__ __device__ inline TriLayout tri_layout(int nh, int nmu, int nbins, int 
   size_t w = 0;
   L.o_rs = w;   w += (size_t)cap * 8;
   L.o_w = w;    w += (size_t)cap * 8;
+  L.o_g = w;    if (adj) w += (size_t)cap * 16;  // gradient (lo, hi) per neighbour
   L.o_col = w;  w += (size_t)cap * 4;
   L.o_meta = w; w += (size_t)cap * 4;
   L.o_orig = w; w += (size_t)cap * 4;
@@ -81,6 +86,10 @@ struct TriCtx {
   unsigned long long* cnt;
   unsigned long long* lo;  // fixed-point sums: lo[k], lo[nh + k] = hi[k]
   double fscale;
+  // adjoint
+  const double* c2;  // cot2 (ncfg, nmu)
+  const double* c3;  // cot3 (ncfg, nmu)
+  double gscale;
 };
 
 __device__ __forceinline__ int rank3_s(const int* F, int nb2, int a, int b, int c) {
@@ -140,6 +149,46 @@ __device__ __forceinline__ int tri_bin(const TriCtx& X, uint8_t fp, int op, doub
   return total;
 }
 
+// Adjoint of one triangle (p, a, c): every non-buffer root r contributes
+// (cot2 - [all random] cot3)[cfg, m_r] (N3 accumulates minus the product);
+// with C the sum, dL/dw_p += C w_a w_c, dL/dw_a += C w_p w_c, dL/dw_c +=
+// C w_p w_a.  p's term goes to the lane's register accumulator, a's and c's
+// to the given fixed-point accumulators.
+__device__ __forceinline__ int tri_grad(const TriCtx& X, uint8_t fp, int op, double wp,
+                                        uint8_t fa, int oa, double wa, uint8_t fc, int oc,
+                                        double wc, uint32_t mpa, uint32_t mpc, uint32_t mac,
+                                        Fix128& racc, unsigned long long* alo,
+                                        unsigned long long* ahi, unsigned long long* clo,
+                                        unsigned long long* chi) {
+  int s1 = meta_bin(mpa), s2 = meta_bin(mpc), s3 = meta_bin(mac);
+  sort3i(s1, s2, s3);
+  const int cfg = rank3_s(X.F, X.nbins + 2, s1, s2, s3);
+  const bool allr = (fp & fa & fc & FLAG_RANDOM) != 0;
+  double C = 0.0;
+  int n = 0;
+  if (!(fp & FLAG_BUFFER)) {
+    const int k = (cfg - 1) + X.ncfg * (normal_bin(X, meta_muf(mpa), meta_muf(mpc), oa < oc) - 1);
+    C += allr ? X.c2[k] - X.c3[k] : X.c2[k];
+    n++;
+  }
+  if (!(fa & FLAG_BUFFER)) {
+    const int k = (cfg - 1) + X.ncfg * (normal_bin(X, meta_mur(mpa), meta_muf(mac), op < oc) - 1);
+    C += allr ? X.c2[k] - X.c3[k] : X.c2[k];
+    n++;
+  }
+  if (!(fc & FLAG_BUFFER)) {
+    const int k = (cfg - 1) + X.ncfg * (normal_bin(X, meta_mur(mpc), meta_mur(mac), op < oa) - 1);
+    C += allr ? X.c2[k] - X.c3[k] : X.c2[k];
+    n++;
+  }
+  if (C != 0.0) {
+    fix_acc(racc, C * (wa * wc), X.gscale);
+    fix_add(alo, ahi, C * (wp * wc), X.gscale);
+    fix_add(clo, chi, C * (wp * wa), X.gscale);
+  }
+  return n;
+}
+
 // first index in sorted a[0..n) with a[i] >= v
 __device__ __forceinline__ int lower_bound_g(const unsigned long long* a, int n, int v) {
   int lo = 0, hi = n;
@@ -157,16 +206,23 @@ __device__ __forceinline__ uint32_t hash_slot(int key, int hmask) {
   return ((uint32_t)key * 2654435761u) & (uint32_t)hmask;
 }
 
-template <bool WEIGHTED, bool SHIST>
+// ADJ: accumulate the weight gradient (g_lo / g_hi, label order) of
+// L = sum cot2 N2 + cot3 N3 instead of the histograms.
+template <bool WEIGHTED, bool SHIST, bool ADJ>
 __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, CSRView G, TriParams T,
                                                            unsigned long long* __restrict__ g_cnt,
                                                            unsigned long long* __restrict__ g_fix,
                                                            double fscale,
                                                            unsigned long long* __restrict__ stats,
-                                                           int* __restrict__ work) {
+                                                           int* __restrict__ work,
+                                                           const double* __restrict__ cot2,
+                                                           const double* __restrict__ cot3,
+                                                           double gscale,
+                                                           unsigned long long* __restrict__ g_lo,
+                                                           unsigned long long* __restrict__ g_hi) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int nh = T.ncfg * T.nmu * 4;
-  const TriLayout L = tri_layout(nh, T.nmu, T.nbins, T.cap, SHIST, WEIGHTED, blockDim.x >> 5);
+  const TriLayout L = tri_layout(nh, T.nmu, T.nbins, T.cap, SHIST, WEIGHTED, blockDim.x >> 5, ADJ);
   TriCtx X;
   X.nbins = T.nbins;
   X.nmu = T.nmu;
@@ -180,6 +236,17 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
   int* s_F = reinterpret_cast<int*>(smem + L.off_rank);
   X.norm = s_norm;
   X.F = s_F;
+  X.gscale = gscale;
+  if (ADJ) {
+    double* s_cot = reinterpret_cast<double*>(smem + L.off_cot);
+    const int nc = T.ncfg * T.nmu;
+    for (int k = threadIdx.x; k < nc; k += blockDim.x) {
+      s_cot[k] = cot2[k];
+      s_cot[nc + k] = cot3 ? cot3[k] : 0.0;
+    }
+    X.c2 = s_cot;
+    X.c3 = s_cot + nc;
+  }
   if (SHIST) {
     for (int k = threadIdx.x; k < nh; k += blockDim.x) {
       X.cnt[k] = 0ull;
@@ -209,6 +276,8 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
   uint8_t* s_flag = wb + L.o_flag;
   uint8_t* s_hval = wb + L.o_hval;
   uint8_t* s_own = wb + L.o_own;
+  unsigned long long* s_glo = reinterpret_cast<unsigned long long*>(wb + L.o_g);
+  unsigned long long* s_ghi = s_glo + T.cap;
   const int hs = hash_size(T.cap);
   const int hmask = hs - 1;
 
@@ -227,6 +296,7 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
       const uint8_t fp = C.flags[p];
       const int op = C.orig[p];
       const double wp = WEIGHTED ? C.w[p] : 0.0;
+      Fix128 racc = {0ull, 0ull};
       if (k <= T.cap) {
         __syncwarp();
         for (int h = lane; h < hs; h += 32) s_hkey[h] = -1;
@@ -247,6 +317,10 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
             s_flag[x] = C.flags[a];
             s_orig[x] = C.orig[a];
             if (WEIGHTED) s_w[x] = C.w[a];
+            if (ADJ) {
+              s_glo[x] = 0ull;
+              s_ghi[x] = 0ull;
+            }
             uint32_t h = hash_slot(a, hmask);
             for (int t = 0; t < hs; ++t) {
               if (atomicCAS(&s_hkey[h], -1, a) == -1) {
@@ -314,9 +388,13 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
               const int e = qn - 32 + lane;
               const uint16_t xy = s_qxy[e];
               const int qx = xy & 0xff, qy = xy >> 8;
-              const int nroot = tri_bin<WEIGHTED>(
-                  X, fp, op, wp, s_flag[qx], s_orig[qx], WEIGHTED ? s_w[qx] : 0.0, s_flag[qy],
-                  s_orig[qy], WEIGHTED ? s_w[qy] : 0.0, s_meta[qx], s_meta[qy], s_qm[e]);
+              const int nroot =
+                  ADJ ? tri_grad(X, fp, op, wp, s_flag[qx], s_orig[qx], s_w[qx], s_flag[qy],
+                                 s_orig[qy], s_w[qy], s_meta[qx], s_meta[qy], s_qm[e], racc,
+                                 &s_glo[qx], &s_ghi[qx], &s_glo[qy], &s_ghi[qy])
+                      : tri_bin<WEIGHTED>(X, fp, op, wp, s_flag[qx], s_orig[qx],
+                                          WEIGHTED ? s_w[qx] : 0.0, s_flag[qy], s_orig[qy],
+                                          WEIGHTED ? s_w[qy] : 0.0, s_meta[qx], s_meta[qy], s_qm[e]);
               tris += nroot > 0;
               rooted += nroot;
               qn -= 32;
@@ -328,11 +406,23 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
         if (lane < qn) {
           const uint16_t xy = s_qxy[lane];
           const int qx = xy & 0xff, qy = xy >> 8;
-          const int nroot = tri_bin<WEIGHTED>(
-              X, fp, op, wp, s_flag[qx], s_orig[qx], WEIGHTED ? s_w[qx] : 0.0, s_flag[qy],
-              s_orig[qy], WEIGHTED ? s_w[qy] : 0.0, s_meta[qx], s_meta[qy], s_qm[lane]);
+          const int nroot =
+              ADJ ? tri_grad(X, fp, op, wp, s_flag[qx], s_orig[qx], s_w[qx], s_flag[qy],
+                             s_orig[qy], s_w[qy], s_meta[qx], s_meta[qy], s_qm[lane], racc,
+                             &s_glo[qx], &s_ghi[qx], &s_glo[qy], &s_ghi[qy])
+                  : tri_bin<WEIGHTED>(X, fp, op, wp, s_flag[qx], s_orig[qx],
+                                      WEIGHTED ? s_w[qx] : 0.0, s_flag[qy], s_orig[qy],
+                                      WEIGHTED ? s_w[qy] : 0.0, s_meta[qx], s_meta[qy], s_qm[lane]);
           tris += nroot > 0;
           rooted += nroot;
+        }
+        if (ADJ) {
+          // flush the neighbours' gradient accumulators of this root
+          __syncwarp();
+          for (int x = lane; x < k; x += 32) {
+            const unsigned long long lo = s_glo[x], hi = s_ghi[x];
+            if (lo | hi) fix_merge(&g_lo[s_col[x]], &g_hi[s_col[x]], lo, hi);
+          }
         }
       } else {
         // Long row: the same enumeration reading the row from global memory.
@@ -352,14 +442,22 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
             const int c = rec_col(r);
             const int y = x + 1 + lower_bound_g(rowp + x + 1, k - x - 1, c);
             if (y < k && rec_col(rowp[y]) == c) {
-              const int nroot = tri_bin<WEIGHTED>(X, fp, op, wp, fa, oa, wa, C.flags[c], C.orig[c],
-                                                  WEIGHTED ? C.w[c] : 0.0, mpa, rec_meta(rowp[y]),
-                                                  rec_meta(r));
+              const int nroot =
+                  ADJ ? tri_grad(X, fp, op, wp, fa, oa, wa, C.flags[c], C.orig[c], C.w[c], mpa,
+                                 rec_meta(rowp[y]), rec_meta(r), racc, &g_lo[a], &g_hi[a], &g_lo[c],
+                                 &g_hi[c])
+                      : tri_bin<WEIGHTED>(X, fp, op, wp, fa, oa, wa, C.flags[c], C.orig[c],
+                                          WEIGHTED ? C.w[c] : 0.0, mpa, rec_meta(rowp[y]),
+                                          rec_meta(r));
               tris += nroot > 0;
               rooted += nroot;
             }
           }
         }
+      }
+      if (ADJ) {
+        racc = fix_warp_sum(racc);
+        if (lane == 0 && (racc.lo | racc.hi)) fix_merge(&g_lo[p], &g_hi[p], racc.lo, racc.hi);
       }
     }
   }
@@ -416,7 +514,7 @@ void launch_tri3(const DevCatalog& C, const CSRView& G, const TriParams& T, bool
   GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));
 #define GR_TRI_LAUNCH(W, S)                                                                   \
   do {                                                                                        \
-    auto kfn = tri3_kernel<W, S>;                                                             \
+    auto kfn = tri3_kernel<W, S, false>;                                                             \
     GR_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
                                      (int)smem));                                             \
     int per_sm = 0;                                                                           \
@@ -425,7 +523,8 @@ void launch_tri3(const DevCatalog& C, const CSRView& G, const TriParams& T, bool
     int64_t blocks = (int64_t)per_sm * 148;                                                   \
     const int64_t need = ((int64_t)C.n + nw * kChunk - 1) / (nw * kChunk);                    \
     if (blocks > need) blocks = need;                                                         \
-    kfn<<<(unsigned)blocks, nw * 32, smem, s>>>(C, G, T, g_cnt, g_fix, fscale, stats, work);   \
+    kfn<<<(unsigned)blocks, nw * 32, smem, s>>>(C, G, T, g_cnt, g_fix, fscale, stats, work,    \
+                                                nullptr, nullptr, 0.0, nullptr, nullptr);     \
   } while (0)
   if (weighted) {
     if (shist) GR_TRI_LAUNCH(true, true); else GR_TRI_LAUNCH(true, false);
@@ -433,6 +532,30 @@ void launch_tri3(const DevCatalog& C, const CSRView& G, const TriParams& T, bool
     if (shist) GR_TRI_LAUNCH(false, true); else GR_TRI_LAUNCH(false, false);
   }
 #undef GR_TRI_LAUNCH
+  GR_CHECK_LAUNCH();
+}
+
+void launch_adj3(const DevCatalog& C, const CSRView& G, const TriParams& T, const double* cot2,
+                 const double* cot3, double gscale, unsigned long long* g_lo,
+                 unsigned long long* g_hi, unsigned long long* stats, int* work, cudaStream_t s) {
+  if (C.n <= 0) return;
+  const int nh = T.ncfg * T.nmu * 4;
+  int nw = kTriMaxWarps;
+  while (nw > 1 && tri_layout(nh, T.nmu, T.nbins, T.cap, false, true, nw, true).total > kSmemLimit)
+    nw >>= 1;
+  const size_t smem = tri_layout(nh, T.nmu, T.nbins, T.cap, false, true, nw, true).total;
+  if (smem > kSmemLimit) throw Error{-2, "3PCF adjoint: shared memory exceeds the SM limit"};
+  GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));
+  auto kfn = tri3_kernel<true, false, true>;
+  GR_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nw * 32, smem));
+  if (per_sm < 1) per_sm = 1;
+  int64_t blocks = (int64_t)per_sm * 148;
+  const int64_t need = ((int64_t)C.n + nw * kChunk - 1) / (nw * kChunk);
+  if (blocks > need) blocks = need;
+  kfn<<<(unsigned)blocks, nw * 32, smem, s>>>(C, G, T, nullptr, nullptr, 0.0, stats, work, cot2,
+                                              cot3, gscale, g_lo, g_hi);
   GR_CHECK_LAUNCH();
 }
 

@@ -132,6 +132,20 @@ int gr_graph_build(gr_ctx* ctx);
 int gr_graph_nedges(gr_ctx* ctx, int64_t* n_edges);
 int gr_graph_export(gr_ctx* ctx, int64_t* row_ptr, int32_t* col, uint8_t* bin, uint8_t* mu);
 
+/* Weight adjoints.  Gradient of L = sum(cot2 * N2) + sum(cot3 * N3) with
+ * respect to every signed normalised weight w_k (grad_w has N entries,
+ * catalogue order).  cot2/cot3 have the shapes of N2/N3 of the matching
+ * count call; cot3 may be NULL.  The reference has no derivatives; these
+ * differentiate the sums of query_graph_2pcf (src/gramsci.F90:362-379) and
+ * query_graph_3pcf_all (:475-510): N2 and N3 are multilinear in the weights
+ * (each point appears at most once per pair or triangle), so
+ * dN2_b/dw_k = sum over the rooted pairs/triangles in bin b that contain k of
+ * the product of the other weights.  gr_adjoint_3pcf reuses the graph of the
+ * last count or graph build when the catalogue and bins are unchanged.
+ * Gradients are accumulated in 128-bit fixed point: deterministic. */
+int gr_adjoint_2pcf(gr_ctx* ctx, const double* cot2, const double* cot3, double* grad_w);
+int gr_adjoint_3pcf(gr_ctx* ctx, const double* cot2, const double* cot3, double* grad_w);
+
 /* Statistics of the last count call. */
 int gr_get_stats(gr_ctx* ctx, gr_stats* out);
 

@@ -32,7 +32,8 @@ def _compare(a_path, b_path):
         va = np.array([float(x) for x in la.split()])
         vb = np.array([float(x) for x in lb.split()])
         same = (va == vb) | (np.isnan(va) & np.isnan(vb))
-        close = np.abs(va - vb) <= 1.5e-7 * np.maximum(np.abs(va), np.abs(vb))
+        with np.errstate(invalid="ignore"):
+            close = np.abs(va - vb) <= 1.5e-7 * np.maximum(np.abs(va), np.abs(vb))
         assert np.all(same | close), (la, lb)
 
 
