@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--scale", type=float, default=1.0, help="workload scale (1.0 = full size)")
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="c2_3pcf", choices=["c2_3pcf", "c4_batched", "c5_adjoint"],
+                    help="c2_3pcf is the headline line; c4_batched and c5_adjoint print the "
+                         "batched-vs-per-region and adjoint-vs-forward comparisons")
     return ap.parse_args()
 
 
@@ -326,10 +329,129 @@ def run_ours(args):
     return 0
 
 
+def run_batched(args):
+    """2PCF over 5^3 regions with Rmax buffers, all regions in one
+    graph-replayed launch, against one launch per region on the same regions."""
+    import torch
+
+    from gramsci_b200 import api, catalogs
+
+    cat = catalogs.make("c4_batched", scale=args.scale)
+    sp = catalogs.WORKLOADS["c4_batched"]
+    w = catalogs.normalise(cat.w, cat.n_data, cat.n_rand)
+    dev = torch.device("cuda:0")
+    stream = torch.cuda.current_stream()
+    ctx = api.Context(0)
+    ctx.set_stream(stream)
+    ctx.set_precision(args.precision)
+    xyz_d = torch.from_numpy(cat.xyz).to(dev)
+    w_d = torch.from_numpy(w).to(dev)
+    ctx.set_catalog(xyz_d, w_d, cat.n_data)
+    ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
+    ctx.set_regions(sp["nsplit"])
+    ref = ctx.count_2pcf_batched()
+    regions = ctx.regions()
+    sizes = [len(o) for o, _ in regions]
+    reg_dev = []
+    for o, bf in regions:
+        if len(o) == 0:
+            continue
+        oi = torch.from_numpy(o.astype(np.int64)).to(dev)
+        reg_dev.append((xyz_d[oi].contiguous(), w_d[oi].contiguous(),
+                        torch.from_numpy(bf).to(dev), int(np.sum(o < cat.n_data))))
+    loop_ctx = api.Context(0)
+    loop_ctx.set_stream(stream)
+    loop_ctx.set_precision(args.precision)
+    loop_ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
+
+    def per_region():
+        tot = 0
+        for x, ww, b, nd in reg_dev:
+            loop_ctx.set_catalog(x, ww, nd, buffer=b)
+            r = loop_ctx.count_2pcf()
+            tot = tot + r["counts"]
+        return tot
+
+    def timed(fn, steps):
+        ms = []
+        for _ in range(steps):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            out = fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        return float(np.median(ms)), out
+
+    for _ in range(max(1, args.warmup)):
+        ctx.count_2pcf_batched()
+    t_batch, out = timed(ctx.count_2pcf_batched, max(1, args.steps))
+    st = ctx.stats()
+    per_region()
+    t_loop, tot = timed(per_region, max(1, min(args.steps, 3)))
+    assert np.array_equal(tot, out["counts"]) and np.array_equal(out["counts"], ref["counts"])
+    pairs = int(out["counts"].sum()) // 2
+    line = {
+        "metric": METRIC + " [batched regions]", "value": pairs / (t_batch / 1e3),
+        "unit": "pairs/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_batch, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64", "data": "synthetic (seeded ramped Neyman-Scott + uniform randoms)",
+        "config": {"workload": f"c4_batched: {cat.n_data} galaxies + {cat.n_rand} randoms, box "
+                               f"{cat.meta['box']:.0f}, rmin 10, rmax 60, 12 bins, nmu 10, "
+                               f"{len(regions)} regions with 60 Mpc/h buffers",
+                   "scale": args.scale, "members": int(sum(sizes)),
+                   "region_members_min_max": [int(min(sizes)), int(max(sizes))],
+                   "pairs": pairs, "rooted": int(out["counts"].sum())},
+        "per_region_ms": t_loop, "per_region_pairs_per_s": pairs / (t_loop / 1e3),
+        "batched_over_per_region": t_loop / t_batch,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_adjoint(args):
+    """weighted 2PCF and 3PCF forward passes and their weight
+    adjoints (device time of the counting vs the adjoint kernels)."""
+    from gramsci_b200 import api, catalogs
+
+    out = {}
+    for name, order in (("c5_adjoint_2pcf", 2), ("c5_adjoint_3pcf", 3)):
+        cat = catalogs.make(name, scale=args.scale)
+        sp = catalogs.WORKLOADS[name]
+        w = catalogs.normalise(cat.w, cat.n_data, cat.n_rand)
+        ctx = api.Context(0)
+        ctx.set_catalog(cat.xyz, w, cat.n_data)
+        ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
+        rng = np.random.default_rng(5)
+        fwd, adj = [], []
+        for k in range(max(2, args.steps)):
+            r = ctx.count_2pcf() if order == 2 else ctx.count_3pcf()
+            s = ctx.stats()
+            c2 = rng.normal(size=r["N2"].shape)
+            c3 = rng.normal(size=r["N3"].shape)
+            g = ctx.adjoint_2pcf(c2, c3) if order == 2 else ctx.adjoint_3pcf(c2, c3)
+            a = ctx.stats()
+            if k > 0:
+                fwd.append(s["ms_query"])
+                adj.append(a["ms_query"])
+        out[name] = {"n_points": cat.n, "forward_query_ms": float(np.median(fwd)),
+                     "adjoint_ms": float(np.median(adj)),
+                     "adjoint_over_forward": float(np.median(adj) / np.median(fwd)),
+                     "tuples": s["tuples"]}
+        ctx.close()
+    print(json.dumps({"metric": METRIC + " [weight adjoint]", "scale": args.scale, **out}), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "c4_batched":
+        return run_batched(args)
+    if args.workload == "c5_adjoint":
+        return run_adjoint(args)
     return run_ours(args)
 
 

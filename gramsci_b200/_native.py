@@ -73,6 +73,10 @@ SIGNATURES = {
     "gr_graph_export": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp]),
     "gr_get_stats": (ctypes.c_int, [_ctx, ctypes.POINTER(GrStats)]),
     "gr_adjoint_2pcf": (ctypes.c_int, [_ctx, _vp, _vp, _vp]),
+    "gr_set_regions": (ctypes.c_int, [_ctx, ctypes.c_int32]),
+    "gr_count_2pcf_batched": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp]),
+    "gr_regions_info": (ctypes.c_int, [_ctx, _vp, _vp]),
+    "gr_regions_export": (ctypes.c_int, [_ctx, _vp, _vp, _vp]),
     "gr_adjoint_3pcf": (ctypes.c_int, [_ctx, _vp, _vp, _vp]),
     "gr_count_2pcf_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.c_int64,
                                              ctypes.c_double, ctypes.c_double, ctypes.c_int32,

@@ -162,6 +162,35 @@ class Context:
                     counts=_fortran(counts, nc, nb, nb, 5), catsum=_fortran(catsum, nc, nb, nb, 5),
                     dcount=_fortran(dcount, nc, nb, nb, 6, 4), dsum=_fortran(dsum, nc, nb, nb, 6, 4))
 
+    # -- batched regions -------------------------------------------------
+    def set_regions(self, nsplit):
+        """Split the catalogue box into nsplit^3 regions with Rmax halos."""
+        self._check(self._lib.gr_set_regions(self._h, int(nsplit)))
+
+    def count_2pcf_batched(self):
+        """2PCF of all regions in one launch (CUDA-graph replay after the
+        first call); equals count_2pcf on the whole catalogue."""
+        nb, nm = self.nbins, self.nmu
+        N2, N3 = np.zeros(nb * nm), np.zeros(nb * nm)
+        counts = np.zeros(nb * nm * 4, np.int64)
+        catsum = np.zeros(nb * nm * 4)
+        self._check(self._lib.gr_count_2pcf_batched(self._h, _ptr(N2), _ptr(N3), _ptr(counts),
+                                                    _ptr(catsum)))
+        return dict(N2=_fortran(N2, nb, nm), N3=_fortran(N3, nb, nm),
+                    counts=_fortran(counts, nb, nm, 4), catsum=_fortran(catsum, nb, nm, 4))
+
+    def regions(self):
+        """Region layout of the last batched call: list of (member catalogue
+        indices, buffer flags) per region."""
+        nr = ctypes.c_int32()
+        nm = ctypes.c_int64()
+        self._check(self._lib.gr_regions_info(self._h, ctypes.byref(nr), ctypes.byref(nm)))
+        off = np.zeros(nr.value + 1, np.int64)
+        orig = np.zeros(max(nm.value, 1), np.int32)
+        buf = np.zeros(max(nm.value, 1), np.int32)
+        self._check(self._lib.gr_regions_export(self._h, _ptr(off), _ptr(orig), _ptr(buf)))
+        return [(orig[off[r]:off[r + 1]], buf[off[r]:off[r + 1]]) for r in range(nr.value)]
+
     def _adjoint(self, fn, cot2, cot3, shape):
         c2 = np.ascontiguousarray(np.asarray(cot2, np.float64).reshape(shape).T.ravel())
         c3 = None if cot3 is None else np.ascontiguousarray(

@@ -11,7 +11,7 @@
 #include <vector>
 
 #include "../../include/gramsci_cuda.h"
-#include "gr_kernels.cuh"
+#include "gr_batch.cuh"
 
 using namespace gr;
 
@@ -47,6 +47,14 @@ struct gr_ctx {
   DevBuf<int> work;
   DevBuf<double> cot, grad;              // adjoint inputs / output
   DevBuf<unsigned long long> gfix;       // adjoint fixed-point gradients (lo[n], hi[n])
+  // batched regions
+  int nsplit = 0;
+  RegionLayout regions;
+  DevBuf<unsigned long long> bcnt, bfix, bstats;
+  DevBuf<int> bwork;
+  bool batch_weighted = false;
+  double batch_fscale = 1.0;
+  cudaEvent_t bev[2] = {nullptr, nullptr};
   gr_stats st{};
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
@@ -308,6 +316,9 @@ int gr_destroy(gr_ctx* c) {
   if (c->own) cudaStreamSynchronize(c->own);
   for (int k = 0; k < 4; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
+  for (int k = 0; k < 2; ++k)
+    if (c->bev[k]) cudaEventDestroy(c->bev[k]);
+  c->regions.release_graph();
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
   return GR_OK;
@@ -369,6 +380,7 @@ static int set_catalog_impl(gr_ctx* c, const double* xyz, const double* w, const
   c->w_ran = wr;
   c->cat_set = true;
   c->csr_valid = false;
+  c->regions.valid = false;
   GR_API_END(c)
 }
 
@@ -396,6 +408,7 @@ int gr_set_bins(gr_ctx* c, double rmin, double rmax, int32_t nbins, int32_t nmu,
   c->logbins = logbins ? 1 : 0;
   c->bins_set = true;
   c->csr_valid = false;
+  c->regions.valid = false;
   GR_API_END(c)
 }
 
@@ -844,6 +857,153 @@ int gr_adjoint_3pcf(gr_ctx* c, const double* cot2, const double* cot3, double* g
   c->st.n_edges = 2 * c->csr.n_edges;
   c->st.upper_edges = c->csr.n_edges;
   c->st.kernel_launches = (rebuilt ? c->index.launches + c->csr.launches : 0) + 2;
+  GR_API_END(c)
+}
+
+// ----------------------------------------------------------- batched regions --
+int gr_set_regions(gr_ctx* c, int32_t nsplit) {
+  GR_API_BEGIN(c)
+  if (nsplit < 0 || nsplit > 64) return set_err(c, GR_E_ARG, "nsplit must be in 0..64");
+  c->nsplit = nsplit;
+  c->regions.valid = false;
+  GR_API_END(c)
+}
+
+// Device work of one batched call: region layout, histogram reset, pair sweep.
+static void enqueue_batched(gr_ctx* c, cudaStream_t s) {
+  const int nh = c->nbins * c->nmu * 4;
+  c->regions.enqueue_layout(c->xyz.p, c->w.p, s);
+  GR_CUDA_TRY(cudaMemsetAsync(c->bcnt.p, 0, sizeof(unsigned long long) * nh, s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->bfix.p, 0, sizeof(unsigned long long) * 2 * nh, s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->bstats.p, 0, sizeof(unsigned long long) * 8, s));
+  launch_pair2(c->regions.view(), c->P, c->batch_weighted, c->bcnt.p, c->bfix.p, c->batch_fscale,
+               c->bstats.p, c->bwork.p, s);
+}
+
+int gr_count_2pcf_batched(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* catsum) {
+  GR_API_BEGIN(c)
+  require_ready(c);
+  if (c->nsplit < 1) return set_err(c, GR_E_ARG, "regions not set (gr_set_regions)");
+  ensure_events(c);
+  for (int k = 0; k < 2; ++k)
+    if (!c->bev[k]) GR_CUDA_TRY(cudaEventCreateWithFlags(&c->bev[k], cudaEventDisableTiming));
+  // the batched work runs on the context's own stream (capturable), ordered
+  // after and before the caller's stream
+  cudaStream_t us = c->stream(), s = c->own;
+  const int nbm = c->nbins * c->nmu, nh = nbm * 4;
+  GR_CUDA_TRY(cudaEventRecord(c->bev[0], us));
+  GR_CUDA_TRY(cudaStreamWaitEvent(s, c->bev[0], 0));
+  GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
+  bool replay = c->regions.valid && c->regions.exec;
+  if (!c->regions.valid) {
+    c->regions.plan(c->xyz.p, c->n, c->n_data, c->rmax, c->nsplit, s);
+    // pair parameters from the catalogue's coordinate bound
+    c->index.build(c->xyz.p, c->w.p, nullptr, c->n, c->n_data, c->rmax, s);
+    make_pair_params(c->P, c->rmin, c->rmax, c->nbins, c->nmu, c->logbins, c->index.coord_max,
+                     c->precision == 1);
+    c->csr_valid = false;
+    c->batch_weighted = !c->uniform;
+    c->batch_fscale = fix_scale(c->wmax * c->wmax);
+    c->bcnt.reserve(nh);
+    c->bfix.reserve(2 * nh);
+    c->bstats.reserve(8);
+    c->bwork.reserve(4);
+    // first run eagerly, then capture the same work for replay
+    enqueue_batched(c, s);
+    GR_CUDA_TRY(cudaStreamSynchronize(s));
+    c->regions.release_graph();
+    GR_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try {
+      enqueue_batched(c, s);
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(s, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    GR_CUDA_TRY(cudaStreamEndCapture(s, &c->regions.graph));
+    GR_CUDA_TRY(cudaGraphInstantiate(&c->regions.exec, c->regions.graph, 0));
+    GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
+    replay = true;
+  }
+  if (replay) GR_CUDA_TRY(cudaGraphLaunch(c->regions.exec, s));
+  GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+  std::vector<unsigned long long> hc(nh), hf(2 * nh, 0ull);
+  std::vector<double> hs(nh, 0.0);
+  unsigned long long st[8];
+  GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->bcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
+  if (c->batch_weighted)
+    GR_CUDA_TRY(cudaMemcpyAsync(hf.data(), c->bfix.p, sizeof(unsigned long long) * 2 * nh, cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaMemcpyAsync(st, c->bstats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaEventRecord(c->bev[1], s));
+  GR_CUDA_TRY(cudaStreamWaitEvent(us, c->bev[1], 0));
+  GR_CUDA_TRY(cudaStreamSynchronize(s));
+  if (c->batch_weighted) {
+    for (int k = 0; k < nh; ++k) hs[k] = fix_value(hf[k], hf[nh + k], c->batch_fscale);
+  } else {
+    for (int cat = 0; cat < 4; ++cat) {
+      const int nr = (cat >> 1) + (cat & 1);
+      const double prod = uniform_product(c->w_gal, c->w_ran, 2 - nr, nr);
+      for (int k = 0; k < nbm; ++k) hs[k + nbm * cat] = (double)hc[k + nbm * cat] * prod;
+    }
+  }
+  int64_t rooted = 0;
+  for (int k = 0; k < nh; ++k) rooted += (int64_t)hc[k];
+  for (int k = 0; k < nbm; ++k) {
+    if (N2) N2[k] = ((hs[k] + hs[k + nbm]) + hs[k + 2 * nbm]) + hs[k + 3 * nbm];
+    if (N3) N3[k] = hs[k + 3 * nbm];
+  }
+  if (counts)
+    for (int k = 0; k < nh; ++k) counts[k] = (int64_t)hc[k];
+  if (catsum)
+    for (int k = 0; k < nh; ++k) catsum[k] = hs[k];
+  std::memset(&c->st, 0, sizeof(c->st));
+  c->st.ms_query = ev_ms(c->ev[0], c->ev[1]);
+  c->st.ms_total = c->st.ms_query;
+  c->st.n_points = c->regions.n_members;
+  c->st.tuples = (int64_t)st[2];
+  c->st.rooted = rooted;
+  c->st.fp64_rechecks = (int64_t)st[0];
+  c->st.candidates = (int64_t)st[1];
+  c->st.kernel_launches = 11;
+  GR_API_END(c)
+}
+
+int gr_regions_info(gr_ctx* c, int32_t* nregions, int64_t* nmembers) {
+  GR_API_BEGIN(c)
+  if (!c->regions.valid) return set_err(c, GR_E_ARG, "no region layout (call gr_count_2pcf_batched)");
+  if (nregions) *nregions = c->regions.nreg;
+  if (nmembers) *nmembers = c->regions.n_members;
+  GR_API_END(c)
+}
+
+int gr_regions_export(gr_ctx* c, int64_t* member_off, int32_t* member_orig, int32_t* member_buffer) {
+  GR_API_BEGIN(c)
+  RegionLayout& L = c->regions;
+  if (!L.valid) return set_err(c, GR_E_ARG, "no region layout (call gr_count_2pcf_batched)");
+  cudaStream_t s = c->own;
+  const int64_t M = L.n_members;
+  std::vector<int> mo(M);
+  std::vector<uint8_t> mf(M);
+  if (M > 0) {
+    GR_CUDA_TRY(cudaMemcpyAsync(mo.data(), L.m_orig.p, sizeof(int) * M, cudaMemcpyDeviceToHost, s));
+    GR_CUDA_TRY(cudaMemcpyAsync(mf.data(), L.m_flag.p, M, cudaMemcpyDeviceToHost, s));
+  }
+  GR_CUDA_TRY(cudaStreamSynchronize(s));
+  // members of each region, ordered by catalogue index
+  for (int r = 0; r < L.nreg; ++r) {
+    const int64_t b = L.h_mem_off[r], e = L.h_mem_off[r + 1];
+    std::vector<std::pair<int, int>> v;
+    v.reserve(e - b);
+    for (int64_t k = b; k < e; ++k) v.push_back({mo[k], (mf[k] & FLAG_BUFFER) ? 1 : 0});
+    std::sort(v.begin(), v.end());
+    for (int64_t k = b; k < e; ++k) {
+      if (member_orig) member_orig[k] = v[k - b].first;
+      if (member_buffer) member_buffer[k] = v[k - b].second;
+    }
+  }
+  if (member_off)
+    for (int r = 0; r <= L.nreg; ++r) member_off[r] = L.h_mem_off[r];
   GR_API_END(c)
 }
 

@@ -1,0 +1,452 @@
+// Batched regions: the 2PCF over a domain decomposition of the catalogue in
+// one persistent launch, replayed from a CUDA graph.
+//
+// The reference handles large catalogues by domain decomposition
+// (src/domain_decomposition.f90:39-80): region j is the bounding box of its
+// points, grown by Rmax on every side (strict inequalities, :64-66); points
+// of other regions inside that halo are buffer points, which serve as
+// neighbours but never as roots (src/gramsci.F90:363).  Each region is then
+// run as a separate program and the outputs summed by hand.  Here the
+// catalogue's bounding box is split into nsplit^3 equal subcubes (region of a
+// point = its subcube), the region boxes and halos are computed on the
+// device in FP64, and every region's members (its own points, plus buffer
+// copies of the other points inside its halo) are laid out together: each
+// region gets its own cell grid over its halo box, the cells of all regions
+// are numbered consecutively (largest region first), and a single launch of
+// the warp-per-cell pair kernel processes the cells of every region from
+// one work counter.  Galaxy/random flags and the global weight
+// normalisation are kept, so the summed histogram equals the unsplit run.
+//
+// The first call for a given catalogue, binning and split computes the
+// geometry on the host (region boxes, halos, member counts, grids) and runs
+// eagerly; the device work of every later call (membership, cell sort,
+// layout, pair sweep) is replayed from a captured CUDA graph.
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+#include "gr_batch.cuh"
+
+namespace gr {
+
+namespace {
+
+__device__ __forceinline__ unsigned long long bkey(double v) {
+  unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+
+inline double bkey_value(unsigned long long k) {
+  unsigned long long b = (k & 0x8000000000000000ull) ? (k & 0x7fffffffffffffffull) : ~k;
+  double v;
+  std::memcpy(&v, &b, 8);
+  return v;
+}
+
+struct SplitGeom {
+  double lo[3], inv_span[3];
+  int ns;
+};
+
+__device__ __forceinline__ int sub_coord(double v, double lo, double inv_span, int ns) {
+  int s = (int)floor((v - lo) * inv_span * ns);
+  return s < 0 ? 0 : (s >= ns ? ns - 1 : s);
+}
+
+// catalogue bounding box: out[0..2] min keys, out[3..5] max keys
+__global__ void b_bbox_kernel(const double* __restrict__ xyz, int n, unsigned long long* out) {
+  unsigned long long mn[3] = {~0ull, ~0ull, ~0ull}, mx[3] = {0, 0, 0};
+  const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i0 >= n) return;
+  for (int i = i0; i < n; i += gridDim.x * blockDim.x)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const unsigned long long k = bkey(xyz[3 * (int64_t)i + d]);
+      mn[d] = k < mn[d] ? k : mn[d];
+      mx[d] = k > mx[d] ? k : mx[d];
+    }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    atomicMin(&out[d], mn[d]);
+    atomicMax(&out[3 + d], mx[d]);
+  }
+}
+
+// subcube of every point, per-region boxes (6 keys per region) and sizes
+__global__ void b_region_box_kernel(const double* __restrict__ xyz, int n, SplitGeom g,
+                                    int* __restrict__ sub, unsigned long long* __restrict__ box,
+                                    int* __restrict__ own_count) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double x = xyz[3 * (int64_t)i], y = xyz[3 * (int64_t)i + 1], z = xyz[3 * (int64_t)i + 2];
+    const int sx = sub_coord(x, g.lo[0], g.inv_span[0], g.ns);
+    const int sy = sub_coord(y, g.lo[1], g.inv_span[1], g.ns);
+    const int sz = sub_coord(z, g.lo[2], g.inv_span[2], g.ns);
+    const int r = (sz * g.ns + sy) * g.ns + sx;
+    sub[i] = r;
+    atomicMin(&box[6 * r + 0], bkey(x));
+    atomicMin(&box[6 * r + 1], bkey(y));
+    atomicMin(&box[6 * r + 2], bkey(z));
+    atomicMax(&box[6 * r + 3], bkey(x));
+    atomicMax(&box[6 * r + 4], bkey(y));
+    atomicMax(&box[6 * r + 5], bkey(z));
+    atomicAdd(&own_count[r], 1);
+  }
+}
+
+__global__ void b_init_box_kernel(unsigned long long* box, int nreg) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < 6 * nreg; k += gridDim.x * blockDim.x)
+    box[k] = (k % 6) < 3 ? ~0ull : 0ull;
+}
+
+struct RegionGeomDev {
+  const double* halo;    // 6 per region: lo xyz, hi xyz (strict bounds)
+  const double* glo;     // 3 per region: grid origin
+  const double* ginv;    // 3 per region: inverse cell size
+  const GridParams* grid;
+  const int* cell_off;   // nreg + 1
+  const int* mem_off;    // nreg + 1
+  int ns;
+};
+
+__device__ __forceinline__ bool in_halo(const double* h, double x, double y, double z) {
+  return x > h[0] && x < h[3] && y > h[1] && y < h[4] && z > h[2] && z < h[5];
+}
+
+// Visit the regions whose halo contains point i (its own subcube and the 26
+// around it; a halo reaches at most Rmax beyond its box, and a region's box
+// lies inside its subcube, so farther subcubes cannot qualify when the
+// subcubes are at least Rmax wide -- the host checks that).
+template <bool FILL>
+__global__ void b_member_kernel(const double* __restrict__ xyz, int n, int n_data,
+                                const int* __restrict__ sub, RegionGeomDev G,
+                                int* __restrict__ count, int* __restrict__ m_orig,
+                                uint8_t* __restrict__ m_flag, int* __restrict__ m_key,
+                                int* __restrict__ m_slot, int* __restrict__ cell_count) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double x = xyz[3 * (int64_t)i], y = xyz[3 * (int64_t)i + 1], z = xyz[3 * (int64_t)i + 2];
+    const int own = sub[i];
+    const int sx = own % G.ns, sy = (own / G.ns) % G.ns, sz = own / (G.ns * G.ns);
+    for (int dz = -1; dz <= 1; ++dz) {
+      const int tz = sz + dz;
+      if (tz < 0 || tz >= G.ns) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int ty = sy + dy;
+        if (ty < 0 || ty >= G.ns) continue;
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int tx = sx + dx;
+          if (tx < 0 || tx >= G.ns) continue;
+          const int r = (tz * G.ns + ty) * G.ns + tx;
+          if (!in_halo(G.halo + 6 * r, x, y, z)) continue;
+          const int slot = atomicAdd(&count[r], 1);
+          if (!FILL) continue;
+          const int m = G.mem_off[r] + slot;
+          m_orig[m] = i;
+          m_flag[m] = (uint8_t)((r != own ? FLAG_BUFFER : 0) | (i >= n_data ? FLAG_RANDOM : 0));
+          const GridParams g = G.grid[r];
+          int c[3];
+          const double v[3] = {x, y, z};
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            int q = (int)floor((v[d] - G.glo[3 * r + d]) * G.ginv[3 * r + d]);
+            const int nc = d == 0 ? g.nx : (d == 1 ? g.ny : g.nz);
+            c[d] = q < 0 ? 0 : (q >= nc ? nc - 1 : q);
+          }
+          const int key = G.cell_off[r] + (c[2] * g.ny + c[1]) * g.nx + c[0];
+          m_key[m] = key;
+          m_slot[m] = atomicAdd(&cell_count[key], 1);
+        }
+      }
+    }
+  }
+}
+
+__global__ void b_scatter_kernel(int64_t m, const int* __restrict__ key, const int* __restrict__ slot,
+                                 const int64_t* __restrict__ start, int* __restrict__ tmp) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m;
+       k += (int64_t)gridDim.x * blockDim.x)
+    tmp[start[key[k]] + slot[k]] = (int)k;
+}
+
+// members of a cell ordered by catalogue index (deterministic layout)
+__global__ void b_order_kernel(int64_t ncell, const int64_t* __restrict__ start,
+                               const int* __restrict__ tmp, const int* __restrict__ m_orig,
+                               int* __restrict__ perm) {
+  const int lane = threadIdx.x & 31;
+  int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t c = warp; c < ncell; c += nwarps) {
+    const int64_t b = start[c];
+    const int cnt = (int)(start[c + 1] - b);
+    for (int k = lane; k < cnt; k += 32) {
+      const int v = tmp[b + k];
+      const int ov = m_orig[v];
+      int r = 0;
+      for (int j = 0; j < cnt; ++j) r += m_orig[tmp[b + j]] < ov;
+      perm[b + r] = v;
+    }
+  }
+}
+
+__global__ void b_gather_kernel(int64_t m, const int* __restrict__ perm,
+                                const int* __restrict__ m_orig, const uint8_t* __restrict__ m_flag,
+                                const int* __restrict__ m_key, const double* __restrict__ xyz,
+                                const double* __restrict__ w, float4* __restrict__ pos4,
+                                double4* __restrict__ posd, double* __restrict__ wl,
+                                int* __restrict__ orig, uint8_t* __restrict__ flags,
+                                int* __restrict__ cell_key) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < m;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const int k = perm[p];
+    const int i = m_orig[k];
+    const double x = xyz[3 * (int64_t)i], y = xyz[3 * (int64_t)i + 1], z = xyz[3 * (int64_t)i + 2];
+    pos4[p] = make_float4(__double2float_rn(x), __double2float_rn(y), __double2float_rn(z), 0.f);
+    posd[p] = make_double4(x, y, z, w[i]);
+    wl[p] = w[i];
+    orig[p] = i;
+    flags[p] = m_flag[k];
+    cell_key[p] = m_key[k];
+  }
+}
+
+__global__ void b_narrow_kernel(const int64_t* __restrict__ in, int* __restrict__ out, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (int)in[i];
+}
+
+int nblocks(int64_t n, int threads, int cap = 148 * 8) {
+  int64_t b = (n + threads - 1) / threads;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(b, cap));
+}
+
+}  // namespace
+
+void RegionLayout::release_graph() {
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  exec = nullptr;
+  graph = nullptr;
+}
+
+RegionLayout::~RegionLayout() { release_graph(); }
+
+// Host-side geometry (first call): region boxes, halos, member counts,
+// grids and offsets; sizes every buffer.
+void RegionLayout::plan(const double* d_xyz, int64_t n_pts, int64_t n_data_pts, double rmax_,
+                        int nsplit_, cudaStream_t s) {
+  release_graph();
+  valid = false;
+  n = n_pts;
+  n_data = n_data_pts;
+  rmax = rmax_;
+  ns = nsplit_;
+  nreg = ns * ns * ns;
+  box_raw.reserve(6 * (size_t)nreg + 8);
+  own_count.reserve(nreg);
+  count.reserve(nreg);
+  sub.reserve(n + 1);
+  // catalogue box
+  {
+    unsigned long long init[6] = {~0ull, ~0ull, ~0ull, 0, 0, 0};
+    GR_CUDA_TRY(cudaMemcpyAsync(box_raw.p + 6 * (size_t)nreg, init, sizeof(init),
+                                cudaMemcpyHostToDevice, s));
+    if (n > 0)
+      b_bbox_kernel<<<nblocks(n, 256, 296), 256, 0, s>>>(d_xyz, (int)n, box_raw.p + 6 * (size_t)nreg);
+    GR_CHECK_LAUNCH();
+  }
+  unsigned long long hb[6];
+  GR_CUDA_TRY(cudaMemcpyAsync(hb, box_raw.p + 6 * (size_t)nreg, sizeof(hb), cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaStreamSynchronize(s));
+  SplitGeom sg;
+  sg.ns = ns;
+  for (int d = 0; d < 3; ++d) {
+    const double lo = n > 0 ? bkey_value(hb[d]) : 0.0, hi = n > 0 ? bkey_value(hb[3 + d]) : 0.0;
+    if (!std::isfinite(lo) || !std::isfinite(hi)) throw Error{-1, "non-finite coordinates"};
+    sg.lo[d] = lo;
+    const double span = hi - lo;
+    sg.inv_span[d] = span > 0 ? 1.0 / span : 0.0;
+    // subcubes narrower than Rmax would let a halo reach beyond the
+    // neighbouring subcubes
+    if (span > 0 && span / ns < rmax) throw Error{-1, "regions narrower than rmax; use a smaller split"};
+  }
+  b_init_box_kernel<<<nblocks(6 * (int64_t)nreg, 256), 256, 0, s>>>(box_raw.p, nreg);
+  GR_CUDA_TRY(cudaMemsetAsync(own_count.p, 0, sizeof(int) * nreg, s));
+  if (n > 0)
+    b_region_box_kernel<<<nblocks(n, 256), 256, 0, s>>>(d_xyz, (int)n, sg, sub.p, box_raw.p,
+                                                        own_count.p);
+  GR_CHECK_LAUNCH();
+  std::vector<unsigned long long> hbox(6 * (size_t)nreg);
+  std::vector<int> hown(nreg);
+  GR_CUDA_TRY(cudaMemcpyAsync(hbox.data(), box_raw.p, sizeof(unsigned long long) * 6 * nreg,
+                              cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaMemcpyAsync(hown.data(), own_count.p, sizeof(int) * nreg, cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaStreamSynchronize(s));
+  // halos: box +- rmax, strict; empty regions get an empty halo
+  h_halo.assign(6 * (size_t)nreg, 0.0);
+  for (int r = 0; r < nreg; ++r) {
+    if (hown[r] == 0) {
+      for (int d = 0; d < 3; ++d) {
+        h_halo[6 * r + d] = 1.0;
+        h_halo[6 * r + 3 + d] = -1.0;
+      }
+      continue;
+    }
+    for (int d = 0; d < 3; ++d) {
+      h_halo[6 * r + d] = bkey_value(hbox[6 * r + d]) - rmax;
+      h_halo[6 * r + 3 + d] = bkey_value(hbox[6 * r + 3 + d]) + rmax;
+    }
+  }
+  halo.reserve(6 * (size_t)nreg);
+  GR_CUDA_TRY(cudaMemcpyAsync(halo.p, h_halo.data(), sizeof(double) * 6 * nreg, cudaMemcpyHostToDevice, s));
+  // member counts
+  GR_CUDA_TRY(cudaMemsetAsync(count.p, 0, sizeof(int) * nreg, s));
+  RegionGeomDev G{};
+  G.halo = halo.p;
+  G.ns = ns;
+  if (n > 0)
+    b_member_kernel<false><<<nblocks(n, 256), 256, 0, s>>>(d_xyz, (int)n, (int)n_data, sub.p, G,
+                                                           count.p, nullptr, nullptr, nullptr,
+                                                           nullptr, nullptr);
+  GR_CHECK_LAUNCH();
+  h_count.assign(nreg, 0);
+  GR_CUDA_TRY(cudaMemcpyAsync(h_count.data(), count.p, sizeof(int) * nreg, cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaStreamSynchronize(s));
+  h_mem_off.assign(nreg + 1, 0);
+  for (int r = 0; r < nreg; ++r) h_mem_off[r + 1] = h_mem_off[r] + h_count[r];
+  n_members = h_mem_off[nreg];
+  if (n_members >= ((int64_t)1 << 31)) throw Error{-2, "too many region members"};
+  // grids over each halo box, cells at least rmax wide; cells numbered
+  // region by region, largest region first
+  h_grid.assign(nreg, GridParams{1, 1, 1, 1});
+  h_glo.assign(3 * (size_t)nreg, 0.0);
+  h_ginv.assign(3 * (size_t)nreg, 1.0);
+  std::vector<int> order(nreg);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return h_count[a] > h_count[b]; });
+  h_cell_off.assign(nreg + 1, 0);
+  std::vector<int> cell_region_h;
+  int64_t next = 0;
+  std::vector<int64_t> off_by_region(nreg, 0);
+  for (int k = 0; k < nreg; ++k) {
+    const int r = order[k];
+    int nc[3] = {1, 1, 1};
+    if (h_count[r] > 0) {
+      for (int d = 0; d < 3; ++d) {
+        const double span = h_halo[6 * r + 3 + d] - h_halo[6 * r + d];
+        double q = std::floor(span / (rmax * 1.000001));
+        if (!(q >= 1)) q = 1;
+        if (q > 1024) q = 1024;
+        nc[d] = (int)q;
+        h_glo[3 * r + d] = h_halo[6 * r + d];
+        h_ginv[3 * r + d] = 1.0 / (span / q);
+      }
+      // keep each region's cell table O(its members)
+      int64_t tot = (int64_t)nc[0] * nc[1] * nc[2];
+      while (tot > std::max<int64_t>(4 * (int64_t)h_count[r], 64)) {
+        int d = 0;
+        for (int e = 1; e < 3; ++e)
+          if (nc[e] > nc[d]) d = e;
+        nc[d] = std::max(1, nc[d] / 2);
+        const double span = h_halo[6 * r + 3 + d] - h_halo[6 * r + d];
+        h_ginv[3 * r + d] = 1.0 / (span / nc[d]);
+        tot = (int64_t)nc[0] * nc[1] * nc[2];
+      }
+    }
+    const int64_t cells = h_count[r] > 0 ? (int64_t)nc[0] * nc[1] * nc[2] : 0;
+    h_grid[r] = GridParams{nc[0], nc[1], nc[2], cells};
+    off_by_region[r] = next;
+    cell_region_h.insert(cell_region_h.end(), (size_t)cells, r);
+    next += cells;
+  }
+  ncell = next;
+  if (ncell >= ((int64_t)1 << 31)) throw Error{-2, "too many cells"};
+  for (int r = 0; r < nreg; ++r) h_cell_off[r] = (int)off_by_region[r];
+  h_cell_off[nreg] = (int)ncell;
+  // device geometry
+  glo.reserve(3 * (size_t)nreg);
+  ginv.reserve(3 * (size_t)nreg);
+  grid.reserve(nreg);
+  cell_off.reserve(nreg + 1);
+  mem_off.reserve(nreg + 1);
+  cell_region.reserve(ncell + 1);
+  std::vector<int> mo(nreg + 1);
+  for (int r = 0; r <= nreg; ++r) mo[r] = (int)h_mem_off[r];
+  GR_CUDA_TRY(cudaMemcpyAsync(glo.p, h_glo.data(), sizeof(double) * 3 * nreg, cudaMemcpyHostToDevice, s));
+  GR_CUDA_TRY(cudaMemcpyAsync(ginv.p, h_ginv.data(), sizeof(double) * 3 * nreg, cudaMemcpyHostToDevice, s));
+  GR_CUDA_TRY(cudaMemcpyAsync(grid.p, h_grid.data(), sizeof(GridParams) * nreg, cudaMemcpyHostToDevice, s));
+  GR_CUDA_TRY(cudaMemcpyAsync(cell_off.p, h_cell_off.data(), sizeof(int) * (nreg + 1), cudaMemcpyHostToDevice, s));
+  GR_CUDA_TRY(cudaMemcpyAsync(mem_off.p, mo.data(), sizeof(int) * (nreg + 1), cudaMemcpyHostToDevice, s));
+  if (ncell > 0)
+    GR_CUDA_TRY(cudaMemcpyAsync(cell_region.p, cell_region_h.data(), sizeof(int) * ncell,
+                                cudaMemcpyHostToDevice, s));
+  // member and layout buffers
+  const int64_t M = n_members;
+  m_orig.reserve(M + 1);
+  m_flag.reserve(M + 1);
+  m_key.reserve(M + 1);
+  m_slot.reserve(M + 1);
+  tmp_perm.reserve(M + 1);
+  perm.reserve(M + 1);
+  cell_count.reserve(ncell + 1);
+  cell_start64.reserve(ncell + 1);
+  cell_start.reserve(ncell + 1);
+  pos4.reserve(M + 1);
+  posd.reserve(M + 1);
+  w.reserve(M + 1);
+  orig.reserve(M + 1);
+  flags.reserve(M + 1);
+  cell_key.reserve(M + 1);
+  GR_CUDA_TRY(cudaStreamSynchronize(s));  // host vectors above must outlive the copies
+  valid = true;
+}
+
+// Device work of one call (no host synchronisation; capturable).
+void RegionLayout::enqueue_layout(const double* d_xyz, const double* d_w, cudaStream_t s) {
+  RegionGeomDev G;
+  G.halo = halo.p;
+  G.glo = glo.p;
+  G.ginv = ginv.p;
+  G.grid = grid.p;
+  G.cell_off = cell_off.p;
+  G.mem_off = mem_off.p;
+  G.ns = ns;
+  GR_CUDA_TRY(cudaMemsetAsync(count.p, 0, sizeof(int) * nreg, s));
+  GR_CUDA_TRY(cudaMemsetAsync(cell_count.p, 0, sizeof(int) * (ncell + 1), s));
+  if (n > 0)
+    b_member_kernel<true><<<nblocks(n, 256), 256, 0, s>>>(d_xyz, (int)n, (int)n_data, sub.p, G,
+                                                          count.p, m_orig.p, m_flag.p, m_key.p,
+                                                          m_slot.p, cell_count.p);
+  GR_CHECK_LAUNCH();
+  scan_i32_to_i64(cell_count.p, cell_start64.p, ncell, s, scan_tmp);
+  if (n_members > 0) {
+    b_scatter_kernel<<<nblocks(n_members, 256), 256, 0, s>>>(n_members, m_key.p, m_slot.p,
+                                                             cell_start64.p, tmp_perm.p);
+    b_order_kernel<<<nblocks(ncell * 32, 256, 148 * 16), 256, 0, s>>>(ncell, cell_start64.p,
+                                                                      tmp_perm.p, m_orig.p, perm.p);
+    b_gather_kernel<<<nblocks(n_members, 256), 256, 0, s>>>(n_members, perm.p, m_orig.p, m_flag.p,
+                                                            m_key.p, d_xyz, d_w, pos4.p, posd.p,
+                                                            w.p, orig.p, flags.p, cell_key.p);
+  }
+  b_narrow_kernel<<<nblocks(ncell + 1, 256), 256, 0, s>>>(cell_start64.p, cell_start.p, ncell + 1);
+  GR_CHECK_LAUNCH();
+}
+
+DevCatalog RegionLayout::view() const {
+  DevCatalog c;
+  c.pos4 = pos4.p;
+  c.posd = posd.p;
+  c.w = w.p;
+  c.orig = orig.p;
+  c.flags = flags.p;
+  c.cell_key = cell_key.p;
+  c.cell_start = cell_start.p;
+  c.n = (int)n_members;
+  c.n_data = (int)n_data;
+  c.grid = GridParams{1, 1, 1, ncell};
+  c.cell_region = cell_region.p;
+  c.region_grid = grid.p;
+  c.region_cell_off = cell_off.p;
+  return c;
+}
+
+}  // namespace gr

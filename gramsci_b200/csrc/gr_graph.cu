@@ -59,7 +59,13 @@ __global__ void __launch_bounds__(kGraphThreads) csr_cells_kernel(
     const int cb = C.cell_start[cell], ce = C.cell_start[cell + 1];
     if (cb == ce) continue;
     Ranges R;
-    forward_ranges(cb - 1, cell, C.grid, C.cell_start, R);
+    {
+      GridParams g;
+      const int* cs;
+      int lkey;
+      cell_grid(C, cell, g, cs, lkey);
+      forward_ranges(cb - 1, lkey, g, cs, R);
+    }
     int pre[5], total = 0;
 #pragma unroll
     for (int k = 0; k < 5; ++k) {

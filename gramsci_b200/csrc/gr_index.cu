@@ -292,6 +292,9 @@ DevCatalog CellIndex::view() const {
   c.n = (int)n;
   c.n_data = (int)n_data;
   c.grid = grid;
+  c.cell_region = nullptr;
+  c.region_grid = nullptr;
+  c.region_cell_off = nullptr;
   return c;
 }
 

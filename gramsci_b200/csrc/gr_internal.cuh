@@ -302,7 +302,29 @@ struct DevCatalog {
   int n;
   int n_data;
   GridParams grid;
+  // Batched regions: when cell_region is set, cells are grouped by region;
+  // region r owns cells [region_cell_off[r], region_cell_off[r+1]) laid out
+  // on its own grid region_grid[r].  NULL for a single grid.
+  const int* cell_region;
+  const GridParams* region_grid;
+  const int* region_cell_off;
 };
+
+// Grid, cell-start table and local key of a cell (single grid or region).
+__device__ __forceinline__ void cell_grid(const DevCatalog& C, int cell, GridParams& g,
+                                          const int*& cs, int& lkey) {
+  if (C.cell_region) {
+    const int r = C.cell_region[cell];
+    const int off = C.region_cell_off[r];
+    g = C.region_grid[r];
+    cs = C.cell_start + off;
+    lkey = cell - off;
+  } else {
+    g = C.grid;
+    cs = C.cell_start;
+    lkey = cell;
+  }
+}
 
 enum : uint8_t { FLAG_RANDOM = 1, FLAG_BUFFER = 2 };
 

@@ -369,6 +369,9 @@ extern "C" int gr_count_2pcf_noalloc(const double* d_xyz, const double* d_w, int
     C.grid.ny = g.nc[1];
     C.grid.nz = g.nc[2];
     C.grid.ncell = total;
+    C.cell_region = nullptr;
+    C.region_grid = nullptr;
+    C.region_cell_off = nullptr;
     PairParams P;
     make_pair_params(P, rmin, rmax, nbins, nmu, 0, coord_max, 0);
     const double fscale = fix_scale(wmax * wmax);

@@ -487,11 +487,11 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
 }  // namespace
 
 // Warps per block: as many as fit in shared memory (at most 32).
-static int tri3_warps(const TriParams& T, bool weighted, bool shist) {
+static int tri3_warps(const TriParams& T, bool weighted, bool shist, bool adj = false) {
   const int nh = T.ncfg * T.nmu * 4;
   int nw = kTriMaxWarps;
-  while (nw > 1 && tri_layout(nh, T.nmu, T.nbins, T.cap, shist, weighted, nw).total > kSmemLimit)
-    nw >>= 1;
+  while (nw > 1 && tri_layout(nh, T.nmu, T.nbins, T.cap, shist, weighted, nw, adj).total > kSmemLimit)
+    nw -= 1;
   return nw;
 }
 
@@ -540,9 +540,7 @@ void launch_adj3(const DevCatalog& C, const CSRView& G, const TriParams& T, cons
                  unsigned long long* g_hi, unsigned long long* stats, int* work, cudaStream_t s) {
   if (C.n <= 0) return;
   const int nh = T.ncfg * T.nmu * 4;
-  int nw = kTriMaxWarps;
-  while (nw > 1 && tri_layout(nh, T.nmu, T.nbins, T.cap, false, true, nw, true).total > kSmemLimit)
-    nw >>= 1;
+  const int nw = tri3_warps(T, true, false, true);
   const size_t smem = tri_layout(nh, T.nmu, T.nbins, T.cap, false, true, nw, true).total;
   if (smem > kSmemLimit) throw Error{-2, "3PCF adjoint: shared memory exceeds the SM limit"};
   GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));

@@ -132,6 +132,27 @@ int gr_graph_build(gr_ctx* ctx);
 int gr_graph_nedges(gr_ctx* ctx, int64_t* n_edges);
 int gr_graph_export(gr_ctx* ctx, int64_t* row_ptr, int32_t* col, uint8_t* bin, uint8_t* mu);
 
+/* Batched regions.  Replaces the reference's domain decomposition
+ * (src/domain_decomposition.f90:39-80) followed by one program run per
+ * region (`-cut`, src/gramsci.F90:1224-1231) and the hand summation of the
+ * outputs.  gr_set_regions(ctx, n) splits the catalogue's bounding box into
+ * n^3 equal regions (0 turns it off); each region's halo is its points'
+ * bounding box grown by rmax (strict bounds); points of other regions inside
+ * a halo are buffer points there.  gr_count_2pcf_batched counts the 2PCF of
+ * all regions in one launch (cells of every region from one work queue,
+ * largest region first), with the global galaxy/random flags and weight
+ * normalisation, so the result equals gr_count_2pcf on the whole catalogue.
+ * The first call for a catalogue/binning/split plans the layout and captures
+ * the device work in a CUDA graph; later calls replay it.  Outputs as
+ * gr_count_2pcf.  gr_regions_info / gr_regions_export describe the layout
+ * (member_off: nregions+1 offsets; per member its catalogue index and 1 if it
+ * is a buffer point), e.g. to run the regions one launch at a time. */
+int gr_set_regions(gr_ctx* ctx, int32_t nsplit);
+int gr_count_2pcf_batched(gr_ctx* ctx, double* N2, double* N3, int64_t* counts, double* catsum);
+int gr_regions_info(gr_ctx* ctx, int32_t* nregions, int64_t* nmembers);
+int gr_regions_export(gr_ctx* ctx, int64_t* member_off, int32_t* member_orig,
+                      int32_t* member_buffer);
+
 /* Weight adjoints.  Gradient of L = sum(cot2 * N2) + sum(cot3 * N3) with
  * respect to every signed normalised weight w_k (grad_w has N entries,
  * catalogue order).  cot2/cot3 have the shapes of N2/N3 of the matching
