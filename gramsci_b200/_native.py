@@ -20,6 +20,7 @@ GR_E_TIMEOUT = -4
 GR_E_UNSUPPORTED = -5
 GR_OPT_PRECISION = 1
 GR_OPT_TIMEOUT_MS = 2
+GR_OPT_AUTOTUNE = 3
 
 
 class GramsciError(RuntimeError):

@@ -120,6 +120,15 @@ class Context:
         v = {"f32": 0, "f64": 1}[mode]
         self._check(self._lib.gr_set_option(self._h, _native.GR_OPT_PRECISION, v))
 
+    def set_autotune(self, mode):
+        """'on' (time kernel variants once per workload class, cached),
+        'off', or an int variant to force (0 warp per cell, 1/2 block per
+        cell of 128/256 threads)."""
+        v = {"off": 0, "on": 1}.get(mode, None)
+        if v is None:
+            v = 2 + int(mode)
+        self._check(self._lib.gr_set_option(self._h, _native.GR_OPT_AUTOTUNE, v))
+
     def stats(self):
         s = _native.GrStats()
         self._check(self._lib.gr_get_stats(self._h, ctypes.byref(s)))

@@ -4,13 +4,14 @@
 // N2_b = sum over rooted pairs (i -> j) in bin b of w_i w_j
 // (src/gramsci.F90:362-379), so dN2_b/dw_k is the sum of w_j over the
 // edges (k, j) in bin b counted from each non-buffer end.  The kernel sweeps
-// every unordered pair once (the half-stencil cell sweep of the forward
-// kernel); a pair (p, q) with coefficient
+// every ordered pair (the full 27-cell neighbourhood of each root); a pair
+// (p, q) with coefficient
 //   c = [p root] (cot2 + [p, q random] cot3)[b, mu(p->q)]
 //     + [q root] (cot2 + [p, q random] cot3)[b, mu(q->p)]
-// adds c w_q to grad_p and c w_p to grad_q.  Gradients are summed as signed
-// 128-bit fixed-point integers, so they are exact up to the quantisation of
-// each term and independent of the summation order (deterministic).
+// adds c w_q to grad_p (and is seen again from q).  Gradients are summed as
+// signed 128-bit fixed-point integers, so they are exact up to the
+// quantisation of each term and independent of the summation order
+// (deterministic).
 #include "gr_kernels.cuh"
 
 namespace gr {
@@ -20,6 +21,39 @@ namespace {
 constexpr int kAdjWarps = 8;
 constexpr int kAdjThreads = kAdjWarps * 32;
 
+// Coefficient of the pair (p, q) in dL/dw: the cotangents of the bins the
+// pair lands in from each non-buffer end (cot3 only for random-random).
+__device__ __forceinline__ double pair_coef(const double* c2, const double* c3, int nbins, int b,
+                                            int mf, int mr, uint8_t fp, uint8_t fq) {
+  const bool rr = (fp & fq & FLAG_RANDOM) != 0;
+  double c = 0.0;
+  if (!(fp & FLAG_BUFFER)) {
+    const int k = (b - 1) + nbins * (mf - 1);
+    c += rr ? c2[k] + c3[k] : c2[k];
+  }
+  if (!(fq & FLAG_BUFFER)) {
+    const int k = (b - 1) + nbins * (mr - 1);
+    c += rr ? c2[k] + c3[k] : c2[k];
+  }
+  return c;
+}
+
+template <bool F32>
+__device__ __forceinline__ bool adj_edge(const DevCatalog& C, const PairParams& P, int p, int q,
+                                         const float4& pi, const float4& pj, int& b, int& mf,
+                                         int& mr) {
+  if (F32) {
+    const int r = classify_f32<true>(pi, pj, P, b, mf, mr);
+    if (r != 2) return r == 1;
+  }
+  return edge_f64(C.posd[p], C.posd[q], P, b, mf, mr);
+}
+
+// Every root visits its full 27-cell neighbourhood, so each ordered pair is
+// seen from both ends and a root only accumulates its own gradient: no
+// atomics, one store per root.  The pair test is symmetric (same edge, bins
+// swapped mu), so both ends agree on every pair.
+// Sparse cells: warp per cell, lanes over staged candidates.
 template <bool F32>
 __global__ void __launch_bounds__(kAdjThreads) adj2_kernel(DevCatalog C, PairParams P,
                                                            const double* __restrict__ cot2,
@@ -49,17 +83,17 @@ __global__ void __launch_bounds__(kAdjThreads) adj2_kernel(DevCatalog C, PairPar
     if (cell >= ncell) break;
     const int cb = C.cell_start[cell], ce = C.cell_start[cell + 1];
     if (cb == ce) continue;
-    Ranges R;
+    Ranges9 R;
     {
       GridParams g;
       const int* cs;
       int lkey;
       cell_grid(C, cell, g, cs, lkey);
-      forward_ranges(cb - 1, lkey, g, cs, R);
+      full_ranges(lkey, g, cs, R);
     }
-    int pre[5], total = 0;
+    int pre[9], total = 0;
 #pragma unroll
-    for (int k = 0; k < 5; ++k) {
+    for (int k = 0; k < 9; ++k) {
       pre[k] = total;
       if (k < R.n) total += R.end[k] - R.beg[k];
     }
@@ -67,48 +101,121 @@ __global__ void __launch_bounds__(kAdjThreads) adj2_kernel(DevCatalog C, PairPar
       const int tn = min(kCellTile, total - t0);
       __syncwarp();
       for (int f = lane; f < tn; f += 32) {
-        const int q = range_label(R, pre, t0 + f);
+        const int q = range9_label(R, pre, t0 + f);
         s_lab[wib][f] = q;
         s_pos[wib][f] = C.pos4[q];
       }
       __syncwarp();
       for (int p = cb; p < ce; ++p) {
-        const int fstart = max(0, p - cb + 1 - t0);
-        if (fstart >= tn) continue;
         const float4 pi = C.pos4[p];
         const uint8_t fp = C.flags[p];
-        const bool root_p = !(fp & FLAG_BUFFER);
-        const bool rp = fp & FLAG_RANDOM;
-        const double wp = C.w[p];
         Fix128 acc = {0ull, 0ull};
-        for (int f = fstart + lane; f < tn; f += 32) {
+        for (int f = lane; f < tn; f += 32) {
           const int q = s_lab[wib][f];
+          if (q == p) continue;
           int b, mf, mr;
-          bool e;
-          if (F32) {
-            const int r = classify_f32<true>(pi, s_pos[wib][f], P, b, mf, mr);
-            e = (r == 2) ? edge_f64(C.posd[p], C.posd[q], P, b, mf, mr) : (r == 1);
-          } else {
-            e = edge_f64(C.posd[p], C.posd[q], P, b, mf, mr);
-          }
-          if (!e) continue;
+          if (!adj_edge<F32>(C, P, p, q, pi, s_pos[wib][f], b, mf, mr)) continue;
           const uint8_t fq = C.flags[q];
-          const bool rr = rp && (fq & FLAG_RANDOM);
-          double c = 0.0;
-          if (root_p) {
-            const int k = (b - 1) + P.nbins * (mf - 1);
-            c += rr ? s_c2[k] + s_c3[k] : s_c2[k];
-          }
-          if (!(fq & FLAG_BUFFER)) {
-            const int k = (b - 1) + P.nbins * (mr - 1);
-            c += rr ? s_c2[k] + s_c3[k] : s_c2[k];
-          }
-          if (c == 0.0) continue;
-          fix_acc(acc, c * C.w[q], gscale);
-          fix_add(&g_lo[q], &g_hi[q], c * wp, gscale);
+          const double c = pair_coef(s_c2, s_c3, P.nbins, b, mf, mr, fp, fq);
+          if (c != 0.0) fix_acc(acc, c * C.w[q], gscale);
         }
         acc = fix_warp_sum(acc);
-        if (lane == 0 && (acc.lo | acc.hi)) fix_merge(&g_lo[p], &g_hi[p], acc.lo, acc.hi);
+        if (lane == 0) {
+          if (t0 == 0) {
+            g_lo[p] = acc.lo;
+            g_hi[p] = acc.hi;
+          } else {  // this warp owns p: plain 128-bit add
+            const unsigned long long lo = g_lo[p] + acc.lo;
+            g_hi[p] = g_hi[p] + acc.hi + (lo < acc.lo ? 1ull : 0ull);
+            g_lo[p] = lo;
+          }
+        }
+      }
+    }
+  }
+}
+
+// Dense cells: block per cell, thread per root, candidates broadcast from
+// shared memory.
+template <bool F32, int NT>
+__global__ void __launch_bounds__(NT) adj2_dense_kernel(DevCatalog C, PairParams P,
+                                                        const double* __restrict__ cot2,
+                                                        const double* __restrict__ cot3,
+                                                        double gscale,
+                                                        unsigned long long* __restrict__ g_lo,
+                                                        unsigned long long* __restrict__ g_hi,
+                                                        int* __restrict__ work) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  constexpr int TILE = 512;
+  __shared__ float4 s_pos[TILE];
+  __shared__ int s_lab[TILE];
+  __shared__ uint8_t s_flag[TILE];
+  __shared__ double s_w[TILE];
+  __shared__ int s_cell;
+  const int nbm = P.nbins * P.nmu;
+  double* s_c2 = reinterpret_cast<double*>(smem);
+  double* s_c3 = s_c2 + nbm;
+  for (int k = threadIdx.x; k < nbm; k += NT) {
+    s_c2[k] = cot2[k];
+    s_c3[k] = cot3 ? cot3[k] : 0.0;
+  }
+  const int ncell = (int)C.grid.ncell;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_cell = atomicAdd(work, 1);
+    __syncthreads();
+    const int cell = s_cell;
+    if (cell >= ncell) break;
+    const int cb = C.cell_start[cell], ce = C.cell_start[cell + 1];
+    if (cb == ce) continue;
+    Ranges9 R;
+    {
+      GridParams g;
+      const int* cs;
+      int lkey;
+      cell_grid(C, cell, g, cs, lkey);
+      full_ranges(lkey, g, cs, R);
+    }
+    int pre[9], total = 0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      pre[k] = total;
+      if (k < R.n) total += R.end[k] - R.beg[k];
+    }
+    for (int rb = cb; rb < ce; rb += NT) {
+      const int p = rb + threadIdx.x;
+      const bool act = p < ce;
+      float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
+      uint8_t fp = 0;
+      if (act) {
+        pi = C.pos4[p];
+        fp = C.flags[p];
+      }
+      Fix128 acc = {0ull, 0ull};
+      for (int t0 = 0; t0 < total; t0 += TILE) {
+        const int tn = min(TILE, total - t0);
+        __syncthreads();
+        for (int f = threadIdx.x; f < tn; f += NT) {
+          const int q = range9_label(R, pre, t0 + f);
+          s_lab[f] = q;
+          s_pos[f] = C.pos4[q];
+          s_flag[f] = C.flags[q];
+          s_w[f] = C.w[q];
+        }
+        __syncthreads();
+        if (!act) continue;
+        for (int f = 0; f < tn; ++f) {
+          const int q = s_lab[f];
+          if (q == p) continue;
+          int b, mf, mr;
+          if (!adj_edge<F32>(C, P, p, q, pi, s_pos[f], b, mf, mr)) continue;
+          const double c = pair_coef(s_c2, s_c3, P.nbins, b, mf, mr, fp, s_flag[f]);
+          if (c != 0.0) fix_acc(acc, c * s_w[f], gscale);
+        }
+      }
+      if (act) {
+        g_lo[p] = acc.lo;
+        g_hi[p] = acc.hi;
       }
     }
   }
@@ -127,10 +234,30 @@ __global__ void grad_finish_kernel(int n, const int* __restrict__ orig,
 
 void launch_adj2(const DevCatalog& C, const PairParams& P, const double* cot2, const double* cot3,
                  double gscale, unsigned long long* g_lo, unsigned long long* g_hi, int* work,
-                 cudaStream_t s) {
+                 cudaStream_t s, int variant) {
   if (C.n <= 0) return;
   const size_t smem = sizeof(double) * 2 * (size_t)P.nbins * P.nmu;
   GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));
+  if (variant == kPairDense128 || variant == kPairDense256) {
+#define GR_ADJ_DENSE(F, NT)                                                                    \
+  do {                                                                                         \
+    auto k = adj2_dense_kernel<F, NT>;                                                         \
+    GR_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    int per_sm = 1;                                                                            \
+    GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, smem));          \
+    int64_t blocks = (int64_t)std::max(1, per_sm) * 148;                                       \
+    if (blocks > C.grid.ncell) blocks = std::max<int64_t>(1, C.grid.ncell);                    \
+    k<<<(unsigned)blocks, NT, smem, s>>>(C, P, cot2, cot3, gscale, g_lo, g_hi, work);          \
+  } while (0)
+    if (P.f32) {
+      if (variant == kPairDense128) GR_ADJ_DENSE(true, 128); else GR_ADJ_DENSE(true, 256);
+    } else {
+      if (variant == kPairDense128) GR_ADJ_DENSE(false, 128); else GR_ADJ_DENSE(false, 256);
+    }
+#undef GR_ADJ_DENSE
+    GR_CHECK_LAUNCH();
+    return;
+  }
   int64_t blocks = (C.grid.ncell + kAdjWarps - 1) / kAdjWarps;
   if (blocks > 148 * 4) blocks = 148 * 4;
   if (blocks < 1) blocks = 1;

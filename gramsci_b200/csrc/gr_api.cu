@@ -5,8 +5,13 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
+#include <fstream>
 #include <limits>
+#include <map>
+#include <mutex>
 #include <new>
+#include <sys/stat.h>
 #include <string>
 #include <vector>
 
@@ -33,6 +38,8 @@ struct gr_ctx {
   double rmin = 0, rmax = 0;
   int nbins = 0, nmu = 1, logbins = 0;
   int precision = 0;
+  int autotune = 1;
+  int last_variant = 0;
   int64_t timeout_ms = 1000;
   // derived state
   CellIndex index;
@@ -53,6 +60,7 @@ struct gr_ctx {
   DevBuf<unsigned long long> bcnt, bfix, bstats;
   DevBuf<int> bwork;
   bool batch_weighted = false;
+  int batch_variant = 0;
   double batch_fscale = 1.0;
   cudaEvent_t bev[2] = {nullptr, nullptr};
   gr_stats st{};
@@ -188,6 +196,55 @@ void normal_table(int nmu, std::vector<uint8_t>& out) {
       }
       out[(size_t)(a - 1) + (size_t)nmu * (b - 1)] = (uint8_t)m;
     }
+}
+
+// ------------------------------------------------------------------ autotune --
+// Kernel variant per workload class, chosen by timing the variants on the
+// first workload of that class and cached in a JSON file
+// ($GRAMSCI_AUTOTUNE, default ~/.cache/gramsci_b200/autotune.json; an
+// unwritable path keeps the cache in memory).  The choice only affects
+// speed: every variant produces identical results.
+struct Tuner {
+  std::mutex mu;
+  bool loaded = false;
+  std::map<std::string, int> choice;
+  std::string path() const {
+    const char* e = std::getenv("GRAMSCI_AUTOTUNE");
+    if (e && e[0]) return e;
+    const char* h = std::getenv("HOME");
+    return std::string(h ? h : "/tmp") + "/.cache/gramsci_b200/autotune.json";
+  }
+  void load() {
+    if (loaded) return;
+    loaded = true;
+    std::ifstream f(path());
+    std::string line;
+    while (std::getline(f, line)) {
+      const size_t a = line.find('"'), b = line.find('"', a + 1), c = line.find(':', b);
+      if (a == std::string::npos || b == std::string::npos || c == std::string::npos) continue;
+      choice[line.substr(a + 1, b - a - 1)] = std::atoi(line.c_str() + c + 1);
+    }
+  }
+  void save() {
+    const std::string p = path();
+    const size_t slash = p.rfind('/');
+    if (slash != std::string::npos) {
+      std::string dir = p.substr(0, slash);
+      for (size_t k = 1; k <= dir.size(); ++k)
+        if (k == dir.size() || dir[k] == '/') mkdir(dir.substr(0, k).c_str(), 0755);
+    }
+    std::ofstream f(p);
+    if (!f) return;
+    f << "{\n";
+    size_t i = 0;
+    for (const auto& kv : choice) f << "  \"" << kv.first << "\": " << kv.second << (++i < choice.size() ? ",\n" : "\n");
+    f << "}\n";
+  }
+};
+
+Tuner& tuner() {
+  static Tuner t;
+  return t;
 }
 
 int set_err(gr_ctx* c, int code, const std::string& m) {
@@ -417,6 +474,9 @@ int gr_set_option(gr_ctx* c, int32_t key, int64_t value) {
   if (key == GR_OPT_PRECISION) {
     if (value != 0 && value != 1) return set_err(c, GR_E_ARG, "precision must be 0 or 1");
     c->precision = (int)value;
+  } else if (key == GR_OPT_AUTOTUNE) {
+    if (value < 0 || value > 1 + kPairVariants) return set_err(c, GR_E_ARG, "autotune must be 0, 1 or 2+variant");
+    c->autotune = (int)value;
   } else if (key == GR_OPT_TIMEOUT_MS) {
     if (value <= 0) return set_err(c, GR_E_ARG, "timeout must be positive");
     c->timeout_ms = value;
@@ -424,6 +484,56 @@ int gr_set_option(gr_ctx* c, int32_t key, int64_t value) {
     return set_err(c, GR_E_UNSUPPORTED, "unknown option");
   }
   GR_API_END(c)
+}
+
+// Pair-sweep variant for a catalogue layout: cached per workload class or
+// timed now (histograms are reset by the caller afterwards).
+static int pick_pair2_variant(gr_ctx* c, const DevCatalog& C, bool weighted, double fscale,
+                              unsigned long long* hcnt, unsigned long long* hfix,
+                              unsigned long long* stats, int* work, cudaStream_t s) {
+  if (c->autotune == 0) return kPairWarpCell;
+  if (c->autotune >= 2) return c->autotune - 2;
+  const double per_cell = C.grid.ncell > 0 ? (double)C.n / (double)C.grid.ncell : 1.0;
+  int dens = 0;
+  while (dens < 20 && std::ldexp(1.0, dens + 1) <= per_cell) ++dens;
+  int hb = 0;
+  while (hb < 20 && (2 << hb) <= c->nbins * c->nmu) ++hb;
+  char key[128];
+  std::snprintf(key, sizeof(key), "pair2|%s|%s|dens%d|hist%d", c->P.f32 ? "f32" : "f64",
+                weighted ? "w" : "u", dens, hb);
+  Tuner& T = tuner();
+  {
+    std::lock_guard<std::mutex> lock(T.mu);
+    T.load();
+    auto it = T.choice.find(key);
+    if (it != T.choice.end()) return it->second;
+  }
+  const int nh = c->nbins * c->nmu * 4;
+  cudaEvent_t a, b;
+  GR_CUDA_TRY(cudaEventCreate(&a));
+  GR_CUDA_TRY(cudaEventCreate(&b));
+  int best = kPairWarpCell;
+  float best_ms = 1e30f;
+  for (int v = 0; v < kPairVariants; ++v) {
+    GR_CUDA_TRY(cudaMemsetAsync(hcnt, 0, sizeof(unsigned long long) * nh, s));
+    GR_CUDA_TRY(cudaMemsetAsync(hfix, 0, sizeof(unsigned long long) * 2 * nh, s));
+    GR_CUDA_TRY(cudaEventRecord(a, s));
+    launch_pair2(C, c->P, weighted, hcnt, hfix, fscale, stats, work, s, v);
+    GR_CUDA_TRY(cudaEventRecord(b, s));
+    GR_CUDA_TRY(cudaEventSynchronize(b));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = v;
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  std::lock_guard<std::mutex> lock(T.mu);
+  T.choice[key] = best;
+  T.save();
+  return best;
 }
 
 int gr_count_2pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* catsum) {
@@ -440,12 +550,16 @@ int gr_count_2pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
   GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
   build_index(c);
   GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+  c->work.reserve(4);
+  const int variant = pick_pair2_variant(c, c->index.view(), weighted, fscale, c->hcnt.p,
+                                         c->hfix.p, c->stats.p, c->work.p, s);
+  c->last_variant = variant;
+  GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
   GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nh, s));
   GR_CUDA_TRY(cudaMemsetAsync(c->hfix.p, 0, sizeof(unsigned long long) * 2 * nh, s));
   GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
-  c->work.reserve(4);
   launch_pair2(c->index.view(), c->P, weighted, c->hcnt.p, c->hfix.p, fscale, c->stats.p,
-               c->work.p, s);
+               c->work.p, s, variant);
   GR_CUDA_TRY(cudaEventRecord(c->ev[2], s));
   std::vector<unsigned long long> hc(nh), hf(2 * nh, 0ull);
   std::vector<double> hs(nh, 0.0);
@@ -796,8 +910,10 @@ int gr_adjoint_2pcf(gr_ctx* c, const double* cot2, const double* cot3, double* g
   GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
   GR_CUDA_TRY(cudaMemsetAsync(c->gfix.p, 0, sizeof(unsigned long long) * (2 * n + 2), s));
   std::memset(&c->st, 0, sizeof(c->st));
+  // same sweep layout as the forward pass on this catalogue
+  const int variant = c->autotune >= 2 ? c->autotune - 2 : c->last_variant;
   launch_adj2(c->index.view(), c->P, c->cot.p, cot3 ? c->cot.p + nbm : nullptr, gscale, c->gfix.p,
-              c->gfix.p + n, c->work.p, s);
+              c->gfix.p + n, c->work.p, s, variant);
   finish_grad(c, gscale, grad_w, c->ev[1]);
   c->st.ms_index = ev_ms(c->ev[0], c->ev[1]);
   c->st.ms_total = c->st.ms_index + c->st.ms_query;
@@ -877,7 +993,7 @@ static void enqueue_batched(gr_ctx* c, cudaStream_t s) {
   GR_CUDA_TRY(cudaMemsetAsync(c->bfix.p, 0, sizeof(unsigned long long) * 2 * nh, s));
   GR_CUDA_TRY(cudaMemsetAsync(c->bstats.p, 0, sizeof(unsigned long long) * 8, s));
   launch_pair2(c->regions.view(), c->P, c->batch_weighted, c->bcnt.p, c->bfix.p, c->batch_fscale,
-               c->bstats.p, c->bwork.p, s);
+               c->bstats.p, c->bwork.p, s, c->batch_variant);
 }
 
 int gr_count_2pcf_batched(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* catsum) {
@@ -908,7 +1024,12 @@ int gr_count_2pcf_batched(gr_ctx* c, double* N2, double* N3, int64_t* counts, do
     c->bfix.reserve(2 * nh);
     c->bstats.reserve(8);
     c->bwork.reserve(4);
-    // first run eagerly, then capture the same work for replay
+    // lay out once, pick the pair-sweep variant on this layout, then run
+    // eagerly and capture the same work for replay
+    c->batch_variant = kPairWarpCell;
+    c->regions.enqueue_layout(c->xyz.p, c->w.p, s);
+    c->batch_variant = pick_pair2_variant(c, c->regions.view(), c->batch_weighted, c->batch_fscale,
+                                          c->bcnt.p, c->bfix.p, c->bstats.p, c->bwork.p, s);
     enqueue_batched(c, s);
     GR_CUDA_TRY(cudaStreamSynchronize(s));
     c->regions.release_graph();

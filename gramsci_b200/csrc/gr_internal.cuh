@@ -240,6 +240,46 @@ __device__ __forceinline__ void forward_ranges(int p, int key, const GridParams&
   }
 }
 
+// All 27 neighbouring cells (own cell included) as at most 9 contiguous
+// label ranges in increasing order.
+struct Ranges9 {
+  int n;
+  int beg[9], end[9];
+};
+
+__device__ __forceinline__ void full_ranges(int key, const GridParams& g,
+                                            const int* __restrict__ cell_start, Ranges9& R) {
+  const int cx = key % g.nx;
+  const int cy = (key / g.nx) % g.ny;
+  const int cz = key / (g.nx * g.ny);
+  const int x0 = cx > 0 ? cx - 1 : 0;
+  const int x1 = cx + 1 < g.nx ? cx + 1 : cx;
+  R.n = 0;
+  for (int dz = -1; dz <= 1; ++dz) {
+    const int z = cz + dz;
+    if (z < 0 || z >= g.nz) continue;
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int y = cy + dy;
+      if (y < 0 || y >= g.ny) continue;
+      const int kb = (z * g.ny + y) * g.nx;
+      const int b = cell_start[kb + x0], e = cell_start[kb + x1 + 1];
+      if (e > b) {
+        R.beg[R.n] = b;
+        R.end[R.n] = e;
+        R.n++;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ int range9_label(const Ranges9& R, const int* pre, int f) {
+  int r = 0;
+#pragma unroll
+  for (int k = 1; k < 9; ++k)
+    if (k < R.n && f >= pre[k]) r = k;
+  return R.beg[r] + (f - pre[r]);
+}
+
 // Map flattened candidate index f (0 <= f < total) to a label.
 __device__ __forceinline__ int range_label(const Ranges& R, const int* pre, int f) {
   int r = 0;

@@ -15,10 +15,14 @@ constexpr size_t kMaxHistSmem = 120 * 1024;
 // 2PCF: pairs binned straight from the half-stencil cell sweep.
 // g_cnt (nh = nbins*nmu*4) and g_fix (2*nh, weighted only) must be zeroed.
 // stats: [0] FP64 rechecks, [1] candidates, [2] binned unordered pairs.
+// variant: kPairWarpCell (warp per cell, lanes over candidates; sparse
+// cells) or kPairDense128/256 (block per cell, thread per root, broadcast
+// candidates; dense cells).  The autotuner picks one per workload class.
+enum { kPairWarpCell = 0, kPairDense128 = 1, kPairDense256 = 2, kPairVariants = 3 };
 size_t pair2_smem_bytes(const PairParams& P, bool weighted);
 void launch_pair2(const DevCatalog& C, const PairParams& P, bool weighted,
                   unsigned long long* g_cnt, unsigned long long* g_fix, double fscale,
-                  unsigned long long* stats, int* work, cudaStream_t s);
+                  unsigned long long* stats, int* work, cudaStream_t s, int variant = kPairWarpCell);
 
 struct TriParams {
   int nbins, nmu, ncfg, rsd;
@@ -38,12 +42,13 @@ void launch_tri3(const DevCatalog& C, const CSRView& G, const TriParams& T, bool
                  unsigned long long* stats, int* work, cudaStream_t s);
 
 // Weight adjoints: gradient of sum(cot2 * N2) + sum(cot3 * N3) with respect
-// to the weights, as 128-bit fixed-point sums (g_lo, g_hi, label order,
-// zeroed by the caller) of scale gscale; launch_grad_finish converts them to
+// to the weights, as 128-bit fixed-point sums (g_lo, g_hi, label order; the
+// 2PCF adjoint writes every entry, the 3PCF adjoint needs them zeroed) of
+// scale gscale; launch_grad_finish converts them to
 // FP64 in catalogue order.  cot3 may be NULL.
 void launch_adj2(const DevCatalog& C, const PairParams& P, const double* cot2, const double* cot3,
                  double gscale, unsigned long long* g_lo, unsigned long long* g_hi, int* work,
-                 cudaStream_t s);
+                 cudaStream_t s, int variant = kPairWarpCell);
 void launch_adj3(const DevCatalog& C, const CSRView& G, const TriParams& T, const double* cot2,
                  const double* cot3, double gscale, unsigned long long* g_lo,
                  unsigned long long* g_hi, unsigned long long* stats, int* work, cudaStream_t s);

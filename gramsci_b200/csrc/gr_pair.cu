@@ -147,6 +147,150 @@ __global__ void __launch_bounds__(kPairThreads) pair2_kernel(DevCatalog C, PairP
   }
 }
 
+
+// Dense-cell variant: one block per cell, one thread per root, the cell's
+// forward candidates staged in shared memory tiles and read by all threads
+// at the same address (broadcast), so each candidate costs one shared load
+// per warp instead of one per lane.  Suits cells holding many points (the
+// warp-per-cell variant suits sparse cells, where most threads here would
+// idle).  Same contributions, same histogram layout.
+template <bool F32, bool WEIGHTED, bool SHIST, int NT>
+__global__ void __launch_bounds__(NT) pair2_dense_kernel(DevCatalog C, PairParams P,
+                                                         unsigned long long* __restrict__ g_cnt,
+                                                         unsigned long long* __restrict__ g_fix,
+                                                         double fscale,
+                                                         unsigned long long* __restrict__ stats,
+                                                         int* __restrict__ work) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  constexpr int TILE = 512;
+  __shared__ float4 s_pos[TILE];
+  __shared__ int s_lab[TILE];
+  __shared__ uint8_t s_flag[TILE];
+  __shared__ double s_w[WEIGHTED ? TILE : 1];
+  __shared__ int s_cell;
+  const int nbm = P.nbins * P.nmu;
+  const int nh = nbm * 4;
+  unsigned long long* s_cnt = SHIST ? reinterpret_cast<unsigned long long*>(smem) : g_cnt;
+  unsigned long long* s_lo = SHIST ? s_cnt + nh : g_fix;
+  unsigned long long* s_hi = s_lo + nh;
+  if (SHIST) {
+    for (int k = threadIdx.x; k < nh; k += NT) {
+      s_cnt[k] = 0ull;
+      if (WEIGHTED) {
+        s_lo[k] = 0ull;
+        s_hi[k] = 0ull;
+      }
+    }
+  }
+  const int ncell = (int)C.grid.ncell;
+  unsigned long long rechecks = 0, cands = 0, pairs = 0;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_cell = atomicAdd(work, 1);
+    __syncthreads();
+    const int cell = s_cell;
+    if (cell >= ncell) break;
+    const int cb = C.cell_start[cell], ce = C.cell_start[cell + 1];
+    if (cb == ce) continue;
+    Ranges R;
+    {
+      GridParams g;
+      const int* cs;
+      int lkey;
+      cell_grid(C, cell, g, cs, lkey);
+      forward_ranges(cb - 1, lkey, g, cs, R);
+    }
+    int pre[5], total = 0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      pre[k] = total;
+      if (k < R.n) total += R.end[k] - R.beg[k];
+    }
+    for (int rb = cb; rb < ce; rb += NT) {
+      const int p = rb + threadIdx.x;
+      const bool act = p < ce;
+      float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
+      uint8_t fp = 0;
+      double wp = 0.0;
+      if (act) {
+        pi = C.pos4[p];
+        fp = C.flags[p];
+        if (WEIGHTED) wp = C.w[p];
+      }
+      const bool root_p = !(fp & FLAG_BUFFER);
+      const int rp = fp & FLAG_RANDOM;
+      for (int t0 = 0; t0 < total; t0 += TILE) {
+        const int tn = min(TILE, total - t0);
+        __syncthreads();
+        for (int f = threadIdx.x; f < tn; f += NT) {
+          const int q = range_label(R, pre, t0 + f);
+          s_lab[f] = q;
+          s_pos[f] = C.pos4[q];
+          s_flag[f] = C.flags[q];
+          if (WEIGHTED) s_w[f] = C.w[q];
+        }
+        __syncthreads();
+        if (!act) continue;
+        // candidates with label > p: own-cell candidates are the first
+        // (ce - cb) flattened entries, labels cb, cb+1, ...
+        const int fstart = max(0, p - cb + 1 - t0);
+        if (fstart < tn) cands += (unsigned long long)(tn - fstart);
+        for (int f = fstart; f < tn; ++f) {
+          int b, mf, mr;
+          bool e;
+          if (F32) {
+            const int r = classify_f32<true>(pi, s_pos[f], P, b, mf, mr);
+            if (r == 2) {
+              rechecks++;
+              e = edge_f64(C.posd[p], C.posd[s_lab[f]], P, b, mf, mr);
+            } else {
+              e = r == 1;
+            }
+          } else {
+            e = edge_f64(C.posd[p], C.posd[s_lab[f]], P, b, mf, mr);
+          }
+          if (!e) continue;
+          const uint8_t fq = s_flag[f];
+          const int rq = fq & FLAG_RANDOM;
+          pairs += (root_p || !(fq & FLAG_BUFFER)) ? 1 : 0;
+          const double prod = WEIGHTED ? wp * s_w[f] : 0.0;
+          if (root_p) {
+            const int k = (b - 1) + P.nbins * (mf - 1) + nbm * (2 * rp + rq);
+            atomicAdd(&s_cnt[k], 1ull);
+            if (WEIGHTED) fix_add(&s_lo[k], &s_hi[k], prod, fscale);
+          }
+          if (!(fq & FLAG_BUFFER)) {
+            const int k = (b - 1) + P.nbins * (mr - 1) + nbm * (2 * rq + rp);
+            atomicAdd(&s_cnt[k], 1ull);
+            if (WEIGHTED) fix_add(&s_lo[k], &s_hi[k], prod, fscale);
+          }
+        }
+      }
+    }
+  }
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    rechecks += __shfl_xor_sync(0xffffffffu, rechecks, o);
+    pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
+    cands += __shfl_xor_sync(0xffffffffu, cands, o);
+  }
+  if (lane == 0) {
+    if (rechecks) atomicAdd(&stats[0], rechecks);
+    if (cands) atomicAdd(&stats[1], cands);
+    if (pairs) atomicAdd(&stats[2], pairs);
+  }
+  if (SHIST) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < nh; k += NT) {
+      if (s_cnt[k]) {
+        atomicAdd(&g_cnt[k], s_cnt[k]);
+        if (WEIGHTED) fix_merge(&g_fix[k], &g_fix[nh + k], s_lo[k], s_hi[k]);
+      }
+    }
+  }
+}
+
 }  // namespace
 
 size_t pair2_smem_bytes(const PairParams& P, bool weighted) {
@@ -156,12 +300,43 @@ size_t pair2_smem_bytes(const PairParams& P, bool weighted) {
 
 void launch_pair2(const DevCatalog& C, const PairParams& P, bool weighted,
                   unsigned long long* g_cnt, unsigned long long* g_fix, double fscale,
-                  unsigned long long* stats, int* work, cudaStream_t s) {
+                  unsigned long long* stats, int* work, cudaStream_t s, int variant) {
   if (C.n <= 0) return;
   size_t smem = pair2_smem_bytes(P, weighted);
   const bool shist = smem <= kMaxHistSmem;
   if (!shist) smem = 0;
   GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));
+  if (variant == kPairDense128 || variant == kPairDense256) {
+    int per_sm = 1;
+#define GR_DENSE_LAUNCH(F, W, S, NT)                                                          \
+  do {                                                                                        \
+    auto k = pair2_dense_kernel<F, W, S, NT>;                                                 \
+    GR_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
+                                     (int)smem));                                             \
+    GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, smem));         \
+    int64_t blocks = (int64_t)std::max(1, per_sm) * 148;                                      \
+    if (blocks > C.grid.ncell) blocks = std::max<int64_t>(1, C.grid.ncell);                   \
+    k<<<(unsigned)blocks, NT, smem, s>>>(C, P, g_cnt, g_fix, fscale, stats, work);            \
+  } while (0)
+#define GR_DENSE_NT(F, W, S)                                                                  \
+  do {                                                                                        \
+    if (variant == kPairDense128) GR_DENSE_LAUNCH(F, W, S, 128); else GR_DENSE_LAUNCH(F, W, S, 256); \
+  } while (0)
+#define GR_DENSE_W(F, S)                                                                      \
+  do {                                                                                        \
+    if (weighted) GR_DENSE_NT(F, true, S); else GR_DENSE_NT(F, false, S);                     \
+  } while (0)
+    if (P.f32) {
+      if (shist) GR_DENSE_W(true, true); else GR_DENSE_W(true, false);
+    } else {
+      if (shist) GR_DENSE_W(false, true); else GR_DENSE_W(false, false);
+    }
+#undef GR_DENSE_W
+#undef GR_DENSE_NT
+#undef GR_DENSE_LAUNCH
+    GR_CHECK_LAUNCH();
+    return;
+  }
   int64_t blocks = (C.grid.ncell + kPairWarps - 1) / kPairWarps;
   if (blocks > 148 * 4) blocks = 148 * 4;
   if (blocks < 1) blocks = 1;

@@ -45,6 +45,9 @@ typedef struct gr_ctx gr_ctx;
 /* Options for gr_set_option. */
 #define GR_OPT_PRECISION 1 /* 0: FP32 separations + FP64 guard band (default); 1: FP64 throughout */
 #define GR_OPT_TIMEOUT_MS 2 /* bound on device-side waits in the persistent batched kernel */
+#define GR_OPT_AUTOTUNE 3   /* 0: fixed kernels; 1: time the pair-sweep variants once per
+                               workload class and cache the choice (default); 2+v: force
+                               variant v (0 warp per cell, 1/2 block per cell of 128/256) */
 
 /* Run statistics of the last count call (gr_get_stats). */
 typedef struct gr_stats {

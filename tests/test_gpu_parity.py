@@ -135,3 +135,24 @@ def test_buffer_points(gpu_ctx, oracle, query):
     else:
         got, ref = gpu_ctx.count_3pcf(), G.pcf3(w, cat.n_data, buffer=buf)
     _check_sums(got, ref)
+
+
+@pytest.mark.parametrize("name,scale,nmu,weighted", [("c1_2pcf", 0.1, 3, True),
+                                                      ("c4_batched", 0.003, 10, False),
+                                                      ("c5_adjoint_2pcf", 0.002, 4, True)])
+def test_pair_sweep_variants_agree(gpu_ctx, oracle, name, scale, nmu, weighted):
+    """Every pair-sweep variant the autotuner can pick gives the oracle's
+    counts (sparse and dense cells)."""
+    cat, w, sp = _cat(name, scale)
+    if weighted:
+        w = catalogs.normalise(np.random.default_rng(1).lognormal(0, 0.3, cat.n), cat.n_data,
+                               cat.n_rand)
+    gpu_ctx.set_catalog(cat.xyz, w, cat.n_data)
+    gpu_ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], nmu)
+    ref = oracle.Graph(cat.xyz, sp["rmin"], sp["rmax"], sp["nbins"], nmu).pcf2(w, cat.n_data)
+    try:
+        for v in range(3):
+            gpu_ctx.set_autotune(v)
+            _check_sums(gpu_ctx.count_2pcf(), ref)
+    finally:
+        gpu_ctx.set_autotune("on")
