@@ -97,7 +97,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -217,11 +217,11 @@ def run_ours(args):
         if world > 1:
             torch.distributed.barrier()
 
+    sampler = ClockSampler(device)
+    sampler.start()
     for _ in range(args.warmup):
         ctx.count_3pcf()
     torch.cuda.synchronize()
-    sampler = ClockSampler(device)
-    sampler.start()
     barrier()
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
@@ -291,6 +291,7 @@ def run_ours(args):
 
     peaks = roofline.peaks()
     rf = roofline.tri3_roofline(ctx, q_ms, peaks)
+    rf["traffic"] = roofline.profiled_traffic("tri3_kernel", args.scale)
 
     line = {
         "metric": METRIC, "value": value, "unit": "tuples/s", "n_gpus": world,

@@ -28,6 +28,7 @@ constexpr size_t kSmemLimit = 227 * 1024;
 constexpr int kOwn = 512;    // flattened work items per owner-table chunk
 constexpr int kQueue = 64;   // hit queue entries per warp
 constexpr int kChunk = 4;    // roots taken per work-counter increment
+constexpr int kCfgTableBins = 16;  // nbins up to which the configuration table is used
 
 __host__ __device__ inline size_t align8(size_t x) { return (x + 7) & ~(size_t)7; }
 __host__ __device__ inline int hash_size(int cap) {
@@ -37,7 +38,7 @@ __host__ __device__ inline int hash_size(int cap) {
 }
 
 struct TriLayout {
-  size_t off_cnt, off_fix, off_cot, off_norm, off_rank, off_warp, warp_bytes, total;
+  size_t off_cnt, off_fix, off_cot, off_norm, off_rank, off_cfg, off_warp, warp_bytes, total;
   // per-warp sub-offsets
   size_t o_rs, o_w, o_g, o_col, o_meta, o_orig, o_pre, o_hkey, o_qm, o_qxy, o_flag, o_hval, o_own;
 };
@@ -58,6 +59,8 @@ __host__ __device__ inline TriLayout tri_layout(int nh, int nmu, int nbins, int 
   o = align8(o + (size_t)nmu * nmu);
   L.off_rank = o;
   o = align8(o + sizeof(int) * 3 * (size_t)(nbins + 2));
+  L.off_cfg = o;  // configuration of every (b1, b2, b3), small nbins only
+  if (nbins <= kCfgTableBins) o = align8(o + sizeof(uint16_t) * (size_t)nbins * nbins * nbins);
   L.off_warp = o;
   const int hs = hash_size(cap);
   size_t w = 0;
@@ -82,6 +85,7 @@ __host__ __device__ inline TriLayout tri_layout(int nh, int nmu, int nbins, int 
 struct TriCtx {
   const uint8_t* norm;
   const int* F;  // 3 x (nbins+2)
+  const uint16_t* cfgtab;  // symmetric configuration table or NULL
   int nbins, nmu, ncfg, rsd, nh;
   unsigned long long* cnt;
   unsigned long long* lo;  // fixed-point sums: lo[k], lo[nh + k] = hi[k]
@@ -96,6 +100,13 @@ __device__ __forceinline__ int rank3_s(const int* F, int nb2, int a, int b, int 
   return 1 + (F[a] - F[1]) + (F[nb2 + b] - F[nb2 + a]) + (F[2 * nb2 + c] - F[2 * nb2 + b]);
 }
 
+// symmetric bin table of the three radial bins (gramsci.F90:1459-1474)
+__device__ __forceinline__ int tri_cfg(const TriCtx& X, int b1, int b2, int b3) {
+  if (X.cfgtab) return X.cfgtab[(b1 - 1) + X.nbins * ((b2 - 1) + X.nbins * (b3 - 1))];
+  sort3i(b1, b2, b3);
+  return rank3_s(X.F, X.nbins + 2, b1, b2, b3);
+}
+
 __device__ __forceinline__ int normal_bin(const TriCtx& X, int mu1, int mu2, bool first_is_1) {
   if (!X.rsd) return 1;
   return first_is_1 ? X.norm[(mu1 - 1) + X.nmu * (mu2 - 1)] : X.norm[(mu2 - 1) + X.nmu * (mu1 - 1)];
@@ -108,9 +119,7 @@ template <bool WEIGHTED>
 __device__ __forceinline__ int tri_bin(const TriCtx& X, uint8_t fp, int op, double wp, uint8_t fa,
                                        int oa, double wa, uint8_t fc, int oc, double wc,
                                        uint32_t mpa, uint32_t mpc, uint32_t mac) {
-  int s1 = meta_bin(mpa), s2 = meta_bin(mpc), s3 = meta_bin(mac);
-  sort3i(s1, s2, s3);
-  const int cfg = rank3_s(X.F, X.nbins + 2, s1, s2, s3);
+  const int cfg = tri_cfg(X, meta_bin(mpa), meta_bin(mpc), meta_bin(mac));
   const int nr = (fp & FLAG_RANDOM) + (fa & FLAG_RANDOM) + (fc & FLAG_RANDOM);
   int m[3] = {-1, -1, -1};
   double pr[3] = {0.0, 0.0, 0.0};
@@ -160,9 +169,7 @@ __device__ __forceinline__ int tri_grad(const TriCtx& X, uint8_t fp, int op, dou
                                         Fix128& racc, unsigned long long* alo,
                                         unsigned long long* ahi, unsigned long long* clo,
                                         unsigned long long* chi) {
-  int s1 = meta_bin(mpa), s2 = meta_bin(mpc), s3 = meta_bin(mac);
-  sort3i(s1, s2, s3);
-  const int cfg = rank3_s(X.F, X.nbins + 2, s1, s2, s3);
+  const int cfg = tri_cfg(X, meta_bin(mpa), meta_bin(mpc), meta_bin(mac));
   const bool allr = (fp & fa & fc & FLAG_RANDOM) != 0;
   double C = 0.0;
   int n = 0;
@@ -260,6 +267,18 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
   const int nb2 = T.nbins + 2;
   for (int k = threadIdx.x; k < 3 * nb2; k += blockDim.x) s_F[k] = T.rank.F[k / nb2][k % nb2];
   __syncthreads();
+  X.cfgtab = nullptr;
+  if (T.nbins <= kCfgTableBins) {
+    uint16_t* tab = reinterpret_cast<uint16_t*>(smem + L.off_cfg);
+    const int nb = T.nbins;
+    for (int k = threadIdx.x; k < nb * nb * nb; k += blockDim.x) {
+      int a = k % nb + 1, b = (k / nb) % nb + 1, c = k / (nb * nb) + 1;
+      sort3i(a, b, c);
+      tab[k] = (uint16_t)rank3_s(s_F, nb2, a, b, c);
+    }
+    __syncthreads();
+    X.cfgtab = tab;
+  }
 
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
@@ -336,7 +355,11 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
             const int y = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += y;
           }
-          if (x < k) s_pre[x + 1] = carry + incl;
+          if (x < k) {
+            s_pre[x + 1] = carry + incl;
+            // record index of work item f = s_rs[x] + f
+            s_rs[x] -= (long long)(carry + incl - len);
+          }
           carry += __shfl_sync(0xffffffffu, incl, 31);
         }
         if (lane == 0) s_pre[0] = 0;
@@ -361,7 +384,7 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
             uint32_t mac = 0;
             if (f < fe) {
               x = s_own[f - fb];
-              const unsigned long long r = G.rec[s_rs[x] + (f - s_pre[x])];
+              const unsigned long long r = G.rec[s_rs[x] + f];
               const int c = rec_col(r);
               mac = rec_meta(r);
               uint32_t h = hash_slot(c, hmask);

@@ -38,3 +38,17 @@ def tri3_roofline(ctx, q_ms, pk):
     return {"bound": "hbm", "kernel": "tri3_kernel", "achieved": achieved, "peak": pk["hbm_gbs"],
             "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "traffic": None,
             "bytes_per_launch": b, "ms_per_launch": ms, "peak_source": pk["source"]}
+
+
+def profiled_traffic(kernel, scale):
+    """DRAM bytes (read + write) per launch of `kernel` from the committed ncu
+    summary profiles/<kernel>_c2.json, for the full-size workload only."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_c2.json")
+    if scale != 1.0 or not os.path.exists(p):
+        return None
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["dram_bytes_read"]) + float(d["dram_bytes_write"])
+    except Exception:
+        return None
