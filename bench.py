@@ -59,6 +59,22 @@ def dist_env():
     return rank, world, local
 
 
+def rank_seed(rank):
+    """Seed of rank `rank`'s mock: rank 0 uses the workload's own seed, the
+    others independent ones (weak scaling over independent mocks)."""
+    return None if rank == 0 else 1000 + rank
+
+
+def reduce_over_ranks(value, op, device):
+    """All-reduce one number over the ranks ('max' or 'sum')."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def make_catalogue(scale, seed):
     from gramsci_b200 import catalogs
 
@@ -201,8 +217,7 @@ def run_ours(args):
     torch.cuda.set_device(device)
     from gramsci_b200 import api
 
-    seed = None if rank == 0 else 1000 + rank
-    cat, w, sp = make_catalogue(args.scale, seed)
+    cat, w, sp = make_catalogue(args.scale, rank_seed(rank))
     stream = torch.cuda.current_stream()
     ctx = api.Context(device)
     ctx.set_stream(stream)
@@ -245,14 +260,8 @@ def run_ours(args):
     t_max = total_ms
     tri_all = tri
     if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([total_ms], device=f"cuda:{device}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-        c = torch.tensor([tri], device=f"cuda:{device}", dtype=torch.float64)
-        dist.all_reduce(c, op=dist.ReduceOp.SUM)
-        tri_all = float(c.item())
+        t_max = reduce_over_ranks(total_ms, "max", f"cuda:{device}")
+        tri_all = reduce_over_ranks(tri, "sum", f"cuda:{device}")
     value = tri_all / (t_max / 1e3)
 
     # end to end through the public API: pinned host catalogue -> device,
@@ -274,11 +283,7 @@ def run_ours(args):
     e2e_tri = ctx.stats()["tuples"]
     e2e_t = float(np.mean(e2e_ms))
     if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([e2e_t], device=f"cuda:{device}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_t = float(t.item())
+        e2e_t = reduce_over_ranks(e2e_t, "max", f"cuda:{device}")
     e2e_value = e2e_tri * world / (e2e_t / 1e3)
     nh = out["catsum"].size
     h2d = int(cat.xyz.nbytes + w.nbytes)
