@@ -69,6 +69,8 @@ SIGNATURES = {
     "gr_count_2pcf": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp]),
     "gr_count_3pcf": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp]),
     "gr_count_4pcf": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "gr_count_equi": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp]),
+    "gr_count_tetra": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gr_graph_build": (ctypes.c_int, [_ctx]),
     "gr_graph_nedges": (ctypes.c_int, [_ctx, _i64]),
     "gr_graph_export": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp]),

@@ -218,6 +218,31 @@ class Context:
         the weights (catalogue order)."""
         return self._adjoint(self._lib.gr_adjoint_3pcf, cot2, cot3, (ncfg3(self.nbins), self.nmu))
 
+    def count_equi(self):
+        """-equi: equilateral triangles per radial bin (and mu bin)."""
+        nb, nm = self.nbins, self.nmu
+        N2, N3 = np.zeros(nb * nm), np.zeros(nb * nm)
+        counts = np.zeros(nb * nm * 4, np.int64)
+        catsum = np.zeros(nb * nm * 4)
+        self._check(self._lib.gr_count_equi(self._h, _ptr(N2), _ptr(N3), _ptr(counts), _ptr(catsum)))
+        return dict(N2=_fortran(N2, nb, nm), N3=_fortran(N3, nb, nm),
+                    counts=_fortran(counts, nb, nm, 4), catsum=_fortran(catsum, nb, nm, 4))
+
+    def count_tetra(self):
+        """-tetra: regular tetrahedra per radial bin, with the six gated terms."""
+        nb = self.nbins
+        N2, N3 = np.zeros(nb), np.zeros(nb)
+        dN, dR = np.zeros(nb * 6), np.zeros(nb * 6)
+        counts = np.zeros(nb * 5, np.int64)
+        catsum = np.zeros(nb * 5)
+        dcount = np.zeros(nb * 30, np.int64)
+        dsum = np.zeros(nb * 30)
+        self._check(self._lib.gr_count_tetra(self._h, _ptr(N2), _ptr(N3), _ptr(dN), _ptr(dR),
+                                             _ptr(counts), _ptr(catsum), _ptr(dcount), _ptr(dsum)))
+        return dict(N2=N2, N3=N3, discN=_fortran(dN, nb, 6), discR=_fortran(dR, nb, 6),
+                    counts=_fortran(counts, nb, 5), catsum=_fortran(catsum, nb, 5),
+                    dcount=_fortran(dcount, nb, 6, 5), dsum=_fortran(dsum, nb, 6, 5))
+
     def graph(self):
         """The (rmin, rmax) neighbour graph in the reference's layout: rows in
         catalogue order, ids sorted, radial bin and mu bin per edge."""

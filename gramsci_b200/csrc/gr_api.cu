@@ -604,13 +604,13 @@ int gr_count_2pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
   GR_API_END(c)
 }
 
-int gr_count_3pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* catsum) {
+static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* counts, double* catsum) {
   GR_API_BEGIN(c)
   require_ready(c);
   ensure_events(c);
   cudaStream_t s = c->stream();
   const int nmu = c->nmu;
-  const int ncfg = (int)(((int64_t)c->nbins * (c->nbins + 1) * (c->nbins + 2)) / 6);
+  const int ncfg = equi ? c->nbins : (int)(((int64_t)c->nbins * (c->nbins + 1) * (c->nbins + 2)) / 6);
   const int nbin = ncfg * nmu, nh = nbin * 4;
   const bool weighted = !c->uniform;
   const double fscale = fix_scale(c->wmax * c->wmax * c->wmax);
@@ -637,6 +637,7 @@ int gr_count_3pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
   T.nmu = nmu;
   T.ncfg = ncfg;
   T.rsd = nmu >= 2;
+  T.equi = equi ? 1 : 0;
   T.cap = round_cap(c->csr.max_deg, 32, 256);
   T.normal = c->normal_dev.p;
   make_rank_tables(T.rank, c->nbins, 3);
@@ -666,7 +667,8 @@ int gr_count_3pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
   }
   for (int k = 0; k < nbin; ++k) {
     if (N2) N2[k] = ((hs[k] + hs[k + nbin]) + hs[k + 2 * nbin]) + hs[k + 3 * nbin];
-    if (N3) N3[k] = -hs[k + 3 * nbin];
+    // -equi with line-of-sight bins sums N2 only (gramsci.F90:425-428)
+    if (N3) N3[k] = (equi && nmu >= 2) ? 0.0 : -hs[k + 3 * nbin];
   }
   if (counts)
     for (int k = 0; k < nh; ++k) counts[k] = (int64_t)hc[k];
@@ -690,21 +692,30 @@ int gr_count_3pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
   GR_API_END(c)
 }
 
-int gr_count_4pcf(gr_ctx* c, double* N2, double* N3, double* discN, double* discR,
-                  int64_t* counts, double* catsum, int64_t* dcount, double* dsum) {
+int gr_count_3pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* catsum) {
+  return count_tri(c, false, N2, N3, counts, catsum);
+}
+
+int gr_count_equi(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* catsum) {
+  return count_tri(c, true, N2, N3, counts, catsum);
+}
+
+static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* discN, double* discR,
+                      int64_t* counts, double* catsum, int64_t* dcount, double* dsum) {
   GR_API_BEGIN(c)
   require_ready(c);
   ensure_events(c);
   cudaStream_t s = c->stream();
   const int nb = c->nbins;
   const int64_t ncfg64 = ((int64_t)nb * (nb + 1) * (nb + 2) * (nb + 3)) / 24;
-  const int64_t nbin64 = ncfg64 * nb * nb;
+  const int64_t nbin64 = tetra ? nb : ncfg64 * nb * nb;
   if (nbin64 * 29 > ((int64_t)1 << 31)) return set_err(c, GR_E_CAPACITY, "4PCF histogram too large");
   const int ncfg = (int)ncfg64, nbin = (int)nbin64;
-  const int nh = nbin * 5, nd = nbin * 24;
+  const int ndc = tetra ? 5 : 4;  // disc categories
+  const int nh = nbin * 5, nd = nbin * 6 * ndc;
   const bool weighted = !c->uniform;
   const double fscale = fix_scale(c->wmax * c->wmax * c->wmax * c->wmax);
-  const double dscale = fix_scale(c->wmax * c->wmax);
+  const double dscale = fix_scale(tetra ? c->wmax * c->wmax * c->wmax : c->wmax * c->wmax);
   c->hcnt.reserve(nh);
   c->hfix.reserve(2 * nh);
   c->dcnt.reserve(nd);
@@ -728,6 +739,7 @@ int gr_count_4pcf(gr_ctx* c, double* N2, double* N3, double* discN, double* disc
   QuadParams Q;
   Q.nbins = nb;
   Q.ncfg = ncfg;
+  Q.tetra = tetra ? 1 : 0;
   Q.cap = round_cap((int64_t)gst[2], 32, 1024);
   make_rank_tables(Q.rank, nb, 4);
   CSRView G{c->csr.row_ptr.p, c->csr.rec.p, c->csr.deg_full.p};
@@ -759,9 +771,12 @@ int gr_count_4pcf(gr_ctx* c, double* N2, double* N3, double* discN, double* disc
       double prod = uniform_product(c->w_gal, c->w_ran, 4 - nr, nr);
       for (int k = 0; k < nbin; ++k) hs[k + (size_t)nbin * nr] = (double)hc[k + (size_t)nbin * nr] * prod;
     }
-    for (int cat = 0; cat < 4; ++cat) {
-      int npr = cat == 3 ? 2 : cat;
-      double prod = uniform_product(c->w_gal, c->w_ran, 2 - npr, npr);
+    for (int cat = 0; cat < ndc; ++cat) {
+      // 4PCF pair terms: cat = randoms in the pair (3 = discR, both random);
+      // -tetra 3-products: cat = randoms in the product (4 = discR, all random)
+      const int q = tetra ? 3 : 2;
+      const int nrnd = tetra ? (cat == 4 ? 3 : cat) : (cat == 3 ? 2 : cat);
+      double prod = uniform_product(c->w_gal, c->w_ran, q - nrnd, nrnd);
       for (int k = 0; k < nbin * 6; ++k)
         ds[k + (size_t)nbin * 6 * cat] = (double)dc[k + (size_t)nbin * 6 * cat] * prod;
     }
@@ -773,8 +788,10 @@ int gr_count_4pcf(gr_ctx* c, double* N2, double* N3, double* discN, double* disc
     if (N3) N3[k] = hs[k + (size_t)nbin * 4];
   }
   for (int k = 0; k < nbin * 6; ++k) {
-    if (discN) discN[k] = (ds[k] + ds[k + (size_t)nbin * 6]) + ds[k + (size_t)nbin * 12];
-    if (discR) discR[k] = ds[k + (size_t)nbin * 18];
+    double acc = 0.0;
+    for (int cat = 0; cat < ndc - 1; ++cat) acc += ds[k + (size_t)nbin * 6 * cat];
+    if (discN) discN[k] = acc;
+    if (discR) discR[k] = ds[k + (size_t)nbin * 6 * (ndc - 1)];
   }
   if (counts)
     for (int k = 0; k < nh; ++k) counts[k] = (int64_t)hc[k];
@@ -800,6 +817,16 @@ int gr_count_4pcf(gr_ctx* c, double* N2, double* N3, double* discN, double* disc
   c->st.candidates = (int64_t)gst[1];
   c->st.kernel_launches = c->index.launches + c->csr.launches + 1;
   GR_API_END(c)
+}
+
+int gr_count_4pcf(gr_ctx* c, double* N2, double* N3, double* discN, double* discR,
+                  int64_t* counts, double* catsum, int64_t* dcount, double* dsum) {
+  return count_quad(c, false, N2, N3, discN, discR, counts, catsum, dcount, dsum);
+}
+
+int gr_count_tetra(gr_ctx* c, double* N2, double* N3, double* discN, double* discR,
+                   int64_t* counts, double* catsum, int64_t* dcount, double* dsum) {
+  return count_quad(c, true, N2, N3, discN, discR, counts, catsum, dcount, dsum);
 }
 
 int gr_graph_build(gr_ctx* c) {

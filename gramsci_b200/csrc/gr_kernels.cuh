@@ -26,6 +26,7 @@ void launch_pair2(const DevCatalog& C, const PairParams& P, bool weighted,
 
 struct TriParams {
   int nbins, nmu, ncfg, rsd;
+  int equi;                // -equi: only triangles with three equal bins, ncfg = nbins
   int cap;                 // per-warp shared row capacity (rows longer go the global path)
   const uint8_t* normal;   // device find_normal table [mu1-1 + nmu*(mu2-1)]
   RankTables rank;         // 3-tuple ranks
@@ -58,10 +59,13 @@ void launch_grad_finish(int n, const int* orig, const unsigned long long* g_lo,
 
 struct QuadParams {
   int nbins, ncfg;
+  int tetra;  // -tetra: only 4-cliques with six equal bins (histograms by bin)
   int cap;
   RankTables rank;  // 4-tuple ranks
 };
 
+// -tetra histograms (tetra = 1): g_cnt nbins*5, d_cnt nbins*30 (6 terms x 5
+// categories: 0..3 number of randoms in the 3-product, 4 = discR).
 // 4PCF: 4-cliques p < a < b < c enumerated once; each adds to the rooted
 // histograms of its non-buffer vertices whose perimeter is canonical.
 // g_cnt: nh = ncfg*nbins*nbins*5 (g_fix 2*nh); d_cnt: nd = ncfg*nbins*nbins*24 (d_fix 2*nd).

@@ -52,7 +52,7 @@ __device__ __forceinline__ int qlower_bound(const int* a, int n, int v) {
 
 struct QuadCtx {
   const int* F;  // 4 x (nbins+2)
-  int nbins, ncfg, nbin;
+  int nbins, ncfg, nbin, tetra;
   unsigned long long *cnt, *dcnt;
   unsigned long long *fix, *dfix;  // fixed-point (lo, hi) sums, hi at +5*nbin / +24*nbin
   double fscale;  // scale of the 4-point products
@@ -64,6 +64,73 @@ struct QuadCtx {
 __constant__ int kGate[6] = {3, 3, 1, 0, 0, 0};
 __constant__ int kPu[6] = {0, 0, 0, 1, 3, 3};
 __constant__ int kPv[6] = {1, 2, 3, 2, 2, 1};
+
+// -tetra terms (gramsci.F90:591-646): gate role, product roles, and the
+// pair that must also be random for discR; roles 0 = root, 1..3 = the
+// other vertices in catalogue-id order.
+__constant__ int kTGate[6] = {3, 3, 1, 0, 0, 0};
+__constant__ int kTPa[6] = {3, 3, 1, 0, 0, 0};
+__constant__ int kTPb[6] = {0, 0, 0, 1, 3, 3};
+__constant__ int kTPc[6] = {1, 2, 3, 2, 2, 1};
+
+// query_graph_tetrahedron: a 4-clique with all six edges in bin b counts from
+// each non-buffer vertex (no row-length condition).
+template <bool WEIGHTED>
+__device__ __forceinline__ int tetra_contrib(const DevCatalog& C, const QuadCtx& X, const int v[4],
+                                             const uint32_t m[6]) {
+  const int b = meta_bin(m[0]);
+#pragma unroll
+  for (int k = 1; k < 6; ++k)
+    if (meta_bin(m[k]) != b) return 0;
+  uint8_t fl[4];
+  int og[4];
+  double w[4];
+  bool rnd[4];
+  int nr = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    fl[k] = C.flags[v[k]];
+    og[k] = C.orig[v[k]];
+    w[k] = WEIGHTED ? C.w[v[k]] : 0.0;
+    rnd[k] = fl[k] & FLAG_RANDOM;
+    nr += rnd[k];
+  }
+  const int nb = X.nbins;
+  int n = 0;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    if (fl[r] & FLAG_BUFFER) continue;
+    int o[3], t = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (k != r) o[t++] = k;
+    int q;
+    if (og[o[0]] > og[o[1]]) { q = o[0]; o[0] = o[1]; o[1] = q; }
+    if (og[o[1]] > og[o[2]]) { q = o[1]; o[1] = o[2]; o[2] = q; }
+    if (og[o[0]] > og[o[1]]) { q = o[0]; o[0] = o[1]; o[1] = q; }
+    const int role[4] = {r, o[0], o[1], o[2]};
+    atomicAdd(&X.cnt[(b - 1) + nb * nr], 1ull);
+    if (WEIGHTED)
+      fix_add(&X.fix[(b - 1) + nb * nr], &X.fix[(b - 1) + nb * (nr + 5)],
+              ((w[r] * w[o[0]]) * w[o[1]]) * w[o[2]], X.fscale);
+#pragma unroll
+    for (int tt = 0; tt < 6; ++tt) {
+      if (!rnd[role[kTGate[tt]]]) continue;
+      const int ua = role[kTPa[tt]], ub = role[kTPb[tt]], uc = role[kTPc[tt]];
+      const int nr3 = (int)rnd[ua] + (int)rnd[ub] + (int)rnd[uc];
+      const int kt = (b - 1) + nb * tt;
+      const double qv = WEIGHTED ? (w[ua] * w[ub]) * w[uc] : 0.0;
+      atomicAdd(&X.dcnt[kt + nb * 6 * nr3], 1ull);
+      if (WEIGHTED) fix_add(&X.dfix[kt + nb * 6 * nr3], &X.dfix[kt + nb * 6 * (nr3 + 5)], qv, X.dscale);
+      if (rnd[ub] && rnd[uc]) {
+        atomicAdd(&X.dcnt[kt + nb * 24], 1ull);
+        if (WEIGHTED) fix_add(&X.dfix[kt + nb * 24], &X.dfix[kt + nb * 54], qv, X.dscale);
+      }
+    }
+    n++;
+  }
+  return n;
+}
 
 template <bool WEIGHTED>
 __device__ __forceinline__ int quad_contrib(const DevCatalog& C, const CSRView& G, const QuadCtx& X,
@@ -154,6 +221,7 @@ __global__ void __launch_bounds__(kQuadThreads) quad4_kernel(DevCatalog C, CSRVi
   X.nbins = Q.nbins;
   X.ncfg = Q.ncfg;
   X.nbin = Q.ncfg * Q.nbins * Q.nbins;
+  X.tetra = Q.tetra;
   X.cnt = g_cnt;
   X.fix = g_fix;
   X.dcnt = d_cnt;
@@ -265,7 +333,8 @@ __global__ void __launch_bounds__(kQuadThreads) quad4_kernel(DevCatalog C, CSRVi
           const int v[4] = {p, a, x_c[z], d};
           const uint32_t m[6] = {r_meta[x], r_meta[x_y[z]], r_meta[x_y[z2]],
                                  x_m[z],    x_m[z2],        rec_meta(rr)};
-          int nroot = quad_contrib<WEIGHTED>(C, G, X, v, m);
+          int nroot = X.tetra ? tetra_contrib<WEIGHTED>(C, X, v, m)
+                              : quad_contrib<WEIGHTED>(C, G, X, v, m);
           quads += nroot > 0;
           rooted += nroot;
         }

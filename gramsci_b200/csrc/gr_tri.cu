@@ -86,7 +86,7 @@ struct TriCtx {
   const uint8_t* norm;
   const int* F;  // 3 x (nbins+2)
   const uint16_t* cfgtab;  // symmetric configuration table or NULL
-  int nbins, nmu, ncfg, rsd, nh;
+  int nbins, nmu, ncfg, rsd, nh, equi;
   unsigned long long* cnt;
   unsigned long long* lo;  // fixed-point sums: lo[k], lo[nh + k] = hi[k]
   double fscale;
@@ -119,7 +119,14 @@ template <bool WEIGHTED>
 __device__ __forceinline__ int tri_bin(const TriCtx& X, uint8_t fp, int op, double wp, uint8_t fa,
                                        int oa, double wa, uint8_t fc, int oc, double wc,
                                        uint32_t mpa, uint32_t mpc, uint32_t mac) {
-  const int cfg = tri_cfg(X, meta_bin(mpa), meta_bin(mpc), meta_bin(mac));
+  int cfg;
+  if (X.equi) {  // query_graph_equilateral_triangle: three equal bins
+    const int b1 = meta_bin(mpa);
+    if (meta_bin(mpc) != b1 || meta_bin(mac) != b1) return 0;
+    cfg = b1;
+  } else {
+    cfg = tri_cfg(X, meta_bin(mpa), meta_bin(mpc), meta_bin(mac));
+  }
   const int nr = (fp & FLAG_RANDOM) + (fa & FLAG_RANDOM) + (fc & FLAG_RANDOM);
   int m[3] = {-1, -1, -1};
   double pr[3] = {0.0, 0.0, 0.0};
@@ -235,6 +242,7 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
   X.nmu = T.nmu;
   X.ncfg = T.ncfg;
   X.rsd = T.rsd;
+  X.equi = T.equi;
   X.nh = nh;
   X.fscale = fscale;
   X.cnt = SHIST ? reinterpret_cast<unsigned long long*>(smem + L.off_cnt) : g_cnt;

@@ -459,4 +459,39 @@ int grh_write_4pcf(const char* path, const double* edges, int32_t nbins, const d
   return std::fclose(f) == 0 ? 0 : -1;
 }
 
+int grh_write_equi(const char* path, const double* edges, int32_t nbins, int32_t nmu,
+                   const double* N2, const double* N3) {
+  // query_graph_equilateral_triangle writer, src/gramsci.F90:451-459
+  FILE* f = std::fopen(path, "w");
+  if (!f) return -1;
+  const double mu_scale = (double)(0.5f * (float)nmu);
+  for (int l = 1; l <= nbins; ++l)
+    for (int k = 1; k <= nmu; ++k) {
+      const int idx = (l - 1) + nbins * (k - 1);
+      const double v[7] = {edges[l - 1], edges[l], (double)((float)k - 1.0f) / mu_scale / 2.0,
+                           (double)(float)k / mu_scale / 2.0, N2[idx], N3[idx], N2[idx] / N3[idx]};
+      write_record(f, v, 7);
+    }
+  return std::fclose(f) == 0 ? 0 : -1;
+}
+
+int grh_write_tetra(const char* path, const double* edges, int32_t nbins, int32_t nmu,
+                    const double* N2, const double* N3, const double* discN, const double* discR) {
+  // query_graph_tetrahedron writer, src/gramsci.F90:648-660: N2(l,k,3) holds
+  // the counts at k = 1 only; the disconnected combination uses (l,1,1,t)
+  FILE* f = std::fopen(path, "w");
+  if (!f) return -1;
+  const double mu_scale = (double)(0.5f * (float)nmu);
+  for (int l = 1; l <= nbins; ++l)
+    for (int k = 1; k <= nmu; ++k) {
+      const double n2 = k == 1 ? N2[l - 1] : 0.0, n3 = k == 1 ? N3[l - 1] : 0.0;
+      auto r = [&](int t) { return discN[(l - 1) + nbins * (t - 1)] / discR[(l - 1) + nbins * (t - 1)]; };
+      const double v[8] = {edges[l - 1], edges[l], (double)((float)k - 1.0f) / mu_scale / 2.0,
+                           (double)(float)k / mu_scale / 2.0, n2, n3, n2 / n3,
+                           r(1) * r(5) + r(3) * r(4) + r(2) * r(6)};
+      write_record(f, v, 8);
+    }
+  return std::fclose(f) == 0 ? 0 : -1;
+}
+
 }  // extern "C"

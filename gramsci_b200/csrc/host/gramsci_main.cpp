@@ -3,7 +3,7 @@
 // on the GPU through libgramsci_cuda.so.
 //
 //   gramsci -gal G [-ran R] -rmin a -rmax b -nbins n [-nmu m] [-log]
-//           [-out F] [-cut region.loadnodes] -2pcf | -3pcf | -4pcf
+//           [-out F] [-cut region.loadnodes] -2pcf | -3pcf | -4pcf | -equi | -tetra
 //
 // Exit status follows the reference: 0 after help, after an unknown option
 // (the reference prints a message and stops) and after a run; 2 for an
@@ -24,13 +24,14 @@ void print_help() {
   std::puts(" ");
   std::puts(" usage: gramsci -gal galaxy_file [-ran random_file] -rmin Rmin -rmax Rmax");
   std::puts("                -nbins Nbins [-nmu Nmu] [-log] [-out out_file]");
-  std::puts("                [-cut region_file] -2pcf | -3pcf | -4pcf");
+  std::puts("                [-cut region_file] -2pcf | -3pcf | -4pcf | -equi | -tetra");
   std::puts(" ");
   std::puts("   galaxy_file, random_file  records of x y z w");
   std::puts("   Rmin, Rmax                range of separations counted");
   std::puts("   Nbins                     radial bins (linear; -log for log10 spacing)");
   std::puts("   Nmu                       line-of-sight bins in -1 < mu < 1 (>= 2 turns them on)");
   std::puts("   out_file                  result table (default result.txt)");
+  std::puts("   -equi, -tetra             equilateral triangles / regular tetrahedra only");
 }
 
 int fail(gr_ctx* ctx, const char* what, int rc) {
@@ -54,10 +55,6 @@ int main(int argc, char** argv) {
   if (o.help) {
     print_help();
     return 0;
-  }
-  if (o.equi || o.tetra) {
-    std::fprintf(stderr, "gramsci: -equi and -tetra are not available in this build\n");
-    return 1;
   }
   if (o.nbins < 1 || o.nbins > 127 || o.nmu < 1 || o.nmu > 127) {
     std::fprintf(stderr, "gramsci: need 1 <= nbins <= 127 and 1 <= nmu <= 127\n");
@@ -118,6 +115,15 @@ int main(int argc, char** argv) {
       return fail(nullptr, "writing the output", -1);
     std::printf(" 3PCF: %lld triangles, %.3f ms on the GPU\n", (long long)st.tuples, st.ms_total);
   }
+  if (o.equi) {
+    std::vector<double> N2((size_t)nb * nm), N3((size_t)nb * nm);
+    if ((rc = gr_count_equi(ctx, N2.data(), N3.data(), nullptr, nullptr)))
+      return fail(ctx, "gr_count_equi", rc);
+    gr_get_stats(ctx, &st);
+    if (grh_write_equi(o.out, edges.data(), nb, nm, N2.data(), N3.data()))
+      return fail(nullptr, "writing the output", -1);
+    std::printf(" -equi: %lld triangles, %.3f ms on the GPU\n", (long long)st.tuples, st.ms_total);
+  }
   if (o.four_pcf) {
     const size_t nc = (size_t)nb * (nb + 1) * (nb + 2) * (nb + 3) / 24;
     const size_t nbin = nc * nb * nb;
@@ -129,6 +135,16 @@ int main(int argc, char** argv) {
     if (grh_write_4pcf(o.out, edges.data(), nb, N2.data(), N3.data(), dN.data(), dR.data()))
       return fail(nullptr, "writing the output", -1);
     std::printf(" 4PCF: %lld 4-cliques, %.3f ms on the GPU\n", (long long)st.tuples, st.ms_total);
+  }
+  if (o.tetra) {
+    std::vector<double> N2(nb), N3(nb), dN((size_t)nb * 6), dR((size_t)nb * 6);
+    if ((rc = gr_count_tetra(ctx, N2.data(), N3.data(), dN.data(), dR.data(), nullptr, nullptr,
+                             nullptr, nullptr)))
+      return fail(ctx, "gr_count_tetra", rc);
+    gr_get_stats(ctx, &st);
+    if (grh_write_tetra(o.out, edges.data(), nb, nm, N2.data(), N3.data(), dN.data(), dR.data()))
+      return fail(nullptr, "writing the output", -1);
+    std::printf(" -tetra: %lld 4-cliques, %.3f ms on the GPU\n", (long long)st.tuples, st.ms_total);
   }
   gr_destroy(ctx);
   grh_free(xyz);

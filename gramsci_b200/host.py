@@ -48,6 +48,9 @@ def load():
         for name in ("grh_write_2pcf", "grh_write_3pcf"):
             getattr(L, name).argtypes = [ctypes.c_char_p, _d, ctypes.c_int32, ctypes.c_int32, _d, _d]
         L.grh_write_4pcf.argtypes = [ctypes.c_char_p, _d, ctypes.c_int32, _d, _d, _d, _d]
+        L.grh_write_equi.argtypes = [ctypes.c_char_p, _d, ctypes.c_int32, ctypes.c_int32, _d, _d]
+        L.grh_write_tetra.argtypes = [ctypes.c_char_p, _d, ctypes.c_int32, ctypes.c_int32, _d, _d,
+                                      _d, _d]
         _lib = L
     return _lib
 
@@ -108,3 +111,16 @@ def write_4pcf(path, edges, nbins, N2, N3, discN, discR):
     e, a, b, c, d = _flat(edges), _flat(N2), _flat(N3), _flat(discN), _flat(discR)
     return load().grh_write_4pcf(path.encode(), e.ctypes.data_as(_d), nbins, a.ctypes.data_as(_d),
                                  b.ctypes.data_as(_d), c.ctypes.data_as(_d), d.ctypes.data_as(_d))
+
+
+def write_equi(path, edges, nbins, nmu, N2, N3):
+    e, a, b = _flat(edges), _flat(N2), _flat(N3)
+    return load().grh_write_equi(path.encode(), e.ctypes.data_as(_d), nbins, nmu,
+                                 a.ctypes.data_as(_d), b.ctypes.data_as(_d))
+
+
+def write_tetra(path, edges, nbins, nmu, N2, N3, discN, discR):
+    e, a, b, c, d = _flat(edges), _flat(N2), _flat(N3), _flat(discN), _flat(discR)
+    return load().grh_write_tetra(path.encode(), e.ctypes.data_as(_d), nbins, nmu,
+                                  a.ctypes.data_as(_d), b.ctypes.data_as(_d), c.ctypes.data_as(_d),
+                                  d.ctypes.data_as(_d))

@@ -126,6 +126,23 @@ int gr_count_3pcf(gr_ctx* ctx, double* N2, double* N3, int64_t* counts, double* 
 int gr_count_4pcf(gr_ctx* ctx, double* N2, double* N3, double* discN, double* discR,
                   int64_t* counts, double* catsum, int64_t* dcount, double* dsum);
 
+/* -equi: equilateral triangles (all three edges in the same radial bin).
+ * Replaces query_graph_equilateral_triangle (src/gramsci.F90:402-448):
+ *   N2, N3  (nbins, nmu)     N3 = minus the all-random sum without mu bins,
+ *                            0 with mu bins (the reference sums only N2 then)
+ *   counts, catsum (nbins, nmu, 4) by number of randoms */
+int gr_count_equi(gr_ctx* ctx, double* N2, double* N3, int64_t* counts, double* catsum);
+
+/* -tetra: regular tetrahedra (all six edges of a 4-clique in the same radial
+ * bin).  Replaces query_graph_tetrahedron (src/gramsci.F90:548-646):
+ *   N2, N3        (nbins)      sums of the 4-products (N3: all random)
+ *   discN, discR  (nbins, 6)   the six gated 3-product terms
+ *   counts, catsum (nbins, 5)  by number of randoms
+ *   dcount, dsum  (nbins, 6, 5) disc terms: 0..3 = discN by randoms in the
+ *                 product, 4 = discR */
+int gr_count_tetra(gr_ctx* ctx, double* N2, double* N3, double* discN, double* discR,
+                   int64_t* counts, double* catsum, int64_t* dcount, double* dsum);
+
 /* Graph access (parity tests, graph reuse).  Builds the (rmin, rmax) graph
  * of create_graph (src/gramsci.F90:288-348) if needed.  Export gives the
  * reference's layout: rows in point order, each row sorted by id (as

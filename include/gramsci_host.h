@@ -65,6 +65,11 @@ int grh_write_3pcf(const char* path, const double* edges, int32_t nbins, int32_t
                    const double* N2, const double* N3);
 int grh_write_4pcf(const char* path, const double* edges, int32_t nbins, const double* N2,
                    const double* N3, const double* discN, const double* discR);
+/* -equi (:451-459) and -tetra (:648-660) tables; no header line. */
+int grh_write_equi(const char* path, const double* edges, int32_t nbins, int32_t nmu,
+                   const double* N2, const double* N3);
+int grh_write_tetra(const char* path, const double* edges, int32_t nbins, int32_t nmu,
+                    const double* N2, const double* N3, const double* discN, const double* discR);
 
 #ifdef __cplusplus
 }

@@ -928,6 +928,145 @@ void orc_4pcf(const orc_graph* h, const double* w, const int32_t* buffer, int64_
   }
 }
 
+// ------------------------------------------------------- -equi and -tetra --
+// query_graph_equilateral_triangle (gramsci.F90:402-448): triangles whose
+// three edges share one radial bin b, from every non-buffer root.  With RSD
+// the mu bin is find_normal of the root's two edges and only N2 is summed;
+// without RSD N3 accumulates minus the all-random products.
+// Outputs (Fortran order): N2, N3 (nbins, nmu); counts, catsum (nbins, nmu, 4)
+// by number of randoms.
+void orc_equi(const orc_graph* h, const double* w, const int32_t* buffer, int64_t n_data,
+              const int32_t* normal_table, double* N2, double* N3, int64_t* counts,
+              double* catsum) {
+  const Graph& G = *reinterpret_cast<const Graph*>(h);
+  const int nb = G.B.nbins, nm = G.B.nmu;
+  const int nbin = nb * nm;
+  std::vector<double> n2(nbin, 0.0), n3(nbin, 0.0);
+  std::vector<int64_t> cnt(nbin * 4, 0);
+  std::vector<acc_t> cs(nbin * 4, 0.0L);
+  for (int64_t i = 0; i < G.n; ++i) {
+    if (buffer && buffer[i] == 1) continue;
+    const bool ri = i >= n_data;
+    const int64_t r0 = G.row_ptr[i], r1 = G.row_ptr[i + 1];
+    for (int64_t k1 = r0; k1 < r1; ++k1) {
+      const int ind1 = G.bin[k1];
+      const int32_t id1 = G.col[k1];
+      for (int64_t k2 = k1 + 1; k2 < r1; ++k2) {
+        if (G.bin[k2] != ind1) continue;
+        const int32_t id2 = G.col[k2];
+        if (find_dist(G, id1, id2) != ind1) continue;
+        const double p = w[i] * w[id1] * w[id2];
+        const bool allr = ri && id1 >= n_data && id2 >= n_data;
+        int m = 1;
+        if (G.B.rsd) {
+          m = normal_table[(G.mu[k1] - 1) + nm * (G.mu[k2] - 1)];
+        } else if (allr) {
+          n3[ind1 - 1] = n3[ind1 - 1] - p;
+        }
+        const int k = (ind1 - 1) + nb * (m - 1);
+        n2[k] = n2[k] + p;
+        const int nr = (int)ri + (int)(id1 >= n_data) + (int)(id2 >= n_data);
+        cnt[k + nbin * nr] += 1;
+        cs[k + nbin * nr] += (acc_t)p;
+      }
+    }
+  }
+  for (int k = 0; k < nbin; ++k) {
+    if (N2) N2[k] = n2[k];
+    if (N3) N3[k] = n3[k];
+  }
+  for (int k = 0; k < nbin * 4; ++k) {
+    if (counts) counts[k] = cnt[k];
+    if (catsum) catsum[k] = (double)cs[k];
+  }
+}
+
+// query_graph_tetrahedron (gramsci.F90:548-660): 4-cliques whose six edges
+// share one radial bin b, from every non-buffer root (no row-length
+// condition), a < b < c in id order.  N2(b) / N3(b) sum the 4-products; the
+// six disconnected terms are 3-products gated on one vertex being a random:
+//   t  gate  product        discR also needs
+//   1  c     w_c w_i w_a    i, a random
+//   2  c     w_c w_i w_b    i, b random
+//   3  a     w_a w_i w_c    i, c random
+//   4  i     w_i w_a w_b    a, b random
+//   5  i     w_i w_c w_b    c, b random
+//   6  i     w_i w_c w_a    c, a random
+// Outputs (Fortran order): N2, N3 (nbins); discN, discR (nbins, 6);
+// counts, catsum (nbins, 5) by number of randoms; dcount, dsum (nbins, 6, 5):
+// categories 0..3 = discN by number of randoms in the product, 4 = discR.
+void orc_tetra(const orc_graph* h, const double* w, const int32_t* buffer, int64_t n_data,
+               double* N2, double* N3, double* discN, double* discR, int64_t* counts,
+               double* catsum, int64_t* dcount, double* dsum) {
+  const Graph& G = *reinterpret_cast<const Graph*>(h);
+  const int nb = G.B.nbins;
+  std::vector<double> n2(nb, 0.0), n3(nb, 0.0), dn(nb * 6, 0.0), dr(nb * 6, 0.0);
+  std::vector<int64_t> cnt(nb * 5, 0), dcnt(nb * 30, 0);
+  std::vector<acc_t> cs(nb * 5, 0.0L), dcs(nb * 30, 0.0L);
+  static const int gate[6] = {3, 3, 1, 0, 0, 0};
+  static const int pa[6] = {3, 3, 1, 0, 0, 0};
+  static const int pb[6] = {0, 0, 0, 1, 3, 3};
+  static const int pc[6] = {1, 2, 3, 2, 2, 1};
+  for (int64_t i = 0; i < G.n; ++i) {
+    if (buffer && buffer[i] == 1) continue;
+    const int64_t r0 = G.row_ptr[i], r1 = G.row_ptr[i + 1];
+    for (int64_t k1 = r0; k1 < r1; ++k1) {
+      const int ind1 = G.bin[k1];
+      const int32_t id1 = G.col[k1];
+      for (int64_t k2 = k1 + 1; k2 < r1; ++k2) {
+        const int32_t id2 = G.col[k2];
+        if (G.bin[k2] != ind1) continue;
+        if (find_dist(G, id1, id2) != ind1) continue;
+        for (int64_t k3 = k2 + 1; k3 < r1; ++k3) {
+          if (G.bin[k3] != ind1) continue;
+          const int32_t id3 = G.col[k3];
+          if (find_dist(G, id2, id3) != ind1) continue;
+          if (find_dist(G, id1, id3) != ind1) continue;
+          const int64_t v[4] = {i, id1, id2, id3};
+          const bool r[4] = {i >= n_data, id1 >= n_data, id2 >= n_data, id3 >= n_data};
+          const int b = ind1 - 1;
+          for (int t = 0; t < 6; ++t) {
+            if (!r[gate[t]]) continue;
+            const double q = w[v[pa[t]]] * w[v[pb[t]]] * w[v[pc[t]]];
+            const int kt = b + nb * t;
+            dn[kt] = dn[kt] + q;
+            const int nr3 = (int)r[pa[t]] + (int)r[pb[t]] + (int)r[pc[t]];
+            dcnt[kt + nb * 6 * nr3] += 1;
+            dcs[kt + nb * 6 * nr3] += (acc_t)q;
+            if (r[pb[t]] && r[pc[t]]) {
+              dr[kt] = dr[kt] + q;
+              dcnt[kt + nb * 6 * 4] += 1;
+              dcs[kt + nb * 6 * 4] += (acc_t)q;
+            }
+          }
+          const double p = w[i] * w[id1] * w[id2] * w[id3];
+          n2[b] = n2[b] + p;
+          if (r[0] && r[1] && r[2] && r[3]) n3[b] = n3[b] + p;
+          const int nr = (int)r[0] + (int)r[1] + (int)r[2] + (int)r[3];
+          cnt[b + nb * nr] += 1;
+          cs[b + nb * nr] += (acc_t)p;
+        }
+      }
+    }
+  }
+  for (int k = 0; k < nb; ++k) {
+    if (N2) N2[k] = n2[k];
+    if (N3) N3[k] = n3[k];
+  }
+  for (int k = 0; k < nb * 6; ++k) {
+    if (discN) discN[k] = dn[k];
+    if (discR) discR[k] = dr[k];
+  }
+  for (int k = 0; k < nb * 5; ++k) {
+    if (counts) counts[k] = cnt[k];
+    if (catsum) catsum[k] = (double)cs[k];
+  }
+  for (int k = 0; k < nb * 30; ++k) {
+    if (dcount) dcount[k] = dcnt[k];
+    if (dsum) dsum[k] = (double)dcs[k];
+  }
+}
+
 // --------------------------------------------------------------- adjoints --
 // Gradient of L = sum(cot2 * N2) + sum(cot3 * N3) with respect to the signed
 // normalised weights, for the 2PCF of orc_2pcf.  dN2_b/dw_k = sum of w_j over

@@ -56,6 +56,9 @@ def lib():
         L.orc_3pcf.argtypes = [ctypes.c_void_p, _d, _i32, ctypes.c_int64, _i32, _d, _d, _i64, _d]
         L.orc_4pcf.argtypes = [ctypes.c_void_p, _d, _i32, ctypes.c_int64, _d, _d, _d, _d, _i64,
                                _d, _i64, _d]
+        L.orc_equi.argtypes = [ctypes.c_void_p, _d, _i32, ctypes.c_int64, _i32, _d, _d, _i64, _d]
+        L.orc_tetra.argtypes = [ctypes.c_void_p, _d, _i32, ctypes.c_int64, _d, _d, _d, _d, _i64, _d,
+                                _i64, _d]
         L.orc_adjoint_2pcf.argtypes = [ctypes.c_void_p, _d, _i32, ctypes.c_int64, _d, _d, _d]
         L.orc_adjoint_3pcf.argtypes = [ctypes.c_void_p, _d, _i32, ctypes.c_int64, _i32, _d, _d, _d]
         L.orc_max_threads.restype = ctypes.c_int32
@@ -160,6 +163,38 @@ class Graph:
                     discR=f(dR, nc, nb, nb, 6), counts=f(counts, nc, nb, nb, 5),
                     catsum=f(catsum, nc, nb, nb, 5), dcount=f(dcount, nc, nb, nb, 6, 4),
                     dsum=f(dsum, nc, nb, nb, 6, 4))
+
+    def equi(self, w, n_data, buffer=None, normal_variant=0):
+        w = np.ascontiguousarray(w, np.float64)
+        buf = None if buffer is None else np.ascontiguousarray(buffer, np.int32)
+        nb, nm = self.nbins, self.nmu
+        tab = normal_table(nm, normal_variant)
+        N2, N3 = np.zeros(nb * nm), np.zeros(nb * nm)
+        counts = np.zeros(nb * nm * 4, np.int64)
+        catsum = np.zeros(nb * nm * 4)
+        lib().orc_equi(self._h, _p(w, _d), _p(buf, _i32), int(n_data),
+                       _p(np.ascontiguousarray(tab.T.ravel()), _i32), _p(N2, _d), _p(N3, _d),
+                       _p(counts, _i64), _p(catsum, _d))
+        f = lambda a, *s: a.reshape(s[::-1]).transpose()
+        return dict(N2=f(N2, nb, nm), N3=f(N3, nb, nm), counts=f(counts, nb, nm, 4),
+                    catsum=f(catsum, nb, nm, 4))
+
+    def tetra(self, w, n_data, buffer=None):
+        w = np.ascontiguousarray(w, np.float64)
+        buf = None if buffer is None else np.ascontiguousarray(buffer, np.int32)
+        nb = self.nbins
+        N2, N3 = np.zeros(nb), np.zeros(nb)
+        dN, dR = np.zeros(nb * 6), np.zeros(nb * 6)
+        counts = np.zeros(nb * 5, np.int64)
+        catsum = np.zeros(nb * 5)
+        dcount = np.zeros(nb * 30, np.int64)
+        dsum = np.zeros(nb * 30)
+        lib().orc_tetra(self._h, _p(w, _d), _p(buf, _i32), int(n_data), _p(N2, _d), _p(N3, _d),
+                        _p(dN, _d), _p(dR, _d), _p(counts, _i64), _p(catsum, _d), _p(dcount, _i64),
+                        _p(dsum, _d))
+        f = lambda a, *s: a.reshape(s[::-1]).transpose()
+        return dict(N2=N2, N3=N3, discN=f(dN, nb, 6), discR=f(dR, nb, 6), counts=f(counts, nb, 5),
+                    catsum=f(catsum, nb, 5), dcount=f(dcount, nb, 6, 5), dsum=f(dsum, nb, 6, 5))
 
     def adjoint2(self, w, n_data, cot2, cot3=None, buffer=None):
         w = np.ascontiguousarray(w, np.float64)

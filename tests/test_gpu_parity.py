@@ -156,3 +156,55 @@ def test_pair_sweep_variants_agree(gpu_ctx, oracle, name, scale, nmu, weighted):
             _check_sums(gpu_ctx.count_2pcf(), ref)
     finally:
         gpu_ctx.set_autotune("on")
+
+
+@pytest.mark.parametrize("nmu", [1, 3])
+def test_equi(gpu_ctx, oracle, nmu):
+    cat, w, sp = _cat("c2_3pcf", 0.02)
+    gpu_ctx.set_catalog(cat.xyz, w, cat.n_data)
+    gpu_ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], nmu)
+    got = gpu_ctx.count_equi()
+    ref = oracle.Graph(cat.xyz, sp["rmin"], sp["rmax"], sp["nbins"], nmu).equi(w, cat.n_data)
+    assert ref["counts"].sum() > 0
+    _check_sums(got, ref)
+    assert np.all(np.abs(got["N3"] - ref["N3"]) <= RTOL * np.abs(ref["N3"]) + 1e-300)
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_tetra(gpu_ctx, oracle, weighted):
+    cat, w, sp = _cat("c3_4pcf", 0.1)
+    if weighted:
+        w = catalogs.normalise(np.random.default_rng(4).lognormal(0, 0.3, cat.n), cat.n_data,
+                               cat.n_rand)
+    buf = (np.random.default_rng(6).random(cat.n) < 0.1).astype(np.int32)
+    gpu_ctx.set_catalog(cat.xyz, w, cat.n_data, buffer=buf)
+    gpu_ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], 1)
+    got = gpu_ctx.count_tetra()
+    ref = oracle.Graph(cat.xyz, sp["rmin"], sp["rmax"], sp["nbins"], 1).tetra(w, cat.n_data, buffer=buf)
+    assert ref["counts"].sum() > 0
+    assert np.array_equal(got["counts"], ref["counts"])
+    assert np.array_equal(got["dcount"], ref["dcount"])
+    assert _rel(got["catsum"], ref["catsum"]) < RTOL
+    assert _rel(got["dsum"], ref["dsum"]) < RTOL
+
+
+@pytest.mark.parametrize("query", ["graph", "2pcf", "3pcf"])
+def test_log_bins(gpu_ctx, oracle, query):
+    """-log bins: the library's FP64 path (log10 on the device, glibc's on
+    the oracle side).  Both are within an ulp, so a bin could differ only for
+    a separation within ~1e-15 relative of a bin edge; at these sizes the
+    expected number of such edges is far below one, and the test is exact."""
+    cat, w, sp = _cat("c2_3pcf", 0.01)
+    rmin = 0.1 * sp["rmax"]
+    gpu_ctx.set_catalog(cat.xyz, w, cat.n_data)
+    gpu_ctx.set_bins(rmin, sp["rmax"], sp["nbins"], sp["nmu"], logbins=True)
+    G = oracle.Graph(cat.xyz, rmin, sp["rmax"], sp["nbins"], sp["nmu"], logbins=True)
+    if query == "graph":
+        got, ref = gpu_ctx.graph(), G.csr()
+        for a, b in zip(got, ref):
+            assert np.array_equal(a, b)
+        assert len(np.unique(got[2])) == sp["nbins"]
+    elif query == "2pcf":
+        _check_sums(gpu_ctx.count_2pcf(), G.pcf2(w, cat.n_data))
+    else:
+        _check_sums(gpu_ctx.count_3pcf(), G.pcf3(w, cat.n_data))

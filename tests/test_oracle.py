@@ -274,3 +274,36 @@ def test_adjoint_3pcf_matches_finite_differences(oracle):
         wm[k] -= h
         fd = (L(wp) - L(wm)) / (2 * h)
         assert abs(fd - g[k]) <= 1e-7 * max(abs(fd), abs(g[k]), 1e-30)
+
+
+def test_equi_and_tetra_match_brute_force(oracle):
+    """-equi / -tetra (gramsci.F90:402-660): same-bin triangles and 4-cliques,
+    against an independent enumeration."""
+    xyz, w, nd = small_catalogue(30, 30, 30.0, 6)
+    nb, nm = 3, 2
+    E = brute_edges(xyz, 1.0, 12.0, nb, nm)
+    n = len(xyz)
+    nbrs = {i: sorted(j for (a, j) in E if a == i) for i in range(n)}
+    normal = oracle.normal_table(nm)
+    ce = np.zeros((nb, nm, 4), np.int64)
+    ct = np.zeros((nb, 5), np.int64)
+    for i in range(n):
+        for a, c in itertools.combinations(nbrs[i], 2):
+            b = E[(i, a)][0]
+            if E[(i, c)][0] != b or E.get((a, c), (0,))[0] != b:
+                continue
+            m = normal[E[(i, a)][1] - 1, E[(i, c)][1] - 1]
+            ce[b - 1, m - 1, (i >= nd) + (a >= nd) + (c >= nd)] += 1
+        for a, b2, c in itertools.combinations(nbrs[i], 3):
+            b = E[(i, a)][0]
+            ok = all(E.get(e, (0,))[0] == b for e in [(i, b2), (i, c), (a, b2), (b2, c), (a, c)])
+            if ok:
+                ct[b - 1, sum(x >= nd for x in (i, a, b2, c))] += 1
+    G = oracle.Graph(xyz, 1.0, 12.0, nb, nm)
+    e = G.equi(w, nd)
+    t = G.tetra(w, nd)
+    assert ce.sum() > 0 and ct.sum() > 0
+    assert np.array_equal(e["counts"], ce)
+    assert np.array_equal(t["counts"], ct)
+    # with RSD the reference sums only N2 for -equi
+    assert np.all(e["N3"] == 0)
