@@ -72,6 +72,8 @@ SIGNATURES = {
     "gr_count_equi": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp]),
     "gr_count_tetra": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "gr_graph_build": (ctypes.c_int, [_ctx]),
+    "gr_graph_save": (ctypes.c_int, [_ctx, ctypes.c_char_p]),
+    "gr_graph_load": (ctypes.c_int, [_ctx, ctypes.c_char_p]),
     "gr_graph_nedges": (ctypes.c_int, [_ctx, _i64]),
     "gr_graph_export": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp]),
     "gr_get_stats": (ctypes.c_int, [_ctx, ctypes.POINTER(GrStats)]),

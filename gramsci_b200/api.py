@@ -218,6 +218,19 @@ class Context:
         the weights (catalogue order)."""
         return self._adjoint(self._lib.gr_adjoint_3pcf, cot2, cot3, (ncfg3(self.nbins), self.nmu))
 
+    def set_keep_graph(self, on):
+        """Reuse the last call's graph until the catalogue, bins or precision change."""
+        self._check(self._lib.gr_set_option(self._h, 4, int(bool(on))))
+
+    def graph_save(self, path):
+        """Write the neighbour graph of the current catalogue and bins to `path`."""
+        self._check(self._lib.gr_graph_save(self._h, str(path).encode()))
+
+    def graph_load(self, path):
+        """Load a graph written by graph_save for the same catalogue and bins;
+        later count calls reuse it."""
+        self._check(self._lib.gr_graph_load(self._h, str(path).encode()))
+
     def count_equi(self):
         """-equi: equilateral triangles per radial bin (and mu bin)."""
         nb, nm = self.nbins, self.nmu

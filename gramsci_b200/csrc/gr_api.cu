@@ -45,6 +45,8 @@ struct gr_ctx {
   CellIndex index;
   UpperCSR csr;
   bool csr_valid = false;
+  bool keep_graph = false;    // GR_OPT_KEEP_GRAPH
+  bool graph_loaded = false;  // graph read by gr_graph_load
   PairParams P{};
   DevBuf<uint8_t> normal_dev;
   DevBuf<unsigned long long> hcnt, dcnt, stats;
@@ -289,6 +291,36 @@ __global__ void uniform_check_kernel(const double* __restrict__ w, int64_t n_dat
   if ((threadIdx.x & 31) == 0 && m) atomicMax(wmax, m);
 }
 
+unsigned long long mix_host(unsigned long long z) {
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+// 64-bit fingerprint of the coordinates in catalogue order: a wrapping sum
+// of a mixed hash of (index, x, y, z), so the order of the additions does
+// not matter.
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  // splitmix64 finaliser
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+__global__ void fingerprint_kernel(const double* __restrict__ xyz, int64_t n,
+                                   unsigned long long* out) {
+  unsigned long long acc = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    unsigned long long h = mix64((unsigned long long)i + 0x9e3779b97f4a7c15ull);
+    for (int c = 0; c < 3; ++c)
+      h = mix64(h ^ (unsigned long long)__double_as_longlong(xyz[3 * i + c]));
+    acc += h;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+
 void require_ready(gr_ctx* c) {
   if (!c->cat_set) throw gr::Error{GR_E_ARG, "catalogue not set (gr_set_catalog)"};
   if (!c->bins_set) throw gr::Error{GR_E_ARG, "bins not set (gr_set_bins)"};
@@ -318,6 +350,10 @@ void build_csr(gr_ctx* c) {
   c->csr.build(c->index.view(), c->P, c->stream());
   c->csr_valid = true;
 }
+
+// The index and graph of the last call (or of gr_graph_load) are current and
+// may be reused by this call.
+bool reuse_graph(const gr_ctx* c) { return c->csr_valid && (c->keep_graph || c->graph_loaded); }
 
 int round_cap(int64_t maxdeg, int lo, int hi) {
   int64_t c = ((maxdeg + 31) / 32) * 32;
@@ -437,6 +473,7 @@ static int set_catalog_impl(gr_ctx* c, const double* xyz, const double* w, const
   c->w_ran = wr;
   c->cat_set = true;
   c->csr_valid = false;
+  c->graph_loaded = false;
   c->regions.valid = false;
   GR_API_END(c)
 }
@@ -465,6 +502,7 @@ int gr_set_bins(gr_ctx* c, double rmin, double rmax, int32_t nbins, int32_t nmu,
   c->logbins = logbins ? 1 : 0;
   c->bins_set = true;
   c->csr_valid = false;
+  c->graph_loaded = false;
   c->regions.valid = false;
   GR_API_END(c)
 }
@@ -473,7 +511,14 @@ int gr_set_option(gr_ctx* c, int32_t key, int64_t value) {
   GR_API_BEGIN(c)
   if (key == GR_OPT_PRECISION) {
     if (value != 0 && value != 1) return set_err(c, GR_E_ARG, "precision must be 0 or 1");
+    if (c->precision != (int)value) {
+      c->csr_valid = false;
+      c->graph_loaded = false;
+    }
     c->precision = (int)value;
+  } else if (key == GR_OPT_KEEP_GRAPH) {
+    if (value != 0 && value != 1) return set_err(c, GR_E_ARG, "keep-graph must be 0 or 1");
+    c->keep_graph = value != 0;
   } else if (key == GR_OPT_AUTOTUNE) {
     if (value < 0 || value > 1 + kPairVariants) return set_err(c, GR_E_ARG, "autotune must be 0, 1 or 2+variant");
     c->autotune = (int)value;
@@ -548,7 +593,7 @@ int gr_count_2pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
   c->hfix.reserve(2 * nh);
   c->stats.reserve(8);
   GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
-  build_index(c);
+  if (!reuse_graph(c)) build_index(c);
   GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
   c->work.reserve(4);
   const int variant = pick_pair2_variant(c, c->index.view(), weighted, fscale, c->hcnt.p,
@@ -621,10 +666,11 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
   normal_table(nmu, nt);
   c->normal_dev.reserve(nt.size());
   GR_CUDA_TRY(cudaMemcpyAsync(c->normal_dev.p, nt.data(), nt.size(), cudaMemcpyHostToDevice, s));
+  const bool reuse = reuse_graph(c);
   GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
-  build_index(c);
+  if (!reuse) build_index(c);
   GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
-  build_csr(c);
+  if (!reuse) build_csr(c);
   GR_CUDA_TRY(cudaEventRecord(c->ev[2], s));
   unsigned long long gst[4];
   GR_CUDA_TRY(cudaMemcpyAsync(gst, c->csr.stats.p, sizeof(gst), cudaMemcpyDeviceToHost, s));
@@ -721,10 +767,11 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   c->dcnt.reserve(nd);
   c->dfix.reserve(2 * nd);
   c->stats.reserve(8);
+  const bool reuse = reuse_graph(c);
   GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
-  build_index(c);
+  if (!reuse) build_index(c);
   GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
-  build_csr(c);
+  if (!reuse) build_csr(c);
   GR_CUDA_TRY(cudaEventRecord(c->ev[2], s));
   unsigned long long gst[4];
   GR_CUDA_TRY(cudaMemcpyAsync(gst, c->csr.stats.p, sizeof(gst), cudaMemcpyDeviceToHost, s));
@@ -832,9 +879,200 @@ int gr_count_tetra(gr_ctx* c, double* N2, double* N3, double* discN, double* dis
 int gr_graph_build(gr_ctx* c) {
   GR_API_BEGIN(c)
   require_ready(c);
-  build_index(c);
-  build_csr(c);
+  if (!reuse_graph(c)) {
+    build_index(c);
+    build_csr(c);
+  }
   GR_CUDA_TRY(cudaStreamSynchronize(c->stream()));
+  GR_API_END(c)
+}
+
+// ------------------------------------------------------ graph persistence ----
+namespace {
+
+struct GraphFileHeader {
+  char magic[8];  // "GRAMSCSR"
+  uint32_t version, header_bytes;
+  int64_t n, n_edges, max_deg;
+  double rmin, rmax;
+  int32_t nbins, nmu, logbins, reserved0;
+  unsigned long long fingerprint, checksum;
+  int64_t rechecks, candidates;
+  unsigned long long labels;  // FNV-1a of the cell labelling (label -> point)
+  unsigned char pad[128 - 8 - 8 - 24 - 16 - 16 - 16 - 16 - 8];
+};
+static_assert(sizeof(GraphFileHeader) == 128, "graph file header is 128 bytes");
+
+unsigned long long fnv1a(unsigned long long h, const void* p, size_t bytes) {
+  const unsigned char* b = static_cast<const unsigned char*>(p);
+  for (size_t k = 0; k < bytes; ++k) h = (h ^ b[k]) * 0x100000001b3ull;
+  return h;
+}
+
+unsigned long long coord_fingerprint(gr_ctx* c) {
+  cudaStream_t s = c->stream();
+  c->uniform_flag.reserve(24);
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(c->uniform_flag.p + 16);
+  GR_CUDA_TRY(cudaMemsetAsync(d, 0, sizeof(unsigned long long), s));
+  if (c->n > 0) {
+    int blocks = (int)std::min<int64_t>((c->n + 255) / 256, 148 * 8);
+    fingerprint_kernel<<<blocks, 256, 0, s>>>(c->xyz.p, c->n, d);
+    GR_CHECK_LAUNCH();
+  }
+  unsigned long long h = 0;
+  GR_CUDA_TRY(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaStreamSynchronize(s));
+  return h ^ mix_host((unsigned long long)c->n);
+}
+
+unsigned long long label_fingerprint(gr_ctx* c) {
+  std::vector<int> orig(c->n);
+  if (c->n > 0) {
+    GR_CUDA_TRY(cudaMemcpyAsync(orig.data(), c->index.orig.p, sizeof(int) * c->n, cudaMemcpyDeviceToHost,
+                                c->stream()));
+    GR_CUDA_TRY(cudaStreamSynchronize(c->stream()));
+  }
+  return fnv1a(0xcbf29ce484222325ull, orig.data(), sizeof(int) * orig.size());
+}
+
+}  // namespace
+
+int gr_graph_save(gr_ctx* c, const char* path) {
+  GR_API_BEGIN(c)
+  if (!path) return set_err(c, GR_E_ARG, "null path");
+  require_ready(c);
+  if (!c->csr_valid) {
+    build_index(c);
+    build_csr(c);
+  }
+  cudaStream_t s = c->stream();
+  const int64_t n = c->n, E = c->csr.n_edges;
+  std::vector<int64_t> rp(n + 1);
+  std::vector<unsigned long long> rec(E);
+  std::vector<int> deg(n);
+  GR_CUDA_TRY(cudaMemcpyAsync(rp.data(), c->csr.row_ptr.p, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, s));
+  if (E > 0)
+    GR_CUDA_TRY(cudaMemcpyAsync(rec.data(), c->csr.rec.p, sizeof(unsigned long long) * E, cudaMemcpyDeviceToHost, s));
+  if (n > 0)
+    GR_CUDA_TRY(cudaMemcpyAsync(deg.data(), c->csr.deg_full.p, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaStreamSynchronize(s));
+  GraphFileHeader H;
+  std::memset(&H, 0, sizeof(H));
+  std::memcpy(H.magic, "GRAMSCSR", 8);
+  H.version = 1;
+  H.header_bytes = sizeof(H);
+  H.n = n;
+  H.n_edges = E;
+  H.max_deg = c->csr.max_deg;
+  H.rmin = c->rmin;
+  H.rmax = c->rmax;
+  H.nbins = c->nbins;
+  H.nmu = c->nmu;
+  H.logbins = c->logbins;
+  H.rechecks = c->csr.rechecks;
+  H.candidates = c->csr.candidates;
+  H.fingerprint = coord_fingerprint(c);
+  H.labels = label_fingerprint(c);
+  unsigned long long h = 0xcbf29ce484222325ull;
+  h = fnv1a(h, rp.data(), sizeof(int64_t) * rp.size());
+  h = fnv1a(h, rec.data(), sizeof(unsigned long long) * rec.size());
+  h = fnv1a(h, deg.data(), sizeof(int) * deg.size());
+  H.checksum = h;
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return set_err(c, GR_E_ARG, std::string("cannot write ") + path);
+  bool ok = std::fwrite(&H, sizeof(H), 1, f) == 1 &&
+            std::fwrite(rp.data(), sizeof(int64_t), rp.size(), f) == rp.size() &&
+            std::fwrite(rec.data(), sizeof(unsigned long long), rec.size(), f) == rec.size() &&
+            std::fwrite(deg.data(), sizeof(int), deg.size(), f) == deg.size();
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) return set_err(c, GR_E_ARG, std::string("short write to ") + path);
+  GR_API_END(c)
+}
+
+int gr_graph_load(gr_ctx* c, const char* path) {
+  GR_API_BEGIN(c)
+  if (!path) return set_err(c, GR_E_ARG, "null path");
+  require_ready(c);
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return set_err(c, GR_E_ARG, std::string("cannot read ") + path);
+  GraphFileHeader H;
+  auto fail = [&](const char* why) {
+    std::fclose(f);
+    return set_err(c, GR_E_ARG, why);
+  };
+  if (std::fread(&H, sizeof(H), 1, f) != 1) return fail("graph file: short header");
+  if (std::memcmp(H.magic, "GRAMSCSR", 8) != 0 || H.version != 1 || H.header_bytes != sizeof(H))
+    return fail("graph file: not a version-1 graph");
+  if (H.n != c->n) return fail("graph file: point count differs from the catalogue");
+  if (H.rmin != c->rmin || H.rmax != c->rmax || H.nbins != c->nbins || H.nmu != c->nmu ||
+      H.logbins != c->logbins)
+    return fail("graph file: binning differs from gr_set_bins");
+  if (H.n_edges < 0 || H.max_deg < 0 || H.max_deg > H.n) return fail("graph file: bad sizes");
+  if (H.fingerprint != coord_fingerprint(c)) return fail("graph file: coordinates differ");
+  const int64_t n = H.n, E = H.n_edges;
+  std::vector<int64_t> rp(n + 1);
+  std::vector<unsigned long long> rec(E);
+  std::vector<int> deg(n);
+  if (std::fread(rp.data(), sizeof(int64_t), rp.size(), f) != rp.size() ||
+      std::fread(rec.data(), sizeof(unsigned long long), rec.size(), f) != rec.size() ||
+      std::fread(deg.data(), sizeof(int), deg.size(), f) != deg.size())
+    return fail("graph file: short payload");
+  std::fclose(f);
+  unsigned long long h = 0xcbf29ce484222325ull;
+  h = fnv1a(h, rp.data(), sizeof(int64_t) * rp.size());
+  h = fnv1a(h, rec.data(), sizeof(unsigned long long) * rec.size());
+  h = fnv1a(h, deg.data(), sizeof(int) * deg.size());
+  if (h != H.checksum) return set_err(c, GR_E_ARG, "graph file: checksum mismatch");
+  // structural checks before anything reaches the device: rows in range,
+  // labels in range and increasing within a row (the query kernels rely on it)
+  // bins in range, full degrees equal to the rows' (the kernels index
+  // histograms by bin and size their staging by degree)
+  if (rp[0] != 0 || rp[n] != E) return set_err(c, GR_E_ARG, "graph file: bad row pointers");
+  int64_t maxd = 0;
+  std::vector<int> dchk(n, 0);
+  for (int64_t p = 0; p < n; ++p) {
+    if (rp[p + 1] < rp[p]) return set_err(c, GR_E_ARG, "graph file: bad row pointers");
+    maxd = std::max(maxd, rp[p + 1] - rp[p]);
+    uint32_t prev = (uint32_t)p;
+    for (int64_t e = rp[p]; e < rp[p + 1]; ++e) {
+      const uint32_t q = (uint32_t)rec[e];
+      if (q <= prev || q >= (uint64_t)n) return set_err(c, GR_E_ARG, "graph file: bad neighbour label");
+      const uint32_t m = (uint32_t)(rec[e] >> 32);
+      const int b = (int)(m & 0xff), mf = (int)((m >> 8) & 0xff), mr = (int)((m >> 16) & 0xff);
+      if ((m >> 24) != 0 || b < 1 || b > c->nbins || mf < 1 || mf > c->nmu || mr < 1 || mr > c->nmu)
+        return set_err(c, GR_E_ARG, "graph file: bad bin");
+      dchk[p]++;
+      dchk[q]++;
+      prev = q;
+    }
+  }
+  if (maxd != H.max_deg) return set_err(c, GR_E_ARG, "graph file: bad degree");
+  if (dchk != deg) return set_err(c, GR_E_ARG, "graph file: bad degree");
+  cudaStream_t s = c->stream();
+  build_index(c);
+  if (label_fingerprint(c) != H.labels)
+    return set_err(c, GR_E_ARG, "graph file: cell labelling differs (written by another version)");
+  UpperCSR& G = c->csr;
+  G.n = n;
+  G.n_edges = E;
+  G.max_deg = H.max_deg;
+  G.rechecks = H.rechecks;
+  G.candidates = H.candidates;
+  G.row_ptr.reserve(n + 1);
+  G.rec.reserve(E + 1);
+  G.deg_full.reserve(n + 1);
+  G.stats.reserve(4);
+  unsigned long long st[4] = {(unsigned long long)H.rechecks, (unsigned long long)H.candidates,
+                              (unsigned long long)H.max_deg, 0ull};
+  GR_CUDA_TRY(cudaMemcpyAsync(G.row_ptr.p, rp.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, s));
+  if (E > 0)
+    GR_CUDA_TRY(cudaMemcpyAsync(G.rec.p, rec.data(), sizeof(unsigned long long) * E, cudaMemcpyHostToDevice, s));
+  if (n > 0)
+    GR_CUDA_TRY(cudaMemcpyAsync(G.deg_full.p, deg.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+  GR_CUDA_TRY(cudaMemcpyAsync(G.stats.p, st, sizeof(st), cudaMemcpyHostToDevice, s));
+  GR_CUDA_TRY(cudaStreamSynchronize(s));
+  c->csr_valid = true;
+  c->graph_loaded = true;
   GR_API_END(c)
 }
 
@@ -933,7 +1171,7 @@ int gr_adjoint_2pcf(gr_ctx* c, const double* cot2, const double* cot3, double* g
   if (cot3)
     GR_CUDA_TRY(cudaMemcpyAsync(c->cot.p + nbm, cot3, sizeof(double) * nbm, cudaMemcpyHostToDevice, s));
   GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
-  build_index(c);
+  if (!reuse_graph(c)) build_index(c);
   GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
   GR_CUDA_TRY(cudaMemsetAsync(c->gfix.p, 0, sizeof(unsigned long long) * (2 * n + 2), s));
   std::memset(&c->st, 0, sizeof(c->st));

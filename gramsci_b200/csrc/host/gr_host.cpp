@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <string>
 #include <vector>
 
@@ -75,6 +76,17 @@ bool parse_real(const std::string& tok, double& v) {
   char* end = nullptr;
   errno = 0;
   v = std::strtod(s.c_str(), &end);
+  return end && *end == '\0';
+}
+
+// A real(4) item: the decimal string rounded once to single precision.
+bool parse_real4(const std::string& tok, float& v) {
+  std::string s = tok;
+  for (char& ch : s)
+    if (ch == 'd' || ch == 'D' || ch == 'q' || ch == 'Q') ch = 'e';
+  if (s.empty()) return false;
+  char* end = nullptr;
+  v = std::strtof(s.c_str(), &end);
   return end && *end == '\0';
 }
 
@@ -238,6 +250,9 @@ int grh_parse_args(int argc, const char* const* argv, grh_options* o) {
     } else if (opt_is(opt, "-equi")) {
       o->equi = 1;
       i += 1;
+    } else if (opt_is(opt, "-gcol")) {
+      o->gcol = 1;
+      i += 1;
     } else if (opt_is(opt, "-2pcf")) {
       o->two_pcf = 1;
       i += 1;
@@ -305,6 +320,52 @@ int grh_read_region(const char* path, double** xyz, double** w, int32_t** buffer
   *w = q;
   *buffer = b;
   *n = m;
+  return 0;
+}
+
+int grh_read_region_gal(const char* path, double** xyz, double** w, int32_t** buffer,
+                        int64_t* n_data, int64_t* n_rand) {
+  Records R;
+  if (!load_records(path, R)) return -1;
+  const int64_t m = count_records(R);
+  std::vector<double> v6((size_t)m * 4);
+  std::vector<long long> g((size_t)m), b((size_t)m);
+  R.next = 0;
+  int64_t n = 0;
+  for (int64_t i = 0; i < m; ++i) {
+    double v[6];
+    long long iv[6];
+    ReadStatus s = list_read(R, 6, "rrrrii", v, iv);
+    if (s != R_OK) break;
+    for (int k = 0; k < 4; ++k) v6[(size_t)n * 4 + k] = v[k];
+    g[n] = iv[4];
+    b[n] = iv[5];
+    n++;
+  }
+  double* p = static_cast<double*>(std::calloc((size_t)(3 * n + 3), sizeof(double)));
+  double* q = static_cast<double*>(std::calloc((size_t)(n + 1), sizeof(double)));
+  int32_t* f = static_cast<int32_t*>(std::calloc((size_t)(n + 1), sizeof(int32_t)));
+  if (!p || !q || !f) {
+    std::free(p);
+    std::free(q);
+    std::free(f);
+    return -3;
+  }
+  int64_t nd = 0, k = 0;
+  for (int pass = 0; pass < 2; ++pass)
+    for (int64_t i = 0; i < n; ++i) {
+      if ((g[i] != 0) != (pass == 0)) continue;
+      for (int c = 0; c < 3; ++c) p[3 * k + c] = v6[(size_t)i * 4 + c];
+      q[k] = v6[(size_t)i * 4 + 3];
+      f[k] = (int32_t)b[i];
+      k++;
+      if (pass == 0) nd++;
+    }
+  *xyz = p;
+  *w = q;
+  *buffer = f;
+  *n_data = nd;
+  *n_rand = n - nd;
   return 0;
 }
 
@@ -492,6 +553,208 @@ int grh_write_tetra(const char* path, const double* edges, int32_t nbins, int32_
       write_record(f, v, 8);
     }
   return std::fclose(f) == 0 ? 0 : -1;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ region files --
+namespace {
+
+struct RegionPoint {
+  double x[3], w;
+  long long gal;
+  long long region;
+};
+
+// Region boxes and memberships with the arithmetic type T (float reproduces
+// the reference program; double for catalogue input).
+template <typename T>
+int write_regions(const std::vector<RegionPoint>& P, T rmax, T grow, int digits,
+                  const std::string& prefix, int32_t* nregion) {
+  long long nreg = 0;
+  for (const RegionPoint& p : P) nreg = p.region > nreg ? p.region : nreg;
+  for (long long j = 1; j <= nreg; ++j) {
+    // minval / maxval with mask=region.eq.j (+-huge for an empty region)
+    T lo[3], hi[3];
+    for (int c = 0; c < 3; ++c) {
+      lo[c] = std::numeric_limits<T>::max();
+      hi[c] = -std::numeric_limits<T>::max();
+    }
+    for (const RegionPoint& p : P)
+      if (p.region == j)
+        for (int c = 0; c < 3; ++c) {
+          const T v = (T)p.x[c];
+          lo[c] = v < lo[c] ? v : lo[c];
+          hi[c] = v > hi[c] ? v : hi[c];
+        }
+    T lo2[3], hi2[3];
+    for (int c = 0; c < 3; ++c) {
+      lo2[c] = lo[c] - rmax * grow;
+      hi2[c] = hi[c] + rmax * grow;
+    }
+    const std::string name = prefix + std::to_string(j) + ".loadnodes";
+    FILE* f = std::fopen(name.c_str(), "w");
+    if (!f) return -2;
+    for (const RegionPoint& p : P) {
+      T v[3] = {(T)p.x[0], (T)p.x[1], (T)p.x[2]};
+      bool in = true, core = true;
+      for (int c = 0; c < 3; ++c) {
+        in = in && v[c] > lo2[c] && v[c] < hi2[c];
+        core = core && v[c] >= lo[c] && v[c] <= hi[c];
+      }
+      if (!in) continue;
+      std::fprintf(f, " %.*g %.*g %.*g %.*g %lld %d\n", digits, (double)v[0], digits, (double)v[1],
+                   digits, (double)v[2], digits, (double)(T)p.w, p.gal, core ? 0 : 1);
+    }
+    if (std::fclose(f) != 0) return -2;
+  }
+  *nregion = (int32_t)nreg;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int grh_decompose(const char* allpoints, const char* gal, const char* ran, double rmax,
+                  int32_t nsplit, const char* prefix, int32_t* nregion) {
+  std::vector<RegionPoint> P;
+  const std::string pre = prefix ? prefix : "";
+  *nregion = 0;
+  if (allpoints && allpoints[0]) {
+    // src/domain_decomposition.f90:14-33: count records, then READ
+    // x y z w gal aux region per record; a READ error skips the record.
+    Records R;
+    if (!load_records(allpoints, R)) return -1;
+    R.next = 0;
+    for (;;) {
+      if (R.next >= R.lines.size()) break;
+      std::vector<std::string> tok;
+      bool slash = false;
+      // one list-directed READ of 7 items
+      std::vector<std::string> items;
+      while (items.size() < 7 && R.next < R.lines.size()) {
+        split_tokens(R.lines[R.next++], tok, slash);
+        for (const std::string& t : tok)
+          if (items.size() < 7) items.push_back(t);
+        if (slash) break;
+      }
+      if (items.size() < 7) break;  // end of file inside the READ
+      float x[4], aux;
+      long long g, r;
+      bool ok = parse_real4(items[0], x[0]) && parse_real4(items[1], x[1]) &&
+                parse_real4(items[2], x[2]) && parse_real4(items[3], x[3]) &&
+                parse_int(items[4], g) && parse_real4(items[5], aux) && parse_int(items[6], r);
+      if (!ok) continue;
+      RegionPoint p;
+      for (int c = 0; c < 3; ++c) p.x[c] = x[c];
+      p.w = x[3];
+      p.gal = g;
+      p.region = r;
+      P.push_back(p);
+    }
+    // `real rmax` read from the command line: one rounding to single precision
+    char buf[64];
+    std::snprintf(buf, sizeof(buf), "%.17g", rmax);
+    float rm;
+    if (!parse_real4(buf, rm)) return -3;
+    return write_regions<float>(P, rm, 1.0f, 9, pre, nregion);
+  }
+  if (!gal || !gal[0] || nsplit < 1 || !(rmax > 0.0)) return -3;
+  double *xyz = nullptr, *w = nullptr;
+  int64_t nd = 0, nr = 0;
+  if (grh_read_catalogue(gal, ran, &xyz, &w, &nd, &nr) != 0) return -1;
+  grh_normalise(w, nd, nr);
+  const int64_t n = nd + nr;
+  double lo[3], hi[3];
+  for (int c = 0; c < 3; ++c) {
+    lo[c] = std::numeric_limits<double>::infinity();
+    hi[c] = -lo[c];
+  }
+  for (int64_t i = 0; i < n; ++i)
+    for (int c = 0; c < 3; ++c) {
+      lo[c] = std::fmin(lo[c], xyz[3 * i + c]);
+      hi[c] = std::fmax(hi[c], xyz[3 * i + c]);
+    }
+  P.resize((size_t)n);
+  for (int64_t i = 0; i < n; ++i) {
+    long long cell[3];
+    for (int c = 0; c < 3; ++c) {
+      const double ext = hi[c] - lo[c];
+      long long k = ext > 0.0 ? (long long)std::floor((xyz[3 * i + c] - lo[c]) / ext * nsplit) : 0;
+      cell[c] = k < 0 ? 0 : (k >= nsplit ? nsplit - 1 : k);
+    }
+    RegionPoint& p = P[(size_t)i];
+    for (int c = 0; c < 3; ++c) p.x[c] = xyz[3 * i + c];
+    p.w = w[i];
+    p.gal = i < nd ? 1 : 0;
+    p.region = 1 + cell[0] + (long long)nsplit * (cell[1] + (long long)nsplit * cell[2]);
+  }
+  grh_free(xyz);
+  grh_free(w);
+  // subcubes are disjoint, so every point is a root in exactly one region;
+  // the halo is grown by 1e-9 relative so that FP64 rounding of box - rmax
+  // cannot drop a neighbour closer than rmax
+  return write_regions<double>(P, rmax, 1.0 + 1e-9, 17, pre, nregion);
+}
+
+int grh_resum(int32_t query, int32_t n, const char* const* inputs, const char* out) {
+  if (n < 1 || query < 2 || query > 6) return -3;
+  // columns after the bin columns: N2, N3, N2/N3 [, disconnected terms]
+  const int ndisc = query == 4 ? 3 : (query == 6 ? 1 : 0);
+  std::vector<std::string> header;
+  std::vector<std::vector<std::string>> bins;  // bin tokens per row
+  std::vector<double> n2, n3;
+  for (int f = 0; f < n; ++f) {
+    Records R;
+    if (!load_records(inputs[f], R)) return -1;
+    size_t row = 0;
+    for (const std::string& line : R.lines) {
+      std::vector<std::string> tok;
+      bool slash;
+      split_tokens(line, tok, slash);
+      double v0;
+      if (tok.empty()) continue;
+      if (!parse_real(tok[0], v0)) {  // header line
+        if (f == 0) header.push_back(line);
+        continue;
+      }
+      const int nt = (int)tok.size();
+      const int nbin_col = nt - 3 - ndisc;
+      if (nbin_col < 1) return -3;
+      std::vector<std::string> b(tok.begin(), tok.begin() + nbin_col);
+      double a, c;
+      if (!parse_real(tok[nbin_col], a) || !parse_real(tok[nbin_col + 1], c)) return -3;
+      if (f == 0) {
+        bins.push_back(b);
+        n2.push_back(a);
+        n3.push_back(c);
+      } else {
+        if (row >= bins.size() || bins[row] != b) return -3;
+        n2[row] += a;
+        n3[row] += c;
+      }
+      row++;
+    }
+    if (row != bins.size()) return -3;
+  }
+  FILE* fo = std::fopen(out, "w");
+  if (!fo) return -2;
+  for (const std::string& h : header) std::fprintf(fo, "%s\n", h.c_str());
+  for (size_t r = 0; r < bins.size(); ++r) {
+    std::vector<double> v;
+    for (const std::string& t : bins[r]) {
+      double x;
+      parse_real(t, x);
+      v.push_back(x);
+    }
+    v.push_back(n2[r]);
+    v.push_back(n3[r]);
+    v.push_back(n2[r] / n3[r]);
+    for (int k = 0; k < ndisc; ++k) v.push_back(std::numeric_limits<double>::quiet_NaN());
+    write_record(fo, v.data(), (int)v.size());
+  }
+  return std::fclose(fo) == 0 ? 0 : -2;
 }
 
 }  // extern "C"

@@ -3,7 +3,7 @@
 // on the GPU through libgramsci_cuda.so.
 //
 //   gramsci -gal G [-ran R] -rmin a -rmax b -nbins n [-nmu m] [-log]
-//           [-out F] [-cut region.loadnodes] -2pcf | -3pcf | -4pcf | -equi | -tetra
+//           [-out F] [-cut region.loadnodes [-gcol]] -2pcf | -3pcf | -4pcf | -equi | -tetra
 //
 // Exit status follows the reference: 0 after help, after an unknown option
 // (the reference prints a message and stops) and after a run; 2 for an
@@ -24,7 +24,7 @@ void print_help() {
   std::puts(" ");
   std::puts(" usage: gramsci -gal galaxy_file [-ran random_file] -rmin Rmin -rmax Rmax");
   std::puts("                -nbins Nbins [-nmu Nmu] [-log] [-out out_file]");
-  std::puts("                [-cut region_file] -2pcf | -3pcf | -4pcf | -equi | -tetra");
+  std::puts("                [-cut region_file [-gcol]] -2pcf | -3pcf | -4pcf | -equi | -tetra");
   std::puts(" ");
   std::puts("   galaxy_file, random_file  records of x y z w");
   std::puts("   Rmin, Rmax                range of separations counted");
@@ -32,6 +32,7 @@ void print_help() {
   std::puts("   Nmu                       line-of-sight bins in -1 < mu < 1 (>= 2 turns them on)");
   std::puts("   out_file                  result table (default result.txt)");
   std::puts("   -equi, -tetra             equilateral triangles / regular tetrahedra only");
+  std::puts("   -gcol                     region file rows are x y z w gal buffer (gramsci-decompose)");
 }
 
 int fail(gr_ctx* ctx, const char* what, int rc) {
@@ -68,11 +69,15 @@ int main(int argc, char** argv) {
   if (o.cut_mode) {
     const char* region = o.mpi ? "1.loadnodes" : o.cut;
     int64_t n = 0;
-    if (grh_read_region(region, &xyz, &w, &buffer, &n) != 0) {
+    // -gcol: x y z w gal buffer files with a galaxy/random split; otherwise
+    // the reference's x y z w buffer read with no split (src/gramsci.F90:1304-1317)
+    const int rr = o.gcol ? grh_read_region_gal(region, &xyz, &w, &buffer, &nd, &nr)
+                          : grh_read_region(region, &xyz, &w, &buffer, &n);
+    if (rr != 0) {
       std::fprintf(stderr, "gramsci: cannot read %s\n", region);
       return 1;
     }
-    nd = n;  // region files carry no galaxy/random split (src/gramsci.F90:1304-1317)
+    if (!o.gcol) nd = n;
   } else {
     if (grh_read_catalogue(o.gal, o.rancat ? o.ran : nullptr, &xyz, &w, &nd, &nr) != 0) {
       std::fprintf(stderr, "gramsci: cannot read the catalogues\n");

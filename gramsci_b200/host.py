@@ -9,6 +9,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libgramsci_host.so")
 CLI_PATH = os.path.join(HERE, "bin", "gramsci")
+DECOMPOSE_PATH = os.path.join(HERE, "bin", "gramsci-decompose")
+RESUM_PATH = os.path.join(HERE, "bin", "gramsci-resum")
 
 
 class Options(ctypes.Structure):
@@ -20,6 +22,7 @@ class Options(ctypes.Structure):
                 ("mpi", ctypes.c_int32), ("rancat", ctypes.c_int32),
                 ("two_pcf", ctypes.c_int32), ("three_pcf", ctypes.c_int32),
                 ("four_pcf", ctypes.c_int32), ("equi", ctypes.c_int32), ("tetra", ctypes.c_int32),
+                ("gcol", ctypes.c_int32),
                 ("help", ctypes.c_int32), ("error", ctypes.c_int32),
                 ("message", ctypes.c_char * 256)]
 
@@ -124,3 +127,48 @@ def write_tetra(path, edges, nbins, nmu, N2, N3, discN, discR):
     return load().grh_write_tetra(path.encode(), e.ctypes.data_as(_d), nbins, nmu,
                                   a.ctypes.data_as(_d), b.ctypes.data_as(_d), c.ctypes.data_as(_d),
                                   d.ctypes.data_as(_d))
+
+
+def decompose(rmax, prefix, allpoints=None, gal=None, ran=None, nsplit=0):
+    """grh_decompose: region files <prefix>j.loadnodes; returns the count."""
+    L = load()
+    L.grh_decompose.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double,
+                                ctypes.c_int32, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int32)]
+    n = ctypes.c_int32(0)
+    enc = lambda s: None if s is None else str(s).encode()
+    rc = L.grh_decompose(enc(allpoints), enc(gal), enc(ran), float(rmax), int(nsplit),
+                         str(prefix).encode(), ctypes.byref(n))
+    if rc:
+        raise OSError(f"grh_decompose failed ({rc})")
+    return n.value
+
+
+def resum(query, inputs, out):
+    """grh_resum; query 2/3/4 (N-point), 5 (-equi), 6 (-tetra).  Returns rc."""
+    L = load()
+    arr = (ctypes.c_char_p * len(inputs))(*[str(p).encode() for p in inputs])
+    L.grh_resum.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_char_p),
+                            ctypes.c_char_p]
+    return L.grh_resum(int(query), len(inputs), arr, str(out).encode())
+
+
+def read_region_gal(path):
+    """grh_read_region_gal: (xyz (N,3), w, buffer, n_data, n_rand)."""
+    L = load()
+    xyz, w = _d(), _d()
+    buf = ctypes.POINTER(ctypes.c_int32)()
+    nd, nr = ctypes.c_int64(0), ctypes.c_int64(0)
+    L.grh_read_region_gal.argtypes = [ctypes.c_char_p, ctypes.POINTER(_d), ctypes.POINTER(_d),
+                                      ctypes.POINTER(ctypes.POINTER(ctypes.c_int32)),
+                                      ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]
+    if L.grh_read_region_gal(str(path).encode(), ctypes.byref(xyz), ctypes.byref(w), ctypes.byref(buf),
+                             ctypes.byref(nd), ctypes.byref(nr)):
+        raise OSError(f"cannot read {path}")
+    n = nd.value + nr.value
+    out = (np.ctypeslib.as_array(xyz, (3 * n,)).reshape(n, 3).copy() if n else np.zeros((0, 3)),
+           np.ctypeslib.as_array(w, (n,)).copy() if n else np.zeros(0),
+           np.ctypeslib.as_array(buf, (n,)).copy() if n else np.zeros(0, np.int32), nd.value, nr.value)
+    L.grh_free.argtypes = [ctypes.c_void_p]
+    for p in (xyz, w, buf):
+        L.grh_free(ctypes.cast(p, ctypes.c_void_p))
+    return out

@@ -48,6 +48,9 @@ typedef struct gr_ctx gr_ctx;
 #define GR_OPT_AUTOTUNE 3   /* 0: fixed kernels; 1: time the pair-sweep variants once per
                                workload class and cache the choice (default); 2+v: force
                                variant v (0 warp per cell, 1/2 block per cell of 128/256) */
+#define GR_OPT_KEEP_GRAPH 4 /* 0 (default): every count call builds the index and graph;
+                               1: keep the graph of the last call and reuse it until the
+                               catalogue, the bins or the precision change */
 
 /* Run statistics of the last count call (gr_get_stats). */
 typedef struct gr_stats {
@@ -151,6 +154,20 @@ int gr_count_tetra(gr_ctx* ctx, double* N2, double* N3, double* discN, double* d
 int gr_graph_build(gr_ctx* ctx);
 int gr_graph_nedges(gr_ctx* ctx, int64_t* n_edges);
 int gr_graph_export(gr_ctx* ctx, int64_t* row_ptr, int32_t* col, uint8_t* bin, uint8_t* mu);
+
+/* Graph persistence (the "graph database" of the reference's README: build
+ * the graph once, query it many times).  gr_graph_save writes the graph of
+ * the current catalogue and bins (building it if needed); gr_graph_load reads
+ * one back for the same catalogue positions and bins -- it checks the point
+ * count, the binning and a 64-bit fingerprint of the coordinates, and returns
+ * GR_E_ARG on a mismatch -- after which the 2/3/4PCF, -equi and -tetra calls
+ * reuse it (no graph build) until the catalogue, bins or precision change.
+ * File: a 128-byte header ("GRAMSCSR", version 1, n, upper edges, max upper
+ * degree, rmin, rmax, nbins, nmu, logbins, coordinate fingerprint, payload
+ * checksum, labelling fingerprint), then row_ptr int64[n+1], records uint64[edges], full degree
+ * int32[n], all little-endian, in the library's internal (cell) labelling. */
+int gr_graph_save(gr_ctx* ctx, const char* path);
+int gr_graph_load(gr_ctx* ctx, const char* path);
 
 /* Batched regions.  Replaces the reference's domain decomposition
  * (src/domain_decomposition.f90:39-80) followed by one program run per

@@ -27,6 +27,7 @@ typedef struct grh_options {
   int32_t nbins, nmu;
   int32_t rsd, logbins, cut_mode, mpi, rancat;
   int32_t two_pcf, three_pcf, four_pcf, equi, tetra;
+  int32_t gcol;           /* -gcol: region files carry the gal column */
   int32_t help;           /* -help given, or fewer than 6 arguments */
   int32_t error;          /* 0 ok, 1 unknown option, 2 unreadable value */
   char message[256];
@@ -45,7 +46,40 @@ int grh_read_catalogue(const char* gal, const char* ran, double** xyz, double** 
 /* Region file of -cut mode (count_files + read_files, :1304-1362): records
  * x y z w buffer; all points are data and weights are not normalised. */
 int grh_read_region(const char* path, double** xyz, double** w, int32_t** buffer, int64_t* n);
+/* -gcol variant (not in the reference): records x y z w gal buffer, the
+ * files gramsci-decompose writes.  gal != 0 marks a galaxy; galaxies are
+ * returned first, then randoms, each in file order; weights as written. */
+int grh_read_region_gal(const char* path, double** xyz, double** w, int32_t** buffer,
+                        int64_t* n_data, int64_t* n_rand);
 void grh_free(void* p);
+
+/* Region files (domain_decomposition, src/domain_decomposition.f90:1-84).
+ *
+ * allpoints != NULL: the reference program.  Records x y z w gal aux region
+ * read as single precision; region j = 1..max(region) gets the bounding box
+ * of its points, the box grown by rmax (single precision), and every point
+ * strictly inside the grown box is written to <prefix>j.loadnodes as
+ * x y z w gal buffer, buffer = 0 inside the region's own box.
+ *
+ * allpoints == NULL: the same files from the catalogues gal (+ ran), with
+ * region labels from nsplit^3 equal subcubes of the catalogue's bounding
+ * box, FP64 throughout (values written with 17 digits), weights normalised
+ * over the whole catalogue (galaxies w/sum, randoms -w/sum) and gal = 1 for
+ * galaxies, 0 for randoms.  Running `gramsci -cut j.loadnodes -gcol` on each
+ * file and summing the tables (grh_resum) gives the unsplit run's table.
+ *
+ * *nregion receives the number of region files written.  Returns 0, or -1
+ * for an unreadable input, -2 for an unwritable output, -3 for bad args. */
+int grh_decompose(const char* allpoints, const char* gal, const char* ran, double rmax,
+                  int32_t nsplit, const char* prefix, int32_t* nregion);
+
+/* Sum of region tables (the reference's missing resum step): N2 and N3 are
+ * summed, N2/N3 recomputed; the bin columns must agree.  query: 2 (2PCF),
+ * 3 (3PCF), 4 (4PCF), 5 (-equi), 6 (-tetra).  The disconnected 4PCF/-tetra
+ * columns are ratios of sums that a table does not hold; they are written
+ * as NaN.  Returns 0, -1 unreadable input, -2 unwritable output, -3
+ * mismatched tables. */
+int grh_resum(int32_t query, int32_t n, const char* const* inputs, const char* out);
 
 /* Weight normalisation (:1390-1391), sums left to right. */
 void grh_normalise(double* w, int64_t n_data, int64_t n_rand);

@@ -74,3 +74,58 @@ def test_cli_matches_oracle_table(tmp_path, oracle, query, name, scale, nmu):
         o = G.tetra(w, cat.n_data)
         host.write_tetra(str(ref), e, sp["nbins"], nmu, o["N2"], o["N3"], o["discN"], o["discR"])
     _compare(str(out), str(ref))
+
+
+def _half_unit(v):
+    """Half a unit in the 7th significant digit of E14.7 values."""
+    v = np.abs(np.asarray(v, np.float64))
+    with np.errstate(divide="ignore"):
+        e = np.where(v > 0, np.floor(np.log10(np.where(v > 0, v, 1.0))) + 1, 0)
+    return np.where(v > 0, 0.5 * 10.0 ** (e - 7), 0.0)
+
+
+def _table(path):
+    return np.array([[float(x) for x in l.split()] for l in open(path).read().splitlines()
+                     if not l.startswith(" r1")])
+
+
+@pytest.mark.parametrize("query,nmu,ncol", [("2pcf", 3, 7), ("3pcf", 1, 9), ("equi", 2, 7)])
+def test_region_pipeline_equals_unsplit(tmp_path, query, nmu, ncol):
+    """gramsci-decompose (2^3 subcubes) -> gramsci -cut j.loadnodes -gcol per
+    region -> gramsci-resum gives the unsplit run's table, to the 8 digits
+    each region table carries."""
+    name = "c2_3pcf"
+    cat, w, g, r = _write_cat(tmp_path, name, 0.01)
+    sp = catalogs.WORKLOADS[name]
+    bins = ["-rmin", repr(sp["rmin"]), "-rmax", repr(sp["rmax"]), "-nbins", str(sp["nbins"]),
+            "-nmu", str(nmu)]
+    full = tmp_path / "full.out"
+    res = subprocess.run([host.CLI_PATH, "-gal", g, "-ran", r, *bins, "-out", str(full), f"-{query}"],
+                         capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr
+    res = subprocess.run([host.DECOMPOSE_PATH, repr(sp["rmax"]), "-gal", g, "-ran", r, "-nsplit", "2",
+                          "-prefix", str(tmp_path / "reg")], capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr
+    parts = []
+    for j in range(1, 9):
+        out = tmp_path / f"part{j}.out"
+        res = subprocess.run([host.CLI_PATH, "-cut", str(tmp_path / f"reg{j}.loadnodes"), "-gcol", *bins,
+                              "-out", str(out), f"-{query}"], capture_output=True, text=True)
+        assert res.returncode == 0, res.stderr
+        parts.append(out)
+    total = tmp_path / "total.out"
+    res = subprocess.run([host.RESUM_PATH, f"-{query}", "-out", str(total), *map(str, parts)],
+                         capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr
+    a, b = _table(total), _table(full)
+    assert a.shape == b.shape and a.shape[1] == ncol
+    assert np.array_equal(a[:, :ncol - 3], b[:, :ncol - 3])
+    # each E14.7 value carries a rounding error of at most half a unit in its
+    # 7th digit: the bound is the sum of those over the parts, the total and
+    # the unsplit table (FP64 summation-order differences are far smaller)
+    cols = slice(ncol - 3, ncol - 1)
+    bound = sum(_half_unit(_table(p)[:, cols]) for p in parts)
+    bound = bound + _half_unit(a[:, cols]) + _half_unit(b[:, cols])
+    err = np.abs(a[:, cols] - b[:, cols])
+    assert np.all(err <= 1.01 * bound + 1e-300)
+    assert np.abs(b[:, ncol - 3]).max() > 0
