@@ -144,15 +144,23 @@ class Context:
         return dict(N2=_fortran(N2, nb, nm), N3=_fortran(N3, nb, nm),
                     counts=_fortran(counts, nb, nm, 4), catsum=_fortran(catsum, nb, nm, 4))
 
-    def count_3pcf(self):
+    def count_3pcf(self, counts=True):
+        """N2, N3 (ncfg, nmu) and the category sums; with counts=False the
+        integer counts (not part of the reference's output) are not kept,
+        which spares the kernel one atomic per rooted triangle when the
+        weights are not uniform."""
         nb, nm = self.nbins, self.nmu
         nc = ncfg3(nb)
         N2, N3 = np.zeros(nc * nm), np.zeros(nc * nm)
-        counts = np.zeros(nc * nm * 4, np.int64)
+        cnt = np.zeros(nc * nm * 4, np.int64) if counts else None
         catsum = np.zeros(nc * nm * 4)
-        self._check(self._lib.gr_count_3pcf(self._h, _ptr(N2), _ptr(N3), _ptr(counts), _ptr(catsum)))
-        return dict(N2=_fortran(N2, nc, nm), N3=_fortran(N3, nc, nm),
-                    counts=_fortran(counts, nc, nm, 4), catsum=_fortran(catsum, nc, nm, 4))
+        self._check(self._lib.gr_count_3pcf(self._h, _ptr(N2), _ptr(N3),
+                                            _ptr(cnt) if counts else None, _ptr(catsum)))
+        out = dict(N2=_fortran(N2, nc, nm), N3=_fortran(N3, nc, nm),
+                   catsum=_fortran(catsum, nc, nm, 4))
+        if counts:
+            out["counts"] = _fortran(cnt, nc, nm, 4)
+        return out
 
     def count_4pcf(self):
         nb = self.nbins

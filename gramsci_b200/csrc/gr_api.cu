@@ -52,6 +52,7 @@ struct gr_ctx {
   DevBuf<unsigned long long> hcnt, dcnt, stats;
   DevBuf<unsigned long long> hfix, dfix;  // fixed-point sums (lo words, then hi words)
   double wmax = 0.0;                      // max |w| over the catalogue
+  double wgmax = 0.0, wrmax = 0.0;        // max |w| over galaxies / randoms
   DevBuf<unsigned char> uniform_flag;
   DevBuf<int> work;
   DevBuf<double> cot, grad;              // adjoint inputs / output
@@ -159,6 +160,18 @@ double fix_scale(double pmax) {
   int e;
   std::frexp(pmax * (1.0 + 1e-9), &e);  // pmax < 2^e
   return std::ldexp(1.0, 60 - e);
+}
+
+double limb_scale(double pmax) {
+  if (!(pmax > 0.0) || !std::isfinite(pmax)) return 1.0;
+  int e;
+  std::frexp(pmax * (1.0 + 1e-9), &e);  // pmax < 2^e
+  return std::ldexp(1.0, 52 - e);
+}
+
+double limb_value(unsigned long long lo, unsigned long long hi, double scale) {
+  const __int128 v = (__int128)(long long)hi * ((__int128)1 << kLimbBits) + (__int128)lo;
+  return (double)v / scale;
 }
 
 double fix_value(unsigned long long lo, unsigned long long hi, double scale) {
@@ -273,22 +286,29 @@ int set_err(gr_ctx* c, int code, const std::string& m) {
   return GR_OK;
 
 // Clears *flag unless all galaxy weights are equal and all random weights are
-// equal; writes max |w| (as the bits of a non-negative double) to *wmax.
+// equal; writes max |w| over galaxies to wmax[0] and over randoms to wmax[1]
+// (as the bits of non-negative doubles).
 __global__ void uniform_check_kernel(const double* __restrict__ w, int64_t n_data, int64_t n,
                                      unsigned char* flag, unsigned long long* wmax) {
-  unsigned long long m = 0;
+  unsigned long long mg = 0, mr = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     double ref = i < n_data ? w[0] : w[n_data];
     if (__double_as_longlong(w[i]) != __double_as_longlong(ref)) *flag = 0;
     unsigned long long a = (unsigned long long)__double_as_longlong(fabs(w[i]));
-    m = a > m ? a : m;
+    if (i < n_data) mg = a > mg ? a : mg;
+    else mr = a > mr ? a : mr;
   }
   for (int o = 16; o > 0; o >>= 1) {
-    unsigned long long u = __shfl_xor_sync(0xffffffffu, m, o);
-    m = u > m ? u : m;
+    unsigned long long u = __shfl_xor_sync(0xffffffffu, mg, o);
+    mg = u > mg ? u : mg;
+    u = __shfl_xor_sync(0xffffffffu, mr, o);
+    mr = u > mr ? u : mr;
   }
-  if ((threadIdx.x & 31) == 0 && m) atomicMax(wmax, m);
+  if ((threadIdx.x & 31) == 0) {
+    if (mg) atomicMax(&wmax[0], mg);
+    if (mr) atomicMax(&wmax[1], mr);
+  }
 }
 
 unsigned long long mix_host(unsigned long long z) {
@@ -449,24 +469,27 @@ static int set_catalog_impl(gr_ctx* c, const double* xyz, const double* w, const
   c->n_rand = n_rand;
   // Uniform weights (all galaxies equal, all randoms equal) let the kernels
   // keep integer counts only; sums are then count x product.
-  c->uniform_flag.reserve(16);
-  unsigned char init[16] = {1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-  unsigned char out[16];
-  GR_CUDA_TRY(cudaMemcpyAsync(c->uniform_flag.p, init, 16, cudaMemcpyHostToDevice, s));
+  // [0] uniform flag, [8] max |w| galaxies, [16] max |w| randoms, [24] fingerprint
+  c->uniform_flag.reserve(32);
+  unsigned char init[24] = {1};
+  unsigned char out[24];
+  GR_CUDA_TRY(cudaMemcpyAsync(c->uniform_flag.p, init, 24, cudaMemcpyHostToDevice, s));
   unsigned long long* d_wmax = reinterpret_cast<unsigned long long*>(c->uniform_flag.p + 8);
   if (n > 0) {
     int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
     uniform_check_kernel<<<blocks, 256, 0, s>>>(c->w.p, n_data, n, c->uniform_flag.p, d_wmax);
     GR_CHECK_LAUNCH();
   }
-  GR_CUDA_TRY(cudaMemcpyAsync(out, c->uniform_flag.p, 16, cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaMemcpyAsync(out, c->uniform_flag.p, 24, cudaMemcpyDeviceToHost, s));
   double wg = 0.0, wr = 0.0;
   if (n_data > 0) GR_CUDA_TRY(cudaMemcpyAsync(&wg, c->w.p, sizeof(double), cudaMemcpyDeviceToHost, s));
   if (n_rand > 0)
     GR_CUDA_TRY(cudaMemcpyAsync(&wr, c->w.p + n_data, sizeof(double), cudaMemcpyDeviceToHost, s));
   GR_CUDA_TRY(cudaStreamSynchronize(s));
   unsigned char flag = out[0];
-  std::memcpy(&c->wmax, out + 8, 8);
+  std::memcpy(&c->wgmax, out + 8, 8);
+  std::memcpy(&c->wrmax, out + 16, 8);
+  c->wmax = std::max(c->wgmax, c->wrmax);
   if (!std::isfinite(c->wmax)) return set_err(c, GR_E_ARG, "non-finite weights");
   c->uniform = flag != 0;
   c->w_gal = wg;
@@ -658,7 +681,10 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
   const int ncfg = equi ? c->nbins : (int)(((int64_t)c->nbins * (c->nbins + 1) * (c->nbins + 2)) / 6);
   const int nbin = ncfg * nmu, nh = nbin * 4;
   const bool weighted = !c->uniform;
-  const double fscale = fix_scale(c->wmax * c->wmax * c->wmax);
+  const bool want_counts = counts != nullptr || !weighted;
+  double fscale[4];
+  for (int nr = 0; nr < 4; ++nr)
+    fscale[nr] = limb_scale(std::pow(c->wgmax, 3 - nr) * std::pow(c->wrmax, nr));
   c->hcnt.reserve(nh);
   c->hfix.reserve(2 * nh);
   c->stats.reserve(8);
@@ -678,7 +704,7 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
   GR_CUDA_TRY(cudaMemsetAsync(c->hfix.p, 0, sizeof(unsigned long long) * 2 * nh, s));
   GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
   GR_CUDA_TRY(cudaStreamSynchronize(s));
-  TriParams T;
+  TriParams T{};
   T.nbins = c->nbins;
   T.nmu = nmu;
   T.ncfg = ncfg;
@@ -687,24 +713,29 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
   T.cap = round_cap(c->csr.max_deg, 32, 256);
   T.normal = c->normal_dev.p;
   make_rank_tables(T.rank, c->nbins, 3);
+  for (int nr = 0; nr < 4; ++nr) T.fscale[nr] = fscale[nr];
   CSRView G{c->csr.row_ptr.p, c->csr.rec.p, c->csr.deg_full.p};
   cudaEvent_t q0;
   GR_CUDA_TRY(cudaEventCreate(&q0));
   GR_CUDA_TRY(cudaEventRecord(q0, s));
   c->work.reserve(4);
-  launch_tri3(c->index.view(), G, T, weighted, c->hcnt.p, c->hfix.p, fscale, c->stats.p,
+  launch_tri3(c->index.view(), G, T, weighted, want_counts, c->hcnt.p, c->hfix.p, c->stats.p,
               c->work.p, s);
   GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
-  std::vector<unsigned long long> hc(nh), hf(2 * nh, 0ull);
+  std::vector<unsigned long long> hc(nh, 0ull), hf(2 * nh, 0ull);
   std::vector<double> hs(nh, 0.0);
   unsigned long long st[8];
-  GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
+  if (want_counts)
+    GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
   if (weighted)
     GR_CUDA_TRY(cudaMemcpyAsync(hf.data(), c->hfix.p, sizeof(unsigned long long) * 2 * nh, cudaMemcpyDeviceToHost, s));
   GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
   GR_CUDA_TRY(cudaStreamSynchronize(s));
+  // limb sums are exact below 2^35 updates per bin; the rooted total bounds them
+  if (weighted && st[1] >= (1ull << 35))
+    return set_err(c, GR_E_CAPACITY, "3PCF: more than 2^35 rooted triangles for the exact sums");
   if (weighted)
-    for (int k = 0; k < nh; ++k) hs[k] = fix_value(hf[k], hf[nh + k], fscale);
+    for (int k = 0; k < nh; ++k) hs[k] = limb_value(hf[k], hf[nh + k], fscale[k / nbin]);
   if (!weighted) {
     for (int nr = 0; nr < 4; ++nr) {
       double prod = uniform_product(c->w_gal, c->w_ran, 3 - nr, nr);
@@ -783,7 +814,7 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   GR_CUDA_TRY(cudaStreamSynchronize(s));
   if ((int64_t)gst[2] > 1024)
     return set_err(c, GR_E_CAPACITY, "4PCF: a point has more than 1024 larger-label neighbours");
-  QuadParams Q;
+  QuadParams Q{};
   Q.nbins = nb;
   Q.ncfg = ncfg;
   Q.tetra = tetra ? 1 : 0;
@@ -911,8 +942,8 @@ unsigned long long fnv1a(unsigned long long h, const void* p, size_t bytes) {
 
 unsigned long long coord_fingerprint(gr_ctx* c) {
   cudaStream_t s = c->stream();
-  c->uniform_flag.reserve(24);
-  unsigned long long* d = reinterpret_cast<unsigned long long*>(c->uniform_flag.p + 16);
+  c->uniform_flag.reserve(32);
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(c->uniform_flag.p + 24);
   GR_CUDA_TRY(cudaMemsetAsync(d, 0, sizeof(unsigned long long), s));
   if (c->n > 0) {
     int blocks = (int)std::min<int64_t>((c->n + 255) / 256, 148 * 8);
@@ -1219,7 +1250,7 @@ int gr_adjoint_3pcf(gr_ctx* c, const double* cot2, const double* cot3, double* g
   GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
   GR_CUDA_TRY(cudaMemsetAsync(c->gfix.p, 0, sizeof(unsigned long long) * (2 * n + 2), s));
   GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
-  TriParams T;
+  TriParams T{};
   T.nbins = c->nbins;
   T.nmu = nmu;
   T.ncfg = ncfg;

@@ -6,17 +6,20 @@
 // Every triangle is enumerated exactly once, from its smallest internal
 // label p.  A warp takes a root p and stages its upper row R+(p) in shared
 // memory together with the flags, catalogue ids and weights of those
-// neighbours, a small open-addressing hash table (label -> row position) and
-// an owner table mapping each flattened work item f to the neighbour a whose
-// row it reads.  The work items (a, c) for c in R+(a) are spread over the
-// lanes; each lane loads one 8-byte CSR record and probes the hash table for
-// c.  Hits (triangles p < a < c) are pushed to a per-warp queue that is
-// drained 32 at a time, so the binning work runs with every lane busy.
+// neighbours, their row starts and lengths, and a per-root open-addressing
+// hash table (label offset -> row position, one 32-bit word per entry,
+// Fibonacci hashing).  The work items (a, c) for c in R+(a) are flattened
+// over batches of 32 rows and spread over the lanes; a lane finds the row
+// of its item by a binary search over the lanes' prefix sums (register
+// shuffles), loads one 8-byte CSR record and probes the hash table for c.
+// Hits (triangles p < a < c) are pushed to a per-warp queue that is drained
+// 32 at a time, so the binning work runs with every lane busy.
 //
 // A triangle contributes to the rooted histogram of each non-buffer vertex r
 // with the bins of its three edges (symmetric bin table), the find_normal mu
 // bin of r's two edges taken in catalogue-id order (k1 < k2 in the
-// reference's id-sorted row) and the product (w_r w_first) w_second.
+// reference's id-sorted row) and the weight product, accumulated as two-limb
+// fixed point with a scale per number of randoms.
 #include "gr_kernels.cuh"
 
 namespace gr {
@@ -25,36 +28,39 @@ namespace {
 
 constexpr int kTriMaxWarps = 32;  // block size is chosen at launch to fit shared memory
 constexpr size_t kSmemLimit = 227 * 1024;
-constexpr int kOwn = 512;    // flattened work items per owner-table chunk
 constexpr int kQueue = 64;   // hit queue entries per warp
 constexpr int kChunk = 4;    // roots taken per work-counter increment
 constexpr int kCfgTableBins = 16;  // nbins up to which the configuration table is used
 
 __host__ __device__ inline size_t align8(size_t x) { return (x + 7) & ~(size_t)7; }
-__host__ __device__ inline int hash_size(int cap) {
-  int h = 32;
-  while (h < 2 * cap) h <<= 1;
-  return h;
-}
-
 struct TriLayout {
-  size_t off_cnt, off_fix, off_cot, off_norm, off_rank, off_cfg, off_warp, warp_bytes, total;
+  size_t off_cnt, off_lim, off_cot, off_norm, off_rank, off_cfg, off_fsc, off_warp, warp_bytes, total;
   // per-warp sub-offsets
-  size_t o_rs, o_w, o_g, o_col, o_meta, o_orig, o_pre, o_hkey, o_qm, o_qxy, o_flag, o_hval, o_own;
+  size_t o_rs, o_w, o_g, o_col, o_meta, o_orig, o_len, o_hkey, o_qm, o_qxy, o_flag;
 };
+
+// Largest per-root hash table: a power of two >= 2 * cap (load <= 1/2).
+__host__ __device__ inline int hash_lg_max(int cap) {
+  int lg = 6;
+  while ((1 << lg) < 2 * cap) ++lg;
+  return lg;
+}
 
 // adj: the adjoint variant (cotangent tables, per-neighbour gradient
 // accumulators) instead of histograms.
 __host__ __device__ inline TriLayout tri_layout(int nh, int nmu, int nbins, int cap, bool shist,
-                                                bool weighted, int nwarps, bool adj = false) {
+                                                bool weighted, bool counts, int nwarps,
+                                                bool adj = false) {
   TriLayout L;
   size_t o = 0;
   L.off_cnt = o;
-  if (shist) o += (size_t)nh * 8;
-  L.off_fix = o;
+  if (shist && counts) o += (size_t)nh * 8;
+  L.off_lim = o;
   if (shist && weighted) o += (size_t)nh * 16;
   L.off_cot = o;
   if (adj) o += (size_t)nh / 4 * 2 * 8;  // cot2, cot3: ncfg * nmu doubles each
+  L.off_fsc = o;
+  o += 4 * 8;
   L.off_norm = o;
   o = align8(o + (size_t)nmu * nmu);
   L.off_rank = o;
@@ -62,21 +68,19 @@ __host__ __device__ inline TriLayout tri_layout(int nh, int nmu, int nbins, int 
   L.off_cfg = o;  // configuration of every (b1, b2, b3), small nbins only
   if (nbins <= kCfgTableBins) o = align8(o + sizeof(uint16_t) * (size_t)nbins * nbins * nbins);
   L.off_warp = o;
-  const int hs = hash_size(cap);
+  const int hs = 1 << hash_lg_max(cap);
   size_t w = 0;
   L.o_rs = w;   w += (size_t)cap * 8;
-  L.o_w = w;    w += (size_t)cap * 8;
+  L.o_w = w;    if (weighted || adj) w += (size_t)cap * 8;
   L.o_g = w;    if (adj) w += (size_t)cap * 16;  // gradient (lo, hi) per neighbour
   L.o_col = w;  w += (size_t)cap * 4;
   L.o_meta = w; w += (size_t)cap * 4;
   L.o_orig = w; w += (size_t)cap * 4;
-  L.o_pre = w;  w += (size_t)(cap + 1) * 4;
+  L.o_len = w;  w += (size_t)cap * 4;
   L.o_hkey = w; w += (size_t)hs * 4;
   L.o_qm = w;   w += (size_t)kQueue * 4;
   L.o_qxy = w;  w += (size_t)kQueue * 2;
   L.o_flag = w; w += (size_t)cap;
-  L.o_hval = w; w += (size_t)hs;
-  L.o_own = w;  w += (size_t)kOwn;
   L.warp_bytes = align8(w);
   L.total = o + L.warp_bytes * nwarps;
   return L;
@@ -86,10 +90,10 @@ struct TriCtx {
   const uint8_t* norm;
   const int* F;  // 3 x (nbins+2)
   const uint16_t* cfgtab;  // symmetric configuration table or NULL
+  const double* fsc;       // limb scale by number of randoms
   int nbins, nmu, ncfg, rsd, nh, equi;
   unsigned long long* cnt;
-  unsigned long long* lo;  // fixed-point sums: lo[k], lo[nh + k] = hi[k]
-  double fscale;
+  unsigned long long* lim;  // limb sums: lim[k] (lo), lim[nh + k] (hi)
   // adjoint
   const double* c2;  // cot2 (ncfg, nmu)
   const double* c3;  // cot3 (ncfg, nmu)
@@ -112,10 +116,21 @@ __device__ __forceinline__ int normal_bin(const TriCtx& X, int mu1, int mu2, boo
   return first_is_1 ? X.norm[(mu1 - 1) + X.nmu * (mu2 - 1)] : X.norm[(mu2 - 1) + X.nmu * (mu1 - 1)];
 }
 
-// One triangle (p, a, c) with p < a < c in labels.  Per-vertex data are
-// passed in; contributions that land in the same bin are merged before the
-// shared-memory atomics.  Returns the number of rooted contributions.
-template <bool WEIGHTED>
+template <bool WEIGHTED, bool COUNTS>
+__device__ __forceinline__ void tri_add(const TriCtx& X, int k, int n, long long v) {
+  if (COUNTS) atomicAdd(&X.cnt[k], (unsigned long long)n);
+  if (WEIGHTED) limb_add(&X.lim[k], &X.lim[X.nh + k], v * n);
+}
+
+// One triangle (p, a, c) with p < a < c in labels.  It adds to the rooted
+// histogram of each non-buffer vertex r: the bins of its three edges
+// (symmetric bin table), the find_normal mu bin of r's two edges taken in
+// catalogue-id order (k1 < k2 in the reference's id-sorted row) and the
+// weight product w_p w_a w_c (one product for all roots: the orders the
+// reference multiplies in differ from it by at most an ulp).  Roots that land
+// in the same bin share one update.  Returns the number of rooted
+// contributions.
+template <bool WEIGHTED, bool COUNTS>
 __device__ __forceinline__ int tri_bin(const TriCtx& X, uint8_t fp, int op, double wp, uint8_t fa,
                                        int oa, double wa, uint8_t fc, int oc, double wc,
                                        uint32_t mpa, uint32_t mpc, uint32_t mac) {
@@ -128,40 +143,25 @@ __device__ __forceinline__ int tri_bin(const TriCtx& X, uint8_t fp, int op, doub
     cfg = tri_cfg(X, meta_bin(mpa), meta_bin(mpc), meta_bin(mac));
   }
   const int nr = (fp & FLAG_RANDOM) + (fa & FLAG_RANDOM) + (fc & FLAG_RANDOM);
-  int m[3] = {-1, -1, -1};
-  double pr[3] = {0.0, 0.0, 0.0};
-  int cnt[3] = {0, 0, 0};
-  if (!(fp & FLAG_BUFFER)) {  // root p: neighbours a, c
-    const bool ac = oa < oc;
-    m[0] = normal_bin(X, meta_muf(mpa), meta_muf(mpc), ac);
-    if (WEIGHTED) pr[0] = ac ? (wp * wa) * wc : (wp * wc) * wa;
-    cnt[0] = 1;
+  long long v = 0;
+  if (WEIGHTED) v = __double2ll_rn(((wp * wa) * wc) * X.fsc[nr]);
+  int m0 = 1, m1 = 1, m2 = 1;
+  if (X.rsd) {
+    m0 = normal_bin(X, meta_muf(mpa), meta_muf(mpc), oa < oc);  // root p: a, c
+    m1 = normal_bin(X, meta_mur(mpa), meta_muf(mac), op < oc);  // root a: p, c
+    m2 = normal_bin(X, meta_mur(mpc), meta_mur(mac), op < oa);  // root c: p, a
   }
-  if (!(fa & FLAG_BUFFER)) {  // root a: neighbours p, c
-    const bool pc = op < oc;
-    m[1] = normal_bin(X, meta_mur(mpa), meta_muf(mac), pc);
-    if (WEIGHTED) pr[1] = pc ? (wa * wp) * wc : (wa * wc) * wp;
-    cnt[1] = 1;
-  }
-  if (!(fc & FLAG_BUFFER)) {  // root c: neighbours p, a
-    const bool pa = op < oa;
-    m[2] = normal_bin(X, meta_mur(mpc), meta_mur(mac), pa);
-    if (WEIGHTED) pr[2] = pa ? (wc * wp) * wa : (wc * wa) * wp;
-    cnt[2] = 1;
-  }
-  const int total = cnt[0] + cnt[1] + cnt[2];
-  // merge equal bins
-  if (m[1] >= 0 && m[1] == m[0]) { cnt[0] += cnt[1]; pr[0] += pr[1]; cnt[1] = 0; }
-  if (m[2] >= 0 && m[2] == m[0]) { cnt[0] += cnt[2]; pr[0] += pr[2]; cnt[2] = 0; }
-  else if (m[2] >= 0 && m[2] == m[1] && cnt[1]) { cnt[1] += cnt[2]; pr[1] += pr[2]; cnt[2] = 0; }
+  int c0 = (fp & FLAG_BUFFER) ? 0 : 1;
+  int c1 = (fa & FLAG_BUFFER) ? 0 : 1;
+  int c2 = (fc & FLAG_BUFFER) ? 0 : 1;
+  const int total = c0 + c1 + c2;
+  if (c1 && m1 == m0 && c0) { c0 += c1; c1 = 0; }
+  if (c2 && m2 == m0 && c0) { c0 += c2; c2 = 0; }
+  else if (c2 && m2 == m1 && c1) { c1 += c2; c2 = 0; }
   const int base = (cfg - 1) + X.ncfg * X.nmu * nr;
-#pragma unroll
-  for (int r = 0; r < 3; ++r) {
-    if (cnt[r] == 0) continue;
-    const int k = base + X.ncfg * (m[r] - 1);
-    atomicAdd(&X.cnt[k], (unsigned long long)cnt[r]);
-    if (WEIGHTED) fix_add(&X.lo[k], &X.lo[X.nh + k], pr[r], X.fscale);
-  }
+  if (c0) tri_add<WEIGHTED, COUNTS>(X, base + X.ncfg * (m0 - 1), c0, v);
+  if (c1) tri_add<WEIGHTED, COUNTS>(X, base + X.ncfg * (m1 - 1), c1, v);
+  if (c2) tri_add<WEIGHTED, COUNTS>(X, base + X.ncfg * (m2 - 1), c2, v);
   return total;
 }
 
@@ -216,17 +216,23 @@ __device__ __forceinline__ int lower_bound_g(const unsigned long long* a, int n,
   return lo;
 }
 
-__device__ __forceinline__ uint32_t hash_slot(int key, int hmask) {
-  return ((uint32_t)key * 2654435761u) & (uint32_t)hmask;
+// Fibonacci hashing of a label offset into a table of 2^lg slots: runs of
+// consecutive offsets (the common case: a cell's points are consecutive
+// labels) spread evenly over the table.
+__device__ __forceinline__ uint32_t fib_slot(uint32_t off, int lg) {
+  return (off * 2654435769u) >> (32 - lg);
 }
+
+// Hash entries: (offset << 8) | position, offset = label - p in [1, 2^24);
+// 0 marks an empty slot.
+constexpr int kMaxOffset = 1 << 24;
 
 // ADJ: accumulate the weight gradient (g_lo / g_hi, label order) of
 // L = sum cot2 N2 + cot3 N3 instead of the histograms.
-template <bool WEIGHTED, bool SHIST, bool ADJ>
+template <bool WEIGHTED, bool COUNTS, bool SHIST, bool ADJ>
 __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, CSRView G, TriParams T,
                                                            unsigned long long* __restrict__ g_cnt,
-                                                           unsigned long long* __restrict__ g_fix,
-                                                           double fscale,
+                                                           unsigned long long* __restrict__ g_lim,
                                                            unsigned long long* __restrict__ stats,
                                                            int* __restrict__ work,
                                                            const double* __restrict__ cot2,
@@ -236,7 +242,8 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
                                                            unsigned long long* __restrict__ g_hi) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int nh = T.ncfg * T.nmu * 4;
-  const TriLayout L = tri_layout(nh, T.nmu, T.nbins, T.cap, SHIST, WEIGHTED, blockDim.x >> 5, ADJ);
+  const TriLayout L =
+      tri_layout(nh, T.nmu, T.nbins, T.cap, SHIST, WEIGHTED, COUNTS, blockDim.x >> 5, ADJ);
   TriCtx X;
   X.nbins = T.nbins;
   X.nmu = T.nmu;
@@ -244,13 +251,14 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
   X.rsd = T.rsd;
   X.equi = T.equi;
   X.nh = nh;
-  X.fscale = fscale;
   X.cnt = SHIST ? reinterpret_cast<unsigned long long*>(smem + L.off_cnt) : g_cnt;
-  X.lo = SHIST ? reinterpret_cast<unsigned long long*>(smem + L.off_fix) : g_fix;
+  X.lim = SHIST ? reinterpret_cast<unsigned long long*>(smem + L.off_lim) : g_lim;
   uint8_t* s_norm = smem + L.off_norm;
   int* s_F = reinterpret_cast<int*>(smem + L.off_rank);
+  double* s_fsc = reinterpret_cast<double*>(smem + L.off_fsc);
   X.norm = s_norm;
   X.F = s_F;
+  X.fsc = s_fsc;
   X.gscale = gscale;
   if (ADJ) {
     double* s_cot = reinterpret_cast<double*>(smem + L.off_cot);
@@ -264,13 +272,14 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
   }
   if (SHIST) {
     for (int k = threadIdx.x; k < nh; k += blockDim.x) {
-      X.cnt[k] = 0ull;
+      if (COUNTS) X.cnt[k] = 0ull;
       if (WEIGHTED) {
-        X.lo[k] = 0ull;
-        X.lo[nh + k] = 0ull;
+        X.lim[k] = 0ull;
+        X.lim[nh + k] = 0ull;
       }
     }
   }
+  if (threadIdx.x < 4) s_fsc[threadIdx.x] = T.fscale[threadIdx.x];
   for (int k = threadIdx.x; k < T.nmu * T.nmu; k += blockDim.x) s_norm[k] = T.rsd ? T.normal[k] : 1;
   const int nb2 = T.nbins + 2;
   for (int k = threadIdx.x; k < 3 * nb2; k += blockDim.x) s_F[k] = T.rank.F[k / nb2][k % nb2];
@@ -296,19 +305,29 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
   int* s_col = reinterpret_cast<int*>(wb + L.o_col);
   uint32_t* s_meta = reinterpret_cast<uint32_t*>(wb + L.o_meta);
   int* s_orig = reinterpret_cast<int*>(wb + L.o_orig);
-  int* s_pre = reinterpret_cast<int*>(wb + L.o_pre);
-  int* s_hkey = reinterpret_cast<int*>(wb + L.o_hkey);
+  int* s_len = reinterpret_cast<int*>(wb + L.o_len);
+  uint32_t* s_hkey = reinterpret_cast<uint32_t*>(wb + L.o_hkey);
   uint32_t* s_qm = reinterpret_cast<uint32_t*>(wb + L.o_qm);
   uint16_t* s_qxy = reinterpret_cast<uint16_t*>(wb + L.o_qxy);
   uint8_t* s_flag = wb + L.o_flag;
-  uint8_t* s_hval = wb + L.o_hval;
-  uint8_t* s_own = wb + L.o_own;
   unsigned long long* s_glo = reinterpret_cast<unsigned long long*>(wb + L.o_g);
   unsigned long long* s_ghi = s_glo + T.cap;
-  const int hs = hash_size(T.cap);
-  const int hmask = hs - 1;
+  const int lg_max = hash_lg_max(T.cap);
 
   unsigned long long tris = 0, rooted = 0, probes = 0;
+
+  // one queued triangle (p, a = row qx, c = row qy) with edge meta (a, c)
+  auto drain_one = [&](int e, uint8_t fp, int op, double wp, Fix128& racc) -> int {
+    const uint16_t xy = s_qxy[e];
+    const int qx = xy & 0xff, qy = xy >> 8;
+    if (ADJ)
+      return tri_grad(X, fp, op, wp, s_flag[qx], s_orig[qx], s_w[qx], s_flag[qy], s_orig[qy],
+                      s_w[qy], s_meta[qx], s_meta[qy], s_qm[e], racc, &s_glo[qx], &s_ghi[qx],
+                      &s_glo[qy], &s_ghi[qy]);
+    return tri_bin<WEIGHTED, COUNTS>(X, fp, op, wp, s_flag[qx], s_orig[qx],
+                                     WEIGHTED ? s_w[qx] : 0.0, s_flag[qy], s_orig[qy],
+                                     WEIGHTED ? s_w[qy] : 0.0, s_meta[qx], s_meta[qy], s_qm[e]);
+  };
 
   for (;;) {
     int base_root = 0;
@@ -322,110 +341,119 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
       if (k < 2) continue;
       const uint8_t fp = C.flags[p];
       const int op = C.orig[p];
-      const double wp = WEIGHTED ? C.w[p] : 0.0;
+      const double wp = (WEIGHTED || ADJ) ? C.w[p] : 0.0;
       Fix128 racc = {0ull, 0ull};
-      if (k <= T.cap) {
+      // rows are sorted: the last entry has the largest label offset
+      if (k <= T.cap && rec_col(G.rec[b0 + k - 1]) - p < kMaxOffset) {
+        // per-root table: >= 4 slots per entry, at most the capacity's table
+        int lg = 6;
+        while (lg < lg_max && (1 << lg) < 4 * k) ++lg;
+        const int hs = 1 << lg;
         __syncwarp();
-        for (int h = lane; h < hs; h += 32) s_hkey[h] = -1;
+        for (int h = lane; h < hs; h += 32) s_hkey[h] = 0u;
         __syncwarp();
         // stage R+(p) and the data of its vertices; insert into the hash table
-        int carry = 0;
         for (int xb = 0; xb < k; xb += 32) {
           const int x = xb + lane;
-          int len = 0;
           if (x < k) {
             const unsigned long long r = G.rec[b0 + x];
             const int a = rec_col(r);
             s_col[x] = a;
             s_meta[x] = rec_meta(r);
             const long long rs = G.row_ptr[a];
+            const int len = (int)(G.row_ptr[a + 1] - rs);
             s_rs[x] = rs;
-            len = (int)(G.row_ptr[a + 1] - rs);
+            s_len[x] = len;
+            probes += (unsigned long long)len;
             s_flag[x] = C.flags[a];
             s_orig[x] = C.orig[a];
-            if (WEIGHTED) s_w[x] = C.w[a];
+            if (WEIGHTED || ADJ) s_w[x] = C.w[a];
             if (ADJ) {
               s_glo[x] = 0ull;
               s_ghi[x] = 0ull;
             }
-            uint32_t h = hash_slot(a, hmask);
+            const uint32_t off = (uint32_t)(a - p);
+            const uint32_t key = (off << 8) | (uint32_t)x;
+            uint32_t h = fib_slot(off, lg);
             for (int t = 0; t < hs; ++t) {
-              if (atomicCAS(&s_hkey[h], -1, a) == -1) {
-                s_hval[h] = (uint8_t)x;
-                break;
-              }
-              h = (h + 1) & hmask;
+              if (atomicCAS(&s_hkey[h], 0u, key) == 0u) break;
+              h = (h + 1) & (uint32_t)(hs - 1);
             }
           }
-          int incl = len;
+        }
+        __syncwarp();
+        int qn = 0;
+        // rows in batches of 32; the batch's non-empty rows are compacted
+        // onto the lanes, their work items (a, c in R+(a)) flattened and
+        // spread over the lanes 32 at a time.  A lane finds the row of its
+        // item from the mask of rows ending inside the window (one warp OR
+        // reduction) and the count of rows that ended before it.
+        for (int xb = 0; xb < k; xb += 32) {
+          const int x = xb + lane;
+          int len = 0;
+          long long rs = 0;
+          if (x < k) {
+            len = s_len[x];
+            rs = s_rs[x];
+          }
+          const unsigned nz = __ballot_sync(0xffffffffu, len > 0);
+          const int nrows = __popc(nz);
+          const int src = lane < nrows ? (int)__fns(nz, 0, lane + 1) : 0;
+          // every lane takes part in each shuffle; the select comes after
+          const int slen = __shfl_sync(0xffffffffu, len, src);
+          const int clen = lane < nrows ? slen : 0;
+          const long long crs = __shfl_sync(0xffffffffu, rs, src);
+          const int cx = xb + src;
+          int incl = clen;
 #pragma unroll
           for (int o = 1; o < 32; o <<= 1) {
             const int y = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += y;
           }
-          if (x < k) {
-            s_pre[x + 1] = carry + incl;
-            // record index of work item f = s_rs[x] + f
-            s_rs[x] -= (long long)(carry + incl - len);
-          }
-          carry += __shfl_sync(0xffffffffu, incl, 31);
-        }
-        if (lane == 0) s_pre[0] = 0;
-        const int W = carry;
-        if (lane == 0) probes += (unsigned long long)W;
-        int qn = 0;
-        int x0 = 0;  // first row overlapping the current owner chunk
-        for (int fb = 0; fb < W; fb += kOwn) {
-          const int fe = min(W, fb + kOwn);
-          __syncwarp();
-          // owner table for work items [fb, fe)
-          while (x0 < k && s_pre[x0 + 1] <= fb) ++x0;
-          for (int x = x0; x < k && s_pre[x] < fe; ++x) {
-            const int lo = max(s_pre[x], fb), hi = min(s_pre[x + 1], fe);
-            for (int f = lo + lane; f < hi; f += 32) s_own[f - fb] = (uint8_t)x;
-          }
-          __syncwarp();
-          for (int f0 = fb; f0 < fe; f0 += 32) {
-            const int f = f0 + lane;
+          const int tot = __shfl_sync(0xffffffffu, incl, 31);
+          const int excl = incl - clen;
+          int done = 0;  // compacted rows that ended before the window
+          for (int t0 = 0; t0 < tot; t0 += 32) {
+            const int t = t0 + lane;
+            const int last = incl - 1 - t0;  // window position of the row's last item
+            const unsigned bit = (lane < nrows && last >= 0 && last < 32) ? (1u << last) : 0u;
+            const unsigned ends = __reduce_or_sync(0xffffffffu, bit);
+            const int j = done + __popc(ends & lt);
+            done += __popc(ends);
+            const long long ors = __shfl_sync(0xffffffffu, crs, j & 31);
+            const int oex = __shfl_sync(0xffffffffu, excl, j & 31);
+            const int ox = __shfl_sync(0xffffffffu, cx, j & 31);
             bool hit = false;
-            int x = 0, y = 0;
+            int y = 0;
             uint32_t mac = 0;
-            if (f < fe) {
-              x = s_own[f - fb];
-              const unsigned long long r = G.rec[s_rs[x] + f];
-              const int c = rec_col(r);
+            if (t < tot) {
+              const unsigned long long r = G.rec[ors + (t - oex)];
+              const int off = rec_col(r) - p;
               mac = rec_meta(r);
-              uint32_t h = hash_slot(c, hmask);
-              for (int t = 0; t < hs; ++t) {
-                const int key = s_hkey[h];
-                if (key == c) {
-                  hit = true;
-                  y = s_hval[h];
-                  break;
+              if (off < kMaxOffset) {
+                uint32_t h = fib_slot((uint32_t)off, lg);
+                for (int it = 0; it < hs; ++it) {
+                  const uint32_t e = s_hkey[h];
+                  if ((e >> 8) == (uint32_t)off) {
+                    hit = true;
+                    y = (int)(e & 0xffu);
+                    break;
+                  }
+                  if (e == 0u) break;
+                  h = (h + 1) & (uint32_t)(hs - 1);
                 }
-                if (key < 0) break;
-                h = (h + 1) & hmask;
               }
             }
             const unsigned m = __ballot_sync(0xffffffffu, hit);
             if (hit) {
               const int pos = qn + __popc(m & lt);
               s_qm[pos] = mac;
-              s_qxy[pos] = (uint16_t)(x | (y << 8));
+              s_qxy[pos] = (uint16_t)(ox | (y << 8));
             }
             qn += __popc(m);
             if (qn >= 32) {
               __syncwarp();
-              const int e = qn - 32 + lane;
-              const uint16_t xy = s_qxy[e];
-              const int qx = xy & 0xff, qy = xy >> 8;
-              const int nroot =
-                  ADJ ? tri_grad(X, fp, op, wp, s_flag[qx], s_orig[qx], s_w[qx], s_flag[qy],
-                                 s_orig[qy], s_w[qy], s_meta[qx], s_meta[qy], s_qm[e], racc,
-                                 &s_glo[qx], &s_ghi[qx], &s_glo[qy], &s_ghi[qy])
-                      : tri_bin<WEIGHTED>(X, fp, op, wp, s_flag[qx], s_orig[qx],
-                                          WEIGHTED ? s_w[qx] : 0.0, s_flag[qy], s_orig[qy],
-                                          WEIGHTED ? s_w[qy] : 0.0, s_meta[qx], s_meta[qy], s_qm[e]);
+              const int nroot = drain_one(qn - 32 + lane, fp, op, wp, racc);
               tris += nroot > 0;
               rooted += nroot;
               qn -= 32;
@@ -435,15 +463,7 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
         }
         __syncwarp();
         if (lane < qn) {
-          const uint16_t xy = s_qxy[lane];
-          const int qx = xy & 0xff, qy = xy >> 8;
-          const int nroot =
-              ADJ ? tri_grad(X, fp, op, wp, s_flag[qx], s_orig[qx], s_w[qx], s_flag[qy],
-                             s_orig[qy], s_w[qy], s_meta[qx], s_meta[qy], s_qm[lane], racc,
-                             &s_glo[qx], &s_ghi[qx], &s_glo[qy], &s_ghi[qy])
-                  : tri_bin<WEIGHTED>(X, fp, op, wp, s_flag[qx], s_orig[qx],
-                                      WEIGHTED ? s_w[qx] : 0.0, s_flag[qy], s_orig[qy],
-                                      WEIGHTED ? s_w[qy] : 0.0, s_meta[qx], s_meta[qy], s_qm[lane]);
+          const int nroot = drain_one(lane, fp, op, wp, racc);
           tris += nroot > 0;
           rooted += nroot;
         }
@@ -466,7 +486,7 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
           const int ka = (int)(G.row_ptr[a + 1] - ra);
           const uint8_t fa = C.flags[a];
           const int oa = C.orig[a];
-          const double wa = WEIGHTED ? C.w[a] : 0.0;
+          const double wa = (WEIGHTED || ADJ) ? C.w[a] : 0.0;
           if (lane == 0) probes += (unsigned long long)ka;
           for (int j = lane; j < ka; j += 32) {
             const unsigned long long r = G.rec[ra + j];
@@ -477,9 +497,9 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
                   ADJ ? tri_grad(X, fp, op, wp, fa, oa, wa, C.flags[c], C.orig[c], C.w[c], mpa,
                                  rec_meta(rowp[y]), rec_meta(r), racc, &g_lo[a], &g_hi[a], &g_lo[c],
                                  &g_hi[c])
-                      : tri_bin<WEIGHTED>(X, fp, op, wp, fa, oa, wa, C.flags[c], C.orig[c],
-                                          WEIGHTED ? C.w[c] : 0.0, mpa, rec_meta(rowp[y]),
-                                          rec_meta(r));
+                      : tri_bin<WEIGHTED, COUNTS>(X, fp, op, wp, fa, oa, wa, C.flags[c], C.orig[c],
+                                                  WEIGHTED ? C.w[c] : 0.0, mpa, rec_meta(rowp[y]),
+                                                  rec_meta(r));
               tris += nroot > 0;
               rooted += nroot;
             }
@@ -506,10 +526,14 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
   if (SHIST) {
     __syncthreads();
     for (int k = threadIdx.x; k < nh; k += blockDim.x) {
-      const unsigned long long v = X.cnt[k];
-      if (v) {
-        atomicAdd(&g_cnt[k], v);
-        if (WEIGHTED) fix_merge(&g_fix[k], &g_fix[nh + k], X.lo[k], X.lo[nh + k]);
+      if (COUNTS) {
+        const unsigned long long v = X.cnt[k];
+        if (v) atomicAdd(&g_cnt[k], v);
+      }
+      if (WEIGHTED) {
+        const unsigned long long lo = X.lim[k], hi = X.lim[nh + k];
+        if (lo) atomicAdd(&g_lim[k], lo);
+        if (hi) atomicAdd(&g_lim[nh + k], hi);
       }
     }
   }
@@ -518,34 +542,41 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
 }  // namespace
 
 // Warps per block: as many as fit in shared memory (at most 32).
-static int tri3_warps(const TriParams& T, bool weighted, bool shist, bool adj = false) {
+static int tri3_warps(const TriParams& T, bool weighted, bool counts, bool shist, bool adj = false) {
   const int nh = T.ncfg * T.nmu * 4;
   int nw = kTriMaxWarps;
-  while (nw > 1 && tri_layout(nh, T.nmu, T.nbins, T.cap, shist, weighted, nw, adj).total > kSmemLimit)
+  while (nw > 1 &&
+         tri_layout(nh, T.nmu, T.nbins, T.cap, shist, weighted, counts, nw, adj).total > kSmemLimit)
     nw -= 1;
   return nw;
 }
 
-size_t tri3_smem_bytes(const TriParams& T, bool weighted) {
+static bool tri3_shist(int nh, bool weighted, bool counts) {
+  return (size_t)nh * 8 * ((counts ? 1 : 0) + (weighted ? 2 : 0)) <= kMaxHistSmem;
+}
+
+size_t tri3_smem_bytes(const TriParams& T, bool weighted, bool counts) {
   const int nh = T.ncfg * T.nmu * 4;
-  const bool shist = (size_t)nh * 8 * (weighted ? 3 : 1) <= kMaxHistSmem;
-  return tri_layout(nh, T.nmu, T.nbins, T.cap, shist, weighted, tri3_warps(T, weighted, shist)).total;
+  const bool shist = tri3_shist(nh, weighted, counts);
+  return tri_layout(nh, T.nmu, T.nbins, T.cap, shist, weighted, counts,
+                    tri3_warps(T, weighted, counts, shist))
+      .total;
 }
 
 void launch_tri3(const DevCatalog& C, const CSRView& G, const TriParams& T, bool weighted,
-                 unsigned long long* g_cnt, unsigned long long* g_fix, double fscale,
+                 bool counts, unsigned long long* g_cnt, unsigned long long* g_lim,
                  unsigned long long* stats, int* work, cudaStream_t s) {
   if (C.n <= 0) return;
+  if (!weighted) counts = true;
   const int nh = T.ncfg * T.nmu * 4;
-  const bool shist = (size_t)nh * 8 * (weighted ? 3 : 1) <= kMaxHistSmem;
-  const int nw = tri3_warps(T, weighted, shist);
-  const TriLayout L = tri_layout(nh, T.nmu, T.nbins, T.cap, shist, weighted, nw);
-  const size_t smem = L.total;
+  const bool shist = tri3_shist(nh, weighted, counts);
+  const int nw = tri3_warps(T, weighted, counts, shist);
+  const size_t smem = tri_layout(nh, T.nmu, T.nbins, T.cap, shist, weighted, counts, nw).total;
   if (smem > kSmemLimit) throw Error{-2, "3PCF: per-warp shared memory exceeds the SM limit"};
   GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));
-#define GR_TRI_LAUNCH(W, S)                                                                   \
+#define GR_TRI_LAUNCH(W, K, S)                                                                \
   do {                                                                                        \
-    auto kfn = tri3_kernel<W, S, false>;                                                             \
+    auto kfn = tri3_kernel<W, K, S, false>;                                                   \
     GR_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
                                      (int)smem));                                             \
     int per_sm = 0;                                                                           \
@@ -554,13 +585,15 @@ void launch_tri3(const DevCatalog& C, const CSRView& G, const TriParams& T, bool
     int64_t blocks = (int64_t)per_sm * 148;                                                   \
     const int64_t need = ((int64_t)C.n + nw * kChunk - 1) / (nw * kChunk);                    \
     if (blocks > need) blocks = need;                                                         \
-    kfn<<<(unsigned)blocks, nw * 32, smem, s>>>(C, G, T, g_cnt, g_fix, fscale, stats, work,    \
-                                                nullptr, nullptr, 0.0, nullptr, nullptr);     \
+    kfn<<<(unsigned)blocks, nw * 32, smem, s>>>(C, G, T, g_cnt, g_lim, stats, work, nullptr,  \
+                                                nullptr, 0.0, nullptr, nullptr);              \
   } while (0)
-  if (weighted) {
-    if (shist) GR_TRI_LAUNCH(true, true); else GR_TRI_LAUNCH(true, false);
+  if (weighted && counts) {
+    if (shist) GR_TRI_LAUNCH(true, true, true); else GR_TRI_LAUNCH(true, true, false);
+  } else if (weighted) {
+    if (shist) GR_TRI_LAUNCH(true, false, true); else GR_TRI_LAUNCH(true, false, false);
   } else {
-    if (shist) GR_TRI_LAUNCH(false, true); else GR_TRI_LAUNCH(false, false);
+    if (shist) GR_TRI_LAUNCH(false, true, true); else GR_TRI_LAUNCH(false, true, false);
   }
 #undef GR_TRI_LAUNCH
   GR_CHECK_LAUNCH();
@@ -571,11 +604,11 @@ void launch_adj3(const DevCatalog& C, const CSRView& G, const TriParams& T, cons
                  unsigned long long* g_hi, unsigned long long* stats, int* work, cudaStream_t s) {
   if (C.n <= 0) return;
   const int nh = T.ncfg * T.nmu * 4;
-  const int nw = tri3_warps(T, true, false, true);
-  const size_t smem = tri_layout(nh, T.nmu, T.nbins, T.cap, false, true, nw, true).total;
+  const int nw = tri3_warps(T, false, false, false, true);
+  const size_t smem = tri_layout(nh, T.nmu, T.nbins, T.cap, false, false, false, nw, true).total;
   if (smem > kSmemLimit) throw Error{-2, "3PCF adjoint: shared memory exceeds the SM limit"};
   GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));
-  auto kfn = tri3_kernel<true, false, true>;
+  auto kfn = tri3_kernel<false, false, false, true>;
   GR_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nw * 32, smem));
@@ -583,8 +616,8 @@ void launch_adj3(const DevCatalog& C, const CSRView& G, const TriParams& T, cons
   int64_t blocks = (int64_t)per_sm * 148;
   const int64_t need = ((int64_t)C.n + nw * kChunk - 1) / (nw * kChunk);
   if (blocks > need) blocks = need;
-  kfn<<<(unsigned)blocks, nw * 32, smem, s>>>(C, G, T, nullptr, nullptr, 0.0, stats, work, cot2,
-                                              cot3, gscale, g_lo, g_hi);
+  kfn<<<(unsigned)blocks, nw * 32, smem, s>>>(C, G, T, nullptr, nullptr, stats, work, cot2, cot3,
+                                              gscale, g_lo, g_hi);
   GR_CHECK_LAUNCH();
 }
 

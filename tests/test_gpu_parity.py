@@ -208,3 +208,25 @@ def test_log_bins(gpu_ctx, oracle, query):
         _check_sums(gpu_ctx.count_2pcf(), G.pcf2(w, cat.n_data))
     else:
         _check_sums(gpu_ctx.count_3pcf(), G.pcf3(w, cat.n_data))
+
+
+def test_3pcf_without_counts_and_skewed_weights(gpu_ctx, oracle):
+    """counts=False gives the same sums (the integer counts are not the
+    reference's output); few galaxies against many randoms (weights 30x
+    apart) keep 1e-12 because each random-count category has its own
+    fixed-point scale."""
+    cat, _, sp = _cat("c2_3pcf", 0.02)
+    keep = np.ones(cat.n, bool)
+    keep[:cat.n_data] = np.random.default_rng(8).random(cat.n_data) < 0.1
+    xyz = cat.xyz[keep]
+    nd = int(keep[:cat.n_data].sum())
+    w = catalogs.normalise(np.random.default_rng(9).lognormal(0, 0.5, len(xyz)), nd, len(xyz) - nd)
+    gpu_ctx.set_catalog(xyz, w, nd)
+    gpu_ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
+    full = gpu_ctx.count_3pcf()
+    lean = gpu_ctx.count_3pcf(counts=False)
+    assert "counts" not in lean
+    assert np.array_equal(full["catsum"], lean["catsum"])
+    assert np.array_equal(full["N2"], lean["N2"]) and np.array_equal(full["N3"], lean["N3"])
+    ref = oracle.Graph(xyz, sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"]).pcf3(w, nd)
+    _check_sums(full, ref)
