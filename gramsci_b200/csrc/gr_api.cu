@@ -114,6 +114,17 @@ void make_pair_params(PairParams& P, double rmin, double rmax, int nbins, int nm
   } else {
     P.rmin2_lo = -1.0f;
   }
+  // inner bounds of the certain-edge band for the membership-only test
+  double in_hi = rmax - 2.0 * d0;
+  if (in_hi > 0.0) {
+    in_hi = in_hi * in_hi * (1.0 - 16.0 * u);
+    P.rmax2_lo = std::nextafter((float)in_hi, -std::numeric_limits<float>::infinity());
+  } else {
+    P.rmax2_lo = -1.0f;
+  }
+  double in_lo = rmin + 2.0 * d0;
+  in_lo = in_lo * in_lo * (1.0 + 16.0 * u);
+  P.rmin2_hi = std::nextafter((float)in_lo, std::numeric_limits<float>::infinity());
   P.f_rmin = (float)rmin;
   P.f_inv_dr = (float)P.inv_dr;
   P.f_mu_scale = (float)P.mu_scale;
@@ -714,7 +725,7 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
   T.normal = c->normal_dev.p;
   make_rank_tables(T.rank, c->nbins, 3);
   for (int nr = 0; nr < 4; ++nr) T.fscale[nr] = fscale[nr];
-  CSRView G{c->csr.row_ptr.p, c->csr.rec.p, c->csr.deg_full.p};
+  const CSRView G = c->csr.view();
   cudaEvent_t q0;
   GR_CUDA_TRY(cudaEventCreate(&q0));
   GR_CUDA_TRY(cudaEventRecord(q0, s));
@@ -820,7 +831,7 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   Q.tetra = tetra ? 1 : 0;
   Q.cap = round_cap((int64_t)gst[2], 32, 1024);
   make_rank_tables(Q.rank, nb, 4);
-  CSRView G{c->csr.row_ptr.p, c->csr.rec.p, c->csr.deg_full.p};
+  const CSRView G = c->csr.view();
   cudaEvent_t q0;
   GR_CUDA_TRY(cudaEventCreate(&q0));
   GR_CUDA_TRY(cudaEventRecord(q0, s));
@@ -977,6 +988,7 @@ int gr_graph_save(gr_ctx* c, const char* path) {
     build_csr(c);
   }
   cudaStream_t s = c->stream();
+  c->csr.compact(s);
   const int64_t n = c->n, E = c->csr.n_edges;
   std::vector<int64_t> rp(n + 1);
   std::vector<unsigned long long> rec(E);
@@ -1089,17 +1101,23 @@ int gr_graph_load(gr_ctx* c, const char* path) {
   G.max_deg = H.max_deg;
   G.rechecks = H.rechecks;
   G.candidates = H.candidates;
-  G.row_ptr.reserve(n + 1);
-  G.rec.reserve(E + 1);
+  // rows go to the scratch layout (rstart = row offsets, deg_up = lengths)
+  std::vector<int> up(n + 1, 0);
+  for (int64_t p = 0; p < n; ++p) up[p] = (int)(rp[p + 1] - rp[p]);
+  G.rstart.reserve(n + 1);
+  G.deg_up.reserve(n + 1);
+  G.scratch.reserve(E + 1);
   G.deg_full.reserve(n + 1);
   G.stats.reserve(4);
   unsigned long long st[4] = {(unsigned long long)H.rechecks, (unsigned long long)H.candidates,
                               (unsigned long long)H.max_deg, 0ull};
-  GR_CUDA_TRY(cudaMemcpyAsync(G.row_ptr.p, rp.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, s));
+  GR_CUDA_TRY(cudaMemcpyAsync(G.rstart.p, rp.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, s));
+  GR_CUDA_TRY(cudaMemcpyAsync(G.deg_up.p, up.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, s));
   if (E > 0)
-    GR_CUDA_TRY(cudaMemcpyAsync(G.rec.p, rec.data(), sizeof(unsigned long long) * E, cudaMemcpyHostToDevice, s));
+    GR_CUDA_TRY(cudaMemcpyAsync(G.scratch.p, rec.data(), sizeof(unsigned long long) * E, cudaMemcpyHostToDevice, s));
   if (n > 0)
     GR_CUDA_TRY(cudaMemcpyAsync(G.deg_full.p, deg.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+  G.compacted = false;
   GR_CUDA_TRY(cudaMemcpyAsync(G.stats.p, st, sizeof(st), cudaMemcpyHostToDevice, s));
   GR_CUDA_TRY(cudaStreamSynchronize(s));
   c->csr_valid = true;
@@ -1127,6 +1145,7 @@ int gr_graph_export(gr_ctx* c, int64_t* row_ptr, int32_t* col, uint8_t* bin, uin
     build_csr(c);
   }
   cudaStream_t s = c->stream();
+  c->csr.compact(s);
   const int64_t n = c->n, E = c->csr.n_edges;
   std::vector<int64_t> rp(n + 1);
   std::vector<int> orig(n);
@@ -1258,7 +1277,7 @@ int gr_adjoint_3pcf(gr_ctx* c, const double* cot2, const double* cot3, double* g
   T.cap = round_cap(c->csr.max_deg, 32, 256);
   T.normal = c->normal_dev.p;
   make_rank_tables(T.rank, c->nbins, 3);
-  CSRView G{c->csr.row_ptr.p, c->csr.rec.p, c->csr.deg_full.p};
+  const CSRView G = c->csr.view();
   std::memset(&c->st, 0, sizeof(c->st));
   launch_adj3(c->index.view(), G, T, c->cot.p, cot3 ? c->cot.p + nc : nullptr, gscale, c->gfix.p,
               c->gfix.p + n, c->stats.p, c->work.p, s);

@@ -2,11 +2,11 @@
 // its kd-tree range queries (src/kdtree2.F90:1204-1363), distance sort and
 // O(k^2) id sort (src/sorting_module.F90:36-47).
 //
-// Two passes over the half stencil of every cell (warp per cell, candidates
-// staged in shared memory, lanes over candidate labels): a count pass giving
-// the upper degrees, an exclusive scan giving row offsets, and a fill pass
-// writing each row.  Candidates are
-// visited in increasing label order and compacted with a warp ballot, so
+// One pass over the half stencil of every cell (warp per cell, candidates
+// staged in shared memory, lanes over candidate labels) writes each row to a
+// per-cell scratch region; an exclusive scan of the upper degrees gives the
+// row offsets and a compaction kernel moves the rows into place.  Candidates
+// are visited in increasing label order and compacted with a warp ballot, so
 // rows come out sorted without a sort.  Each undirected edge is stored once,
 // in the row of its smaller label, with the bins seen from both ends.
 #include "gr_index.cuh"
@@ -31,26 +31,80 @@ __device__ __forceinline__ bool pair_edge(const DevCatalog& C, const PairParams&
   return edge_f64(C.posd[p], C.posd[q], P, bin, muf, mur);
 }
 
-// Warp-per-cell sweep shared by the count and fill passes.  A warp takes a
-// cell, computes the forward candidate ranges once for all its points and
-// stages the candidates (labels and float4 positions) in shared memory in
-// tiles of kCellTile.  Every root p of the cell is then tested against the
-// staged candidates with label > p, lanes over candidates.  FILL=false
-// counts upper degrees (and full degrees); FILL=true writes the rows, with
-// a per-row cursor carried across tiles in `cursor`.
-template <bool F32, bool FILL>
-__global__ void __launch_bounds__(kGraphThreads) csr_cells_kernel(
+// One pass over the half stencil of every cell.  A warp takes a cell,
+// computes its forward candidate ranges once for all its points and stages
+// the candidates (labels and float4 positions) in shared memory in tiles of
+// kCellTile.  Every root p of the cell is tested against the staged
+// candidates with label > p, lanes over candidates, with the cheap
+// membership test (FP32 separation, FP64 only inside the guard band at rmin
+// and rmax).  Edges are compacted with a ballot into a per-warp queue in
+// label order, each with its final position; the queue is drained 32 at a
+// time, so the radial and mu bins (the costly part) are computed with every
+// lane busy.  Rows are written to a scratch area in which each cell owns its
+// candidate bound (prefix sums of cell_bound_kernel); root p (local index i)
+// of a cell with T forward candidates owns the slots base + i*T - i(i+1)/2
+// onward.  compact() moves the rows to CSR order when a caller needs it.
+constexpr int kQueue = 64;
+
+// Candidate bound of every cell (scratch slots its rows may need): a cell
+// with n points and T forward candidates gives root i at most T - i - 1
+// edges, n*T - n(n+1)/2 in all.
+__global__ void cell_bound_kernel(DevCatalog C, int64_t* __restrict__ bound) {
+  const int ncell = (int)C.grid.ncell;
+  for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < ncell; cell += gridDim.x * blockDim.x) {
+    const int cb = C.cell_start[cell], ce = C.cell_start[cell + 1];
+    int64_t b = 0;
+    if (ce > cb) {
+      Ranges R;
+      GridParams g;
+      const int* cs;
+      int lkey;
+      cell_grid(C, cell, g, cs, lkey);
+      forward_ranges(cb - 1, lkey, g, cs, R);
+      int64_t total = 0;
+      for (int k = 0; k < R.n; ++k) total += R.end[k] - R.beg[k];
+      const int64_t nloc = ce - cb;
+      b = nloc * total - nloc * (nloc + 1) / 2;
+    }
+    bound[cell] = b;
+  }
+}
+
+template <bool F32>
+__global__ void __launch_bounds__(kGraphThreads) csr_fill_kernel(
     DevCatalog C, PairParams P, int* __restrict__ deg_up, int* __restrict__ deg_full,
-    const int64_t* __restrict__ row_ptr, unsigned long long* __restrict__ rec,
-    int* __restrict__ cursor, unsigned long long* __restrict__ stats, int* __restrict__ work) {
+    int64_t* __restrict__ rstart, const int64_t* __restrict__ cbase,
+    unsigned long long* __restrict__ scratch, int64_t cap, unsigned long long* __restrict__ ctl,
+    unsigned long long* __restrict__ stats, int* __restrict__ work) {
   __shared__ float4 s_pos[kGraphWarps][kCellTile];
   __shared__ int s_lab[kGraphWarps][kCellTile];
+  __shared__ long long s_qpos[kGraphWarps][kQueue];  // scratch slot, -1 when out of room
+  __shared__ int s_qp[kGraphWarps][kQueue];          // root label
+  __shared__ unsigned short s_qf[kGraphWarps][kQueue];  // tile index of the neighbour
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
-  unsigned long long rechecks = 0, cands = 0;
+  unsigned long long rechecks = 0, cands = 0, disagree = 0, edges = 0;
   unsigned long long maxdeg = 0;
   const int ncell = (int)C.grid.ncell;
+
+  // bins of one queued edge, written to its slot
+  auto drain_one = [&](int e) {
+    const int p = s_qp[wib][e];
+    const int f = s_qf[wib][e];
+    const long long pos = s_qpos[wib][e];
+    const int q = s_lab[wib][f];
+    int b = 1, mf = 1, mr = 1;
+    if (!pair_edge<F32, true>(C, P, p, q, C.pos4[p], s_pos[wib][f], b, mf, mr, rechecks)) {
+      // the membership test and the binning disagree: reported, never expected
+      disagree++;
+      b = 1;
+      mf = 1;
+      mr = 1;
+    }
+    if (pos >= 0) scratch[pos] = ((unsigned long long)pack_meta(b, mf, mr) << 32) | (uint32_t)q;
+  };
+
   for (;;) {
     int cell = 0;
     if (lane == 0) cell = atomicAdd(work, 1);
@@ -72,6 +126,12 @@ __global__ void __launch_bounds__(kGraphThreads) csr_cells_kernel(
       pre[k] = total;
       if (k < R.n) total += R.end[k] - R.beg[k];
     }
+    // the cell's scratch slots: [cbase[cell], cbase[cell + 1]); root i
+    // has total - i - 1 candidates
+    const long long base = cbase[cell];
+    const bool room = cbase[cell + 1] <= cap;
+    if (!room && lane == 0) atomicMax(&ctl[1], 1ull);
+    int qn = 0;
     for (int t0 = 0; t0 < total; t0 += kCellTile) {
       const int tn = min(kCellTile, total - t0);
       const bool last_tile = t0 + kCellTile >= total;
@@ -83,58 +143,101 @@ __global__ void __launch_bounds__(kGraphThreads) csr_cells_kernel(
       }
       __syncwarp();
       for (int p = cb; p < ce; ++p) {
-        // flattened index p - cb is p itself (range 0 starts at cb)
-        const int fstart = max(0, p - cb + 1 - t0);
+        // flattened index of p is p - cb (range 0 starts at cb)
+        const int i = p - cb;
+        const int fstart = max(0, i + 1 - t0);
         if (fstart >= tn) continue;
         const float4 pi = C.pos4[p];
-        int off = 0;
-        int64_t rowb = 0, rowe = 0;
-        if (FILL) {
-          rowb = row_ptr[p];
-          rowe = row_ptr[p + 1];
-          off = (t0 == 0) ? 0 : cursor[p];
-        }
-        int cnt = 0;
+        const long long rs = base + (long long)i * total - (long long)i * (i + 1) / 2;
+        int off = (t0 == 0) ? 0 : deg_up[p];  // edges of p in earlier tiles
         for (int f0 = fstart; f0 < tn; f0 += 32) {
           const int f = f0 + lane;
           bool e = false;
-          int q = 0, b = 0, mf = 0, mr = 0;
           if (f < tn) {
-            q = s_lab[wib][f];
-            e = pair_edge<F32, FILL>(C, P, p, q, pi, s_pos[wib][f], b, mf, mr, rechecks);
-            if (!FILL && e) atomicAdd(&deg_full[q], 1);
+            const int q = s_lab[wib][f];
+            int b, mf, mr;
+            int r = F32 ? member_f32(pi, s_pos[wib][f], P) : 2;
+            if (r == 2) {
+              rechecks++;
+              r = edge_f64(C.posd[p], C.posd[q], P, b, mf, mr) ? 1 : 0;
+            }
+            e = r == 1;
+            if (e) atomicAdd(&deg_full[q], 1);
           }
           const unsigned m = __ballot_sync(0xffffffffu, e);
-          if (FILL && e) {
-            const int64_t pos = rowb + off + __popc(m & lt);
-            if (pos < rowe)  // the count pass decided the same edges
-              rec[pos] = ((unsigned long long)pack_meta(b, mf, mr) << 32) | (uint32_t)q;
+          if (e) {
+            const int rank = __popc(m & lt);
+            s_qp[wib][qn + rank] = p;
+            s_qf[wib][qn + rank] = (unsigned short)f;
+            s_qpos[wib][qn + rank] = room ? rs + off + rank : -1ll;
           }
           off += __popc(m);
-          cnt += __popc(m);
+          qn += __popc(m);
+          if (qn >= 32) {
+            __syncwarp();
+            drain_one(qn - 32 + lane);
+            qn -= 32;
+            __syncwarp();
+          }
         }
         if (lane == 0) {
-          if (FILL) {
-            if (!last_tile) cursor[p] = off;
-          } else {
-            const int d = deg_up[p] + cnt;
-            deg_up[p] = d;
-            atomicAdd(&deg_full[p], cnt);
-            if (last_tile) maxdeg = maxdeg > (unsigned long long)d ? maxdeg : (unsigned long long)d;
-            cands += (unsigned long long)(tn - fstart);
+          deg_up[p] = off;
+          rstart[p] = rs;
+          cands += (unsigned long long)(tn - fstart);
+          if (last_tile) {
+            atomicAdd(&deg_full[p], off);
+            edges += (unsigned long long)off;
+            maxdeg = maxdeg > (unsigned long long)off ? maxdeg : (unsigned long long)off;
           }
         }
         __syncwarp();
       }
+      // the tile's staged candidates are about to be replaced
+      if (lane < qn) drain_one(lane);
+      qn = 0;
+      __syncwarp();
     }
   }
-  if (!FILL) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) rechecks += __shfl_xor_sync(0xffffffffu, rechecks, o);
-    if (lane == 0) {
-      if (rechecks) atomicAdd(&stats[0], rechecks);
-      if (cands) atomicAdd(&stats[1], cands);
-      if (maxdeg) atomicMax(&stats[2], maxdeg);
+  for (int o = 16; o > 0; o >>= 1) {
+    rechecks += __shfl_xor_sync(0xffffffffu, rechecks, o);
+    disagree += __shfl_xor_sync(0xffffffffu, disagree, o);
+  }
+  if (lane == 0) {
+    if (rechecks) atomicAdd(&stats[0], rechecks);
+    if (cands) atomicAdd(&stats[1], cands);
+    if (maxdeg) atomicMax(&stats[2], maxdeg);
+    if (disagree) atomicAdd(&ctl[2], disagree);
+    if (edges) atomicAdd(&ctl[3], edges);
+  }
+}
+
+// Rows from the scratch area to CSR order.  A warp takes 32 consecutive
+// roots (their lengths and offsets in one coalesced load) and copies the
+// rows one after the other, lanes over records.
+__global__ void csr_compact_kernel(int64_t n, const int* __restrict__ deg_up,
+                                   const int64_t* __restrict__ rstart,
+                                   const int64_t* __restrict__ row_ptr,
+                                   const unsigned long long* __restrict__ scratch,
+                                   unsigned long long* __restrict__ rec) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t p0 = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; p0 < n;
+       p0 += warps * 32) {
+    const int64_t p = p0 + lane;
+    int d = 0;
+    int64_t src = 0, dst = 0;
+    if (p < n) {
+      d = deg_up[p];
+      src = rstart[p];
+      dst = row_ptr[p];
+    }
+#pragma unroll 4
+    for (int r = 0; r < 32; ++r) {
+      const int dr = __shfl_sync(0xffffffffu, d, r);
+      const int64_t sr = __shfl_sync(0xffffffffu, src, r);
+      const int64_t tr = __shfl_sync(0xffffffffu, dst, r);
+      for (int j = lane; j < dr; j += 32) rec[tr + j] = scratch[sr + j];
     }
   }
 }
@@ -154,45 +257,75 @@ void UpperCSR::build(const DevCatalog& C, const PairParams& P, cudaStream_t s) {
   launches = 0;
   deg_up.reserve(n + 1);
   deg_full.reserve(n + 1);
-  cursor.reserve(n + 1);
-  row_ptr.reserve(n + 1);
+  rstart.reserve(n + 1);
   stats.reserve(4);
+  ctl.reserve(4);
   work.reserve(2);
-  GR_CUDA_TRY(cudaMemsetAsync(deg_up.p, 0, sizeof(int) * (n + 1), s));
-  GR_CUDA_TRY(cudaMemsetAsync(deg_full.p, 0, sizeof(int) * (n + 1), s));
-  GR_CUDA_TRY(cudaMemsetAsync(stats.p, 0, sizeof(unsigned long long) * 4, s));
-  GR_CUDA_TRY(cudaMemsetAsync(work.p, 0, sizeof(int) * 2, s));
+  // scratch: kept from earlier builds (grown to the candidate bound when short)
+  if (scratch.n < (size_t)(64 * n + 1024)) scratch.reserve((size_t)(64 * n + 1024));
   const int blocks = graph_blocks(C.grid.ncell);
-  if (n > 0) {
-    if (P.f32)
-      csr_cells_kernel<true, false><<<blocks, kGraphThreads, 0, s>>>(
-          C, P, deg_up.p, deg_full.p, nullptr, nullptr, nullptr, stats.p, work.p);
-    else
-      csr_cells_kernel<false, false><<<blocks, kGraphThreads, 0, s>>>(
-          C, P, deg_up.p, deg_full.p, nullptr, nullptr, nullptr, stats.p, work.p);
-    launches++;
+  const int64_t ncell = C.grid.ncell;
+  cbound.reserve(ncell + 1);
+  cbase.reserve(ncell + 2);
+  if (ncell > 0) {
+    const int bb = (int)std::min<int64_t>((ncell + 255) / 256, 148 * 8);
+    cell_bound_kernel<<<bb, 256, 0, s>>>(C, cbound.p);
     GR_CHECK_LAUNCH();
+    scan_i64(cbound.p, cbase.p, ncell, s, scan_tmp);
+    launches += 4;
   }
-  scan_i32_to_i64(deg_up.p, row_ptr.p, n, s, scan_tmp);
-  launches += 3;
-  GR_CUDA_TRY(cudaMemcpyAsync(&n_edges, row_ptr.p + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-  unsigned long long hs[3] = {0, 0, 0};
-  GR_CUDA_TRY(cudaMemcpyAsync(hs, stats.p, sizeof(hs), cudaMemcpyDeviceToHost, s));
-  GR_CUDA_TRY(cudaStreamSynchronize(s));
+  unsigned long long hc[4] = {0, 0, 0, 0}, hs[3] = {0, 0, 0};
+  int64_t need = 0;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    GR_CUDA_TRY(cudaMemsetAsync(deg_up.p, 0, sizeof(int) * (n + 1), s));
+    GR_CUDA_TRY(cudaMemsetAsync(rstart.p, 0, sizeof(int64_t) * (n + 1), s));
+    GR_CUDA_TRY(cudaMemsetAsync(deg_full.p, 0, sizeof(int) * (n + 1), s));
+    GR_CUDA_TRY(cudaMemsetAsync(stats.p, 0, sizeof(unsigned long long) * 4, s));
+    GR_CUDA_TRY(cudaMemsetAsync(ctl.p, 0, sizeof(unsigned long long) * 4, s));
+    GR_CUDA_TRY(cudaMemsetAsync(work.p, 0, sizeof(int) * 2, s));
+    if (n > 0) {
+      const int64_t cap = (int64_t)scratch.n;
+      if (P.f32)
+        csr_fill_kernel<true><<<blocks, kGraphThreads, 0, s>>>(C, P, deg_up.p, deg_full.p, rstart.p,
+                                                               cbase.p, scratch.p, cap, ctl.p, stats.p,
+                                                               work.p);
+      else
+        csr_fill_kernel<false><<<blocks, kGraphThreads, 0, s>>>(C, P, deg_up.p, deg_full.p, rstart.p,
+                                                                cbase.p, scratch.p, cap, ctl.p, stats.p,
+                                                                work.p);
+      launches++;
+      GR_CHECK_LAUNCH();
+    }
+    GR_CUDA_TRY(cudaMemcpyAsync(hc, ctl.p, sizeof(hc), cudaMemcpyDeviceToHost, s));
+    GR_CUDA_TRY(cudaMemcpyAsync(hs, stats.p, sizeof(hs), cudaMemcpyDeviceToHost, s));
+    if (ncell > 0)
+      GR_CUDA_TRY(cudaMemcpyAsync(&need, cbase.p + ncell, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    GR_CUDA_TRY(cudaStreamSynchronize(s));
+    if (hc[1] == 0) break;
+    // out of room: grow to the exact bound and run again
+    scratch.reserve((size_t)need + 1024);
+  }
+  if (hc[1] != 0) throw Error{-2, "CSR build: scratch overflow after growing"};
+  if (hc[2] != 0) throw Error{-3, "CSR build: FP32 membership and FP64 binning disagree"};
+  n_edges = (int64_t)hc[3];
   rechecks = (int64_t)hs[0];
   candidates = (int64_t)hs[1];
   max_deg = (int64_t)hs[2];
-  rec.reserve(n_edges);
+  compacted = false;
+}
+
+void UpperCSR::compact(cudaStream_t s) {
+  if (compacted) return;
+  row_ptr.reserve(n + 1);
+  scan_i32_to_i64(deg_up.p, row_ptr.p, n, s, scan_tmp);
+  rec.reserve(n_edges + 1);
   if (n > 0 && n_edges > 0) {
-    if (P.f32)
-      csr_cells_kernel<true, true><<<blocks, kGraphThreads, 0, s>>>(
-          C, P, nullptr, nullptr, row_ptr.p, rec.p, cursor.p, stats.p, work.p + 1);
-    else
-      csr_cells_kernel<false, true><<<blocks, kGraphThreads, 0, s>>>(
-          C, P, nullptr, nullptr, row_ptr.p, rec.p, cursor.p, stats.p, work.p + 1);
-    launches++;
+    const int64_t groups = (n + 31) / 32;
+    const int blocks = (int)std::min<int64_t>((groups + 7) / 8, 148 * 16);
+    csr_compact_kernel<<<blocks, 256, 0, s>>>(n, deg_up.p, rstart.p, row_ptr.p, scratch.p, rec.p);
     GR_CHECK_LAUNCH();
   }
+  compacted = true;
 }
 
 }  // namespace gr

@@ -402,6 +402,12 @@ size_t scan_tmp_need(int64_t n) {
 
 }  // namespace
 
+void scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s, DevBuf<int64_t>& tmp) {
+  size_t need = scan_tmp_need(n);
+  if (tmp.n < need) tmp.reserve(need);
+  scan_impl<int64_t>(in, out, n, s, tmp, 0);
+}
+
 void scan_i32_to_i64(const int* in, int64_t* out, int64_t n, cudaStream_t s, DevBuf<int64_t>& tmp) {
   size_t need = scan_tmp_need(n);
   if (tmp.n < need) tmp.reserve(need);

@@ -35,23 +35,31 @@ void narrow_kernel_launch(const int64_t* in, int* out, int64_t n, cudaStream_t s
 // Upper adjacency: row p lists the neighbours q > p (internal labels) of the
 // (rmin, rmax) graph in increasing label order, with packed bin / mu
 // metadata.  deg_full[p] is the full degree (the reference's row length nn).
+// Rows live in `scratch` at rstart[p] with deg_up[p] records (per-cell
+// candidate-bound layout, with gaps); compact() also lays them out as a
+// classic CSR (row_ptr, rec) for export and persistence.
+struct CSRView {
+  const int64_t* start;           // first record of row p
+  const int* len;                 // records in row p
+  const unsigned long long* rec;  // (meta << 32) | neighbour label
+  const int* deg_full;
+};
+
 struct UpperCSR {
   int64_t n = 0, n_edges = 0;  // n_edges counts upper (undirected) edges
   int64_t max_deg = 0;         // largest upper degree
   int64_t rechecks = 0, candidates = 0;
   int launches = 0;
-  DevBuf<int> deg_up, deg_full, cursor, work;
-  DevBuf<int64_t> row_ptr, scan_tmp;
-  DevBuf<unsigned long long> rec;    // (meta << 32) | neighbour label
-  DevBuf<unsigned long long> stats;  // [0] FP64 rechecks, [1] candidates, [2] max upper degree
-
+  bool compacted = false;      // row_ptr / rec hold the current rows
+  DevBuf<int> deg_up, deg_full, work;
+  DevBuf<int64_t> row_ptr, scan_tmp, rstart, cbound, cbase;
+  DevBuf<unsigned long long> rec;      // compacted rows (compact())
+  DevBuf<unsigned long long> scratch;  // rows as built: rstart / deg_up
+  DevBuf<unsigned long long> stats;    // [0] FP64 rechecks, [1] candidates, [2] max upper degree
+  DevBuf<unsigned long long> ctl;      // [1] out of room, [2] disagreements, [3] edges
   void build(const DevCatalog& C, const PairParams& P, cudaStream_t s);
-};
-
-struct CSRView {
-  const int64_t* row_ptr;
-  const unsigned long long* rec;  // (meta << 32) | neighbour label
-  const int* deg_full;
+  void compact(cudaStream_t s);
+  CSRView view() const { return CSRView{rstart.p, deg_up.p, scratch.p, deg_full.p}; }
 };
 
 __device__ __forceinline__ int rec_col(unsigned long long r) { return (int)(uint32_t)r; }

@@ -64,6 +64,8 @@ struct PairParams {
   float f_rmin, f_inv_dr, f_mu_scale;
   float rmax2_hi;    // d2 >= rmax2_hi: certainly d >= rmax
   float rmin2_lo;    // d2 <= rmin2_lo: certainly d <= rmin (or -1)
+  float rmax2_lo;    // d2 < rmax2_lo: certainly d < rmax (or -1)
+  float rmin2_hi;    // d2 > rmin2_hi: certainly d > rmin
   float tguard;      // |t - nearest integer| below this -> FP64
   float d0;          // bound on |d_f - d_true|
   float eA, eB, mB, eC;  // cosine error model eA/(d-d0) + eB/(|m|-mB) + eC
@@ -183,6 +185,19 @@ __device__ __forceinline__ int classify_f32(const float4 pi, const float4 pj, co
     mur = 1;
   }
   return 1;
+}
+
+// Membership only (no bins) from the FP32 squared separation: 0 not an
+// edge, 1 an edge, 2 undecided (inside the guard band at rmin or rmax:
+// evaluate with edge_f64).
+__device__ __forceinline__ int member_f32(const float4 pi, const float4 pj, const PairParams& P) {
+  const float dx = pj.x - pi.x;
+  const float dy = pj.y - pi.y;
+  const float dz = pj.z - pi.z;
+  const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+  if (d2 >= P.rmax2_hi || d2 <= P.rmin2_lo) return 0;
+  if (d2 > P.rmin2_hi && d2 < P.rmax2_lo) return 1;
+  return 2;
 }
 
 // ---------------------------------------------------------------- cell grid --
@@ -453,5 +468,6 @@ double fix_value(unsigned long long lo, unsigned long long hi, double scale);
 // -------------------------------------------------------------- host launch --
 // Exclusive scan of n int32 values into n+1 int64 values (out[n] = total).
 void scan_i32_to_i64(const int* in, int64_t* out, int64_t n, cudaStream_t s, DevBuf<int64_t>& tmp);
+void scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s, DevBuf<int64_t>& tmp);
 
 }  // namespace gr

@@ -249,8 +249,8 @@ __global__ void __launch_bounds__(kQuadThreads) quad4_kernel(DevCatalog C, CSRVi
   unsigned long long quads = 0, rooted = 0, probes = 0;
 
   for (int p = warp; p < C.n; p += nwarps) {
-    const int64_t b0 = G.row_ptr[p];
-    const int k = (int)(G.row_ptr[p + 1] - b0);
+    const int64_t b0 = G.start[p];
+    const int k = G.len[p];
     if (k < 3 || k > cap) continue;  // rows longer than cap are rejected on the host
     __syncwarp();
     for (int x = lane; x < k; x += 32) {
@@ -258,9 +258,8 @@ __global__ void __launch_bounds__(kQuadThreads) quad4_kernel(DevCatalog C, CSRVi
       int a = rec_col(rr);
       r_col[x] = a;
       r_meta[x] = rec_meta(rr);
-      long long rs = G.row_ptr[a];
-      r_start[x] = rs;
-      r_len[x] = (int)(G.row_ptr[a + 1] - rs);
+      r_start[x] = G.start[a];
+      r_len[x] = G.len[a];
     }
     __syncwarp();
     for (int x = 0; x < k - 2; ++x) {
@@ -286,8 +285,7 @@ __global__ void __launch_bounds__(kQuadThreads) quad4_kernel(DevCatalog C, CSRVi
           x_c[pos] = c;
           x_y[pos] = y;
           x_m[pos] = rec_meta(rr);
-          long long cs = G.row_ptr[c];
-          x_start[pos] = cs;
+          x_start[pos] = G.start[c];
         }
         nx += __popc(msk);
       }
@@ -299,7 +297,7 @@ __global__ void __launch_bounds__(kQuadThreads) quad4_kernel(DevCatalog C, CSRVi
       for (int zb = 0; zb < nx; zb += 32) {
         int z = zb + lane;
         int len = 0;
-        if (z < nx) len = (int)(G.row_ptr[x_c[z] + 1] - x_start[z]);
+        if (z < nx) len = G.len[x_c[z]];
         int incl = len;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {

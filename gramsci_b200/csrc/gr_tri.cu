@@ -28,7 +28,7 @@ namespace {
 
 constexpr int kTriMaxWarps = 32;  // block size is chosen at launch to fit shared memory
 constexpr size_t kSmemLimit = 227 * 1024;
-constexpr int kQueue = 64;   // hit queue entries per warp
+constexpr int kQueue = 96;   // hit queue entries per warp (< 32 left + 64 pushed)
 constexpr int kChunk = 4;    // roots taken per work-counter increment
 constexpr int kCfgTableBins = 16;  // nbins up to which the configuration table is used
 
@@ -336,8 +336,8 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
     if (base_root >= C.n) break;
     const int end_root = min(base_root + kChunk, C.n);
     for (int p = base_root; p < end_root; ++p) {
-      const int64_t b0 = G.row_ptr[p];
-      const int k = (int)(G.row_ptr[p + 1] - b0);
+      const int64_t b0 = G.start[p];
+      const int k = G.len[p];
       if (k < 2) continue;
       const uint8_t fp = C.flags[p];
       const int op = C.orig[p];
@@ -360,8 +360,8 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
             const int a = rec_col(r);
             s_col[x] = a;
             s_meta[x] = rec_meta(r);
-            const long long rs = G.row_ptr[a];
-            const int len = (int)(G.row_ptr[a + 1] - rs);
+            const long long rs = G.start[a];
+            const int len = G.len[a];
             s_rs[x] = rs;
             s_len[x] = len;
             probes += (unsigned long long)len;
@@ -413,45 +413,59 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
           const int tot = __shfl_sync(0xffffffffu, incl, 31);
           const int excl = incl - clen;
           int done = 0;  // compacted rows that ended before the window
-          for (int t0 = 0; t0 < tot; t0 += 32) {
-            const int t = t0 + lane;
-            const int last = incl - 1 - t0;  // window position of the row's last item
-            const unsigned bit = (lane < nrows && last >= 0 && last < 32) ? (1u << last) : 0u;
-            const unsigned ends = __reduce_or_sync(0xffffffffu, bit);
-            const int j = done + __popc(ends & lt);
-            done += __popc(ends);
-            const long long ors = __shfl_sync(0xffffffffu, crs, j & 31);
-            const int oex = __shfl_sync(0xffffffffu, excl, j & 31);
-            const int ox = __shfl_sync(0xffffffffu, cx, j & 31);
-            bool hit = false;
-            int y = 0;
-            uint32_t mac = 0;
-            if (t < tot) {
-              const unsigned long long r = G.rec[ors + (t - oex)];
-              const int off = rec_col(r) - p;
-              mac = rec_meta(r);
-              if (off < kMaxOffset) {
-                uint32_t h = fib_slot((uint32_t)off, lg);
-                for (int it = 0; it < hs; ++it) {
-                  const uint32_t e = s_hkey[h];
-                  if ((e >> 8) == (uint32_t)off) {
-                    hit = true;
-                    y = (int)(e & 0xffu);
-                    break;
+          // two windows of 32 items per iteration: both record loads are in
+          // flight before either is probed
+          for (int t0 = 0; t0 < tot; t0 += 64) {
+            int tw[2], ox[2];
+            long long ridx[2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+              const int w0 = t0 + 32 * u;
+              const int last = incl - 1 - w0;  // window position of the row's last item
+              const unsigned bit = (lane < nrows && last >= 0 && last < 32) ? (1u << last) : 0u;
+              const unsigned ends = __reduce_or_sync(0xffffffffu, bit);
+              const int j = (done + __popc(ends & lt)) & 31;
+              done += __popc(ends);
+              const long long ors = __shfl_sync(0xffffffffu, crs, j);
+              const int oex = __shfl_sync(0xffffffffu, excl, j);
+              ox[u] = __shfl_sync(0xffffffffu, cx, j);
+              tw[u] = w0 + lane;
+              ridx[u] = ors + (tw[u] - oex);
+            }
+            unsigned long long rr[2] = {0ull, 0ull};
+#pragma unroll
+            for (int u = 0; u < 2; ++u)
+              if (tw[u] < tot) rr[u] = G.rec[ridx[u]];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+              bool hit = false;
+              int y = 0;
+              const uint32_t mac = rec_meta(rr[u]);
+              if (tw[u] < tot) {
+                const int off = rec_col(rr[u]) - p;
+                if (off < kMaxOffset) {
+                  uint32_t h = fib_slot((uint32_t)off, lg);
+                  for (int it = 0; it < hs; ++it) {
+                    const uint32_t e = s_hkey[h];
+                    if ((e >> 8) == (uint32_t)off) {
+                      hit = true;
+                      y = (int)(e & 0xffu);
+                      break;
+                    }
+                    if (e == 0u) break;
+                    h = (h + 1) & (uint32_t)(hs - 1);
                   }
-                  if (e == 0u) break;
-                  h = (h + 1) & (uint32_t)(hs - 1);
                 }
               }
+              const unsigned m = __ballot_sync(0xffffffffu, hit);
+              if (hit) {
+                const int pos = qn + __popc(m & lt);
+                s_qm[pos] = mac;
+                s_qxy[pos] = (uint16_t)(ox[u] | (y << 8));
+              }
+              qn += __popc(m);
             }
-            const unsigned m = __ballot_sync(0xffffffffu, hit);
-            if (hit) {
-              const int pos = qn + __popc(m & lt);
-              s_qm[pos] = mac;
-              s_qxy[pos] = (uint16_t)(ox | (y << 8));
-            }
-            qn += __popc(m);
-            if (qn >= 32) {
+            while (qn >= 32) {
               __syncwarp();
               const int nroot = drain_one(qn - 32 + lane, fp, op, wp, racc);
               tris += nroot > 0;
@@ -482,8 +496,8 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
           const unsigned long long ra_rec = rowp[x];
           const int a = rec_col(ra_rec);
           const uint32_t mpa = rec_meta(ra_rec);
-          const int64_t ra = G.row_ptr[a];
-          const int ka = (int)(G.row_ptr[a + 1] - ra);
+          const int64_t ra = G.start[a];
+          const int ka = G.len[a];
           const uint8_t fa = C.flags[a];
           const int oa = C.orig[a];
           const double wa = (WEIGHTED || ADJ) ? C.w[a] : 0.0;
