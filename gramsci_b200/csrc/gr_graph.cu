@@ -78,9 +78,8 @@ __global__ void __launch_bounds__(kGraphThreads) csr_fill_kernel(
     unsigned long long* __restrict__ stats, int* __restrict__ work) {
   __shared__ float4 s_pos[kGraphWarps][kCellTile];
   __shared__ int s_lab[kGraphWarps][kCellTile];
-  __shared__ long long s_qpos[kGraphWarps][kQueue];  // scratch slot, -1 when out of room
-  __shared__ int s_qp[kGraphWarps][kQueue];          // root label
-  __shared__ unsigned short s_qf[kGraphWarps][kQueue];  // tile index of the neighbour
+  __shared__ uint32_t s_qa[kGraphWarps][kQueue];  // tile index | (root index in the cell << 8)
+  __shared__ uint32_t s_qo[kGraphWarps][kQueue];  // position in the root's row
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
@@ -88,11 +87,15 @@ __global__ void __launch_bounds__(kGraphThreads) csr_fill_kernel(
   unsigned long long maxdeg = 0;
   const int ncell = (int)C.grid.ncell;
 
-  // bins of one queued edge, written to its slot
+  int cb = 0, total = 0;
+  long long base = 0;
+  bool room = true;
+  // bins of one queued edge, written to its slot of the root's row
   auto drain_one = [&](int e) {
-    const int p = s_qp[wib][e];
-    const int f = s_qf[wib][e];
-    const long long pos = s_qpos[wib][e];
+    const uint32_t a = s_qa[wib][e];
+    const int f = (int)(a & 0xffu);
+    const long long i = (long long)(a >> 8);
+    const int p = cb + (int)i;
     const int q = s_lab[wib][f];
     int b = 1, mf = 1, mr = 1;
     if (!pair_edge<F32, true>(C, P, p, q, C.pos4[p], s_pos[wib][f], b, mf, mr, rechecks)) {
@@ -102,7 +105,10 @@ __global__ void __launch_bounds__(kGraphThreads) csr_fill_kernel(
       mf = 1;
       mr = 1;
     }
-    if (pos >= 0) scratch[pos] = ((unsigned long long)pack_meta(b, mf, mr) << 32) | (uint32_t)q;
+    if (room) {
+      const long long pos = base + i * total - i * (i + 1) / 2 + (long long)s_qo[wib][e];
+      scratch[pos] = ((unsigned long long)pack_meta(b, mf, mr) << 32) | (uint32_t)q;
+    }
   };
 
   for (;;) {
@@ -110,8 +116,13 @@ __global__ void __launch_bounds__(kGraphThreads) csr_fill_kernel(
     if (lane == 0) cell = atomicAdd(work, 1);
     cell = __shfl_sync(0xffffffffu, cell, 0);
     if (cell >= ncell) break;
-    const int cb = C.cell_start[cell], ce = C.cell_start[cell + 1];
+    cb = C.cell_start[cell];
+    const int ce = C.cell_start[cell + 1];
     if (cb == ce) continue;
+    if (ce - cb >= (1 << 24)) {  // queue entries hold the root index in 24 bits
+      if (lane == 0) atomicMax(&ctl[1], 2ull);
+      continue;
+    }
     Ranges R;
     {
       GridParams g;
@@ -120,7 +131,8 @@ __global__ void __launch_bounds__(kGraphThreads) csr_fill_kernel(
       cell_grid(C, cell, g, cs, lkey);
       forward_ranges(cb - 1, lkey, g, cs, R);
     }
-    int pre[5], total = 0;
+    int pre[5];
+    total = 0;
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
       pre[k] = total;
@@ -128,8 +140,8 @@ __global__ void __launch_bounds__(kGraphThreads) csr_fill_kernel(
     }
     // the cell's scratch slots: [cbase[cell], cbase[cell + 1]); root i
     // has total - i - 1 candidates
-    const long long base = cbase[cell];
-    const bool room = cbase[cell + 1] <= cap;
+    base = cbase[cell];
+    room = cbase[cell + 1] <= cap;
     if (!room && lane == 0) atomicMax(&ctl[1], 1ull);
     int qn = 0;
     for (int t0 = 0; t0 < total; t0 += kCellTile) {
@@ -147,8 +159,8 @@ __global__ void __launch_bounds__(kGraphThreads) csr_fill_kernel(
         const int i = p - cb;
         const int fstart = max(0, i + 1 - t0);
         if (fstart >= tn) continue;
-        const float4 pi = C.pos4[p];
-        const long long rs = base + (long long)i * total - (long long)i * (i + 1) / 2;
+        // p itself is candidate i of the flattened ranges
+        const float4 pi = (i >= t0 && i - t0 < tn) ? s_pos[wib][i - t0] : C.pos4[p];
         int off = (t0 == 0) ? 0 : deg_up[p];  // edges of p in earlier tiles
         for (int f0 = fstart; f0 < tn; f0 += 32) {
           const int f = f0 + lane;
@@ -167,9 +179,8 @@ __global__ void __launch_bounds__(kGraphThreads) csr_fill_kernel(
           const unsigned m = __ballot_sync(0xffffffffu, e);
           if (e) {
             const int rank = __popc(m & lt);
-            s_qp[wib][qn + rank] = p;
-            s_qf[wib][qn + rank] = (unsigned short)f;
-            s_qpos[wib][qn + rank] = room ? rs + off + rank : -1ll;
+            s_qa[wib][qn + rank] = (uint32_t)f | ((uint32_t)i << 8);
+            s_qo[wib][qn + rank] = (uint32_t)(off + rank);
           }
           off += __popc(m);
           qn += __popc(m);
@@ -182,7 +193,7 @@ __global__ void __launch_bounds__(kGraphThreads) csr_fill_kernel(
         }
         if (lane == 0) {
           deg_up[p] = off;
-          rstart[p] = rs;
+          rstart[p] = base + (long long)i * total - (long long)i * (i + 1) / 2;
           cands += (unsigned long long)(tn - fstart);
           if (last_tile) {
             atomicAdd(&deg_full[p], off);
@@ -302,6 +313,7 @@ void UpperCSR::build(const DevCatalog& C, const PairParams& P, cudaStream_t s) {
       GR_CUDA_TRY(cudaMemcpyAsync(&need, cbase.p + ncell, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     GR_CUDA_TRY(cudaStreamSynchronize(s));
     if (hc[1] == 0) break;
+    if (hc[1] == 2) throw Error{-2, "CSR build: a grid cell holds 2^24 points or more"};
     // out of room: grow to the exact bound and run again
     scratch.reserve((size_t)need + 1024);
   }

@@ -217,41 +217,40 @@ struct Ranges {
 
 __device__ __forceinline__ void forward_ranges(int p, int key, const GridParams& g,
                                                const int* __restrict__ cell_start, Ranges& R) {
-  int cx = key % g.nx;
-  int cy = (key / g.nx) % g.ny;
-  int cz = key / (g.nx * g.ny);
-  int x0 = cx > 0 ? cx - 1 : 0;
-  int x1 = cx + 1 < g.nx ? cx + 1 : cx;
-  R.n = 0;
+  // five fixed slots (empty ones have beg == end), written with constant
+  // indices so that R stays in registers
+  const int cx = key % g.nx;
+  const int cy = (key / g.nx) % g.ny;
+  const int cz = key / (g.nx * g.ny);
+  const int x0 = cx > 0 ? cx - 1 : 0;
+  const int x1 = cx + 1 < g.nx ? cx + 1 : cx;
+  R.n = 5;
   {
-    int e = cell_start[key + (cx + 1 < g.nx ? 2 : 1)];
-    if (e > p + 1) {
-      R.beg[R.n] = p + 1;
-      R.end[R.n] = e;
-      R.n++;
-    }
+    const int e = cell_start[key + (cx + 1 < g.nx ? 2 : 1)];
+    R.beg[0] = p + 1;
+    R.end[0] = e > p + 1 ? e : p + 1;
   }
-  if (cy + 1 < g.ny) {
-    int kb = (cz * g.ny + cy + 1) * g.nx;
-    int b = cell_start[kb + x0], e = cell_start[kb + x1 + 1];
-    if (e > b) {
-      R.beg[R.n] = b;
-      R.end[R.n] = e;
-      R.n++;
+  {
+    int b = 0, e = 0;
+    if (cy + 1 < g.ny) {
+      const int kb = (cz * g.ny + cy + 1) * g.nx;
+      b = cell_start[kb + x0];
+      e = cell_start[kb + x1 + 1];
     }
+    R.beg[1] = b;
+    R.end[1] = e > b ? e : b;
   }
-  if (cz + 1 < g.nz) {
-    for (int dy = -1; dy <= 1; ++dy) {
-      int y = cy + dy;
-      if (y < 0 || y >= g.ny) continue;
-      int kb = ((cz + 1) * g.ny + y) * g.nx;
-      int b = cell_start[kb + x0], e = cell_start[kb + x1 + 1];
-      if (e > b) {
-        R.beg[R.n] = b;
-        R.end[R.n] = e;
-        R.n++;
-      }
+#pragma unroll
+  for (int dy = -1; dy <= 1; ++dy) {
+    const int y = cy + dy;
+    int b = 0, e = 0;
+    if (cz + 1 < g.nz && y >= 0 && y < g.ny) {
+      const int kb = ((cz + 1) * g.ny + y) * g.nx;
+      b = cell_start[kb + x0];
+      e = cell_start[kb + x1 + 1];
     }
+    R.beg[3 + dy] = b;
+    R.end[3 + dy] = e > b ? e : b;
   }
 }
 
@@ -297,11 +296,15 @@ __device__ __forceinline__ int range9_label(const Ranges9& R, const int* pre, in
 
 // Map flattened candidate index f (0 <= f < total) to a label.
 __device__ __forceinline__ int range_label(const Ranges& R, const int* pre, int f) {
-  int r = 0;
+  // constant indices only, so R and pre stay in registers
+  int b = R.beg[0], o = pre[0];
 #pragma unroll
   for (int k = 1; k < 5; ++k)
-    if (k < R.n && f >= pre[k]) r = k;
-  return R.beg[r] + (f - pre[r]);
+    if (k < R.n && f >= pre[k]) {
+      b = R.beg[k];
+      o = pre[k];
+    }
+  return b + (f - o);
 }
 
 // --------------------------------------------------------- tuple rank tables --

@@ -36,13 +36,13 @@ __host__ __device__ inline size_t align8(size_t x) { return (x + 7) & ~(size_t)7
 struct TriLayout {
   size_t off_cnt, off_lim, off_cot, off_norm, off_rank, off_cfg, off_fsc, off_warp, warp_bytes, total;
   // per-warp sub-offsets
-  size_t o_rs, o_w, o_g, o_col, o_meta, o_orig, o_len, o_hkey, o_qm, o_qxy, o_flag;
+  size_t o_rs, o_w, o_g, o_col, o_meta, o_orig, o_len, o_hkey, o_q;
 };
 
-// Largest per-root hash table: a power of two >= 2 * cap (load <= 1/2).
+// Largest per-root hash table: a power of two >= 4 * cap (load <= 1/4).
 __host__ __device__ inline int hash_lg_max(int cap) {
   int lg = 6;
-  while ((1 << lg) < 2 * cap) ++lg;
+  while ((1 << lg) < 4 * cap) ++lg;
   return lg;
 }
 
@@ -78,9 +78,7 @@ __host__ __device__ inline TriLayout tri_layout(int nh, int nmu, int nbins, int 
   L.o_orig = w; w += (size_t)cap * 4;
   L.o_len = w;  w += (size_t)cap * 4;
   L.o_hkey = w; w += (size_t)hs * 4;
-  L.o_qm = w;   w += (size_t)kQueue * 4;
-  L.o_qxy = w;  w += (size_t)kQueue * 2;
-  L.o_flag = w; w += (size_t)cap;
+  L.o_q = w;    w += (size_t)kQueue * 8;
   L.warp_bytes = align8(w);
   L.total = o + L.warp_bytes * nwarps;
   return L;
@@ -307,9 +305,8 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
   int* s_orig = reinterpret_cast<int*>(wb + L.o_orig);
   int* s_len = reinterpret_cast<int*>(wb + L.o_len);
   uint32_t* s_hkey = reinterpret_cast<uint32_t*>(wb + L.o_hkey);
-  uint32_t* s_qm = reinterpret_cast<uint32_t*>(wb + L.o_qm);
-  uint16_t* s_qxy = reinterpret_cast<uint16_t*>(wb + L.o_qxy);
-  uint8_t* s_flag = wb + L.o_flag;
+  // queue entry: (meta of edge (a, c) << 32) | row of a | (row of c << 8)
+  unsigned long long* s_q = reinterpret_cast<unsigned long long*>(wb + L.o_q);
   unsigned long long* s_glo = reinterpret_cast<unsigned long long*>(wb + L.o_g);
   unsigned long long* s_ghi = s_glo + T.cap;
   const int lg_max = hash_lg_max(T.cap);
@@ -318,15 +315,16 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
 
   // one queued triangle (p, a = row qx, c = row qy) with edge meta (a, c)
   auto drain_one = [&](int e, uint8_t fp, int op, double wp, Fix128& racc) -> int {
-    const uint16_t xy = s_qxy[e];
-    const int qx = xy & 0xff, qy = xy >> 8;
+    const unsigned long long qe = s_q[e];
+    const int qx = (int)(qe & 0xffu), qy = (int)((qe >> 8) & 0xffu);
+    const uint32_t mac = (uint32_t)(qe >> 32);
+    const uint32_t ma = s_meta[qx], mc = s_meta[qy];
+    const uint8_t fa = (uint8_t)(ma >> 24), fc = (uint8_t)(mc >> 24);
     if (ADJ)
-      return tri_grad(X, fp, op, wp, s_flag[qx], s_orig[qx], s_w[qx], s_flag[qy], s_orig[qy],
-                      s_w[qy], s_meta[qx], s_meta[qy], s_qm[e], racc, &s_glo[qx], &s_ghi[qx],
-                      &s_glo[qy], &s_ghi[qy]);
-    return tri_bin<WEIGHTED, COUNTS>(X, fp, op, wp, s_flag[qx], s_orig[qx],
-                                     WEIGHTED ? s_w[qx] : 0.0, s_flag[qy], s_orig[qy],
-                                     WEIGHTED ? s_w[qy] : 0.0, s_meta[qx], s_meta[qy], s_qm[e]);
+      return tri_grad(X, fp, op, wp, fa, s_orig[qx], s_w[qx], fc, s_orig[qy], s_w[qy], ma, mc, mac,
+                      racc, &s_glo[qx], &s_ghi[qx], &s_glo[qy], &s_ghi[qy]);
+    return tri_bin<WEIGHTED, COUNTS>(X, fp, op, wp, fa, s_orig[qx], WEIGHTED ? s_w[qx] : 0.0, fc,
+                                     s_orig[qy], WEIGHTED ? s_w[qy] : 0.0, ma, mc, mac);
   };
 
   for (;;) {
@@ -345,9 +343,9 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
       Fix128 racc = {0ull, 0ull};
       // rows are sorted: the last entry has the largest label offset
       if (k <= T.cap && rec_col(G.rec[b0 + k - 1]) - p < kMaxOffset) {
-        // per-root table: >= 4 slots per entry, at most the capacity's table
+        // per-root table: >= 8 slots per entry, at most the capacity's table
         int lg = 6;
-        while (lg < lg_max && (1 << lg) < 4 * k) ++lg;
+        while (lg < lg_max && (1 << lg) < 8 * k) ++lg;
         const int hs = 1 << lg;
         __syncwarp();
         for (int h = lane; h < hs; h += 32) s_hkey[h] = 0u;
@@ -359,13 +357,13 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
             const unsigned long long r = G.rec[b0 + x];
             const int a = rec_col(r);
             s_col[x] = a;
-            s_meta[x] = rec_meta(r);
             const long long rs = G.start[a];
             const int len = G.len[a];
             s_rs[x] = rs;
             s_len[x] = len;
             probes += (unsigned long long)len;
-            s_flag[x] = C.flags[a];
+            // the vertex flags ride in the top byte of the edge meta word
+            s_meta[x] = rec_meta(r) | ((uint32_t)C.flags[a] << 24);
             s_orig[x] = C.orig[a];
             if (WEIGHTED || ADJ) s_w[x] = C.w[a];
             if (ADJ) {
@@ -441,27 +439,27 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
               bool hit = false;
               int y = 0;
               const uint32_t mac = rec_meta(rr[u]);
-              if (tw[u] < tot) {
-                const int off = rec_col(rr[u]) - p;
-                if (off < kMaxOffset) {
-                  uint32_t h = fib_slot((uint32_t)off, lg);
-                  for (int it = 0; it < hs; ++it) {
-                    const uint32_t e = s_hkey[h];
-                    if ((e >> 8) == (uint32_t)off) {
-                      hit = true;
-                      y = (int)(e & 0xffu);
-                      break;
-                    }
-                    if (e == 0u) break;
-                    h = (h + 1) & (uint32_t)(hs - 1);
-                  }
+              // first probe for every lane; the rare collisions continue
+              // in a loop that only runs while some lane is unresolved
+              const int off = rec_col(rr[u]) - p;
+              const bool live = tw[u] < tot && off < kMaxOffset;
+              uint32_t h = fib_slot((uint32_t)off, lg);
+              uint32_t e = live ? s_hkey[h] : 0u;
+              hit = live && (e >> 8) == (uint32_t)off;
+              bool open = live && !hit && e != 0u;
+              for (int it = 1; it < hs && __any_sync(0xffffffffu, open); ++it) {
+                if (open) {
+                  h = (h + 1) & (uint32_t)(hs - 1);
+                  e = s_hkey[h];
+                  hit = (e >> 8) == (uint32_t)off;
+                  open = !hit && e != 0u;
                 }
               }
+              if (hit) y = (int)(e & 0xffu);
               const unsigned m = __ballot_sync(0xffffffffu, hit);
               if (hit) {
                 const int pos = qn + __popc(m & lt);
-                s_qm[pos] = mac;
-                s_qxy[pos] = (uint16_t)(ox[u] | (y << 8));
+                s_q[pos] = ((unsigned long long)mac << 32) | (uint32_t)(ox[u] | (y << 8));
               }
               qn += __popc(m);
             }
