@@ -40,7 +40,7 @@ WORKLOAD = "c2_3pcf"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0, help="workload scale (1.0 = full size)")
@@ -98,7 +98,9 @@ def workload_config(cat, sp, scale, extra=None):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled during the timed region
+    (every 20 ms; samples are time-stamped and only those inside the region
+    passed to stop() are summarised)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -113,18 +115,22 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "50"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # wait (bounded) for the first sample so that the region is covered
+            t_end = time.monotonic() + 5.0
+            while not self.lines and time.monotonic() < t_end:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
 
-    def stop(self):
+    def stop(self, t0=None, t1=None):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -134,7 +140,12 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        inside = [ln for t, ln in self.lines if (t0 is None or t >= t0) and (t1 is None or t <= t1)]
+        window = "timed region"
+        if not inside:  # region shorter than the sampling period: nearest samples
+            inside = [ln for _, ln in self.lines]
+            window = "whole run (timed region shorter than the sampling period)"
+        for ln in inside:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -147,7 +158,7 @@ class ClockSampler:
                 if v.lower() in ("active", "0x1", "1"):
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "window": window}
 
 
 def cpu_reference_run(cat, w, sp, threads):
@@ -240,6 +251,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
+    t_region0 = time.monotonic()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
     q_ms, tri, launches = [], 0, 0
@@ -254,8 +266,9 @@ def run_ours(args):
         tri += st["tuples"]
         launches += st["kernel_launches"]
     torch.cuda.synchronize()
+    t_region1 = time.monotonic()
     barrier()
-    clocks = sampler.stop()
+    clocks = sampler.stop(t_region0, t_region1)
     step_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = float(sum(step_ms))
     t_max = total_ms

@@ -298,15 +298,22 @@ int set_err(gr_ctx* c, int code, const std::string& m) {
 
 // Clears *flag unless all galaxy weights are equal and all random weights are
 // equal; writes max |w| over galaxies to wmax[0] and over randoms to wmax[1]
-// (as the bits of non-negative doubles).
+// (as the bits of non-negative doubles).  Reduced per block first, so each
+// block makes at most three global updates.
 __global__ void uniform_check_kernel(const double* __restrict__ w, int64_t n_data, int64_t n,
                                      unsigned char* flag, unsigned long long* wmax) {
+  __shared__ unsigned long long s_mg[32], s_mr[32];
+  __shared__ int s_bad[32];
   unsigned long long mg = 0, mr = 0;
+  bool bad = false;
+  const double refg = n_data > 0 ? w[0] : 0.0;
+  const double refr = n > n_data ? w[n_data] : 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
-    double ref = i < n_data ? w[0] : w[n_data];
-    if (__double_as_longlong(w[i]) != __double_as_longlong(ref)) *flag = 0;
-    unsigned long long a = (unsigned long long)__double_as_longlong(fabs(w[i]));
+    const double v = w[i];
+    const double ref = i < n_data ? refg : refr;
+    bad = bad || __double_as_longlong(v) != __double_as_longlong(ref);
+    const unsigned long long a = (unsigned long long)__double_as_longlong(fabs(v));
     if (i < n_data) mg = a > mg ? a : mg;
     else mr = a > mr ? a : mr;
   }
@@ -316,9 +323,24 @@ __global__ void uniform_check_kernel(const double* __restrict__ w, int64_t n_dat
     u = __shfl_xor_sync(0xffffffffu, mr, o);
     mr = u > mr ? u : mr;
   }
+  bad = __any_sync(0xffffffffu, bad);
+  const int wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   if ((threadIdx.x & 31) == 0) {
+    s_mg[wid] = mg;
+    s_mr[wid] = mr;
+    s_bad[wid] = bad ? 1 : 0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int b = 0;
+    for (int k = 0; k < nw; ++k) {
+      mg = s_mg[k] > mg ? s_mg[k] : mg;
+      mr = s_mr[k] > mr ? s_mr[k] : mr;
+      b |= s_bad[k];
+    }
     if (mg) atomicMax(&wmax[0], mg);
     if (mr) atomicMax(&wmax[1], mr);
+    if (b) *flag = 0;
   }
 }
 
@@ -487,7 +509,7 @@ static int set_catalog_impl(gr_ctx* c, const double* xyz, const double* w, const
   GR_CUDA_TRY(cudaMemcpyAsync(c->uniform_flag.p, init, 24, cudaMemcpyHostToDevice, s));
   unsigned long long* d_wmax = reinterpret_cast<unsigned long long*>(c->uniform_flag.p + 8);
   if (n > 0) {
-    int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
+    int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 2);
     uniform_check_kernel<<<blocks, 256, 0, s>>>(c->w.p, n_data, n, c->uniform_flag.p, d_wmax);
     GR_CHECK_LAUNCH();
   }

@@ -36,7 +36,7 @@ __host__ __device__ inline size_t align8(size_t x) { return (x + 7) & ~(size_t)7
 struct TriLayout {
   size_t off_cnt, off_lim, off_cot, off_norm, off_rank, off_cfg, off_fsc, off_warp, warp_bytes, total;
   // per-warp sub-offsets
-  size_t o_rs, o_w, o_g, o_col, o_meta, o_orig, o_len, o_hkey, o_q;
+  size_t o_rs, o_w, o_g, o_col, o_mo, o_len, o_hkey, o_q;
 };
 
 // Largest per-root hash table: a power of two >= 4 * cap (load <= 1/4).
@@ -74,8 +74,7 @@ __host__ __device__ inline TriLayout tri_layout(int nh, int nmu, int nbins, int 
   L.o_w = w;    if (weighted || adj) w += (size_t)cap * 8;
   L.o_g = w;    if (adj) w += (size_t)cap * 16;  // gradient (lo, hi) per neighbour
   L.o_col = w;  w += (size_t)cap * 4;
-  L.o_meta = w; w += (size_t)cap * 4;
-  L.o_orig = w; w += (size_t)cap * 4;
+  L.o_mo = w;   w += (size_t)cap * 8;  // (catalogue id << 32) | flags << 24 | edge meta
   L.o_len = w;  w += (size_t)cap * 4;
   L.o_hkey = w; w += (size_t)hs * 4;
   L.o_q = w;    w += (size_t)kQueue * 8;
@@ -253,10 +252,11 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
   X.lim = SHIST ? reinterpret_cast<unsigned long long*>(smem + L.off_lim) : g_lim;
   uint8_t* s_norm = smem + L.off_norm;
   int* s_F = reinterpret_cast<int*>(smem + L.off_rank);
-  double* s_fsc = reinterpret_cast<double*>(smem + L.off_fsc);
   X.norm = s_norm;
   X.F = s_F;
+  double* s_fsc = reinterpret_cast<double*>(smem + L.off_fsc);
   X.fsc = s_fsc;
+  if (threadIdx.x < 4) s_fsc[threadIdx.x] = T.fscale[threadIdx.x];
   X.gscale = gscale;
   if (ADJ) {
     double* s_cot = reinterpret_cast<double*>(smem + L.off_cot);
@@ -277,7 +277,6 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
       }
     }
   }
-  if (threadIdx.x < 4) s_fsc[threadIdx.x] = T.fscale[threadIdx.x];
   for (int k = threadIdx.x; k < T.nmu * T.nmu; k += blockDim.x) s_norm[k] = T.rsd ? T.normal[k] : 1;
   const int nb2 = T.nbins + 2;
   for (int k = threadIdx.x; k < 3 * nb2; k += blockDim.x) s_F[k] = T.rank.F[k / nb2][k % nb2];
@@ -301,8 +300,7 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
   long long* s_rs = reinterpret_cast<long long*>(wb + L.o_rs);
   double* s_w = reinterpret_cast<double*>(wb + L.o_w);
   int* s_col = reinterpret_cast<int*>(wb + L.o_col);
-  uint32_t* s_meta = reinterpret_cast<uint32_t*>(wb + L.o_meta);
-  int* s_orig = reinterpret_cast<int*>(wb + L.o_orig);
+  unsigned long long* s_mo = reinterpret_cast<unsigned long long*>(wb + L.o_mo);
   int* s_len = reinterpret_cast<int*>(wb + L.o_len);
   uint32_t* s_hkey = reinterpret_cast<uint32_t*>(wb + L.o_hkey);
   // queue entry: (meta of edge (a, c) << 32) | row of a | (row of c << 8)
@@ -318,13 +316,15 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
     const unsigned long long qe = s_q[e];
     const int qx = (int)(qe & 0xffu), qy = (int)((qe >> 8) & 0xffu);
     const uint32_t mac = (uint32_t)(qe >> 32);
-    const uint32_t ma = s_meta[qx], mc = s_meta[qy];
+    const unsigned long long moa = s_mo[qx], moc = s_mo[qy];
+    const uint32_t ma = (uint32_t)moa, mc = (uint32_t)moc;
+    const int oa = (int)(moa >> 32), oc = (int)(moc >> 32);
     const uint8_t fa = (uint8_t)(ma >> 24), fc = (uint8_t)(mc >> 24);
     if (ADJ)
-      return tri_grad(X, fp, op, wp, fa, s_orig[qx], s_w[qx], fc, s_orig[qy], s_w[qy], ma, mc, mac,
-                      racc, &s_glo[qx], &s_ghi[qx], &s_glo[qy], &s_ghi[qy]);
-    return tri_bin<WEIGHTED, COUNTS>(X, fp, op, wp, fa, s_orig[qx], WEIGHTED ? s_w[qx] : 0.0, fc,
-                                     s_orig[qy], WEIGHTED ? s_w[qy] : 0.0, ma, mc, mac);
+      return tri_grad(X, fp, op, wp, fa, oa, s_w[qx], fc, oc, s_w[qy], ma, mc, mac, racc,
+                      &s_glo[qx], &s_ghi[qx], &s_glo[qy], &s_ghi[qy]);
+    return tri_bin<WEIGHTED, COUNTS>(X, fp, op, wp, fa, oa, WEIGHTED ? s_w[qx] : 0.0, fc, oc,
+                                     WEIGHTED ? s_w[qy] : 0.0, ma, mc, mac);
   };
 
   for (;;) {
@@ -363,8 +363,8 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
             s_len[x] = len;
             probes += (unsigned long long)len;
             // the vertex flags ride in the top byte of the edge meta word
-            s_meta[x] = rec_meta(r) | ((uint32_t)C.flags[a] << 24);
-            s_orig[x] = C.orig[a];
+            s_mo[x] = ((unsigned long long)(uint32_t)C.orig[a] << 32) |
+                      (rec_meta(r) | ((uint32_t)C.flags[a] << 24));
             if (WEIGHTED || ADJ) s_w[x] = C.w[a];
             if (ADJ) {
               s_glo[x] = 0ull;
