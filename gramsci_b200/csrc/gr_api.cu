@@ -731,12 +731,13 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
   GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
   if (!reuse) build_csr(c);
   GR_CUDA_TRY(cudaEventRecord(c->ev[2], s));
-  unsigned long long gst[4];
-  GR_CUDA_TRY(cudaMemcpyAsync(gst, c->csr.stats.p, sizeof(gst), cudaMemcpyDeviceToHost, s));
+  // graph statistics are on the host after the build (or the load)
+  const unsigned long long gst[3] = {(unsigned long long)c->csr.rechecks,
+                                     (unsigned long long)c->csr.candidates,
+                                     (unsigned long long)c->csr.max_deg};
   GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nh, s));
   GR_CUDA_TRY(cudaMemsetAsync(c->hfix.p, 0, sizeof(unsigned long long) * 2 * nh, s));
   GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
-  GR_CUDA_TRY(cudaStreamSynchronize(s));
   TriParams T{};
   T.nbins = c->nbins;
   T.nmu = nmu;
@@ -837,14 +838,14 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
   if (!reuse) build_csr(c);
   GR_CUDA_TRY(cudaEventRecord(c->ev[2], s));
-  unsigned long long gst[4];
-  GR_CUDA_TRY(cudaMemcpyAsync(gst, c->csr.stats.p, sizeof(gst), cudaMemcpyDeviceToHost, s));
+  const unsigned long long gst[3] = {(unsigned long long)c->csr.rechecks,
+                                     (unsigned long long)c->csr.candidates,
+                                     (unsigned long long)c->csr.max_deg};
   GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nh, s));
   GR_CUDA_TRY(cudaMemsetAsync(c->hfix.p, 0, sizeof(unsigned long long) * 2 * nh, s));
   GR_CUDA_TRY(cudaMemsetAsync(c->dcnt.p, 0, sizeof(unsigned long long) * nd, s));
   GR_CUDA_TRY(cudaMemsetAsync(c->dfix.p, 0, sizeof(unsigned long long) * 2 * nd, s));
   GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
-  GR_CUDA_TRY(cudaStreamSynchronize(s));
   if ((int64_t)gst[2] > 1024)
     return set_err(c, GR_E_CAPACITY, "4PCF: a point has more than 1024 larger-label neighbours");
   QuadParams Q{};
