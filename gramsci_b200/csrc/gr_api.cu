@@ -173,18 +173,6 @@ double fix_scale(double pmax) {
   return std::ldexp(1.0, 60 - e);
 }
 
-double limb_scale(double pmax) {
-  if (!(pmax > 0.0) || !std::isfinite(pmax)) return 1.0;
-  int e;
-  std::frexp(pmax * (1.0 + 1e-9), &e);  // pmax < 2^e
-  return std::ldexp(1.0, 52 - e);
-}
-
-double limb_value(unsigned long long lo, unsigned long long hi, double scale) {
-  const __int128 v = (__int128)(long long)hi * ((__int128)1 << kLimbBits) + (__int128)lo;
-  return (double)v / scale;
-}
-
 double fix_value(unsigned long long lo, unsigned long long hi, double scale) {
   const long double v = (long double)(long long)hi * 18446744073709551616.0L + (long double)lo;
   return (double)(v / (long double)scale);
@@ -717,7 +705,7 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
   const bool want_counts = counts != nullptr || !weighted;
   double fscale[4];
   for (int nr = 0; nr < 4; ++nr)
-    fscale[nr] = limb_scale(std::pow(c->wgmax, 3 - nr) * std::pow(c->wrmax, nr));
+    fscale[nr] = fix_scale(std::pow(c->wgmax, 3 - nr) * std::pow(c->wrmax, nr));
   c->hcnt.reserve(nh);
   c->hfix.reserve(2 * nh);
   c->stats.reserve(8);
@@ -765,11 +753,8 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
     GR_CUDA_TRY(cudaMemcpyAsync(hf.data(), c->hfix.p, sizeof(unsigned long long) * 2 * nh, cudaMemcpyDeviceToHost, s));
   GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
   GR_CUDA_TRY(cudaStreamSynchronize(s));
-  // limb sums are exact below 2^35 updates per bin; the rooted total bounds them
-  if (weighted && st[1] >= (1ull << 35))
-    return set_err(c, GR_E_CAPACITY, "3PCF: more than 2^35 rooted triangles for the exact sums");
   if (weighted)
-    for (int k = 0; k < nh; ++k) hs[k] = limb_value(hf[k], hf[nh + k], fscale[k / nbin]);
+    for (int k = 0; k < nh; ++k) hs[k] = fix_value(hf[k], hf[nh + k], fscale[k / nbin]);
   if (!weighted) {
     for (int nr = 0; nr < 4; ++nr) {
       double prod = uniform_product(c->w_gal, c->w_ran, 3 - nr, nr);

@@ -403,6 +403,16 @@ __device__ __forceinline__ void fix_add(unsigned long long* lo, unsigned long lo
   if (d) atomicAdd(hi, d);
 }
 
+// the same for an integer already scaled (|v| < 2^62)
+__device__ __forceinline__ void fix_add_int(unsigned long long* lo, unsigned long long* hi,
+                                            long long v) {
+  const unsigned long long add = (unsigned long long)v;
+  const unsigned long long old = atomicAdd(lo, add);
+  const unsigned long long carry = (old + add < old) ? 1ull : 0ull;
+  const unsigned long long d = (v < 0 ? ~0ull : 0ull) + carry;
+  if (d) atomicAdd(hi, d);
+}
+
 // merge a partial (lo, hi) pair into another with atomics
 __device__ __forceinline__ void fix_merge(unsigned long long* lo, unsigned long long* hi,
                                           unsigned long long plo, unsigned long long phi) {
@@ -410,20 +420,6 @@ __device__ __forceinline__ void fix_merge(unsigned long long* lo, unsigned long 
   const unsigned long long d = phi + ((old + plo < old) ? 1ull : 0ull);
   if (d) atomicAdd(hi, d);
 }
-
-// Two-limb fixed point without carries: a product scaled to |v| <= 2^52 is
-// added as lo = v mod 2^26 (unsigned) and hi = floor(v / 2^26) (signed) to
-// two 64-bit sums.  Both sums stay exact for fewer than 2^37 terms, and the
-// atomics need no return value (no carry to propagate).
-constexpr int kLimbBits = 26;
-__device__ __forceinline__ void limb_add(unsigned long long* lo, unsigned long long* hi, long long v) {
-  atomicAdd(lo, (unsigned long long)(v & ((1ll << kLimbBits) - 1)));
-  atomicAdd(hi, (unsigned long long)(v >> kLimbBits));
-}
-// Host: scale 2^e with max_abs_product * 2^e <= 2^52 (1.0 for a zero bound).
-double limb_scale(double max_abs_product);
-// Host: (hi * 2^26 + lo) / scale for 64-bit limb sums (hi two's complement).
-double limb_value(unsigned long long lo, unsigned long long hi, double scale);
 
 // A 128-bit fixed-point accumulator held in registers.
 struct Fix128 {

@@ -30,13 +30,13 @@ struct TriParams {
   int cap;                 // per-warp shared row capacity (rows longer go the global path)
   const uint8_t* normal;   // device find_normal table [mu1-1 + nmu*(mu2-1)]
   RankTables rank;         // 3-tuple ranks
-  double fscale[4];        // limb scale of the products with 0..3 randoms
+  double fscale[4];        // fixed-point scale of the products with 0..3 randoms
 };
 
 // 3PCF: triangles p < a < c enumerated once over the upper CSR; each adds to
 // the rooted histogram of every non-buffer vertex.  g_cnt (nh = ncfg*nmu*4,
-// when counts) and g_lim (2*nh limb sums: lo words then hi words, weighted
-// only) must be zeroed.  stats: [0] distinct triangles binned, [1] rooted
+// when counts) and g_lim (2*nh: 128-bit fixed-point sums, lo words then hi
+// words, weighted only) must be zeroed.  stats: [0] distinct triangles binned, [1] rooted
 // incidences, [2] intersection probes.
 // work: one device int used as the dynamic root counter (reset by the launch).
 size_t tri3_smem_bytes(const TriParams& T, bool weighted, bool counts);

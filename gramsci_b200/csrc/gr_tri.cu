@@ -18,7 +18,7 @@
 // A triangle contributes to the rooted histogram of each non-buffer vertex r
 // with the bins of its three edges (symmetric bin table), the find_normal mu
 // bin of r's two edges taken in catalogue-id order (k1 < k2 in the
-// reference's id-sorted row) and the weight product, accumulated as two-limb
+// reference's id-sorted row) and the weight product, accumulated as 128-bit
 // fixed point with a scale per number of randoms.
 #include "gr_kernels.cuh"
 
@@ -87,10 +87,10 @@ struct TriCtx {
   const uint8_t* norm;
   const int* F;  // 3 x (nbins+2)
   const uint16_t* cfgtab;  // symmetric configuration table or NULL
-  const double* fsc;       // limb scale by number of randoms
+  const double* fsc;       // fixed-point scale by number of randoms
   int nbins, nmu, ncfg, rsd, nh, equi;
   unsigned long long* cnt;
-  unsigned long long* lim;  // limb sums: lim[k] (lo), lim[nh + k] (hi)
+  unsigned long long* lim;  // fixed-point sums: lim[k] (lo), lim[nh + k] (hi)
   // adjoint
   const double* c2;  // cot2 (ncfg, nmu)
   const double* c3;  // cot3 (ncfg, nmu)
@@ -116,7 +116,7 @@ __device__ __forceinline__ int normal_bin(const TriCtx& X, int mu1, int mu2, boo
 template <bool WEIGHTED, bool COUNTS>
 __device__ __forceinline__ void tri_add(const TriCtx& X, int k, int n, long long v) {
   if (COUNTS) atomicAdd(&X.cnt[k], (unsigned long long)n);
-  if (WEIGHTED) limb_add(&X.lim[k], &X.lim[X.nh + k], v * n);
+  if (WEIGHTED) fix_add_int(&X.lim[k], &X.lim[X.nh + k], v * n);
 }
 
 // One triangle (p, a, c) with p < a < c in labels.  It adds to the rooted
@@ -544,8 +544,7 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
       }
       if (WEIGHTED) {
         const unsigned long long lo = X.lim[k], hi = X.lim[nh + k];
-        if (lo) atomicAdd(&g_lim[k], lo);
-        if (hi) atomicAdd(&g_lim[nh + k], hi);
+        if (lo | hi) fix_merge(&g_lim[k], &g_lim[nh + k], lo, hi);
       }
     }
   }
