@@ -29,7 +29,7 @@ namespace {
 constexpr int kTriMaxWarps = 32;  // block size is chosen at launch to fit shared memory
 constexpr size_t kSmemLimit = 227 * 1024;
 constexpr int kQueue = 96;   // hit queue entries per warp (< 32 left + 64 pushed)
-constexpr int kChunk = 4;    // roots taken per work-counter increment
+constexpr int kChunk = 1;    // roots taken per work-counter increment (more causes tail imbalance)
 constexpr int kCfgTableBins = 16;  // nbins up to which the configuration table is used
 
 __host__ __device__ inline size_t align8(size_t x) { return (x + 7) & ~(size_t)7; }
