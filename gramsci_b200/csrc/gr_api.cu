@@ -50,6 +50,7 @@ struct gr_ctx {
   PairParams P{};
   DevBuf<uint8_t> normal_dev;
   DevBuf<unsigned long long> hcnt, dcnt, stats;
+  DevBuf<unsigned long long> qpriv;       // 4PCF per-block histogram copies
   DevBuf<unsigned long long> hfix, dfix;  // fixed-point sums (lo words, then hi words)
   double wmax = 0.0;                      // max |w| over the catalogue
   double wgmax = 0.0, wrmax = 0.0;        // max |w| over galaxies / randoms
@@ -843,8 +844,9 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   cudaEvent_t q0;
   GR_CUDA_TRY(cudaEventCreate(&q0));
   GR_CUDA_TRY(cudaEventRecord(q0, s));
-  launch_quad4(c->index.view(), G, Q, weighted, c->hcnt.p, c->hfix.p, c->dcnt.p, c->dfix.p,
-               fscale, dscale, c->stats.p, s);
+  c->work.reserve(4);
+  launch_quad4(c->index.view(), G, Q, weighted, c->hcnt.p, c->hfix.p, c->dcnt.p, c->dfix.p, nh, nd,
+               fscale, dscale, c->qpriv, c->stats.p, c->work.p, s);
   GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
   std::vector<unsigned long long> hc(nh), dc(nd), hf, df;
   std::vector<double> hs(nh, 0.0), ds(nd, 0.0);
@@ -859,6 +861,8 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   }
   GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
   GR_CUDA_TRY(cudaStreamSynchronize(s));
+  if (st[3] != 0)
+    return set_err(c, GR_E_CAPACITY, "4PCF: label offsets within a row exceed the hash key range");
   if (weighted) {
     for (int k = 0; k < nh; ++k) hs[k] = fix_value(hf[k], hf[(size_t)nh + k], fscale);
     for (int k = 0; k < nd; ++k) ds[k] = fix_value(df[k], df[(size_t)nd + k], dscale);

@@ -71,10 +71,16 @@ struct QuadParams {
 // 4PCF: 4-cliques p < a < b < c enumerated once; each adds to the rooted
 // histograms of its non-buffer vertices whose perimeter is canonical.
 // g_cnt: nh = ncfg*nbins*nbins*5 (g_fix 2*nh); d_cnt: nd = ncfg*nbins*nbins*24 (d_fix 2*nd).
-// stats: [0] distinct 4-cliques binned, [1] rooted incidences, [2] probes.
+// stats (4 entries, zeroed): [0] distinct 4-cliques binned, [1] rooted
+// incidences, [2] probes, [3] set when a root's label offsets exceed the
+// hash key range (the host reports it).  work: one device int, the dynamic
+// root counter (reset by the launch).
+// The outputs (g_cnt nh, g_fix 2 nh, d_cnt nd, d_fix 2 nd; fix arrays only
+// when weighted) are written whole; `priv` holds the per-block copies.
 void launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bool weighted,
                   unsigned long long* g_cnt, unsigned long long* g_fix, unsigned long long* d_cnt,
-                  unsigned long long* d_fix, double fscale, double dscale,
-                  unsigned long long* stats, cudaStream_t s);
+                  unsigned long long* d_fix, int nh, int nd, double fscale, double dscale,
+                  DevBuf<unsigned long long>& priv, unsigned long long* stats, int* work,
+                  cudaStream_t s);
 
 }  // namespace gr

@@ -1,53 +1,70 @@
 // 4PCF 4-clique counting: replaces query_4pcf_all2 (src/gramsci.F90:662-825),
 // whose per-root triple loop performs three find_dist binary searches per
-// candidate triple.
+// candidate triple, and the -tetra counter query_graph_tetrahedron
+// (:548-660).
 //
-// Every 4-clique is enumerated exactly once, from its smallest label p: for
-// each a in R+(p), the warp builds X = R+(a) ∩ R+(p) in shared memory
-// (ballot compaction keeps it sorted), then for each b in X and each c in
-// R+(b) looks c up in X.  The clique's six edge bins are known at that point;
-// it then contributes, for every vertex r that is a root in the reference
-// (not a buffer point, row length > 3), with the other three vertices taken
-// in catalogue-id order (a < b < c of the reference's k1 < k2 < k3), if the
-// perimeter r-a-b-c-r is canonical (bintable entry > 0), to N2 / N3 at
-// (cfg, bin(r,b), bin(a,c)) and to the six disconnected pair terms.
+// Every 4-clique is enumerated exactly once, from its smallest label p.  A
+// warp takes roots from a work counter and stages R+(p) in shared memory
+// (catalogue id, flags, weight, row start and length of every neighbour)
+// with a per-root hash table (label offset -> row position).  For each a in
+// R+(p) it builds X = R+(a) ∩ R+(p) beyond a's position, as a compacted list
+// and a bitmask over R+(p)'s positions; then the work items (b, d) for b in X
+// and d in R+(b) are flattened over the lanes (warp OR-reduction owners, as
+// in the triangle kernel), d is looked up in the hash table and tested in
+// the bitmask, and hits (cliques p < a < b < d) are queued and binned 32 at
+// a time with all their data in shared memory.  A clique contributes, for
+// every vertex r that is a root in the reference (not a buffer point, row
+// length > 3), with the other three vertices taken in catalogue-id order
+// (k1 < k2 < k3 of the reference), if the perimeter r-k1-k2-k3-r is
+// canonical (bintable entry > 0), to N2 / N3 at (cfg, bin(r,k2), bin(k1,k3))
+// and to the six disconnected pair terms.
 #include "gr_kernels.cuh"
 
 namespace gr {
 
 namespace {
 
-constexpr int kQuadWarps = 4;
-constexpr int kQuadThreads = kQuadWarps * 32;
+constexpr int kQuadMaxWarps = 16;  // block size chosen at launch to fit shared memory (128 registers)
+constexpr size_t kQuadSmemLimit = 227 * 1024;
+constexpr int kQQueue = 96;         // hit queue entries per warp (< 32 left + 64 pushed)
+constexpr int kQMaxOffset = 1 << 22;  // hash entries: (label offset << 10) | position
+constexpr uint8_t kFlagDeg4 = 4;    // staged flag: full row length > 3 (a reference root)
 
 __host__ __device__ inline size_t qalign8(size_t x) { return (x + 7) & ~(size_t)7; }
 
+__host__ __device__ inline int qhash_lg_max(int cap) {
+  int lg = 6;
+  while ((1 << lg) < 4 * cap) ++lg;
+  return lg;
+}
+
 struct QuadLayout {
   size_t off_rank, off_warp, warp_bytes, total;
+  // per-warp sub-offsets
+  size_t o_rs, o_w, o_mo, o_col, o_len, o_xm, o_hkey, o_q, o_xy, o_xz, o_bits;
 };
 
-__host__ __device__ inline QuadLayout quad_layout(int nbins, int cap) {
+__host__ __device__ inline QuadLayout quad_layout(int nbins, int cap, int nwarps) {
   QuadLayout L;
   size_t o = 0;
   L.off_rank = o;
   o = qalign8(o + sizeof(int) * 4 * (size_t)(nbins + 2));
   L.off_warp = o;
-  // row: rstart(8) col(4) meta(4) len(4); X: xstart(8) xc(4) xy(4) xm(4) xpre(4, cap+1)
-  L.warp_bytes = qalign8((size_t)cap * (8 + 4 + 4 + 4) + (size_t)cap * (8 + 4 + 4 + 4) + (size_t)(cap + 1) * 4);
-  L.total = o + L.warp_bytes * kQuadWarps;
+  size_t w = 0;
+  L.o_rs = w;   w += (size_t)cap * 8;   // row start of each neighbour
+  L.o_w = w;    w += (size_t)cap * 8;   // weight
+  L.o_mo = w;   w += (size_t)cap * 8;   // (catalogue id << 32) | flags << 24 | meta(p, a)
+  L.o_col = w;  w += (size_t)cap * 4;   // label
+  L.o_len = w;  w += (size_t)cap * 4;   // row length
+  L.o_xm = w;   w += (size_t)cap * 4;   // X entry z: meta(a, b)
+  L.o_hkey = w; w += (size_t)(1u << qhash_lg_max(cap)) * 4;
+  L.o_q = w;    w += (size_t)kQQueue * 8;
+  L.o_xy = w;   w += (size_t)cap * 2;   // X entry z: position of b in R+(p)
+  L.o_xz = w;   w += (size_t)cap * 2;   // position y: X entry (when its bit is set)
+  L.o_bits = w; w += (size_t)((cap + 31) / 32) * 4;
+  L.warp_bytes = qalign8(w);
+  L.total = o + L.warp_bytes * nwarps;
   return L;
-}
-
-__device__ __forceinline__ int qlower_bound(const int* a, int n, int v) {
-  int lo = 0, hi = n;
-  while (lo < hi) {
-    int mid = (lo + hi) >> 1;
-    if (a[mid] < v)
-      lo = mid + 1;
-    else
-      hi = mid;
-  }
-  return lo;
 }
 
 struct QuadCtx {
@@ -59,159 +76,168 @@ struct QuadCtx {
   double dscale;  // scale of the pair products of the disconnected terms
 };
 
-// disc term t: gate role and pair roles (0 = root i, 1 = a, 2 = b, 3 = c),
-// gramsci.F90:754-818 (t = 1..6 there).
-__constant__ int kGate[6] = {3, 3, 1, 0, 0, 0};
-__constant__ int kPu[6] = {0, 0, 0, 1, 3, 3};
-__constant__ int kPv[6] = {1, 2, 3, 2, 2, 1};
+// The four vertices of a clique: flags (with kFlagDeg4), catalogue ids and
+// weights.
+struct QVerts {
+  uint8_t fl[4];
+  int og[4];
+  double w[4];
+};
 
-// -tetra terms (gramsci.F90:591-646): gate role, product roles, and the
-// pair that must also be random for discR; roles 0 = root, 1..3 = the
-// other vertices in catalogue-id order.
-__constant__ int kTGate[6] = {3, 3, 1, 0, 0, 0};
-__constant__ int kTPa[6] = {3, 3, 1, 0, 0, 0};
-__constant__ int kTPb[6] = {0, 0, 0, 1, 3, 3};
-__constant__ int kTPc[6] = {1, 2, 3, 2, 2, 1};
+// Disconnected term t (t = 1..6 of gramsci.F90:754-818, here 0..5): the
+// role whose randomness gates it and the two roles of its pair product
+// (roles: 0 = root, 1..3 = the other vertices in catalogue-id order).  The
+// -tetra terms (:591-646) use the same gate with the 3-product (gate, pu, pv).
+// Written as functions of a loop index that is unrolled, so every use folds
+// to a constant and no table is indexed at run time.
+__host__ __device__ constexpr int term_gate(int t) { return t < 2 ? 3 : (t == 2 ? 1 : 0); }
+__host__ __device__ constexpr int term_pu(int t) { return t < 3 ? 0 : (t == 3 ? 1 : 3); }
+__host__ __device__ constexpr int term_pv(int t) { return t < 3 ? t + 1 : (t == 5 ? 1 : 2); }
+
+// index (0..5) of the clique edge between vertices u != v: (0,1) (0,2) (0,3)
+// (1,2) (1,3) (2,3)
+__device__ __forceinline__ int qedge(int u, int v) {
+  const int a = min(u, v), b = max(u, v);
+  return a * (7 - a) / 2 - 1 + b - a;
+}
+// radial bin of edge (u, v) from the six bins packed a byte each
+__device__ __forceinline__ int qbin(unsigned long long packed, int u, int v) {
+  return (int)((packed >> (8 * qedge(u, v))) & 0xffull);
+}
+__device__ __forceinline__ double qsel(int i, const QVerts& V) {
+  return i == 0 ? V.w[0] : (i == 1 ? V.w[1] : (i == 2 ? V.w[2] : V.w[3]));
+}
+
+// The three vertices other than root r, ordered by catalogue id (the
+// reference's id-sorted row): a three-element sorting network on registers.
+template <int R>
+__device__ __forceinline__ void others_by_id(const QVerts& V, int& u0, int& u1, int& u2) {
+  constexpr int O0 = R == 0 ? 1 : 0, O1 = R <= 1 ? 2 : 1, O2 = R <= 2 ? 3 : 2;
+  int g0 = V.og[O0], g1 = V.og[O1], g2 = V.og[O2];
+  u0 = O0;
+  u1 = O1;
+  u2 = O2;
+  int t;
+  if (g0 > g1) { t = g0; g0 = g1; g1 = t; t = u0; u0 = u1; u1 = t; }
+  if (g1 > g2) { t = g1; g1 = g2; g2 = t; t = u1; u1 = u2; u2 = t; }
+  if (g0 > g1) { t = g0; g0 = g1; g1 = t; t = u0; u0 = u1; u1 = t; }
+}
 
 // query_graph_tetrahedron: a 4-clique with all six edges in bin b counts from
 // each non-buffer vertex (no row-length condition).
+template <bool WEIGHTED, int R>
+__device__ __forceinline__ int tetra_root(const QuadCtx& X, const QVerts& V, int b, unsigned rndm,
+                                          int nr) {
+  if (V.fl[R] & FLAG_BUFFER) return 0;
+  int u0, u1, u2;
+  others_by_id<R>(V, u0, u1, u2);
+  const int role[4] = {R, u0, u1, u2};
+  const int nb = X.nbins;
+  atomicAdd(&X.cnt[(b - 1) + nb * nr], 1ull);
+  if (WEIGHTED)
+    fix_add(&X.fix[(b - 1) + nb * nr], &X.fix[(b - 1) + nb * (nr + 5)],
+            ((V.w[R] * qsel(u0, V)) * qsel(u1, V)) * qsel(u2, V), X.fscale);
+#pragma unroll
+  for (int tt = 0; tt < 6; ++tt) {
+    if (!((rndm >> role[term_gate(tt)]) & 1u)) continue;
+    const int ua = role[term_gate(tt)], ub = role[term_pu(tt)], uc = role[term_pv(tt)];
+    const int nr3 = (int)((rndm >> ua) & 1u) + (int)((rndm >> ub) & 1u) + (int)((rndm >> uc) & 1u);
+    const int kt = (b - 1) + nb * tt;
+    const double qv = WEIGHTED ? (qsel(ua, V) * qsel(ub, V)) * qsel(uc, V) : 0.0;
+    atomicAdd(&X.dcnt[kt + nb * 6 * nr3], 1ull);
+    if (WEIGHTED) fix_add(&X.dfix[kt + nb * 6 * nr3], &X.dfix[kt + nb * 6 * (nr3 + 5)], qv, X.dscale);
+    if (((rndm >> ub) & 1u) && ((rndm >> uc) & 1u)) {
+      atomicAdd(&X.dcnt[kt + nb * 24], 1ull);
+      if (WEIGHTED) fix_add(&X.dfix[kt + nb * 24], &X.dfix[kt + nb * 54], qv, X.dscale);
+    }
+  }
+  return 1;
+}
+
 template <bool WEIGHTED>
-__device__ __forceinline__ int tetra_contrib(const DevCatalog& C, const QuadCtx& X, const int v[4],
-                                             const uint32_t m[6]) {
+__device__ __forceinline__ int tetra_contrib(const QuadCtx& X, const QVerts& V, const uint32_t m[6]) {
   const int b = meta_bin(m[0]);
 #pragma unroll
   for (int k = 1; k < 6; ++k)
     if (meta_bin(m[k]) != b) return 0;
-  uint8_t fl[4];
-  int og[4];
-  double w[4];
-  bool rnd[4];
-  int nr = 0;
+  unsigned rndm = 0;
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    fl[k] = C.flags[v[k]];
-    og[k] = C.orig[v[k]];
-    w[k] = WEIGHTED ? C.w[v[k]] : 0.0;
-    rnd[k] = fl[k] & FLAG_RANDOM;
-    nr += rnd[k];
-  }
-  const int nb = X.nbins;
-  int n = 0;
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    if (fl[r] & FLAG_BUFFER) continue;
-    int o[3], t = 0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-      if (k != r) o[t++] = k;
-    int q;
-    if (og[o[0]] > og[o[1]]) { q = o[0]; o[0] = o[1]; o[1] = q; }
-    if (og[o[1]] > og[o[2]]) { q = o[1]; o[1] = o[2]; o[2] = q; }
-    if (og[o[0]] > og[o[1]]) { q = o[0]; o[0] = o[1]; o[1] = q; }
-    const int role[4] = {r, o[0], o[1], o[2]};
-    atomicAdd(&X.cnt[(b - 1) + nb * nr], 1ull);
-    if (WEIGHTED)
-      fix_add(&X.fix[(b - 1) + nb * nr], &X.fix[(b - 1) + nb * (nr + 5)],
-              ((w[r] * w[o[0]]) * w[o[1]]) * w[o[2]], X.fscale);
-#pragma unroll
-    for (int tt = 0; tt < 6; ++tt) {
-      if (!rnd[role[kTGate[tt]]]) continue;
-      const int ua = role[kTPa[tt]], ub = role[kTPb[tt]], uc = role[kTPc[tt]];
-      const int nr3 = (int)rnd[ua] + (int)rnd[ub] + (int)rnd[uc];
-      const int kt = (b - 1) + nb * tt;
-      const double qv = WEIGHTED ? (w[ua] * w[ub]) * w[uc] : 0.0;
-      atomicAdd(&X.dcnt[kt + nb * 6 * nr3], 1ull);
-      if (WEIGHTED) fix_add(&X.dfix[kt + nb * 6 * nr3], &X.dfix[kt + nb * 6 * (nr3 + 5)], qv, X.dscale);
-      if (rnd[ub] && rnd[uc]) {
-        atomicAdd(&X.dcnt[kt + nb * 24], 1ull);
-        if (WEIGHTED) fix_add(&X.dfix[kt + nb * 24], &X.dfix[kt + nb * 54], qv, X.dscale);
-      }
-    }
-    n++;
-  }
-  return n;
+  for (int k = 0; k < 4; ++k) rndm |= (unsigned)(V.fl[k] & FLAG_RANDOM) << k;
+  const int nr = __popc(rndm);
+  return tetra_root<WEIGHTED, 0>(X, V, b, rndm, nr) + tetra_root<WEIGHTED, 1>(X, V, b, rndm, nr) +
+         tetra_root<WEIGHTED, 2>(X, V, b, rndm, nr) + tetra_root<WEIGHTED, 3>(X, V, b, rndm, nr);
 }
 
-template <bool WEIGHTED>
-__device__ __forceinline__ int quad_contrib(const DevCatalog& C, const CSRView& G, const QuadCtx& X,
-                                            const int v[4], const uint32_t m[6]) {
-  // m: (0,1) (0,2) (0,3) (1,2) (1,3) (2,3)
-  int B[4][4];
-  B[0][1] = B[1][0] = meta_bin(m[0]);
-  B[0][2] = B[2][0] = meta_bin(m[1]);
-  B[0][3] = B[3][0] = meta_bin(m[2]);
-  B[1][2] = B[2][1] = meta_bin(m[3]);
-  B[1][3] = B[3][1] = meta_bin(m[4]);
-  B[2][3] = B[3][2] = meta_bin(m[5]);
-  uint8_t fl[4];
-  int og[4];
-  double w[4];
-  bool rnd[4];
-  int nr = 0;
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    fl[k] = C.flags[v[k]];
-    og[k] = C.orig[v[k]];
-    w[k] = WEIGHTED ? C.w[v[k]] : 0.0;
-    rnd[k] = fl[k] & FLAG_RANDOM;
-    nr += rnd[k];
-  }
+// One root R of a 4-clique for query_4pcf_all2: canonical perimeter check,
+// N2 / N3 at (cfg, bin(r,k2), bin(k1,k3)) and the six disconnected terms.
+template <bool WEIGHTED, int R>
+__device__ __forceinline__ int quad_root(const QuadCtx& X, const QVerts& V, unsigned long long packed,
+                                         unsigned rndm, int nr) {
+  if (V.fl[R] & FLAG_BUFFER) return 0;
+  if (!(V.fl[R] & kFlagDeg4)) return 0;
+  int u0, u1, u2;
+  others_by_id<R>(V, u0, u1, u2);
+  const int b1 = qbin(packed, R, u0), b2 = qbin(packed, u0, u1), b3 = qbin(packed, u1, u2),
+            b4 = qbin(packed, R, u2);
+  if (!(b1 <= b2 && b2 <= b3 && b3 <= b4)) return 0;
   const int nb2 = X.nbins + 2;
-  int n = 0;
+  const int cfg = 1 + (X.F[b1] - X.F[1]) + (X.F[nb2 + b2] - X.F[nb2 + b1]) +
+                  (X.F[2 * nb2 + b3] - X.F[2 * nb2 + b2]) + (X.F[3 * nb2 + b4] - X.F[3 * nb2 + b3]);
+  const int d1 = qbin(packed, R, u1), d2 = qbin(packed, u0, u2);
+  const int kk = (cfg - 1) + X.ncfg * ((d1 - 1) + X.nbins * (d2 - 1));
+  atomicAdd(&X.cnt[kk + X.nbin * nr], 1ull);
+  if (WEIGHTED)
+    fix_add(&X.fix[kk + X.nbin * nr], &X.fix[kk + X.nbin * (nr + 5)],
+            ((V.w[R] * qsel(u0, V)) * qsel(u1, V)) * qsel(u2, V), X.fscale);
+  const int role[4] = {R, u0, u1, u2};
 #pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    if (fl[r] & FLAG_BUFFER) continue;
-    if (G.deg_full[v[r]] <= 3) continue;
-    int o[3], t = 0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-      if (k != r) o[t++] = k;
-    // order the other three by catalogue id
-    int q;
-    if (og[o[0]] > og[o[1]]) { q = o[0]; o[0] = o[1]; o[1] = q; }
-    if (og[o[1]] > og[o[2]]) { q = o[1]; o[1] = o[2]; o[2] = q; }
-    if (og[o[0]] > og[o[1]]) { q = o[0]; o[0] = o[1]; o[1] = q; }
-    const int b1 = B[r][o[0]], b2 = B[o[0]][o[1]], b3 = B[o[1]][o[2]], b4 = B[r][o[2]];
-    if (!(b1 <= b2 && b2 <= b3 && b3 <= b4)) continue;
-    const int cfg = 1 + (X.F[b1] - X.F[1]) + (X.F[nb2 + b2] - X.F[nb2 + b1]) +
-                    (X.F[2 * nb2 + b3] - X.F[2 * nb2 + b2]) + (X.F[3 * nb2 + b4] - X.F[3 * nb2 + b3]);
-    const int d1 = B[r][o[1]], d2 = B[o[0]][o[2]];
-    const int kk = (cfg - 1) + X.ncfg * ((d1 - 1) + X.nbins * (d2 - 1));
-    atomicAdd(&X.cnt[kk + X.nbin * nr], 1ull);
+  for (int tt = 0; tt < 6; ++tt) {
+    if (!((rndm >> role[term_gate(tt)]) & 1u)) continue;
+    const int u = role[term_pu(tt)], vv = role[term_pv(tt)];
+    const int npr = (int)((rndm >> u) & 1u) + (int)((rndm >> vv) & 1u);
+    const int kt = kk + X.nbin * tt;
+    const double q = WEIGHTED ? qsel(u, V) * qsel(vv, V) : 0.0;
+    atomicAdd(&X.dcnt[kt + X.nbin * 6 * npr], 1ull);
     if (WEIGHTED)
-      fix_add(&X.fix[kk + X.nbin * nr], &X.fix[kk + X.nbin * (nr + 5)],
-              ((w[r] * w[o[0]]) * w[o[1]]) * w[o[2]], X.fscale);
-    const int role[4] = {r, o[0], o[1], o[2]};
-#pragma unroll
-    for (int tt = 0; tt < 6; ++tt) {
-      if (!rnd[role[kGate[tt]]]) continue;
-      const int u = role[kPu[tt]], vv = role[kPv[tt]];
-      const int npr = (int)rnd[u] + (int)rnd[vv];
-      const int kt = kk + X.nbin * tt;
-      const double q = WEIGHTED ? w[u] * w[vv] : 0.0;
-      atomicAdd(&X.dcnt[kt + X.nbin * 6 * npr], 1ull);
-      if (WEIGHTED)
-        fix_add(&X.dfix[kt + X.nbin * 6 * npr], &X.dfix[kt + X.nbin * (6 * npr + 24)], q, X.dscale);
-      if (npr == 2) {
-        atomicAdd(&X.dcnt[kt + X.nbin * 18], 1ull);
-        if (WEIGHTED) fix_add(&X.dfix[kt + X.nbin * 18], &X.dfix[kt + X.nbin * 42], q, X.dscale);
-      }
+      fix_add(&X.dfix[kt + X.nbin * 6 * npr], &X.dfix[kt + X.nbin * (6 * npr + 24)], q, X.dscale);
+    if (npr == 2) {
+      atomicAdd(&X.dcnt[kt + X.nbin * 18], 1ull);
+      if (WEIGHTED) fix_add(&X.dfix[kt + X.nbin * 18], &X.dfix[kt + X.nbin * 42], q, X.dscale);
     }
-    n++;
   }
-  return n;
+  return 1;
 }
 
+// m: bins of (0,1) (0,2) (0,3) (1,2) (1,3) (2,3) for vertices 0 = p, 1 = a,
+// 2 = b, 3 = d.
 template <bool WEIGHTED>
-__global__ void __launch_bounds__(kQuadThreads) quad4_kernel(DevCatalog C, CSRView G, QuadParams Q,
-                                                             unsigned long long* __restrict__ g_cnt,
-                                                             unsigned long long* __restrict__ g_fix,
-                                                             unsigned long long* __restrict__ d_cnt,
-                                                             unsigned long long* __restrict__ d_fix,
-                                                             double fscale, double dscale,
-                                                             unsigned long long* __restrict__ stats) {
+__device__ __forceinline__ int quad_contrib(const QuadCtx& X, const QVerts& V, const uint32_t m[6]) {
+  unsigned long long packed = 0;
+#pragma unroll
+  for (int e = 0; e < 6; ++e) packed |= (unsigned long long)meta_bin(m[e]) << (8 * e);
+  unsigned rndm = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) rndm |= (unsigned)(V.fl[k] & FLAG_RANDOM) << k;
+  const int nr = __popc(rndm);
+  return quad_root<WEIGHTED, 0>(X, V, packed, rndm, nr) + quad_root<WEIGHTED, 1>(X, V, packed, rndm, nr) +
+         quad_root<WEIGHTED, 2>(X, V, packed, rndm, nr) + quad_root<WEIGHTED, 3>(X, V, packed, rndm, nr);
+}
+
+__device__ __forceinline__ uint32_t qfib_slot(uint32_t off, int lg) {
+  return (off * 2654435769u) >> (32 - lg);
+}
+
+// Histogram copies: block b accumulates into copy b % ncopy of the layout
+// [cnt nh][dcnt nd][fix 2 nh][dfix 2 nd] (fix arrays when weighted), so
+// that blocks do not contend for the same global addresses; quad_merge_kernel
+// sums the copies.
+template <bool WEIGHTED>
+__global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
+    DevCatalog C, CSRView G, QuadParams Q, unsigned long long* __restrict__ priv, int ncopy,
+    int nh, int nd, double fscale, double dscale, unsigned long long* __restrict__ stats,
+    int* __restrict__ work) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const QuadLayout L = quad_layout(Q.nbins, Q.cap);
+  const QuadLayout L = quad_layout(Q.nbins, Q.cap, blockDim.x >> 5);
   int* s_F = reinterpret_cast<int*>(smem + L.off_rank);
   const int nb2 = Q.nbins + 2;
   for (int k = threadIdx.x; k < 4 * nb2; k += blockDim.x) s_F[k] = Q.rank.F[k / nb2][k % nb2];
@@ -220,123 +246,216 @@ __global__ void __launch_bounds__(kQuadThreads) quad4_kernel(DevCatalog C, CSRVi
   X.F = s_F;
   X.nbins = Q.nbins;
   X.ncfg = Q.ncfg;
-  X.nbin = Q.ncfg * Q.nbins * Q.nbins;
+  X.nbin = Q.tetra ? Q.nbins : Q.ncfg * Q.nbins * Q.nbins;
   X.tetra = Q.tetra;
-  X.cnt = g_cnt;
-  X.fix = g_fix;
-  X.dcnt = d_cnt;
-  X.dfix = d_fix;
+  {
+    const size_t per = (size_t)(nh + nd) * (WEIGHTED ? 3 : 1);
+    unsigned long long* base = priv + per * (size_t)(blockIdx.x % ncopy);
+    X.cnt = base;
+    X.dcnt = base + nh;
+    X.fix = WEIGHTED ? base + nh + nd : nullptr;
+    X.dfix = WEIGHTED ? base + nh + nd + 2 * (size_t)nh : nullptr;
+  }
   X.fscale = fscale;
   X.dscale = dscale;
 
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
-  const int wib = threadIdx.x >> 5;
-  unsigned char* wb = smem + L.off_warp + L.warp_bytes * wib;
+  unsigned char* wb = smem + L.off_warp + L.warp_bytes * (threadIdx.x >> 5);
+  long long* s_rs = reinterpret_cast<long long*>(wb + L.o_rs);
+  double* s_w = reinterpret_cast<double*>(wb + L.o_w);
+  unsigned long long* s_mo = reinterpret_cast<unsigned long long*>(wb + L.o_mo);
+  int* s_col = reinterpret_cast<int*>(wb + L.o_col);
+  int* s_len = reinterpret_cast<int*>(wb + L.o_len);
+  uint32_t* s_xm = reinterpret_cast<uint32_t*>(wb + L.o_xm);
+  uint32_t* s_hkey = reinterpret_cast<uint32_t*>(wb + L.o_hkey);
+  unsigned long long* s_q = reinterpret_cast<unsigned long long*>(wb + L.o_q);
+  uint16_t* s_xy = reinterpret_cast<uint16_t*>(wb + L.o_xy);
+  uint16_t* s_xz = reinterpret_cast<uint16_t*>(wb + L.o_xz);
+  uint32_t* s_bits = reinterpret_cast<uint32_t*>(wb + L.o_bits);
   const int cap = Q.cap;
-  long long* r_start = reinterpret_cast<long long*>(wb);
-  long long* x_start = reinterpret_cast<long long*>(wb + (size_t)cap * 8);
-  int* r_col = reinterpret_cast<int*>(wb + (size_t)cap * 16);
-  uint32_t* r_meta = reinterpret_cast<uint32_t*>(wb + (size_t)cap * 20);
-  int* r_len = reinterpret_cast<int*>(wb + (size_t)cap * 24);
-  int* x_c = reinterpret_cast<int*>(wb + (size_t)cap * 28);
-  int* x_y = reinterpret_cast<int*>(wb + (size_t)cap * 32);
-  uint32_t* x_m = reinterpret_cast<uint32_t*>(wb + (size_t)cap * 36);
-  int* x_pre = reinterpret_cast<int*>(wb + (size_t)cap * 40);
-
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int lg_max = qhash_lg_max(cap);
   unsigned long long quads = 0, rooted = 0, probes = 0;
 
-  for (int p = warp; p < C.n; p += nwarps) {
+  // position of label c in R+(p) via the hash table, or -1
+  auto lookup = [&](int c, int p, int lg, bool live) -> int {
+    const int off = c - p;
+    live = live && off > 0 && off < kQMaxOffset;
+    const int hs = 1 << lg;
+    uint32_t h = qfib_slot((uint32_t)off, lg);
+    uint32_t e = live ? s_hkey[h] : 0u;
+    bool hit = live && (e >> 10) == (uint32_t)off;
+    bool open = live && !hit && e != 0u;
+    for (int it = 1; it < hs && __any_sync(0xffffffffu, open); ++it) {
+      if (open) {
+        h = (h + 1) & (uint32_t)(hs - 1);
+        e = s_hkey[h];
+        hit = (e >> 10) == (uint32_t)off;
+        open = !hit && e != 0u;
+      }
+    }
+    return hit ? (int)(e & 0x3ffu) : -1;
+  };
+
+  for (;;) {
+    int p = 0;
+    if (lane == 0) p = atomicAdd(work, 1);
+    p = __shfl_sync(0xffffffffu, p, 0);
+    if (p >= C.n) break;
     const int64_t b0 = G.start[p];
     const int k = G.len[p];
     if (k < 3 || k > cap) continue;  // rows longer than cap are rejected on the host
+    if (rec_col(G.rec[b0 + k - 1]) - p >= kQMaxOffset) {
+      if (lane == 0) atomicMax(&stats[3], 1ull);  // reported to the host
+      continue;
+    }
+    const uint8_t fp = C.flags[p] | (G.deg_full[p] > 3 ? kFlagDeg4 : 0);
+    const int op = C.orig[p];
+    const double wp = WEIGHTED ? C.w[p] : 0.0;
+    int lg = 6;
+    while (lg < lg_max && (1 << lg) < 8 * k) ++lg;
+    const int hs = 1 << lg;
     __syncwarp();
-    for (int x = lane; x < k; x += 32) {
-      const unsigned long long rr = G.rec[b0 + x];
-      int a = rec_col(rr);
-      r_col[x] = a;
-      r_meta[x] = rec_meta(rr);
-      r_start[x] = G.start[a];
-      r_len[x] = G.len[a];
+    for (int h = lane; h < hs; h += 32) s_hkey[h] = 0u;
+    __syncwarp();
+    for (int xb = 0; xb < k; xb += 32) {
+      const int x = xb + lane;
+      if (x < k) {
+        const unsigned long long r = G.rec[b0 + x];
+        const int a = rec_col(r);
+        s_col[x] = a;
+        s_rs[x] = G.start[a];
+        s_len[x] = G.len[a];
+        const uint8_t fa = C.flags[a] | (G.deg_full[a] > 3 ? kFlagDeg4 : 0);
+        s_mo[x] = ((unsigned long long)(uint32_t)C.orig[a] << 32) |
+                  (rec_meta(r) | ((uint32_t)fa << 24));
+        if (WEIGHTED) s_w[x] = C.w[a];
+        const uint32_t off = (uint32_t)(a - p);
+        const uint32_t key = (off << 10) | (uint32_t)x;
+        uint32_t h = qfib_slot(off, lg);
+        for (int t = 0; t < hs; ++t) {
+          if (atomicCAS(&s_hkey[h], 0u, key) == 0u) break;
+          h = (h + 1) & (uint32_t)(hs - 1);
+        }
+      }
     }
     __syncwarp();
+    const int nwords = (k + 31) >> 5;
     for (int x = 0; x < k - 2; ++x) {
-      const int a = r_col[x];
-      const int64_t ra = r_start[x];
-      const int ka = r_len[x];
-      // X = R+(a) ∩ R+(p), entries beyond position x of R+(p)
+      // X = R+(a) ∩ R+(p) beyond position x, listed in label order and
+      // marked in the bitmask
+      for (int wd = lane; wd < nwords; wd += 32) s_bits[wd] = 0u;
+      __syncwarp();
+      const int64_t ra = s_rs[x];
+      const int ka = s_len[x];
+      if (lane == 0) probes += (unsigned long long)ka;
       int nx = 0;
       for (int j0 = 0; j0 < ka; j0 += 32) {
-        int j = j0 + lane;
-        bool found = false;
-        int c = 0, y = 0;
+        const int j = j0 + lane;
         unsigned long long rr = 0;
-        if (j < ka) {
-          rr = G.rec[ra + j];
-          c = rec_col(rr);
-          y = x + 1 + qlower_bound(r_col + x + 1, k - x - 1, c);
-          found = y < k && r_col[y] == c;
-        }
-        unsigned msk = __ballot_sync(0xffffffffu, found);
+        if (j < ka) rr = G.rec[ra + j];
+        const int y = lookup(rec_col(rr), p, lg, j < ka);
+        const bool found = y > x;
+        const unsigned msk = __ballot_sync(0xffffffffu, found);
         if (found) {
-          int pos = nx + __popc(msk & lt);
-          x_c[pos] = c;
-          x_y[pos] = y;
-          x_m[pos] = rec_meta(rr);
-          x_start[pos] = G.start[c];
+          const int z = nx + __popc(msk & lt);
+          s_xy[z] = (uint16_t)y;
+          s_xm[z] = rec_meta(rr);
+          s_xz[y] = (uint16_t)z;
+          atomicOr(&s_bits[y >> 5], 1u << (y & 31));
         }
         nx += __popc(msk);
       }
-      if (lane == 0) probes += (unsigned long long)ka;
       __syncwarp();
       if (nx < 2) continue;
-      // prefix over |R+(b)| for b in X
-      int carry = 0;
+      const unsigned long long mpa_w = s_mo[x];
+      int qn = 0;
+      // one queued clique: (p, a = row x, b = X entry z, d = row y_d)
+      auto drain_one = [&](int e) {
+        const unsigned long long qe = s_q[e];
+        const int z = (int)(qe & 0x3ffu), yd = (int)((qe >> 10) & 0x3ffu);
+        const uint32_t mbd = (uint32_t)(qe >> 32);
+        const int yb = s_xy[z];
+        const unsigned long long mpb_w = s_mo[yb], mpd_w = s_mo[yd];
+        QVerts V;
+        V.fl[0] = fp;
+        V.fl[1] = (uint8_t)((uint32_t)mpa_w >> 24);
+        V.fl[2] = (uint8_t)((uint32_t)mpb_w >> 24);
+        V.fl[3] = (uint8_t)((uint32_t)mpd_w >> 24);
+        V.og[0] = op;
+        V.og[1] = (int)(mpa_w >> 32);
+        V.og[2] = (int)(mpb_w >> 32);
+        V.og[3] = (int)(mpd_w >> 32);
+        V.w[0] = wp;
+        V.w[1] = WEIGHTED ? s_w[x] : 0.0;
+        V.w[2] = WEIGHTED ? s_w[yb] : 0.0;
+        V.w[3] = WEIGHTED ? s_w[yd] : 0.0;
+        // m: (p,a) (p,b) (p,d) (a,b) (a,d) (b,d)
+        const uint32_t m[6] = {(uint32_t)mpa_w & 0xffffffu, (uint32_t)mpb_w & 0xffffffu,
+                               (uint32_t)mpd_w & 0xffffffu, s_xm[z], s_xm[s_xz[yd]], mbd};
+        const int nroot = X.tetra ? tetra_contrib<WEIGHTED>(X, V, m) : quad_contrib<WEIGHTED>(X, V, m);
+        quads += nroot > 0;
+        rooted += nroot;
+      };
+      // work items (b = X[z], d in R+(b)), X entries in batches of 32
       for (int zb = 0; zb < nx; zb += 32) {
-        int z = zb + lane;
+        const int z = zb + lane;
         int len = 0;
-        if (z < nx) len = G.len[x_c[z]];
-        int incl = len;
+        long long rs = 0;
+        if (z < nx) {
+          const int yb = s_xy[z];
+          len = s_len[yb];
+          rs = s_rs[yb];
+        }
+        const unsigned nz = __ballot_sync(0xffffffffu, len > 0);
+        const int nrows = __popc(nz);
+        const int src = lane < nrows ? (int)__fns(nz, 0, lane + 1) : 0;
+        // every lane takes part in each shuffle; the select comes after
+        const int slen = __shfl_sync(0xffffffffu, len, src);
+        const int clen = lane < nrows ? slen : 0;
+        const long long crs = __shfl_sync(0xffffffffu, rs, src);
+        const int cz = zb + src;
+        int incl = clen;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-          int yy = __shfl_up_sync(0xffffffffu, incl, o);
-          if (lane >= o) incl += yy;
+          const int yv = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += yv;
         }
-        if (z < nx) x_pre[z + 1] = carry + incl;
-        carry += __shfl_sync(0xffffffffu, incl, 31);
+        const int tot = __shfl_sync(0xffffffffu, incl, 31);
+        const int excl = incl - clen;
+        if (lane == 0) probes += (unsigned long long)tot;
+        int done = 0;  // compacted rows that ended before the window
+        for (int t0 = 0; t0 < tot; t0 += 32) {
+          const int last = incl - 1 - t0;
+          const unsigned bit = (lane < nrows && last >= 0 && last < 32) ? (1u << last) : 0u;
+          const unsigned ends = __reduce_or_sync(0xffffffffu, bit);
+          const int j = (done + __popc(ends & lt)) & 31;
+          done += __popc(ends);
+          const long long ors = __shfl_sync(0xffffffffu, crs, j);
+          const int oex = __shfl_sync(0xffffffffu, excl, j);
+          const int oz = __shfl_sync(0xffffffffu, cz, j);
+          const int t = t0 + lane;
+          unsigned long long rr = 0;
+          if (t < tot) rr = G.rec[ors + (t - oex)];
+          const int yd = lookup(rec_col(rr), p, lg, t < tot);
+          const bool hit = yd >= 0 && ((s_bits[yd >> 5] >> (yd & 31)) & 1u);
+          const unsigned m = __ballot_sync(0xffffffffu, hit);
+          if (hit) {
+            const int pos = qn + __popc(m & lt);
+            s_q[pos] = ((unsigned long long)rec_meta(rr) << 32) | (uint32_t)(oz | (yd << 10));
+          }
+          qn += __popc(m);
+          if (qn >= 32) {
+            __syncwarp();
+            drain_one(qn - 32 + lane);
+            qn -= 32;
+            __syncwarp();
+          }
+        }
       }
-      if (lane == 0) x_pre[0] = 0;
+      // the X data of this a are replaced next: drain what is left
       __syncwarp();
-      const int W = carry;
-      if (lane == 0) probes += (unsigned long long)W;
-      for (int base = 0; base < W; base += 32) {
-        const int f = base + lane;
-        if (f >= W) break;
-        int lo = 0, hi = nx - 1;
-        while (lo < hi) {
-          int mid = (lo + hi + 1) >> 1;
-          if (x_pre[mid] <= f)
-            lo = mid;
-          else
-            hi = mid - 1;
-        }
-        const int z = lo;
-        const int64_t e = x_start[z] + (f - x_pre[z]);
-        const unsigned long long rr = G.rec[e];
-        const int d = rec_col(rr);
-        const int z2 = z + 1 + qlower_bound(x_c + z + 1, nx - z - 1, d);
-        if (z2 < nx && x_c[z2] == d) {
-          const int v[4] = {p, a, x_c[z], d};
-          const uint32_t m[6] = {r_meta[x], r_meta[x_y[z]], r_meta[x_y[z2]],
-                                 x_m[z],    x_m[z2],        rec_meta(rr)};
-          int nroot = X.tetra ? tetra_contrib<WEIGHTED>(C, X, v, m)
-                              : quad_contrib<WEIGHTED>(C, G, X, v, m);
-          quads += nroot > 0;
-          rooted += nroot;
-        }
-      }
+      if (lane < qn) drain_one(lane);
       __syncwarp();
     }
   }
@@ -353,33 +472,93 @@ __global__ void __launch_bounds__(kQuadThreads) quad4_kernel(DevCatalog C, CSRVi
   }
 }
 
+// Sum of the histogram copies into the outputs (counts as integers, fixed
+// point as 128-bit pairs): deterministic, every output entry written.
+__global__ void quad_merge_kernel(const unsigned long long* __restrict__ priv, int ncopy, int nh,
+                                  int nd, bool weighted, unsigned long long* __restrict__ g_cnt,
+                                  unsigned long long* __restrict__ g_fix,
+                                  unsigned long long* __restrict__ d_cnt,
+                                  unsigned long long* __restrict__ d_fix) {
+  const size_t per = (size_t)(nh + nd) * (weighted ? 3 : 1);
+  const int total = nh + nd;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+    const bool dterm = k >= nh;
+    const int kk = dterm ? k - nh : k;
+    const int nn = dterm ? nd : nh;
+    unsigned long long cnt = 0, lo = 0, hi = 0;
+    for (int c = 0; c < ncopy; ++c) {
+      const unsigned long long* b = priv + per * (size_t)c;
+      cnt += b[k];
+      if (weighted) {
+        const unsigned long long* f = b + nh + nd + (dterm ? 2 * (size_t)nh : 0);
+        const unsigned long long l2 = f[kk], h2 = f[nn + kk];
+        const unsigned long long s = lo + l2;
+        hi += h2 + (s < lo ? 1ull : 0ull);
+        lo = s;
+      }
+    }
+    if (dterm) {
+      d_cnt[kk] = cnt;
+      if (weighted) {
+        d_fix[kk] = lo;
+        d_fix[nn + kk] = hi;
+      }
+    } else {
+      g_cnt[kk] = cnt;
+      if (weighted) {
+        g_fix[kk] = lo;
+        g_fix[nn + kk] = hi;
+      }
+    }
+  }
+}
+
+// Warps per block: as many as fit in shared memory (at most 32).
+int quad4_warps(int nbins, int cap) {
+  int nw = kQuadMaxWarps;
+  while (nw > 1 && quad_layout(nbins, cap, nw).total > kQuadSmemLimit) nw -= 1;
+  return nw;
+}
+
 }  // namespace
 
 void launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bool weighted,
                   unsigned long long* g_cnt, unsigned long long* g_fix, unsigned long long* d_cnt,
-                  unsigned long long* d_fix, double fscale, double dscale,
-                  unsigned long long* stats, cudaStream_t s) {
-  if (C.n <= 0) return;
-  QuadLayout L = quad_layout(Q.nbins, Q.cap);
-  size_t smem = L.total;
-#define GR_QUAD_LAUNCH(W)                                                                     \
-  do {                                                                                        \
-    auto kfn = quad4_kernel<W>;                                                               \
-    GR_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
-                                     (int)smem));                                             \
-    int per_sm = 0;                                                                           \
-    GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kQuadThreads, smem)); \
-    if (per_sm < 1) per_sm = 1;                                                               \
-    int64_t blocks = (int64_t)per_sm * 148;                                                   \
-    int64_t need = ((int64_t)C.n + kQuadWarps - 1) / kQuadWarps;                              \
-    if (blocks > need) blocks = need;                                                         \
-    kfn<<<(unsigned)blocks, kQuadThreads, smem, s>>>(C, G, Q, g_cnt, g_fix, d_cnt, d_fix, fscale, dscale, stats); \
-  } while (0)
-  if (weighted) GR_QUAD_LAUNCH(true); else GR_QUAD_LAUNCH(false);
-#undef GR_QUAD_LAUNCH
+                  unsigned long long* d_fix, int nh, int nd, double fscale, double dscale,
+                  DevBuf<unsigned long long>& priv, unsigned long long* stats, int* work,
+                  cudaStream_t s) {
+  const int nw = quad4_warps(Q.nbins, Q.cap);
+  const size_t smem = quad_layout(Q.nbins, Q.cap, nw).total;
+  if (smem > kQuadSmemLimit) throw Error{-2, "4PCF: per-warp shared memory exceeds the SM limit"};
+  const size_t per = (size_t)(nh + nd) * (weighted ? 3 : 1);
+  auto kfn = weighted ? quad4_kernel<true> : quad4_kernel<false>;
+  GR_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nw * 32, smem));
+  if (per_sm < 1) per_sm = 1;
+  int64_t blocks = (int64_t)per_sm * 148;
+  const int64_t need = ((int64_t)C.n + nw - 1) / nw;
+  if (blocks > need) blocks = need;
+  if (blocks < 1) blocks = 1;
+  // one copy of the histograms: per-block copies measured no faster (L2
+  // atomics on distinct blocks' copies cost the same on this workload)
+  const int64_t ncopy = 1;
+  priv.reserve((size_t)ncopy * per);
+  GR_CUDA_TRY(cudaMemsetAsync(priv.p, 0, sizeof(unsigned long long) * (size_t)ncopy * per, s));
+  if (C.n > 0) {
+    GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));
+    kfn<<<(unsigned)blocks, nw * 32, smem, s>>>(C, G, Q, priv.p, (int)ncopy, nh, nd, fscale, dscale,
+                                                stats, work);
+    GR_CHECK_LAUNCH();
+  }
+  const int mb = (int)std::min<int64_t>((nh + nd + 255) / 256, 148 * 8);
+  quad_merge_kernel<<<mb, 256, 0, s>>>(priv.p, (int)ncopy, nh, nd, weighted, g_cnt, g_fix, d_cnt,
+                                       d_fix);
   GR_CHECK_LAUNCH();
 }
 
-size_t quad4_smem_bytes(int nbins, int cap) { return quad_layout(nbins, cap).total; }
+size_t quad4_smem_bytes(int nbins, int cap) {
+  return quad_layout(nbins, cap, quad4_warps(nbins, cap)).total;
+}
 
 }  // namespace gr
