@@ -148,6 +148,172 @@ __global__ void __launch_bounds__(kPairThreads) pair2_kernel(DevCatalog C, PairP
 }
 
 
+// Queued variant of the warp-per-cell sweep: the membership test (FP32
+// squared separation, FP64 inside the guard band at rmin and rmax) runs for
+// every candidate, the edges go to a per-warp queue, and the bins, the
+// line-of-sight cosines and the histogram updates run 32 edges at a time
+// with every lane busy.  Pays off where most candidates are not edges.
+constexpr int kPairQueue = 64;
+
+template <bool F32, bool WEIGHTED, bool SHIST>
+__global__ void __launch_bounds__(kPairThreads) pair2_queue_kernel(
+    DevCatalog C, PairParams P, unsigned long long* __restrict__ g_cnt,
+    unsigned long long* __restrict__ g_fix, double fscale, unsigned long long* __restrict__ stats,
+    int* __restrict__ work) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ float4 s_pos[kPairWarps][kCellTile];
+  __shared__ int s_lab[kPairWarps][kCellTile];
+  __shared__ int s_qi[kPairWarps][kPairQueue];      // root index in the cell
+  __shared__ uint8_t s_qf[kPairWarps][kPairQueue];  // tile index of the neighbour
+  const int nbm = P.nbins * P.nmu;
+  const int nh = nbm * 4;
+  unsigned long long* s_cnt = SHIST ? reinterpret_cast<unsigned long long*>(smem) : g_cnt;
+  unsigned long long* s_lo = SHIST ? s_cnt + nh : g_fix;
+  unsigned long long* s_hi = s_lo + nh;
+  if (SHIST) {
+    for (int k = threadIdx.x; k < nh; k += blockDim.x) {
+      s_cnt[k] = 0ull;
+      if (WEIGHTED) {
+        s_lo[k] = 0ull;
+        s_hi[k] = 0ull;
+      }
+    }
+    __syncthreads();
+  }
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  const int ncell = (int)C.grid.ncell;
+  unsigned long long rechecks = 0, cands = 0, pairs = 0;
+  int cb = 0;
+  // bins and both rooted updates of one queued pair (p, q)
+  auto drain_one = [&](int e) {
+    const int f = s_qf[wib][e];
+    const int p = cb + s_qi[wib][e];
+    const int q = s_lab[wib][f];
+    int b = 1, mf = 1, mr = 1;
+    bool ok;
+    if (F32) {
+      const int r = classify_f32<true>(C.pos4[p], s_pos[wib][f], P, b, mf, mr);
+      if (r == 2) {
+        rechecks++;
+        ok = edge_f64(C.posd[p], C.posd[q], P, b, mf, mr);
+      } else {
+        ok = r == 1;
+      }
+    } else {
+      ok = edge_f64(C.posd[p], C.posd[q], P, b, mf, mr);
+    }
+    if (!ok) return;  // cannot happen: the membership test decided the same pair
+    const uint8_t fp = C.flags[p], fq = C.flags[q];
+    const bool root_p = !(fp & FLAG_BUFFER), root_q = !(fq & FLAG_BUFFER);
+    const int rp = fp & FLAG_RANDOM, rq = fq & FLAG_RANDOM;
+    pairs += (root_p || root_q) ? 1 : 0;
+    const double prod = WEIGHTED ? C.w[p] * C.w[q] : 0.0;
+    if (root_p) {
+      const int k = (b - 1) + P.nbins * (mf - 1) + nbm * (2 * rp + rq);
+      atomicAdd(&s_cnt[k], 1ull);
+      if (WEIGHTED) fix_add(&s_lo[k], &s_hi[k], prod, fscale);
+    }
+    if (root_q) {
+      const int k = (b - 1) + P.nbins * (mr - 1) + nbm * (2 * rq + rp);
+      atomicAdd(&s_cnt[k], 1ull);
+      if (WEIGHTED) fix_add(&s_lo[k], &s_hi[k], prod, fscale);
+    }
+  };
+  for (;;) {
+    int cell = 0;
+    if (lane == 0) cell = atomicAdd(work, 1);
+    cell = __shfl_sync(0xffffffffu, cell, 0);
+    if (cell >= ncell) break;
+    cb = C.cell_start[cell];
+    const int ce = C.cell_start[cell + 1];
+    if (cb == ce) continue;
+    Ranges R;
+    {
+      GridParams g;
+      const int* cs;
+      int lkey;
+      cell_grid(C, cell, g, cs, lkey);
+      forward_ranges(cb - 1, lkey, g, cs, R);
+    }
+    int pre[5], total = 0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      pre[k] = total;
+      if (k < R.n) total += R.end[k] - R.beg[k];
+    }
+    int qn = 0;
+    for (int t0 = 0; t0 < total; t0 += kCellTile) {
+      const int tn = min(kCellTile, total - t0);
+      __syncwarp();
+      for (int f = lane; f < tn; f += 32) {
+        const int q = range_label(R, pre, t0 + f);
+        s_lab[wib][f] = q;
+        s_pos[wib][f] = C.pos4[q];
+      }
+      __syncwarp();
+      for (int p = cb; p < ce; ++p) {
+        const int i = p - cb;
+        const int fstart = max(0, i + 1 - t0);
+        if (fstart >= tn) continue;
+        // p itself is candidate i of the flattened ranges
+        const float4 pi = (i >= t0 && i - t0 < tn) ? s_pos[wib][i - t0] : C.pos4[p];
+        for (int f0 = fstart; f0 < tn; f0 += 32) {
+          const int f = f0 + lane;
+          bool e = false;
+          if (f < tn) {
+            int r = F32 ? member_f32(pi, s_pos[wib][f], P) : 2;
+            if (r == 2) {
+              int b, mf, mr;
+              rechecks++;
+              r = edge_f64(C.posd[p], C.posd[s_lab[wib][f]], P, b, mf, mr) ? 1 : 0;
+            }
+            e = r == 1;
+          }
+          const unsigned m = __ballot_sync(0xffffffffu, e);
+          if (e) {
+            s_qi[wib][qn + __popc(m & lt)] = i;
+            s_qf[wib][qn + __popc(m & lt)] = (uint8_t)f;
+          }
+          qn += __popc(m);
+          if (qn >= 32) {
+            __syncwarp();
+            drain_one(qn - 32 + lane);
+            qn -= 32;
+            __syncwarp();
+          }
+        }
+        if (lane == 0) cands += (unsigned long long)(tn - fstart);
+      }
+      // the tile's staged candidates are about to be replaced
+      __syncwarp();
+      if (lane < qn) drain_one(lane);
+      qn = 0;
+      __syncwarp();
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    rechecks += __shfl_xor_sync(0xffffffffu, rechecks, o);
+    pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
+  }
+  if (lane == 0) {
+    if (rechecks) atomicAdd(&stats[0], rechecks);
+    if (cands) atomicAdd(&stats[1], cands);
+    if (pairs) atomicAdd(&stats[2], pairs);
+  }
+  if (SHIST) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < nh; k += blockDim.x) {
+      if (s_cnt[k]) {
+        atomicAdd(&g_cnt[k], s_cnt[k]);
+        if (WEIGHTED) fix_merge(&g_fix[k], &g_fix[nh + k], s_lo[k], s_hi[k]);
+      }
+    }
+  }
+}
+
 // Dense-cell variant: one block per cell, one thread per root, the cell's
 // forward candidates staged in shared memory tiles and read by all threads
 // at the same address (broadcast), so each candidate costs one shared load
@@ -342,7 +508,7 @@ void launch_pair2(const DevCatalog& C, const PairParams& P, bool weighted,
   if (blocks < 1) blocks = 1;
 #define GR_PAIR_LAUNCH(F, W, S)                                                          \
   do {                                                                                   \
-    auto k = pair2_kernel<F, W, S>;                                                      \
+    auto k = variant == kPairWarpQueue ? pair2_queue_kernel<F, W, S> : pair2_kernel<F, W, S>; \
     GR_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
                                      (int)smem));                                        \
     k<<<(unsigned)blocks, kPairThreads, smem, s>>>(C, P, g_cnt, g_fix, fscale, stats, work);           \
