@@ -123,7 +123,8 @@ class Context:
     def set_autotune(self, mode):
         """'on' (time kernel variants once per workload class, cached),
         'off', or an int variant to force (0 warp per cell, 1/2 block per
-        cell of 128/256 threads, 3 warp per cell with queued binning)."""
+        cell of 128/256 threads, 3 warp per cell with queued binning, 4/5
+        block per cell of 128/256 with queued binning)."""
         v = {"off": 0, "on": 1}.get(mode, None)
         if v is None:
             v = 2 + int(mode)

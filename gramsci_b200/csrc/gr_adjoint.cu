@@ -238,7 +238,12 @@ void launch_adj2(const DevCatalog& C, const PairParams& P, const double* cot2, c
   if (C.n <= 0) return;
   const size_t smem = sizeof(double) * 2 * (size_t)P.nbins * P.nmu;
   GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));
-  if (variant == kPairDense128 || variant == kPairDense256) {
+  // the forward sweep's choice of layout: block per cell for the dense
+  // variants (plain or queued), warp per cell otherwise
+  const bool dense = variant == kPairDense128 || variant == kPairDense256 ||
+                     variant == kPairDenseQ128 || variant == kPairDenseQ256;
+  const bool small = variant == kPairDense128 || variant == kPairDenseQ128;
+  if (dense) {
 #define GR_ADJ_DENSE(F, NT)                                                                    \
   do {                                                                                         \
     auto k = adj2_dense_kernel<F, NT>;                                                         \
@@ -250,9 +255,9 @@ void launch_adj2(const DevCatalog& C, const PairParams& P, const double* cot2, c
     k<<<(unsigned)blocks, NT, smem, s>>>(C, P, cot2, cot3, gscale, g_lo, g_hi, work);          \
   } while (0)
     if (P.f32) {
-      if (variant == kPairDense128) GR_ADJ_DENSE(true, 128); else GR_ADJ_DENSE(true, 256);
+      if (small) GR_ADJ_DENSE(true, 128); else GR_ADJ_DENSE(true, 256);
     } else {
-      if (variant == kPairDense128) GR_ADJ_DENSE(false, 128); else GR_ADJ_DENSE(false, 256);
+      if (small) GR_ADJ_DENSE(false, 128); else GR_ADJ_DENSE(false, 256);
     }
 #undef GR_ADJ_DENSE
     GR_CHECK_LAUNCH();

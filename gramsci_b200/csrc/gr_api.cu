@@ -589,7 +589,7 @@ static int pick_pair2_variant(gr_ctx* c, const DevCatalog& C, bool weighted, dou
   int hb = 0;
   while (hb < 20 && (2 << hb) <= c->nbins * c->nmu) ++hb;
   char key[128];
-  std::snprintf(key, sizeof(key), "pair2v4|%s|%s|dens%d|hist%d", c->P.f32 ? "f32" : "f64",
+  std::snprintf(key, sizeof(key), "pair2v6|%s|%s|dens%d|hist%d", c->P.f32 ? "f32" : "f64",
                 weighted ? "w" : "u", dens, hb);
   Tuner& T = tuner();
   {

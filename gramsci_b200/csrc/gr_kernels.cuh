@@ -18,9 +18,18 @@ constexpr size_t kMaxHistSmem = 120 * 1024;
 // variant: kPairWarpCell (warp per cell, lanes over candidates; sparse
 // cells) or kPairDense128/256 (block per cell, thread per root, broadcast
 // candidates; dense cells).  The autotuner picks one per workload class.
-// kPairWarpQueue: warp per cell with a membership-only test per candidate
-// and the binning of the edges queued and run with full warps.
-enum { kPairWarpCell = 0, kPairDense128 = 1, kPairDense256 = 2, kPairWarpQueue = 3, kPairVariants = 4 };
+// kPairWarpQueue / kPairDenseQ128/256: the same sweeps with a
+// membership-only test per candidate and the binning of the edges queued and
+// run with full warps.
+enum {
+  kPairWarpCell = 0,
+  kPairDense128 = 1,
+  kPairDense256 = 2,
+  kPairWarpQueue = 3,
+  kPairDenseQ128 = 4,
+  kPairDenseQ256 = 5,
+  kPairVariants = 6
+};
 size_t pair2_smem_bytes(const PairParams& P, bool weighted);
 void launch_pair2(const DevCatalog& C, const PairParams& P, bool weighted,
                   unsigned long long* g_cnt, unsigned long long* g_fix, double fscale,

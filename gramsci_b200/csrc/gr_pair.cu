@@ -457,6 +457,177 @@ __global__ void __launch_bounds__(NT) pair2_dense_kernel(DevCatalog C, PairParam
   }
 }
 
+// Dense-cell variant with queued binning: as pair2_dense_kernel, but the
+// lanes of a warp walk the staged candidates in step (lanes whose root has
+// not reached a candidate yet sit it out), test membership only, and queue
+// the edges per warp; bins, cosines and histogram updates run 32 edges at a
+// time with every lane busy.
+template <bool F32, bool WEIGHTED, bool SHIST, int NT>
+__global__ void __launch_bounds__(NT) pair2_dense_queue_kernel(
+    DevCatalog C, PairParams P, unsigned long long* __restrict__ g_cnt,
+    unsigned long long* __restrict__ g_fix, double fscale, unsigned long long* __restrict__ stats,
+    int* __restrict__ work) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  constexpr int TILE = 512;
+  constexpr int NW = NT / 32;
+  __shared__ float4 s_pos[TILE];
+  __shared__ int s_lab[TILE];
+  __shared__ uint8_t s_flag[TILE];
+  __shared__ double s_w[WEIGHTED ? TILE : 1];
+  __shared__ int s_qp[NW][kPairQueue];       // root label
+  __shared__ uint16_t s_qf[NW][kPairQueue];  // tile index of the neighbour
+  __shared__ int s_cell;
+  const int nbm = P.nbins * P.nmu;
+  const int nh = nbm * 4;
+  unsigned long long* s_cnt = SHIST ? reinterpret_cast<unsigned long long*>(smem) : g_cnt;
+  unsigned long long* s_lo = SHIST ? s_cnt + nh : g_fix;
+  unsigned long long* s_hi = s_lo + nh;
+  if (SHIST) {
+    for (int k = threadIdx.x; k < nh; k += NT) {
+      s_cnt[k] = 0ull;
+      if (WEIGHTED) {
+        s_lo[k] = 0ull;
+        s_hi[k] = 0ull;
+      }
+    }
+  }
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  const int ncell = (int)C.grid.ncell;
+  unsigned long long rechecks = 0, cands = 0, pairs = 0;
+  auto drain_one = [&](int e) {
+    const int p = s_qp[wib][e];
+    const int f = s_qf[wib][e];
+    const int q = s_lab[f];
+    int b = 1, mf = 1, mr = 1;
+    bool ok;
+    if (F32) {
+      const int r = classify_f32<true>(C.pos4[p], s_pos[f], P, b, mf, mr);
+      if (r == 2) {
+        rechecks++;
+        ok = edge_f64(C.posd[p], C.posd[q], P, b, mf, mr);
+      } else {
+        ok = r == 1;
+      }
+    } else {
+      ok = edge_f64(C.posd[p], C.posd[q], P, b, mf, mr);
+    }
+    if (!ok) return;  // cannot happen: the membership test decided the same pair
+    const uint8_t fp = C.flags[p], fq = s_flag[f];
+    const bool root_p = !(fp & FLAG_BUFFER), root_q = !(fq & FLAG_BUFFER);
+    const int rp = fp & FLAG_RANDOM, rq = fq & FLAG_RANDOM;
+    pairs += (root_p || root_q) ? 1 : 0;
+    const double prod = WEIGHTED ? C.w[p] * s_w[f] : 0.0;
+    if (root_p) {
+      const int k = (b - 1) + P.nbins * (mf - 1) + nbm * (2 * rp + rq);
+      atomicAdd(&s_cnt[k], 1ull);
+      if (WEIGHTED) fix_add(&s_lo[k], &s_hi[k], prod, fscale);
+    }
+    if (root_q) {
+      const int k = (b - 1) + P.nbins * (mr - 1) + nbm * (2 * rq + rp);
+      atomicAdd(&s_cnt[k], 1ull);
+      if (WEIGHTED) fix_add(&s_lo[k], &s_hi[k], prod, fscale);
+    }
+  };
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_cell = atomicAdd(work, 1);
+    __syncthreads();
+    const int cell = s_cell;
+    if (cell >= ncell) break;
+    const int cb = C.cell_start[cell], ce = C.cell_start[cell + 1];
+    if (cb == ce) continue;
+    Ranges R;
+    {
+      GridParams g;
+      const int* cs;
+      int lkey;
+      cell_grid(C, cell, g, cs, lkey);
+      forward_ranges(cb - 1, lkey, g, cs, R);
+    }
+    int pre[5], total = 0;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      pre[k] = total;
+      if (k < R.n) total += R.end[k] - R.beg[k];
+    }
+    for (int rb = cb; rb < ce; rb += NT) {
+      const int p = rb + threadIdx.x;
+      const bool act = p < ce;
+      const float4 pi = act ? C.pos4[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int t0 = 0; t0 < total; t0 += TILE) {
+        const int tn = min(TILE, total - t0);
+        __syncthreads();
+        for (int f = threadIdx.x; f < tn; f += NT) {
+          const int q = range_label(R, pre, t0 + f);
+          s_lab[f] = q;
+          s_pos[f] = C.pos4[q];
+          s_flag[f] = C.flags[q];
+          if (WEIGHTED) s_w[f] = C.w[q];
+        }
+        __syncthreads();
+        // candidates with label > p: own-cell candidates are the first
+        // (ce - cb) flattened entries, labels cb, cb+1, ...
+        const int fstart = act ? max(0, p - cb + 1 - t0) : tn;
+        if (fstart < tn) cands += (unsigned long long)(tn - fstart);
+        int f0 = fstart;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) f0 = min(f0, __shfl_xor_sync(0xffffffffu, f0, o));
+        int qn = 0;
+        for (int f = f0; f < tn; ++f) {  // warp-uniform walk over the candidates
+          bool e = false;
+          if (f >= fstart) {
+            int r = F32 ? member_f32(pi, s_pos[f], P) : 2;
+            if (r == 2) {
+              int b, mf, mr;
+              rechecks++;
+              r = edge_f64(C.posd[p], C.posd[s_lab[f]], P, b, mf, mr) ? 1 : 0;
+            }
+            e = r == 1;
+          }
+          const unsigned m = __ballot_sync(0xffffffffu, e);
+          if (e) {
+            s_qp[wib][qn + __popc(m & lt)] = p;
+            s_qf[wib][qn + __popc(m & lt)] = (uint16_t)f;
+          }
+          qn += __popc(m);
+          if (qn >= 32) {
+            __syncwarp();
+            drain_one(qn - 32 + lane);
+            qn -= 32;
+            __syncwarp();
+          }
+        }
+        // the staged tile is replaced after the next block barrier
+        __syncwarp();
+        if (lane < qn) drain_one(lane);
+        __syncwarp();
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    rechecks += __shfl_xor_sync(0xffffffffu, rechecks, o);
+    pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
+    cands += __shfl_xor_sync(0xffffffffu, cands, o);
+  }
+  if (lane == 0) {
+    if (rechecks) atomicAdd(&stats[0], rechecks);
+    if (cands) atomicAdd(&stats[1], cands);
+    if (pairs) atomicAdd(&stats[2], pairs);
+  }
+  if (SHIST) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < nh; k += NT) {
+      if (s_cnt[k]) {
+        atomicAdd(&g_cnt[k], s_cnt[k]);
+        if (WEIGHTED) fix_merge(&g_fix[k], &g_fix[nh + k], s_lo[k], s_hi[k]);
+      }
+    }
+  }
+}
+
 }  // namespace
 
 size_t pair2_smem_bytes(const PairParams& P, bool weighted) {
@@ -472,11 +643,14 @@ void launch_pair2(const DevCatalog& C, const PairParams& P, bool weighted,
   const bool shist = smem <= kMaxHistSmem;
   if (!shist) smem = 0;
   GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));
-  if (variant == kPairDense128 || variant == kPairDense256) {
+  if (variant == kPairDense128 || variant == kPairDense256 || variant == kPairDenseQ128 ||
+      variant == kPairDenseQ256) {
+    const bool q = variant == kPairDenseQ128 || variant == kPairDenseQ256;
+    const bool small = variant == kPairDense128 || variant == kPairDenseQ128;
     int per_sm = 1;
 #define GR_DENSE_LAUNCH(F, W, S, NT)                                                          \
   do {                                                                                        \
-    auto k = pair2_dense_kernel<F, W, S, NT>;                                                 \
+    auto k = q ? pair2_dense_queue_kernel<F, W, S, NT> : pair2_dense_kernel<F, W, S, NT>;      \
     GR_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
                                      (int)smem));                                             \
     GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, smem));         \
@@ -486,7 +660,7 @@ void launch_pair2(const DevCatalog& C, const PairParams& P, bool weighted,
   } while (0)
 #define GR_DENSE_NT(F, W, S)                                                                  \
   do {                                                                                        \
-    if (variant == kPairDense128) GR_DENSE_LAUNCH(F, W, S, 128); else GR_DENSE_LAUNCH(F, W, S, 256); \
+    if (small) GR_DENSE_LAUNCH(F, W, S, 128); else GR_DENSE_LAUNCH(F, W, S, 256);             \
   } while (0)
 #define GR_DENSE_W(F, S)                                                                      \
   do {                                                                                        \

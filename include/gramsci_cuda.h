@@ -48,7 +48,8 @@ typedef struct gr_ctx gr_ctx;
 #define GR_OPT_AUTOTUNE 3   /* 0: fixed kernels; 1: time the pair-sweep variants once per
                                workload class and cache the choice (default); 2+v: force
                                variant v (0 warp per cell, 1/2 block per cell of 128/256,
-                               3 warp per cell with queued binning) */
+                               3 warp per cell with queued binning, 4/5 block per cell of
+                               128/256 with queued binning) */
 #define GR_OPT_KEEP_GRAPH 4 /* 0 (default): every count call builds the index and graph;
                                1: keep the graph of the last call and reuse it until the
                                catalogue, the bins or the precision change */

@@ -151,7 +151,7 @@ def test_pair_sweep_variants_agree(gpu_ctx, oracle, name, scale, nmu, weighted):
     gpu_ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], nmu)
     ref = oracle.Graph(cat.xyz, sp["rmin"], sp["rmax"], sp["nbins"], nmu).pcf2(w, cat.n_data)
     try:
-        for v in range(4):
+        for v in range(6):
             gpu_ctx.set_autotune(v)
             _check_sums(gpu_ctx.count_2pcf(), ref)
     finally:
