@@ -845,22 +845,31 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   GR_CUDA_TRY(cudaEventCreate(&q0));
   GR_CUDA_TRY(cudaEventRecord(q0, s));
   c->work.reserve(4);
-  launch_quad4(c->index.view(), G, Q, weighted, c->hcnt.p, c->hfix.p, c->dcnt.p, c->dfix.p, nh, nd,
-               fscale, dscale, c->qpriv, c->stats.p, c->work.p, s);
-  GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
   std::vector<unsigned long long> hc(nh), dc(nd), hf, df;
   std::vector<double> hs(nh, 0.0), ds(nd, 0.0);
   unsigned long long st[8];
-  GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
-  GR_CUDA_TRY(cudaMemcpyAsync(dc.data(), c->dcnt.p, sizeof(unsigned long long) * nd, cudaMemcpyDeviceToHost, s));
-  if (weighted) {
-    hf.resize(2 * (size_t)nh);
-    df.resize(2 * (size_t)nd);
-    GR_CUDA_TRY(cudaMemcpyAsync(hf.data(), c->hfix.p, sizeof(unsigned long long) * 2 * nh, cudaMemcpyDeviceToHost, s));
-    GR_CUDA_TRY(cudaMemcpyAsync(df.data(), c->dfix.p, sizeof(unsigned long long) * 2 * nd, cudaMemcpyDeviceToHost, s));
+  // block-private 32-bit counters first; exact below 2^32 rooted cliques,
+  // else the launch is repeated with 64-bit global counters
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    if (attempt > 0) {
+      GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
+      GR_CUDA_TRY(cudaEventRecord(q0, s));
+    }
+    launch_quad4(c->index.view(), G, Q, weighted, c->hcnt.p, c->hfix.p, c->dcnt.p, c->dfix.p, nh,
+                 nd, fscale, dscale, c->qpriv, attempt == 0, c->stats.p, c->work.p, s);
+    GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
+    GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
+    GR_CUDA_TRY(cudaMemcpyAsync(dc.data(), c->dcnt.p, sizeof(unsigned long long) * nd, cudaMemcpyDeviceToHost, s));
+    if (weighted) {
+      hf.resize(2 * (size_t)nh);
+      df.resize(2 * (size_t)nd);
+      GR_CUDA_TRY(cudaMemcpyAsync(hf.data(), c->hfix.p, sizeof(unsigned long long) * 2 * nh, cudaMemcpyDeviceToHost, s));
+      GR_CUDA_TRY(cudaMemcpyAsync(df.data(), c->dfix.p, sizeof(unsigned long long) * 2 * nd, cudaMemcpyDeviceToHost, s));
+    }
+    GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
+    GR_CUDA_TRY(cudaStreamSynchronize(s));
+    if (st[1] < (1ull << 32)) break;
   }
-  GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
-  GR_CUDA_TRY(cudaStreamSynchronize(s));
   if (st[3] != 0)
     return set_err(c, GR_E_CAPACITY, "4PCF: label offsets within a row exceed the hash key range");
   if (weighted) {

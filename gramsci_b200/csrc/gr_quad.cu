@@ -39,16 +39,19 @@ __host__ __device__ inline int qhash_lg_max(int cap) {
 }
 
 struct QuadLayout {
-  size_t off_rank, off_warp, warp_bytes, total;
+  size_t off_rank, off_cnt, off_warp, warp_bytes, total;
   // per-warp sub-offsets
   size_t o_rs, o_w, o_mo, o_col, o_len, o_xm, o_hkey, o_q, o_xy, o_xz, o_bits;
 };
 
-__host__ __device__ inline QuadLayout quad_layout(int nbins, int cap, int nwarps) {
+// ncounts: block-private 32-bit counters in shared memory (0: none)
+__host__ __device__ inline QuadLayout quad_layout(int nbins, int cap, int nwarps, int ncounts) {
   QuadLayout L;
   size_t o = 0;
   L.off_rank = o;
   o = qalign8(o + sizeof(int) * 4 * (size_t)(nbins + 2));
+  L.off_cnt = o;
+  o = qalign8(o + sizeof(unsigned int) * (size_t)ncounts);
   L.off_warp = o;
   size_t w = 0;
   L.o_rs = w;   w += (size_t)cap * 8;   // row start of each neighbour
@@ -71,10 +74,22 @@ struct QuadCtx {
   const int* F;  // 4 x (nbins+2)
   int nbins, ncfg, nbin, tetra;
   unsigned long long *cnt, *dcnt;
+  unsigned int *scnt, *sdcnt;  // block-private 32-bit counts in shared memory, or null
   unsigned long long *fix, *dfix;  // fixed-point (lo, hi) sums, hi at +5*nbin / +24*nbin
   double fscale;  // scale of the 4-point products
   double dscale;  // scale of the pair products of the disconnected terms
 };
+
+template <bool SHC>
+__device__ __forceinline__ void qcount(const QuadCtx& X, int k) {
+  if (SHC) atomicAdd(&X.scnt[k], 1u);
+  else atomicAdd(&X.cnt[k], 1ull);
+}
+template <bool SHC>
+__device__ __forceinline__ void qdcount(const QuadCtx& X, int k) {
+  if (SHC) atomicAdd(&X.sdcnt[k], 1u);
+  else atomicAdd(&X.dcnt[k], 1ull);
+}
 
 // The four vertices of a clique: flags (with kFlagDeg4), catalogue ids and
 // weights.
@@ -125,7 +140,7 @@ __device__ __forceinline__ void others_by_id(const QVerts& V, int& u0, int& u1, 
 
 // query_graph_tetrahedron: a 4-clique with all six edges in bin b counts from
 // each non-buffer vertex (no row-length condition).
-template <bool WEIGHTED, int R>
+template <bool WEIGHTED, bool SHC, int R>
 __device__ __forceinline__ int tetra_root(const QuadCtx& X, const QVerts& V, int b, unsigned rndm,
                                           int nr) {
   if (V.fl[R] & FLAG_BUFFER) return 0;
@@ -133,7 +148,7 @@ __device__ __forceinline__ int tetra_root(const QuadCtx& X, const QVerts& V, int
   others_by_id<R>(V, u0, u1, u2);
   const int role[4] = {R, u0, u1, u2};
   const int nb = X.nbins;
-  atomicAdd(&X.cnt[(b - 1) + nb * nr], 1ull);
+  qcount<SHC>(X, (b - 1) + nb * nr);
   if (WEIGHTED)
     fix_add(&X.fix[(b - 1) + nb * nr], &X.fix[(b - 1) + nb * (nr + 5)],
             ((V.w[R] * qsel(u0, V)) * qsel(u1, V)) * qsel(u2, V), X.fscale);
@@ -144,17 +159,17 @@ __device__ __forceinline__ int tetra_root(const QuadCtx& X, const QVerts& V, int
     const int nr3 = (int)((rndm >> ua) & 1u) + (int)((rndm >> ub) & 1u) + (int)((rndm >> uc) & 1u);
     const int kt = (b - 1) + nb * tt;
     const double qv = WEIGHTED ? (qsel(ua, V) * qsel(ub, V)) * qsel(uc, V) : 0.0;
-    atomicAdd(&X.dcnt[kt + nb * 6 * nr3], 1ull);
+    qdcount<SHC>(X, kt + nb * 6 * nr3);
     if (WEIGHTED) fix_add(&X.dfix[kt + nb * 6 * nr3], &X.dfix[kt + nb * 6 * (nr3 + 5)], qv, X.dscale);
     if (((rndm >> ub) & 1u) && ((rndm >> uc) & 1u)) {
-      atomicAdd(&X.dcnt[kt + nb * 24], 1ull);
+      qdcount<SHC>(X, kt + nb * 24);
       if (WEIGHTED) fix_add(&X.dfix[kt + nb * 24], &X.dfix[kt + nb * 54], qv, X.dscale);
     }
   }
   return 1;
 }
 
-template <bool WEIGHTED>
+template <bool WEIGHTED, bool SHC>
 __device__ __forceinline__ int tetra_contrib(const QuadCtx& X, const QVerts& V, const uint32_t m[6]) {
   const int b = meta_bin(m[0]);
 #pragma unroll
@@ -164,13 +179,13 @@ __device__ __forceinline__ int tetra_contrib(const QuadCtx& X, const QVerts& V, 
 #pragma unroll
   for (int k = 0; k < 4; ++k) rndm |= (unsigned)(V.fl[k] & FLAG_RANDOM) << k;
   const int nr = __popc(rndm);
-  return tetra_root<WEIGHTED, 0>(X, V, b, rndm, nr) + tetra_root<WEIGHTED, 1>(X, V, b, rndm, nr) +
-         tetra_root<WEIGHTED, 2>(X, V, b, rndm, nr) + tetra_root<WEIGHTED, 3>(X, V, b, rndm, nr);
+  return tetra_root<WEIGHTED, SHC, 0>(X, V, b, rndm, nr) + tetra_root<WEIGHTED, SHC, 1>(X, V, b, rndm, nr) +
+         tetra_root<WEIGHTED, SHC, 2>(X, V, b, rndm, nr) + tetra_root<WEIGHTED, SHC, 3>(X, V, b, rndm, nr);
 }
 
 // One root R of a 4-clique for query_4pcf_all2: canonical perimeter check,
 // N2 / N3 at (cfg, bin(r,k2), bin(k1,k3)) and the six disconnected terms.
-template <bool WEIGHTED, int R>
+template <bool WEIGHTED, bool SHC, int R>
 __device__ __forceinline__ int quad_root(const QuadCtx& X, const QVerts& V, unsigned long long packed,
                                          unsigned rndm, int nr) {
   if (V.fl[R] & FLAG_BUFFER) return 0;
@@ -185,7 +200,7 @@ __device__ __forceinline__ int quad_root(const QuadCtx& X, const QVerts& V, unsi
                   (X.F[2 * nb2 + b3] - X.F[2 * nb2 + b2]) + (X.F[3 * nb2 + b4] - X.F[3 * nb2 + b3]);
   const int d1 = qbin(packed, R, u1), d2 = qbin(packed, u0, u2);
   const int kk = (cfg - 1) + X.ncfg * ((d1 - 1) + X.nbins * (d2 - 1));
-  atomicAdd(&X.cnt[kk + X.nbin * nr], 1ull);
+  qcount<SHC>(X, kk + X.nbin * nr);
   if (WEIGHTED)
     fix_add(&X.fix[kk + X.nbin * nr], &X.fix[kk + X.nbin * (nr + 5)],
             ((V.w[R] * qsel(u0, V)) * qsel(u1, V)) * qsel(u2, V), X.fscale);
@@ -197,11 +212,11 @@ __device__ __forceinline__ int quad_root(const QuadCtx& X, const QVerts& V, unsi
     const int npr = (int)((rndm >> u) & 1u) + (int)((rndm >> vv) & 1u);
     const int kt = kk + X.nbin * tt;
     const double q = WEIGHTED ? qsel(u, V) * qsel(vv, V) : 0.0;
-    atomicAdd(&X.dcnt[kt + X.nbin * 6 * npr], 1ull);
+    qdcount<SHC>(X, kt + X.nbin * 6 * npr);
     if (WEIGHTED)
       fix_add(&X.dfix[kt + X.nbin * 6 * npr], &X.dfix[kt + X.nbin * (6 * npr + 24)], q, X.dscale);
     if (npr == 2) {
-      atomicAdd(&X.dcnt[kt + X.nbin * 18], 1ull);
+      qdcount<SHC>(X, kt + X.nbin * 18);
       if (WEIGHTED) fix_add(&X.dfix[kt + X.nbin * 18], &X.dfix[kt + X.nbin * 42], q, X.dscale);
     }
   }
@@ -210,7 +225,7 @@ __device__ __forceinline__ int quad_root(const QuadCtx& X, const QVerts& V, unsi
 
 // m: bins of (0,1) (0,2) (0,3) (1,2) (1,3) (2,3) for vertices 0 = p, 1 = a,
 // 2 = b, 3 = d.
-template <bool WEIGHTED>
+template <bool WEIGHTED, bool SHC>
 __device__ __forceinline__ int quad_contrib(const QuadCtx& X, const QVerts& V, const uint32_t m[6]) {
   unsigned long long packed = 0;
 #pragma unroll
@@ -219,8 +234,8 @@ __device__ __forceinline__ int quad_contrib(const QuadCtx& X, const QVerts& V, c
 #pragma unroll
   for (int k = 0; k < 4; ++k) rndm |= (unsigned)(V.fl[k] & FLAG_RANDOM) << k;
   const int nr = __popc(rndm);
-  return quad_root<WEIGHTED, 0>(X, V, packed, rndm, nr) + quad_root<WEIGHTED, 1>(X, V, packed, rndm, nr) +
-         quad_root<WEIGHTED, 2>(X, V, packed, rndm, nr) + quad_root<WEIGHTED, 3>(X, V, packed, rndm, nr);
+  return quad_root<WEIGHTED, SHC, 0>(X, V, packed, rndm, nr) + quad_root<WEIGHTED, SHC, 1>(X, V, packed, rndm, nr) +
+         quad_root<WEIGHTED, SHC, 2>(X, V, packed, rndm, nr) + quad_root<WEIGHTED, SHC, 3>(X, V, packed, rndm, nr);
 }
 
 __device__ __forceinline__ uint32_t qfib_slot(uint32_t off, int lg) {
@@ -231,13 +246,13 @@ __device__ __forceinline__ uint32_t qfib_slot(uint32_t off, int lg) {
 // [cnt nh][dcnt nd][fix 2 nh][dfix 2 nd] (fix arrays when weighted), so
 // that blocks do not contend for the same global addresses; quad_merge_kernel
 // sums the copies.
-template <bool WEIGHTED>
+template <bool WEIGHTED, bool SHC>
 __global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
     DevCatalog C, CSRView G, QuadParams Q, unsigned long long* __restrict__ priv, int ncopy,
-    int nh, int nd, double fscale, double dscale, unsigned long long* __restrict__ stats,
-    int* __restrict__ work) {
+    int nh, int nd, double fscale, double dscale,
+    unsigned long long* __restrict__ stats, int* __restrict__ work) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const QuadLayout L = quad_layout(Q.nbins, Q.cap, blockDim.x >> 5);
+  const QuadLayout L = quad_layout(Q.nbins, Q.cap, blockDim.x >> 5, SHC ? nh + nd : 0);
   int* s_F = reinterpret_cast<int*>(smem + L.off_rank);
   const int nb2 = Q.nbins + 2;
   for (int k = threadIdx.x; k < 4 * nb2; k += blockDim.x) s_F[k] = Q.rank.F[k / nb2][k % nb2];
@@ -255,6 +270,15 @@ __global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
     X.dcnt = base + nh;
     X.fix = WEIGHTED ? base + nh + nd : nullptr;
     X.dfix = WEIGHTED ? base + nh + nd + 2 * (size_t)nh : nullptr;
+  }
+  X.scnt = nullptr;
+  X.sdcnt = nullptr;
+  if (SHC) {
+    unsigned int* sc = reinterpret_cast<unsigned int*>(smem + L.off_cnt);
+    for (int k = threadIdx.x; k < nh + nd; k += blockDim.x) sc[k] = 0u;
+    __syncthreads();
+    X.scnt = sc;
+    X.sdcnt = sc + nh;
   }
   X.fscale = fscale;
   X.dscale = dscale;
@@ -393,7 +417,7 @@ __global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
         // m: (p,a) (p,b) (p,d) (a,b) (a,d) (b,d)
         const uint32_t m[6] = {(uint32_t)mpa_w & 0xffffffu, (uint32_t)mpb_w & 0xffffffu,
                                (uint32_t)mpd_w & 0xffffffu, s_xm[z], s_xm[s_xz[yd]], mbd};
-        const int nroot = X.tetra ? tetra_contrib<WEIGHTED>(X, V, m) : quad_contrib<WEIGHTED>(X, V, m);
+        const int nroot = X.tetra ? tetra_contrib<WEIGHTED, SHC>(X, V, m) : quad_contrib<WEIGHTED, SHC>(X, V, m);
         quads += nroot > 0;
         rooted += nroot;
       };
@@ -470,6 +494,13 @@ __global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
     if (rooted) atomicAdd(&stats[1], rooted);
     if (probes) atomicAdd(&stats[2], probes);
   }
+  if (SHC) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < nh + nd; k += blockDim.x) {
+      const unsigned int v = X.scnt[k];
+      if (v) atomicAdd(k < nh ? &X.cnt[k] : &X.dcnt[k - nh], (unsigned long long)v);
+    }
+  }
 }
 
 // Sum of the histogram copies into the outputs (counts as integers, fixed
@@ -514,9 +545,9 @@ __global__ void quad_merge_kernel(const unsigned long long* __restrict__ priv, i
 }
 
 // Warps per block: as many as fit in shared memory (at most 32).
-int quad4_warps(int nbins, int cap) {
+int quad4_warps(int nbins, int cap, int ncounts) {
   int nw = kQuadMaxWarps;
-  while (nw > 1 && quad_layout(nbins, cap, nw).total > kQuadSmemLimit) nw -= 1;
+  while (nw > 1 && quad_layout(nbins, cap, nw, ncounts).total > kQuadSmemLimit) nw -= 1;
   return nw;
 }
 
@@ -525,13 +556,18 @@ int quad4_warps(int nbins, int cap) {
 void launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bool weighted,
                   unsigned long long* g_cnt, unsigned long long* g_fix, unsigned long long* d_cnt,
                   unsigned long long* d_fix, int nh, int nd, double fscale, double dscale,
-                  DevBuf<unsigned long long>& priv, unsigned long long* stats, int* work,
-                  cudaStream_t s) {
-  const int nw = quad4_warps(Q.nbins, Q.cap);
-  const size_t smem = quad_layout(Q.nbins, Q.cap, nw).total;
+                  DevBuf<unsigned long long>& priv, bool shared_counts,
+                  unsigned long long* stats, int* work, cudaStream_t s) {
+  // block-private counters for unweighted catalogues when they leave room
+  // for at least 8 warps
+  const int ncnt = nh + nd;
+  if (weighted || quad4_warps(Q.nbins, Q.cap, ncnt) < 8) shared_counts = false;
+  const int nw = quad4_warps(Q.nbins, Q.cap, shared_counts ? ncnt : 0);
+  const size_t smem = quad_layout(Q.nbins, Q.cap, nw, shared_counts ? ncnt : 0).total;
   if (smem > kQuadSmemLimit) throw Error{-2, "4PCF: per-warp shared memory exceeds the SM limit"};
   const size_t per = (size_t)(nh + nd) * (weighted ? 3 : 1);
-  auto kfn = weighted ? quad4_kernel<true> : quad4_kernel<false>;
+  auto kfn = weighted ? quad4_kernel<true, false>
+                      : (shared_counts ? quad4_kernel<false, true> : quad4_kernel<false, false>);
   GR_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nw * 32, smem));
@@ -558,7 +594,7 @@ void launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bo
 }
 
 size_t quad4_smem_bytes(int nbins, int cap) {
-  return quad_layout(nbins, cap, quad4_warps(nbins, cap)).total;
+  return quad_layout(nbins, cap, quad4_warps(nbins, cap, 0), 0).total;
 }
 
 }  // namespace gr
