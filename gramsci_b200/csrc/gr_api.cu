@@ -50,7 +50,6 @@ struct gr_ctx {
   PairParams P{};
   DevBuf<uint8_t> normal_dev;
   DevBuf<unsigned long long> hcnt, dcnt, stats;
-  DevBuf<unsigned long long> qpriv;       // 4PCF per-block histogram copies
   DevBuf<unsigned long long> hfix, dfix;  // fixed-point sums (lo words, then hi words)
   double wmax = 0.0;                      // max |w| over the catalogue
   double wgmax = 0.0, wrmax = 0.0;        // max |w| over galaxies / randoms
@@ -852,11 +851,14 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   // else the launch is repeated with 64-bit global counters
   for (int attempt = 0; attempt < 2; ++attempt) {
     if (attempt > 0) {
+      GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nh, s));
+      GR_CUDA_TRY(cudaMemsetAsync(c->dcnt.p, 0, sizeof(unsigned long long) * nd, s));
       GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
       GR_CUDA_TRY(cudaEventRecord(q0, s));
     }
-    launch_quad4(c->index.view(), G, Q, weighted, c->hcnt.p, c->hfix.p, c->dcnt.p, c->dfix.p, nh,
-                 nd, fscale, dscale, c->qpriv, attempt == 0, c->stats.p, c->work.p, s);
+    const bool shared = launch_quad4(c->index.view(), G, Q, weighted, c->hcnt.p, c->hfix.p,
+                                     c->dcnt.p, c->dfix.p, nh, nd, fscale, dscale, attempt == 0,
+                                     c->stats.p, c->work.p, s);
     GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
     GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
     GR_CUDA_TRY(cudaMemcpyAsync(dc.data(), c->dcnt.p, sizeof(unsigned long long) * nd, cudaMemcpyDeviceToHost, s));
@@ -868,7 +870,7 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
     }
     GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
     GR_CUDA_TRY(cudaStreamSynchronize(s));
-    if (st[1] < (1ull << 32)) break;
+    if (!shared || st[1] < (1ull << 32)) break;
   }
   if (st[3] != 0)
     return set_err(c, GR_E_CAPACITY, "4PCF: label offsets within a row exceed the hash key range");

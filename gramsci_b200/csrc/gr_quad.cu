@@ -242,14 +242,13 @@ __device__ __forceinline__ uint32_t qfib_slot(uint32_t off, int lg) {
   return (off * 2654435769u) >> (32 - lg);
 }
 
-// Histogram copies: block b accumulates into copy b % ncopy of the layout
-// [cnt nh][dcnt nd][fix 2 nh][dfix 2 nd] (fix arrays when weighted), so
-// that blocks do not contend for the same global addresses; quad_merge_kernel
-// sums the copies.
+// SHC: unweighted counts in block-private 32-bit shared-memory counters,
+// added to the global histograms at the end of the block.
 template <bool WEIGHTED, bool SHC>
 __global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
-    DevCatalog C, CSRView G, QuadParams Q, unsigned long long* __restrict__ priv, int ncopy,
-    int nh, int nd, double fscale, double dscale,
+    DevCatalog C, CSRView G, QuadParams Q, unsigned long long* __restrict__ g_cnt,
+    unsigned long long* __restrict__ g_fix, unsigned long long* __restrict__ d_cnt,
+    unsigned long long* __restrict__ d_fix, int nh, int nd, double fscale, double dscale,
     unsigned long long* __restrict__ stats, int* __restrict__ work) {
   extern __shared__ __align__(16) unsigned char smem[];
   const QuadLayout L = quad_layout(Q.nbins, Q.cap, blockDim.x >> 5, SHC ? nh + nd : 0);
@@ -263,14 +262,10 @@ __global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
   X.ncfg = Q.ncfg;
   X.nbin = Q.tetra ? Q.nbins : Q.ncfg * Q.nbins * Q.nbins;
   X.tetra = Q.tetra;
-  {
-    const size_t per = (size_t)(nh + nd) * (WEIGHTED ? 3 : 1);
-    unsigned long long* base = priv + per * (size_t)(blockIdx.x % ncopy);
-    X.cnt = base;
-    X.dcnt = base + nh;
-    X.fix = WEIGHTED ? base + nh + nd : nullptr;
-    X.dfix = WEIGHTED ? base + nh + nd + 2 * (size_t)nh : nullptr;
-  }
+  X.cnt = g_cnt;
+  X.dcnt = d_cnt;
+  X.fix = g_fix;
+  X.dfix = d_fix;
   X.scnt = nullptr;
   X.sdcnt = nullptr;
   if (SHC) {
@@ -503,47 +498,6 @@ __global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
   }
 }
 
-// Sum of the histogram copies into the outputs (counts as integers, fixed
-// point as 128-bit pairs): deterministic, every output entry written.
-__global__ void quad_merge_kernel(const unsigned long long* __restrict__ priv, int ncopy, int nh,
-                                  int nd, bool weighted, unsigned long long* __restrict__ g_cnt,
-                                  unsigned long long* __restrict__ g_fix,
-                                  unsigned long long* __restrict__ d_cnt,
-                                  unsigned long long* __restrict__ d_fix) {
-  const size_t per = (size_t)(nh + nd) * (weighted ? 3 : 1);
-  const int total = nh + nd;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
-    const bool dterm = k >= nh;
-    const int kk = dterm ? k - nh : k;
-    const int nn = dterm ? nd : nh;
-    unsigned long long cnt = 0, lo = 0, hi = 0;
-    for (int c = 0; c < ncopy; ++c) {
-      const unsigned long long* b = priv + per * (size_t)c;
-      cnt += b[k];
-      if (weighted) {
-        const unsigned long long* f = b + nh + nd + (dterm ? 2 * (size_t)nh : 0);
-        const unsigned long long l2 = f[kk], h2 = f[nn + kk];
-        const unsigned long long s = lo + l2;
-        hi += h2 + (s < lo ? 1ull : 0ull);
-        lo = s;
-      }
-    }
-    if (dterm) {
-      d_cnt[kk] = cnt;
-      if (weighted) {
-        d_fix[kk] = lo;
-        d_fix[nn + kk] = hi;
-      }
-    } else {
-      g_cnt[kk] = cnt;
-      if (weighted) {
-        g_fix[kk] = lo;
-        g_fix[nn + kk] = hi;
-      }
-    }
-  }
-}
-
 // Warps per block: as many as fit in shared memory (at most 32).
 int quad4_warps(int nbins, int cap, int ncounts) {
   int nw = kQuadMaxWarps;
@@ -553,11 +507,11 @@ int quad4_warps(int nbins, int cap, int ncounts) {
 
 }  // namespace
 
-void launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bool weighted,
+bool launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bool weighted,
                   unsigned long long* g_cnt, unsigned long long* g_fix, unsigned long long* d_cnt,
                   unsigned long long* d_fix, int nh, int nd, double fscale, double dscale,
-                  DevBuf<unsigned long long>& priv, bool shared_counts,
-                  unsigned long long* stats, int* work, cudaStream_t s) {
+                  bool shared_counts, unsigned long long* stats, int* work, cudaStream_t s) {
+  if (C.n <= 0) return false;
   // block-private counters for unweighted catalogues when they leave room
   // for at least 8 warps
   const int ncnt = nh + nd;
@@ -565,7 +519,6 @@ void launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bo
   const int nw = quad4_warps(Q.nbins, Q.cap, shared_counts ? ncnt : 0);
   const size_t smem = quad_layout(Q.nbins, Q.cap, nw, shared_counts ? ncnt : 0).total;
   if (smem > kQuadSmemLimit) throw Error{-2, "4PCF: per-warp shared memory exceeds the SM limit"};
-  const size_t per = (size_t)(nh + nd) * (weighted ? 3 : 1);
   auto kfn = weighted ? quad4_kernel<true, false>
                       : (shared_counts ? quad4_kernel<false, true> : quad4_kernel<false, false>);
   GR_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -576,21 +529,11 @@ void launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bo
   const int64_t need = ((int64_t)C.n + nw - 1) / nw;
   if (blocks > need) blocks = need;
   if (blocks < 1) blocks = 1;
-  // one copy of the histograms: per-block copies measured no faster (L2
-  // atomics on distinct blocks' copies cost the same on this workload)
-  const int64_t ncopy = 1;
-  priv.reserve((size_t)ncopy * per);
-  GR_CUDA_TRY(cudaMemsetAsync(priv.p, 0, sizeof(unsigned long long) * (size_t)ncopy * per, s));
-  if (C.n > 0) {
-    GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));
-    kfn<<<(unsigned)blocks, nw * 32, smem, s>>>(C, G, Q, priv.p, (int)ncopy, nh, nd, fscale, dscale,
-                                                stats, work);
-    GR_CHECK_LAUNCH();
-  }
-  const int mb = (int)std::min<int64_t>((nh + nd + 255) / 256, 148 * 8);
-  quad_merge_kernel<<<mb, 256, 0, s>>>(priv.p, (int)ncopy, nh, nd, weighted, g_cnt, g_fix, d_cnt,
-                                       d_fix);
+  GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));
+  kfn<<<(unsigned)blocks, nw * 32, smem, s>>>(C, G, Q, g_cnt, g_fix, d_cnt, d_fix, nh, nd, fscale,
+                                              dscale, stats, work);
   GR_CHECK_LAUNCH();
+  return shared_counts;
 }
 
 size_t quad4_smem_bytes(int nbins, int cap) {
