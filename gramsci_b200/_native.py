@@ -83,6 +83,7 @@ SIGNATURES = {
     "gr_regions_info": (ctypes.c_int, [_ctx, _vp, _vp]),
     "gr_regions_export": (ctypes.c_int, [_ctx, _vp, _vp, _vp]),
     "gr_adjoint_3pcf": (ctypes.c_int, [_ctx, _vp, _vp, _vp]),
+    "gr_adjoint_4pcf": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp, _vp]),
     "gr_count_2pcf_noalloc": (ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.c_int64,
                                              ctypes.c_double, ctypes.c_double, ctypes.c_int32,
                                              ctypes.c_int32, _vp, _vp, _vp, _vp, _vp]),

@@ -227,6 +227,25 @@ class Context:
         the weights (catalogue order)."""
         return self._adjoint(self._lib.gr_adjoint_3pcf, cot2, cot3, (ncfg3(self.nbins), self.nmu))
 
+    def adjoint_4pcf(self, cot2, cot3=None, cotN=None, cotR=None):
+        """Gradient of sum(cot2*N2) + sum(cot3*N3) + sum(cotN*discN) +
+        sum(cotR*discR) of the 4PCF with respect to the weights (catalogue
+        order); cotangents in the shapes count_4pcf returns."""
+        nb = self.nbins
+        nc = ncfg4(nb)
+
+        def f(a, *shape):
+            if a is None:
+                return None
+            return np.ascontiguousarray(np.asarray(a, np.float64).reshape(shape).T.ravel())
+
+        c2, c3 = f(cot2, nc, nb, nb), f(cot3, nc, nb, nb)
+        cN, cR = f(cotN, nc, nb, nb, 6), f(cotR, nc, nb, nb, 6)
+        g = np.zeros(self.n)
+        self._check(self._lib.gr_adjoint_4pcf(self._h, _ptr(c2), _ptr(c3), _ptr(cN), _ptr(cR),
+                                              _ptr(g)))
+        return g
+
     def set_keep_graph(self, on):
         """Reuse the last call's graph until the catalogue, bins or precision change."""
         self._check(self._lib.gr_set_option(self._h, 4, int(bool(on))))

@@ -1,10 +1,11 @@
-"""Differentiable weighted 2PCF / 3PCF counts (torch.autograd.Function).
+"""Differentiable weighted 2PCF / 3PCF / 4PCF counts (torch.autograd.Function).
 
 The forward pass runs the counting kernels; the backward pass runs the
-hand-written adjoint kernels (gr_adjoint_2pcf / gr_adjoint_3pcf): for
-L = sum(gN2 * N2) + sum(gN3 * N3), dL/dw_k is the sum over the rooted pairs
-or triangles containing k of the cotangent of their bin times the product of
-the other weights.  Positions and bin membership are exact and not
+hand-written adjoint kernels (gr_adjoint_2pcf / _3pcf / _4pcf): for
+L = sum(gN2 * N2) + sum(gN3 * N3) (+ sum(gdN * discN) + sum(gdR * discR)
+for the 4PCF), dL/dw_k is the sum over the rooted pairs, triangles or
+4-cliques containing k of the cotangent of their bin times the product of
+the other weights (the partner's weight for the 4PCF pair terms).  Positions and bin membership are exact and not
 differentiated.  The weights here are the signed normalised weights the
 reference forms after reading (src/gramsci.F90:1390-1391); normalise raw
 weights with `normalise` to differentiate through that step too.
@@ -38,24 +39,26 @@ class _PCF(torch.autograd.Function):
         c = _context(w.device)
         c.set_catalog(xyz.detach().cpu().numpy(), w.detach().cpu().numpy(), n_data)
         c.set_bins(*bins)
-        out = c.count_2pcf() if order == 2 else c.count_3pcf()
+        count = {2: c.count_2pcf, 3: c.count_3pcf, 4: c.count_4pcf}[order]
+        out = count()
         ctx.save_for_backward(w, xyz)
         ctx.n_data, ctx.bins, ctx.order = n_data, bins, order
         to = dict(dtype=torch.float64, device=w.device)
-        return torch.as_tensor(out["N2"], **to), torch.as_tensor(out["N3"], **to)
+        names = ("N2", "N3", "discN", "discR") if order == 4 else ("N2", "N3")
+        ctx.shapes = [out[k].shape for k in names]
+        return tuple(torch.as_tensor(out[k], **to) for k in names)
 
     @staticmethod
-    def backward(ctx, gN2, gN3):
+    def backward(ctx, *grads):
         w, xyz = ctx.saved_tensors
         c = _context(w.device)
         c.set_catalog(xyz.detach().cpu().numpy(), w.detach().cpu().numpy(), ctx.n_data)
         c.set_bins(*ctx.bins)
-        g2 = np.zeros(1) if gN2 is None else gN2.detach().cpu().numpy()
-        g3 = None if gN3 is None else gN3.detach().cpu().numpy()
-        if gN2 is None:
-            g2 = np.zeros_like(g3)
-        fn = c.adjoint_2pcf if ctx.order == 2 else c.adjoint_3pcf
-        g = fn(g2, g3)
+        cots = [None if g is None else g.detach().cpu().numpy() for g in grads]
+        if cots[0] is None:
+            cots[0] = np.zeros(ctx.shapes[0])
+        fn = {2: c.adjoint_2pcf, 3: c.adjoint_3pcf, 4: c.adjoint_4pcf}[ctx.order]
+        g = fn(*cots)
         return torch.as_tensor(g, dtype=w.dtype, device=w.device), None, None, None, None
 
 
@@ -67,3 +70,9 @@ def pcf2(w, xyz, n_data, rmin, rmax, nbins, nmu=1):
 def pcf3(w, xyz, n_data, rmin, rmax, nbins, nmu=1):
     """Weighted 3PCF sums (N2, N3), each (ncfg, nmu), differentiable in w."""
     return _PCF.apply(w, xyz, int(n_data), (float(rmin), float(rmax), int(nbins), int(nmu)), 3)
+
+
+def pcf4(w, xyz, n_data, rmin, rmax, nbins):
+    """Weighted 4PCF sums (N2, N3, discN, discR): N2 and N3 (ncfg, nbins,
+    nbins), discN and discR (ncfg, nbins, nbins, 6), differentiable in w."""
+    return _PCF.apply(w, xyz, int(n_data), (float(rmin), float(rmax), int(nbins), 1), 4)

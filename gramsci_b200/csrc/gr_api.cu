@@ -1314,6 +1314,73 @@ int gr_adjoint_3pcf(gr_ctx* c, const double* cot2, const double* cot3, double* g
   GR_API_END(c)
 }
 
+int gr_adjoint_4pcf(gr_ctx* c, const double* cot2, const double* cot3, const double* cotN,
+                    const double* cotR, double* grad_w) {
+  GR_API_BEGIN(c)
+  require_ready(c);
+  if (!cot2 || !grad_w) return set_err(c, GR_E_ARG, "null cot2 or grad_w");
+  ensure_events(c);
+  cudaStream_t s = c->stream();
+  const int nb = c->nbins;
+  const int64_t ncfg64 = ((int64_t)nb * (nb + 1) * (nb + 2) * (nb + 3)) / 24;
+  const int64_t nbin64 = ncfg64 * nb * nb;
+  if (nbin64 * 29 > ((int64_t)1 << 31)) return set_err(c, GR_E_CAPACITY, "4PCF histogram too large");
+  const int nbin = (int)nbin64;
+  const int64_t n = c->n;
+  // largest |gradient| one clique adds to one vertex: four roots, each with
+  // a 4-product cotangent times three weights and three pair terms times one
+  const double w = c->wmax;
+  const double c4 = max_abs(cot2, nbin) + max_abs(cot3, nbin);
+  const double cd = max_abs(cotN, 6 * (int64_t)nbin) + max_abs(cotR, 6 * (int64_t)nbin);
+  const double gscale = fix_scale(4.0 * (c4 * w * w * w + 3.0 * cd * w));
+  std::vector<double> cot((size_t)14 * nbin, 0.0);
+  std::memcpy(cot.data(), cot2, sizeof(double) * nbin);
+  if (cot3) std::memcpy(cot.data() + nbin, cot3, sizeof(double) * nbin);
+  if (cotN) std::memcpy(cot.data() + 2 * (size_t)nbin, cotN, sizeof(double) * 6 * nbin);
+  if (cotR) std::memcpy(cot.data() + 8 * (size_t)nbin, cotR, sizeof(double) * 6 * nbin);
+  c->cot.reserve(14 * (int64_t)nbin);
+  c->gfix.reserve(2 * n + 2);
+  c->work.reserve(4);
+  c->stats.reserve(8);
+  GR_CUDA_TRY(cudaMemcpyAsync(c->cot.p, cot.data(), sizeof(double) * cot.size(),
+                              cudaMemcpyHostToDevice, s));
+  GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
+  const bool reuse = c->csr_valid;
+  if (!reuse) {
+    build_index(c);
+    build_csr(c);
+  }
+  GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+  if (c->csr.max_deg > 1024)
+    return set_err(c, GR_E_CAPACITY, "4PCF: a point has more than 1024 larger-label neighbours");
+  GR_CUDA_TRY(cudaMemsetAsync(c->gfix.p, 0, sizeof(unsigned long long) * (2 * n + 2), s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
+  QuadParams Q{};
+  Q.nbins = nb;
+  Q.ncfg = (int)ncfg64;
+  Q.tetra = 0;
+  Q.cap = round_cap(c->csr.max_deg, 32, 1024);
+  make_rank_tables(Q.rank, nb, 4);
+  std::memset(&c->st, 0, sizeof(c->st));
+  launch_adj4(c->index.view(), c->csr.view(), Q, c->cot.p, gscale, c->gfix.p, c->gfix.p + n,
+              c->stats.p, c->work.p, s);
+  unsigned long long st[8];
+  GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
+  finish_grad(c, gscale, grad_w, c->ev[1]);
+  if (st[3] != 0)
+    return set_err(c, GR_E_CAPACITY, "4PCF: label offsets within a row exceed the hash key range");
+  c->st.ms_graph = reuse ? 0.0 : ev_ms(c->ev[0], c->ev[1]);
+  c->st.ms_total = c->st.ms_graph + c->st.ms_query;
+  c->st.n_points = n;
+  c->st.n_edges = 2 * c->csr.n_edges;
+  c->st.upper_edges = c->csr.n_edges;
+  c->st.tuples = (int64_t)st[0];
+  c->st.rooted = (int64_t)st[1];
+  c->st.probes = (int64_t)st[2];
+  c->st.kernel_launches = (reuse ? 0 : c->index.launches + c->csr.launches) + 2;
+  GR_API_END(c)
+}
+
 // ----------------------------------------------------------- batched regions --
 int gr_set_regions(gr_ctx* c, int32_t nsplit) {
   GR_API_BEGIN(c)

@@ -95,5 +95,13 @@ bool launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bo
                   unsigned long long* g_cnt, unsigned long long* g_fix, unsigned long long* d_cnt,
                   unsigned long long* d_fix, int nh, int nd, double fscale, double dscale,
                   bool shared_counts, unsigned long long* stats, int* work, cudaStream_t s);
+// 4PCF adjoint: gradient of sum(cot2 N2) + sum(cot3 N3) + sum(cotN discN)
+// + sum(cotR discR), cot = [cot2 nbin | cot3 nbin | cotN 6 nbin | cotR 6 nbin]
+// (nbin = ncfg nbins^2), into g_lo / g_hi (label order, zeroed) at scale
+// gscale.  Q as for launch_quad4 with tetra = 0.
+void launch_adj4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, const double* cot,
+                 double gscale, unsigned long long* g_lo, unsigned long long* g_hi,
+                 unsigned long long* stats, int* work, cudaStream_t s);
+
 
 }  // namespace gr

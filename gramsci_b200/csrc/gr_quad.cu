@@ -41,11 +41,13 @@ __host__ __device__ inline int qhash_lg_max(int cap) {
 struct QuadLayout {
   size_t off_rank, off_cnt, off_warp, warp_bytes, total;
   // per-warp sub-offsets
-  size_t o_rs, o_w, o_mo, o_col, o_len, o_xm, o_hkey, o_q, o_xy, o_xz, o_bits;
+  size_t o_rs, o_w, o_mo, o_g, o_col, o_len, o_xm, o_hkey, o_q, o_xy, o_xz, o_bits;
 };
 
-// ncounts: block-private 32-bit counters in shared memory (0: none)
-__host__ __device__ inline QuadLayout quad_layout(int nbins, int cap, int nwarps, int ncounts) {
+// ncounts: block-private 32-bit counters in shared memory (0: none);
+// adj: per-neighbour 128-bit gradient accumulators (adjoint mode)
+__host__ __device__ inline QuadLayout quad_layout(int nbins, int cap, int nwarps, int ncounts,
+                                                  bool adj = false) {
   QuadLayout L;
   size_t o = 0;
   L.off_rank = o;
@@ -57,6 +59,7 @@ __host__ __device__ inline QuadLayout quad_layout(int nbins, int cap, int nwarps
   L.o_rs = w;   w += (size_t)cap * 8;   // row start of each neighbour
   L.o_w = w;    w += (size_t)cap * 8;   // weight
   L.o_mo = w;   w += (size_t)cap * 8;   // (catalogue id << 32) | flags << 24 | meta(p, a)
+  L.o_g = w;    w += adj ? (size_t)cap * 16 : 0;  // gradient (lo, hi) of each neighbour
   L.o_col = w;  w += (size_t)cap * 4;   // label
   L.o_len = w;  w += (size_t)cap * 4;   // row length
   L.o_xm = w;   w += (size_t)cap * 4;   // X entry z: meta(a, b)
@@ -78,6 +81,8 @@ struct QuadCtx {
   unsigned long long *fix, *dfix;  // fixed-point (lo, hi) sums, hi at +5*nbin / +24*nbin
   double fscale;  // scale of the 4-point products
   double dscale;  // scale of the pair products of the disconnected terms
+  // adjoint: cotangents of N2, N3 (nbin each), discN, discR (6 nbin each)
+  const double *c2, *c3, *cN, *cR;
 };
 
 template <bool SHC>
@@ -183,23 +188,34 @@ __device__ __forceinline__ int tetra_contrib(const QuadCtx& X, const QVerts& V, 
          tetra_root<WEIGHTED, SHC, 2>(X, V, b, rndm, nr) + tetra_root<WEIGHTED, SHC, 3>(X, V, b, rndm, nr);
 }
 
-// One root R of a 4-clique for query_4pcf_all2: canonical perimeter check,
-// N2 / N3 at (cfg, bin(r,k2), bin(k1,k3)) and the six disconnected terms.
-template <bool WEIGHTED, bool SHC, int R>
-__device__ __forceinline__ int quad_root(const QuadCtx& X, const QVerts& V, unsigned long long packed,
-                                         unsigned rndm, int nr) {
-  if (V.fl[R] & FLAG_BUFFER) return 0;
-  if (!(V.fl[R] & kFlagDeg4)) return 0;
-  int u0, u1, u2;
+// Root R of a 4-clique for query_4pcf_all2: the histogram index of its
+// contribution, (cfg, bin(r,k2), bin(k1,k3)) with k1 < k2 < k3 the other
+// vertices in catalogue-id order (returned in u0..u2), or -1 when R is no
+// root (buffer point, row length <= 3) or its perimeter is not canonical.
+template <int R>
+__device__ __forceinline__ int quad_root_index(const QuadCtx& X, const QVerts& V,
+                                               unsigned long long packed, int& u0, int& u1,
+                                               int& u2) {
+  if (V.fl[R] & FLAG_BUFFER) return -1;
+  if (!(V.fl[R] & kFlagDeg4)) return -1;
   others_by_id<R>(V, u0, u1, u2);
   const int b1 = qbin(packed, R, u0), b2 = qbin(packed, u0, u1), b3 = qbin(packed, u1, u2),
             b4 = qbin(packed, R, u2);
-  if (!(b1 <= b2 && b2 <= b3 && b3 <= b4)) return 0;
+  if (!(b1 <= b2 && b2 <= b3 && b3 <= b4)) return -1;
   const int nb2 = X.nbins + 2;
   const int cfg = 1 + (X.F[b1] - X.F[1]) + (X.F[nb2 + b2] - X.F[nb2 + b1]) +
                   (X.F[2 * nb2 + b3] - X.F[2 * nb2 + b2]) + (X.F[3 * nb2 + b4] - X.F[3 * nb2 + b3]);
   const int d1 = qbin(packed, R, u1), d2 = qbin(packed, u0, u2);
-  const int kk = (cfg - 1) + X.ncfg * ((d1 - 1) + X.nbins * (d2 - 1));
+  return (cfg - 1) + X.ncfg * ((d1 - 1) + X.nbins * (d2 - 1));
+}
+
+// N2 / N3 and the six disconnected terms of root R.
+template <bool WEIGHTED, bool SHC, int R>
+__device__ __forceinline__ int quad_root(const QuadCtx& X, const QVerts& V, unsigned long long packed,
+                                         unsigned rndm, int nr) {
+  int u0, u1, u2;
+  const int kk = quad_root_index<R>(X, V, packed, u0, u1, u2);
+  if (kk < 0) return 0;
   qcount<SHC>(X, kk + X.nbin * nr);
   if (WEIGHTED)
     fix_add(&X.fix[kk + X.nbin * nr], &X.fix[kk + X.nbin * (nr + 5)],
@@ -223,6 +239,60 @@ __device__ __forceinline__ int quad_root(const QuadCtx& X, const QVerts& V, unsi
   return 1;
 }
 
+// Adjoint of root R: adds the cotangent of its 4-product to c4 and the
+// cotangents of its gated pair terms to D[edge of the pair].
+template <int R>
+__device__ __forceinline__ int quad_root_grad(const QuadCtx& X, const QVerts& V,
+                                              unsigned long long packed, unsigned rndm, int nr,
+                                              double& c4, double D[6]) {
+  int u0, u1, u2;
+  const int kk = quad_root_index<R>(X, V, packed, u0, u1, u2);
+  if (kk < 0) return 0;
+  c4 += __ldg(&X.c2[kk]) + (nr == 4 ? __ldg(&X.c3[kk]) : 0.0);
+  const int role[4] = {R, u0, u1, u2};
+#pragma unroll
+  for (int tt = 0; tt < 6; ++tt) {
+    if (!((rndm >> role[term_gate(tt)]) & 1u)) continue;
+    const int u = role[term_pu(tt)], vv = role[term_pv(tt)];
+    const int kt = kk + X.nbin * tt;
+    const bool both = ((rndm >> u) & 1u) && ((rndm >> vv) & 1u);
+    const double cd = __ldg(&X.cN[kt]) + (both ? __ldg(&X.cR[kt]) : 0.0);
+    const int e = qedge(u, vv);
+#pragma unroll
+    for (int ee = 0; ee < 6; ++ee)
+      if (ee == e) D[ee] += cd;
+  }
+  return 1;
+}
+
+// Gradient of the cotangent-weighted sums with respect to the four vertex
+// weights of one clique (g[v] = d/dw_v, vertices as in quad_contrib).  The
+// sums are multilinear: a 4-product contributes its cotangent times the
+// product of the other three weights, a pair term its cotangent times the
+// partner's weight.
+__device__ __forceinline__ int quad_grad(const QuadCtx& X, const QVerts& V, const uint32_t m[6],
+                                         double g[4]) {
+  unsigned long long packed = 0;
+#pragma unroll
+  for (int e = 0; e < 6; ++e) packed |= (unsigned long long)meta_bin(m[e]) << (8 * e);
+  unsigned rndm = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) rndm |= (unsigned)(V.fl[k] & FLAG_RANDOM) << k;
+  const int nr = __popc(rndm);
+  double c4 = 0.0, D[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  const int n = quad_root_grad<0>(X, V, packed, rndm, nr, c4, D) +
+                quad_root_grad<1>(X, V, packed, rndm, nr, c4, D) +
+                quad_root_grad<2>(X, V, packed, rndm, nr, c4, D) +
+                quad_root_grad<3>(X, V, packed, rndm, nr, c4, D);
+  const double w0 = V.w[0], w1 = V.w[1], w2 = V.w[2], w3 = V.w[3];
+  // edges: 0 (0,1) 1 (0,2) 2 (0,3) 3 (1,2) 4 (1,3) 5 (2,3)
+  g[0] = c4 * (w1 * w2 * w3) + D[0] * w1 + D[1] * w2 + D[2] * w3;
+  g[1] = c4 * (w0 * w2 * w3) + D[0] * w0 + D[3] * w2 + D[4] * w3;
+  g[2] = c4 * (w0 * w1 * w3) + D[1] * w0 + D[3] * w1 + D[5] * w3;
+  g[3] = c4 * (w0 * w1 * w2) + D[2] * w0 + D[4] * w1 + D[5] * w2;
+  return n;
+}
+
 // m: bins of (0,1) (0,2) (0,3) (1,2) (1,3) (2,3) for vertices 0 = p, 1 = a,
 // 2 = b, 3 = d.
 template <bool WEIGHTED, bool SHC>
@@ -244,14 +314,20 @@ __device__ __forceinline__ uint32_t qfib_slot(uint32_t off, int lg) {
 
 // SHC: unweighted counts in block-private 32-bit shared-memory counters,
 // added to the global histograms at the end of the block.
-template <bool WEIGHTED, bool SHC>
+// ADJ: instead of the histograms, the weight gradient (g_lo / g_hi, label
+// order, scale gscale) of sum(c2 N2) + sum(c3 N3) + sum(cN discN) +
+// sum(cR discR), cot = [c2 | c3 | cN | cR].
+template <bool WEIGHTED, bool SHC, bool ADJ>
 __global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
     DevCatalog C, CSRView G, QuadParams Q, unsigned long long* __restrict__ g_cnt,
     unsigned long long* __restrict__ g_fix, unsigned long long* __restrict__ d_cnt,
     unsigned long long* __restrict__ d_fix, int nh, int nd, double fscale, double dscale,
-    unsigned long long* __restrict__ stats, int* __restrict__ work) {
+    unsigned long long* __restrict__ stats, int* __restrict__ work,
+    const double* __restrict__ cot, double gscale, unsigned long long* __restrict__ g_lo,
+    unsigned long long* __restrict__ g_hi) {
+  constexpr bool LW = WEIGHTED || ADJ;  // weights staged
   extern __shared__ __align__(16) unsigned char smem[];
-  const QuadLayout L = quad_layout(Q.nbins, Q.cap, blockDim.x >> 5, SHC ? nh + nd : 0);
+  const QuadLayout L = quad_layout(Q.nbins, Q.cap, blockDim.x >> 5, SHC ? nh + nd : 0, ADJ);
   int* s_F = reinterpret_cast<int*>(smem + L.off_rank);
   const int nb2 = Q.nbins + 2;
   for (int k = threadIdx.x; k < 4 * nb2; k += blockDim.x) s_F[k] = Q.rank.F[k / nb2][k % nb2];
@@ -277,6 +353,10 @@ __global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
   }
   X.fscale = fscale;
   X.dscale = dscale;
+  X.c2 = cot;
+  X.c3 = ADJ ? cot + X.nbin : nullptr;
+  X.cN = ADJ ? cot + 2 * (size_t)X.nbin : nullptr;
+  X.cR = ADJ ? cot + 8 * (size_t)X.nbin : nullptr;
 
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
@@ -292,6 +372,8 @@ __global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
   uint16_t* s_xy = reinterpret_cast<uint16_t*>(wb + L.o_xy);
   uint16_t* s_xz = reinterpret_cast<uint16_t*>(wb + L.o_xz);
   uint32_t* s_bits = reinterpret_cast<uint32_t*>(wb + L.o_bits);
+  unsigned long long* s_glo = reinterpret_cast<unsigned long long*>(wb + L.o_g);
+  unsigned long long* s_ghi = s_glo + Q.cap;
   const int cap = Q.cap;
   const int lg_max = qhash_lg_max(cap);
   unsigned long long quads = 0, rooted = 0, probes = 0;
@@ -330,7 +412,8 @@ __global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
     }
     const uint8_t fp = C.flags[p] | (G.deg_full[p] > 3 ? kFlagDeg4 : 0);
     const int op = C.orig[p];
-    const double wp = WEIGHTED ? C.w[p] : 0.0;
+    const double wp = LW ? C.w[p] : 0.0;
+    Fix128 racc = {0ull, 0ull};  // adjoint: gradient of the root, per lane
     int lg = 6;
     while (lg < lg_max && (1 << lg) < 8 * k) ++lg;
     const int hs = 1 << lg;
@@ -348,7 +431,11 @@ __global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
         const uint8_t fa = C.flags[a] | (G.deg_full[a] > 3 ? kFlagDeg4 : 0);
         s_mo[x] = ((unsigned long long)(uint32_t)C.orig[a] << 32) |
                   (rec_meta(r) | ((uint32_t)fa << 24));
-        if (WEIGHTED) s_w[x] = C.w[a];
+        if (LW) s_w[x] = C.w[a];
+        if (ADJ) {
+          s_glo[x] = 0ull;
+          s_ghi[x] = 0ull;
+        }
         const uint32_t off = (uint32_t)(a - p);
         const uint32_t key = (off << 10) | (uint32_t)x;
         uint32_t h = qfib_slot(off, lg);
@@ -406,13 +493,25 @@ __global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
         V.og[2] = (int)(mpb_w >> 32);
         V.og[3] = (int)(mpd_w >> 32);
         V.w[0] = wp;
-        V.w[1] = WEIGHTED ? s_w[x] : 0.0;
-        V.w[2] = WEIGHTED ? s_w[yb] : 0.0;
-        V.w[3] = WEIGHTED ? s_w[yd] : 0.0;
+        V.w[1] = LW ? s_w[x] : 0.0;
+        V.w[2] = LW ? s_w[yb] : 0.0;
+        V.w[3] = LW ? s_w[yd] : 0.0;
         // m: (p,a) (p,b) (p,d) (a,b) (a,d) (b,d)
         const uint32_t m[6] = {(uint32_t)mpa_w & 0xffffffu, (uint32_t)mpb_w & 0xffffffu,
                                (uint32_t)mpd_w & 0xffffffu, s_xm[z], s_xm[s_xz[yd]], mbd};
-        const int nroot = X.tetra ? tetra_contrib<WEIGHTED, SHC>(X, V, m) : quad_contrib<WEIGHTED, SHC>(X, V, m);
+        int nroot;
+        if (ADJ) {
+          double g[4];
+          nroot = quad_grad(X, V, m, g);
+          if (nroot) {
+            fix_acc(racc, g[0], gscale);
+            fix_add(&s_glo[x], &s_ghi[x], g[1], gscale);
+            fix_add(&s_glo[yb], &s_ghi[yb], g[2], gscale);
+            fix_add(&s_glo[yd], &s_ghi[yd], g[3], gscale);
+          }
+        } else {
+          nroot = X.tetra ? tetra_contrib<WEIGHTED, SHC>(X, V, m) : quad_contrib<WEIGHTED, SHC>(X, V, m);
+        }
         quads += nroot > 0;
         rooted += nroot;
       };
@@ -477,6 +576,15 @@ __global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
       if (lane < qn) drain_one(lane);
       __syncwarp();
     }
+    if (ADJ) {
+      // flush the gradients of this root and of its neighbours
+      for (int x = lane; x < k; x += 32) {
+        const unsigned long long lo = s_glo[x], hi = s_ghi[x];
+        if (lo | hi) fix_merge(&g_lo[s_col[x]], &g_hi[s_col[x]], lo, hi);
+      }
+      racc = fix_warp_sum(racc);
+      if (lane == 0 && (racc.lo | racc.hi)) fix_merge(&g_lo[p], &g_hi[p], racc.lo, racc.hi);
+    }
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -498,10 +606,10 @@ __global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
   }
 }
 
-// Warps per block: as many as fit in shared memory (at most 32).
-int quad4_warps(int nbins, int cap, int ncounts) {
+// Warps per block: as many as fit in shared memory (at most kQuadMaxWarps).
+int quad4_warps(int nbins, int cap, int ncounts, bool adj = false) {
   int nw = kQuadMaxWarps;
-  while (nw > 1 && quad_layout(nbins, cap, nw, ncounts).total > kQuadSmemLimit) nw -= 1;
+  while (nw > 1 && quad_layout(nbins, cap, nw, ncounts, adj).total > kQuadSmemLimit) nw -= 1;
   return nw;
 }
 
@@ -519,8 +627,9 @@ bool launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bo
   const int nw = quad4_warps(Q.nbins, Q.cap, shared_counts ? ncnt : 0);
   const size_t smem = quad_layout(Q.nbins, Q.cap, nw, shared_counts ? ncnt : 0).total;
   if (smem > kQuadSmemLimit) throw Error{-2, "4PCF: per-warp shared memory exceeds the SM limit"};
-  auto kfn = weighted ? quad4_kernel<true, false>
-                      : (shared_counts ? quad4_kernel<false, true> : quad4_kernel<false, false>);
+  auto kfn = weighted ? quad4_kernel<true, false, false>
+                      : (shared_counts ? quad4_kernel<false, true, false>
+                                       : quad4_kernel<false, false, false>);
   GR_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nw * 32, smem));
@@ -531,9 +640,31 @@ bool launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bo
   if (blocks < 1) blocks = 1;
   GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));
   kfn<<<(unsigned)blocks, nw * 32, smem, s>>>(C, G, Q, g_cnt, g_fix, d_cnt, d_fix, nh, nd, fscale,
-                                              dscale, stats, work);
+                                              dscale, stats, work, nullptr, 1.0, nullptr, nullptr);
   GR_CHECK_LAUNCH();
   return shared_counts;
+}
+
+void launch_adj4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, const double* cot,
+                 double gscale, unsigned long long* g_lo, unsigned long long* g_hi,
+                 unsigned long long* stats, int* work, cudaStream_t s) {
+  if (C.n <= 0) return;
+  const int nw = quad4_warps(Q.nbins, Q.cap, 0, true);
+  const size_t smem = quad_layout(Q.nbins, Q.cap, nw, 0, true).total;
+  if (smem > kQuadSmemLimit) throw Error{-2, "4PCF adjoint: per-warp shared memory exceeds the SM limit"};
+  auto kfn = quad4_kernel<false, false, true>;
+  GR_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nw * 32, smem));
+  if (per_sm < 1) per_sm = 1;
+  int64_t blocks = (int64_t)per_sm * 148;
+  const int64_t need = ((int64_t)C.n + nw - 1) / nw;
+  if (blocks > need) blocks = need;
+  if (blocks < 1) blocks = 1;
+  GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));
+  kfn<<<(unsigned)blocks, nw * 32, smem, s>>>(C, G, Q, nullptr, nullptr, nullptr, nullptr, 0, 0,
+                                              1.0, 1.0, stats, work, cot, gscale, g_lo, g_hi);
+  GR_CHECK_LAUNCH();
 }
 
 size_t quad4_smem_bytes(int nbins, int cap) {

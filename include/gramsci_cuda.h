@@ -206,6 +206,18 @@ int gr_regions_export(gr_ctx* ctx, int64_t* member_off, int32_t* member_orig,
 int gr_adjoint_2pcf(gr_ctx* ctx, const double* cot2, const double* cot3, double* grad_w);
 int gr_adjoint_3pcf(gr_ctx* ctx, const double* cot2, const double* cot3, double* grad_w);
 
+/* 4PCF weight adjoint: gradient of L = sum(cot2 N2) + sum(cot3 N3) +
+ * sum(cotN discN) + sum(cotR discR) of gr_count_4pcf (query_4pcf_all2,
+ * src/gramsci.F90:662-825) with respect to every signed normalised weight.
+ * cot2/cot3 have N2's shape (ncfg, nbins, nbins), cotN/cotR discN's
+ * (ncfg, nbins, nbins, 6); all but cot2 may be NULL.  Every rooted 4-clique
+ * adds to each of its vertices the cotangent of its bin times the product of
+ * the other three weights, and each gated pair term its cotangent times the
+ * partner's weight.  Reuses the graph of the last count or graph build when
+ * the catalogue and bins are unchanged; 128-bit fixed-point accumulation. */
+int gr_adjoint_4pcf(gr_ctx* ctx, const double* cot2, const double* cot3, const double* cotN,
+                    const double* cotR, double* grad_w);
+
 /* Statistics of the last count call. */
 int gr_get_stats(gr_ctx* ctx, gr_stats* out);
 

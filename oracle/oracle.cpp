@@ -1157,6 +1157,79 @@ void orc_adjoint_3pcf(const orc_graph* h, const double* w, const int32_t* buffer
   }
 }
 
+// Gradient of L = sum(cot2 N2) + sum(cot3 N3) + sum(cotN discN) +
+// sum(cotR discR) for the 4PCF of orc_4pcf (the same enumeration: root i,
+// a < b < c in its row).  Each rooted quad adds to every one of its four
+// vertices (cot2[k] + cot3[k] if all four are randoms) times the product of
+// the other three weights; each gated pair term t adds (cotN[kt] + cotR[kt]
+// if both pair vertices are randoms) times the partner's weight to each of
+// its two vertices.  Per-thread long double gradients, summed at the end.
+void orc_adjoint_4pcf(const orc_graph* h, const double* w, const int32_t* buffer, int64_t n_data,
+                      const double* cot2, const double* cot3, const double* cotN,
+                      const double* cotR, double* grad) {
+  const Graph& G = *reinterpret_cast<const Graph*>(h);
+  const int nb = G.B.nbins;
+  const int ncfg = (int)ncomb_multiset(nb, 4);
+  const int64_t nbin = (int64_t)ncfg * nb * nb;
+  const int nt = omp_get_max_threads();
+  std::vector<acc_t> part((size_t)nt * G.n, 0.0L);
+  static const int gate[6] = {3, 3, 1, 0, 0, 0};
+  static const int pu[6] = {0, 0, 0, 1, 3, 3};
+  static const int pv[6] = {1, 2, 3, 2, 2, 1};
+#pragma omp parallel
+  {
+    acc_t* g = &part[(size_t)omp_get_thread_num() * G.n];
+#pragma omp for schedule(dynamic, 8)
+    for (int64_t i = 0; i < G.n; ++i) {
+      if (buffer && buffer[i] == 1) continue;
+      int64_t r0 = G.row_ptr[i], r1 = G.row_ptr[i + 1];
+      if (r1 - r0 <= 3) continue;
+      for (int64_t k1 = r0; k1 < r1; ++k1) {
+        int32_t id1 = G.col[k1];
+        for (int64_t k2 = k1 + 1; k2 < r1; ++k2) {
+          int32_t id2 = G.col[k2];
+          int ind4 = find_dist(G, id1, id2);
+          if (ind4 == 0) continue;
+          for (int64_t k3 = k2 + 1; k3 < r1; ++k3) {
+            int32_t id3 = G.col[k3];
+            int ind5 = find_dist(G, id2, id3);
+            if (ind5 == 0) continue;
+            int ind6 = find_dist(G, id1, id3);
+            if (ind6 == 0) continue;
+            int cfg = bintable4(G.bin[k1], ind4, ind5, G.bin[k3], nb);
+            if (cfg <= 0) continue;
+            int64_t k = (cfg - 1) + ncfg * ((G.bin[k2] - 1) + nb * (int64_t)(ind6 - 1));
+            int64_t v[4] = {i, id1, id2, id3};
+            bool r[4] = {i >= n_data, id1 >= n_data, id2 >= n_data, id3 >= n_data};
+            acc_t c4 = cot2[k];
+            if (cot3 && r[0] && r[1] && r[2] && r[3]) c4 += cot3[k];
+            for (int a = 0; a < 4; ++a) {
+              acc_t p = c4;
+              for (int b = 0; b < 4; ++b)
+                if (b != a) p *= (acc_t)w[v[b]];
+              g[v[a]] += p;
+            }
+            for (int tt = 0; tt < 6; ++tt) {
+              if (!r[gate[tt]]) continue;
+              int64_t kt = k + nbin * tt;
+              acc_t cd = cotN ? (acc_t)cotN[kt] : 0.0L;
+              if (cotR && r[pu[tt]] && r[pv[tt]]) cd += cotR[kt];
+              g[v[pu[tt]]] += cd * (acc_t)w[v[pv[tt]]];
+              g[v[pv[tt]]] += cd * (acc_t)w[v[pu[tt]]];
+            }
+          }
+        }
+      }
+    }
+  }
+#pragma omp parallel for
+  for (int64_t k = 0; k < G.n; ++k) {
+    acc_t s = 0.0L;
+    for (int t = 0; t < nt; ++t) s += part[(size_t)t * G.n + k];
+    grad[k] = (double)s;
+  }
+}
+
 int32_t orc_max_threads() { return omp_get_max_threads(); }
 
 }  // extern "C"

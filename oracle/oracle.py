@@ -61,6 +61,8 @@ def lib():
                                 _i64, _d]
         L.orc_adjoint_2pcf.argtypes = [ctypes.c_void_p, _d, _i32, ctypes.c_int64, _d, _d, _d]
         L.orc_adjoint_3pcf.argtypes = [ctypes.c_void_p, _d, _i32, ctypes.c_int64, _i32, _d, _d, _d]
+        L.orc_adjoint_4pcf.argtypes = [ctypes.c_void_p, _d, _i32, ctypes.c_int64, _d, _d, _d, _d,
+                                       _d]
         L.orc_max_threads.restype = ctypes.c_int32
         _lib = L
     return _lib
@@ -216,6 +218,17 @@ class Graph:
         lib().orc_adjoint_3pcf(self._h, _p(w, _d), _p(buf, _i32), int(n_data),
                                _p(np.ascontiguousarray(tab.T.ravel()), _i32), _p(c2, _d),
                                _p(c3, _d), _p(g, _d))
+        return g
+
+    def adjoint4(self, w, n_data, cot2, cot3=None, cotN=None, cotR=None, buffer=None):
+        """Gradient of sum(cot2 N2 + cot3 N3 + cotN discN + cotR discR) of
+        pcf4 with respect to w; cotangents in the shapes pcf4 returns."""
+        w = np.ascontiguousarray(w, np.float64)
+        buf = None if buffer is None else np.ascontiguousarray(buffer, np.int32)
+        f = lambda a: None if a is None else np.ascontiguousarray(np.asarray(a, np.float64).T.ravel())
+        g = np.zeros(self.n)
+        lib().orc_adjoint_4pcf(self._h, _p(w, _d), _p(buf, _i32), int(n_data), _p(f(cot2), _d),
+                               _p(f(cot3), _d), _p(f(cotN), _d), _p(f(cotR), _d), _p(g, _d))
         return g
 
 

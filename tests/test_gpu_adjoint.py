@@ -10,6 +10,10 @@ galaxies with lognormal weights plus uniform randoms, same number density).
   any step; a step of half the weight keeps the FP64 cancellation in
   L(w+h) - L(w-h) far below the tolerance;
 * through the weight normalisation with torch autograd.
+
+The 4PCF adjoint (all four cotangent terms N2, N3, discN, discR) is checked
+the same two ways on the 4PCF workload (Neyman-Scott galaxies, 4 bins) at
+reduced scale, with lognormal weights and with buffer points.
 """
 import numpy as np
 import pytest
@@ -47,6 +51,67 @@ def test_adjoint_matches_oracle(gpu_ctx, oracle, order, name, scale):
         ref = G.adjoint3(w, cat.n_data, c2, c3)
     assert np.abs(ref).max() > 0
     assert np.all(np.abs(g - ref) <= 1e-12 * np.abs(ref).max())
+
+
+@pytest.mark.parametrize("case", ["lognormal", "buffer", "unit_partial"])
+def test_adjoint_4pcf_matches_oracle(gpu_ctx, oracle, case):
+    cat = catalogs.make("c3_4pcf", scale=0.05)
+    sp = catalogs.WORKLOADS["c3_4pcf"]
+    rng = np.random.default_rng(40 + len(case))
+    raw = np.ones(cat.n) if case == "unit_partial" else rng.lognormal(0, 0.3, cat.n)
+    w = catalogs.normalise(raw, cat.n_data, cat.n_rand)
+    buf = (rng.random(cat.n) < 0.2).astype(np.int32) if case == "buffer" else None
+    gpu_ctx.set_catalog(cat.xyz, w, cat.n_data, buffer=buf)
+    gpu_ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
+    nb = sp["nbins"]
+    nc = oracle.ncfg4(nb)
+    c2, c3 = rng.normal(size=(nc, nb, nb)), rng.normal(size=(nc, nb, nb))
+    cN, cR = rng.normal(size=(nc, nb, nb, 6)), rng.normal(size=(nc, nb, nb, 6))
+    if case == "unit_partial":
+        c3, cR = None, None
+        gpu_ctx.count_4pcf()  # the adjoint reuses this graph
+    g = gpu_ctx.adjoint_4pcf(c2, c3, cN, cR)
+    G = oracle.Graph(cat.xyz, sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
+    ref = G.adjoint4(w, cat.n_data, c2, c3, cN, cR, buffer=buf)
+    assert np.count_nonzero(ref) > cat.n // 10
+    assert np.all(np.abs(g - ref) <= 1e-12 * np.abs(ref).max())
+    if buf is not None:
+        # buffer points are never roots but still carry gradient as members
+        assert np.count_nonzero(g[buf == 1]) > 0
+
+
+def test_autograd_4pcf_matches_finite_differences():
+    import torch
+
+    from gramsci_b200 import autograd
+
+    cat = catalogs.make("c3_4pcf", scale=0.02, seed=23)
+    sp = catalogs.WORKLOADS["c3_4pcf"]
+    rng = np.random.default_rng(104)
+    w = catalogs.normalise(rng.lognormal(0, 0.3, cat.n), cat.n_data, cat.n_rand)
+    dev = torch.device("cuda:0")
+    xyz = torch.from_numpy(cat.xyz).to(dev)
+    wt = torch.tensor(w, dtype=torch.float64, device=dev, requires_grad=True)
+    args = (cat.n_data, sp["rmin"], sp["rmax"], sp["nbins"])
+    outs = autograd.pcf4(wt, xyz, *args)
+    cots = [torch.tensor(rng.normal(size=o.shape), device=dev) for o in outs]
+    L = sum((c * o).sum() for c, o in zip(cots, outs))
+    (g,) = torch.autograd.grad(L, wt)
+    g = g.cpu().numpy()
+
+    def loss(wv):
+        o = autograd.pcf4(torch.tensor(wv, dtype=torch.float64, device=dev), xyz, *args)
+        return float(sum((c * x).sum() for c, x in zip(cots, o)))
+
+    nz = np.flatnonzero(g)
+    assert len(nz) >= 32
+    for k in rng.choice(nz, 32, replace=False):
+        h = 0.5 * abs(w[k])
+        wp, wm = w.copy(), w.copy()
+        wp[k] += h
+        wm[k] -= h
+        fd = (loss(wp) - loss(wm)) / (2 * h)
+        assert abs(fd - g[k]) <= 1e-8 * max(abs(fd), abs(g[k])), (k, fd, g[k])
 
 
 @pytest.mark.parametrize("order", [2, 3])

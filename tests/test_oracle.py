@@ -276,6 +276,36 @@ def test_adjoint_3pcf_matches_finite_differences(oracle):
         assert abs(fd - g[k]) <= 1e-7 * max(abs(fd), abs(g[k]), 1e-30)
 
 
+def test_adjoint_4pcf_matches_finite_differences(oracle):
+    """All four cotangent terms (N2, N3, discN, discR), buffer roots
+    included.  The sums are multilinear in the weights, so central
+    differences carry only rounding error."""
+    xyz, w, nd = small_catalogue(25, 25, 30.0, 3)
+    nb = 3
+    G = oracle.Graph(xyz, 1.0, 12.0, nb, 1)
+    rng = np.random.default_rng(12)
+    buf = (rng.random(len(w)) < 0.15).astype(np.int32)
+    nc = oracle.ncfg4(nb)
+    c2, c3 = rng.normal(size=(nc, nb, nb)), rng.normal(size=(nc, nb, nb))
+    cN, cR = rng.normal(size=(nc, nb, nb, 6)), rng.normal(size=(nc, nb, nb, 6))
+    g = G.adjoint4(w, nd, c2, c3, cN, cR, buffer=buf)
+
+    def L(wv):
+        r = G.pcf4(wv, nd, buffer=buf)
+        return float((c2 * r["N2"]).sum() + (c3 * r["N3"]).sum() + (cN * r["discN"]).sum()
+                     + (cR * r["discR"]).sum())
+
+    assert np.count_nonzero(g) > len(w) // 4
+    gmax = np.abs(g).max()
+    for k in rng.choice(np.flatnonzero(g), 10, replace=False):
+        h = 0.5 * abs(w[k])
+        wp, wm = w.copy(), w.copy()
+        wp[k] += h
+        wm[k] -= h
+        fd = (L(wp) - L(wm)) / (2 * h)
+        assert abs(fd - g[k]) <= 1e-10 * gmax, (k, fd, g[k])
+
+
 def test_equi_and_tetra_match_brute_force(oracle):
     """-equi / -tetra (gramsci.F90:402-660): same-bin triangles and 4-cliques,
     against an independent enumeration."""
