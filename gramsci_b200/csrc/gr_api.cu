@@ -808,14 +808,16 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   if (nbin64 * 29 > ((int64_t)1 << 31)) return set_err(c, GR_E_CAPACITY, "4PCF histogram too large");
   const int ncfg = (int)ncfg64, nbin = (int)nbin64;
   const int ndc = tetra ? 5 : 4;  // disc categories
-  const int nh = nbin * 5, nd = nbin * 6 * ndc;
+  // the last category (discR) equals the one before it (all randoms) and is
+  // copied here instead of accumulated on the device
+  const int nh = nbin * 5, nd = nbin * 6 * ndc, ndv = nbin * 6 * (ndc - 1);
   const bool weighted = !c->uniform;
   const double fscale = fix_scale(c->wmax * c->wmax * c->wmax * c->wmax);
   const double dscale = fix_scale(tetra ? c->wmax * c->wmax * c->wmax : c->wmax * c->wmax);
   c->hcnt.reserve(nh);
   c->hfix.reserve(2 * nh);
-  c->dcnt.reserve(nd);
-  c->dfix.reserve(2 * nd);
+  c->dcnt.reserve(ndv);
+  c->dfix.reserve(2 * ndv);
   c->stats.reserve(8);
   const bool reuse = reuse_graph(c);
   GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
@@ -827,9 +829,11 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
                                      (unsigned long long)c->csr.candidates,
                                      (unsigned long long)c->csr.max_deg};
   GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nh, s));
-  GR_CUDA_TRY(cudaMemsetAsync(c->hfix.p, 0, sizeof(unsigned long long) * 2 * nh, s));
-  GR_CUDA_TRY(cudaMemsetAsync(c->dcnt.p, 0, sizeof(unsigned long long) * nd, s));
-  GR_CUDA_TRY(cudaMemsetAsync(c->dfix.p, 0, sizeof(unsigned long long) * 2 * nd, s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->dcnt.p, 0, sizeof(unsigned long long) * ndv, s));
+  if (weighted) {
+    GR_CUDA_TRY(cudaMemsetAsync(c->hfix.p, 0, sizeof(unsigned long long) * 2 * nh, s));
+    GR_CUDA_TRY(cudaMemsetAsync(c->dfix.p, 0, sizeof(unsigned long long) * 2 * ndv, s));
+  }
   GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
   if ((int64_t)gst[2] > 1024)
     return set_err(c, GR_E_CAPACITY, "4PCF: a point has more than 1024 larger-label neighbours");
@@ -852,21 +856,21 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   for (int attempt = 0; attempt < 2; ++attempt) {
     if (attempt > 0) {
       GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nh, s));
-      GR_CUDA_TRY(cudaMemsetAsync(c->dcnt.p, 0, sizeof(unsigned long long) * nd, s));
+      GR_CUDA_TRY(cudaMemsetAsync(c->dcnt.p, 0, sizeof(unsigned long long) * ndv, s));
       GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
       GR_CUDA_TRY(cudaEventRecord(q0, s));
     }
     const bool shared = launch_quad4(c->index.view(), G, Q, weighted, c->hcnt.p, c->hfix.p,
-                                     c->dcnt.p, c->dfix.p, nh, nd, fscale, dscale, attempt == 0,
+                                     c->dcnt.p, c->dfix.p, nh, ndv, fscale, dscale, attempt == 0,
                                      c->stats.p, c->work.p, s);
     GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
     GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
-    GR_CUDA_TRY(cudaMemcpyAsync(dc.data(), c->dcnt.p, sizeof(unsigned long long) * nd, cudaMemcpyDeviceToHost, s));
+    GR_CUDA_TRY(cudaMemcpyAsync(dc.data(), c->dcnt.p, sizeof(unsigned long long) * ndv, cudaMemcpyDeviceToHost, s));
     if (weighted) {
       hf.resize(2 * (size_t)nh);
-      df.resize(2 * (size_t)nd);
+      df.resize(2 * (size_t)ndv);
       GR_CUDA_TRY(cudaMemcpyAsync(hf.data(), c->hfix.p, sizeof(unsigned long long) * 2 * nh, cudaMemcpyDeviceToHost, s));
-      GR_CUDA_TRY(cudaMemcpyAsync(df.data(), c->dfix.p, sizeof(unsigned long long) * 2 * nd, cudaMemcpyDeviceToHost, s));
+      GR_CUDA_TRY(cudaMemcpyAsync(df.data(), c->dfix.p, sizeof(unsigned long long) * 2 * ndv, cudaMemcpyDeviceToHost, s));
     }
     GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
     GR_CUDA_TRY(cudaStreamSynchronize(s));
@@ -874,9 +878,12 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   }
   if (st[3] != 0)
     return set_err(c, GR_E_CAPACITY, "4PCF: label offsets within a row exceed the hash key range");
+  // discR category = the all-random category before it
+  for (int k = 0; k < nbin * 6; ++k) dc[(size_t)ndv + k] = dc[(size_t)ndv - nbin * 6 + k];
   if (weighted) {
     for (int k = 0; k < nh; ++k) hs[k] = fix_value(hf[k], hf[(size_t)nh + k], fscale);
-    for (int k = 0; k < nd; ++k) ds[k] = fix_value(df[k], df[(size_t)nd + k], dscale);
+    for (int k = 0; k < ndv; ++k) ds[k] = fix_value(df[k], df[(size_t)ndv + k], dscale);
+    for (int k = 0; k < nbin * 6; ++k) ds[(size_t)ndv + k] = ds[(size_t)ndv - nbin * 6 + k];
   }
   if (!weighted) {
     for (int nr = 0; nr < 5; ++nr) {

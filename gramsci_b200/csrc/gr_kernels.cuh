@@ -87,10 +87,12 @@ struct QuadParams {
 // hash key range (the host reports it).  work: one device int, the dynamic
 // root counter (reset by the launch).
 // The outputs (g_cnt nh, g_fix 2 nh, d_cnt nd, d_fix 2 nd; fix arrays only
-// when weighted) must be zeroed.  shared_counts: unweighted counts in
-// block-private 32-bit shared-memory counters (exact while the rooted total
-// stays below 2^32; the caller checks stats[1] and reruns without them
-// otherwise).  Returns whether the shared counters were used.
+// when weighted) must be zeroed; the last disc category (discR, equal to the
+// all-random one before it) is not written, nd covers the others.
+// shared_counts: unweighted counts in block-private 32-bit shared-memory
+// counters (exact while the rooted total stays below 2^32; the caller
+// checks stats[1] and reruns without them otherwise).  Returns whether the
+// shared counters were used.
 bool launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bool weighted,
                   unsigned long long* g_cnt, unsigned long long* g_fix, unsigned long long* d_cnt,
                   unsigned long long* d_fix, int nh, int nd, double fscale, double dscale,

@@ -78,7 +78,8 @@ struct QuadCtx {
   int nbins, ncfg, nbin, tetra;
   unsigned long long *cnt, *dcnt;
   unsigned int *scnt, *sdcnt;  // block-private 32-bit counts in shared memory, or null
-  unsigned long long *fix, *dfix;  // fixed-point (lo, hi) sums, hi at +5*nbin / +24*nbin
+  unsigned long long *fix, *dfix;  // fixed-point (lo, hi) sums, hi at +5*nbin / +dhi
+  int dhi;                          // disc entries on the device (hi offset in dfix)
   double fscale;  // scale of the 4-point products
   double dscale;  // scale of the pair products of the disconnected terms
   // adjoint: cotangents of N2, N3 (nbin each), discN, discR (6 nbin each)
@@ -164,12 +165,9 @@ __device__ __forceinline__ int tetra_root(const QuadCtx& X, const QVerts& V, int
     const int nr3 = (int)((rndm >> ua) & 1u) + (int)((rndm >> ub) & 1u) + (int)((rndm >> uc) & 1u);
     const int kt = (b - 1) + nb * tt;
     const double qv = WEIGHTED ? (qsel(ua, V) * qsel(ub, V)) * qsel(uc, V) : 0.0;
+    // discR (all three random) equals category 3 and is copied on the host
     qdcount<SHC>(X, kt + nb * 6 * nr3);
-    if (WEIGHTED) fix_add(&X.dfix[kt + nb * 6 * nr3], &X.dfix[kt + nb * 6 * (nr3 + 5)], qv, X.dscale);
-    if (((rndm >> ub) & 1u) && ((rndm >> uc) & 1u)) {
-      qdcount<SHC>(X, kt + nb * 24);
-      if (WEIGHTED) fix_add(&X.dfix[kt + nb * 24], &X.dfix[kt + nb * 54], qv, X.dscale);
-    }
+    if (WEIGHTED) fix_add(&X.dfix[kt + nb * 6 * nr3], &X.dfix[kt + nb * 6 * nr3 + X.dhi], qv, X.dscale);
   }
   return 1;
 }
@@ -228,13 +226,10 @@ __device__ __forceinline__ int quad_root(const QuadCtx& X, const QVerts& V, unsi
     const int npr = (int)((rndm >> u) & 1u) + (int)((rndm >> vv) & 1u);
     const int kt = kk + X.nbin * tt;
     const double q = WEIGHTED ? qsel(u, V) * qsel(vv, V) : 0.0;
+    // discR (both random) equals category 2 and is copied on the host
     qdcount<SHC>(X, kt + X.nbin * 6 * npr);
     if (WEIGHTED)
-      fix_add(&X.dfix[kt + X.nbin * 6 * npr], &X.dfix[kt + X.nbin * (6 * npr + 24)], q, X.dscale);
-    if (npr == 2) {
-      qdcount<SHC>(X, kt + X.nbin * 18);
-      if (WEIGHTED) fix_add(&X.dfix[kt + X.nbin * 18], &X.dfix[kt + X.nbin * 42], q, X.dscale);
-    }
+      fix_add(&X.dfix[kt + X.nbin * 6 * npr], &X.dfix[kt + X.nbin * 6 * npr + X.dhi], q, X.dscale);
   }
   return 1;
 }
@@ -308,6 +303,91 @@ __device__ __forceinline__ int quad_contrib(const QuadCtx& X, const QVerts& V, c
          quad_root<WEIGHTED, SHC, 2>(X, V, packed, rndm, nr) + quad_root<WEIGHTED, SHC, 3>(X, V, packed, rndm, nr);
 }
 
+// Compact form of quad_contrib: the four roots and the six terms are loops
+// that are not unrolled, so the code of the (long) weighted updates appears
+// once; the clique's id order, flags and roles are packed into registers
+// (two bits per vertex index, eight per flag byte) so that runtime indices
+// need no local memory.
+// Vertex indices 0..3 in ascending catalogue id, two bits each.
+__device__ __forceinline__ unsigned id_order(const QVerts& V) {
+  int g0 = V.og[0], g1 = V.og[1], g2 = V.og[2], g3 = V.og[3];
+  unsigned a0 = 0, a1 = 1, a2 = 2, a3 = 3;
+  auto cx = [](int& ga, int& gb, unsigned& ia, unsigned& ib) {
+    if (ga > gb) {
+      const int t = ga; ga = gb; gb = t;
+      const unsigned u = ia; ia = ib; ib = u;
+    }
+  };
+  cx(g0, g1, a0, a1);
+  cx(g2, g3, a2, a3);
+  cx(g0, g2, a0, a2);
+  cx(g1, g3, a1, a3);
+  cx(g1, g2, a1, a2);
+  return a0 | (a1 << 2) | (a2 << 4) | (a3 << 6);
+}
+
+template <bool WEIGHTED, bool SHC>
+__device__ __forceinline__ int quad_root_rt(const QuadCtx& X, const QVerts& V,
+                                            unsigned long long packed, unsigned rndm, int nr,
+                                            int R, unsigned perm, unsigned flw) {
+  const unsigned fr = flw >> (8 * R);
+  if (fr & FLAG_BUFFER) return 0;
+  if (!(fr & kFlagDeg4)) return 0;
+  // the other three in id order: drop R's field from the id order
+  int pos = 0;
+#pragma unroll
+  for (int i = 1; i < 4; ++i)
+    if ((int)((perm >> (2 * i)) & 3u) == R) pos = i;
+  const unsigned lowm = (1u << (2 * pos)) - 1u;
+  const unsigned oth = (perm & lowm) | ((perm >> (2 * pos + 2)) << (2 * pos));
+  const int u0 = (int)(oth & 3u), u1 = (int)((oth >> 2) & 3u), u2 = (int)((oth >> 4) & 3u);
+  const int b1 = qbin(packed, R, u0), b2 = qbin(packed, u0, u1), b3 = qbin(packed, u1, u2),
+            b4 = qbin(packed, R, u2);
+  if (!(b1 <= b2 && b2 <= b3 && b3 <= b4)) return 0;
+  const int nb2 = X.nbins + 2;
+  const int cfg = 1 + (X.F[b1] - X.F[1]) + (X.F[nb2 + b2] - X.F[nb2 + b1]) +
+                  (X.F[2 * nb2 + b3] - X.F[2 * nb2 + b2]) + (X.F[3 * nb2 + b4] - X.F[3 * nb2 + b3]);
+  const int d1 = qbin(packed, R, u1), d2 = qbin(packed, u0, u2);
+  const int kk = (cfg - 1) + X.ncfg * ((d1 - 1) + X.nbins * (d2 - 1));
+  qcount<SHC>(X, kk + X.nbin * nr);
+  if (WEIGHTED)
+    fix_add(&X.fix[kk + X.nbin * nr], &X.fix[kk + X.nbin * (nr + 5)],
+            ((qsel(R, V) * qsel(u0, V)) * qsel(u1, V)) * qsel(u2, V), X.fscale);
+  const unsigned rp = (unsigned)R | ((unsigned)u0 << 2) | ((unsigned)u1 << 4) | ((unsigned)u2 << 6);
+#pragma unroll 1
+  for (int tt = 0; tt < 6; ++tt) {
+    const int ga = (int)((rp >> (2 * term_gate(tt))) & 3u);
+    if (!((rndm >> ga) & 1u)) continue;
+    const int u = (int)((rp >> (2 * term_pu(tt))) & 3u), vv = (int)((rp >> (2 * term_pv(tt))) & 3u);
+    const int npr = (int)((rndm >> u) & 1u) + (int)((rndm >> vv) & 1u);
+    const int kt = kk + X.nbin * tt;
+    qdcount<SHC>(X, kt + X.nbin * 6 * npr);
+    if (WEIGHTED)
+      fix_add(&X.dfix[kt + X.nbin * 6 * npr], &X.dfix[kt + X.nbin * 6 * npr + X.dhi],
+              qsel(u, V) * qsel(vv, V), X.dscale);
+  }
+  return 1;
+}
+
+template <bool WEIGHTED, bool SHC>
+__device__ __forceinline__ int quad_contrib_c(const QuadCtx& X, const QVerts& V, const uint32_t m[6]) {
+  unsigned long long packed = 0;
+#pragma unroll
+  for (int e = 0; e < 6; ++e) packed |= (unsigned long long)meta_bin(m[e]) << (8 * e);
+  unsigned rndm = 0, flw = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    rndm |= (unsigned)(V.fl[k] & FLAG_RANDOM) << k;
+    flw |= (unsigned)V.fl[k] << (8 * k);
+  }
+  const int nr = __popc(rndm);
+  const unsigned perm = id_order(V);
+  int n = 0;
+#pragma unroll 1
+  for (int R = 0; R < 4; ++R) n += quad_root_rt<WEIGHTED, SHC>(X, V, packed, rndm, nr, R, perm, flw);
+  return n;
+}
+
 __device__ __forceinline__ uint32_t qfib_slot(uint32_t off, int lg) {
   return (off * 2654435769u) >> (32 - lg);
 }
@@ -317,7 +397,9 @@ __device__ __forceinline__ uint32_t qfib_slot(uint32_t off, int lg) {
 // ADJ: instead of the histograms, the weight gradient (g_lo / g_hi, label
 // order, scale gscale) of sum(c2 N2) + sum(c3 N3) + sum(cN discN) +
 // sum(cR discR), cot = [c2 | c3 | cN | cR].
-template <bool WEIGHTED, bool SHC, bool ADJ>
+// COMPACT: the 4PCF contributions through quad_contrib_c (loops over roots
+// and terms) instead of the unrolled quad_contrib.
+template <bool WEIGHTED, bool SHC, bool ADJ, bool COMPACT>
 __global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
     DevCatalog C, CSRView G, QuadParams Q, unsigned long long* __restrict__ g_cnt,
     unsigned long long* __restrict__ g_fix, unsigned long long* __restrict__ d_cnt,
@@ -342,6 +424,7 @@ __global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
   X.dcnt = d_cnt;
   X.fix = g_fix;
   X.dfix = d_fix;
+  X.dhi = nd;
   X.scnt = nullptr;
   X.sdcnt = nullptr;
   if (SHC) {
@@ -510,7 +593,9 @@ __global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
             fix_add(&s_glo[yd], &s_ghi[yd], g[3], gscale);
           }
         } else {
-          nroot = X.tetra ? tetra_contrib<WEIGHTED, SHC>(X, V, m) : quad_contrib<WEIGHTED, SHC>(X, V, m);
+          nroot = X.tetra ? tetra_contrib<WEIGHTED, SHC>(X, V, m)
+                          : (COMPACT ? quad_contrib_c<WEIGHTED, SHC>(X, V, m)
+                                     : quad_contrib<WEIGHTED, SHC>(X, V, m));
         }
         quads += nroot > 0;
         rooted += nroot;
@@ -627,9 +712,11 @@ bool launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bo
   const int nw = quad4_warps(Q.nbins, Q.cap, shared_counts ? ncnt : 0);
   const size_t smem = quad_layout(Q.nbins, Q.cap, nw, shared_counts ? ncnt : 0).total;
   if (smem > kQuadSmemLimit) throw Error{-2, "4PCF: per-warp shared memory exceeds the SM limit"};
-  auto kfn = weighted ? quad4_kernel<true, false, false>
-                      : (shared_counts ? quad4_kernel<false, true, false>
-                                       : quad4_kernel<false, false, false>);
+  // weighted: the compact contribution code (the unrolled form of its long
+  // fixed-point updates overflows the instruction cache); unweighted: unrolled
+  auto kfn = weighted ? quad4_kernel<true, false, false, true>
+                      : (shared_counts ? quad4_kernel<false, true, false, false>
+                                       : quad4_kernel<false, false, false, false>);
   GR_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nw * 32, smem));
@@ -652,7 +739,7 @@ void launch_adj4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, con
   const int nw = quad4_warps(Q.nbins, Q.cap, 0, true);
   const size_t smem = quad_layout(Q.nbins, Q.cap, nw, 0, true).total;
   if (smem > kQuadSmemLimit) throw Error{-2, "4PCF adjoint: per-warp shared memory exceeds the SM limit"};
-  auto kfn = quad4_kernel<false, false, true>;
+  auto kfn = quad4_kernel<false, false, true, false>;
   GR_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nw * 32, smem));
