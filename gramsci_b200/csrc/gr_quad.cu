@@ -234,60 +234,6 @@ __device__ __forceinline__ int quad_root(const QuadCtx& X, const QVerts& V, unsi
   return 1;
 }
 
-// Adjoint of root R: adds the cotangent of its 4-product to c4 and the
-// cotangents of its gated pair terms to D[edge of the pair].
-template <int R>
-__device__ __forceinline__ int quad_root_grad(const QuadCtx& X, const QVerts& V,
-                                              unsigned long long packed, unsigned rndm, int nr,
-                                              double& c4, double D[6]) {
-  int u0, u1, u2;
-  const int kk = quad_root_index<R>(X, V, packed, u0, u1, u2);
-  if (kk < 0) return 0;
-  c4 += __ldg(&X.c2[kk]) + (nr == 4 ? __ldg(&X.c3[kk]) : 0.0);
-  const int role[4] = {R, u0, u1, u2};
-#pragma unroll
-  for (int tt = 0; tt < 6; ++tt) {
-    if (!((rndm >> role[term_gate(tt)]) & 1u)) continue;
-    const int u = role[term_pu(tt)], vv = role[term_pv(tt)];
-    const int kt = kk + X.nbin * tt;
-    const bool both = ((rndm >> u) & 1u) && ((rndm >> vv) & 1u);
-    const double cd = __ldg(&X.cN[kt]) + (both ? __ldg(&X.cR[kt]) : 0.0);
-    const int e = qedge(u, vv);
-#pragma unroll
-    for (int ee = 0; ee < 6; ++ee)
-      if (ee == e) D[ee] += cd;
-  }
-  return 1;
-}
-
-// Gradient of the cotangent-weighted sums with respect to the four vertex
-// weights of one clique (g[v] = d/dw_v, vertices as in quad_contrib).  The
-// sums are multilinear: a 4-product contributes its cotangent times the
-// product of the other three weights, a pair term its cotangent times the
-// partner's weight.
-__device__ __forceinline__ int quad_grad(const QuadCtx& X, const QVerts& V, const uint32_t m[6],
-                                         double g[4]) {
-  unsigned long long packed = 0;
-#pragma unroll
-  for (int e = 0; e < 6; ++e) packed |= (unsigned long long)meta_bin(m[e]) << (8 * e);
-  unsigned rndm = 0;
-#pragma unroll
-  for (int k = 0; k < 4; ++k) rndm |= (unsigned)(V.fl[k] & FLAG_RANDOM) << k;
-  const int nr = __popc(rndm);
-  double c4 = 0.0, D[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  const int n = quad_root_grad<0>(X, V, packed, rndm, nr, c4, D) +
-                quad_root_grad<1>(X, V, packed, rndm, nr, c4, D) +
-                quad_root_grad<2>(X, V, packed, rndm, nr, c4, D) +
-                quad_root_grad<3>(X, V, packed, rndm, nr, c4, D);
-  const double w0 = V.w[0], w1 = V.w[1], w2 = V.w[2], w3 = V.w[3];
-  // edges: 0 (0,1) 1 (0,2) 2 (0,3) 3 (1,2) 4 (1,3) 5 (2,3)
-  g[0] = c4 * (w1 * w2 * w3) + D[0] * w1 + D[1] * w2 + D[2] * w3;
-  g[1] = c4 * (w0 * w2 * w3) + D[0] * w0 + D[3] * w2 + D[4] * w3;
-  g[2] = c4 * (w0 * w1 * w3) + D[1] * w0 + D[3] * w1 + D[5] * w3;
-  g[3] = c4 * (w0 * w1 * w2) + D[2] * w0 + D[4] * w1 + D[5] * w2;
-  return n;
-}
-
 // m: bins of (0,1) (0,2) (0,3) (1,2) (1,3) (2,3) for vertices 0 = p, 1 = a,
 // 2 = b, 3 = d.
 template <bool WEIGHTED, bool SHC>
@@ -385,6 +331,73 @@ __device__ __forceinline__ int quad_contrib_c(const QuadCtx& X, const QVerts& V,
   int n = 0;
 #pragma unroll 1
   for (int R = 0; R < 4; ++R) n += quad_root_rt<WEIGHTED, SHC>(X, V, packed, rndm, nr, R, perm, flw);
+  return n;
+}
+
+// Gradient of the cotangent-weighted sums with respect to the four vertex
+// weights of one clique (g[v] = d/dw_v, vertices as in quad_contrib).  The
+// sums are multilinear: a 4-product contributes its cotangent times the
+// product of the other three weights, a pair term its cotangent times the
+// partner's weight.  The valid roots' cotangents are gathered into one
+// 4-product coefficient c4 and one coefficient per clique edge D[e] (edges
+// 0 (0,1) 1 (0,2) 2 (0,3) 3 (1,2) 4 (1,3) 5 (2,3)); the roots are a loop
+// that is not unrolled, as in quad_contrib_c.
+__device__ __forceinline__ int quad_grad_c(const QuadCtx& X, const QVerts& V, const uint32_t m[6],
+                                           double g[4]) {
+  unsigned long long packed = 0;
+#pragma unroll
+  for (int e = 0; e < 6; ++e) packed |= (unsigned long long)meta_bin(m[e]) << (8 * e);
+  unsigned rndm = 0, flw = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    rndm |= (unsigned)(V.fl[k] & FLAG_RANDOM) << k;
+    flw |= (unsigned)V.fl[k] << (8 * k);
+  }
+  const int nr = __popc(rndm);
+  const unsigned perm = id_order(V);
+  double c4 = 0.0, D[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  int n = 0;
+#pragma unroll 1
+  for (int R = 0; R < 4; ++R) {
+    const unsigned fr = flw >> (8 * R);
+    if ((fr & FLAG_BUFFER) || !(fr & kFlagDeg4)) continue;
+    int pos = 0;
+#pragma unroll
+    for (int i = 1; i < 4; ++i)
+      if ((int)((perm >> (2 * i)) & 3u) == R) pos = i;
+    const unsigned lowm = (1u << (2 * pos)) - 1u;
+    const unsigned oth = (perm & lowm) | ((perm >> (2 * pos + 2)) << (2 * pos));
+    const int u0 = (int)(oth & 3u), u1 = (int)((oth >> 2) & 3u), u2 = (int)((oth >> 4) & 3u);
+    const int b1 = qbin(packed, R, u0), b2 = qbin(packed, u0, u1), b3 = qbin(packed, u1, u2),
+              b4 = qbin(packed, R, u2);
+    if (!(b1 <= b2 && b2 <= b3 && b3 <= b4)) continue;
+    const int nb2 = X.nbins + 2;
+    const int cfg = 1 + (X.F[b1] - X.F[1]) + (X.F[nb2 + b2] - X.F[nb2 + b1]) +
+                    (X.F[2 * nb2 + b3] - X.F[2 * nb2 + b2]) + (X.F[3 * nb2 + b4] - X.F[3 * nb2 + b3]);
+    const int d1 = qbin(packed, R, u1), d2 = qbin(packed, u0, u2);
+    const int kk = (cfg - 1) + X.ncfg * ((d1 - 1) + X.nbins * (d2 - 1));
+    ++n;
+    c4 += __ldg(&X.c2[kk]) + (nr == 4 ? __ldg(&X.c3[kk]) : 0.0);
+    const unsigned rp = (unsigned)R | ((unsigned)u0 << 2) | ((unsigned)u1 << 4) | ((unsigned)u2 << 6);
+#pragma unroll
+    for (int tt = 0; tt < 6; ++tt) {
+      const int ga = (int)((rp >> (2 * term_gate(tt))) & 3u);
+      if (!((rndm >> ga) & 1u)) continue;
+      const int u = (int)((rp >> (2 * term_pu(tt))) & 3u), vv = (int)((rp >> (2 * term_pv(tt))) & 3u);
+      const int kt = kk + X.nbin * tt;
+      const bool both = ((rndm >> u) & 1u) && ((rndm >> vv) & 1u);
+      const double cd = __ldg(&X.cN[kt]) + (both ? __ldg(&X.cR[kt]) : 0.0);
+      const int e = qedge(u, vv);
+#pragma unroll
+      for (int ee = 0; ee < 6; ++ee)
+        if (ee == e) D[ee] += cd;
+    }
+  }
+  const double w0 = V.w[0], w1 = V.w[1], w2 = V.w[2], w3 = V.w[3];
+  g[0] = c4 * (w1 * w2 * w3) + D[0] * w1 + D[1] * w2 + D[2] * w3;
+  g[1] = c4 * (w0 * w2 * w3) + D[0] * w0 + D[3] * w2 + D[4] * w3;
+  g[2] = c4 * (w0 * w1 * w3) + D[1] * w0 + D[3] * w1 + D[5] * w3;
+  g[3] = c4 * (w0 * w1 * w2) + D[2] * w0 + D[4] * w1 + D[5] * w2;
   return n;
 }
 
@@ -585,7 +598,7 @@ __global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
         int nroot;
         if (ADJ) {
           double g[4];
-          nroot = quad_grad(X, V, m, g);
+          nroot = quad_grad_c(X, V, m, g);
           if (nroot) {
             fix_acc(racc, g[0], gscale);
             fix_add(&s_glo[x], &s_ghi[x], g[1], gscale);
@@ -739,7 +752,7 @@ void launch_adj4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, con
   const int nw = quad4_warps(Q.nbins, Q.cap, 0, true);
   const size_t smem = quad_layout(Q.nbins, Q.cap, nw, 0, true).total;
   if (smem > kQuadSmemLimit) throw Error{-2, "4PCF adjoint: per-warp shared memory exceeds the SM limit"};
-  auto kfn = quad4_kernel<false, false, true, false>;
+  auto kfn = quad4_kernel<false, false, true, true>;
   GR_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nw * 32, smem));
