@@ -40,10 +40,33 @@ def tri3_roofline(ctx, q_ms, pk):
             "bytes_per_launch": b, "ms_per_launch": ms, "peak_source": pk["source"]}
 
 
-def profiled_traffic(kernel, scale):
+def quad4_bytes(stats):
+    """Algorithmic bytes of one 4-clique-kernel launch.
+
+    Per upper edge (p, a): the root row entry (8 B) and the two row offsets
+    of a (16 B).  Per probe (a record of the row of a, or of the row of an X
+    entry b, read and looked up in the row of p): the record (8 B).  Per
+    rooted 4-clique contribution the (b, d) edge metadata and the far
+    vertex's flags, id and weight: counted as 4 + 13 B.
+    """
+    return 24 * stats["upper_edges"] + 8 * stats["probes"] + 17 * stats["rooted"]
+
+
+def quad4_roofline(ctx, q_ms, pk):
+    st = ctx.stats()
+    ms = sum(q_ms) / len(q_ms)
+    b = quad4_bytes(st)
+    achieved = b / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": "quad4_kernel", "achieved": achieved, "peak": pk["hbm_gbs"],
+            "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "traffic": None,
+            "bytes_per_launch": b, "ms_per_launch": ms, "peak_source": pk["source"]}
+
+
+def profiled_traffic(kernel, scale, workload="c2"):
     """DRAM bytes (read + write) per launch of `kernel` from the committed ncu
-    summary profiles/<kernel>_c2.json, for the full-size workload only."""
-    p = os.path.join(ROOT, "profiles", f"{kernel}_c2.json")
+    summary profiles/<kernel>_<workload>.json, for the full-size workload
+    only."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.json")
     if scale != 1.0 or not os.path.exists(p):
         return None
     try:
