@@ -24,7 +24,8 @@ namespace gr {
 
 namespace {
 
-constexpr int kQuadMaxWarps = 16;  // block size chosen at launch to fit shared memory (128 registers)
+constexpr int kQuadMaxWarps = 16;   // weighted / adjoint kernels (up to 128 registers)
+constexpr int kQuadMaxWarpsU = 24;  // unweighted kernels (up to 85 registers)
 constexpr size_t kQuadSmemLimit = 227 * 1024;
 constexpr int kQQueue = 96;         // hit queue entries per warp (< 32 left + 64 pushed)
 constexpr int kQMaxOffset = 1 << 22;  // hash entries: (label offset << 10) | position
@@ -413,7 +414,7 @@ __device__ __forceinline__ uint32_t qfib_slot(uint32_t off, int lg) {
 // COMPACT: the 4PCF contributions through quad_contrib_c (loops over roots
 // and terms) instead of the unrolled quad_contrib.
 template <bool WEIGHTED, bool SHC, bool ADJ, bool COMPACT>
-__global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
+__global__ void __launch_bounds__((WEIGHTED || ADJ ? kQuadMaxWarps : kQuadMaxWarpsU) * 32) quad4_kernel(
     DevCatalog C, CSRView G, QuadParams Q, unsigned long long* __restrict__ g_cnt,
     unsigned long long* __restrict__ g_fix, unsigned long long* __restrict__ d_cnt,
     unsigned long long* __restrict__ d_fix, int nh, int nd, double fscale, double dscale,
@@ -704,9 +705,9 @@ __global__ void __launch_bounds__(kQuadMaxWarps * 32) quad4_kernel(
   }
 }
 
-// Warps per block: as many as fit in shared memory (at most kQuadMaxWarps).
-int quad4_warps(int nbins, int cap, int ncounts, bool adj = false) {
-  int nw = kQuadMaxWarps;
+// Warps per block: as many as fit in shared memory (at most maxw).
+int quad4_warps(int nbins, int cap, int ncounts, bool adj = false, int maxw = kQuadMaxWarps) {
+  int nw = maxw;
   while (nw > 1 && quad_layout(nbins, cap, nw, ncounts, adj).total > kQuadSmemLimit) nw -= 1;
   return nw;
 }
@@ -722,7 +723,8 @@ bool launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bo
   // for at least 8 warps
   const int ncnt = nh + nd;
   if (weighted || quad4_warps(Q.nbins, Q.cap, ncnt) < 8) shared_counts = false;
-  const int nw = quad4_warps(Q.nbins, Q.cap, shared_counts ? ncnt : 0);
+  const int maxw = weighted ? kQuadMaxWarps : kQuadMaxWarpsU;
+  const int nw = quad4_warps(Q.nbins, Q.cap, shared_counts ? ncnt : 0, false, maxw);
   const size_t smem = quad_layout(Q.nbins, Q.cap, nw, shared_counts ? ncnt : 0).total;
   if (smem > kQuadSmemLimit) throw Error{-2, "4PCF: per-warp shared memory exceeds the SM limit"};
   // weighted: the compact contribution code (the unrolled form of its long
