@@ -693,6 +693,17 @@ int gr_count_2pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
   GR_API_END(c)
 }
 
+// Third-edge test of the triangle kernel: the geometric pair test unless mu
+// bins are on and rows are short (mean upper degree below 24), where
+// re-binning every third edge costs more than the hash probes it saves
+// (measured: 3PCF catalogue with 5 mu bins and upper degree 13.7, 0.78 ms
+// geometric against 0.75 ms; without mu bins 0.56 against 0.64 ms; upper
+// degree 156, 197 against 250 ms with 5 mu bins).
+static int tri_geometric(const gr_ctx* c, int rsd) {
+  if (!rsd) return 1;
+  return c->n > 0 && (double)c->csr.n_edges >= 24.0 * (double)c->n ? 1 : 0;
+}
+
 static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* counts, double* catsum) {
   GR_API_BEGIN(c)
   require_ready(c);
@@ -736,6 +747,8 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
   T.normal = c->normal_dev.p;
   make_rank_tables(T.rank, c->nbins, 3);
   for (int nr = 0; nr < 4; ++nr) T.fscale[nr] = fscale[nr];
+  T.P = c->P;
+  T.geo = tri_geometric(c, T.rsd);
   const CSRView G = c->csr.view();
   cudaEvent_t q0;
   GR_CUDA_TRY(cudaEventCreate(&q0));
@@ -1307,6 +1320,8 @@ int gr_adjoint_3pcf(gr_ctx* c, const double* cot2, const double* cot3, double* g
   T.cap = round_cap(c->csr.max_deg, 32, 256);
   T.normal = c->normal_dev.p;
   make_rank_tables(T.rank, c->nbins, 3);
+  T.P = c->P;
+  T.geo = 1;  // faster for the adjoint at every degree measured
   const CSRView G = c->csr.view();
   std::memset(&c->st, 0, sizeof(c->st));
   launch_adj3(c->index.view(), G, T, c->cot.p, cot3 ? c->cot.p + nc : nullptr, gscale, c->gfix.p,

@@ -42,6 +42,8 @@ struct TriParams {
   const uint8_t* normal;   // device find_normal table [mu1-1 + nmu*(mu2-1)]
   RankTables rank;         // 3-tuple ranks
   double fscale[4];        // fixed-point scale of the products with 0..3 randoms
+  PairParams P;            // edge predicate and binning of the graph
+  int geo;                 // 1: third edges by the geometric pair test, 0: hash probes of rows
 };
 
 // 3PCF: triangles p < a < c enumerated once over the upper CSR; each adds to

@@ -15,6 +15,18 @@
 // Hits (triangles p < a < c) are pushed to a per-warp queue that is drained
 // 32 at a time, so the binning work runs with every lane busy.
 //
+// Geometric mode (TriParams::geo): the third edge (a, c) of a triangle joins
+// two members of R+(p), and it is an edge exactly when the pair passes the
+// graph's own membership test (FP32 squared separation, FP64 inside the
+// guard band).  The warp stages the positions of R+(p) instead of the row
+// starts and the hash table, spreads the k(k-1)/2 pairs of R+(p) over the
+// lanes (closed-form inversion of the triangular pair index) and queues the
+// pairs that pass; the drain bins (a, c) with the graph's binning.  It tests
+// k(k-1)/2 pairs per root instead of the sum of |R+(a)| and reads no other
+// rows, but bins every third edge again: it wins at high degree and without
+// mu bins, the hash mode at low degree with mu bins.  Both give identical
+// results.
+//
 // A triangle contributes to the rooted histogram of each non-buffer vertex r
 // with the bins of its three edges (symmetric bin table), the find_normal mu
 // bin of r's two edges taken in catalogue-id order (k1 < k2 in the
@@ -36,7 +48,7 @@ __host__ __device__ inline size_t align8(size_t x) { return (x + 7) & ~(size_t)7
 struct TriLayout {
   size_t off_cnt, off_lim, off_cot, off_norm, off_rank, off_cfg, off_fsc, off_warp, warp_bytes, total;
   // per-warp sub-offsets
-  size_t o_rs, o_w, o_g, o_col, o_mo, o_len, o_hkey, o_q;
+  size_t o_pos, o_rs, o_w, o_g, o_col, o_mo, o_len, o_hkey, o_q;
 };
 
 // Largest per-root hash table: a power of two >= 4 * cap (load <= 1/4).
@@ -47,10 +59,11 @@ __host__ __device__ inline int hash_lg_max(int cap) {
 }
 
 // adj: the adjoint variant (cotangent tables, per-neighbour gradient
-// accumulators) instead of histograms.
+// accumulators) instead of histograms.  geo: neighbour positions instead of
+// row starts, lengths and the hash table.
 __host__ __device__ inline TriLayout tri_layout(int nh, int nmu, int nbins, int cap, bool shist,
                                                 bool weighted, bool counts, int nwarps,
-                                                bool adj = false) {
+                                                bool adj = false, bool geo = false) {
   TriLayout L;
   size_t o = 0;
   L.off_cnt = o;
@@ -67,18 +80,20 @@ __host__ __device__ inline TriLayout tri_layout(int nh, int nmu, int nbins, int 
   o = align8(o + sizeof(int) * 3 * (size_t)(nbins + 2));
   L.off_cfg = o;  // configuration of every (b1, b2, b3), small nbins only
   if (nbins <= kCfgTableBins) o = align8(o + sizeof(uint16_t) * (size_t)nbins * nbins * nbins);
+  o = (o + 15) & ~(size_t)15;  // float4 positions in the warp areas
   L.off_warp = o;
   const int hs = 1 << hash_lg_max(cap);
   size_t w = 0;
-  L.o_rs = w;   w += (size_t)cap * 8;
+  L.o_pos = w;  if (geo) w += (size_t)cap * 16;  // float4 position per neighbour
+  L.o_rs = w;   if (!geo) w += (size_t)cap * 8;
   L.o_w = w;    if (weighted || adj) w += (size_t)cap * 8;
   L.o_g = w;    if (adj) w += (size_t)cap * 16;  // gradient (lo, hi) per neighbour
   L.o_col = w;  w += (size_t)cap * 4;
   L.o_mo = w;   w += (size_t)cap * 8;  // (catalogue id << 32) | flags << 24 | edge meta
-  L.o_len = w;  w += (size_t)cap * 4;
-  L.o_hkey = w; w += (size_t)hs * 4;
+  L.o_len = w;  if (!geo) w += (size_t)cap * 4;
+  L.o_hkey = w; if (!geo) w += (size_t)hs * 4;
   L.o_q = w;    w += (size_t)kQueue * 8;
-  L.warp_bytes = align8(w);
+  L.warp_bytes = (w + 15) & ~(size_t)15;
   L.total = o + L.warp_bytes * nwarps;
   return L;
 }
@@ -226,7 +241,7 @@ constexpr int kMaxOffset = 1 << 24;
 
 // ADJ: accumulate the weight gradient (g_lo / g_hi, label order) of
 // L = sum cot2 N2 + cot3 N3 instead of the histograms.
-template <bool WEIGHTED, bool COUNTS, bool SHIST, bool ADJ>
+template <bool WEIGHTED, bool COUNTS, bool SHIST, bool ADJ, bool GEO>
 __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, CSRView G, TriParams T,
                                                            unsigned long long* __restrict__ g_cnt,
                                                            unsigned long long* __restrict__ g_lim,
@@ -240,7 +255,7 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
   extern __shared__ __align__(16) unsigned char smem[];
   const int nh = T.ncfg * T.nmu * 4;
   const TriLayout L =
-      tri_layout(nh, T.nmu, T.nbins, T.cap, SHIST, WEIGHTED, COUNTS, blockDim.x >> 5, ADJ);
+      tri_layout(nh, T.nmu, T.nbins, T.cap, SHIST, WEIGHTED, COUNTS, blockDim.x >> 5, ADJ, GEO);
   TriCtx X;
   X.nbins = T.nbins;
   X.nmu = T.nmu;
@@ -297,6 +312,7 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   unsigned char* wb = smem + L.off_warp + L.warp_bytes * (threadIdx.x >> 5);
+  float4* s_pos = reinterpret_cast<float4*>(wb + L.o_pos);
   long long* s_rs = reinterpret_cast<long long*>(wb + L.o_rs);
   double* s_w = reinterpret_cast<double*>(wb + L.o_w);
   int* s_col = reinterpret_cast<int*>(wb + L.o_col);
@@ -315,7 +331,14 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
   auto drain_one = [&](int e, uint8_t fp, int op, double wp, Fix128& racc) -> int {
     const unsigned long long qe = s_q[e];
     const int qx = (int)(qe & 0xffu), qy = (int)((qe >> 8) & 0xffu);
-    const uint32_t mac = (uint32_t)(qe >> 32);
+    uint32_t mac = (uint32_t)(qe >> 32);
+    if (GEO) {
+      // bins of the edge (a, c) exactly as the graph build computes them
+      int b = 1, mf = 1, mr = 1;
+      const int r = T.P.f32 ? classify_f32<true>(s_pos[qx], s_pos[qy], T.P, b, mf, mr) : 2;
+      if (r == 2) edge_f64(C.posd[s_col[qx]], C.posd[s_col[qy]], T.P, b, mf, mr);
+      mac = pack_meta(b, mf, mr);
+    }
     const unsigned long long moa = s_mo[qx], moc = s_mo[qy];
     const uint32_t ma = (uint32_t)moa, mc = (uint32_t)moc;
     const int oa = (int)(moa >> 32), oc = (int)(moc >> 32);
@@ -342,13 +365,14 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
       const double wp = (WEIGHTED || ADJ) ? C.w[p] : 0.0;
       Fix128 racc = {0ull, 0ull};
       // rows are sorted: the last entry has the largest label offset
-      if (k <= T.cap && rec_col(G.rec[b0 + k - 1]) - p < kMaxOffset) {
+      if (k <= T.cap && (GEO || rec_col(G.rec[b0 + k - 1]) - p < kMaxOffset)) {
         // per-root table: >= 8 slots per entry, at most the capacity's table
         int lg = 6;
         while (lg < lg_max && (1 << lg) < 8 * k) ++lg;
         const int hs = 1 << lg;
         __syncwarp();
-        for (int h = lane; h < hs; h += 32) s_hkey[h] = 0u;
+        if (!GEO)
+          for (int h = lane; h < hs; h += 32) s_hkey[h] = 0u;
         __syncwarp();
         // stage R+(p) and the data of its vertices; insert into the hash table
         for (int xb = 0; xb < k; xb += 32) {
@@ -357,11 +381,15 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
             const unsigned long long r = G.rec[b0 + x];
             const int a = rec_col(r);
             s_col[x] = a;
-            const long long rs = G.start[a];
-            const int len = G.len[a];
-            s_rs[x] = rs;
-            s_len[x] = len;
-            probes += (unsigned long long)len;
+            if (GEO) {
+              s_pos[x] = C.pos4[a];
+            } else {
+              const long long rs = G.start[a];
+              const int len = G.len[a];
+              s_rs[x] = rs;
+              s_len[x] = len;
+              probes += (unsigned long long)len;
+            }
             // the vertex flags ride in the top byte of the edge meta word
             s_mo[x] = ((unsigned long long)(uint32_t)C.orig[a] << 32) |
                       (rec_meta(r) | ((uint32_t)C.flags[a] << 24));
@@ -370,17 +398,57 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
               s_glo[x] = 0ull;
               s_ghi[x] = 0ull;
             }
-            const uint32_t off = (uint32_t)(a - p);
-            const uint32_t key = (off << 8) | (uint32_t)x;
-            uint32_t h = fib_slot(off, lg);
-            for (int t = 0; t < hs; ++t) {
-              if (atomicCAS(&s_hkey[h], 0u, key) == 0u) break;
-              h = (h + 1) & (uint32_t)(hs - 1);
+            if (!GEO) {
+              const uint32_t off = (uint32_t)(a - p);
+              const uint32_t key = (off << 8) | (uint32_t)x;
+              uint32_t h = fib_slot(off, lg);
+              for (int t = 0; t < hs; ++t) {
+                if (atomicCAS(&s_hkey[h], 0u, key) == 0u) break;
+                h = (h + 1) & (uint32_t)(hs - 1);
+              }
             }
           }
         }
         __syncwarp();
         int qn = 0;
+        if (GEO) {
+          // every pair (x, y), x < y, of R+(p) over the lanes: (a, c) is an
+          // edge when the pair passes the graph's own membership test
+          const int npair = k * (k - 1) / 2;
+          const int k2m1 = 2 * k - 1;
+          if (lane == 0) probes += (unsigned long long)npair;
+          for (int t0 = 0; t0 < npair; t0 += 32) {
+            const int t = t0 + lane;
+            bool hit = false;
+            int x = 0, y = 0;
+            if (t < npair) {
+              // x: the largest row with x (2k - 1 - x) / 2 <= t pairs before it
+              const float disc = (float)(k2m1 * k2m1) - 8.0f * (float)t;
+              x = (int)(0.5f * ((float)k2m1 - sqrtf(fmaxf(disc, 0.0f))));
+              x = max(0, min(x, k - 2));
+              if ((x + 1) * (k2m1 - x - 1) / 2 <= t) ++x;
+              if (x * (k2m1 - x) / 2 > t) --x;
+              y = t - x * (k2m1 - x) / 2 + x + 1;
+              int r = T.P.f32 ? member_f32(s_pos[x], s_pos[y], T.P) : 2;
+              if (r == 2) {
+                int b, mf, mr;
+                r = edge_f64(C.posd[s_col[x]], C.posd[s_col[y]], T.P, b, mf, mr) ? 1 : 0;
+              }
+              hit = r == 1;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (hit) s_q[qn + __popc(m & lt)] = (unsigned long long)(x | (y << 8));
+            qn += __popc(m);
+            if (qn >= 32) {
+              __syncwarp();
+              const int nroot = drain_one(qn - 32 + lane, fp, op, wp, racc);
+              tris += nroot > 0;
+              rooted += nroot;
+              qn -= 32;
+              __syncwarp();
+            }
+          }
+        } else
         // rows in batches of 32; the batch's non-empty rows are compacted
         // onto the lanes, their work items (a, c in R+(a)) flattened and
         // spread over the lanes 32 at a time.  A lane finds the row of its
@@ -553,14 +621,17 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
 }  // namespace
 
 // Warps per block: as many as fit in shared memory (at most 32).
-static int tri3_warps(const TriParams& T, bool weighted, bool counts, bool shist, bool adj = false) {
+static int tri3_warps(const TriParams& T, bool weighted, bool counts, bool shist, bool adj = false,
+                      bool geo = false) {
   const int nh = T.ncfg * T.nmu * 4;
   int nw = kTriMaxWarps;
   while (nw > 1 &&
-         tri_layout(nh, T.nmu, T.nbins, T.cap, shist, weighted, counts, nw, adj).total > kSmemLimit)
+         tri_layout(nh, T.nmu, T.nbins, T.cap, shist, weighted, counts, nw, adj, geo).total >
+             kSmemLimit)
     nw -= 1;
   return nw;
 }
+
 
 static bool tri3_shist(int nh, bool weighted, bool counts) {
   return (size_t)nh * 8 * ((counts ? 1 : 0) + (weighted ? 2 : 0)) <= kMaxHistSmem;
@@ -581,13 +652,15 @@ void launch_tri3(const DevCatalog& C, const CSRView& G, const TriParams& T, bool
   if (!weighted) counts = true;
   const int nh = T.ncfg * T.nmu * 4;
   const bool shist = tri3_shist(nh, weighted, counts);
-  const int nw = tri3_warps(T, weighted, counts, shist);
-  const size_t smem = tri_layout(nh, T.nmu, T.nbins, T.cap, shist, weighted, counts, nw).total;
+  const bool geo = T.geo != 0;
+  const int nw = tri3_warps(T, weighted, counts, shist, false, geo);
+  const size_t smem =
+      tri_layout(nh, T.nmu, T.nbins, T.cap, shist, weighted, counts, nw, false, geo).total;
   if (smem > kSmemLimit) throw Error{-2, "3PCF: per-warp shared memory exceeds the SM limit"};
   GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));
 #define GR_TRI_LAUNCH(W, K, S)                                                                \
   do {                                                                                        \
-    auto kfn = tri3_kernel<W, K, S, false>;                                                   \
+    auto kfn = geo ? tri3_kernel<W, K, S, false, true> : tri3_kernel<W, K, S, false, false>;  \
     GR_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
                                      (int)smem));                                             \
     int per_sm = 0;                                                                           \
@@ -615,11 +688,14 @@ void launch_adj3(const DevCatalog& C, const CSRView& G, const TriParams& T, cons
                  unsigned long long* g_hi, unsigned long long* stats, int* work, cudaStream_t s) {
   if (C.n <= 0) return;
   const int nh = T.ncfg * T.nmu * 4;
-  const int nw = tri3_warps(T, false, false, false, true);
-  const size_t smem = tri_layout(nh, T.nmu, T.nbins, T.cap, false, false, false, nw, true).total;
+  const bool geo = T.geo != 0;
+  const int nw = tri3_warps(T, false, false, false, true, geo);
+  const size_t smem =
+      tri_layout(nh, T.nmu, T.nbins, T.cap, false, false, false, nw, true, geo).total;
   if (smem > kSmemLimit) throw Error{-2, "3PCF adjoint: shared memory exceeds the SM limit"};
   GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));
-  auto kfn = tri3_kernel<false, false, false, true>;
+  auto kfn = geo ? tri3_kernel<false, false, false, true, true>
+                 : tri3_kernel<false, false, false, true, false>;
   GR_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nw * 32, smem));

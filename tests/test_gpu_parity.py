@@ -84,6 +84,27 @@ def test_3pcf_c2(gpu_ctx, oracle, precision):
     gpu_ctx.set_precision("f32")
 
 
+@pytest.mark.parametrize("name,scale,nmu,precision", [
+    ("c2_3pcf", 0.02, 1, "f32"),          # geometric third-edge test (no mu bins)
+    ("c2_3pcf", 0.02, 1, "f64"),
+    ("c2_3pcf", 0.02, 5, "f32"),          # hash probes (mu bins, short rows)
+    ("c5_adjoint_3pcf", 0.002, 5, "f32"),  # geometric with mu bins (long rows)
+    ("c5_adjoint_3pcf", 0.002, 5, "f64")])
+def test_3pcf_third_edge_modes(gpu_ctx, oracle, name, scale, nmu, precision):
+    """Both ways of finding the third edge of a triangle (a hash probe of the
+    rows, or the graph's membership test on the pair) give the oracle's
+    counts and sums."""
+    cat, w, sp = _cat(name, scale)
+    gpu_ctx.set_precision(precision)
+    gpu_ctx.set_catalog(cat.xyz, w, cat.n_data)
+    gpu_ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], nmu)
+    got = gpu_ctx.count_3pcf()
+    ref = oracle.Graph(cat.xyz, sp["rmin"], sp["rmax"], sp["nbins"], nmu).pcf3(w, cat.n_data)
+    _check_sums(got, ref)
+    assert gpu_ctx.stats()["rooted"] == int(ref["counts"].sum()) > 0
+    gpu_ctx.set_precision("f32")
+
+
 def test_3pcf_unit_weights(gpu_ctx, oracle):
     cat, w, sp = _cat("c5_adjoint_3pcf", 0.002)
     w = catalogs.normalise(np.ones(cat.n), cat.n_data, cat.n_rand)
