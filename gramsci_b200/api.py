@@ -246,6 +246,14 @@ class Context:
                                               _ptr(g)))
         return g
 
+    def set_clique_mode(self, mode):
+        """How the 3PCF / 4PCF kernels find the edges among a root's
+        larger-label neighbours: "auto", "hash" (probes of the neighbours'
+        rows) or "geometric" (the graph's membership test on the pairs).
+        Results are identical."""
+        v = {"auto": 0, "hash": 1, "geometric": 2}[mode]
+        self._check(self._lib.gr_set_option(self._h, 5, v))
+
     def set_keep_graph(self, on):
         """Reuse the last call's graph until the catalogue, bins or precision change."""
         self._check(self._lib.gr_set_option(self._h, 4, int(bool(on))))

@@ -45,6 +45,7 @@ struct gr_ctx {
   CellIndex index;
   UpperCSR csr;
   bool csr_valid = false;
+  int clique_mode = 0;  // GR_OPT_CLIQUE_MODE
   bool keep_graph = false;    // GR_OPT_KEEP_GRAPH
   bool graph_loaded = false;  // graph read by gr_graph_load
   PairParams P{};
@@ -566,6 +567,9 @@ int gr_set_option(gr_ctx* c, int32_t key, int64_t value) {
   } else if (key == GR_OPT_AUTOTUNE) {
     if (value < 0 || value > 1 + kPairVariants) return set_err(c, GR_E_ARG, "autotune must be 0, 1 or 2+variant");
     c->autotune = (int)value;
+  } else if (key == GR_OPT_CLIQUE_MODE) {
+    if (value < 0 || value > 2) return set_err(c, GR_E_ARG, "clique mode must be 0, 1 or 2");
+    c->clique_mode = (int)value;
   } else if (key == GR_OPT_TIMEOUT_MS) {
     if (value <= 0) return set_err(c, GR_E_ARG, "timeout must be positive");
     c->timeout_ms = value;
@@ -700,6 +704,7 @@ int gr_count_2pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
 // geometric against 0.75 ms; without mu bins 0.56 against 0.64 ms; upper
 // degree 156, 197 against 250 ms with 5 mu bins).
 static int tri_geometric(const gr_ctx* c, int rsd) {
+  if (c->clique_mode != 0) return c->clique_mode == 2 ? 1 : 0;
   if (!rsd) return 1;
   return c->n > 0 && (double)c->csr.n_edges >= 24.0 * (double)c->n ? 1 : 0;
 }
@@ -809,6 +814,16 @@ int gr_count_equi(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
   return count_tri(c, true, N2, N3, counts, catsum);
 }
 
+// Edges among R+(p) in the 4-clique kernels: the geometric pair test (rows
+// up to 256 members) or hash probes of the members' rows.  Measured on the
+// 4PCF workload (upper degree 17.5): unit weights 5.0 ms geometric against
+// 7.0 ms, adjoint 13.0 against 15.3 ms, but lognormal weights 24.9 against
+// 22.8 ms, so weighted sums keep the hash probes.
+static int quad_geometric(const gr_ctx* c, int cap, int nbins, bool weighted_sums) {
+  if (cap > 256 || nbins > 255 || c->clique_mode == 1) return 0;
+  return c->clique_mode == 2 || !weighted_sums ? 1 : 0;
+}
+
 static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* discN, double* discR,
                       int64_t* counts, double* catsum, int64_t* dcount, double* dsum) {
   GR_API_BEGIN(c)
@@ -856,6 +871,8 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   Q.tetra = tetra ? 1 : 0;
   Q.cap = round_cap((int64_t)gst[2], 32, 1024);
   make_rank_tables(Q.rank, nb, 4);
+  Q.P = c->P;
+  Q.geo = quad_geometric(c, Q.cap, nb, weighted);
   const CSRView G = c->csr.view();
   cudaEvent_t q0;
   GR_CUDA_TRY(cudaEventCreate(&q0));
@@ -1321,7 +1338,7 @@ int gr_adjoint_3pcf(gr_ctx* c, const double* cot2, const double* cot3, double* g
   T.normal = c->normal_dev.p;
   make_rank_tables(T.rank, c->nbins, 3);
   T.P = c->P;
-  T.geo = 1;  // faster for the adjoint at every degree measured
+  T.geo = c->clique_mode == 1 ? 0 : 1;  // faster for the adjoint at every degree measured
   const CSRView G = c->csr.view();
   std::memset(&c->st, 0, sizeof(c->st));
   launch_adj3(c->index.view(), G, T, c->cot.p, cot3 ? c->cot.p + nc : nullptr, gscale, c->gfix.p,
@@ -1383,6 +1400,8 @@ int gr_adjoint_4pcf(gr_ctx* c, const double* cot2, const double* cot3, const dou
   Q.tetra = 0;
   Q.cap = round_cap(c->csr.max_deg, 32, 1024);
   make_rank_tables(Q.rank, nb, 4);
+  Q.P = c->P;
+  Q.geo = quad_geometric(c, Q.cap, nb, false);
   std::memset(&c->st, 0, sizeof(c->st));
   launch_adj4(c->index.view(), c->csr.view(), Q, c->cot.p, gscale, c->gfix.p, c->gfix.p + n,
               c->stats.p, c->work.p, s);

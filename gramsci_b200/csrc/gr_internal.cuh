@@ -200,6 +200,27 @@ __device__ __forceinline__ int member_f32(const float4 pi, const float4 pj, cons
   return 2;
 }
 
+// Radial bin of a pair already known to be an edge of the graph, exactly as
+// the graph build bins it: the FP32 bin outside the guard band around the bin
+// edges (where it equals the FP64 one), else the FP64 reference arithmetic.
+// a < c are the internal labels, pa / pc their FP32 positions.
+__device__ __forceinline__ int edge_rbin(const double4* __restrict__ posd, const PairParams& P,
+                                         int a, int c, const float4 pa, const float4 pc) {
+  if (P.f32) {
+    const float dx = pc.x - pa.x;
+    const float dy = pc.y - pa.y;
+    const float dz = pc.z - pa.z;
+    const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    const float d = __fsqrt_rn(d2);
+    const float t = (d - P.f_rmin) * P.f_inv_dr;
+    const float tn = rintf(t);
+    if (fabsf(t - tn) >= P.tguard && t > 0.0f && t < (float)P.nbins) return (int)t + 1;
+  }
+  int b = 1, mf = 1, mr = 1;
+  edge_f64(posd[a], posd[c], P, b, mf, mr);
+  return b;
+}
+
 // ---------------------------------------------------------------- cell grid --
 struct GridParams {
   int nx, ny, nz;

@@ -77,6 +77,8 @@ struct QuadParams {
   int tetra;  // -tetra: only 4-cliques with six equal bins (histograms by bin)
   int cap;
   RankTables rank;  // 4-tuple ranks
+  PairParams P;     // edge predicate and binning of the graph
+  int geo;          // 1: edges among R+(p) by the geometric pair test (cap <= 256)
 };
 
 // -tetra histograms (tetra = 1): g_cnt nbins*5, d_cnt nbins*30 (6 terms x 5

@@ -18,6 +18,11 @@
 // (k1 < k2 < k3 of the reference), if the perimeter r-k1-k2-k3-r is
 // canonical (bintable entry > 0), to N2 / N3 at (cfg, bin(r,k2), bin(k1,k3))
 // and to the six disconnected pair terms.
+//
+// A second kernel (quad4g_kernel, the geometric mode) finds the edges among
+// the members of R+(p) with the graph's own membership test on their
+// positions instead of probing the members' rows; it is used for unweighted
+// counts and the adjoint (rows up to 256 members).
 #include "gr_kernels.cuh"
 
 namespace gr {
@@ -406,6 +411,69 @@ __device__ __forceinline__ uint32_t qfib_slot(uint32_t off, int lg) {
   return (off * 2654435769u) >> (32 - lg);
 }
 
+// Block-level context shared by the 4-clique kernels: rank tables in shared
+// memory, output pointers, block-private counters (SHC), cotangents (ADJ).
+template <bool SHC, bool ADJ>
+__device__ __forceinline__ void quad_setup(QuadCtx& X, const QuadParams& Q, unsigned char* rank_smem,
+                                           unsigned char* cnt_smem, unsigned long long* g_cnt,
+                                           unsigned long long* g_fix, unsigned long long* d_cnt,
+                                           unsigned long long* d_fix, int nh, int nd,
+                                           double fscale, double dscale, const double* cot) {
+  int* s_F = reinterpret_cast<int*>(rank_smem);
+  const int nb2 = Q.nbins + 2;
+  for (int k = threadIdx.x; k < 4 * nb2; k += blockDim.x) s_F[k] = Q.rank.F[k / nb2][k % nb2];
+  __syncthreads();
+  X.F = s_F;
+  X.nbins = Q.nbins;
+  X.ncfg = Q.ncfg;
+  X.nbin = Q.tetra ? Q.nbins : Q.ncfg * Q.nbins * Q.nbins;
+  X.tetra = Q.tetra;
+  X.cnt = g_cnt;
+  X.dcnt = d_cnt;
+  X.fix = g_fix;
+  X.dfix = d_fix;
+  X.dhi = nd;
+  X.scnt = nullptr;
+  X.sdcnt = nullptr;
+  if (SHC) {
+    unsigned int* sc = reinterpret_cast<unsigned int*>(cnt_smem);
+    for (int k = threadIdx.x; k < nh + nd; k += blockDim.x) sc[k] = 0u;
+    __syncthreads();
+    X.scnt = sc;
+    X.sdcnt = sc + nh;
+  }
+  X.fscale = fscale;
+  X.dscale = dscale;
+  X.c2 = cot;
+  X.c3 = ADJ ? cot + X.nbin : nullptr;
+  X.cN = ADJ ? cot + 2 * (size_t)X.nbin : nullptr;
+  X.cR = ADJ ? cot + 8 * (size_t)X.nbin : nullptr;
+}
+
+// One 4-clique (p, a, b, d) = vertices 0..3 with edge metas m: its
+// contributions to the histograms, or (ADJ) its weight gradient: the root's
+// to racc, those of a, b, d to the per-neighbour accumulators at positions
+// ya, yb, yd.  Returns the number of rooted contributions.
+template <bool WEIGHTED, bool SHC, bool ADJ, bool COMPACT>
+__device__ __forceinline__ int quad_emit(const QuadCtx& X, const QVerts& V, const uint32_t m[6],
+                                         double gscale, Fix128& racc, unsigned long long* s_glo,
+                                         unsigned long long* s_ghi, int ya, int yb, int yd) {
+  if (ADJ) {
+    double g[4];
+    const int nroot = quad_grad_c(X, V, m, g);
+    if (nroot) {
+      fix_acc(racc, g[0], gscale);
+      fix_add(&s_glo[ya], &s_ghi[ya], g[1], gscale);
+      fix_add(&s_glo[yb], &s_ghi[yb], g[2], gscale);
+      fix_add(&s_glo[yd], &s_ghi[yd], g[3], gscale);
+    }
+    return nroot;
+  }
+  return X.tetra ? tetra_contrib<WEIGHTED, SHC>(X, V, m)
+                 : (COMPACT ? quad_contrib_c<WEIGHTED, SHC>(X, V, m)
+                            : quad_contrib<WEIGHTED, SHC>(X, V, m));
+}
+
 // SHC: unweighted counts in block-private 32-bit shared-memory counters,
 // added to the global histograms at the end of the block.
 // ADJ: instead of the histograms, the weight gradient (g_lo / g_hi, label
@@ -424,36 +492,9 @@ __global__ void __launch_bounds__((WEIGHTED || ADJ ? kQuadMaxWarps : kQuadMaxWar
   constexpr bool LW = WEIGHTED || ADJ;  // weights staged
   extern __shared__ __align__(16) unsigned char smem[];
   const QuadLayout L = quad_layout(Q.nbins, Q.cap, blockDim.x >> 5, SHC ? nh + nd : 0, ADJ);
-  int* s_F = reinterpret_cast<int*>(smem + L.off_rank);
-  const int nb2 = Q.nbins + 2;
-  for (int k = threadIdx.x; k < 4 * nb2; k += blockDim.x) s_F[k] = Q.rank.F[k / nb2][k % nb2];
-  __syncthreads();
   QuadCtx X;
-  X.F = s_F;
-  X.nbins = Q.nbins;
-  X.ncfg = Q.ncfg;
-  X.nbin = Q.tetra ? Q.nbins : Q.ncfg * Q.nbins * Q.nbins;
-  X.tetra = Q.tetra;
-  X.cnt = g_cnt;
-  X.dcnt = d_cnt;
-  X.fix = g_fix;
-  X.dfix = d_fix;
-  X.dhi = nd;
-  X.scnt = nullptr;
-  X.sdcnt = nullptr;
-  if (SHC) {
-    unsigned int* sc = reinterpret_cast<unsigned int*>(smem + L.off_cnt);
-    for (int k = threadIdx.x; k < nh + nd; k += blockDim.x) sc[k] = 0u;
-    __syncthreads();
-    X.scnt = sc;
-    X.sdcnt = sc + nh;
-  }
-  X.fscale = fscale;
-  X.dscale = dscale;
-  X.c2 = cot;
-  X.c3 = ADJ ? cot + X.nbin : nullptr;
-  X.cN = ADJ ? cot + 2 * (size_t)X.nbin : nullptr;
-  X.cR = ADJ ? cot + 8 * (size_t)X.nbin : nullptr;
+  quad_setup<SHC, ADJ>(X, Q, smem + L.off_rank, smem + L.off_cnt, g_cnt, g_fix, d_cnt, d_fix, nh,
+                       nd, fscale, dscale, cot);
 
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
@@ -596,21 +637,8 @@ __global__ void __launch_bounds__((WEIGHTED || ADJ ? kQuadMaxWarps : kQuadMaxWar
         // m: (p,a) (p,b) (p,d) (a,b) (a,d) (b,d)
         const uint32_t m[6] = {(uint32_t)mpa_w & 0xffffffu, (uint32_t)mpb_w & 0xffffffu,
                                (uint32_t)mpd_w & 0xffffffu, s_xm[z], s_xm[s_xz[yd]], mbd};
-        int nroot;
-        if (ADJ) {
-          double g[4];
-          nroot = quad_grad_c(X, V, m, g);
-          if (nroot) {
-            fix_acc(racc, g[0], gscale);
-            fix_add(&s_glo[x], &s_ghi[x], g[1], gscale);
-            fix_add(&s_glo[yb], &s_ghi[yb], g[2], gscale);
-            fix_add(&s_glo[yd], &s_ghi[yd], g[3], gscale);
-          }
-        } else {
-          nroot = X.tetra ? tetra_contrib<WEIGHTED, SHC>(X, V, m)
-                          : (COMPACT ? quad_contrib_c<WEIGHTED, SHC>(X, V, m)
-                                     : quad_contrib<WEIGHTED, SHC>(X, V, m));
-        }
+        const int nroot =
+            quad_emit<WEIGHTED, SHC, ADJ, COMPACT>(X, V, m, gscale, racc, s_glo, s_ghi, x, yb, yd);
         quads += nroot > 0;
         rooted += nroot;
       };
@@ -705,6 +733,257 @@ __global__ void __launch_bounds__((WEIGHTED || ADJ ? kQuadMaxWarps : kQuadMaxWar
   }
 }
 
+// Geometric mode.  The edges among the members of R+(p) are exactly the
+// pairs that pass the graph's membership test, so the warp tests the
+// k(k-1)/2 pairs of R+(p) once (closed-form inversion of the triangular pair
+// index over the lanes) and records them as one adjacency bitmask row per
+// member (bits of the later members).  The 4-cliques p < a < b < d are then
+// the set bits d of row(a) AND row(b) for every edge (a, b): the edges are
+// queued 32 at a time, each lane ANDs its two rows word by word and emits one
+// clique per set bit into the clique queue.  The bins of (a, b), (a, d) and
+// (b, d) are computed from the positions as the graph build computes them
+// (edge_rbin), the bin of (a, b) once per edge.  No row other than R+(p) is
+// read; the tests are k(k-1)/2 per root instead of the sum over R+(p) of the
+// members' row lengths.  Rows up to 256 members (8-bit positions).
+constexpr int kQEdgeQueue = 64;  // edge queue entries per warp (< 32 left + 32 pushed)
+
+struct QuadGLayout {
+  size_t off_rank, off_cnt, off_warp, warp_bytes, total;
+  size_t o_pos, o_w, o_mo, o_g, o_col, o_adj, o_q, o_eq;
+};
+
+__host__ __device__ inline QuadGLayout quadg_layout(int nbins, int cap, int nwarps, int ncounts,
+                                                    bool adj, bool lw) {
+  QuadGLayout L;
+  size_t o = 0;
+  L.off_rank = o;
+  o = qalign8(o + sizeof(int) * 4 * (size_t)(nbins + 2));
+  L.off_cnt = o;
+  o = o + sizeof(unsigned int) * (size_t)ncounts;
+  o = (o + 15) & ~(size_t)15;
+  L.off_warp = o;
+  const size_t nwd = (size_t)(cap + 31) / 32;
+  size_t w = 0;
+  L.o_pos = w;  w += (size_t)cap * 16;              // float4 position of each member
+  L.o_w = w;    w += lw ? (size_t)cap * 8 : 0;      // weight
+  L.o_mo = w;   w += (size_t)cap * 8;               // (catalogue id << 32) | flags << 24 | meta(p, a)
+  L.o_g = w;    w += adj ? (size_t)cap * 16 : 0;    // gradient (lo, hi)
+  L.o_col = w;  w += (size_t)cap * 4;               // label
+  L.o_adj = w;  w += (size_t)cap * nwd * 4;         // adjacency rows
+  L.o_q = w;    w += (size_t)kQQueue * 4;           // cliques: a | b << 8 | d << 16 | bin(a,b) << 24
+  L.o_eq = w;   w += (size_t)kQEdgeQueue * 4;       // edges: a | b << 8
+  L.warp_bytes = (w + 15) & ~(size_t)15;
+  L.total = o + L.warp_bytes * nwarps;
+  return L;
+}
+
+template <bool WEIGHTED, bool SHC, bool ADJ, bool COMPACT>
+__global__ void __launch_bounds__((WEIGHTED || ADJ ? kQuadMaxWarps : kQuadMaxWarpsU) * 32) quad4g_kernel(
+    DevCatalog C, CSRView G, QuadParams Q, unsigned long long* __restrict__ g_cnt,
+    unsigned long long* __restrict__ g_fix, unsigned long long* __restrict__ d_cnt,
+    unsigned long long* __restrict__ d_fix, int nh, int nd, double fscale, double dscale,
+    unsigned long long* __restrict__ stats, int* __restrict__ work,
+    const double* __restrict__ cot, double gscale, unsigned long long* __restrict__ g_lo,
+    unsigned long long* __restrict__ g_hi) {
+  constexpr bool LW = WEIGHTED || ADJ;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const QuadGLayout L = quadg_layout(Q.nbins, Q.cap, blockDim.x >> 5, SHC ? nh + nd : 0, ADJ, LW);
+  QuadCtx X;
+  quad_setup<SHC, ADJ>(X, Q, smem + L.off_rank, smem + L.off_cnt, g_cnt, g_fix, d_cnt, d_fix, nh,
+                       nd, fscale, dscale, cot);
+  const PairParams& P = Q.P;
+
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  unsigned char* wb = smem + L.off_warp + L.warp_bytes * (threadIdx.x >> 5);
+  float4* s_pos = reinterpret_cast<float4*>(wb + L.o_pos);
+  double* s_w = reinterpret_cast<double*>(wb + L.o_w);
+  unsigned long long* s_mo = reinterpret_cast<unsigned long long*>(wb + L.o_mo);
+  unsigned long long* s_glo = reinterpret_cast<unsigned long long*>(wb + L.o_g);
+  unsigned long long* s_ghi = s_glo + Q.cap;
+  int* s_col = reinterpret_cast<int*>(wb + L.o_col);
+  uint32_t* s_adj = reinterpret_cast<uint32_t*>(wb + L.o_adj);
+  uint32_t* s_q = reinterpret_cast<uint32_t*>(wb + L.o_q);
+  uint32_t* s_eq = reinterpret_cast<uint32_t*>(wb + L.o_eq);
+  unsigned long long quads = 0, rooted = 0, probes = 0;
+
+  for (;;) {
+    int p = 0;
+    if (lane == 0) p = atomicAdd(work, 1);
+    p = __shfl_sync(0xffffffffu, p, 0);
+    if (p >= C.n) break;
+    const int64_t b0 = G.start[p];
+    const int k = G.len[p];
+    if (k < 3 || k > Q.cap) continue;  // rows longer than cap are rejected on the host
+    const uint8_t fp = C.flags[p] | (G.deg_full[p] > 3 ? kFlagDeg4 : 0);
+    const int op = C.orig[p];
+    const double wp = LW ? C.w[p] : 0.0;
+    Fix128 racc = {0ull, 0ull};
+    const int nwk = (k + 31) >> 5;  // adjacency words per row for this root
+    __syncwarp();
+    for (int x = lane; x < k; x += 32) {
+      const unsigned long long r = G.rec[b0 + x];
+      const int a = rec_col(r);
+      s_col[x] = a;
+      s_pos[x] = C.pos4[a];
+      const uint8_t fa = C.flags[a] | (G.deg_full[a] > 3 ? kFlagDeg4 : 0);
+      s_mo[x] = ((unsigned long long)(uint32_t)C.orig[a] << 32) | (rec_meta(r) | ((uint32_t)fa << 24));
+      if (LW) s_w[x] = C.w[a];
+      if (ADJ) {
+        s_glo[x] = 0ull;
+        s_ghi[x] = 0ull;
+      }
+    }
+    for (int i = lane; i < k * nwk; i += 32) s_adj[i] = 0u;
+    __syncwarp();
+    // pass 1: adjacency among the members of R+(p)
+    const int npair = k * (k - 1) / 2;
+    const int k2m1 = 2 * k - 1;
+    if (lane == 0) probes += (unsigned long long)npair;
+    auto pair_of = [&](int t, int& x, int& y) {
+      // x: the largest row with x (2k - 1 - x) / 2 <= t pairs before it
+      const float disc = (float)(k2m1 * k2m1) - 8.0f * (float)t;
+      x = (int)(0.5f * ((float)k2m1 - sqrtf(fmaxf(disc, 0.0f))));
+      x = max(0, min(x, k - 2));
+      if ((x + 1) * (k2m1 - x - 1) / 2 <= t) ++x;
+      if (x * (k2m1 - x) / 2 > t) --x;
+      y = t - x * (k2m1 - x) / 2 + x + 1;
+    };
+    for (int t = lane; t < npair; t += 32) {
+      int x, y;
+      pair_of(t, x, y);
+      int r = P.f32 ? member_f32(s_pos[x], s_pos[y], P) : 2;
+      if (r == 2) {
+        int b, mf, mr;
+        r = edge_f64(C.posd[s_col[x]], C.posd[s_col[y]], P, b, mf, mr) ? 1 : 0;
+      }
+      if (r == 1) atomicOr(&s_adj[x * nwk + (y >> 5)], 1u << (y & 31));
+    }
+    __syncwarp();
+    int qn = 0, en = 0;
+    // one queued clique: (p, a = member x, b = member y, d = member z)
+    auto drain_one = [&](int e) {
+      const uint32_t qe = s_q[e];
+      const int x = (int)(qe & 0xffu), y = (int)((qe >> 8) & 0xffu), z = (int)((qe >> 16) & 0xffu);
+      const int bxy = (int)(qe >> 24);
+      const int bxz = edge_rbin(C.posd, P, s_col[x], s_col[z], s_pos[x], s_pos[z]);
+      const int byz = edge_rbin(C.posd, P, s_col[y], s_col[z], s_pos[y], s_pos[z]);
+      const unsigned long long ma = s_mo[x], mb = s_mo[y], md = s_mo[z];
+      QVerts V;
+      V.fl[0] = fp;
+      V.fl[1] = (uint8_t)((uint32_t)ma >> 24);
+      V.fl[2] = (uint8_t)((uint32_t)mb >> 24);
+      V.fl[3] = (uint8_t)((uint32_t)md >> 24);
+      V.og[0] = op;
+      V.og[1] = (int)(ma >> 32);
+      V.og[2] = (int)(mb >> 32);
+      V.og[3] = (int)(md >> 32);
+      V.w[0] = wp;
+      V.w[1] = LW ? s_w[x] : 0.0;
+      V.w[2] = LW ? s_w[y] : 0.0;
+      V.w[3] = LW ? s_w[z] : 0.0;
+      // m: (p,a) (p,b) (p,d) (a,b) (a,d) (b,d)
+      const uint32_t m[6] = {(uint32_t)ma & 0xffffffu, (uint32_t)mb & 0xffffffu,
+                             (uint32_t)md & 0xffffffu, pack_meta(bxy, 1, 1), pack_meta(bxz, 1, 1),
+                             pack_meta(byz, 1, 1)};
+      const int nroot =
+          quad_emit<WEIGHTED, SHC, ADJ, COMPACT>(X, V, m, gscale, racc, s_glo, s_ghi, x, y, z);
+      quads += nroot > 0;
+      rooted += nroot;
+    };
+    // the cliques of up to 32 queued edges (entry e, or none when e < 0);
+    // every lane takes part.  fin: also drain the cliques still queued.
+    // (One call site each for this and drain_one: their code is long.)
+    auto run_edges = [&](int e, bool fin) {
+      const bool live = e >= 0;
+      int x = 0, y = 0, bxy = 0, cw = 0;
+      unsigned cm = 0u;
+      if (live) {
+        const uint32_t ent = s_eq[e];
+        x = (int)(ent & 0xffu);
+        y = (int)((ent >> 8) & 0xffu);
+        cw = y >> 5;
+        cm = s_adj[x * nwk + cw] & s_adj[y * nwk + cw];
+        bxy = edge_rbin(C.posd, P, s_col[x], s_col[y], s_pos[x], s_pos[y]);
+      }
+      for (;;) {
+        if (live)
+          while (cm == 0u && cw + 1 < nwk) {
+            ++cw;
+            cm = s_adj[x * nwk + cw] & s_adj[y * nwk + cw];
+          }
+        const bool has = live && cm != 0u;
+        const unsigned hm = __ballot_sync(0xffffffffu, has);
+        if (has) {
+          const int z = cw * 32 + __ffs(cm) - 1;
+          cm &= cm - 1u;
+          s_q[qn + __popc(hm & lt)] = (uint32_t)(x | (y << 8) | (z << 16) | (bxy << 24));
+        }
+        qn += __popc(hm);
+        if (qn >= 32 || (fin && hm == 0u && qn > 0)) {
+          const int nq = min(qn, 32);
+          __syncwarp();
+          if (lane < nq) drain_one(qn - nq + lane);
+          qn -= nq;
+          __syncwarp();
+        }
+        if (hm == 0u && (!fin || qn == 0)) break;
+      }
+    };
+    // pass 2: the edges in pair order, 32 at a time, then what is queued
+    for (int t0 = 0;; t0 += 32) {
+      if (t0 < npair) {
+        const int t = t0 + lane;
+        bool edge = false;
+        int x = 0, y = 0;
+        if (t < npair) {
+          pair_of(t, x, y);
+          edge = (s_adj[x * nwk + (y >> 5)] >> (y & 31)) & 1u;
+        }
+        const unsigned em = __ballot_sync(0xffffffffu, edge);
+        if (edge) s_eq[en + __popc(em & lt)] = (uint32_t)(x | (y << 8));
+        en += __popc(em);
+      }
+      const bool last = t0 + 32 >= npair;
+      if (en >= 32 || last) {
+        const int ne = min(en, 32);
+        const bool fin = last && en == ne;
+        __syncwarp();
+        run_edges(lane < ne ? en - ne + lane : -1, fin);
+        en -= ne;
+        __syncwarp();
+        if (fin) break;
+      }
+    }
+    if (ADJ) {
+      for (int x = lane; x < k; x += 32) {
+        const unsigned long long lo = s_glo[x], hi = s_ghi[x];
+        if (lo | hi) fix_merge(&g_lo[s_col[x]], &g_hi[s_col[x]], lo, hi);
+      }
+      racc = fix_warp_sum(racc);
+      if (lane == 0 && (racc.lo | racc.hi)) fix_merge(&g_lo[p], &g_hi[p], racc.lo, racc.hi);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    quads += __shfl_xor_sync(0xffffffffu, quads, o);
+    rooted += __shfl_xor_sync(0xffffffffu, rooted, o);
+    probes += __shfl_xor_sync(0xffffffffu, probes, o);
+  }
+  if (lane == 0) {
+    if (quads) atomicAdd(&stats[0], quads);
+    if (rooted) atomicAdd(&stats[1], rooted);
+    if (probes) atomicAdd(&stats[2], probes);
+  }
+  if (SHC) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < nh + nd; k += blockDim.x) {
+      const unsigned int v = X.scnt[k];
+      if (v) atomicAdd(k < nh ? &X.cnt[k] : &X.dcnt[k - nh], (unsigned long long)v);
+    }
+  }
+}
+
 // Warps per block: as many as fit in shared memory (at most maxw).
 int quad4_warps(int nbins, int cap, int ncounts, bool adj = false, int maxw = kQuadMaxWarps) {
   int nw = maxw;
@@ -714,36 +993,78 @@ int quad4_warps(int nbins, int cap, int ncounts, bool adj = false, int maxw = kQ
 
 }  // namespace
 
-bool launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bool weighted,
-                  unsigned long long* g_cnt, unsigned long long* g_fix, unsigned long long* d_cnt,
-                  unsigned long long* d_fix, int nh, int nd, double fscale, double dscale,
-                  bool shared_counts, unsigned long long* stats, int* work, cudaStream_t s) {
-  if (C.n <= 0) return false;
-  // block-private counters for unweighted catalogues when they leave room
-  // for at least 8 warps
-  const int ncnt = nh + nd;
-  if (weighted || quad4_warps(Q.nbins, Q.cap, ncnt) < 8) shared_counts = false;
-  const int maxw = weighted ? kQuadMaxWarps : kQuadMaxWarpsU;
-  const int nw = quad4_warps(Q.nbins, Q.cap, shared_counts ? ncnt : 0, false, maxw);
-  const size_t smem = quad_layout(Q.nbins, Q.cap, nw, shared_counts ? ncnt : 0).total;
+// Warps per block of the geometric kernel (at most maxw).
+static int quadg_warps(int nbins, int cap, int ncounts, bool adj, bool lw, int maxw) {
+  int nw = maxw;
+  while (nw > 1 && quadg_layout(nbins, cap, nw, ncounts, adj, lw).total > kQuadSmemLimit) nw -= 1;
+  return nw;
+}
+
+// Launch of either 4-clique kernel: grid of resident blocks, dynamic roots.
+template <typename K>
+static void launch_quad_grid(K kfn, int nw, size_t smem, int n, int* work, cudaStream_t s,
+                             const DevCatalog& C, const CSRView& G, const QuadParams& Q,
+                             unsigned long long* g_cnt, unsigned long long* g_fix,
+                             unsigned long long* d_cnt, unsigned long long* d_fix, int nh, int nd,
+                             double fscale, double dscale, unsigned long long* stats,
+                             const double* cot, double gscale, unsigned long long* g_lo,
+                             unsigned long long* g_hi) {
   if (smem > kQuadSmemLimit) throw Error{-2, "4PCF: per-warp shared memory exceeds the SM limit"};
-  // weighted: the compact contribution code (the unrolled form of its long
-  // fixed-point updates overflows the instruction cache); unweighted: unrolled
-  auto kfn = weighted ? quad4_kernel<true, false, false, true>
-                      : (shared_counts ? quad4_kernel<false, true, false, false>
-                                       : quad4_kernel<false, false, false, false>);
   GR_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nw * 32, smem));
   if (per_sm < 1) per_sm = 1;
   int64_t blocks = (int64_t)per_sm * 148;
-  const int64_t need = ((int64_t)C.n + nw - 1) / nw;
+  const int64_t need = ((int64_t)n + nw - 1) / nw;
   if (blocks > need) blocks = need;
   if (blocks < 1) blocks = 1;
   GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));
   kfn<<<(unsigned)blocks, nw * 32, smem, s>>>(C, G, Q, g_cnt, g_fix, d_cnt, d_fix, nh, nd, fscale,
-                                              dscale, stats, work, nullptr, 1.0, nullptr, nullptr);
+                                              dscale, stats, work, cot, gscale, g_lo, g_hi);
   GR_CHECK_LAUNCH();
+}
+
+bool launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bool weighted,
+                  unsigned long long* g_cnt, unsigned long long* g_fix, unsigned long long* d_cnt,
+                  unsigned long long* d_fix, int nh, int nd, double fscale, double dscale,
+                  bool shared_counts, unsigned long long* stats, int* work, cudaStream_t s) {
+  if (C.n <= 0) return false;
+  const bool geo = Q.geo != 0;
+  const int maxw = weighted ? kQuadMaxWarps : kQuadMaxWarpsU;
+  auto warps = [&](int ncounts, int mw) {
+    return geo ? quadg_warps(Q.nbins, Q.cap, ncounts, false, weighted, mw)
+               : quad4_warps(Q.nbins, Q.cap, ncounts, false, mw);
+  };
+  // block-private counters for unweighted catalogues when they leave room
+  // for at least 8 warps
+  const int ncnt = nh + nd;
+  if (weighted || warps(ncnt, kQuadMaxWarps) < 8) shared_counts = false;
+  const int nc = shared_counts ? ncnt : 0;
+  const int nw = warps(nc, maxw);
+  const size_t smem = geo ? quadg_layout(Q.nbins, Q.cap, nw, nc, false, weighted).total
+                          : quad_layout(Q.nbins, Q.cap, nw, nc).total;
+  // weighted: the compact contribution code (the unrolled form of its long
+  // fixed-point updates overflows the instruction cache); unweighted: unrolled
+#define GR_QUAD_LAUNCH(KERNEL)                                                                  \
+  do {                                                                                          \
+    if (weighted)                                                                               \
+      launch_quad_grid(KERNEL<true, false, false, true>, nw, smem, C.n, work, s, C, G, Q, g_cnt, \
+                       g_fix, d_cnt, d_fix, nh, nd, fscale, dscale, stats, nullptr, 1.0,        \
+                       nullptr, nullptr);                                                       \
+    else if (shared_counts)                                                                     \
+      launch_quad_grid(KERNEL<false, true, false, false>, nw, smem, C.n, work, s, C, G, Q,       \
+                       g_cnt, g_fix, d_cnt, d_fix, nh, nd, fscale, dscale, stats, nullptr, 1.0, \
+                       nullptr, nullptr);                                                       \
+    else                                                                                        \
+      launch_quad_grid(KERNEL<false, false, false, false>, nw, smem, C.n, work, s, C, G, Q,      \
+                       g_cnt, g_fix, d_cnt, d_fix, nh, nd, fscale, dscale, stats, nullptr, 1.0, \
+                       nullptr, nullptr);                                                       \
+  } while (0)
+  if (geo)
+    GR_QUAD_LAUNCH(quad4g_kernel);
+  else
+    GR_QUAD_LAUNCH(quad4_kernel);
+#undef GR_QUAD_LAUNCH
   return shared_counts;
 }
 
@@ -751,22 +1072,19 @@ void launch_adj4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, con
                  double gscale, unsigned long long* g_lo, unsigned long long* g_hi,
                  unsigned long long* stats, int* work, cudaStream_t s) {
   if (C.n <= 0) return;
-  const int nw = quad4_warps(Q.nbins, Q.cap, 0, true);
-  const size_t smem = quad_layout(Q.nbins, Q.cap, nw, 0, true).total;
-  if (smem > kQuadSmemLimit) throw Error{-2, "4PCF adjoint: per-warp shared memory exceeds the SM limit"};
-  auto kfn = quad4_kernel<false, false, true, true>;
-  GR_CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int per_sm = 0;
-  GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nw * 32, smem));
-  if (per_sm < 1) per_sm = 1;
-  int64_t blocks = (int64_t)per_sm * 148;
-  const int64_t need = ((int64_t)C.n + nw - 1) / nw;
-  if (blocks > need) blocks = need;
-  if (blocks < 1) blocks = 1;
-  GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));
-  kfn<<<(unsigned)blocks, nw * 32, smem, s>>>(C, G, Q, nullptr, nullptr, nullptr, nullptr, 0, 0,
-                                              1.0, 1.0, stats, work, cot, gscale, g_lo, g_hi);
-  GR_CHECK_LAUNCH();
+  if (Q.geo) {
+    const int nw = quadg_warps(Q.nbins, Q.cap, 0, true, true, kQuadMaxWarps);
+    const size_t smem = quadg_layout(Q.nbins, Q.cap, nw, 0, true, true).total;
+    launch_quad_grid(quad4g_kernel<false, false, true, true>, nw, smem, C.n, work, s, C, G, Q,
+                     nullptr, nullptr, nullptr, nullptr, 0, 0, 1.0, 1.0, stats, cot, gscale, g_lo,
+                     g_hi);
+  } else {
+    const int nw = quad4_warps(Q.nbins, Q.cap, 0, true);
+    const size_t smem = quad_layout(Q.nbins, Q.cap, nw, 0, true).total;
+    launch_quad_grid(quad4_kernel<false, false, true, true>, nw, smem, C.n, work, s, C, G, Q,
+                     nullptr, nullptr, nullptr, nullptr, 0, 0, 1.0, 1.0, stats, cot, gscale, g_lo,
+                     g_hi);
+  }
 }
 
 size_t quad4_smem_bytes(int nbins, int cap) {

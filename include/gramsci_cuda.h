@@ -53,6 +53,11 @@ typedef struct gr_ctx gr_ctx;
 #define GR_OPT_KEEP_GRAPH 4 /* 0 (default): every count call builds the index and graph;
                                1: keep the graph of the last call and reuse it until the
                                catalogue, the bins or the precision change */
+#define GR_OPT_CLIQUE_MODE 5 /* how the 3PCF / 4PCF kernels find the edges among a root's
+                               larger-label neighbours: 0 automatic (default), 1 hash probes
+                               of the neighbours' rows, 2 the graph's membership test on the
+                               pairs of neighbours (rows up to 256 neighbours; longer rows
+                               fall back to 1).  Results are identical; only speed differs */
 
 /* Run statistics of the last count call (gr_get_stats). */
 typedef struct gr_stats {

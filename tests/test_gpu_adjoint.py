@@ -29,10 +29,19 @@ def _cat(name, scale, seed=None):
     return cat, w, catalogs.WORKLOADS[name]
 
 
-@pytest.mark.parametrize("order,name,scale", [(2, "c5_adjoint_2pcf", 0.003),
-                                              (3, "c5_adjoint_3pcf", 0.002),
-                                              (3, "c2_3pcf", 0.01)])
-def test_adjoint_matches_oracle(gpu_ctx, oracle, order, name, scale):
+@pytest.mark.parametrize("order,name,scale,mode", [(2, "c5_adjoint_2pcf", 0.003, "auto"),
+                                                   (3, "c5_adjoint_3pcf", 0.002, "auto"),
+                                                   (3, "c2_3pcf", 0.01, "auto"),
+                                                   (3, "c2_3pcf", 0.01, "hash")])
+def test_adjoint_matches_oracle(gpu_ctx, oracle, order, name, scale, mode):
+    gpu_ctx.set_clique_mode(mode)
+    try:
+        _adjoint_matches_oracle(gpu_ctx, oracle, order, name, scale)
+    finally:
+        gpu_ctx.set_clique_mode("auto")
+
+
+def _adjoint_matches_oracle(gpu_ctx, oracle, order, name, scale):
     cat, w, sp = _cat(name, scale)
     rng = np.random.default_rng(order)
     gpu_ctx.set_catalog(cat.xyz, w, cat.n_data)
@@ -53,7 +62,7 @@ def test_adjoint_matches_oracle(gpu_ctx, oracle, order, name, scale):
     assert np.all(np.abs(g - ref) <= 1e-12 * np.abs(ref).max())
 
 
-@pytest.mark.parametrize("case", ["lognormal", "buffer", "unit_partial"])
+@pytest.mark.parametrize("case", ["lognormal", "buffer", "unit_partial", "hash"])
 def test_adjoint_4pcf_matches_oracle(gpu_ctx, oracle, case):
     cat = catalogs.make("c3_4pcf", scale=0.05)
     sp = catalogs.WORKLOADS["c3_4pcf"]
@@ -70,7 +79,12 @@ def test_adjoint_4pcf_matches_oracle(gpu_ctx, oracle, case):
     if case == "unit_partial":
         c3, cR = None, None
         gpu_ctx.count_4pcf()  # the adjoint reuses this graph
-    g = gpu_ctx.adjoint_4pcf(c2, c3, cN, cR)
+    if case == "hash":
+        gpu_ctx.set_clique_mode("hash")
+    try:
+        g = gpu_ctx.adjoint_4pcf(c2, c3, cN, cR)
+    finally:
+        gpu_ctx.set_clique_mode("auto")
     G = oracle.Graph(cat.xyz, sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
     ref = G.adjoint4(w, cat.n_data, c2, c3, cN, cR, buffer=buf)
     assert np.count_nonzero(ref) > cat.n // 10

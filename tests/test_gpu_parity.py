@@ -105,6 +105,44 @@ def test_3pcf_third_edge_modes(gpu_ctx, oracle, name, scale, nmu, precision):
     gpu_ctx.set_precision("f32")
 
 
+@pytest.mark.parametrize("mode", ["hash", "geometric"])
+@pytest.mark.parametrize("query", ["3pcf", "equi", "4pcf", "4pcf_weighted", "tetra"])
+def test_clique_modes(gpu_ctx, oracle, query, mode):
+    """Both ways of finding the edges among a root's neighbours, forced,
+    against the oracle (buffer points included)."""
+    if query.startswith("4pcf") or query == "tetra":
+        cat, w, sp = _cat("c3_4pcf", 0.05)
+    else:
+        cat, w, sp = _cat("c2_3pcf", 0.02)
+    rng = np.random.default_rng(17)
+    if query == "4pcf_weighted":
+        w = catalogs.normalise(rng.lognormal(0, 0.3, cat.n), cat.n_data, cat.n_rand)
+    buf = (rng.random(cat.n) < 0.1).astype(np.int32)
+    gpu_ctx.set_clique_mode(mode)
+    try:
+        gpu_ctx.set_catalog(cat.xyz, w, cat.n_data, buffer=buf)
+        gpu_ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
+        G = oracle.Graph(cat.xyz, sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
+        if query == "3pcf":
+            got, ref = gpu_ctx.count_3pcf(), G.pcf3(w, cat.n_data, buffer=buf)
+        elif query == "equi":
+            got, ref = gpu_ctx.count_equi(), G.equi(w, cat.n_data, buffer=buf)
+        elif query == "tetra":
+            got, ref = gpu_ctx.count_tetra(), G.tetra(w, cat.n_data, buffer=buf)
+        else:
+            got, ref = gpu_ctx.count_4pcf(), G.pcf4(w, cat.n_data, buffer=buf)
+        assert int(ref["counts"].sum()) > 0
+        assert np.array_equal(got["counts"], ref["counts"])
+        assert _rel(got["catsum"], ref["catsum"]) < RTOL
+        for k in ("dcount",):
+            if k in ref:
+                assert np.array_equal(got[k], ref[k])
+        if "dsum" in ref:
+            assert _rel(got["dsum"], ref["dsum"]) < RTOL
+    finally:
+        gpu_ctx.set_clique_mode("auto")
+
+
 def test_3pcf_unit_weights(gpu_ctx, oracle):
     cat, w, sp = _cat("c5_adjoint_3pcf", 0.002)
     w = catalogs.normalise(np.ones(cat.n), cat.n_data, cat.n_rand)
