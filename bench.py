@@ -489,6 +489,11 @@ def run_quad(args):
     w_d = torch.from_numpy(w).to("cuda:0")
     ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
     ctx.set_catalog(xyz_d, w_d, cat.n_data)
+    # the geometric 4-clique kernel: what the automatic choice takes for
+    # unit weights with rows of at most 256 neighbours (this catalogue's
+    # longest upper row has 96), set explicitly so that the roofline below
+    # names the kernel that ran
+    ctx.set_clique_mode("geometric")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda:0")
     sampler = ClockSampler(0)
     sampler.start()
@@ -533,10 +538,12 @@ def run_quad(args):
     d2h = int(sum(v.nbytes for v in out.values()) + 8 * 8)
 
     pk = roofline.peaks()
-    rf = roofline.quad4_roofline(ctx, q_ms, pk)
-    rf["traffic"] = roofline.profiled_traffic("quad4_kernel", args.scale, "c3")
+    rf = roofline.quad4_roofline(ctx, q_ms, pk, geometric=True)
+    rf["traffic"] = roofline.profiled_traffic("quad4g_kernel", args.scale, "c3")
 
-    # the same catalogue with lognormal weights: weighted sums and adjoint
+    # the same catalogue with lognormal weights (automatic kernel choice):
+    # weighted sums and adjoint
+    ctx.set_clique_mode("auto")
     rng = np.random.default_rng(5)
     wl = catalogs.normalise(rng.lognormal(0.0, 0.3, cat.n), cat.n_data, cat.n_rand)
     ctx.set_catalog(torch.from_numpy(cat.xyz).to("cuda:0"), torch.from_numpy(wl).to("cuda:0"),

@@ -40,24 +40,32 @@ def tri3_roofline(ctx, q_ms, pk):
             "bytes_per_launch": b, "ms_per_launch": ms, "peak_source": pk["source"]}
 
 
-def quad4_bytes(stats):
+def quad4_bytes(stats, geometric):
     """Algorithmic bytes of one 4-clique-kernel launch.
 
-    Per upper edge (p, a): the root row entry (8 B) and the two row offsets
-    of a (16 B).  Per probe (a record of the row of a, or of the row of an X
-    entry b, read and looked up in the row of p): the record (8 B).  Per
-    rooted 4-clique contribution the (b, d) edge metadata and the far
-    vertex's flags, id and weight: counted as 4 + 13 B.
+    Hash mode (quad4_kernel): per upper edge (p, a) the root row entry (8 B)
+    and the two row offsets of a (16 B); per probe (a record of the row of a,
+    or of the row of an X entry b, read and looked up in the row of p) the
+    record (8 B); per rooted contribution the (b, d) edge metadata and the
+    far vertex's flags, id and weight (4 + 13 B).
+    Geometric mode (quad4g_kernel): it reads only the roots' rows and the
+    members' data: per upper edge the record (8 B), the FP32 position
+    (16 B), flags, catalogue id and full degree (9 B); per point its row
+    start, length, flags, id and full degree (21 B).  Its pair tests run on
+    shared memory.
     """
+    if geometric:
+        return 33 * stats["upper_edges"] + 21 * stats["n_points"]
     return 24 * stats["upper_edges"] + 8 * stats["probes"] + 17 * stats["rooted"]
 
 
-def quad4_roofline(ctx, q_ms, pk):
+def quad4_roofline(ctx, q_ms, pk, geometric):
     st = ctx.stats()
     ms = sum(q_ms) / len(q_ms)
-    b = quad4_bytes(st)
+    b = quad4_bytes(st, geometric)
     achieved = b / (ms * 1e-3) / 1e9
-    return {"bound": "hbm", "kernel": "quad4_kernel", "achieved": achieved, "peak": pk["hbm_gbs"],
+    kernel = "quad4g_kernel" if geometric else "quad4_kernel"
+    return {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": pk["hbm_gbs"],
             "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "traffic": None,
             "bytes_per_launch": b, "ms_per_launch": ms, "peak_source": pk["source"]}
 

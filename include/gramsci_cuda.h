@@ -73,7 +73,8 @@ typedef struct gr_stats {
   int64_t candidates;     /* candidate pairs tested                              */
   int64_t kernel_launches;/* kernels launched by the call                        */
   int64_t probes;         /* intersection probes (3PCF/4PCF): neighbour-row entries
-                             looked up in the root's row                          */
+                             looked up in the root's row, or in the geometric
+                             clique mode the pairs of the root's neighbours tested */
   int64_t upper_edges;    /* undirected edges stored in the upper CSR            */
 } gr_stats;
 
