@@ -46,6 +46,11 @@ struct gr_ctx {
   UpperCSR csr;
   bool csr_valid = false;
   int clique_mode = 0;  // GR_OPT_CLIQUE_MODE
+  // speculative rebuilds (count_tri): catalogue generation (set_catalog),
+  // generation of the last verified build, and whether speculating on a new
+  // catalogue is still worth it (off after it once found a changed grid)
+  uint64_t cat_gen = 0, spec_gen = ~0ull;
+  bool spec_new_ok = true;
   bool keep_graph = false;    // GR_OPT_KEEP_GRAPH
   bool graph_loaded = false;  // graph read by gr_graph_load
   PairParams P{};
@@ -380,17 +385,19 @@ float ev_ms(cudaEvent_t a, cudaEvent_t b) {
 }
 
 // Index build + pair parameters (shared by every query).
-void build_index(gr_ctx* c) {
+// speculate: see CellIndex / UpperCSR; the caller checks the flags
+void build_index(gr_ctx* c, bool speculate = false) {
   cudaStream_t s = c->stream();
-  c->index.build(c->xyz.p, c->w.p, c->has_buffer ? c->buffer.p : nullptr, c->n, c->n_data, c->rmax, s);
+  c->index.build(c->xyz.p, c->w.p, c->has_buffer ? c->buffer.p : nullptr, c->n, c->n_data, c->rmax, s,
+                 speculate);
   make_pair_params(c->P, c->rmin, c->rmax, c->nbins, c->nmu, c->logbins, c->index.coord_max,
                    c->precision == 1);
   c->csr_valid = false;
 }
 
-void build_csr(gr_ctx* c) {
-  c->csr.build(c->index.view(), c->P, c->stream());
-  c->csr_valid = true;
+void build_csr(gr_ctx* c, bool speculate = false) {
+  c->csr.build(c->index.view(), c->P, c->stream(), speculate);
+  c->csr_valid = !speculate;  // a speculative graph is valid once settled
 }
 
 // The index and graph of the last call (or of gr_graph_load) are current and
@@ -475,6 +482,7 @@ static int set_catalog_impl(gr_ctx* c, const double* xyz, const double* w, const
   if (n >= (int64_t)1 << 31) return set_err(c, GR_E_CAPACITY, "catalogue larger than 2^31-1 points");
   if (n > 0 && (!xyz || !w)) return set_err(c, GR_E_ARG, "null xyz or w");
   cudaStream_t s = c->stream();
+  c->cat_gen++;
   c->xyz.reserve(3 * n + 1);
   c->w.reserve(n + 1);
   if (n > 0) {
@@ -730,47 +738,77 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
   c->normal_dev.reserve(nt.size());
   GR_CUDA_TRY(cudaMemcpyAsync(c->normal_dev.p, nt.data(), nt.size(), cudaMemcpyHostToDevice, s));
   const bool reuse = reuse_graph(c);
-  GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
-  if (!reuse) build_index(c);
-  GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
-  if (!reuse) build_csr(c);
-  GR_CUDA_TRY(cudaEventRecord(c->ev[2], s));
+  // A rebuild of a catalogue seen before runs without waiting on the host:
+  // the grid is taken from the last bounding box, the graph is filled in the
+  // scratch area as it is, and the triangle kernel's row capacity is taken
+  // from the last graph (longer rows take its global-memory path, so any
+  // capacity gives the same result).  A device flag records a changed
+  // bounding box and the graph build one that ran out of room; both are
+  // read with the results, and the call is then repeated with waits.
+  const bool can_spec =
+      !reuse && c->index.have_prev && (c->cat_gen == c->spec_gen || c->spec_new_ok);
+  std::vector<unsigned long long> hc(nh, 0ull), hf(2 * nh, 0ull);
+  std::vector<double> hs(nh, 0.0);
+  unsigned long long st[8];
+  cudaEvent_t q0;
+  GR_CUDA_TRY(cudaEventCreate(&q0));
+  c->work.reserve(4);
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    const bool spec = can_spec && attempt == 0;
+    GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
+    if (!reuse) build_index(c, spec);
+    GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+    if (!reuse) build_csr(c, spec);
+    GR_CUDA_TRY(cudaEventRecord(c->ev[2], s));
+    GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nh, s));
+    GR_CUDA_TRY(cudaMemsetAsync(c->hfix.p, 0, sizeof(unsigned long long) * 2 * nh, s));
+    GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
+    TriParams T{};
+    T.nbins = c->nbins;
+    T.nmu = nmu;
+    T.ncfg = ncfg;
+    T.rsd = nmu >= 2;
+    T.equi = equi ? 1 : 0;
+    T.cap = round_cap(c->csr.max_deg, 32, 256);
+    T.normal = c->normal_dev.p;
+    make_rank_tables(T.rank, c->nbins, 3);
+    for (int nr = 0; nr < 4; ++nr) T.fscale[nr] = fscale[nr];
+    T.P = c->P;
+    T.geo = tri_geometric(c, T.rsd);
+    const CSRView G = c->csr.view();
+    GR_CUDA_TRY(cudaEventRecord(q0, s));
+    launch_tri3(c->index.view(), G, T, weighted, want_counts, c->hcnt.p, c->hfix.p, c->stats.p,
+                c->work.p, s);
+    GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
+    if (want_counts)
+      GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
+    if (weighted)
+      GR_CUDA_TRY(cudaMemcpyAsync(hf.data(), c->hfix.p, sizeof(unsigned long long) * 2 * nh, cudaMemcpyDeviceToHost, s));
+    GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
+    unsigned long long gctl[4] = {0, 0, 0, 0}, gsts[3] = {0, 0, 0}, gflag = 0;
+    if (spec) {
+      GR_CUDA_TRY(cudaMemcpyAsync(gctl, c->csr.ctl.p, sizeof(gctl), cudaMemcpyDeviceToHost, s));
+      GR_CUDA_TRY(cudaMemcpyAsync(gsts, c->csr.stats.p, sizeof(gsts), cudaMemcpyDeviceToHost, s));
+      if (c->index.speculated)
+        GR_CUDA_TRY(cudaMemcpyAsync(&gflag, c->index.mismatch_flag(), sizeof(gflag),
+                                    cudaMemcpyDeviceToHost, s));
+    }
+    GR_CUDA_TRY(cudaStreamSynchronize(s));
+    if (spec) {
+      if (gflag != 0 || gctl[1] == 1) {  // repeat with waits
+        if (c->cat_gen != c->spec_gen) c->spec_new_ok = false;
+        continue;
+      }
+      c->csr.settle(gctl, gsts);
+      c->csr_valid = true;
+    }
+    break;
+  }
+  if (!reuse) c->spec_gen = c->cat_gen;
   // graph statistics are on the host after the build (or the load)
   const unsigned long long gst[3] = {(unsigned long long)c->csr.rechecks,
                                      (unsigned long long)c->csr.candidates,
                                      (unsigned long long)c->csr.max_deg};
-  GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nh, s));
-  GR_CUDA_TRY(cudaMemsetAsync(c->hfix.p, 0, sizeof(unsigned long long) * 2 * nh, s));
-  GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
-  TriParams T{};
-  T.nbins = c->nbins;
-  T.nmu = nmu;
-  T.ncfg = ncfg;
-  T.rsd = nmu >= 2;
-  T.equi = equi ? 1 : 0;
-  T.cap = round_cap(c->csr.max_deg, 32, 256);
-  T.normal = c->normal_dev.p;
-  make_rank_tables(T.rank, c->nbins, 3);
-  for (int nr = 0; nr < 4; ++nr) T.fscale[nr] = fscale[nr];
-  T.P = c->P;
-  T.geo = tri_geometric(c, T.rsd);
-  const CSRView G = c->csr.view();
-  cudaEvent_t q0;
-  GR_CUDA_TRY(cudaEventCreate(&q0));
-  GR_CUDA_TRY(cudaEventRecord(q0, s));
-  c->work.reserve(4);
-  launch_tri3(c->index.view(), G, T, weighted, want_counts, c->hcnt.p, c->hfix.p, c->stats.p,
-              c->work.p, s);
-  GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
-  std::vector<unsigned long long> hc(nh, 0ull), hf(2 * nh, 0ull);
-  std::vector<double> hs(nh, 0.0);
-  unsigned long long st[8];
-  if (want_counts)
-    GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
-  if (weighted)
-    GR_CUDA_TRY(cudaMemcpyAsync(hf.data(), c->hfix.p, sizeof(unsigned long long) * 2 * nh, cudaMemcpyDeviceToHost, s));
-  GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
-  GR_CUDA_TRY(cudaStreamSynchronize(s));
   if (weighted)
     for (int k = 0; k < nh; ++k) hs[k] = fix_value(hf[k], hf[nh + k], fscale[k / nbin]);
   if (!weighted) {

@@ -192,8 +192,12 @@ __global__ void __launch_bounds__(kGraphThreads) csr_fill_kernel(
           }
         }
         if (lane == 0) {
-          deg_up[p] = off;
-          rstart[p] = base + (long long)i * total - (long long)i * (i + 1) / 2;
+          // a cell without room keeps no rows: after its last tile its roots
+          // have empty rows, so that nothing reads past the scratch area
+          // (the build is repeated with room; deg_up carries the running
+          // count between tiles)
+          deg_up[p] = (room || !last_tile) ? off : 0;
+          rstart[p] = room ? base + (long long)i * total - (long long)i * (i + 1) / 2 : 0;
           cands += (unsigned long long)(tn - fstart);
           if (last_tile) {
             atomicAdd(&deg_full[p], off);
@@ -263,7 +267,7 @@ int graph_blocks(int64_t ncell) {
 
 }  // namespace
 
-void UpperCSR::build(const DevCatalog& C, const PairParams& P, cudaStream_t s) {
+void UpperCSR::build(const DevCatalog& C, const PairParams& P, cudaStream_t s, bool speculate) {
   n = C.n;
   launches = 0;
   deg_up.reserve(n + 1);
@@ -307,6 +311,11 @@ void UpperCSR::build(const DevCatalog& C, const PairParams& P, cudaStream_t s) {
       launches++;
       GR_CHECK_LAUNCH();
     }
+    if (speculate) {
+      // the caller reads ctl and stats with its results and calls settle()
+      compacted = false;
+      return;
+    }
     GR_CUDA_TRY(cudaMemcpyAsync(hc, ctl.p, sizeof(hc), cudaMemcpyDeviceToHost, s));
     GR_CUDA_TRY(cudaMemcpyAsync(hs, stats.p, sizeof(hs), cudaMemcpyDeviceToHost, s));
     if (ncell > 0)
@@ -324,6 +333,15 @@ void UpperCSR::build(const DevCatalog& C, const PairParams& P, cudaStream_t s) {
   candidates = (int64_t)hs[1];
   max_deg = (int64_t)hs[2];
   compacted = false;
+}
+
+void UpperCSR::settle(const unsigned long long hc[4], const unsigned long long hs[3]) {
+  if (hc[1] == 2) throw Error{-2, "CSR build: a grid cell holds 2^24 points or more"};
+  if (hc[2] != 0) throw Error{-3, "CSR build: FP32 membership and FP64 binning disagree"};
+  n_edges = (int64_t)hc[3];
+  rechecks = (int64_t)hs[0];
+  candidates = (int64_t)hs[1];
+  max_deg = (int64_t)hs[2];
 }
 
 void UpperCSR::compact(cudaStream_t s) {

@@ -5,6 +5,8 @@
 // float4 (FP32 fast path) and double4 (FP64 guard band, weight) arrays.
 #include "gr_index.cuh"
 
+#include <cstring>
+
 namespace gr {
 
 namespace {
@@ -66,6 +68,17 @@ __global__ void bbox_kernel(const double* __restrict__ xyz, int64_t n, unsigned 
       atomicMin(&out[t], v);
     else
       atomicMax(&out[t], v);
+  }
+}
+
+// Speculative builds: flag [7] = 1 when the new bounding box differs from
+// the one the grid was taken from.
+__global__ void bbox_check_kernel(const unsigned long long* __restrict__ now,
+                                  unsigned long long* __restrict__ prev) {
+  if (threadIdx.x == 0) {
+    unsigned long long d = 0;
+    for (int k = 0; k < 7; ++k) d |= now[k] ^ prev[k];
+    prev[7] = d != 0 ? 1ull : 0ull;
   }
 }
 
@@ -172,11 +185,12 @@ int blocks_for(int64_t n, int threads, int cap = 148 * 16) {
 }  // namespace
 
 void CellIndex::build(const double* d_xyz, const double* d_w, const int* d_buffer, int64_t n_pts,
-                      int64_t n_data_pts, double rmax, cudaStream_t s) {
+                      int64_t n_data_pts, double rmax, cudaStream_t s, bool speculate) {
   n = n_pts;
   n_data = n_data_pts;
   launches = 0;
   bbox_raw.reserve(8);
+  bbox_prev.reserve(8);
   init_bbox_kernel<<<1, 32, 0, s>>>(bbox_raw.p);
   launches++;
   if (n > 0) {
@@ -185,8 +199,22 @@ void CellIndex::build(const double* d_xyz, const double* d_w, const int* d_buffe
   }
   GR_CHECK_LAUNCH();
   unsigned long long h[7];
-  GR_CUDA_TRY(cudaMemcpyAsync(h, bbox_raw.p, sizeof(h), cudaMemcpyDeviceToHost, s));
-  GR_CUDA_TRY(cudaStreamSynchronize(s));
+  speculated = speculate && have_prev && prev_n == n && prev_rmax == rmax;
+  if (speculated) {
+    std::memcpy(h, prev_raw, sizeof(h));
+    bbox_check_kernel<<<1, 32, 0, s>>>(bbox_raw.p, bbox_prev.p);
+    launches++;
+    GR_CHECK_LAUNCH();
+  } else {
+    GR_CUDA_TRY(cudaMemcpyAsync(h, bbox_raw.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    GR_CUDA_TRY(cudaStreamSynchronize(s));
+    std::memcpy(prev_raw, h, sizeof(h));
+    prev_n = n;
+    prev_rmax = rmax;
+    have_prev = true;
+    GR_CUDA_TRY(cudaMemcpyAsync(bbox_prev.p, prev_raw, sizeof(prev_raw), cudaMemcpyHostToDevice, s));
+    GR_CUDA_TRY(cudaMemsetAsync(bbox_prev.p + 7, 0, sizeof(unsigned long long), s));
+  }
   double lo[3], hi[3];
   for (int d = 0; d < 3; ++d) {
     lo[d] = n > 0 ? key_to_dbl(h[d]) : 0.0;

@@ -18,6 +18,16 @@ struct CellIndex {
   GridParams grid{};
   int launches = 0;
   DevBuf<unsigned long long> bbox_raw;
+  // Speculative build: the grid depends only on the bounding box, the point
+  // count and rmax, so a build may take the previous build's bounding box
+  // without waiting for the new one and let a device check record whether
+  // it differs (bbox_prev[7] = 1); the caller reads the flag with its results
+  // and rebuilds without speculation when it is set.
+  bool have_prev = false, speculated = false;
+  int64_t prev_n = -1;
+  double prev_rmax = 0.0;
+  unsigned long long prev_raw[7] = {0, 0, 0, 0, 0, 0, 0};
+  DevBuf<unsigned long long> bbox_prev;  // previous raw bounding box [0..6], mismatch flag [7]
   DevBuf<int> cell_count, key_orig, slot, tmp_perm, perm, cell_start, orig, cell_key;
   DevBuf<int64_t> cell_start64, scan_tmp;
   DevBuf<float4> pos4;
@@ -26,7 +36,8 @@ struct CellIndex {
   DevBuf<uint8_t> flags;
 
   void build(const double* d_xyz, const double* d_w, const int* d_buffer, int64_t n, int64_t n_data,
-             double rmax, cudaStream_t s);
+             double rmax, cudaStream_t s, bool speculate = false);
+  const unsigned long long* mismatch_flag() const { return bbox_prev.p + 7; }
   DevCatalog view() const;
 };
 
@@ -57,7 +68,11 @@ struct UpperCSR {
   DevBuf<unsigned long long> scratch;  // rows as built: rstart / deg_up
   DevBuf<unsigned long long> stats;    // [0] FP64 rechecks, [1] candidates, [2] max upper degree
   DevBuf<unsigned long long> ctl;      // [1] out of room, [2] disagreements, [3] edges
-  void build(const DevCatalog& C, const PairParams& P, cudaStream_t s);
+  // speculate: one fill with the scratch area as it is and no wait; the
+  // caller reads ctl[0..3] and stats[0..2] with its results, calls settle()
+  // and rebuilds without speculation when ctl[1] == 1 (out of room).
+  void build(const DevCatalog& C, const PairParams& P, cudaStream_t s, bool speculate = false);
+  void settle(const unsigned long long hc[4], const unsigned long long hs[3]);
   void compact(cudaStream_t s);
   CSRView view() const { return CSRView{rstart.p, deg_up.p, scratch.p, deg_full.p}; }
 };
