@@ -599,9 +599,13 @@ static int pick_pair2_variant(gr_ctx* c, const DevCatalog& C, bool weighted, dou
   while (dens < 20 && std::ldexp(1.0, dens + 1) <= per_cell) ++dens;
   int hb = 0;
   while (hb < 20 && (2 << hb) <= c->nbins * c->nmu) ++hb;
+  // number of cells in factors of 4: how well a variant fills the SMs with
+  // warps or blocks per cell depends on it
+  int cb = 0;
+  while (cb < 20 && ((int64_t)4 << (2 * cb)) <= C.grid.ncell) ++cb;
   char key[128];
-  std::snprintf(key, sizeof(key), "pair2v6|%s|%s|dens%d|hist%d", c->P.f32 ? "f32" : "f64",
-                weighted ? "w" : "u", dens, hb);
+  std::snprintf(key, sizeof(key), "pair2v8|%s|%s|dens%d|hist%d|cells%d", c->P.f32 ? "f32" : "f64",
+                weighted ? "w" : "u", dens, hb, cb);
   Tuner& T = tuner();
   {
     std::lock_guard<std::mutex> lock(T.mu);
@@ -613,22 +617,29 @@ static int pick_pair2_variant(gr_ctx* c, const DevCatalog& C, bool weighted, dou
   cudaEvent_t a, b;
   GR_CUDA_TRY(cudaEventCreate(&a));
   GR_CUDA_TRY(cudaEventCreate(&b));
-  int best = kPairWarpCell;
-  float best_ms = 1e30f;
+  // every variant once untimed (its first launch loads its code), then the
+  // fastest of three interleaved rounds
+  float t[kPairVariants];
   for (int v = 0; v < kPairVariants; ++v) {
-    GR_CUDA_TRY(cudaMemsetAsync(hcnt, 0, sizeof(unsigned long long) * nh, s));
-    GR_CUDA_TRY(cudaMemsetAsync(hfix, 0, sizeof(unsigned long long) * 2 * nh, s));
-    GR_CUDA_TRY(cudaEventRecord(a, s));
+    t[v] = 1e30f;
     launch_pair2(C, c->P, weighted, hcnt, hfix, fscale, stats, work, s, v);
-    GR_CUDA_TRY(cudaEventRecord(b, s));
-    GR_CUDA_TRY(cudaEventSynchronize(b));
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, a, b);
-    if (ms < best_ms) {
-      best_ms = ms;
-      best = v;
+  }
+  for (int round = 0; round < 3; ++round) {
+    for (int v = 0; v < kPairVariants; ++v) {
+      GR_CUDA_TRY(cudaMemsetAsync(hcnt, 0, sizeof(unsigned long long) * nh, s));
+      GR_CUDA_TRY(cudaMemsetAsync(hfix, 0, sizeof(unsigned long long) * 2 * nh, s));
+      GR_CUDA_TRY(cudaEventRecord(a, s));
+      launch_pair2(C, c->P, weighted, hcnt, hfix, fscale, stats, work, s, v);
+      GR_CUDA_TRY(cudaEventRecord(b, s));
+      GR_CUDA_TRY(cudaEventSynchronize(b));
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, a, b);
+      t[v] = std::min(t[v], ms);
     }
   }
+  int best = kPairWarpCell;
+  for (int v = 1; v < kPairVariants; ++v)
+    if (t[v] < t[best]) best = v;
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   std::lock_guard<std::mutex> lock(T.mu);
@@ -775,6 +786,8 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
     for (int nr = 0; nr < 4; ++nr) T.fscale[nr] = fscale[nr];
     T.P = c->P;
     T.geo = tri_geometric(c, T.rsd);
+    T.maxdeg = (int)std::min<int64_t>(c->csr.max_deg, 1 << 30);
+    T.long_geo = c->clique_mode != 1;
     const CSRView G = c->csr.view();
     GR_CUDA_TRY(cudaEventRecord(q0, s));
     launch_tri3(c->index.view(), G, T, weighted, want_counts, c->hcnt.p, c->hfix.p, c->stats.p,
@@ -1302,6 +1315,59 @@ static void finish_grad(gr_ctx* c, double gscale, double* grad_w, cudaEvent_t q0
   c->st.ms_query = ev_ms(q0, c->ev[3]);
 }
 
+// Layout of the 2PCF adjoint sweep (warp per cell, or block per cell of 128
+// or 256 threads): timed and cached like the forward sweep's variant, under
+// its own key (the fastest adjoint layout is not always the forward's).
+static int pick_adj2_layout(gr_ctx* c, const DevCatalog& C, const double* c2, const double* c3,
+                            double gscale, unsigned long long* g_lo, unsigned long long* g_hi,
+                            int* work, cudaStream_t s) {
+  if (c->autotune == 0) return kPairWarpCell;
+  if (c->autotune >= 2) return c->autotune - 2;
+  const double per_cell = C.grid.ncell > 0 ? (double)C.n / (double)C.grid.ncell : 1.0;
+  int dens = 0;
+  while (dens < 20 && std::ldexp(1.0, dens + 1) <= per_cell) ++dens;
+  int hb = 0;
+  while (hb < 20 && (2 << hb) <= c->nbins * c->nmu) ++hb;
+  int cb = 0;
+  while (cb < 20 && ((int64_t)4 << (2 * cb)) <= C.grid.ncell) ++cb;
+  char key[128];
+  std::snprintf(key, sizeof(key), "adj2v1|%s|dens%d|hist%d|cells%d", c->P.f32 ? "f32" : "f64", dens,
+                hb, cb);
+  Tuner& T = tuner();
+  {
+    std::lock_guard<std::mutex> lock(T.mu);
+    T.load();
+    auto it = T.choice.find(key);
+    if (it != T.choice.end()) return it->second;
+  }
+  const int layouts[3] = {kPairWarpCell, kPairDense128, kPairDense256};
+  cudaEvent_t a, b;
+  GR_CUDA_TRY(cudaEventCreate(&a));
+  GR_CUDA_TRY(cudaEventCreate(&b));
+  float t[3] = {1e30f, 1e30f, 1e30f};
+  for (int v = 0; v < 3; ++v)
+    launch_adj2(C, c->P, c2, c3, gscale, g_lo, g_hi, work, s, layouts[v]);
+  for (int round = 0; round < 3; ++round)
+    for (int v = 0; v < 3; ++v) {
+      GR_CUDA_TRY(cudaEventRecord(a, s));
+      launch_adj2(C, c->P, c2, c3, gscale, g_lo, g_hi, work, s, layouts[v]);
+      GR_CUDA_TRY(cudaEventRecord(b, s));
+      GR_CUDA_TRY(cudaEventSynchronize(b));
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, a, b);
+      t[v] = std::min(t[v], ms);
+    }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  int best = 0;
+  for (int v = 1; v < 3; ++v)
+    if (t[v] < t[best]) best = v;
+  std::lock_guard<std::mutex> lock(T.mu);
+  T.choice[key] = layouts[best];
+  T.save();
+  return layouts[best];
+}
+
 int gr_adjoint_2pcf(gr_ctx* c, const double* cot2, const double* cot3, double* grad_w) {
   GR_API_BEGIN(c)
   require_ready(c);
@@ -1323,11 +1389,13 @@ int gr_adjoint_2pcf(gr_ctx* c, const double* cot2, const double* cot3, double* g
   GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
   GR_CUDA_TRY(cudaMemsetAsync(c->gfix.p, 0, sizeof(unsigned long long) * (2 * n + 2), s));
   std::memset(&c->st, 0, sizeof(c->st));
-  // same sweep layout as the forward pass on this catalogue
-  const int variant = c->autotune >= 2 ? c->autotune - 2 : c->last_variant;
-  launch_adj2(c->index.view(), c->P, c->cot.p, cot3 ? c->cot.p + nbm : nullptr, gscale, c->gfix.p,
-              c->gfix.p + n, c->work.p, s, variant);
-  finish_grad(c, gscale, grad_w, c->ev[1]);
+  const double* dc3 = cot3 ? c->cot.p + nbm : nullptr;
+  const int variant = pick_adj2_layout(c, c->index.view(), c->cot.p, dc3, gscale, c->gfix.p,
+                                       c->gfix.p + n, c->work.p, s);
+  GR_CUDA_TRY(cudaEventRecord(c->ev[2], s));  // after any tuning runs
+  launch_adj2(c->index.view(), c->P, c->cot.p, dc3, gscale, c->gfix.p, c->gfix.p + n, c->work.p, s,
+              variant);
+  finish_grad(c, gscale, grad_w, c->ev[2]);
   c->st.ms_index = ev_ms(c->ev[0], c->ev[1]);
   c->st.ms_total = c->st.ms_index + c->st.ms_query;
   c->st.n_points = n;
@@ -1346,7 +1414,9 @@ int gr_adjoint_3pcf(gr_ctx* c, const double* cot2, const double* cot3, double* g
   const int nc = ncfg * nmu;
   const int64_t n = c->n;
   const double cmax = max_abs(cot2, nc) + max_abs(cot3, nc);
-  const double gscale = fix_scale(3.0 * cmax * c->wmax * c->wmax);
+  // 2^10 below the per-term bound: the kernel sums up to 1023 terms of one
+  // root per neighbour in signed 64 bits before the 128-bit totals
+  const double gscale = fix_scale(3.0 * cmax * c->wmax * c->wmax * 1024.0);
   std::vector<uint8_t> nt;
   normal_table(nmu, nt);
   c->normal_dev.reserve(nt.size());
@@ -1377,6 +1447,8 @@ int gr_adjoint_3pcf(gr_ctx* c, const double* cot2, const double* cot3, double* g
   make_rank_tables(T.rank, c->nbins, 3);
   T.P = c->P;
   T.geo = c->clique_mode == 1 ? 0 : 1;  // faster for the adjoint at every degree measured
+  T.maxdeg = (int)std::min<int64_t>(c->csr.max_deg, 1 << 30);
+  T.long_geo = c->clique_mode != 1;
   const CSRView G = c->csr.view();
   std::memset(&c->st, 0, sizeof(c->st));
   launch_adj3(c->index.view(), G, T, c->cot.p, cot3 ? c->cot.p + nc : nullptr, gscale, c->gfix.p,

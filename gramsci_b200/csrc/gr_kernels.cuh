@@ -44,6 +44,9 @@ struct TriParams {
   double fscale[4];        // fixed-point scale of the products with 0..3 randoms
   PairParams P;            // edge predicate and binning of the graph
   int geo;                 // 1: third edges by the geometric pair test, 0: hash probes of rows
+  int maxdeg;              // longest upper row
+  int long_geo;            // 1: rows beyond cap take a second, geometric launch
+  int kmin, kskip;         // roots handled by one launch: kmin < row length <= kskip
 };
 
 // 3PCF: triangles p < a < c enumerated once over the upper CSR; each adds to

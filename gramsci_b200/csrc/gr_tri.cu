@@ -34,6 +34,8 @@
 // fixed point with a scale per number of randoms.
 #include "gr_kernels.cuh"
 
+#include <algorithm>
+
 namespace gr {
 
 namespace {
@@ -87,7 +89,7 @@ __host__ __device__ inline TriLayout tri_layout(int nh, int nmu, int nbins, int 
   L.o_pos = w;  if (geo) w += (size_t)cap * 16;  // float4 position per neighbour
   L.o_rs = w;   if (!geo) w += (size_t)cap * 8;
   L.o_w = w;    if (weighted || adj) w += (size_t)cap * 8;
-  L.o_g = w;    if (adj) w += (size_t)cap * 16;  // gradient (lo, hi) per neighbour
+  L.o_g = w;    if (adj) w += (size_t)cap * 8;  // signed 64-bit gradient per neighbour
   L.o_col = w;  w += (size_t)cap * 4;
   L.o_mo = w;   w += (size_t)cap * 8;  // (catalogue id << 32) | flags << 24 | edge meta
   L.o_len = w;  if (!geo) w += (size_t)cap * 4;
@@ -181,7 +183,10 @@ __device__ __forceinline__ int tri_bin(const TriCtx& X, uint8_t fp, int op, doub
 // (cot2 - [all random] cot3)[cfg, m_r] (N3 accumulates minus the product);
 // with C the sum, dL/dw_p += C w_a w_c, dL/dw_a += C w_p w_c, dL/dw_c +=
 // C w_p w_a.  p's term goes to the lane's register accumulator, a's and c's
-// to the given fixed-point accumulators.
+// to the given fixed-point accumulators: S64, signed 64-bit partial sums of
+// one root (alo / clo; the scale leaves room for 1024 terms), else 128-bit
+// (lo, hi) pairs.
+template <bool S64>
 __device__ __forceinline__ int tri_grad(const TriCtx& X, uint8_t fp, int op, double wp,
                                         uint8_t fa, int oa, double wa, uint8_t fc, int oc,
                                         double wc, uint32_t mpa, uint32_t mpc, uint32_t mac,
@@ -209,8 +214,13 @@ __device__ __forceinline__ int tri_grad(const TriCtx& X, uint8_t fp, int op, dou
   }
   if (C != 0.0) {
     fix_acc(racc, C * (wa * wc), X.gscale);
-    fix_add(alo, ahi, C * (wp * wc), X.gscale);
-    fix_add(clo, chi, C * (wp * wa), X.gscale);
+    if (S64) {
+      atomicAdd(alo, (unsigned long long)__double2ll_rn(C * (wp * wc) * X.gscale));
+      atomicAdd(clo, (unsigned long long)__double2ll_rn(C * (wp * wa) * X.gscale));
+    } else {
+      fix_add(alo, ahi, C * (wp * wc), X.gscale);
+      fix_add(clo, chi, C * (wp * wa), X.gscale);
+    }
   }
   return n;
 }
@@ -319,10 +329,9 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
   unsigned long long* s_mo = reinterpret_cast<unsigned long long*>(wb + L.o_mo);
   int* s_len = reinterpret_cast<int*>(wb + L.o_len);
   uint32_t* s_hkey = reinterpret_cast<uint32_t*>(wb + L.o_hkey);
-  // queue entry: (meta of edge (a, c) << 32) | row of a | (row of c << 8)
+  // queue entry: (meta of edge (a, c) << 32) | row of a | (row of c << 16)
   unsigned long long* s_q = reinterpret_cast<unsigned long long*>(wb + L.o_q);
-  unsigned long long* s_glo = reinterpret_cast<unsigned long long*>(wb + L.o_g);
-  unsigned long long* s_ghi = s_glo + T.cap;
+  unsigned long long* s_g = reinterpret_cast<unsigned long long*>(wb + L.o_g);
   const int lg_max = hash_lg_max(T.cap);
 
   unsigned long long tris = 0, rooted = 0, probes = 0;
@@ -330,7 +339,7 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
   // one queued triangle (p, a = row qx, c = row qy) with edge meta (a, c)
   auto drain_one = [&](int e, uint8_t fp, int op, double wp, Fix128& racc) -> int {
     const unsigned long long qe = s_q[e];
-    const int qx = (int)(qe & 0xffu), qy = (int)((qe >> 8) & 0xffu);
+    const int qx = (int)(qe & 0xffffu), qy = (int)((qe >> 16) & 0xffffu);
     uint32_t mac = (uint32_t)(qe >> 32);
     if (GEO) {
       // bins of the edge (a, c) exactly as the graph build computes them
@@ -344,8 +353,8 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
     const int oa = (int)(moa >> 32), oc = (int)(moc >> 32);
     const uint8_t fa = (uint8_t)(ma >> 24), fc = (uint8_t)(mc >> 24);
     if (ADJ)
-      return tri_grad(X, fp, op, wp, fa, oa, s_w[qx], fc, oc, s_w[qy], ma, mc, mac, racc,
-                      &s_glo[qx], &s_ghi[qx], &s_glo[qy], &s_ghi[qy]);
+      return tri_grad<true>(X, fp, op, wp, fa, oa, s_w[qx], fc, oc, s_w[qy], ma, mc, mac, racc,
+                            &s_g[qx], nullptr, &s_g[qy], nullptr);
     return tri_bin<WEIGHTED, COUNTS>(X, fp, op, wp, fa, oa, WEIGHTED ? s_w[qx] : 0.0, fc, oc,
                                      WEIGHTED ? s_w[qy] : 0.0, ma, mc, mac);
   };
@@ -359,7 +368,7 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
     for (int p = base_root; p < end_root; ++p) {
       const int64_t b0 = G.start[p];
       const int k = G.len[p];
-      if (k < 2) continue;
+      if (k < 2 || k <= T.kmin || k > T.kskip) continue;  // rows of the other launch
       const uint8_t fp = C.flags[p];
       const int op = C.orig[p];
       const double wp = (WEIGHTED || ADJ) ? C.w[p] : 0.0;
@@ -394,10 +403,7 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
             s_mo[x] = ((unsigned long long)(uint32_t)C.orig[a] << 32) |
                       (rec_meta(r) | ((uint32_t)C.flags[a] << 24));
             if (WEIGHTED || ADJ) s_w[x] = C.w[a];
-            if (ADJ) {
-              s_glo[x] = 0ull;
-              s_ghi[x] = 0ull;
-            }
+            if (ADJ) s_g[x] = 0ull;
             if (!GEO) {
               const uint32_t off = (uint32_t)(a - p);
               const uint32_t key = (off << 8) | (uint32_t)x;
@@ -437,7 +443,7 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
               hit = r == 1;
             }
             const unsigned m = __ballot_sync(0xffffffffu, hit);
-            if (hit) s_q[qn + __popc(m & lt)] = (unsigned long long)(x | (y << 8));
+            if (hit) s_q[qn + __popc(m & lt)] = (unsigned long long)(x | (y << 16));
             qn += __popc(m);
             if (qn >= 32) {
               __syncwarp();
@@ -527,7 +533,7 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
               const unsigned m = __ballot_sync(0xffffffffu, hit);
               if (hit) {
                 const int pos = qn + __popc(m & lt);
-                s_q[pos] = ((unsigned long long)mac << 32) | (uint32_t)(ox[u] | (y << 8));
+                s_q[pos] = ((unsigned long long)mac << 32) | (uint32_t)(ox[u] | (y << 16));
               }
               qn += __popc(m);
             }
@@ -551,8 +557,8 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
           // flush the neighbours' gradient accumulators of this root
           __syncwarp();
           for (int x = lane; x < k; x += 32) {
-            const unsigned long long lo = s_glo[x], hi = s_ghi[x];
-            if (lo | hi) fix_merge(&g_lo[s_col[x]], &g_hi[s_col[x]], lo, hi);
+            const unsigned long long v = s_g[x];
+            if (v) fix_merge(&g_lo[s_col[x]], &g_hi[s_col[x]], v, (long long)v < 0 ? ~0ull : 0ull);
           }
         }
       } else {
@@ -574,7 +580,7 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
             const int y = x + 1 + lower_bound_g(rowp + x + 1, k - x - 1, c);
             if (y < k && rec_col(rowp[y]) == c) {
               const int nroot =
-                  ADJ ? tri_grad(X, fp, op, wp, fa, oa, wa, C.flags[c], C.orig[c], C.w[c], mpa,
+                  ADJ ? tri_grad<false>(X, fp, op, wp, fa, oa, wa, C.flags[c], C.orig[c], C.w[c], mpa,
                                  rec_meta(rowp[y]), rec_meta(r), racc, &g_lo[a], &g_hi[a], &g_lo[c],
                                  &g_hi[c])
                       : tri_bin<WEIGHTED, COUNTS>(X, fp, op, wp, fa, oa, wa, C.flags[c], C.orig[c],
@@ -645,11 +651,11 @@ size_t tri3_smem_bytes(const TriParams& T, bool weighted, bool counts) {
       .total;
 }
 
-void launch_tri3(const DevCatalog& C, const CSRView& G, const TriParams& T, bool weighted,
-                 bool counts, unsigned long long* g_cnt, unsigned long long* g_lim,
-                 unsigned long long* stats, int* work, cudaStream_t s) {
-  if (C.n <= 0) return;
-  if (!weighted) counts = true;
+// One launch of the triangle kernel for the roots kmin < k <= kskip of T.
+static void launch_tri3_part(const DevCatalog& C, const CSRView& G, const TriParams& T,
+                             bool weighted, bool counts, unsigned long long* g_cnt,
+                             unsigned long long* g_lim, unsigned long long* stats, int* work,
+                             cudaStream_t s) {
   const int nh = T.ncfg * T.nmu * 4;
   const bool shist = tri3_shist(nh, weighted, counts);
   const bool geo = T.geo != 0;
@@ -683,10 +689,43 @@ void launch_tri3(const DevCatalog& C, const CSRView& G, const TriParams& T, bool
   GR_CHECK_LAUNCH();
 }
 
-void launch_adj3(const DevCatalog& C, const CSRView& G, const TriParams& T, const double* cot2,
-                 const double* cot3, double gscale, unsigned long long* g_lo,
-                 unsigned long long* g_hi, unsigned long long* stats, int* work, cudaStream_t s) {
+// Rows longer than the main launch's capacity (at most kTriCapShort, which
+// keeps 16 to 32 warps per block) go to a second, geometric launch whose
+// capacity fits them (up to kTriCapLong, fewer warps); rows beyond that take
+// the global-memory path.  The two launches add into the same outputs.
+constexpr int kTriCapShort = 256;
+constexpr int kTriCapLong = 1024;
+
+static void tri3_split(const TriParams& T, TriParams& A, TriParams& B, bool& two) {
+  A = T;
+  A.kmin = 0;
+  A.kskip = 0x7fffffff;
+  two = T.long_geo && T.maxdeg > T.cap && T.cap >= kTriCapShort;
+  if (!two) return;
+  A.kskip = T.cap;
+  B = T;
+  B.geo = 1;
+  B.cap = (int)std::min<int64_t>(((int64_t)T.maxdeg + 31) / 32 * 32, kTriCapLong);
+  B.kmin = T.cap;
+  B.kskip = 0x7fffffff;
+}
+
+void launch_tri3(const DevCatalog& C, const CSRView& G, const TriParams& T, bool weighted,
+                 bool counts, unsigned long long* g_cnt, unsigned long long* g_lim,
+                 unsigned long long* stats, int* work, cudaStream_t s) {
   if (C.n <= 0) return;
+  if (!weighted) counts = true;
+  TriParams A, B;
+  bool two = false;
+  tri3_split(T, A, B, two);
+  launch_tri3_part(C, G, A, weighted, counts, g_cnt, g_lim, stats, work, s);
+  if (two) launch_tri3_part(C, G, B, weighted, counts, g_cnt, g_lim, stats, work, s);
+}
+
+static void launch_adj3_part(const DevCatalog& C, const CSRView& G, const TriParams& T,
+                             const double* cot2, const double* cot3, double gscale,
+                             unsigned long long* g_lo, unsigned long long* g_hi,
+                             unsigned long long* stats, int* work, cudaStream_t s) {
   const int nh = T.ncfg * T.nmu * 4;
   const bool geo = T.geo != 0;
   const int nw = tri3_warps(T, false, false, false, true, geo);
@@ -706,6 +745,17 @@ void launch_adj3(const DevCatalog& C, const CSRView& G, const TriParams& T, cons
   kfn<<<(unsigned)blocks, nw * 32, smem, s>>>(C, G, T, nullptr, nullptr, stats, work, cot2, cot3,
                                               gscale, g_lo, g_hi);
   GR_CHECK_LAUNCH();
+}
+
+void launch_adj3(const DevCatalog& C, const CSRView& G, const TriParams& T, const double* cot2,
+                 const double* cot3, double gscale, unsigned long long* g_lo,
+                 unsigned long long* g_hi, unsigned long long* stats, int* work, cudaStream_t s) {
+  if (C.n <= 0) return;
+  TriParams A, B;
+  bool two = false;
+  tri3_split(T, A, B, two);
+  launch_adj3_part(C, G, A, cot2, cot3, gscale, g_lo, g_hi, stats, work, s);
+  if (two) launch_adj3_part(C, G, B, cot2, cot3, gscale, g_lo, g_hi, stats, work, s);
 }
 
 }  // namespace gr
