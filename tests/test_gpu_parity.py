@@ -247,7 +247,7 @@ def test_tetra(gpu_ctx, oracle, weighted):
     assert _rel(got["dsum"], ref["dsum"]) < RTOL
 
 
-@pytest.mark.parametrize("query", ["graph", "2pcf", "3pcf"])
+@pytest.mark.parametrize("query", ["graph", "2pcf", "3pcf", "4pcf"])
 def test_log_bins(gpu_ctx, oracle, query):
     """-log bins: the library's FP64 path (log10 on the device, glibc's on
     the oracle side).  Both are within an ulp, so a bin could differ only for
@@ -265,8 +265,24 @@ def test_log_bins(gpu_ctx, oracle, query):
         assert len(np.unique(got[2])) == sp["nbins"]
     elif query == "2pcf":
         _check_sums(gpu_ctx.count_2pcf(), G.pcf2(w, cat.n_data))
-    else:
+    elif query == "3pcf":
         _check_sums(gpu_ctx.count_3pcf(), G.pcf3(w, cat.n_data))
+    else:
+        # both 4-clique kernels (the geometric one bins its inner edges from
+        # the positions, here in FP64 with log10)
+        G4 = oracle.Graph(cat.xyz, rmin, sp["rmax"], 4, 1, logbins=True)
+        gpu_ctx.set_bins(rmin, sp["rmax"], 4, 1, logbins=True)
+        ref = G4.pcf4(w, cat.n_data)
+        for mode in ("geometric", "hash"):
+            gpu_ctx.set_clique_mode(mode)
+            try:
+                got = gpu_ctx.count_4pcf()
+            finally:
+                gpu_ctx.set_clique_mode("auto")
+            assert int(ref["counts"].sum()) > 0
+            assert np.array_equal(got["counts"], ref["counts"])
+            assert np.array_equal(got["dcount"], ref["dcount"])
+            assert _rel(got["catsum"], ref["catsum"]) < RTOL
 
 
 def test_3pcf_without_counts_and_skewed_weights(gpu_ctx, oracle):
