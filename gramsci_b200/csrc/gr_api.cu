@@ -764,6 +764,7 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
   cudaEvent_t q0;
   GR_CUDA_TRY(cudaEventCreate(&q0));
   c->work.reserve(4);
+  int tri_launches = 0;
   for (int attempt = 0; attempt < 2; ++attempt) {
     const bool spec = can_spec && attempt == 0;
     GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
@@ -771,9 +772,13 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
     GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
     if (!reuse) build_csr(c, spec);
     GR_CUDA_TRY(cudaEventRecord(c->ev[2], s));
-    GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nh, s));
-    GR_CUDA_TRY(cudaMemsetAsync(c->hfix.p, 0, sizeof(unsigned long long) * 2 * nh, s));
-    GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
+    {
+      ZeroList z;
+      z.add(c->hcnt.p, sizeof(unsigned long long) * nh);
+      z.add(c->hfix.p, sizeof(unsigned long long) * 2 * nh);
+      z.add(c->stats.p, sizeof(unsigned long long) * 8);
+      zero_async(z, s);
+    }
     TriParams T{};
     T.nbins = c->nbins;
     T.nmu = nmu;
@@ -790,8 +795,8 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
     T.long_geo = c->clique_mode != 1;
     const CSRView G = c->csr.view();
     GR_CUDA_TRY(cudaEventRecord(q0, s));
-    launch_tri3(c->index.view(), G, T, weighted, want_counts, c->hcnt.p, c->hfix.p, c->stats.p,
-                c->work.p, s);
+    tri_launches = 1 + launch_tri3(c->index.view(), G, T, weighted, want_counts, c->hcnt.p,
+                                   c->hfix.p, c->stats.p, c->work.p, s);  // + the zero fill
     GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
     if (want_counts)
       GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
@@ -853,7 +858,7 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
   c->st.upper_edges = c->csr.n_edges;
   c->st.fp64_rechecks = (int64_t)gst[0];
   c->st.candidates = (int64_t)gst[1];
-  c->st.kernel_launches = c->index.launches + c->csr.launches + 1;
+  c->st.kernel_launches = (reuse ? 0 : c->index.launches + c->csr.launches) + tri_launches;
   GR_API_END(c)
 }
 

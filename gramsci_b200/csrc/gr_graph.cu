@@ -292,12 +292,15 @@ void UpperCSR::build(const DevCatalog& C, const PairParams& P, cudaStream_t s, b
   unsigned long long hc[4] = {0, 0, 0, 0}, hs[3] = {0, 0, 0};
   int64_t need = 0;
   for (int attempt = 0; attempt < 2; ++attempt) {
-    GR_CUDA_TRY(cudaMemsetAsync(deg_up.p, 0, sizeof(int) * (n + 1), s));
-    GR_CUDA_TRY(cudaMemsetAsync(rstart.p, 0, sizeof(int64_t) * (n + 1), s));
-    GR_CUDA_TRY(cudaMemsetAsync(deg_full.p, 0, sizeof(int) * (n + 1), s));
-    GR_CUDA_TRY(cudaMemsetAsync(stats.p, 0, sizeof(unsigned long long) * 4, s));
-    GR_CUDA_TRY(cudaMemsetAsync(ctl.p, 0, sizeof(unsigned long long) * 4, s));
-    GR_CUDA_TRY(cudaMemsetAsync(work.p, 0, sizeof(int) * 2, s));
+    ZeroList z;
+    z.add(deg_up.p, sizeof(int) * (n + 1));
+    z.add(rstart.p, sizeof(int64_t) * (n + 1));
+    z.add(deg_full.p, sizeof(int) * (n + 1));
+    z.add(stats.p, sizeof(unsigned long long) * 4);
+    z.add(ctl.p, sizeof(unsigned long long) * 4);
+    z.add(work.p, sizeof(int) * 2);
+    zero_async(z, s);
+    launches++;
     if (n > 0) {
       const int64_t cap = (int64_t)scratch.n;
       if (P.f32)

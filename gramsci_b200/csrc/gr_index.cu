@@ -430,6 +430,41 @@ size_t scan_tmp_need(int64_t n) {
 
 }  // namespace
 
+namespace {
+
+// Buffers from cudaMalloc start 256-byte aligned; each is zeroed with 16-byte
+// stores for its body and 4-byte stores for a tail (sizes are multiples of 4).
+__global__ void zero_many_kernel(ZeroList z) {
+  const size_t tid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const size_t nthr = (size_t)gridDim.x * blockDim.x;
+  for (int k = 0; k < z.n; ++k) {
+    const size_t nv = z.bytes[k] / 16;
+    uint4* v = reinterpret_cast<uint4*>(z.p[k]);
+    for (size_t i = tid; i < nv; i += nthr) v[i] = make_uint4(0u, 0u, 0u, 0u);
+    const size_t tail = (z.bytes[k] - nv * 16) / 4;
+    uint32_t* t = reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(z.p[k]) + nv * 16);
+    if (tid < tail) t[tid] = 0u;
+  }
+}
+
+}  // namespace
+
+void zero_async(const ZeroList& z, cudaStream_t s) {
+  if (z.n == 0) return;
+  size_t total = 0;
+  for (int k = 0; k < z.n; ++k) {
+    if ((reinterpret_cast<uintptr_t>(z.p[k]) & 15) != 0 || (z.bytes[k] & 3) != 0)
+      throw Error{-2, "zero_async: buffer not 16-byte aligned or size not a multiple of 4"};
+    total += z.bytes[k];
+  }
+  const size_t threads = 256;
+  size_t blocks = (total / 16 + threads - 1) / threads;
+  if (blocks < 1) blocks = 1;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  zero_many_kernel<<<(unsigned)blocks, (unsigned)threads, 0, s>>>(z);
+  GR_CHECK_LAUNCH();
+}
+
 void scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s, DevBuf<int64_t>& tmp) {
   size_t need = scan_tmp_need(n);
   if (tmp.n < need) tmp.reserve(need);

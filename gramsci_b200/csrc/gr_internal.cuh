@@ -486,6 +486,21 @@ double fix_scale(double max_abs_product);
 double fix_value(unsigned long long lo, unsigned long long hi, double scale);
 
 // -------------------------------------------------------------- host launch --
+// Zero up to 8 device buffers in one launch (instead of one memset each).
+struct ZeroList {
+  void* p[8];
+  size_t bytes[8];
+  int n = 0;
+  void add(void* ptr, size_t b) {
+    if (b > 0) {
+      p[n] = ptr;
+      bytes[n] = b;
+      ++n;
+    }
+  }
+};
+void zero_async(const ZeroList& z, cudaStream_t s);
+
 // Exclusive scan of n int32 values into n+1 int64 values (out[n] = total).
 void scan_i32_to_i64(const int* in, int64_t* out, int64_t n, cudaStream_t s, DevBuf<int64_t>& tmp);
 void scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s, DevBuf<int64_t>& tmp);

@@ -55,8 +55,9 @@ struct TriParams {
 // words, weighted only) must be zeroed.  stats: [0] distinct triangles binned, [1] rooted
 // incidences, [2] intersection probes.
 // work: one device int used as the dynamic root counter (reset by the launch).
+// Returns the number of kernel launches (2 when long rows take a second one).
 size_t tri3_smem_bytes(const TriParams& T, bool weighted, bool counts);
-void launch_tri3(const DevCatalog& C, const CSRView& G, const TriParams& T, bool weighted,
+int launch_tri3(const DevCatalog& C, const CSRView& G, const TriParams& T, bool weighted,
                  bool counts, unsigned long long* g_cnt, unsigned long long* g_lim,
                  unsigned long long* stats, int* work, cudaStream_t s);
 
@@ -68,7 +69,7 @@ void launch_tri3(const DevCatalog& C, const CSRView& G, const TriParams& T, bool
 void launch_adj2(const DevCatalog& C, const PairParams& P, const double* cot2, const double* cot3,
                  double gscale, unsigned long long* g_lo, unsigned long long* g_hi, int* work,
                  cudaStream_t s, int variant = kPairWarpCell);
-void launch_adj3(const DevCatalog& C, const CSRView& G, const TriParams& T, const double* cot2,
+int launch_adj3(const DevCatalog& C, const CSRView& G, const TriParams& T, const double* cot2,
                  const double* cot3, double gscale, unsigned long long* g_lo,
                  unsigned long long* g_hi, unsigned long long* stats, int* work, cudaStream_t s);
 void launch_grad_finish(int n, const int* orig, const unsigned long long* g_lo,

@@ -710,16 +710,17 @@ static void tri3_split(const TriParams& T, TriParams& A, TriParams& B, bool& two
   B.kskip = 0x7fffffff;
 }
 
-void launch_tri3(const DevCatalog& C, const CSRView& G, const TriParams& T, bool weighted,
+int launch_tri3(const DevCatalog& C, const CSRView& G, const TriParams& T, bool weighted,
                  bool counts, unsigned long long* g_cnt, unsigned long long* g_lim,
                  unsigned long long* stats, int* work, cudaStream_t s) {
-  if (C.n <= 0) return;
+  if (C.n <= 0) return 0;
   if (!weighted) counts = true;
   TriParams A, B;
   bool two = false;
   tri3_split(T, A, B, two);
   launch_tri3_part(C, G, A, weighted, counts, g_cnt, g_lim, stats, work, s);
   if (two) launch_tri3_part(C, G, B, weighted, counts, g_cnt, g_lim, stats, work, s);
+  return two ? 2 : 1;
 }
 
 static void launch_adj3_part(const DevCatalog& C, const CSRView& G, const TriParams& T,
@@ -747,15 +748,16 @@ static void launch_adj3_part(const DevCatalog& C, const CSRView& G, const TriPar
   GR_CHECK_LAUNCH();
 }
 
-void launch_adj3(const DevCatalog& C, const CSRView& G, const TriParams& T, const double* cot2,
+int launch_adj3(const DevCatalog& C, const CSRView& G, const TriParams& T, const double* cot2,
                  const double* cot3, double gscale, unsigned long long* g_lo,
                  unsigned long long* g_hi, unsigned long long* stats, int* work, cudaStream_t s) {
-  if (C.n <= 0) return;
+  if (C.n <= 0) return 0;
   TriParams A, B;
   bool two = false;
   tri3_split(T, A, B, two);
   launch_adj3_part(C, G, A, cot2, cot3, gscale, g_lo, g_hi, stats, work, s);
   if (two) launch_adj3_part(C, G, B, cot2, cot3, gscale, g_lo, g_hi, stats, work, s);
+  return two ? 2 : 1;
 }
 
 }  // namespace gr
