@@ -73,7 +73,7 @@ struct gr_ctx {
   double batch_fscale = 1.0;
   cudaEvent_t bev[2] = {nullptr, nullptr};
   gr_stats st{};
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // [4]: query start
 
   cudaStream_t stream() const { return user ? user : own; }
 };
@@ -374,7 +374,7 @@ void require_ready(gr_ctx* c) {
 }
 
 void ensure_events(gr_ctx* c) {
-  for (int k = 0; k < 4; ++k)
+  for (int k = 0; k < 5; ++k)
     if (!c->ev[k]) GR_CUDA_TRY(cudaEventCreate(&c->ev[k]));
 }
 
@@ -456,7 +456,7 @@ int gr_destroy(gr_ctx* c) {
   if (!c) return GR_E_ARG;
   cudaSetDevice(c->device);
   if (c->own) cudaStreamSynchronize(c->own);
-  for (int k = 0; k < 4; ++k)
+  for (int k = 0; k < 5; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
   for (int k = 0; k < 2; ++k)
     if (c->bev[k]) cudaEventDestroy(c->bev[k]);
@@ -761,8 +761,7 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
   std::vector<unsigned long long> hc(nh, 0ull), hf(2 * nh, 0ull);
   std::vector<double> hs(nh, 0.0);
   unsigned long long st[8];
-  cudaEvent_t q0;
-  GR_CUDA_TRY(cudaEventCreate(&q0));
+  cudaEvent_t q0 = c->ev[4];  // owned by the context
   c->work.reserve(4);
   int tri_launches = 0;
   for (int attempt = 0; attempt < 2; ++attempt) {
@@ -849,7 +848,6 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
   c->st.ms_graph = ev_ms(c->ev[1], c->ev[2]);
   c->st.ms_query = ev_ms(q0, c->ev[3]);
   c->st.ms_total = c->st.ms_index + c->st.ms_graph + c->st.ms_query;
-  cudaEventDestroy(q0);
   c->st.n_points = c->n;
   c->st.n_edges = 2 * c->csr.n_edges;
   c->st.tuples = (int64_t)st[0];
@@ -930,8 +928,7 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   Q.P = c->P;
   Q.geo = quad_geometric(c, Q.cap, nb, weighted);
   const CSRView G = c->csr.view();
-  cudaEvent_t q0;
-  GR_CUDA_TRY(cudaEventCreate(&q0));
+  cudaEvent_t q0 = c->ev[4];  // owned by the context
   GR_CUDA_TRY(cudaEventRecord(q0, s));
   c->work.reserve(4);
   std::vector<unsigned long long> hc(nh), dc(nd), hf, df;
@@ -1011,7 +1008,6 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   c->st.ms_graph = ev_ms(c->ev[1], c->ev[2]);
   c->st.ms_query = ev_ms(q0, c->ev[3]);
   c->st.ms_total = c->st.ms_index + c->st.ms_graph + c->st.ms_query;
-  cudaEventDestroy(q0);
   c->st.n_points = c->n;
   c->st.n_edges = 2 * c->csr.n_edges;
   c->st.tuples = (int64_t)st[0];
