@@ -587,6 +587,21 @@ int gr_set_option(gr_ctx* c, int32_t key, int64_t value) {
   GR_API_END(c)
 }
 
+// Two timing events destroyed on every exit path (the tuners below).
+struct ScopedEvents {
+  cudaEvent_t a = nullptr, b = nullptr;
+  ScopedEvents() {
+    GR_CUDA_TRY(cudaEventCreate(&a));
+    GR_CUDA_TRY(cudaEventCreate(&b));
+  }
+  ~ScopedEvents() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+  ScopedEvents(const ScopedEvents&) = delete;
+  ScopedEvents& operator=(const ScopedEvents&) = delete;
+};
+
 // Pair-sweep variant for a catalogue layout: cached per workload class or
 // timed now (histograms are reset by the caller afterwards).
 static int pick_pair2_variant(gr_ctx* c, const DevCatalog& C, bool weighted, double fscale,
@@ -614,9 +629,8 @@ static int pick_pair2_variant(gr_ctx* c, const DevCatalog& C, bool weighted, dou
     if (it != T.choice.end()) return it->second;
   }
   const int nh = c->nbins * c->nmu * 4;
-  cudaEvent_t a, b;
-  GR_CUDA_TRY(cudaEventCreate(&a));
-  GR_CUDA_TRY(cudaEventCreate(&b));
+  ScopedEvents ev;
+  cudaEvent_t a = ev.a, b = ev.b;
   // every variant once untimed (its first launch loads its code), then the
   // fastest of three interleaved rounds
   float t[kPairVariants];
@@ -640,8 +654,6 @@ static int pick_pair2_variant(gr_ctx* c, const DevCatalog& C, bool weighted, dou
   int best = kPairWarpCell;
   for (int v = 1; v < kPairVariants; ++v)
     if (t[v] < t[best]) best = v;
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
   std::lock_guard<std::mutex> lock(T.mu);
   T.choice[key] = best;
   T.save();
@@ -1342,9 +1354,8 @@ static int pick_adj2_layout(gr_ctx* c, const DevCatalog& C, const double* c2, co
     if (it != T.choice.end()) return it->second;
   }
   const int layouts[3] = {kPairWarpCell, kPairDense128, kPairDense256};
-  cudaEvent_t a, b;
-  GR_CUDA_TRY(cudaEventCreate(&a));
-  GR_CUDA_TRY(cudaEventCreate(&b));
+  ScopedEvents ev;
+  cudaEvent_t a = ev.a, b = ev.b;
   float t[3] = {1e30f, 1e30f, 1e30f};
   for (int v = 0; v < 3; ++v)
     launch_adj2(C, c->P, c2, c3, gscale, g_lo, g_hi, work, s, layouts[v]);
@@ -1358,8 +1369,6 @@ static int pick_adj2_layout(gr_ctx* c, const DevCatalog& C, const double* c2, co
       cudaEventElapsedTime(&ms, a, b);
       t[v] = std::min(t[v], ms);
     }
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
   int best = 0;
   for (int v = 1; v < 3; ++v)
     if (t[v] < t[best]) best = v;
