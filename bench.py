@@ -13,6 +13,8 @@ e2e        the same through the public API with host inputs: pinned host ->
 roofline   the triangle kernel: algorithmic bytes / its CUDA-event time
 cpu_baseline  the CPU restatement of the reference algorithm (kd-tree range
            search, id-sorted rows, the reference's 3PCF loop) on the host cores
+fp64_path  the same steps with every pair in FP64 (GR_OPT_PRECISION=1), and
+           whether its counts and sums are identical to the FP32 path's
 
 --impl reference times that CPU restatement on the same workload (it is the
 reference's algorithm; the Fortran reference itself cannot be built here).
@@ -333,6 +335,32 @@ def run_ours(args):
         "clocks": clocks,
         "gpu_launches": launches,
     }
+    if world == 1 and args.precision == "f32":
+        # configs[1]'s comparison: the same steps through the plain FP64 path
+        # (every pair in FP64 arithmetic); results must be identical
+        ref32 = ctx.count_3pcf()
+        ctx.set_catalog(xyz_d, w_d, cat.n_data)
+        ctx.set_precision("f64")
+        for _ in range(args.warmup):
+            ctx.count_3pcf(counts=False)
+        n64 = max(1, min(args.steps, 50))
+        ev64 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                for _ in range(n64)]
+        for k in range(n64):
+            flush.zero_()
+            ev64[k][0].record(stream)
+            ctx.count_3pcf(counts=False)
+            ev64[k][1].record(stream)
+        torch.cuda.synchronize()
+        ms64 = float(sum(a.elapsed_time(b) for a, b in ev64)) / n64
+        ref64 = ctx.count_3pcf()
+        st64 = ctx.stats()
+        same = all(np.array_equal(ref32[k], ref64[k]) for k in ("counts", "catsum", "N2", "N3"))
+        line["fp64_path"] = {"ms_per_step": ms64, "value": st64["tuples"] / (ms64 / 1e3),
+                             "steps": n64, "identical_to_fp32_path": bool(same),
+                             "phase_ms": {"index": st64["ms_index"], "graph": st64["ms_graph"],
+                                          "query": st64["ms_query"]}}
+        ctx.set_precision("f32")
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         r = cpu_reference_run(cat, w, sp, threads)
