@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(kAdjThreads) adj2_kernel(DevCatalog C, PairPar
         Fix128 acc = {0ull, 0ull};
         for (int f = lane; f < tn; f += 32) {
           const int q = s_lab[wib][f];
-          if (q == p) continue;
+          if (q == p || both_buffer(pi, s_pos[wib][f])) continue;
           int b, mf, mr;
           if (!adj_edge<F32>(C, P, p, q, pi, s_pos[wib][f], b, mf, mr)) continue;
           const uint8_t fq = C.flags[q];
@@ -206,7 +206,7 @@ __global__ void __launch_bounds__(NT) adj2_dense_kernel(DevCatalog C, PairParams
         if (!act) continue;
         for (int f = 0; f < tn; ++f) {
           const int q = s_lab[f];
-          if (q == p) continue;
+          if (q == p || both_buffer(pi, s_pos[f])) continue;
           int b, mf, mr;
           if (!adj_edge<F32>(C, P, p, q, pi, s_pos[f], b, mf, mr)) continue;
           const double c = pair_coef(s_c2, s_c3, P.nbins, b, mf, mr, fp, s_flag[f]);

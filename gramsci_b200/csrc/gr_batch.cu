@@ -199,11 +199,14 @@ __global__ void b_gather_kernel(int64_t m, const int* __restrict__ perm,
     const int k = perm[p];
     const int i = m_orig[k];
     const double x = xyz[3 * (int64_t)i], y = xyz[3 * (int64_t)i + 1], z = xyz[3 * (int64_t)i + 2];
-    pos4[p] = make_float4(__double2float_rn(x), __double2float_rn(y), __double2float_rn(z), 0.f);
+    const uint8_t f = m_flag[k];
+    // the fourth component marks buffer points (pair sweeps skip pairs of two)
+    pos4[p] = make_float4(__double2float_rn(x), __double2float_rn(y), __double2float_rn(z),
+                          (f & FLAG_BUFFER) ? 1.f : 0.f);
     posd[p] = make_double4(x, y, z, w[i]);
     wl[p] = w[i];
     orig[p] = i;
-    flags[p] = m_flag[k];
+    flags[p] = f;
     cell_key[p] = m_key[k];
   }
 }

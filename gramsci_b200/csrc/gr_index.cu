@@ -157,12 +157,14 @@ __global__ void gather_kernel(int64_t n, const int* __restrict__ perm,
     int i = perm[p];
     double x = xyz[3 * (int64_t)i + 0], y = xyz[3 * (int64_t)i + 1], z = xyz[3 * (int64_t)i + 2];
     double wi = w[i];
-    pos4[p] = make_float4(__double2float_rn(x), __double2float_rn(y), __double2float_rn(z), 0.0f);
+    uint8_t f = (i >= n_data) ? FLAG_RANDOM : 0;
+    if (buffer && buffer[i] == 1) f |= FLAG_BUFFER;
+    // the fourth component marks buffer points (pair sweeps skip pairs of two)
+    pos4[p] = make_float4(__double2float_rn(x), __double2float_rn(y), __double2float_rn(z),
+                          (f & FLAG_BUFFER) ? 1.0f : 0.0f);
     posd[p] = make_double4(x, y, z, wi);
     wl[p] = wi;
     orig[p] = i;
-    uint8_t f = (i >= n_data) ? FLAG_RANDOM : 0;
-    if (buffer && buffer[i] == 1) f |= FLAG_BUFFER;
     flags[p] = f;
     cell_key[p] = key_orig[i];
   }

@@ -187,6 +187,14 @@ __device__ __forceinline__ int classify_f32(const float4 pi, const float4 pj, co
   return 1;
 }
 
+// Both points of a pair are buffer points (pos4.w = 1 marks them): the pair
+// has no root and adds nothing to any 2PCF histogram or gradient, so the
+// pair sweeps skip it before testing it.  (The neighbour graph keeps such
+// edges: they close triangles and 4-cliques rooted elsewhere.)
+__device__ __forceinline__ bool both_buffer(const float4& a, const float4& b) {
+  return a.w != 0.0f && b.w != 0.0f;
+}
+
 // Membership only (no bins) from the FP32 squared separation: 0 not an
 // edge, 1 an edge, 2 undecided (inside the guard band at rmin or rmax:
 // evaluate with edge_f64).

@@ -92,6 +92,7 @@ __global__ void __launch_bounds__(kPairThreads) pair2_kernel(DevCatalog C, PairP
         const double wp = WEIGHTED ? C.w[p] : 0.0;
         for (int f = fstart + lane; f < tn; f += 32) {
           const int q = s_lab[wib][f];
+          if (both_buffer(pi, s_pos[wib][f])) continue;
           int b, mf, mr;
           bool e;
           if (F32) {
@@ -262,7 +263,7 @@ __global__ void __launch_bounds__(kPairThreads) pair2_queue_kernel(
         for (int f0 = fstart; f0 < tn; f0 += 32) {
           const int f = f0 + lane;
           bool e = false;
-          if (f < tn) {
+          if (f < tn && !both_buffer(pi, s_pos[wib][f])) {
             int r = F32 ? member_f32(pi, s_pos[wib][f], P) : 2;
             if (r == 2) {
               int b, mf, mr;
@@ -402,6 +403,7 @@ __global__ void __launch_bounds__(NT) pair2_dense_kernel(DevCatalog C, PairParam
         const int fstart = max(0, p - cb + 1 - t0);
         if (fstart < tn) cands += (unsigned long long)(tn - fstart);
         for (int f = fstart; f < tn; ++f) {
+          if (both_buffer(pi, s_pos[f])) continue;
           int b, mf, mr;
           bool e;
           if (F32) {
@@ -577,7 +579,7 @@ __global__ void __launch_bounds__(NT) pair2_dense_queue_kernel(
         int qn = 0;
         for (int f = f0; f < tn; ++f) {  // warp-uniform walk over the candidates
           bool e = false;
-          if (f >= fstart) {
+          if (f >= fstart && !both_buffer(pi, s_pos[f])) {
             int r = F32 ? member_f32(pi, s_pos[f], P) : 2;
             if (r == 2) {
               int b, mf, mr;
