@@ -56,8 +56,11 @@ typedef struct gr_ctx gr_ctx;
 #define GR_OPT_CLIQUE_MODE 5 /* how the 3PCF / 4PCF kernels find the edges among a root's
                                larger-label neighbours: 0 automatic (default), 1 hash probes
                                of the neighbours' rows, 2 the graph's membership test on the
-                               pairs of neighbours (rows up to 256 neighbours; longer rows
-                               fall back to 1).  Results are identical; only speed differs */
+                               pairs of neighbours.  4PCF: mode 2 takes rows up to 256
+                               neighbours (longer rows use 1).  3PCF: rows longer than 256
+                               neighbours take a second launch in mode 2 (up to 1024, then a
+                               global-memory path) unless mode 1 is forced.  Results are
+                               identical; only speed differs */
 
 /* Run statistics of the last count call (gr_get_stats). */
 typedef struct gr_stats {
