@@ -13,7 +13,8 @@ HEADER = _native.HEADER
 
 
 def declared():
-    src = open(HEADER).read()
+    with open(HEADER) as f:
+        src = f.read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     return sorted(set(re.findall(r"\b(gr_[a-z0-9_]+)\s*\(", src)))
 

@@ -9,7 +9,8 @@ import pytest
 
 from gramsci_b200 import catalogs
 
-CASES = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "known_answers.json")))
+with open(os.path.join(os.path.dirname(__file__), "golden", "known_answers.json")) as _f:
+    CASES = json.load(_f)
 
 
 def _prep(c):

@@ -39,7 +39,7 @@ def _worker(rank, world, port, out):
 def test_two_ranks_gloo():
     world = 2
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_worker, args=(world, port, out), nprocs=world, join=True)
         res = dict(out)

@@ -16,8 +16,13 @@ import pytest
 from gramsci_b200 import catalogs, host
 
 
+def _text(path):
+    with open(path) as f:
+        return f.read()
+
+
 def _parse(path):
-    rows = [l.split() for l in open(path).read().splitlines() if l.strip()]
+    rows = [l.split() for l in _text(path).splitlines() if l.strip()]
     if not rows:
         return np.zeros((0, 4)), np.zeros(0, int), np.zeros(0, int)
     v = np.array([[float(x) for x in r[:4]] for r in rows])
@@ -116,8 +121,8 @@ def test_resum_sums_tables(tmp_path):
         tot2, tot3 = tot2 + N2, tot3 + N3
     out = tmp_path / "sum"
     assert host.resum(2, parts, out) == 0
-    lines = open(out).read().splitlines()
-    assert lines[0] == open(parts[0]).read().splitlines()[0]
+    lines = _text(out).splitlines()
+    assert lines[0] == _text(parts[0]).splitlines()[0]
     v = np.array([[float(x) for x in l.split()] for l in lines[1:]])
     np.testing.assert_allclose(v[:, 4], tot2.ravel(), rtol=3e-7, atol=3e-7)
     np.testing.assert_allclose(v[:, 5], tot3.ravel(), rtol=3e-7)
@@ -132,5 +137,5 @@ def test_resum_tetra_disc_column_is_nan(tmp_path):
     p = tmp_path / "t"
     host.write_tetra(str(p), e, 2, 1, np.ones(2), np.ones(2), np.ones((2, 6)), np.ones((2, 6)))
     assert host.resum(6, [p, p], tmp_path / "s") == 0
-    v = np.array([[float(x) for x in l.split()] for l in open(tmp_path / "s").read().splitlines()])
+    v = np.array([[float(x) for x in l.split()] for l in _text(tmp_path / "s").splitlines()])
     assert np.all(v[:, 4] == 2.0) and np.all(np.isnan(v[:, 7]))
