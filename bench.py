@@ -189,8 +189,6 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     cat, w, sp = make_catalogue(args.scale, None)
     cfg = workload_config(cat, sp, args.scale)
-    for _ in range(max(args.warmup, 0) and 1):
-        pass
     times, tri = [], 0
     nsteps = max(1, min(args.steps, 3))
     r = cpu_reference_run(cat, w, sp, threads)  # warm-up (page-in, thread pool)

@@ -2,7 +2,8 @@
 restatement of the reference algorithm (the oracle port) and prints one JSON
 line with the fields the benchmark contract asks for (impl, metric, value,
 unit, cpu_baseline with kind / cores / sample, and an e2e block with no
-host-device traffic)."""
+host-device traffic).  Under torchrun only rank 0 runs it; the other ranks
+exit 0 without work or output."""
 import json
 import os
 import subprocess
@@ -28,3 +29,12 @@ def test_reference_arm_prints_contract_line():
     e2e = line["e2e"]
     assert e2e["value"] == line["value"] and e2e["h2d_bytes_per_step"] == 0
     assert e2e["d2h_bytes_per_step"] == 0
+
+
+def test_reference_arm_other_ranks_exit_without_work():
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                        "--gpus", "2", "--steps", "1", "--warmup", "1"],
+                       capture_output=True, text=True, timeout=300, cwd=ROOT, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip() == ""
