@@ -6,6 +6,7 @@ import os
 import re
 
 import pytest
+import torch
 
 from gramsci_b200 import _native
 
@@ -44,3 +45,19 @@ def test_null_context_is_rejected():
 
 def test_library_is_in_tree():
     assert os.path.dirname(_native.LIB_PATH).endswith(os.path.join("gramsci_b200", "lib"))
+
+
+def test_missing_library_raises(tmp_path, monkeypatch):
+    monkeypatch.setattr(_native, "_lib", None)
+    with pytest.raises(ImportError, match="missing"):
+        _native.load(str(tmp_path / "libgramsci_cuda.so"))
+
+
+@pytest.mark.skipif(torch.cuda.is_available(), reason="needs a host without a GPU")
+def test_no_device_fails_loudly():
+    """Without a CUDA device a context cannot be made: the counts are never
+    computed by a host fallback."""
+    from gramsci_b200 import api
+
+    with pytest.raises(_native.GramsciError, match="gr_create"):
+        api.Context(0)
