@@ -11,10 +11,15 @@ import pytest
 from gramsci_b200 import catalogs
 
 
-def brute_edges(xyz, rmin, rmax, nbins, nmu):
-    """Reference predicate written independently: all ordered pairs."""
+def brute_edges(xyz, rmin, rmax, nbins, nmu, logbins=False):
+    """Reference predicate written independently: all ordered pairs.  Log
+    bins take floor((log10 r - log10 rmin) / delta) + 1 with delta =
+    (log10 rmax - log10 rmin) / nbins (gramsci.F90:136-139, :334-335)."""
     n = len(xyz)
-    inv_dr = 1.0 / ((rmax - rmin) / nbins)
+    if logbins:
+        inv_dr = 1.0 / ((math.log10(rmax) - math.log10(rmin)) / nbins)
+    else:
+        inv_dr = 1.0 / ((rmax - rmin) / nbins)
     mu_scale = 0.5 * nmu
     E = {}
     for i in range(n):
@@ -30,7 +35,8 @@ def brute_edges(xyz, rmin, rmax, nbins, nmu):
             r = math.sqrt(sd)
             if r <= rmin or r >= rmax:
                 continue
-            b = min(int(math.floor((r - rmin) * inv_dr)) + 1, nbins)
+            t = (math.log10(r) - math.log10(rmin)) * inv_dr if logbins else (r - rmin) * inv_dr
+            b = min(int(math.floor(t)) + 1, nbins)
             m = 1
             if nmu >= 2:
                 mid = 0.5 * (xyz[i] + xyz[j])
@@ -73,6 +79,20 @@ def test_graph_matches_brute_force(oracle, nmu, method):
         for k in range(rp[i], rp[i + 1]):
             got[(i, int(col[k]))] = (int(b[k]), int(mu[k]))
     assert got == E
+
+
+@pytest.mark.parametrize("nmu", [1, 3])
+def test_log_bin_graph_matches_brute_force(oracle, nmu):
+    xyz, w, nd = small_catalogue(40, 60, 100.0, 4)
+    G = oracle.Graph(xyz, 1.5, 40.0, 7, nmu, logbins=True)
+    rp, col, b, mu = G.csr()
+    E = brute_edges(xyz, 1.5, 40.0, 7, nmu, logbins=True)
+    got = {(i, int(col[k])): (int(b[k]), int(mu[k]))
+           for i in range(len(xyz)) for k in range(rp[i], rp[i + 1])}
+    assert got == E
+    # log bins differ from linear ones on this range
+    lin = brute_edges(xyz, 1.5, 40.0, 7, nmu)
+    assert lin.keys() == E.keys() and any(lin[e][0] != E[e][0] for e in E)
 
 
 def test_grid_and_kdtree_agree(oracle):
