@@ -161,8 +161,10 @@ def test_2pcf_3pcf_match_brute_force(oracle, nmu):
     assert np.allclose(r3["N3"], -r3["catsum"][:, :, 3], rtol=1e-13, atol=1e-300)
 
 
-def test_4pcf_matches_brute_force(oracle):
+@pytest.mark.parametrize("with_buffer", [False, True])
+def test_4pcf_matches_brute_force(oracle, with_buffer):
     xyz, w, nd = small_catalogue(25, 25, 30.0, 3)
+    buf = (np.arange(len(xyz)) % 5 == 2).astype(np.int32) if with_buffer else None
     nbins = 3
     E = brute_edges(xyz, 1.0, 12.0, nbins, 1)
     n = len(xyz)
@@ -170,11 +172,13 @@ def test_4pcf_matches_brute_force(oracle):
     nc = oracle.ncfg4(nbins)
     cnt = np.zeros((nc, nbins, nbins, 5), np.int64)
     dcnt = np.zeros((nc, nbins, nbins, 6, 4), np.int64)
+    n2 = np.zeros((nc, nbins, nbins))
+    n3 = np.zeros((nc, nbins, nbins))
     gate = [3, 3, 1, 0, 0, 0]
     pu = [0, 0, 0, 1, 3, 3]
     pv = [1, 2, 3, 2, 2, 1]
     for i in range(n):
-        if len(nbrs[i]) <= 3:
+        if len(nbrs[i]) <= 3 or (buf is not None and buf[i]):
             continue
         for a, b, c in itertools.combinations(nbrs[i], 3):
             if (a, b) not in E or (b, c) not in E or (a, c) not in E:
@@ -186,6 +190,12 @@ def test_4pcf_matches_brute_force(oracle):
             v = [i, a, b, c]
             r = [x >= nd for x in v]
             cnt[cfg - 1, d1 - 1, d2 - 1, sum(r)] += 1
+            # N2 takes every clique's weight product, N3 the all-random ones
+            # (gramsci.F90:704-707)
+            wp = w[i] * w[a] * w[b] * w[c]
+            n2[cfg - 1, d1 - 1, d2 - 1] += wp
+            if all(r):
+                n3[cfg - 1, d1 - 1, d2 - 1] += wp
             for t in range(6):
                 if r[gate[t]]:
                     npr = r[pu[t]] + r[pv[t]]
@@ -193,10 +203,13 @@ def test_4pcf_matches_brute_force(oracle):
                     if npr == 2:
                         dcnt[cfg - 1, d1 - 1, d2 - 1, t, 3] += 1
     G = oracle.Graph(xyz, 1.0, 12.0, nbins, 1)
-    r4 = G.pcf4(w, nd)
+    r4 = G.pcf4(w, nd, buffer=buf)
     assert cnt.sum() > 0
     assert np.array_equal(r4["counts"], cnt)
     assert np.array_equal(r4["dcount"], dcnt)
+    scale = np.abs(n2).max()
+    np.testing.assert_allclose(r4["N2"], n2, rtol=1e-12, atol=1e-13 * scale)
+    np.testing.assert_allclose(r4["N3"], n3, rtol=1e-12, atol=1e-13 * scale)
 
 
 def test_bintables(oracle):
