@@ -174,6 +174,8 @@ def test_4pcf_matches_brute_force(oracle, with_buffer):
     dcnt = np.zeros((nc, nbins, nbins, 6, 4), np.int64)
     n2 = np.zeros((nc, nbins, nbins))
     n3 = np.zeros((nc, nbins, nbins))
+    dn = np.zeros((nc, nbins, nbins, 6))
+    dr = np.zeros((nc, nbins, nbins, 6))
     gate = [3, 3, 1, 0, 0, 0]
     pu = [0, 0, 0, 1, 3, 3]
     pv = [1, 2, 3, 2, 2, 1]
@@ -200,8 +202,14 @@ def test_4pcf_matches_brute_force(oracle, with_buffer):
                 if r[gate[t]]:
                     npr = r[pu[t]] + r[pv[t]]
                     dcnt[cfg - 1, d1 - 1, d2 - 1, t, npr] += 1
+                    # discN takes the pair's weight product when the gate
+                    # vertex is a random, discR when the pair is too
+                    # (gramsci.F90:752-818)
+                    pw = w[v[pu[t]]] * w[v[pv[t]]]
+                    dn[cfg - 1, d1 - 1, d2 - 1, t] += pw
                     if npr == 2:
                         dcnt[cfg - 1, d1 - 1, d2 - 1, t, 3] += 1
+                        dr[cfg - 1, d1 - 1, d2 - 1, t] += pw
     G = oracle.Graph(xyz, 1.0, 12.0, nbins, 1)
     r4 = G.pcf4(w, nd, buffer=buf)
     assert cnt.sum() > 0
@@ -210,6 +218,10 @@ def test_4pcf_matches_brute_force(oracle, with_buffer):
     scale = np.abs(n2).max()
     np.testing.assert_allclose(r4["N2"], n2, rtol=1e-12, atol=1e-13 * scale)
     np.testing.assert_allclose(r4["N3"], n3, rtol=1e-12, atol=1e-13 * scale)
+    dscale = np.abs(dn).max()
+    assert dscale > 0
+    np.testing.assert_allclose(r4["discN"], dn, rtol=1e-12, atol=1e-13 * dscale)
+    np.testing.assert_allclose(r4["discR"], dr, rtol=1e-12, atol=1e-13 * dscale)
 
 
 def test_bintables(oracle):
