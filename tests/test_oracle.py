@@ -382,3 +382,30 @@ def test_equi_and_tetra_match_brute_force(oracle):
     assert np.array_equal(t["counts"], ct)
     # with RSD the reference sums only N2 for -equi
     assert np.all(e["N3"] == 0)
+
+
+def test_empty_single_and_all_buffer_catalogues(oracle):
+    for xyz in (np.zeros((0, 3)), np.array([[1.0, 2.0, 3.0]])):
+        n = len(xyz)
+        G = oracle.Graph(xyz, 1.0, 10.0, 3, 2)
+        assert np.array_equal(G.csr()[0], np.zeros(n + 1, np.int64))
+        w = np.full(n, 1.0)
+        for r in (G.pcf2(w, n), G.pcf3(w, n), G.pcf4(w, n)):
+            assert not r["N2"].any() and not r["N3"].any() and not r["counts"].any()
+    xyz, w, nd = small_catalogue(30, 30, 40.0, 5)
+    G = oracle.Graph(xyz, 1.0, 12.0, 3, 2)
+    allbuf = np.ones(len(xyz), np.int32)
+    assert G.pcf3(w, nd)["counts"].sum() > 0
+    for r in (G.pcf2(w, nd, buffer=allbuf), G.pcf3(w, nd, buffer=allbuf),
+              G.pcf4(w, nd, buffer=allbuf)):
+        assert not r["N2"].any() and not r["counts"].any()
+
+
+def test_galaxies_only_have_no_random_terms(oracle):
+    xyz, w, nd = small_catalogue(60, 0, 40.0, 6)
+    G = oracle.Graph(xyz, 1.0, 12.0, 3, 1)
+    r2, r3, r4 = G.pcf2(w, nd), G.pcf3(w, nd), G.pcf4(w, nd)
+    assert r2["counts"][..., 0].sum() > 0 and r3["counts"][..., 0].sum() > 0
+    for r in (r2, r3, r4):
+        assert not r["N3"].any() and not r["counts"][..., 1:].any()
+    assert not r4["discN"].any() and not r4["discR"].any()
