@@ -13,8 +13,17 @@ Cases
   los           two pairs 1000 Mpc/h from the observer, one radial, one
                 transverse, nmu 4: mu bins from each end (radial: 1 and 4
                 after clamping; transverse: 2 and 3).
+  tetrahedron   regular tetrahedron of edge sqrt(32) (radial bin 2) and its
+                centre, sqrt(12) from every vertex (bin 1); rmin 1, rmax 10,
+                3 bins.  Vertices 0-2 are galaxies, vertex 3 and the centre
+                (id 4) randoms, unit weights.  2PCF, 3PCF and 4PCF answers
+                below are derived by hand from the reference loops; the 4PCF
+                pins the perimeter order, the root-row length rule (every row
+                holds 4 > 3 neighbours), the non-canonical table entries
+                (taken as 0) and the six disconnected-term gates.
 Run: python tests/golden/make_golden.py
 """
+import itertools
 import json
 import math
 import os
@@ -67,6 +76,51 @@ def main():
                       nbins=3, nmu=4,
                       counts2={"2,1,0": 1, "2,4,0": 1, "2,2,0": 1, "2,3,0": 1},
                       edges={"0,1": [2, 1], "1,0": [2, 4], "2,3": [2, 2], "3,2": [2, 3]}))
+    # regular tetrahedron + centre.  Every separation is sqrt(32) (vertex to
+    # vertex, t = (5.657 - 1)/3 = 1.55, bin 2) or sqrt(12) (to the centre,
+    # t = 0.82, bin 1), far from the bin edges 1, 4, 7, 10.
+    pts = [[102.0, 102.0, 102.0], [102.0, 98.0, 98.0], [98.0, 102.0, 98.0],
+           [98.0, 98.0, 102.0], [100.0, 100.0, 100.0]]
+    for i in range(4):
+        for j in range(i + 1, 4):
+            assert sum((a - b) ** 2 for a, b in zip(pts[i], pts[j])) == 32.0
+        assert sum((a - b) ** 2 for a, b in zip(pts[i], pts[4])) == 12.0
+    g, r = 1.0 / 3.0, -1.0 / 2.0  # normalised weights: 3 galaxies, 2 randoms
+    nc4 = 0  # rank of (2,2,2,2) among i<=j<=k<=l<=3, lexicographic
+    for t in sorted(q for q in itertools.product(range(1, 4), repeat=4) if list(q) == sorted(q)):
+        nc4 += 1
+        if t == (2, 2, 2, 2):
+            break
+    assert nc4 == 11
+    cases.append(dict(
+        name="tetrahedron", xyz=pts, w=[1.0] * 5, n_data=3, rmin=1.0, rmax=10.0,
+        nbins=3, nmu=1, rtol=1e-13,
+        # directed pairs, category 2*random(root) + random(neighbour):
+        # vertex-vertex (bin 2): galaxy-galaxy 6, galaxy->v3 3, v3->galaxy 3;
+        # centre (bin 1): galaxy->centre 3, centre->galaxy 3, v3<->centre 2
+        counts2={"2,1,0": 6, "2,1,1": 3, "2,1,2": 3, "1,1,1": 3, "1,1,2": 3, "1,1,3": 2},
+        # 3PCF, each triangle once per vertex: the four faces are (2,2,2) =
+        # rank 7, face 012 with no random, the three faces with v3 with one;
+        # the six centre triangles are (1,1,2) = rank 2, one random (the
+        # centre) for galaxy pairs, two for pairs with v3
+        counts3={"7,1,0": 3, "7,1,1": 9, "2,1,1": 9, "2,1,2": 9},
+        N2_3={"7,1": 3 * g ** 3 + 9 * g * g * r, "2,1": 9 * g * g * r + 9 * g * r * r},
+        # 4PCF: a vertex root's triples with the centre (always the largest
+        # id) have the perimeter (2,2,1,1), the centre root's (1,2,2,1):
+        # both non-canonical, so only the tetrahedron contributes, once
+        # from each vertex, at (cfg 11, bin(i,b) 2, bin(a,c) 2) with one
+        # random (v3)
+        counts4={"11,2,2,1": 4},
+        N2_4={"11,2,2": 4 * g ** 3 * r},
+        # disconnected terms: roots 0-2 see v3 as their last member c (gate
+        # of terms 1 and 2, pairs (i,a) and (i,b)); root 3 is the random
+        # gate of terms 4-6 (pairs among its three galaxy members); all
+        # pairs are galaxy pairs, so discR is 0
+        dcount4={"11,2,2,1,0": 3, "11,2,2,2,0": 3, "11,2,2,4,0": 1, "11,2,2,5,0": 1,
+                 "11,2,2,6,0": 1},
+        discN4={"11,2,2,1": 3 * g * g, "11,2,2,2": 3 * g * g, "11,2,2,4": g * g,
+                "11,2,2,5": g * g, "11,2,2,6": g * g},
+        edges={"0,1": [2, 1], "0,4": [1, 1], "4,3": [1, 1]}))
     with open(os.path.join(HERE, "known_answers.json"), "w") as f:
         json.dump(cases, f, indent=1)
 

@@ -1,6 +1,8 @@
 """Known-answer configurations (tests/golden/known_answers.json, made by
 tests/golden/make_golden.py from geometry alone) against the oracle (CPU)
-and against the CUDA library (GPU)."""
+and against the CUDA library (GPU).  The 4PCF answers of the tetrahedron
+case pin the oracle; the library's 4PCF is held to the oracle by the GPU
+parity tests."""
 import json
 import os
 
@@ -35,7 +37,29 @@ def _check(c, counts2, counts3=None, N2_3=None):
     if N2_3 is not None and "N2_3" in c:
         for k, v in c["N2_3"].items():
             cfg, m = map(int, k.split(","))
-            assert abs(N2_3[cfg - 1, m - 1] - v) <= 1e-15 * abs(v)
+            assert abs(N2_3[cfg - 1, m - 1] - v) <= c.get("rtol", 1e-15) * abs(v)
+
+
+def _check4(c, r4):
+    """4PCF known answers: counts by number of randoms, N2, disconnected-term
+    counts (term 1-6, randoms in the pair) and discN sums; every entry not
+    listed is 0."""
+    exp = np.zeros_like(r4["counts"])
+    for k, v in c["counts4"].items():
+        cfg, d1, d2, nr = map(int, k.split(","))
+        exp[cfg - 1, d1 - 1, d2 - 1, nr] = v
+    assert np.array_equal(r4["counts"], exp), c["name"]
+    exp = np.zeros_like(r4["dcount"])
+    for k, v in c["dcount4"].items():
+        cfg, d1, d2, t, npr = map(int, k.split(","))
+        exp[cfg - 1, d1 - 1, d2 - 1, t - 1, npr] = v
+    assert np.array_equal(r4["dcount"], exp), c["name"]
+    for key, got in (("N2_4", r4["N2"]), ("discN4", r4["discN"])):
+        exp = np.zeros_like(got)
+        for k, v in c[key].items():
+            exp[tuple(int(x) - 1 for x in k.split(","))] = v
+        np.testing.assert_allclose(got, exp, rtol=c["rtol"], atol=0)
+    assert not r4["N3"].any() and not r4["discR"].any()
 
 
 @pytest.mark.parametrize("c", CASES, ids=[c["name"] for c in CASES])
@@ -45,6 +69,8 @@ def test_oracle_known_answers(oracle, c):
     r2 = G.pcf2(w, c["n_data"])
     r3 = G.pcf3(w, c["n_data"]) if c["n_data"] >= 3 else None
     _check(c, r2["counts"], r3["counts"] if r3 else None, r3["N2"] if r3 else None)
+    if "counts4" in c:
+        _check4(c, G.pcf4(w, c["n_data"]))
     if "edges" in c:
         rp, col, b, mu = G.csr()
         for k, (eb, em) in c["edges"].items():
