@@ -20,7 +20,8 @@ Cases
                 below are derived by hand from the reference loops; the 4PCF
                 pins the perimeter order, the root-row length rule (every row
                 holds 4 > 3 neighbours), the non-canonical table entries
-                (taken as 0) and the six disconnected-term gates.
+                (taken as 0) and the six disconnected-term gates; the
+                -equi and -tetra answers likewise.
 Run: python tests/golden/make_golden.py
 """
 import itertools
@@ -120,6 +121,19 @@ def main():
                  "11,2,2,6,0": 1},
         discN4={"11,2,2,1": 3 * g * g, "11,2,2,2": 3 * g * g, "11,2,2,4": g * g,
                 "11,2,2,5": g * g, "11,2,2,6": g * g},
+        # -equi (gramsci.F90:402-446): triangles with three edges in one bin
+        # are the four faces (bin 2), rooted at each vertex
+        counts_equi={"2,1,0": 3, "2,1,1": 9},
+        N2_equi={"2,1": 3 * g ** 3 + 9 * g * g * r},
+        # -tetra (:548-640): cliques with six edges in one bin, no row-length
+        # rule: the tetrahedron from each vertex.  Its disconnected terms
+        # are triple products with the gate vertex's weight: roots 0-2 have
+        # v3 as id3 (gate of terms 1 and 2), root 3 is the random root (gate
+        # of terms 4, 5, 6); term 3's gate id1 is always a galaxy
+        counts_tetra={"2,1": 4},
+        N2_tetra={"2": 4 * g ** 3 * r},
+        discN_tetra={"2,1": 3 * r * g * g, "2,2": 3 * r * g * g, "2,4": r * g * g,
+                     "2,5": r * g * g, "2,6": r * g * g},
         edges={"0,1": [2, 1], "0,4": [1, 1], "4,3": [1, 1]}))
     with open(os.path.join(HERE, "known_answers.json"), "w") as f:
         json.dump(cases, f, indent=1)

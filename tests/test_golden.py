@@ -62,6 +62,28 @@ def _check4(c, r4):
     assert not r4["N3"].any() and not r4["discR"].any()
 
 
+def _check_special(c, eq, te):
+    """-equi and -tetra known answers: counts by number of randoms, N2 and
+    (-tetra) discN; N3 and discR are 0 in these cases."""
+    exp = np.zeros_like(eq["counts"])
+    for k, v in c["counts_equi"].items():
+        b, m, nr = map(int, k.split(","))
+        exp[b - 1, m - 1, nr] = v
+    assert np.array_equal(eq["counts"], exp), c["name"]
+    exp = np.zeros_like(te["counts"])
+    for k, v in c["counts_tetra"].items():
+        b, nr = map(int, k.split(","))
+        exp[b - 1, nr] = v
+    assert np.array_equal(te["counts"], exp), c["name"]
+    for entries, got in ((c["N2_equi"], eq["N2"]), (c["N2_tetra"], te["N2"]),
+                         (c["discN_tetra"], te["discN"])):
+        exp = np.zeros_like(got)
+        for k, v in entries.items():
+            exp[tuple(int(x) - 1 for x in k.split(","))] = v
+        np.testing.assert_allclose(got, exp, rtol=c["rtol"], atol=0)
+    assert not eq["N3"].any() and not te["N3"].any() and not te["discR"].any()
+
+
 @pytest.mark.parametrize("c", CASES, ids=[c["name"] for c in CASES])
 def test_oracle_known_answers(oracle, c):
     xyz, w = _prep(c)
@@ -71,6 +93,8 @@ def test_oracle_known_answers(oracle, c):
     _check(c, r2["counts"], r3["counts"] if r3 else None, r3["N2"] if r3 else None)
     if "counts4" in c:
         _check4(c, G.pcf4(w, c["n_data"]))
+    if "counts_equi" in c:
+        _check_special(c, G.equi(w, c["n_data"]), G.tetra(w, c["n_data"]))
     if "edges" in c:
         rp, col, b, mu = G.csr()
         for k, (eb, em) in c["edges"].items():
