@@ -13,6 +13,8 @@ Cases
   los           two pairs 1000 Mpc/h from the observer, one radial, one
                 transverse, nmu 4: mu bins from each end (radial: 1 and 4
                 after clamping; transverse: 2 and 3).
+  los_triangle  equilateral triangle of side 5 across the line of sight,
+                nmu 4: edge mu bins 2 / 3, every root's find_normal bin 4.
   tetrahedron   regular tetrahedron of edge sqrt(32) (radial bin 2) and its
                 centre, sqrt(12) from every vertex (bin 1); rmin 1, rmax 10,
                 3 bins.  Vertices 0-2 are galaxies, vertex 3 and the centre
@@ -77,6 +79,24 @@ def main():
                       nbins=3, nmu=4,
                       counts2={"2,1,0": 1, "2,4,0": 1, "2,2,0": 1, "2,3,0": 1},
                       edges={"0,1": [2, 1], "1,0": [2, 4], "2,3": [2, 2], "3,2": [2, 3]}))
+    # equilateral triangle of side 5 across the line of sight, 1000 Mpc/h
+    # out, nmu 4.  m.s = (|p_i|^2 - |p_j|^2) / 2 is -62.5, -37.5, 25 for the
+    # pairs (0,1), (0,2), (1,2): cosines -0.0125, -0.0075, 0.005 seen from
+    # the first vertex, so mu bin 2 from one end and 3 from the other
+    # (floor((theta + 1) * 2) + 1).  The roots' mu pairs are (2,2), (3,3),
+    # (3,2); find_normal (gramsci.F90:1611-1625) maps bin centres -0.25 /
+    # 0.25 through 1.1547 * sqrt(0.6875) * 4 = 3.83 and
+    # 1.1547 * sqrt(0.5625) * 4 = 3.46 to bin 4 for all three.
+    h = 2.5 * math.sqrt(3.0)
+    pts = [[10.0, 0.0, 1000.0], [15.0, 0.0, 1000.0], [12.5, h, 1000.0]]
+    cases.append(dict(
+        name="los_triangle", xyz=pts, w=[1.0] * 3, n_data=3, rmin=1.0, rmax=10.0,
+        nbins=3, nmu=4,
+        counts2={"2,2,0": 3, "2,3,0": 3},
+        counts3={"7,4,0": 3},
+        N2_3={"7,4": 3 * (1.0 / 3.0) ** 3},
+        edges={"0,1": [2, 2], "1,0": [2, 3], "0,2": [2, 2], "2,0": [2, 3], "1,2": [2, 3],
+               "2,1": [2, 2]}))
     # regular tetrahedron + centre.  Every separation is sqrt(32) (vertex to
     # vertex, t = (5.657 - 1)/3 = 1.55, bin 2) or sqrt(12) (to the centre,
     # t = 0.82, bin 1), far from the bin edges 1, 4, 7, 10.
