@@ -23,7 +23,8 @@ Cases
                 pins the perimeter order, the root-row length rule (every row
                 holds 4 > 3 neighbours), the non-canonical table entries
                 (taken as 0) and the six disconnected-term gates; the
-                -equi and -tetra answers likewise.
+                -equi and -tetra answers likewise, and the closed-form
+                weight gradients of the 2/3/4PCF sums.
 Run: python tests/golden/make_golden.py
 """
 import itertools
@@ -154,7 +155,16 @@ def main():
         N2_tetra={"2": 4 * g ** 3 * r},
         discN_tetra={"2,1": 3 * r * g * g, "2,2": 3 * r * g * g, "2,4": r * g * g,
                      "2,5": r * g * g, "2,6": r * g * g},
-        edges={"0,1": [2, 1], "0,4": [1, 1], "4,3": [1, 1]}))
+        edges={"0,1": [2, 1], "0,4": [1, 1], "4,3": [1, 1]},
+        # weight gradients of L = sum(N2) (every cotangent 1), normalised
+        # weights w = (g, g, g, r, r).  All ten pairs are edges and the ten
+        # triples triangles: 2PCF dL/dw_k = 2 (sum(w) - w_k) = -2 w_k since
+        # sum(w) = 0; 3PCF (each triangle rooted 3 times) dL/dw_k = 3 e2 of
+        # the other four weights; 4PCF (the tetrahedron rooted 4 times)
+        # dL/dw_k = 4 * product of the other three vertices, 0 for the centre
+        grad2=[-2 * g] * 3 + [-2 * r] * 2,
+        grad3=[3 * (g * g + 4 * g * r + r * r)] * 3 + [3 * (3 * g * g + 3 * g * r)] * 2,
+        grad4=[4 * g * g * r] * 3 + [4 * g ** 3, 0.0]))
     with open(os.path.join(HERE, "known_answers.json"), "w") as f:
         json.dump(cases, f, indent=1)
 

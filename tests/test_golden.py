@@ -95,6 +95,14 @@ def test_oracle_known_answers(oracle, c):
         _check4(c, G.pcf4(w, c["n_data"]))
     if "counts_equi" in c:
         _check_special(c, G.equi(w, c["n_data"]), G.tetra(w, c["n_data"]))
+    if "grad2" in c:
+        nd, nb, nm = c["n_data"], c["nbins"], c["nmu"]
+        r4 = G.pcf4(w, nd)
+        got = [G.adjoint2(w, nd, np.ones((nb, nm))),
+               G.adjoint3(w, nd, np.ones((oracle.ncfg3(nb), nm))),
+               G.adjoint4(w, nd, np.ones_like(r4["N2"]))]
+        for k, g in zip(("grad2", "grad3", "grad4"), got):
+            np.testing.assert_allclose(g, c[k], rtol=c["rtol"], atol=1e-15, err_msg=k)
     if "edges" in c:
         rp, col, b, mu = G.csr()
         for k, (eb, em) in c["edges"].items():
