@@ -35,8 +35,22 @@ void print_help() {
   std::puts("   -gcol                     region file rows are x y z w gal buffer (gramsci-decompose)");
 }
 
+// Without a context (gr_create failed) there is no message to read: name the
+// status instead.
+const char* status_text(int rc) {
+  switch (rc) {
+    case GR_E_ARG: return "invalid argument";
+    case GR_E_CAPACITY: return "out of memory or over a size limit";
+    case GR_E_CUDA: return "no usable CUDA device";
+    case GR_E_TIMEOUT: return "a device wait ran out";
+    case GR_E_UNSUPPORTED: return "unsupported option";
+    default: return "unknown status";
+  }
+}
+
 int fail(gr_ctx* ctx, const char* what, int rc) {
-  std::fprintf(stderr, "gramsci: %s failed (%d): %s\n", what, rc, ctx ? gr_last_error(ctx) : "");
+  std::fprintf(stderr, "gramsci: %s failed (%d): %s\n", what, rc,
+               ctx ? gr_last_error(ctx) : status_text(rc));
   return 1;
 }
 

@@ -115,3 +115,23 @@ def test_cli_help_and_unknown_option():
     r = subprocess.run([host.CLI_PATH, "-gal", "a", "-ran", "b", "-rmin", "x", "-rmax", "2"],
                        capture_output=True, text=True)
     assert r.returncode == 2
+
+
+def test_cli_without_gpu_fails_loudly(tmp_path):
+    """On a host without a CUDA device the driver stops with status 1 and
+    names the cause; no table is written (there is no host fallback)."""
+    import subprocess
+
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("needs a host without a GPU")
+    g, r, out = tmp_path / "g", tmp_path / "r", tmp_path / "out"
+    g.write_text("1 2 3 1\n4 5 6 1\n")
+    r.write_text("1 2 4 1\n4 5 7 1\n")
+    res = subprocess.run([host.CLI_PATH, "-gal", str(g), "-ran", str(r), "-rmin", "1", "-rmax", "10",
+                          "-nbins", "3", "-2pcf", "-out", str(out)],
+                         capture_output=True, text=True, timeout=120)
+    assert res.returncode == 1
+    assert "gr_create failed (-3): no usable CUDA device" in res.stderr
+    assert not out.exists()
