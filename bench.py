@@ -334,7 +334,8 @@ def run_ours(args):
         "gpu_launches": launches,
     }
     if world == 1 and args.precision == "f32":
-        # configs[1]'s comparison: the same steps through the plain FP64 path
+        # the 3PCF workload's precision comparison: the same steps through
+        # the plain FP64 path
         # (every pair in FP64 arithmetic); results must be identical
         ref32 = ctx.count_3pcf()
         ctx.set_catalog(xyz_d, w_d, cat.n_data)
@@ -379,7 +380,8 @@ def run_ours(args):
 
 
 def run_batched(args):
-    """2PCF over 5^3 regions with Rmax buffers, all regions in one
+    """Batched regions: 2PCF of 4M density-ramped galaxies + 8M randoms over
+    5^3 regions with Rmax buffers, all regions in one
     graph-replayed launch, against one launch per region on the same regions."""
     import torch
 
@@ -460,7 +462,8 @@ def run_batched(args):
 
 
 def run_adjoint(args):
-    """weighted 2PCF and 3PCF forward passes and their weight
+    """Adjoints: weighted 2PCF and 3PCF forward passes over 1M lognormal-
+    weighted galaxies + 2M randoms and their weight
     adjoints (device time of the counting vs the adjoint kernels)."""
     from gramsci_b200 import api, catalogs
 
@@ -494,7 +497,8 @@ def run_adjoint(args):
 
 
 def run_quad(args):
-    """4PCF on the small dense clustered set (unit weights).
+    """4PCF on the small dense clustered set (30k galaxies + 90k randoms in a
+    300 Mpc/h box, unit weights).
     value: rooted 4-clique contributions binned per second of device time
     (index + graph + 4-clique kernel per step); e2e through the public API
     with host inputs; beside it the same catalogue with lognormal weights

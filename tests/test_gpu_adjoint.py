@@ -1,4 +1,4 @@
-"""Weight adjoints on the GPU (configs[4] at reduced scale: Neyman-Scott
+"""Weight adjoints on the GPU (the adjoint workload at reduced scale: Neyman-Scott
 galaxies with lognormal weights plus uniform randoms, same number density).
 
 * against the oracle's gradient (long double accumulation on the CPU):

@@ -1,4 +1,4 @@
-"""Batched regions (configs[3] at reduced scale): the 2PCF of all regions in
+"""Batched regions (the 5^3-region workload at reduced scale): the 2PCF of all regions in
 one graph-replayed launch equals the 2PCF of the whole catalogue and the sum
 of the regions run one launch at a time (integer counts bit-exact, weighted
 sums within 1e-12), on the density-ramped Neyman-Scott catalogue."""
