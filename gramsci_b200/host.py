@@ -1,6 +1,6 @@
 """ctypes binding of libgramsci_host.so (include/gramsci_host.h): option
 parsing, catalogue reading, weight normalisation and output writers of the
-`gramsci` driver.  None of these needs a GPU."""
+`gramsci` command.  None of these needs a GPU."""
 import ctypes
 import os
 

@@ -3,8 +3,9 @@
 // TEST INFRASTRUCTURE ONLY.  This file restates, on the CPU and in plain IEEE
 // FP64 with no FMA contraction, the algorithm of the reference program
 // (src/gramsci.F90, src/kdtree2.F90, src/sorting_module.F90).  Only tests/,
-// the smoke check and the CPU-baseline leg of bench.py load it, and only as a
-// checker or as the timed CPU baseline.  The CUDA library never calls it.
+// the smoke check and the CPU-baseline leg of bench.py load it, and only to
+// check the library's results or as the timed CPU baseline.  The CUDA library
+// never calls it.
 //
 // Parity status: UNPINNED against reference outputs.  The reference is
 // Fortran; no Fortran compiler exists in the build container or on the GPU

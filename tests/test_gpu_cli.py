@@ -1,5 +1,5 @@
-"""End to end through the `gramsci` driver: ASCII catalogues in, the
-reference's result table out.  The table written by the driver (counts from
+"""End to end through the `gramsci` command: ASCII catalogues in, the
+reference's result table out.  The table written by the command (counts from
 the GPU) is compared with the table the same writer produces from the CPU
 oracle's N2/N3: identical layout and bin columns, values equal to the 7
 digits of E14.7 (a last-digit difference is allowed only where the two FP64

@@ -1,4 +1,4 @@
-"""CPU tests of the `gramsci` driver's host side (libgramsci_host.so):
+"""CPU tests of the `gramsci` command's host side (libgramsci_host.so):
 option parsing as the reference's parseOptions does it, list-directed
 catalogue reading, weight normalisation, radial bin edges and the E14.7
 output records."""
@@ -118,7 +118,7 @@ def test_cli_help_and_unknown_option():
 
 
 def test_cli_without_gpu_fails_loudly(tmp_path):
-    """On a host without a CUDA device the driver stops with status 1 and
+    """On a host without a CUDA device the command stops with status 1 and
     names the cause; no table is written (there is no host fallback)."""
     import subprocess
 
