@@ -21,6 +21,8 @@ GR_E_UNSUPPORTED = -5
 GR_OPT_PRECISION = 1
 GR_OPT_TIMEOUT_MS = 2
 GR_OPT_AUTOTUNE = 3
+GR_OPT_KEEP_GRAPH = 4
+GR_OPT_CLIQUE_MODE = 5
 
 
 class GramsciError(RuntimeError):

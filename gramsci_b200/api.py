@@ -252,11 +252,12 @@ class Context:
         rows) or "geometric" (the graph's membership test on the pairs).
         Results are identical."""
         v = {"auto": 0, "hash": 1, "geometric": 2}[mode]
-        self._check(self._lib.gr_set_option(self._h, 5, v))
+        self._check(self._lib.gr_set_option(self._h, _native.GR_OPT_CLIQUE_MODE, v))
 
     def set_keep_graph(self, on):
         """Reuse the last call's graph until the catalogue, bins or precision change."""
-        self._check(self._lib.gr_set_option(self._h, 4, int(bool(on))))
+        self._check(self._lib.gr_set_option(self._h, _native.GR_OPT_KEEP_GRAPH,
+                                            int(bool(on))))
 
     def graph_save(self, path):
         """Write the neighbour graph of the current catalogue and bins to `path`."""

@@ -61,3 +61,39 @@ def test_no_device_fails_loudly():
 
     with pytest.raises(_native.GramsciError, match="gr_create"):
         api.Context(0)
+
+
+def test_header_constants_match_binding():
+    with open(HEADER) as f:
+        defs = dict(re.findall(r"^#define (GR_[A-Z0-9_]+) \(?(-?\d+)\)?", f.read(), flags=re.M))
+    assert {"GR_OK", "GR_E_CUDA", "GR_OPT_CLIQUE_MODE", "GR_NOALLOC_MAX_BINS"} <= set(defs)
+    for name, v in defs.items():
+        assert getattr(_native, name) == int(v), name
+
+
+class _FakeLib:
+    """Records gr_set_option calls; every call succeeds."""
+
+    def __init__(self):
+        self.calls = []
+
+    def gr_set_option(self, h, key, value):
+        self.calls.append((key, value))
+        return 0
+
+
+def test_option_setters_pass_header_keys():
+    from gramsci_b200 import api
+
+    ctx = object.__new__(api.Context)
+    ctx._lib, ctx._h = _FakeLib(), None
+    ctx.set_precision("f64")
+    ctx.set_autotune("off")
+    ctx.set_autotune(3)
+    ctx.set_keep_graph(True)
+    ctx.set_clique_mode("geometric")
+    ctx.set_clique_mode("hash")
+    assert ctx._lib.calls == [(_native.GR_OPT_PRECISION, 1), (_native.GR_OPT_AUTOTUNE, 0),
+                              (_native.GR_OPT_AUTOTUNE, 5), (_native.GR_OPT_KEEP_GRAPH, 1),
+                              (_native.GR_OPT_CLIQUE_MODE, 2), (_native.GR_OPT_CLIQUE_MODE, 1)]
+    assert (_native.GR_OPT_KEEP_GRAPH, _native.GR_OPT_CLIQUE_MODE) == (4, 5)
