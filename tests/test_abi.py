@@ -97,3 +97,65 @@ def test_option_setters_pass_header_keys():
                               (_native.GR_OPT_AUTOTUNE, 5), (_native.GR_OPT_KEEP_GRAPH, 1),
                               (_native.GR_OPT_CLIQUE_MODE, 2), (_native.GR_OPT_CLIQUE_MODE, 1)]
     assert (_native.GR_OPT_KEEP_GRAPH, _native.GR_OPT_CLIQUE_MODE) == (4, 5)
+
+
+def _prototypes():
+    with open(HEADER) as f:
+        src = re.sub(r"/\*.*?\*/", "", f.read(), flags=re.S)
+    src = re.sub(r"^\s*#.*$", "", src, flags=re.M)
+    out = {}
+    for ret, name, args in re.findall(r"([A-Za-z_][\w\s\*]*?)\b(gr_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;",
+                                      src, flags=re.S):
+        params = [] if args.strip() in ("", "void") else [a.strip() for a in args.split(",")]
+        types = [" ".join(re.match(r"(.*?)\w+$", p, flags=re.S).group(1).split()) for p in params]
+        out[name] = (" ".join(ret.split()), types)
+    return out
+
+
+def _kind_c(t):
+    t = t.replace("const ", "").replace(" *", "*").strip()
+    if t.endswith("*"):
+        return "ptr"
+    return {"int": ("int", 4), "int32_t": ("int", 4), "int64_t": ("int", 8),
+            "double": ("float", 8)}[t]
+
+
+def _kind_ctypes(c):
+    if c in (ctypes.c_void_p, ctypes.c_char_p) or hasattr(c, "_type_") and isinstance(c._type_, type):
+        return "ptr"
+    kind = "float" if c in (ctypes.c_double, ctypes.c_float) else "int"
+    return (kind, ctypes.sizeof(c))
+
+
+def test_binding_signatures_match_prototypes():
+    """Every ctypes signature agrees with its C prototype: pointers for
+    pointers, and scalars of the same kind and width (a narrower integer
+    here would silently truncate a size)."""
+    protos = _prototypes()
+    assert sorted(protos) == sorted(_native.SIGNATURES)
+    for name, (ret, types) in protos.items():
+        res, argtypes = _native.SIGNATURES[name]
+        assert [_kind_c(t) for t in types] == [_kind_ctypes(a) for a in argtypes], name
+        assert _kind_c(ret) == _kind_ctypes(res), name
+
+
+def test_stats_struct_layout(tmp_path):
+    """gr_stats as the C compiler lays it out equals the ctypes structure."""
+    import shutil
+    import subprocess
+
+    if shutil.which("gcc") is None:
+        pytest.skip("needs gcc")
+    fields = [f for f, _ in _native.GrStats._fields_]
+    prog = ("#include <stdio.h>\n#include <stddef.h>\n#include \"gramsci_cuda.h\"\n"
+            "int main(void) {\n  printf(\"%zu\\n\", sizeof(gr_stats));\n"
+            + "".join(f"  printf(\"%zu\\n\", offsetof(gr_stats, {f}));\n" for f in fields)
+            + "  return 0;\n}\n")
+    (tmp_path / "s.c").write_text(prog)
+    r = subprocess.run(["gcc", "-std=c99", "-I", os.path.dirname(HEADER), str(tmp_path / "s.c"),
+                        "-o", str(tmp_path / "s")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    vals = [int(x) for x in subprocess.run([str(tmp_path / "s")], capture_output=True,
+                                           text=True).stdout.split()]
+    assert vals[0] == ctypes.sizeof(_native.GrStats)
+    assert vals[1:] == [getattr(_native.GrStats, f).offset for f in fields]
