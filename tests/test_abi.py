@@ -139,17 +139,26 @@ def test_binding_signatures_match_prototypes():
         assert _kind_c(ret) == _kind_ctypes(res), name
 
 
-def test_stats_struct_layout(tmp_path):
-    """gr_stats as the C compiler lays it out equals the ctypes structure."""
+def _struct_cases():
+    from gramsci_b200 import host
+
+    return [("gramsci_cuda.h", "gr_stats", _native.GrStats),
+            ("gramsci_host.h", "grh_options", host.Options)]
+
+
+@pytest.mark.parametrize("header,cname,cls", _struct_cases(), ids=["gr_stats", "grh_options"])
+def test_struct_layout(tmp_path, header, cname, cls):
+    """The C compiler's layout of a struct crossing the ABI (size and every
+    field offset) equals the ctypes structure's."""
     import shutil
     import subprocess
 
     if shutil.which("gcc") is None:
         pytest.skip("needs gcc")
-    fields = [f for f, _ in _native.GrStats._fields_]
-    prog = ("#include <stdio.h>\n#include <stddef.h>\n#include \"gramsci_cuda.h\"\n"
-            "int main(void) {\n  printf(\"%zu\\n\", sizeof(gr_stats));\n"
-            + "".join(f"  printf(\"%zu\\n\", offsetof(gr_stats, {f}));\n" for f in fields)
+    fields = [f for f, _ in cls._fields_]
+    prog = (f"#include <stdio.h>\n#include <stddef.h>\n#include \"{header}\"\n"
+            f"int main(void) {{\n  printf(\"%zu\\n\", sizeof({cname}));\n"
+            + "".join(f"  printf(\"%zu\\n\", offsetof({cname}, {f}));\n" for f in fields)
             + "  return 0;\n}\n")
     (tmp_path / "s.c").write_text(prog)
     r = subprocess.run(["gcc", "-std=c99", "-I", os.path.dirname(HEADER), str(tmp_path / "s.c"),
@@ -157,5 +166,5 @@ def test_stats_struct_layout(tmp_path):
     assert r.returncode == 0, r.stderr
     vals = [int(x) for x in subprocess.run([str(tmp_path / "s")], capture_output=True,
                                            text=True).stdout.split()]
-    assert vals[0] == ctypes.sizeof(_native.GrStats)
-    assert vals[1:] == [getattr(_native.GrStats, f).offset for f in fields]
+    assert vals[0] == ctypes.sizeof(cls)
+    assert vals[1:] == [getattr(cls, f).offset for f in fields]
