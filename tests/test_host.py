@@ -135,3 +135,33 @@ def test_cli_without_gpu_fails_loudly(tmp_path):
     assert res.returncode == 1
     assert "gr_create failed (-3): no usable CUDA device" in res.stderr
     assert not out.exists()
+
+
+def test_tables_read_by_the_reference_harness(tmp_path):
+    """The reference's own test harness reads result tables with
+    np.loadtxt(out, skiprows=1) and averages columns 4 / 5 (2PCF, N2 / N3)
+    and 6 / 7 (3PCF) (tests/run_correlation_tests.py:24-40).  Tables written
+    here parse the same way, with the ratio column NaN or Infinity where
+    N3 is 0, and the column means agree with the histograms to E14.7's 7
+    digits."""
+    rng = np.random.default_rng(4)
+    e = host.radial_bins(1.0, 30.0, 10)
+    N2, N3 = rng.uniform(1e-8, 1e-6, (10, 10)), rng.uniform(1e-8, 1e-6, (10, 10))
+    N3[0, 0] = 0.0
+    N2[1, 1] = N3[1, 1] = 0.0
+    p2 = tmp_path / "tmp_2pcf.out"
+    assert host.write_2pcf(str(p2), e, 10, 10, N2, N3) == 0
+    t2 = np.loadtxt(p2, skiprows=1)
+    assert t2.shape == (100, 7)
+    np.testing.assert_allclose(np.mean(t2[:, 4]), N2.mean(), rtol=1e-7)
+    np.testing.assert_allclose(np.mean(t2[:, 5]), N3.mean(), rtol=1e-7)
+    assert np.isinf(t2[0, 6]) and np.isnan(t2[11, 6])
+    e6 = host.radial_bins(1.0, 30.0, 6)
+    nc = 6 * 7 * 8 // 6
+    M2, M3 = rng.uniform(1e-13, 1e-11, (nc, 1)), rng.uniform(1e-13, 1e-11, (nc, 1))
+    p3 = tmp_path / "tmp_3pcf.out"
+    assert host.write_3pcf(str(p3), e6, 6, 1, M2, M3) == 0
+    t3 = np.loadtxt(p3, skiprows=1)
+    assert t3.shape == (nc, 9)
+    np.testing.assert_allclose(np.mean(t3[:, 6]), M2.mean(), rtol=1e-7)
+    np.testing.assert_allclose(np.mean(t3[:, 7]), M3.mean(), rtol=1e-7)
