@@ -165,3 +165,30 @@ def test_tables_read_by_the_reference_harness(tmp_path):
     assert t3.shape == (nc, 9)
     np.testing.assert_allclose(np.mean(t3[:, 6]), M2.mean(), rtol=1e-7)
     np.testing.assert_allclose(np.mean(t3[:, 7]), M3.mean(), rtol=1e-7)
+
+
+def _e14_7_model(v):
+    """Fortran E14.7 of a finite double with a two-digit exponent, from the
+    exact decimal value: 0.ddddddd x 10^e with 0.1 <= mantissa < 1, rounded
+    to nearest, right-aligned in 14 characters."""
+    from decimal import ROUND_HALF_EVEN, Decimal
+
+    if v == 0.0:
+        return " 0.0000000E+00"
+    d = abs(Decimal(v))
+    e = d.adjusted() + 1  # d = m * 10^e with 0.1 <= m < 1
+    m = (d.scaleb(-e)).quantize(Decimal("1e-7"), rounding=ROUND_HALF_EVEN)
+    if m >= 1:
+        m, e = Decimal("0.1000000"), e + 1
+    body = f"{m:.7f}E{'+' if e >= 0 else '-'}{abs(e):02d}"
+    return ("-" if v < 0 else "") + body.rjust(13 if v < 0 else 14)
+
+
+def test_e14_7_matches_exact_decimal_model():
+    rng = np.random.default_rng(7)
+    vals = rng.uniform(-1, 1, 4000) * 10.0 ** rng.integers(-95, 95, 4000)
+    # values next to a rounding boundary of the 7th digit and to a power of 10
+    vals = np.concatenate([vals, [9.99999995, 9.9999999499999, 0.99999995, 1.00000005e-3,
+                                  -9.99999996e50, 1e-99, 9.99999e98]])
+    for v in vals:
+        assert host.format_e14_7(float(v)) == _e14_7_model(float(v)), repr(v)
