@@ -192,3 +192,25 @@ def test_e14_7_matches_exact_decimal_model():
                                   -9.99999996e50, 1e-99, 9.99999e98]])
     for v in vals:
         assert host.format_e14_7(float(v)) == _e14_7_model(float(v)), repr(v)
+
+
+def test_read_catalogue_number_forms_roundtrip(tmp_path):
+    """17-significant-digit values in the forms list-directed input takes
+    (plain, E or D exponent, lower or upper case) and with space, comma or
+    tab separators read back bit-exactly."""
+    rng = np.random.default_rng(9)
+    n = 600
+    vals = rng.uniform(-1, 1, (n, 4)) * 10.0 ** rng.integers(-30, 30, (n, 4))
+    forms = [lambda x: f"{x:.17g}", lambda x: f"{x:.16E}", lambda x: f"{x:.16e}".replace("e", "d"),
+             lambda x: f"{x:.16E}".replace("E", "D")]
+    seps = [" ", ", ", "\t", "   "]
+    lines = []
+    for i, row in enumerate(vals):
+        f, s = forms[i % len(forms)], seps[(i // len(forms)) % len(seps)]
+        lines.append(s.join(f(float(x)) for x in row))
+    g, r = tmp_path / "g", tmp_path / "r"
+    g.write_text("\n".join(lines[:400]) + "\n")
+    r.write_text("\n".join(lines[400:]) + "\n")
+    xyz, w, nd, nr = host.read_catalogue(str(g), str(r))
+    assert (nd, nr) == (400, 200)
+    assert np.array_equal(xyz, vals[:, :3]) and np.array_equal(w, vals[:, 3])
