@@ -37,14 +37,15 @@ extern "C" {
 #define GR_E_ARG (-1)         /* invalid argument or call order            */
 #define GR_E_CAPACITY (-2)    /* a size exceeds what the library supports  */
 #define GR_E_CUDA (-3)        /* CUDA runtime error                        */
-#define GR_E_TIMEOUT (-4)     /* a bounded device wait ran out             */
+#define GR_E_TIMEOUT (-4)     /* reserved: no call waits on the device     */
 #define GR_E_UNSUPPORTED (-5) /* option not available                      */
 
 typedef struct gr_ctx gr_ctx;
 
 /* Options for gr_set_option. */
 #define GR_OPT_PRECISION 1 /* 0: FP32 separations + FP64 guard band (default); 1: FP64 throughout */
-#define GR_OPT_TIMEOUT_MS 2 /* bound on device-side waits in the persistent batched kernel */
+#define GR_OPT_TIMEOUT_MS 2 /* accepted (> 0) and stored; no kernel of this library waits on
+                               another block, a flag or another device, so nothing uses it */
 #define GR_OPT_AUTOTUNE 3   /* 0: fixed kernels; 1: time the pair-sweep variants once per
                                workload class and cache the choice (default); 2+v: force
                                variant v (0 warp per cell, 1/2 block per cell of 128/256,
