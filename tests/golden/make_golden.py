@@ -23,8 +23,9 @@ Cases
                 pins the perimeter order, the root-row length rule (every row
                 holds 4 > 3 neighbours), the non-canonical table entries
                 (taken as 0) and the six disconnected-term gates; the
-                -equi and -tetra answers likewise, and the closed-form
-                weight gradients of the 2/3/4PCF sums.
+                -equi and -tetra answers likewise, the closed-form
+                weight gradients of the 2/3/4PCF sums, and the counts with
+                the centre as a buffer point.
 Run: python tests/golden/make_golden.py
 """
 import itertools
@@ -164,7 +165,17 @@ def main():
         # dL/dw_k = 4 * product of the other three vertices, 0 for the centre
         grad2=[-2 * g] * 3 + [-2 * r] * 2,
         grad3=[3 * (g * g + 4 * g * r + r * r)] * 3 + [3 * (3 * g * g + 3 * g * r)] * 2,
-        grad4=[4 * g * g * r] * 3 + [4 * g ** 3, 0.0]))
+        grad4=[4 * g * g * r] * 3 + [4 * g ** 3, 0.0],
+        # the centre as a buffer point (gramsci.F90:363,476,672): it roots
+        # nothing, so its 3 + 1 directed pairs go and the six centre
+        # triangles are counted from two vertices instead of three; the
+        # 4PCF is unchanged because a buffer point still counts in its
+        # neighbours' rows (every vertex row keeps 4 > 3 entries)
+        buffer_case=dict(
+            buffer=[0, 0, 0, 0, 1],
+            counts2={"2,1,0": 6, "2,1,1": 3, "2,1,2": 3, "1,1,1": 3, "1,1,3": 1},
+            counts3={"7,1,0": 3, "7,1,1": 9, "2,1,1": 6, "2,1,2": 6},
+            N2_3={"7,1": 3 * g ** 3 + 9 * g * g * r, "2,1": 6 * g * g * r + 6 * g * r * r})))
     with open(os.path.join(HERE, "known_answers.json"), "w") as f:
         json.dump(cases, f, indent=1)
 

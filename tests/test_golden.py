@@ -95,6 +95,14 @@ def test_oracle_known_answers(oracle, c):
         _check4(c, G.pcf4(w, c["n_data"]))
     if "counts_equi" in c:
         _check_special(c, G.equi(w, c["n_data"]), G.tetra(w, c["n_data"]))
+    if "buffer_case" in c:
+        bc = dict(c, **c["buffer_case"])
+        buf = np.array(bc["buffer"], np.int32)
+        nd = c["n_data"]
+        r3b = G.pcf3(w, nd, buffer=buf)
+        _check(bc, G.pcf2(w, nd, buffer=buf)["counts"], r3b["counts"], r3b["N2"])
+        if "counts4" in bc:
+            _check4(bc, G.pcf4(w, nd, buffer=buf))
     if "grad2" in c:
         nd, nb, nm = c["n_data"], c["nbins"], c["nmu"]
         r4 = G.pcf4(w, nd)
