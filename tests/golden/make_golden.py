@@ -9,7 +9,8 @@ Cases
   collinear     points at x = 0, 3, 4, 7, 10, 11: separations that land
                 exactly on bin edges (t = 1.0 and 2.0 after IEEE rounding of
                 (d - rmin) * fl(1/3)), on rmin (excluded) and on rmax
-                (excluded).
+                (excluded); in log bins (rmin 1, rmax 100, 2 bins) a
+                separation on the edge at 10.
   los           two pairs 1000 Mpc/h from the observer, one radial, one
                 transverse, nmu 4: mu bins from each end (radial: 1 and 4
                 after clamping; transverse: 2 and 3).
@@ -70,8 +71,26 @@ def main():
     # written out: bin 1 {0-3, 4-7, 7-10}, bin 2 {0-4, 3-7, 4-10, 7-11},
     # bin 3 {0-7, 3-10, 3-11, 4-11}; each pair counted from both ends
     assert counts2 == {"1,1,0": 6, "2,1,0": 8, "3,1,0": 8}, counts2
+    # the same points in log bins: rmin 1, rmax 100, 2 bins, edges 1, 10, 100
+    # (gramsci.F90:136-139, :334-335).  Separations 3, 4, 7 (three pairs
+    # each), 6 and 8 fall in bin 1; 10 lands exactly on the edge
+    # (log10(10) = 1, t = 1.0) and 11 above it: bin 2; the two pairs at
+    # d = 1 = rmin are excluded
+    log2 = {}
+    for i, a in enumerate(xs):
+        for j, b in enumerate(xs):
+            d = abs(b - a)
+            if i == j or d <= 1.0 or d >= 100.0:
+                continue
+            bb = min(int(math.floor((math.log10(d) - math.log10(1.0)) * (1.0 / (2.0 / 2)))) + 1, 2)
+            k = f"{bb},1,0"
+            log2[k] = log2.get(k, 0) + 1
+    assert log2 == {"1,1,0": 22, "2,1,0": 4}, log2
     cases.append(dict(name="collinear", xyz=pts, w=[1.0] * 6, n_data=6, rmin=1.0, rmax=10.0,
-                      nbins=3, nmu=1, counts2=counts2))
+                      nbins=3, nmu=1, counts2=counts2,
+                      log_case=dict(rmin=1.0, rmax=100.0, nbins=2, counts2=log2,
+                                    edges={"0,4": [2, 1], "4,0": [2, 1], "0,5": [2, 1],
+                                           "0,3": [1, 1]})))
     # line of sight: observer at the origin, nmu = 4
     pts = [[1000.0, 0.0, 0.0], [1005.0, 0.0, 0.0], [0.0, 1000.0, 0.0], [0.0, 1000.0, 5.0]]
     # radial pair: theta(0->1) = -1 -> bin 1; theta(1->0) = +1 -> bin 5 -> 4

@@ -95,6 +95,15 @@ def test_oracle_known_answers(oracle, c):
         _check4(c, G.pcf4(w, c["n_data"]))
     if "counts_equi" in c:
         _check_special(c, G.equi(w, c["n_data"]), G.tetra(w, c["n_data"]))
+    if "log_case" in c:
+        lc = dict(c, **c["log_case"])
+        GL = oracle.Graph(xyz, lc["rmin"], lc["rmax"], lc["nbins"], lc["nmu"], logbins=True)
+        _check(lc, GL.pcf2(w, c["n_data"])["counts"])
+        rp, col, b, mu = GL.csr()
+        for k, (eb, em) in lc["edges"].items():
+            i, j = map(int, k.split(","))
+            e = rp[i] + list(col[rp[i]:rp[i + 1]]).index(j)
+            assert (b[e], mu[e]) == (eb, em), k
     if "buffer_case" in c:
         bc = dict(c, **c["buffer_case"])
         buf = np.array(bc["buffer"], np.int32)
