@@ -82,9 +82,10 @@ def test_graph_matches_brute_force(oracle, nmu, method):
 
 
 @pytest.mark.parametrize("nmu", [1, 3])
-def test_log_bin_graph_matches_brute_force(oracle, nmu):
+@pytest.mark.parametrize("method", ["grid", "kdtree"])
+def test_log_bin_graph_matches_brute_force(oracle, nmu, method):
     xyz, w, nd = small_catalogue(40, 60, 100.0, 4)
-    G = oracle.Graph(xyz, 1.5, 40.0, 7, nmu, logbins=True)
+    G = oracle.Graph(xyz, 1.5, 40.0, 7, nmu, logbins=True, method=method)
     rp, col, b, mu = G.csr()
     E = brute_edges(xyz, 1.5, 40.0, 7, nmu, logbins=True)
     got = {(i, int(col[k])): (int(b[k]), int(mu[k]))
