@@ -162,12 +162,13 @@ def test_2pcf_3pcf_match_brute_force(oracle, nmu):
     assert np.allclose(r3["N3"], -r3["catsum"][:, :, 3], rtol=1e-13, atol=1e-300)
 
 
+@pytest.mark.parametrize("logbins", [False, True])
 @pytest.mark.parametrize("with_buffer", [False, True])
-def test_4pcf_matches_brute_force(oracle, with_buffer):
+def test_4pcf_matches_brute_force(oracle, with_buffer, logbins):
     xyz, w, nd = small_catalogue(25, 25, 30.0, 3)
     buf = (np.arange(len(xyz)) % 5 == 2).astype(np.int32) if with_buffer else None
     nbins = 3
-    E = brute_edges(xyz, 1.0, 12.0, nbins, 1)
+    E = brute_edges(xyz, 1.0, 12.0, nbins, 1, logbins=logbins)
     n = len(xyz)
     nbrs = {i: sorted(j for (a, j) in E if a == i) for i in range(n)}
     nc = oracle.ncfg4(nbins)
@@ -211,7 +212,7 @@ def test_4pcf_matches_brute_force(oracle, with_buffer):
                     if npr == 2:
                         dcnt[cfg - 1, d1 - 1, d2 - 1, t, 3] += 1
                         dr[cfg - 1, d1 - 1, d2 - 1, t] += pw
-    G = oracle.Graph(xyz, 1.0, 12.0, nbins, 1)
+    G = oracle.Graph(xyz, 1.0, 12.0, nbins, 1, logbins=logbins)
     r4 = G.pcf4(w, nd, buffer=buf)
     assert cnt.sum() > 0
     assert np.array_equal(r4["counts"], cnt)
