@@ -114,8 +114,8 @@ def test_rmin_zero_and_duplicates(oracle):
     assert rp[5] - rp[4] == 0
 
 
-def _brute_counts(xyz, w, nd, rmin, rmax, nbins, nmu, normal, buffer=None):
-    E = brute_edges(xyz, rmin, rmax, nbins, nmu)
+def _brute_counts(xyz, w, nd, rmin, rmax, nbins, nmu, normal, buffer=None, logbins=False):
+    E = brute_edges(xyz, rmin, rmax, nbins, nmu, logbins=logbins)
     n = len(xyz)
     nb = {i: sorted(j for (a, j) in E if a == i) for i in range(n)}
     rnd = lambda i: i >= nd  # noqa: E731
@@ -146,13 +146,14 @@ def _brute_counts(xyz, w, nd, rmin, rmax, nbins, nmu, normal, buffer=None):
     return c2, c3, s3
 
 
+@pytest.mark.parametrize("logbins", [False, True])
 @pytest.mark.parametrize("nmu", [1, 3])
-def test_2pcf_3pcf_match_brute_force(oracle, nmu):
+def test_2pcf_3pcf_match_brute_force(oracle, nmu, logbins):
     xyz, w, nd = small_catalogue(30, 45, 60.0, 2)
     buf = (np.arange(len(xyz)) % 7 == 3).astype(np.int32)
     normal = oracle.normal_table(nmu)
-    c2, c3, s3 = _brute_counts(xyz, w, nd, 2.0, 20.0, 5, nmu, normal, buffer=buf)
-    G = oracle.Graph(xyz, 2.0, 20.0, 5, nmu)
+    c2, c3, s3 = _brute_counts(xyz, w, nd, 2.0, 20.0, 5, nmu, normal, buffer=buf, logbins=logbins)
+    G = oracle.Graph(xyz, 2.0, 20.0, 5, nmu, logbins=logbins)
     r2 = G.pcf2(w, nd, buffer=buf)
     r3 = G.pcf3(w, nd, buffer=buf)
     assert np.array_equal(r2["counts"], c2)
