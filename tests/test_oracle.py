@@ -354,37 +354,67 @@ def test_adjoint_4pcf_matches_finite_differences(oracle):
         assert abs(fd - g[k]) <= 1e-10 * gmax, (k, fd, g[k])
 
 
-def test_equi_and_tetra_match_brute_force(oracle):
+@pytest.mark.parametrize("nm,with_buffer", [(2, False), (1, False), (1, True)])
+def test_equi_and_tetra_match_brute_force(oracle, nm, with_buffer):
     """-equi / -tetra (gramsci.F90:402-660): same-bin triangles and 4-cliques,
-    against an independent enumeration."""
+    counts and weighted sums, against an independent enumeration."""
     xyz, w, nd = small_catalogue(30, 30, 30.0, 6)
-    nb, nm = 3, 2
+    nb = 3
+    buf = (np.arange(len(xyz)) % 6 == 1).astype(np.int32) if with_buffer else None
     E = brute_edges(xyz, 1.0, 12.0, nb, nm)
     n = len(xyz)
     nbrs = {i: sorted(j for (a, j) in E if a == i) for i in range(n)}
     normal = oracle.normal_table(nm)
+    rnd = lambda i: i >= nd  # noqa: E731
     ce = np.zeros((nb, nm, 4), np.int64)
+    e2, e3 = np.zeros((nb, nm)), np.zeros((nb, nm))
     ct = np.zeros((nb, 5), np.int64)
+    t2, t3 = np.zeros(nb), np.zeros(nb)
+    dn, dr = np.zeros((nb, 6)), np.zeros((nb, 6))
     for i in range(n):
+        if buf is not None and buf[i]:
+            continue
         for a, c in itertools.combinations(nbrs[i], 2):
             b = E[(i, a)][0]
             if E[(i, c)][0] != b or E.get((a, c), (0,))[0] != b:
                 continue
-            m = normal[E[(i, a)][1] - 1, E[(i, c)][1] - 1]
-            ce[b - 1, m - 1, (i >= nd) + (a >= nd) + (c >= nd)] += 1
+            m = normal[E[(i, a)][1] - 1, E[(i, c)][1] - 1] if nm >= 2 else 1
+            ce[b - 1, m - 1, rnd(i) + rnd(a) + rnd(c)] += 1
+            e2[b - 1, m - 1] += w[i] * w[a] * w[c]
+            # without mu bins N3 takes minus the all-random products
+            # (gramsci.F90:430-433); with them only N2 is summed
+            if nm == 1 and rnd(i) and rnd(a) and rnd(c):
+                e3[b - 1, 0] -= w[i] * w[a] * w[c]
         for a, b2, c in itertools.combinations(nbrs[i], 3):
             b = E[(i, a)][0]
-            ok = all(E.get(e, (0,))[0] == b for e in [(i, b2), (i, c), (a, b2), (b2, c), (a, c)])
-            if ok:
-                ct[b - 1, sum(x >= nd for x in (i, a, b2, c))] += 1
+            if not all(E.get(e, (0,))[0] == b for e in [(i, b2), (i, c), (a, b2), (b2, c), (a, c)]):
+                continue
+            ct[b - 1, sum(rnd(x) for x in (i, a, b2, c))] += 1
+            p4 = w[i] * w[a] * w[b2] * w[c]
+            t2[b - 1] += p4
+            if all(rnd(x) for x in (i, a, b2, c)):
+                t3[b - 1] += p4
+            # the six disconnected terms: (gate, the two other vertices of
+            # the triple product), term t at index t-1 (:581-628)
+            for t, (gate, u, v) in enumerate([(c, i, a), (c, i, b2), (a, i, c),
+                                              (i, a, b2), (i, c, b2), (i, c, a)]):
+                if rnd(gate):
+                    pw = w[gate] * w[u] * w[v]
+                    dn[b - 1, t] += pw
+                    if rnd(u) and rnd(v):
+                        dr[b - 1, t] += pw
     G = oracle.Graph(xyz, 1.0, 12.0, nb, nm)
-    e = G.equi(w, nd)
-    t = G.tetra(w, nd)
+    e = G.equi(w, nd, buffer=buf)
+    t = G.tetra(w, nd, buffer=buf)
     assert ce.sum() > 0 and ct.sum() > 0
     assert np.array_equal(e["counts"], ce)
     assert np.array_equal(t["counts"], ct)
-    # with RSD the reference sums only N2 for -equi
-    assert np.all(e["N3"] == 0)
+    for got, ref in ((e["N2"], e2), (e["N3"], e3), (t["N2"], t2), (t["N3"], t3),
+                     (t["discN"], dn), (t["discR"], dr)):
+        np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-14 * max(np.abs(ref).max(), 1e-300))
+    if nm >= 2:
+        # with mu bins the reference sums only N2 for -equi
+        assert np.all(e["N3"] == 0)
 
 
 def test_empty_single_and_all_buffer_catalogues(oracle):
