@@ -280,16 +280,18 @@ def test_normalise_matches_reference_rule(oracle):
     assert abs(a[:400].sum() - 1) < 1e-12 and abs(a[400:].sum() + 1) < 1e-12
 
 
-def test_adjoint_2pcf_matches_finite_differences(oracle):
+@pytest.mark.parametrize("with_buffer", [False, True])
+def test_adjoint_2pcf_matches_finite_differences(oracle, with_buffer):
     xyz, w, nd = small_catalogue(30, 40, 60.0, 4)
+    buf = (np.arange(len(w)) % 4 == 1).astype(np.int32) if with_buffer else None
     G = oracle.Graph(xyz, 2.0, 20.0, 4, 3)
     rng = np.random.default_rng(9)
     cot2 = rng.normal(size=(4, 3))
     cot3 = rng.normal(size=(4, 3))
-    g = G.adjoint2(w, nd, cot2, cot3)
+    g = G.adjoint2(w, nd, cot2, cot3, buffer=buf)
 
     def L(wv):
-        r = G.pcf2(wv, nd)
+        r = G.pcf2(wv, nd, buffer=buf)
         return float((cot2 * r["N2"]).sum() + (cot3 * r["N3"]).sum())
 
     for k in rng.choice(len(w), 8, replace=False):
@@ -301,18 +303,20 @@ def test_adjoint_2pcf_matches_finite_differences(oracle):
         assert abs(fd - g[k]) <= 1e-8 * max(abs(fd), abs(g[k]), 1e-30)
 
 
-def test_adjoint_3pcf_matches_finite_differences(oracle):
+@pytest.mark.parametrize("with_buffer", [False, True])
+def test_adjoint_3pcf_matches_finite_differences(oracle, with_buffer):
     xyz, w, nd = small_catalogue(30, 40, 50.0, 5)
+    buf = (np.arange(len(w)) % 4 == 1).astype(np.int32) if with_buffer else None
     nb, nm = 3, 2
     G = oracle.Graph(xyz, 2.0, 20.0, nb, nm)
     rng = np.random.default_rng(10)
     nc = oracle.ncfg3(nb)
     cot2 = rng.normal(size=(nc, nm))
     cot3 = rng.normal(size=(nc, nm))
-    g = G.adjoint3(w, nd, cot2, cot3)
+    g = G.adjoint3(w, nd, cot2, cot3, buffer=buf)
 
     def L(wv):
-        r = G.pcf3(wv, nd)
+        r = G.pcf3(wv, nd, buffer=buf)
         return float((cot2 * r["N2"]).sum() + (cot3 * r["N3"]).sum())
 
     for k in rng.choice(len(w), 8, replace=False):
