@@ -446,3 +446,21 @@ def test_galaxies_only_have_no_random_terms(oracle):
     for r in (r2, r3, r4):
         assert not r["N3"].any() and not r["counts"][..., 1:].any()
     assert not r4["discN"].any() and not r4["discR"].any()
+
+
+@pytest.mark.parametrize("method", ["grid", "kdtree"])
+def test_thread_count_does_not_change_results(oracle, method):
+    """The reference arm runs the oracle on every host thread: the graph and
+    the integer counts do not depend on the thread count, and the sums
+    only to rounding."""
+    cat = catalogs.make("c2_3pcf", scale=0.01)
+    w = catalogs.normalise(cat.w, cat.n_data, cat.n_rand)
+    sp = catalogs.WORKLOADS["c2_3pcf"]
+    args = (cat.xyz, sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
+    G1 = oracle.Graph(*args, method=method, threads=1)
+    G4 = oracle.Graph(*args, method=method, threads=4)
+    for x, y in zip(G1.csr(), G4.csr()):
+        assert np.array_equal(x, y)
+    a, b = G1.pcf3(w, cat.n_data), G4.pcf3(w, cat.n_data)
+    assert a["counts"].sum() > 0 and np.array_equal(a["counts"], b["counts"])
+    np.testing.assert_allclose(a["catsum"], b["catsum"], rtol=1e-12, atol=1e-15 * np.abs(a["catsum"]).max())
