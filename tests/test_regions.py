@@ -139,3 +139,53 @@ def test_resum_tetra_disc_column_is_nan(tmp_path):
     assert host.resum(6, [p, p], tmp_path / "s") == 0
     v = np.array([[float(x) for x in l.split()] for l in _text(tmp_path / "s").splitlines()])
     assert np.all(v[:, 4] == 2.0) and np.all(np.isnan(v[:, 7]))
+
+
+def _rows(path, header=True):
+    lines = _text(path).splitlines()[1 if header else 0:]
+    return np.array([[float(x) for x in l.split()] for l in lines])
+
+
+@pytest.mark.parametrize("query,nmu", [(3, 1), (3, 3), (4, 1), (5, 2)])
+def test_resum_other_tables(tmp_path, query, nmu):
+    """gramsci-resum on 3PCF (with and without mu columns), 4PCF and -equi
+    tables: header and bin columns copied, N2 and N3 summed from the tables' values,
+    the ratio recomputed; the 4PCF disconnected-term columns, ratios of
+    sums the tables do not hold, come out NaN."""
+    rng = np.random.default_rng(query * 10 + nmu)
+    nb = 3
+    e = host.radial_bins(1.0, 9.0, nb)
+    parts = []
+    for k in range(3):
+        p = tmp_path / f"t{k}"
+        if query == 3:
+            nc = nb * (nb + 1) * (nb + 2) // 6
+            N2, N3 = rng.uniform(-1, 1, (nc, nmu)), rng.uniform(0.5, 1, (nc, nmu))
+            assert host.write_3pcf(str(p), e, nb, nmu, N2, N3) == 0
+        elif query == 4:
+            nc = nb * (nb + 1) * (nb + 2) * (nb + 3) // 24
+            N2, N3 = rng.uniform(-1, 1, (nc, nb, nb)), rng.uniform(0.5, 1, (nc, nb, nb))
+            d = rng.uniform(0.5, 1, (nc, nb, nb, 6))
+            assert host.write_4pcf(str(p), e, nb, N2, N3, d, d) == 0
+        else:
+            N2, N3 = rng.uniform(-1, 1, (nb, nmu)), rng.uniform(0.5, 1, (nb, nmu))
+            assert host.write_equi(str(p), e, nb, nmu, N2, N3) == 0
+        parts.append(p)
+    out = tmp_path / "sum"
+    assert host.resum(query, parts, out) == 0
+    # the -equi table has no header line (gramsci.F90:448-458)
+    hdr = query != 5
+    rows = [_rows(p, hdr) for p in parts]
+    got = _rows(out, hdr)
+    if hdr:
+        assert _text(out).splitlines()[0] == _text(parts[0]).splitlines()[0]
+    # column of N2: after the bin columns (3PCF: 6 edges [+ 2 mu];
+    # 4PCF: 8 edges; -equi: 2 edges + 2 mu)
+    c = {3: 6 if nmu == 1 else 8, 4: 8, 5: 4}[query]
+    assert got.shape == rows[0].shape
+    np.testing.assert_array_equal(got[:, :c], rows[0][:, :c])
+    tot = sum(r[:, c:c + 2] for r in rows)
+    np.testing.assert_allclose(got[:, c:c + 2], tot, rtol=1e-6, atol=1e-7)
+    np.testing.assert_allclose(got[:, c + 2], got[:, c] / got[:, c + 1], rtol=1e-6)
+    if query == 4:
+        assert np.all(np.isnan(got[:, c + 3:]))
