@@ -50,3 +50,28 @@ def test_normalise_follows_the_reference_rule(name):
     w = catalogs.normalise(cat.w, cat.n_data, cat.n_rand)
     assert np.all(w[:cat.n_data] > 0) and np.all(w[cat.n_data:] < 0)
     assert abs(w[:cat.n_data].sum() - 1.0) < 1e-12 and abs(w[cat.n_data:].sum() + 1.0) < 1e-12
+
+
+def test_torch_normalise_matches_and_differentiates():
+    """autograd.normalise (torch, differentiable) equals catalogs.normalise,
+    and its Jacobian is the quotient rule of w_k / sum(w) per catalogue."""
+    import torch
+
+    from gramsci_b200 import autograd
+
+    rng = np.random.default_rng(5)
+    nd, nr = 4, 3
+    raw = rng.lognormal(0, 0.3, nd + nr)
+    t = torch.tensor(raw, dtype=torch.float64, requires_grad=True)
+    out = autograd.normalise(t, nd)
+    np.testing.assert_allclose(out.detach().numpy(), catalogs.normalise(raw, nd, nr), rtol=1e-15)
+    J = torch.autograd.functional.jacobian(lambda x: autograd.normalise(x, nd), t).numpy()
+    for lo, hi, sign in ((0, nd, 1.0), (nd, nd + nr, -1.0)):
+        S = raw[lo:hi].sum()
+        for i in range(lo, hi):
+            for k in range(lo, hi):
+                exp = sign * ((i == k) / S - raw[i] / S ** 2)
+                assert abs(J[i, k] - exp) <= 1e-14 * max(1.0, abs(exp)), (i, k)
+        # no coupling between the two catalogues
+        other = [k for k in range(nd + nr) if not lo <= k < hi]
+        assert np.all(J[lo:hi][:, other] == 0)
