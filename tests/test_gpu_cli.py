@@ -4,6 +4,7 @@ the GPU) is compared with the table the same writer produces from the CPU
 oracle's N2/N3: identical layout and bin columns, values equal to the 7
 digits of E14.7 (a last-digit difference is allowed only where the two FP64
 sums straddle a rounding boundary of the 7th digit)."""
+import pathlib
 import subprocess
 
 import numpy as np
@@ -24,8 +25,8 @@ def _write_cat(tmp_path, name, scale):
 
 
 def _compare(a_path, b_path):
-    a = open(a_path).read().splitlines()
-    b = open(b_path).read().splitlines()
+    a = pathlib.Path(a_path).read_text().splitlines()
+    b = pathlib.Path(b_path).read_text().splitlines()
     assert len(a) == len(b)
     if a and a[0].startswith(" r1"):  # header line (2/3/4PCF tables)
         assert a[0] == b[0]
@@ -85,7 +86,7 @@ def _half_unit(v):
 
 
 def _table(path):
-    return np.array([[float(x) for x in l.split()] for l in open(path).read().splitlines()
+    return np.array([[float(x) for x in l.split()] for l in pathlib.Path(path).read_text().splitlines()
                      if not l.startswith(" r1")])
 
 

@@ -4,6 +4,8 @@
 A loaded graph must give the same counts as a fresh build (and as the
 oracle); any mismatch between the file and the context (bins, coordinates,
 damaged bytes) is refused on the host before anything reaches the device."""
+import pathlib
+
 import numpy as np
 import pytest
 
@@ -83,7 +85,7 @@ def test_load_refuses_mismatches(tmp_path):
             ctx.graph_load(path)
         # damaged payload
         ctx.set_catalog(cat.xyz, w, cat.n_data)
-        raw = bytearray(open(path, "rb").read())
+        raw = bytearray(pathlib.Path(path).read_bytes())
         raw[200] ^= 0x40
         bad = tmp_path / "bad.csr"
         bad.write_bytes(bytes(raw))
