@@ -121,10 +121,12 @@ class Context:
         self._check(self._lib.gr_set_option(self._h, _native.GR_OPT_PRECISION, v))
 
     def set_autotune(self, mode):
-        """'on' (time kernel variants once per workload class, cached),
-        'off', or an int variant to force (0 warp per cell, 1/2 block per
-        cell of 128/256 threads, 3 warp per cell with queued binning, 4/5
-        block per cell of 128/256 with queued binning)."""
+        """'on' (time kernel variants once per workload class, cached; dense
+        catalogues take cells of rmax/2 and the tile sweep), 'off', or an
+        int variant to force (0 warp per cell, 1/2 block per cell of 128/256
+        threads, 3 warp per cell with queued binning, 4/5 block per cell of
+        128/256 with queued binning, 6 the tile sweep, 7 the tile sweep on
+        cells of rmax/2; 6 and 7 need the FP32 path)."""
         v = {"off": 0, "on": 1}.get(mode, None)
         if v is None:
             v = 2 + int(mode)

@@ -10,12 +10,17 @@ differentiated.  The weights here are the signed normalised weights the
 reference forms after reading (src/gramsci.F90:1390-1391); normalise raw
 weights with `normalise` to differentiate through that step too.
 """
+import itertools
+
 import numpy as np
 import torch
 
 from . import api
 
 _contexts = {}
+# the forward call whose catalogue and bins each context holds (by device)
+_holder = {}
+_tokens = itertools.count(1)
 
 
 def _context(device):
@@ -23,6 +28,16 @@ def _context(device):
     if idx not in _contexts:
         _contexts[idx] = api.Context(idx)
     return _contexts[idx]
+
+
+def _load(c, w, xyz, n_data, bins):
+    """Hand the catalogue to the library: CUDA tensors by device pointer
+    (gr_set_catalog_dev, no host round trip), host tensors through NumPy."""
+    if xyz.is_cuda and w.is_cuda:
+        c.set_catalog(xyz.detach(), w.detach(), n_data)
+    else:
+        c.set_catalog(xyz.detach().cpu().numpy(), w.detach().cpu().numpy(), n_data)
+    c.set_bins(*bins)
 
 
 def normalise(w_raw, n_data):
@@ -37,12 +52,15 @@ class _PCF(torch.autograd.Function):
     @staticmethod
     def forward(ctx, w, xyz, n_data, bins, order):
         c = _context(w.device)
-        c.set_catalog(xyz.detach().cpu().numpy(), w.detach().cpu().numpy(), n_data)
-        c.set_bins(*bins)
+        _load(c, w, xyz, n_data, bins)
         count = {2: c.count_2pcf, 3: c.count_3pcf, 4: c.count_4pcf}[order]
         out = count()
         ctx.save_for_backward(w, xyz)
         ctx.n_data, ctx.bins, ctx.order = n_data, bins, order
+        # the context keeps this catalogue (and its graph) until another
+        # forward pass replaces it; the backward pass then skips the upload
+        ctx.token = next(_tokens)
+        _holder[id(c)] = ctx.token
         to = dict(dtype=torch.float64, device=w.device)
         names = ("N2", "N3", "discN", "discR") if order == 4 else ("N2", "N3")
         ctx.shapes = [out[k].shape for k in names]
@@ -52,8 +70,11 @@ class _PCF(torch.autograd.Function):
     def backward(ctx, *grads):
         w, xyz = ctx.saved_tensors
         c = _context(w.device)
-        c.set_catalog(xyz.detach().cpu().numpy(), w.detach().cpu().numpy(), ctx.n_data)
-        c.set_bins(*ctx.bins)
+        if _holder.get(id(c)) != ctx.token:
+            # another forward pass ran in between: upload this one's inputs
+            # again (the graph is then rebuilt by the adjoint call)
+            _load(c, w, xyz, ctx.n_data, ctx.bins)
+            _holder[id(c)] = ctx.token
         cots = [None if g is None else g.detach().cpu().numpy() for g in grads]
         if cots[0] is None:
             cots[0] = np.zeros(ctx.shapes[0])

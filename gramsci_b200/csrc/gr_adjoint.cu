@@ -250,7 +250,7 @@ void launch_adj2(const DevCatalog& C, const PairParams& P, const double* cot2, c
     GR_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
     int per_sm = 1;                                                                            \
     GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, smem));          \
-    int64_t blocks = (int64_t)std::max(1, per_sm) * 148;                                       \
+    int64_t blocks = (int64_t)std::max(1, per_sm) * sm_count();                                       \
     if (blocks > C.grid.ncell) blocks = std::max<int64_t>(1, C.grid.ncell);                    \
     k<<<(unsigned)blocks, NT, smem, s>>>(C, P, cot2, cot3, gscale, g_lo, g_hi, work);          \
   } while (0)
@@ -264,7 +264,7 @@ void launch_adj2(const DevCatalog& C, const PairParams& P, const double* cot2, c
     return;
   }
   int64_t blocks = (C.grid.ncell + kAdjWarps - 1) / kAdjWarps;
-  if (blocks > 148 * 4) blocks = 148 * 4;
+  if (blocks > (int64_t)4 * sm_count()) blocks = (int64_t)4 * sm_count();
   if (blocks < 1) blocks = 1;
   if (P.f32) {
     GR_CUDA_TRY(cudaFuncSetAttribute(adj2_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -284,7 +284,7 @@ void launch_grad_finish(int n, const int* orig, const unsigned long long* g_lo,
                         const unsigned long long* g_hi, double gscale, double* grad,
                         cudaStream_t s) {
   if (n <= 0) return;
-  const int blocks = (int)std::min<int64_t>(((int64_t)n + 255) / 256, 148 * 8);
+  const int blocks = (int)std::min<int64_t>(((int64_t)n + 255) / 256, (int64_t)8 * sm_count());
   grad_finish_kernel<<<blocks, 256, 0, s>>>(n, orig, g_lo, g_hi, 1.0 / gscale, grad);
   GR_CHECK_LAUNCH();
 }

@@ -103,12 +103,15 @@ void make_pair_params(PairParams& P, double rmin, double rmax, int nbins, int nm
   // FP32 fast path: error bounds for coordinates rounded to float.
   //   coordinate error            <= X u            (u = 2^-24)
   //   separation component error  <= e1 = 2 X u + R u
-  //   |d_f - d|                   <= sqrt(3) e1 + 2.5 u R
-  // doubled for safety.
+  //   |d_f - d|                   <= sqrt(3) e1 + 8 u R
+  // The 8 u R covers the squared separation (three roundings, 1.5 u R on d)
+  // and a square root taken as d2 * rsqrtf(d2) (2 ulp = 4 u, plus u for the
+  // product), so kernels may use either that or the rounded square root.
+  // Doubled for safety.
   const double u = std::ldexp(1.0, -24);
   const double R = rmax * 1.01 + 1e-30;
   const double e1 = 2.0 * X * u + R * u;
-  const double d0 = 2.0 * (std::sqrt(3.0) * e1 + 2.5 * u * R);
+  const double d0 = 2.0 * (std::sqrt(3.0) * e1 + 8.0 * u * R);
   P.d0 = (float)(d0 * (1.0 + 1e-6));
   double hi = rmax + 2.0 * d0;
   hi = hi * hi * (1.0 + 16.0 * u);
@@ -139,12 +142,15 @@ void make_pair_params(PairParams& P, double rmin, double rmax, int nbins, int nm
   double tg = (d0 + u * std::fabs(rmin) + u * R) * P.inv_dr + 4.0 * u * tmax;
   tg = 2.0 * tg + 1e-9 * tmax;
   P.tguard = (float)tg;
-  // line-of-sight cosine: (pi/2)(|ds|/|s| + |dm|/|m|) + arithmetic, doubled
+  // line-of-sight cosine: (pi/2)(|ds|/|s| + |dm|/|m|) + arithmetic, doubled.
+  // The arithmetic term eC = 128 u covers the cosine evaluated with
+  // approximate square roots and division (about 21 u: dot product 3 u,
+  // |m| and d 6.5 u each, product u, __fdividef 4 u) with a margin of six.
   const double pi = 3.14159265358979323846;
   P.eA = (float)(pi * std::sqrt(3.0) * e1);
   P.mB = (float)(8.0 * X * u + 1e-30);
   P.eB = (float)(pi * 2.0 * std::sqrt(3.0) * X * u);
-  P.eC = (float)(64.0 * u);
+  P.eC = (float)(128.0 * u);
   P.f32 = (!force_fp64 && !logbins && std::isfinite(tg) && tg < 0.05 && std::isfinite(X)) ? 1 : 0;
 }
 
@@ -180,8 +186,15 @@ double fix_scale(double pmax) {
 }
 
 double fix_value(unsigned long long lo, unsigned long long hi, double scale) {
-  const long double v = (long double)(long long)hi * 18446744073709551616.0L + (long double)lo;
-  return (double)(v / (long double)scale);
+  // scale is a power of two: one rounding in the conversion, none after it
+  return i128_to_double(lo, hi) / scale;
+}
+
+double fix_split_value(unsigned long long lo, unsigned long long hi, double scale) {
+  // hi * 2^32 + lo as a signed 128-bit integer (exact), then one rounding
+  const __int128 v = ((__int128)(long long)hi << 32) + (__int128)lo;
+  const unsigned __int128 u = (unsigned __int128)v;
+  return i128_to_double((unsigned long long)u, (unsigned long long)(u >> 64)) / scale;
 }
 
 }  // namespace gr
@@ -386,10 +399,12 @@ float ev_ms(cudaEvent_t a, cudaEvent_t b) {
 
 // Index build + pair parameters (shared by every query).
 // speculate: see CellIndex / UpperCSR; the caller checks the flags
-void build_index(gr_ctx* c, bool speculate = false) {
+// sub: cell grid of the index (1: cells at least rmax wide, 2: rmax/2,
+// 0: chosen by density, see CellIndex::build)
+void build_index(gr_ctx* c, bool speculate = false, int sub = 1) {
   cudaStream_t s = c->stream();
   c->index.build(c->xyz.p, c->w.p, c->has_buffer ? c->buffer.p : nullptr, c->n, c->n_data, c->rmax, s,
-                 speculate);
+                 speculate, sub, kDenseCellPoints);
   make_pair_params(c->P, c->rmin, c->rmax, c->nbins, c->nmu, c->logbins, c->index.coord_max,
                    c->precision == 1);
   c->csr_valid = false;
@@ -506,7 +521,7 @@ static int set_catalog_impl(gr_ctx* c, const double* xyz, const double* w, const
   GR_CUDA_TRY(cudaMemcpyAsync(c->uniform_flag.p, init, 24, cudaMemcpyHostToDevice, s));
   unsigned long long* d_wmax = reinterpret_cast<unsigned long long*>(c->uniform_flag.p + 8);
   if (n > 0) {
-    int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 2);
+    int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)2 * sm_count());
     uniform_check_kernel<<<blocks, 256, 0, s>>>(c->w.p, n_data, n, c->uniform_flag.p, d_wmax);
     GR_CHECK_LAUNCH();
   }
@@ -607,8 +622,17 @@ struct ScopedEvents {
 static int pick_pair2_variant(gr_ctx* c, const DevCatalog& C, bool weighted, double fscale,
                               unsigned long long* hcnt, unsigned long long* hfix,
                               unsigned long long* stats, int* work, cudaStream_t s) {
+  // a grid of rmax/2 cells is read by the tile sweep only
+  if (C.grid.sub == 2) return kPairTile2;
   if (c->autotune == 0) return kPairWarpCell;
-  if (c->autotune >= 2) return c->autotune - 2;
+  if (c->autotune >= 2) {
+    int v = c->autotune - 2;
+    if (v == kPairTile2) v = kPairTile;
+    if (v == kPairTile && !c->P.f32) v = kPairWarpCell;
+    return v;
+  }
+  // the tile sweep runs on the FP32 path only
+  const int nvar = c->P.f32 ? kPairTile + 1 : kPairTile;
   const double per_cell = C.grid.ncell > 0 ? (double)C.n / (double)C.grid.ncell : 1.0;
   int dens = 0;
   while (dens < 20 && std::ldexp(1.0, dens + 1) <= per_cell) ++dens;
@@ -619,7 +643,7 @@ static int pick_pair2_variant(gr_ctx* c, const DevCatalog& C, bool weighted, dou
   int cb = 0;
   while (cb < 20 && ((int64_t)4 << (2 * cb)) <= C.grid.ncell) ++cb;
   char key[128];
-  std::snprintf(key, sizeof(key), "pair2v8|%s|%s|dens%d|hist%d|cells%d", c->P.f32 ? "f32" : "f64",
+  std::snprintf(key, sizeof(key), "pair2v9|%s|%s|dens%d|hist%d|cells%d", c->P.f32 ? "f32" : "f64",
                 weighted ? "w" : "u", dens, hb, cb);
   Tuner& T = tuner();
   {
@@ -634,12 +658,12 @@ static int pick_pair2_variant(gr_ctx* c, const DevCatalog& C, bool weighted, dou
   // every variant once untimed (its first launch loads its code), then the
   // fastest of three interleaved rounds
   float t[kPairVariants];
-  for (int v = 0; v < kPairVariants; ++v) {
+  for (int v = 0; v < nvar; ++v) {
     t[v] = 1e30f;
     launch_pair2(C, c->P, weighted, hcnt, hfix, fscale, stats, work, s, v);
   }
   for (int round = 0; round < 3; ++round) {
-    for (int v = 0; v < kPairVariants; ++v) {
+    for (int v = 0; v < nvar; ++v) {
       GR_CUDA_TRY(cudaMemsetAsync(hcnt, 0, sizeof(unsigned long long) * nh, s));
       GR_CUDA_TRY(cudaMemsetAsync(hfix, 0, sizeof(unsigned long long) * 2 * nh, s));
       GR_CUDA_TRY(cudaEventRecord(a, s));
@@ -652,7 +676,7 @@ static int pick_pair2_variant(gr_ctx* c, const DevCatalog& C, bool weighted, dou
     }
   }
   int best = kPairWarpCell;
-  for (int v = 1; v < kPairVariants; ++v)
+  for (int v = 1; v < nvar; ++v)
     if (t[v] < t[best]) best = v;
   std::lock_guard<std::mutex> lock(T.mu);
   T.choice[key] = best;
@@ -672,7 +696,16 @@ int gr_count_2pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
   c->hfix.reserve(2 * nh);
   c->stats.reserve(8);
   GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
-  if (!reuse_graph(c)) build_index(c);
+  if (!reuse_graph(c)) {
+    // dense catalogues on the FP32 path: cells of rmax/2 and the tile sweep
+    int sub = 1;
+    if (c->precision == 0 && !c->logbins) {
+      if (c->autotune == 1) sub = 0;
+      if (c->autotune == 2 + kPairTile2) sub = 2;
+    }
+    build_index(c, false, sub);
+    if (c->index.grid.sub == 2 && !c->P.f32) build_index(c, false, 1);
+  }
   GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
   c->work.reserve(4);
   const int variant = pick_pair2_variant(c, c->index.view(), weighted, fscale, c->hcnt.p,
@@ -946,15 +979,24 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   std::vector<unsigned long long> hc(nh), dc(nd), hf, df;
   std::vector<double> hs(nh, 0.0), ds(nd, 0.0);
   unsigned long long st[8];
-  // block-private 32-bit counters first; exact below 2^32 rooted cliques,
-  // else the launch is repeated with 64-bit global counters
+  // First attempt: unweighted counts in block-private 32-bit counters, and
+  // weighted sums as split limbs added without returned values (fix_red).
+  // Both are exact while every bin receives fewer than 2^32 updates, which
+  // holds when the rooted total is below 2^32 (a rooted clique updates each
+  // N2 / N3 bin and each disconnected-term bin at most once); otherwise the
+  // launch is repeated with 64-bit counters and carried 128-bit sums.
   for (int attempt = 0; attempt < 2; ++attempt) {
     if (attempt > 0) {
       GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nh, s));
       GR_CUDA_TRY(cudaMemsetAsync(c->dcnt.p, 0, sizeof(unsigned long long) * ndv, s));
+      if (weighted) {
+        GR_CUDA_TRY(cudaMemsetAsync(c->hfix.p, 0, sizeof(unsigned long long) * 2 * nh, s));
+        GR_CUDA_TRY(cudaMemsetAsync(c->dfix.p, 0, sizeof(unsigned long long) * 2 * ndv, s));
+      }
       GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
       GR_CUDA_TRY(cudaEventRecord(q0, s));
     }
+    Q.split = (weighted && attempt == 0) ? 1 : 0;
     const bool shared = launch_quad4(c->index.view(), G, Q, weighted, c->hcnt.p, c->hfix.p,
                                      c->dcnt.p, c->dfix.p, nh, ndv, fscale, dscale, attempt == 0,
                                      c->stats.p, c->work.p, s);
@@ -969,15 +1011,16 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
     }
     GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
     GR_CUDA_TRY(cudaStreamSynchronize(s));
-    if (!shared || st[1] < (1ull << 32)) break;
+    if (!(shared || Q.split) || st[1] < (1ull << 32)) break;
   }
   if (st[3] != 0)
     return set_err(c, GR_E_CAPACITY, "4PCF: label offsets within a row exceed the hash key range");
   // discR category = the all-random category before it
   for (int k = 0; k < nbin * 6; ++k) dc[(size_t)ndv + k] = dc[(size_t)ndv - nbin * 6 + k];
   if (weighted) {
-    for (int k = 0; k < nh; ++k) hs[k] = fix_value(hf[k], hf[(size_t)nh + k], fscale);
-    for (int k = 0; k < ndv; ++k) ds[k] = fix_value(df[k], df[(size_t)ndv + k], dscale);
+    auto val = Q.split ? fix_split_value : fix_value;
+    for (int k = 0; k < nh; ++k) hs[k] = val(hf[k], hf[(size_t)nh + k], fscale);
+    for (int k = 0; k < ndv; ++k) ds[k] = val(df[k], df[(size_t)ndv + k], dscale);
     for (int k = 0; k < nbin * 6; ++k) ds[(size_t)ndv + k] = ds[(size_t)ndv - nbin * 6 + k];
   }
   if (!weighted) {
@@ -1081,7 +1124,7 @@ unsigned long long coord_fingerprint(gr_ctx* c) {
   unsigned long long* d = reinterpret_cast<unsigned long long*>(c->uniform_flag.p + 24);
   GR_CUDA_TRY(cudaMemsetAsync(d, 0, sizeof(unsigned long long), s));
   if (c->n > 0) {
-    int blocks = (int)std::min<int64_t>((c->n + 255) / 256, 148 * 8);
+    int blocks = (int)std::min<int64_t>((c->n + 255) / 256, (int64_t)8 * sm_count());
     fingerprint_kernel<<<blocks, 256, 0, s>>>(c->xyz.p, c->n, d);
     GR_CHECK_LAUNCH();
   }
@@ -1578,11 +1621,17 @@ int gr_count_2pcf_batched(gr_ctx* c, double* N2, double* N3, int64_t* counts, do
   GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
   bool replay = c->regions.valid && c->regions.exec;
   if (!c->regions.valid) {
-    c->regions.plan(c->xyz.p, c->n, c->n_data, c->rmax, c->nsplit, s);
     // pair parameters from the catalogue's coordinate bound
     c->index.build(c->xyz.p, c->w.p, nullptr, c->n, c->n_data, c->rmax, s);
     make_pair_params(c->P, c->rmin, c->rmax, c->nbins, c->nmu, c->logbins, c->index.coord_max,
                      c->precision == 1);
+    // dense regions on the FP32 path: cells of rmax/2 and the tile sweep
+    int sub = 1;
+    if (c->P.f32) {
+      if (c->autotune == 1) sub = 0;
+      if (c->autotune == 2 + kPairTile2) sub = 2;
+    }
+    c->regions.plan(c->xyz.p, c->n, c->n_data, c->rmax, c->nsplit, s, sub, kDenseCellPoints);
     c->csr_valid = false;
     c->batch_weighted = !c->uniform;
     c->batch_fscale = fix_scale(c->wmax * c->wmax);

@@ -217,7 +217,9 @@ __global__ void b_narrow_kernel(const int64_t* __restrict__ in, int* __restrict_
     out[i] = (int)in[i];
 }
 
-int nblocks(int64_t n, int threads, int cap = 148 * 8) {
+// blocks for n items, at most `waves` blocks per SM
+int nblocks(int64_t n, int threads, int waves = 8) {
+  const int64_t cap = (int64_t)waves * sm_count();
   int64_t b = (n + threads - 1) / threads;
   return (int)std::max<int64_t>(1, std::min<int64_t>(b, cap));
 }
@@ -236,7 +238,7 @@ RegionLayout::~RegionLayout() { release_graph(); }
 // Host-side geometry (first call): region boxes, halos, member counts,
 // grids and offsets; sizes every buffer.
 void RegionLayout::plan(const double* d_xyz, int64_t n_pts, int64_t n_data_pts, double rmax_,
-                        int nsplit_, cudaStream_t s) {
+                        int nsplit_, cudaStream_t s, int sub_policy, double dense_per_cell) {
   release_graph();
   valid = false;
   n = n_pts;
@@ -254,7 +256,7 @@ void RegionLayout::plan(const double* d_xyz, int64_t n_pts, int64_t n_data_pts, 
     GR_CUDA_TRY(cudaMemcpyAsync(box_raw.p + 6 * (size_t)nreg, init, sizeof(init),
                                 cudaMemcpyHostToDevice, s));
     if (n > 0)
-      b_bbox_kernel<<<nblocks(n, 256, 296), 256, 0, s>>>(d_xyz, (int)n, box_raw.p + 6 * (size_t)nreg);
+      b_bbox_kernel<<<nblocks(n, 256, 2), 256, 0, s>>>(d_xyz, (int)n, box_raw.p + 6 * (size_t)nreg);
     GR_CHECK_LAUNCH();
   }
   unsigned long long hb[6];
@@ -318,9 +320,29 @@ void RegionLayout::plan(const double* d_xyz, int64_t n_pts, int64_t n_data_pts, 
   for (int r = 0; r < nreg; ++r) h_mem_off[r + 1] = h_mem_off[r] + h_count[r];
   n_members = h_mem_off[nreg];
   if (n_members >= ((int64_t)1 << 31)) throw Error{-2, "too many region members"};
-  // grids over each halo box, cells at least rmax wide; cells numbered
-  // region by region, largest region first
-  h_grid.assign(nreg, GridParams{1, 1, 1, 1});
+  // grids over each halo box, cells at least rmax (or rmax/2) wide; cells
+  // numbered region by region, largest region first
+  auto region_grid = [&](int r, double cell, GridGeom& gg) {
+    double lo3[3], hi3[3];
+    for (int d = 0; d < 3; ++d) {
+      lo3[d] = h_halo[6 * r + d];
+      hi3[d] = h_halo[6 * r + 3 + d];
+    }
+    return make_grid_geom(lo3, hi3, cell, 1024, std::max<int64_t>(4 * (int64_t)h_count[r], 64), gg);
+  };
+  grid_sub = sub_policy == 2 ? 2 : 1;
+  if (sub_policy == 0) {
+    int64_t cells1 = 0;
+    for (int r = 0; r < nreg; ++r) {
+      GridGeom gg;
+      if (h_count[r] > 0) cells1 += region_grid(r, rmax, gg);
+    }
+    grid_sub = (dense_per_cell > 0.0 && cells1 > 0 &&
+                (double)n_members / (double)cells1 >= dense_per_cell)
+                   ? 2
+                   : 1;
+  }
+  h_grid.assign(nreg, GridParams{1, 1, 1, 1, grid_sub});
   h_glo.assign(3 * (size_t)nreg, 0.0);
   h_ginv.assign(3 * (size_t)nreg, 1.0);
   std::vector<int> order(nreg);
@@ -334,29 +356,17 @@ void RegionLayout::plan(const double* d_xyz, int64_t n_pts, int64_t n_data_pts, 
     const int r = order[k];
     int nc[3] = {1, 1, 1};
     if (h_count[r] > 0) {
-      for (int d = 0; d < 3; ++d) {
-        const double span = h_halo[6 * r + 3 + d] - h_halo[6 * r + d];
-        double q = std::floor(span / (rmax * 1.000001));
-        if (!(q >= 1)) q = 1;
-        if (q > 1024) q = 1024;
-        nc[d] = (int)q;
-        h_glo[3 * r + d] = h_halo[6 * r + d];
-        h_ginv[3 * r + d] = 1.0 / (span / q);
-      }
       // keep each region's cell table O(its members)
-      int64_t tot = (int64_t)nc[0] * nc[1] * nc[2];
-      while (tot > std::max<int64_t>(4 * (int64_t)h_count[r], 64)) {
-        int d = 0;
-        for (int e = 1; e < 3; ++e)
-          if (nc[e] > nc[d]) d = e;
-        nc[d] = std::max(1, nc[d] / 2);
-        const double span = h_halo[6 * r + 3 + d] - h_halo[6 * r + d];
-        h_ginv[3 * r + d] = 1.0 / (span / nc[d]);
-        tot = (int64_t)nc[0] * nc[1] * nc[2];
+      GridGeom gg;
+      region_grid(r, rmax / grid_sub, gg);
+      for (int d = 0; d < 3; ++d) {
+        nc[d] = gg.nc[d];
+        h_glo[3 * r + d] = gg.lo[d];
+        h_ginv[3 * r + d] = gg.inv_cs[d];
       }
     }
     const int64_t cells = h_count[r] > 0 ? (int64_t)nc[0] * nc[1] * nc[2] : 0;
-    h_grid[r] = GridParams{nc[0], nc[1], nc[2], cells};
+    h_grid[r] = GridParams{nc[0], nc[1], nc[2], cells, grid_sub};
     off_by_region[r] = next;
     cell_region_h.insert(cell_region_h.end(), (size_t)cells, r);
     next += cells;
@@ -424,7 +434,7 @@ void RegionLayout::enqueue_layout(const double* d_xyz, const double* d_w, cudaSt
   if (n_members > 0) {
     b_scatter_kernel<<<nblocks(n_members, 256), 256, 0, s>>>(n_members, m_key.p, m_slot.p,
                                                              cell_start64.p, tmp_perm.p);
-    b_order_kernel<<<nblocks(ncell * 32, 256, 148 * 16), 256, 0, s>>>(ncell, cell_start64.p,
+    b_order_kernel<<<nblocks(ncell * 32, 256, 16), 256, 0, s>>>(ncell, cell_start64.p,
                                                                       tmp_perm.p, m_orig.p, perm.p);
     b_gather_kernel<<<nblocks(n_members, 256), 256, 0, s>>>(n_members, perm.p, m_orig.p, m_flag.p,
                                                             m_key.p, d_xyz, d_w, pos4.p, posd.p,
@@ -445,7 +455,7 @@ DevCatalog RegionLayout::view() const {
   c.cell_start = cell_start.p;
   c.n = (int)n_members;
   c.n_data = (int)n_data;
-  c.grid = GridParams{1, 1, 1, ncell};
+  c.grid = GridParams{1, 1, 1, ncell, grid_sub};
   c.cell_region = cell_region.p;
   c.region_grid = grid.p;
   c.region_cell_off = cell_off.p;

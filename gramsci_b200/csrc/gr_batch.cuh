@@ -35,7 +35,12 @@ struct RegionLayout {
 
   ~RegionLayout();
   void release_graph();
-  void plan(const double* d_xyz, int64_t n, int64_t n_data, double rmax, int nsplit, cudaStream_t s);
+  // grid_sub: region grids of cells at least rmax (1) or rmax/2 (2) wide;
+  // plan's sub_policy 0 picks 2 when the rmax-wide grids would hold at least
+  // dense_per_cell members per cell
+  int grid_sub = 1;
+  void plan(const double* d_xyz, int64_t n, int64_t n_data, double rmax, int nsplit, cudaStream_t s,
+            int sub_policy = 1, double dense_per_cell = 0.0);
   void enqueue_layout(const double* d_xyz, const double* d_w, cudaStream_t s);
   DevCatalog view() const;
 };

@@ -259,7 +259,7 @@ __global__ void csr_compact_kernel(int64_t n, const int* __restrict__ deg_up,
 
 int graph_blocks(int64_t ncell) {
   int64_t b = (ncell + kGraphWarps - 1) / kGraphWarps;
-  int64_t cap = 148 * 8;
+  const int64_t cap = (int64_t)8 * sm_count();
   if (b > cap) b = cap;
   if (b < 1) b = 1;
   return (int)b;
@@ -283,7 +283,7 @@ void UpperCSR::build(const DevCatalog& C, const PairParams& P, cudaStream_t s, b
   cbound.reserve(ncell + 1);
   cbase.reserve(ncell + 2);
   if (ncell > 0) {
-    const int bb = (int)std::min<int64_t>((ncell + 255) / 256, 148 * 8);
+    const int bb = (int)std::min<int64_t>((ncell + 255) / 256, (int64_t)8 * sm_count());
     cell_bound_kernel<<<bb, 256, 0, s>>>(C, cbound.p);
     GR_CHECK_LAUNCH();
     scan_i64(cbound.p, cbase.p, ncell, s, scan_tmp);
@@ -354,7 +354,7 @@ void UpperCSR::compact(cudaStream_t s) {
   rec.reserve(n_edges + 1);
   if (n > 0 && n_edges > 0) {
     const int64_t groups = (n + 31) / 32;
-    const int blocks = (int)std::min<int64_t>((groups + 7) / 8, 148 * 16);
+    const int blocks = (int)std::min<int64_t>((groups + 7) / 8, (int64_t)16 * sm_count());
     csr_compact_kernel<<<blocks, 256, 0, s>>>(n, deg_up.p, rstart.p, row_ptr.p, scratch.p, rec.p);
     GR_CHECK_LAUNCH();
   }

@@ -5,6 +5,7 @@
 // float4 (FP32 fast path) and double4 (FP64 guard band, weight) arrays.
 #include "gr_index.cuh"
 
+#include <atomic>
 #include <cstring>
 
 namespace gr {
@@ -87,12 +88,6 @@ __global__ void init_bbox_kernel(unsigned long long* out) {
   if (t < 3) out[t] = ~0ull;
   if (t >= 3 && t < 7) out[t] = 0ull;
 }
-
-struct GridGeom {
-  double lo[3];
-  double inv_cs[3];
-  int nc[3];
-};
 
 __device__ __forceinline__ int cell_coord(double v, double lo, double inv_cs, int nc) {
   int c = (int)floor((v - lo) * inv_cs);
@@ -177,7 +172,9 @@ inline double key_to_dbl(unsigned long long k) {
   return v;
 }
 
-int blocks_for(int64_t n, int threads, int cap = 148 * 16) {
+// blocks for n items, at most `waves` blocks per SM
+int blocks_for(int64_t n, int threads, int waves = 16) {
+  const int64_t cap = (int64_t)waves * sm_count();
   int64_t b = (n + threads - 1) / threads;
   if (b < 1) b = 1;
   if (b > cap) b = cap;
@@ -187,7 +184,10 @@ int blocks_for(int64_t n, int threads, int cap = 148 * 16) {
 }  // namespace
 
 void CellIndex::build(const double* d_xyz, const double* d_w, const int* d_buffer, int64_t n_pts,
-                      int64_t n_data_pts, double rmax, cudaStream_t s, bool speculate) {
+                      int64_t n_data_pts, double rmax, cudaStream_t s, bool speculate, int sub,
+                      double dense_per_cell) {
+  const bool auto_sub = sub == 0;
+  if (sub != 2) sub = 1;
   n = n_pts;
   n_data = n_data_pts;
   launches = 0;
@@ -196,12 +196,13 @@ void CellIndex::build(const double* d_xyz, const double* d_w, const int* d_buffe
   init_bbox_kernel<<<1, 32, 0, s>>>(bbox_raw.p);
   launches++;
   if (n > 0) {
-    bbox_kernel<<<blocks_for(n, 256, 296), 256, 0, s>>>(d_xyz, n, bbox_raw.p);
+    bbox_kernel<<<blocks_for(n, 256, 2), 256, 0, s>>>(d_xyz, n, bbox_raw.p);
     launches++;
   }
   GR_CHECK_LAUNCH();
   unsigned long long h[7];
-  speculated = speculate && have_prev && prev_n == n && prev_rmax == rmax;
+  speculated = speculate && !auto_sub && have_prev && prev_n == n && prev_rmax == rmax &&
+               prev_sub == sub;
   if (speculated) {
     std::memcpy(h, prev_raw, sizeof(h));
     bbox_check_kernel<<<1, 32, 0, s>>>(bbox_raw.p, bbox_prev.p);
@@ -213,6 +214,7 @@ void CellIndex::build(const double* d_xyz, const double* d_w, const int* d_buffe
     std::memcpy(prev_raw, h, sizeof(h));
     prev_n = n;
     prev_rmax = rmax;
+    prev_sub = sub;
     have_prev = true;
     GR_CUDA_TRY(cudaMemcpyAsync(bbox_prev.p, prev_raw, sizeof(prev_raw), cudaMemcpyHostToDevice, s));
     GR_CUDA_TRY(cudaMemsetAsync(bbox_prev.p + 7, 0, sizeof(unsigned long long), s));
@@ -226,39 +228,20 @@ void CellIndex::build(const double* d_xyz, const double* d_w, const int* d_buffe
   for (int d = 0; d < 3; ++d)
     if (!std::isfinite(lo[d]) || !std::isfinite(hi[d]))
       throw Error{-1, "catalogue has non-finite coordinates"};
-  // Cells at least rmax (with a relative margin) wide, so that every pair
-  // closer than rmax lies in the same or adjacent cells despite rounding in
-  // the cell-coordinate computation.
-  double cell_min = rmax * 1.000001;
-  if (!(cell_min > 0)) cell_min = 1e300;
+  // cells at least rmax (sub 2: rmax/2) wide; the cell table stays O(N)
   GridGeom g;
-  int64_t total = 1;
-  for (int d = 0; d < 3; ++d) {
-    double span = hi[d] - lo[d];
-    double k = std::floor(span / cell_min);
-    if (!(k >= 1)) k = 1;
-    if (k > 2048) k = 2048;
-    g.nc[d] = (int)k;
-    g.lo[d] = lo[d];
-    double cs = span > 0 ? span / k : 1.0;
-    g.inv_cs[d] = 1.0 / cs;
-    total *= (int64_t)k;
+  {
+    const int64_t cells1 = make_grid_geom(lo, hi, rmax, 2048, std::max<int64_t>(4 * n, 4096), g);
+    per_cell_rmax = cells1 > 0 ? (double)n / (double)cells1 : 0.0;
+    if (auto_sub) sub = (dense_per_cell > 0.0 && per_cell_rmax >= dense_per_cell) ? 2 : 1;
   }
-  // Keep the cell table O(N): merge cells along the longest axes if needed.
-  int64_t cap = std::max<int64_t>(4 * n, 4096);
-  while (total > cap) {
-    int d = 0;
-    for (int k = 1; k < 3; ++k)
-      if (g.nc[k] > g.nc[d]) d = k;
-    g.nc[d] = std::max(1, g.nc[d] / 2);
-    double span = hi[d] - lo[d];
-    g.inv_cs[d] = 1.0 / (span > 0 ? span / g.nc[d] : 1.0);
-    total = (int64_t)g.nc[0] * g.nc[1] * g.nc[2];
-  }
+  const int64_t total =
+      make_grid_geom(lo, hi, rmax / sub, 2048, std::max<int64_t>(4 * n, 4096), g);
   grid.nx = g.nc[0];
   grid.ny = g.nc[1];
   grid.nz = g.nc[2];
   grid.ncell = total;
+  grid.sub = sub;
 
   cell_count.reserve(total + 1);
   key_orig.reserve(n);
@@ -296,6 +279,49 @@ void CellIndex::build(const double* d_xyz, const double* d_w, const int* d_buffe
   narrow_kernel_launch(cell_start64.p, cell_start.p, total + 1, s);
   launches++;
   GR_CHECK_LAUNCH();
+}
+
+int sm_count() {
+  constexpr int kDev = 64;
+  static std::atomic<int> cache[kDev];
+  int dev = 0;
+  GR_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < kDev) {
+    const int v = cache[dev].load(std::memory_order_relaxed);
+    if (v > 0) return v;
+  }
+  int v = 0;
+  GR_CUDA_TRY(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev));
+  if (v < 1) v = 1;
+  if (dev >= 0 && dev < kDev) cache[dev].store(v, std::memory_order_relaxed);
+  return v;
+}
+
+int64_t make_grid_geom(const double lo[3], const double hi[3], double rmax, int max_per_axis,
+                       int64_t max_cells, GridGeom& g) {
+  double cell_min = rmax * 1.000001;
+  if (!(cell_min > 0)) cell_min = 1e300;
+  int64_t total = 1;
+  for (int d = 0; d < 3; ++d) {
+    const double span = hi[d] - lo[d];
+    double k = std::floor(span / cell_min);
+    if (!(k >= 1)) k = 1;
+    if (k > max_per_axis) k = max_per_axis;
+    g.nc[d] = (int)k;
+    g.lo[d] = lo[d];
+    g.inv_cs[d] = 1.0 / (span > 0 ? span / k : 1.0);
+    total *= (int64_t)k;
+  }
+  while (total > max_cells && total > 1) {
+    int d = 0;
+    for (int k = 1; k < 3; ++k)
+      if (g.nc[k] > g.nc[d]) d = k;
+    g.nc[d] = std::max(1, g.nc[d] / 2);
+    const double span = hi[d] - lo[d];
+    g.inv_cs[d] = 1.0 / (span > 0 ? span / g.nc[d] : 1.0);
+    total = (int64_t)g.nc[0] * g.nc[1] * g.nc[2];
+  }
+  return total;
 }
 
 namespace {
@@ -462,7 +488,7 @@ void zero_async(const ZeroList& z, cudaStream_t s) {
   const size_t threads = 256;
   size_t blocks = (total / 16 + threads - 1) / threads;
   if (blocks < 1) blocks = 1;
-  if (blocks > 148 * 8) blocks = 148 * 8;
+  if (blocks > (size_t)8 * sm_count()) blocks = (size_t)8 * sm_count();
   zero_many_kernel<<<(unsigned)blocks, (unsigned)threads, 0, s>>>(z);
   GR_CHECK_LAUNCH();
 }

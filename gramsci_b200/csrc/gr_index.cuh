@@ -26,6 +26,7 @@ struct CellIndex {
   bool have_prev = false, speculated = false;
   int64_t prev_n = -1;
   double prev_rmax = 0.0;
+  int prev_sub = 0;
   unsigned long long prev_raw[7] = {0, 0, 0, 0, 0, 0, 0};
   DevBuf<unsigned long long> bbox_prev;  // previous raw bounding box [0..6], mismatch flag [7]
   DevBuf<int> cell_count, key_orig, slot, tmp_perm, perm, cell_start, orig, cell_key;
@@ -35,8 +36,13 @@ struct CellIndex {
   DevBuf<double> w;
   DevBuf<uint8_t> flags;
 
+  // sub = 1: cells at least rmax wide; sub = 2: at least rmax/2 wide (for
+  // the tile pair sweep); sub = 0: 2 when an rmax-wide grid would hold at
+  // least dense_per_cell points per cell, else 1.
   void build(const double* d_xyz, const double* d_w, const int* d_buffer, int64_t n, int64_t n_data,
-             double rmax, cudaStream_t s, bool speculate = false);
+             double rmax, cudaStream_t s, bool speculate = false, int sub = 1,
+             double dense_per_cell = 0.0);
+  double per_cell_rmax = 0.0;  // points per cell of an rmax-wide grid (last build)
   const unsigned long long* mismatch_flag() const { return bbox_prev.p + 7; }
   DevCatalog view() const;
 };

@@ -233,7 +233,32 @@ __device__ __forceinline__ int edge_rbin(const double4* __restrict__ posd, const
 struct GridParams {
   int nx, ny, nz;
   int64_t ncell;
+  int sub;  // 0 or 1: cells at least rmax wide (27-cell neighbourhoods);
+            // 2: cells at least rmax/2 wide (125-cell neighbourhoods, read
+            // only by the tile pair sweep)
 };
+
+// Number of SMs of the current device (cudaDevAttrMultiProcessorCount,
+// queried once per device ordinal), for grids sized in whole waves.
+int sm_count();
+
+// Host-side geometry of a uniform cell grid over the box [lo, hi]: origin,
+// inverse cell size and cells per axis.
+struct GridGeom {
+  double lo[3];
+  double inv_cs[3];
+  int nc[3];
+};
+
+// Cells at least rmax wide (with a relative margin of 1e-6, so that every
+// pair closer than rmax lies in the same or adjacent cells despite rounding
+// in the cell-coordinate computation), at most max_per_axis per axis, then
+// merged (halving the longest axis) until the grid has at most max_cells
+// cells.  Every pair sweep relies on the cells being at least rmax wide, so
+// all grids over a catalogue come from this one function.  Returns the
+// number of cells.
+int64_t make_grid_geom(const double lo[3], const double hi[3], double rmax, int max_per_axis,
+                       int64_t max_cells, GridGeom& g);
 
 // Forward (half-stencil) candidate ranges of a root at internal label p in
 // cell `key`: labels q > p in the root's own cell and the 13 neighbouring
@@ -281,6 +306,45 @@ __device__ __forceinline__ void forward_ranges(int p, int key, const GridParams&
     R.beg[3 + dy] = b;
     R.end[3 + dy] = e > b ? e : b;
   }
+}
+
+// Forward candidate ranges on a grid of cells at least rmax/2 wide (sub 2):
+// labels from `first` on in the root's own cell and every cell after it in
+// key order within two cells on each axis, as 13 contiguous label ranges in
+// increasing order: the root's x-row up to two cells on (slot 0), the two
+// following rows of its z plane (slots 1-2), and the five rows of each of
+// the next two z planes (slots 3-12).  Lane k of the calling warp (k < 13)
+// returns slot k's [beg, end).
+__device__ __forceinline__ void forward_range2_slot(int k, int first, int key, const GridParams& g,
+                                                    const int* __restrict__ cell_start, int& beg,
+                                                    int& end) {
+  const int cx = key % g.nx;
+  const int cy = (key / g.nx) % g.ny;
+  const int cz = key / (g.nx * g.ny);
+  const int x0 = cx > 1 ? cx - 2 : 0;
+  const int x1 = cx + 2 < g.nx ? cx + 2 : g.nx - 1;
+  int b = 0, e = 0;
+  if (k == 0) {
+    b = first;
+    e = cell_start[key - cx + x1 + 1];
+  } else if (k < 3) {
+    const int y = cy + k;
+    if (y < g.ny) {
+      const int kb = (cz * g.ny + y) * g.nx;
+      b = cell_start[kb + x0];
+      e = cell_start[kb + x1 + 1];
+    }
+  } else if (k < 13) {
+    const int z = cz + 1 + (k - 3) / 5;
+    const int y = cy - 2 + (k - 3) % 5;
+    if (z < g.nz && y >= 0 && y < g.ny) {
+      const int kb = (z * g.ny + y) * g.nx;
+      b = cell_start[kb + x0];
+      e = cell_start[kb + x1 + 1];
+    }
+  }
+  beg = b;
+  end = e > b ? e : b;
 }
 
 // All 27 neighbouring cells (own cell included) as at most 9 contiguous
@@ -442,6 +506,20 @@ __device__ __forceinline__ void fix_add_int(unsigned long long* lo, unsigned lon
   if (d) atomicAdd(hi, d);
 }
 
+// Fixed-point sums whose updates return nothing: V = round(x * scale)
+// (|V| < 2^62) is split into its low 32 bits (unsigned) and its high part
+// V >> 32 (signed), and each is added with a reduction, so the issuing warp
+// never waits for an atomic's old value (the carry of fix_add needs it).
+// The pair (lo, hi) then holds sum(low limbs) and sum(high limbs); its value
+// is hi * 2^32 + lo (fix_split_value).  Exact while a sum receives fewer
+// than 2^32 updates (the low-limb sum stays below 2^64).
+__device__ __forceinline__ void fix_red(unsigned long long* lo, unsigned long long* hi, double x,
+                                        double scale) {
+  const long long v = __double2ll_rn(x * scale);
+  atomicAdd(lo, (unsigned long long)(v & 0xffffffffll));
+  atomicAdd(hi, (unsigned long long)(v >> 32));
+}
+
 // merge a partial (lo, hi) pair into another with atomics
 __device__ __forceinline__ void fix_merge(unsigned long long* lo, unsigned long long* hi,
                                           unsigned long long plo, unsigned long long phi) {
@@ -476,22 +554,55 @@ __device__ __forceinline__ Fix128 fix_warp_sum(Fix128 a) {
   return a;
 }
 
-// Device: value of a signed 128-bit (lo, hi) pair divided by scale.
-__device__ __forceinline__ double fix_to_double(unsigned long long lo, unsigned long long hi,
-                                                double inv_scale) {
+// Value of the signed 128-bit integer (hi, lo) as a double, rounded once
+// (to nearest, ties to even), on the host and on the device alike: the
+// magnitude's top 64 bits are converted with the bits below them folded
+// into a sticky bit, then scaled by a power of two (exact).
+__host__ __device__ __forceinline__ double i128_to_double(unsigned long long lo,
+                                                          unsigned long long hi) {
   const bool neg = (long long)hi < 0;
   if (neg) {
     lo = ~lo + 1ull;
     hi = ~hi + (lo == 0ull ? 1ull : 0ull);
   }
-  const double mag = (double)hi * 18446744073709551616.0 + (double)lo;
-  return (neg ? -mag : mag) * inv_scale;
+  double mag;
+  if (hi == 0ull) {
+#ifdef __CUDA_ARCH__
+    mag = __ull2double_rn(lo);
+#else
+    mag = (double)lo;
+#endif
+  } else {
+#ifdef __CUDA_ARCH__
+    const int sh = 64 - __clzll((long long)hi);  // significant bits of hi, 1..64
+#else
+    const int sh = 64 - __builtin_clzll(hi);
+#endif
+    unsigned long long top = sh == 64 ? hi : ((hi << (64 - sh)) | (lo >> sh));
+    const unsigned long long rest = sh == 64 ? lo : (lo << (64 - sh));
+    top |= rest != 0ull ? 1ull : 0ull;
+#ifdef __CUDA_ARCH__
+    mag = ldexp(__ull2double_rn(top), sh);
+#else
+    mag = std::ldexp((double)top, sh);
+#endif
+  }
+  return neg ? -mag : mag;
+}
+
+// Device: value of a signed 128-bit (lo, hi) pair divided by scale (a power
+// of two, so the division adds no rounding).
+__device__ __forceinline__ double fix_to_double(unsigned long long lo, unsigned long long hi,
+                                                double inv_scale) {
+  return i128_to_double(lo, hi) * inv_scale;
 }
 
 // Host: scale 2^e with max_abs_product * 2^e < 2^62.
 double fix_scale(double max_abs_product);
 // Host: value of a (lo, hi) pair.
 double fix_value(unsigned long long lo, unsigned long long hi, double scale);
+// Host: value of a split-limb pair written by fix_red.
+double fix_split_value(unsigned long long lo, unsigned long long hi, double scale);
 
 // -------------------------------------------------------------- host launch --
 // Zero up to 8 device buffers in one launch (instead of one memset each).

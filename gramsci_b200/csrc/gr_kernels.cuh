@@ -21,6 +21,9 @@ constexpr size_t kMaxHistSmem = 120 * 1024;
 // kPairWarpQueue / kPairDenseQ128/256: the same sweeps with a
 // membership-only test per candidate and the binning of the edges queued and
 // run with full warps.
+// kPairTile: the tile sweep (gr_tile.cu) on cells at least rmax wide;
+// kPairTile2: the same on cells at least rmax/2 wide (the only variant that
+// reads such grids).  The tile sweeps need the FP32 path (PairParams::f32).
 enum {
   kPairWarpCell = 0,
   kPairDense128 = 1,
@@ -28,9 +31,26 @@ enum {
   kPairWarpQueue = 3,
   kPairDenseQ128 = 4,
   kPairDenseQ256 = 5,
-  kPairVariants = 6
+  kPairTile = 6,
+  kPairTile2 = 7,
+  kPairVariants = 8
 };
+// Points per rmax-wide cell from which the 2PCF sweeps use cells of rmax/2
+// and the tile sweep (FP32 path only).
+constexpr double kDenseCellPoints = 64.0;
 size_t pair2_smem_bytes(const PairParams& P, bool weighted);
+
+// Tile sweep for dense cells (gr_tile.cu): warp per cell, lanes over 32
+// roots, candidates staged 32 at a time per warp and tested two per packed
+// FP32x2 instruction, hits binned from a per-warp queue; reads grids with
+// cells at least rmax wide (sub 1) or rmax/2 wide (sub 2).  Same inputs,
+// outputs and results as launch_pair2.  Histograms private to each warp in
+// shared memory when they need at most kMaxTileHistSmem bytes.
+constexpr size_t kMaxTileHistSmem = 160 * 1024;
+size_t pair2_tile_smem_bytes(const PairParams& P, bool weighted);
+void launch_pair2_tile(const DevCatalog& C, const PairParams& P, bool weighted,
+                       unsigned long long* g_cnt, unsigned long long* g_fix, double fscale,
+                       unsigned long long* stats, int* work, cudaStream_t s);
 void launch_pair2(const DevCatalog& C, const PairParams& P, bool weighted,
                   unsigned long long* g_cnt, unsigned long long* g_fix, double fscale,
                   unsigned long long* stats, int* work, cudaStream_t s, int variant = kPairWarpCell);
@@ -83,6 +103,8 @@ struct QuadParams {
   RankTables rank;  // 4-tuple ranks
   PairParams P;     // edge predicate and binning of the graph
   int geo;          // 1: edges among R+(p) by the geometric pair test (cap <= 256)
+  int split;        // weighted sums as split limbs without returned values (fix_red);
+                    // exact while every bin receives fewer than 2^32 updates
 };
 
 // -tetra histograms (tetra = 1): g_cnt nbins*5, d_cnt nbins*30 (6 terms x 5

@@ -22,14 +22,21 @@
 // work overlaps on the GPU (two host threads, or two streams in flight at
 // once) race on the scratch and must be serialised by the caller.
 //
+// Each call waits once on its stream: the catalogue's bounding box is read
+// back to size the cell grid before the sweep is queued.
+//
 // Host code cannot use the array's name as a device address, so the first
-// call on each device, with that device current, looks the address up with
-// cudaGetSymbolAddress and caches it; that first call should come before any
-// stream capture.
+// call on each device (and CUDA context), with that device current, looks
+// the address up with cudaGetSymbolAddress and caches it; that first call
+// should come before any stream capture.  The cache is keyed by the current
+// context, so a context created later on the same device (a non-primary
+// context, or the primary context again after cudaDeviceReset) gets its own
+// lookup.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "../../include/gramsci_cuda.h"
 #include "gr_kernels.cuh"
@@ -66,8 +73,14 @@ constexpr size_t kNoAllocBytes = al256(kOffWork + 16);
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
+// cached device addresses of the scratch array, per (device, context)
+struct SymbolEntry {
+  int device;
+  void* context;
+  unsigned char* addr;
+};
 std::mutex g_symbol_mutex;
-unsigned char* g_symbol_addr[64] = {nullptr};
+std::vector<SymbolEntry> g_symbol_cache;
 
 // misc words: [0..2] min keys, [3..5] max keys, [6] max |coord| key,
 // [7] max |w| bits
@@ -109,12 +122,7 @@ __global__ void na_bounds_kernel(const double* __restrict__ xyz, const double* _
   atomicMax(&misc[7], wm);
 }
 
-struct NaGrid {
-  double lo[3], inv_cs[3];
-  int nc[3];
-};
-
-__global__ void na_assign_kernel(const double* __restrict__ xyz, int n, NaGrid g,
+__global__ void na_assign_kernel(const double* __restrict__ xyz, int n, GridGeom g,
                                  int* __restrict__ key, int* __restrict__ slot,
                                  int* __restrict__ count) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -213,15 +221,8 @@ __global__ void na_finish_kernel(const unsigned long long* __restrict__ hcnt,
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       const int j = k + nbm * c;
-      // signed 128-bit (hi, lo) -> magnitude and sign, then / scale
-      unsigned long long lo = hfix[j], hi = hfix[nh + j];
-      const bool neg = (long long)hi < 0;
-      if (neg) {
-        lo = ~lo + 1ull;
-        hi = ~hi + (lo == 0ull ? 1ull : 0ull);
-      }
-      const double mag = (double)hi * 18446744073709551616.0 + (double)lo;
-      s[c] = (neg ? -mag : mag) * inv_scale;
+      // one rounding, as gr_count_2pcf converts its sums on the host
+      s[c] = fix_to_double(hfix[j], hfix[nh + j], inv_scale);
       if (counts) counts[j] = (int64_t)hcnt[j];
       if (catsum) catsum[j] = s[c];
     }
@@ -230,22 +231,43 @@ __global__ void na_finish_kernel(const unsigned long long* __restrict__ hcnt,
   }
 }
 
+// The CUDA context current on this thread (cuCtxGetCurrent, reached through
+// the runtime's driver entry point so that the library does not link
+// against the driver library); nullptr when it cannot be queried.
+void* current_context() {
+  typedef int (*CtxGetCurrent)(void**);
+  static CtxGetCurrent fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<CtxGetCurrent>(f);
+  }();
+  void* ctx = nullptr;
+  if (fn && fn(&ctx) != 0) ctx = nullptr;
+  return ctx;
+}
+
+// Device address of the scratch array in the current device and context:
+// looked up with cudaGetSymbolAddress on the first call there, then cached.
 unsigned char* scratch_address(int device, int* status) {
+  void* ctx = current_context();
   std::lock_guard<std::mutex> lock(g_symbol_mutex);
-  if (device < 0 || device >= 64) {
-    *status = GR_E_ARG;
+  for (const SymbolEntry& e : g_symbol_cache)
+    if (e.device == device && e.context == ctx) {
+      *status = GR_OK;
+      return e.addr;
+    }
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+    *status = GR_E_CUDA;
     return nullptr;
   }
-  if (!g_symbol_addr[device]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
-      *status = GR_E_CUDA;
-      return nullptr;
-    }
-    g_symbol_addr[device] = static_cast<unsigned char*>(p);
-  }
+  g_symbol_cache.push_back(SymbolEntry{device, ctx, static_cast<unsigned char*>(p)});
   *status = GR_OK;
-  return g_symbol_addr[device];
+  return static_cast<unsigned char*>(p);
 }
 
 inline double key_value(unsigned long long k) {
@@ -300,7 +322,8 @@ extern "C" int gr_count_2pcf_noalloc(const double* d_xyz, const double* d_w, int
 
     // bounds of the catalogue and of |w|
     na_init_kernel<<<1, 32, 0, s>>>(misc);
-    if (ni > 0) na_bounds_kernel<<<std::min(148, (ni + 255) / 256), 256, 0, s>>>(d_xyz, d_w, ni, misc);
+    const int nsm = sm_count();
+    if (ni > 0) na_bounds_kernel<<<std::min(nsm, (ni + 255) / 256), 256, 0, s>>>(d_xyz, d_w, ni, misc);
     GR_CHECK_LAUNCH();
     unsigned long long h[8];
     GR_CUDA_TRY(cudaMemcpyAsync(h, misc, sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -317,38 +340,20 @@ extern "C" int gr_count_2pcf_noalloc(const double* d_xyz, const double* d_w, int
       std::memcpy(&wmax, &h[7], 8);
       if (!std::isfinite(wmax)) return GR_E_ARG;
     }
-    // grid: cells at least rmax wide, merged until at most kMaxCells
-    NaGrid g;
-    int64_t total = 1;
-    for (int d = 0; d < 3; ++d) {
-      const double span = hi[d] - lo[d];
-      double k = std::floor(span / (rmax * 1.000001));
-      if (!(k >= 1)) k = 1;
-      if (k > 2048) k = 2048;
-      g.nc[d] = (int)k;
-      g.lo[d] = lo[d];
-      g.inv_cs[d] = 1.0 / (span > 0 ? span / k : 1.0);
-      total *= (int64_t)k;
-    }
-    while (total > kMaxCells) {
-      int d = 0;
-      for (int k = 1; k < 3; ++k)
-        if (g.nc[k] > g.nc[d]) d = k;
-      g.nc[d] = std::max(1, g.nc[d] / 2);
-      const double span = hi[d] - lo[d];
-      g.inv_cs[d] = 1.0 / (span > 0 ? span / g.nc[d] : 1.0);
-      total = (int64_t)g.nc[0] * g.nc[1] * g.nc[2];
-    }
+    // grid: cells at least rmax wide, at most kMaxCells of them (the same
+    // geometry as the allocating path's index, with this array's cap)
+    GridGeom g;
+    const int64_t total = make_grid_geom(lo, hi, rmax, 2048, kMaxCells, g);
     const int ncell = (int)total;
 
     // cell index in the scratch array
     GR_CUDA_TRY(cudaMemsetAsync(count, 0, sizeof(int) * (ncell + 1), s));
-    const int blocks = std::max(1, std::min(148 * 4, (ni + 255) / 256));
+    const int blocks = std::max(1, std::min(4 * nsm, (ni + 255) / 256));
     if (ni > 0) na_assign_kernel<<<blocks, 256, 0, s>>>(d_xyz, ni, g, key, slot, count);
     na_scan_kernel<<<1, 1024, 0, s>>>(count, ncell, start64, start);
     if (ni > 0) {
       na_scatter_kernel<<<blocks, 256, 0, s>>>(ni, key, slot, start64, tmp_perm);
-      na_order_kernel<<<std::max(1, std::min(148 * 4, (ncell * 32 + 255) / 256)), 256, 0, s>>>(
+      na_order_kernel<<<std::max(1, std::min(4 * nsm, (ncell * 32 + 255) / 256)), 256, 0, s>>>(
           ncell, start64, tmp_perm, perm);
       na_gather_kernel<<<blocks, 256, 0, s>>>(ni, (int)n_data, perm, d_xyz, d_w, key, pos4, posd,
                                               wl, orig, flags, cell_key);
@@ -369,6 +374,7 @@ extern "C" int gr_count_2pcf_noalloc(const double* d_xyz, const double* d_w, int
     C.grid.ny = g.nc[1];
     C.grid.nz = g.nc[2];
     C.grid.ncell = total;
+    C.grid.sub = 1;
     C.cell_region = nullptr;
     C.region_grid = nullptr;
     C.region_cell_off = nullptr;
@@ -381,7 +387,7 @@ extern "C" int gr_count_2pcf_noalloc(const double* d_xyz, const double* d_w, int
     GR_CUDA_TRY(cudaMemsetAsync(hfix, 0, sizeof(unsigned long long) * 2 * nh, s));
     GR_CUDA_TRY(cudaMemsetAsync(stats, 0, sizeof(unsigned long long) * 8, s));
     launch_pair2(C, P, true, hcnt, hfix, fscale, stats, work, s);
-    na_finish_kernel<<<std::max(1, std::min(148, (nbm + 255) / 256)), 256, 0, s>>>(
+    na_finish_kernel<<<std::max(1, std::min(nsm, (nbm + 255) / 256)), 256, 0, s>>>(
         hcnt, hfix, nbm, 1.0 / fscale, d_counts, d_catsum, d_N2, d_N3);
     GR_CHECK_LAUNCH();
   } catch (const gr::Error& e) {

@@ -641,6 +641,11 @@ void launch_pair2(const DevCatalog& C, const PairParams& P, bool weighted,
                   unsigned long long* g_cnt, unsigned long long* g_fix, double fscale,
                   unsigned long long* stats, int* work, cudaStream_t s, int variant) {
   if (C.n <= 0) return;
+  if (variant == kPairTile || variant == kPairTile2 || C.grid.sub == 2) {
+    if (!P.f32) throw Error{-1, "the tile pair sweep needs the FP32 path"};
+    launch_pair2_tile(C, P, weighted, g_cnt, g_fix, fscale, stats, work, s);
+    return;
+  }
   size_t smem = pair2_smem_bytes(P, weighted);
   const bool shist = smem <= kMaxHistSmem;
   if (!shist) smem = 0;
@@ -656,7 +661,7 @@ void launch_pair2(const DevCatalog& C, const PairParams& P, bool weighted,
     GR_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
                                      (int)smem));                                             \
     GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, smem));         \
-    int64_t blocks = (int64_t)std::max(1, per_sm) * 148;                                      \
+    int64_t blocks = (int64_t)std::max(1, per_sm) * sm_count();                                      \
     if (blocks > C.grid.ncell) blocks = std::max<int64_t>(1, C.grid.ncell);                   \
     k<<<(unsigned)blocks, NT, smem, s>>>(C, P, g_cnt, g_fix, fscale, stats, work);            \
   } while (0)
@@ -680,7 +685,7 @@ void launch_pair2(const DevCatalog& C, const PairParams& P, bool weighted,
     return;
   }
   int64_t blocks = (C.grid.ncell + kPairWarps - 1) / kPairWarps;
-  if (blocks > 148 * 4) blocks = 148 * 4;
+  if (blocks > (int64_t)4 * sm_count()) blocks = (int64_t)4 * sm_count();
   if (blocks < 1) blocks = 1;
 #define GR_PAIR_LAUNCH(F, W, S)                                                          \
   do {                                                                                   \

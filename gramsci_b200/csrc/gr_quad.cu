@@ -86,11 +86,21 @@ struct QuadCtx {
   unsigned int *scnt, *sdcnt;  // block-private 32-bit counts in shared memory, or null
   unsigned long long *fix, *dfix;  // fixed-point (lo, hi) sums, hi at +5*nbin / +dhi
   int dhi;                          // disc entries on the device (hi offset in dfix)
+  int split;                        // 1: sums as split limbs (fix_red), 0: carries (fix_add)
   double fscale;  // scale of the 4-point products
   double dscale;  // scale of the pair products of the disconnected terms
   // adjoint: cotangents of N2, N3 (nbin each), discN, discR (6 nbin each)
   const double *c2, *c3, *cN, *cR;
 };
+
+// one weighted update of a global fixed-point sum
+__device__ __forceinline__ void qfix(const QuadCtx& X, unsigned long long* lo, unsigned long long* hi,
+                                     double x, double scale) {
+  if (X.split)
+    fix_red(lo, hi, x, scale);
+  else
+    fix_add(lo, hi, x, scale);
+}
 
 template <bool SHC>
 __device__ __forceinline__ void qcount(const QuadCtx& X, int k) {
@@ -162,7 +172,7 @@ __device__ __forceinline__ int tetra_root(const QuadCtx& X, const QVerts& V, int
   const int nb = X.nbins;
   qcount<SHC>(X, (b - 1) + nb * nr);
   if (WEIGHTED)
-    fix_add(&X.fix[(b - 1) + nb * nr], &X.fix[(b - 1) + nb * (nr + 5)],
+    qfix(X, &X.fix[(b - 1) + nb * nr], &X.fix[(b - 1) + nb * (nr + 5)],
             ((V.w[R] * qsel(u0, V)) * qsel(u1, V)) * qsel(u2, V), X.fscale);
 #pragma unroll
   for (int tt = 0; tt < 6; ++tt) {
@@ -173,7 +183,7 @@ __device__ __forceinline__ int tetra_root(const QuadCtx& X, const QVerts& V, int
     const double qv = WEIGHTED ? (qsel(ua, V) * qsel(ub, V)) * qsel(uc, V) : 0.0;
     // discR (all three random) equals category 3 and is copied on the host
     qdcount<SHC>(X, kt + nb * 6 * nr3);
-    if (WEIGHTED) fix_add(&X.dfix[kt + nb * 6 * nr3], &X.dfix[kt + nb * 6 * nr3 + X.dhi], qv, X.dscale);
+    if (WEIGHTED) qfix(X, &X.dfix[kt + nb * 6 * nr3], &X.dfix[kt + nb * 6 * nr3 + X.dhi], qv, X.dscale);
   }
   return 1;
 }
@@ -222,7 +232,7 @@ __device__ __forceinline__ int quad_root(const QuadCtx& X, const QVerts& V, unsi
   if (kk < 0) return 0;
   qcount<SHC>(X, kk + X.nbin * nr);
   if (WEIGHTED)
-    fix_add(&X.fix[kk + X.nbin * nr], &X.fix[kk + X.nbin * (nr + 5)],
+    qfix(X, &X.fix[kk + X.nbin * nr], &X.fix[kk + X.nbin * (nr + 5)],
             ((V.w[R] * qsel(u0, V)) * qsel(u1, V)) * qsel(u2, V), X.fscale);
   const int role[4] = {R, u0, u1, u2};
 #pragma unroll
@@ -235,7 +245,7 @@ __device__ __forceinline__ int quad_root(const QuadCtx& X, const QVerts& V, unsi
     // discR (both random) equals category 2 and is copied on the host
     qdcount<SHC>(X, kt + X.nbin * 6 * npr);
     if (WEIGHTED)
-      fix_add(&X.dfix[kt + X.nbin * 6 * npr], &X.dfix[kt + X.nbin * 6 * npr + X.dhi], q, X.dscale);
+      qfix(X, &X.dfix[kt + X.nbin * 6 * npr], &X.dfix[kt + X.nbin * 6 * npr + X.dhi], q, X.dscale);
   }
   return 1;
 }
@@ -303,7 +313,7 @@ __device__ __forceinline__ int quad_root_rt(const QuadCtx& X, const QVerts& V,
   const int kk = (cfg - 1) + X.ncfg * ((d1 - 1) + X.nbins * (d2 - 1));
   qcount<SHC>(X, kk + X.nbin * nr);
   if (WEIGHTED)
-    fix_add(&X.fix[kk + X.nbin * nr], &X.fix[kk + X.nbin * (nr + 5)],
+    qfix(X, &X.fix[kk + X.nbin * nr], &X.fix[kk + X.nbin * (nr + 5)],
             ((qsel(R, V) * qsel(u0, V)) * qsel(u1, V)) * qsel(u2, V), X.fscale);
   const unsigned rp = (unsigned)R | ((unsigned)u0 << 2) | ((unsigned)u1 << 4) | ((unsigned)u2 << 6);
 #pragma unroll 1
@@ -315,7 +325,7 @@ __device__ __forceinline__ int quad_root_rt(const QuadCtx& X, const QVerts& V,
     const int kt = kk + X.nbin * tt;
     qdcount<SHC>(X, kt + X.nbin * 6 * npr);
     if (WEIGHTED)
-      fix_add(&X.dfix[kt + X.nbin * 6 * npr], &X.dfix[kt + X.nbin * 6 * npr + X.dhi],
+      qfix(X, &X.dfix[kt + X.nbin * 6 * npr], &X.dfix[kt + X.nbin * 6 * npr + X.dhi],
               qsel(u, V) * qsel(vv, V), X.dscale);
   }
   return 1;
@@ -433,6 +443,7 @@ __device__ __forceinline__ void quad_setup(QuadCtx& X, const QuadParams& Q, unsi
   X.fix = g_fix;
   X.dfix = d_fix;
   X.dhi = nd;
+  X.split = Q.split;
   X.scnt = nullptr;
   X.sdcnt = nullptr;
   if (SHC) {
@@ -1014,7 +1025,7 @@ static void launch_quad_grid(K kfn, int nw, size_t smem, int n, int* work, cudaS
   int per_sm = 0;
   GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nw * 32, smem));
   if (per_sm < 1) per_sm = 1;
-  int64_t blocks = (int64_t)per_sm * 148;
+  int64_t blocks = (int64_t)per_sm * sm_count();
   const int64_t need = ((int64_t)n + nw - 1) / nw;
   if (blocks > need) blocks = need;
   if (blocks < 1) blocks = 1;

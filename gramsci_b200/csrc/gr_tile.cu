@@ -1,0 +1,384 @@
+// Tile pair sweep for dense cells: the 2PCF pair binning of gr_pair.cu
+// (create_graph + query_graph_2pcf, src/gramsci.F90:288-379) reorganised for
+// cells holding tens to hundreds of points.
+//
+// A warp takes a cell from the work counter; its lanes hold 32 of the
+// cell's points as roots.  The forward candidates (labels above the roots in
+// the half stencil) are staged 32 at a time in the warp's own shared-memory
+// tile, as separate x / y / z / buffer-flag arrays, and every lane tests all
+// 32 against its root with packed FP32x2 arithmetic (two candidates per
+// instruction) on the squared separation, without a square root, against the
+// outer bounds of the guard band.  Each lane records its hits in a 32-bit
+// mask; after the tile the masks are compacted into a per-warp queue and the
+// hits are binned 32 at a time with every lane busy: exact classification
+// (FP32 with the guard band, FP64 inside it), then the two rooted updates of
+// the pair, as in the other sweeps.  No block barrier is taken.
+//
+// On grids of cells at least rmax/2 wide (GridParams::sub = 2) the stencil
+// is two cells on every axis: 15.6 rmax^3 of candidate volume per root
+// against 27 rmax^3 with cells at least rmax wide, for the same 4.2 rmax^3
+// of neighbour volume.
+//
+// Histograms are private to each warp in shared memory when they fit (32-bit
+// counts, flushed to the global 64-bit counts before any could overflow, and
+// 128-bit fixed-point sums for weighted catalogues), else updated with
+// global atomics.
+#include "gr_kernels.cuh"
+
+namespace gr {
+
+namespace {
+
+constexpr int kTileWarps = 8;
+constexpr int kTileThreads = kTileWarps * 32;
+constexpr int kTileQueue = 32 * 32;  // one tile's hits at most
+constexpr float kBufferPush = 1.0e30f;  // added to d2 of a pair of two buffer points
+
+// Exact bins of a pair that passed the outer membership bounds: FP32 with
+// the guard band (approximate square roots and divisions, whose errors the
+// band covers: see make_pair_params), FP64 reference arithmetic inside it.
+// Returns false when the pair is not an edge.
+template <bool F32>
+__device__ __forceinline__ bool tile_bins(const DevCatalog& C, const PairParams& P, int p, int q,
+                                          const float4 pi, const float4 pj, int& bin, int& muf,
+                                          int& mur, unsigned long long& rechecks) {
+  if (F32) {
+    const float dx = pj.x - pi.x;
+    const float dy = pj.y - pi.y;
+    const float dz = pj.z - pi.z;
+    const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    int r = 1;
+    if (d2 >= P.rmax2_hi || d2 <= P.rmin2_lo) return false;
+    const float d = d2 > 0.0f ? d2 * rsqrtf(d2) : 0.0f;  // 0: t = -rmin, decided in FP64
+    const float t = (d - P.f_rmin) * P.f_inv_dr;
+    const float tn = rintf(t);
+    if (fabsf(t - tn) < P.tguard) {
+      r = 2;
+    } else if (t <= 0.0f || t >= (float)P.nbins) {
+      return false;
+    } else {
+      bin = (int)t + 1;
+      muf = 1;
+      mur = 1;
+      if (P.rsd) {
+        const float dd = d - P.d0;
+        const float mx = 0.5f * (pi.x + pj.x);
+        const float my = 0.5f * (pi.y + pj.y);
+        const float mz = 0.5f * (pi.z + pj.z);
+        const float m2 = fmaf(mz, mz, fmaf(my, my, mx * mx));
+        const float mm = m2 * rsqrtf(m2);
+        const float mmm = mm - P.mB;
+        // __fdividef needs denominators of at least 2^-126
+        if (!(dd > 1e-30f) || !(mmm > 1e-30f) || !(m2 > 0.0f)) {
+          r = 2;
+        } else {
+          const float dot = fmaf(mz, -dz, fmaf(my, -dy, mx * -dx));
+          const float th = __fdividef(dot, mm * d);
+          const float eth = __fdividef(P.eA, dd) + __fdividef(P.eB, mmm) + P.eC;
+          const float ug = eth * P.f_mu_scale + 8.0f * 5.96046448e-8f * P.f_nmu;
+          const float u1 = (th + 1.0f) * P.f_mu_scale;
+          const float u2 = (1.0f - th) * P.f_mu_scale;
+          const float k1 = rintf(u1), k2 = rintf(u2);
+          if ((k1 >= 1.0f && k1 <= P.f_nmu - 1.0f && fabsf(u1 - k1) < ug) ||
+              (k2 >= 1.0f && k2 <= P.f_nmu - 1.0f && fabsf(u2 - k2) < ug)) {
+            r = 2;
+          } else {
+            const int a = (int)floorf(u1) + 1;
+            const int b = (int)floorf(u2) + 1;
+            muf = a < 1 ? 1 : (a > P.nmu ? P.nmu : a);
+            mur = b < 1 ? 1 : (b > P.nmu ? P.nmu : b);
+          }
+        }
+      }
+    }
+    if (r == 1) return true;
+    rechecks++;
+  }
+  return edge_f64(C.posd[p], C.posd[q], P, bin, muf, mur);
+}
+
+// Shared memory of one warp: candidate tile (structure of arrays), labels,
+// the chunk's root positions and the hit queue.
+struct TileWarp {
+  float x[32], y[32], z[32], w[32];
+  int q[32];
+  float4 root[32];
+  uint16_t queue[kTileQueue];
+  int rb[16], rpre[16];  // candidate ranges of the current chunk: begin, prefix
+};
+
+// WHIST: histograms private to each warp in shared memory (else global).
+// SUB: 1 (cells >= rmax, 5 ranges) or 2 (cells >= rmax/2, 13 ranges).
+template <bool F32, bool WEIGHTED, bool WHIST, int SUB>
+__global__ void __launch_bounds__(kTileThreads, 2)
+    pair2_tile_kernel(DevCatalog C, PairParams P, unsigned long long* __restrict__ g_cnt,
+                      unsigned long long* __restrict__ g_fix, double fscale,
+                      unsigned long long* __restrict__ stats, int* __restrict__ work) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ TileWarp s_tw[kTileWarps];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  TileWarp& T = s_tw[wib];
+  const int nbm = P.nbins * P.nmu;
+  const int nh = nbm * 4;
+  // per-warp histograms: counts (32-bit), then fixed-point lo and hi words
+  const size_t wstride = WHIST ? (size_t)nh * (WEIGHTED ? 20 : 4) : 0;
+  unsigned int* w_cnt = reinterpret_cast<unsigned int*>(smem + wstride * wib);
+  unsigned long long* w_lo =
+      reinterpret_cast<unsigned long long*>(smem + wstride * wib + (size_t)nh * 4);
+  unsigned long long* w_hi = w_lo + nh;
+  if (WHIST) {
+    for (int k = lane; k < nh; k += 32) {
+      w_cnt[k] = 0u;
+      if (WEIGHTED) {
+        w_lo[k] = 0ull;
+        w_hi[k] = 0ull;
+      }
+    }
+  }
+  __syncwarp();
+  const int ncell = (int)C.grid.ncell;
+  constexpr int NR = SUB == 2 ? 13 : 5;
+  unsigned long long rechecks = 0, cands = 0, pairs = 0;
+  unsigned int pending = 0;  // edges drained since the last flush (warp-uniform)
+
+  auto flush = [&]() {
+    if (!WHIST) return;
+    __syncwarp();
+    for (int k = lane; k < nh; k += 32) {
+      if (w_cnt[k]) {
+        atomicAdd(&g_cnt[k], (unsigned long long)w_cnt[k]);
+        w_cnt[k] = 0u;
+      }
+      if (WEIGHTED && (w_lo[k] | w_hi[k])) {
+        fix_merge(&g_fix[k], &g_fix[nh + k], w_lo[k], w_hi[k]);
+        w_lo[k] = 0ull;
+        w_hi[k] = 0ull;
+      }
+    }
+    __syncwarp();
+  };
+
+  for (;;) {
+    int cell = 0;
+    if (lane == 0) cell = atomicAdd(work, 1);
+    cell = __shfl_sync(0xffffffffu, cell, 0);
+    if (cell >= ncell) break;
+    const int cb = C.cell_start[cell], ce = C.cell_start[cell + 1];
+    if (cb == ce) continue;
+    GridParams g;
+    const int* cs;
+    int lkey;
+    cell_grid(C, cell, g, cs, lkey);
+    for (int c0 = cb; c0 < ce; c0 += 32) {
+      // this chunk's candidate ranges, starting just after its first root
+      int rbeg = 0, rend = 0;
+      if (SUB == 2) {
+        if (lane < NR) forward_range2_slot(lane, c0 + 1, lkey, g, cs, rbeg, rend);
+      } else {
+        Ranges R5;
+        forward_ranges(c0, lkey, g, cs, R5);
+#pragma unroll
+        for (int k = 0; k < 5; ++k)
+          if (lane == k) {
+            rbeg = R5.beg[k];
+            rend = R5.end[k];
+          }
+      }
+      int len = lane < NR ? rend - rbeg : 0;
+      int incl = len;
+#pragma unroll
+      for (int o = 1; o < 16; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const int total = __shfl_sync(0xffffffffu, incl, NR - 1);
+      if (lane < NR) {
+        T.rb[lane] = rbeg;
+        T.rpre[lane] = incl - len;
+      }
+      const int p = c0 + lane;
+      const bool act = p < ce;
+      float4 pi = act ? C.pos4[p] : make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
+      T.root[lane] = pi;
+      const float pwb = (act && pi.w != 0.0f) ? kBufferPush : 0.0f;
+      const float2 npx = make_float2(-pi.x, -pi.x), npy = make_float2(-pi.y, -pi.y),
+                   npz = make_float2(-pi.z, -pi.z), pwb2 = make_float2(pwb, pwb);
+      const float hi = P.rmax2_hi, lo = P.rmin2_lo;
+      __syncwarp();
+      int kr = 0;  // range of the tile's first candidate (warp-uniform)
+      for (int t0 = 0; t0 < total; t0 += 32) {
+        // stage candidate t0 + lane
+        const int f = t0 + lane;
+        while (kr + 1 < NR && t0 >= T.rpre[kr + 1]) ++kr;
+        int k = kr;
+        while (k + 1 < NR && f >= T.rpre[k + 1]) ++k;
+        const int tn = min(32, total - t0);
+        if (lane < tn) {
+          const int q = T.rb[k] + (f - T.rpre[k]);
+          const float4 c = C.pos4[q];
+          T.x[lane] = c.x;
+          T.y[lane] = c.y;
+          T.z[lane] = c.z;
+          T.w[lane] = c.w;
+          T.q[lane] = q;
+        } else {
+          T.x[lane] = __int_as_float(0x7fc00000);  // NaN: never a hit
+          T.y[lane] = 0.f;
+          T.z[lane] = 0.f;
+          T.w[lane] = 0.f;
+          T.q[lane] = 0x7fffffff;
+        }
+        __syncwarp();
+        unsigned m = 0u;
+        if (act) {
+#pragma unroll
+          for (int j = 0; j < 32; j += 2) {
+            const float2 cx = *reinterpret_cast<const float2*>(&T.x[j]);
+            const float2 cy = *reinterpret_cast<const float2*>(&T.y[j]);
+            const float2 cz = *reinterpret_cast<const float2*>(&T.z[j]);
+            const float2 cw = *reinterpret_cast<const float2*>(&T.w[j]);
+            const float2 dx = __fadd2_rn(cx, npx);
+            const float2 dy = __fadd2_rn(cy, npy);
+            const float2 dz = __fadd2_rn(cz, npz);
+            float2 d2 = __fmul2_rn(dx, dx);
+            d2 = __ffma2_rn(dy, dy, d2);
+            d2 = __ffma2_rn(dz, dz, d2);
+            d2 = __ffma2_rn(cw, pwb2, d2);
+            if (d2.x < hi && d2.x > lo) m |= 1u << j;
+            if (d2.y < hi && d2.y > lo) m |= 2u << j;
+          }
+          // the first tile holds own-cell candidates with labels at or
+          // below some lanes' roots
+          if (t0 == 0) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              if (T.q[j] <= p) m &= ~(1u << j);
+          }
+          cands += (unsigned long long)tn;
+        }
+        // compact the hits into the warp's queue, then bin them
+        const int cnt = __popc(m);
+        int ex = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(0xffffffffu, ex, o);
+          if (lane >= o) ex += v;
+        }
+        const int tot = __shfl_sync(0xffffffffu, ex, 31);
+        int pos = ex - cnt;
+        while (m) {
+          const int j = __ffs(m) - 1;
+          T.queue[pos++] = (uint16_t)((lane << 5) | j);
+          m &= m - 1u;
+        }
+        __syncwarp();
+        for (int e0 = 0; e0 < tot; e0 += 32) {
+          if (e0 + lane < tot) {
+            const int ent = T.queue[e0 + lane];
+            const int r = ent >> 5, j = ent & 31;
+            const int pr = c0 + r, q = T.q[j];
+            const float4 a = T.root[r];
+            const float4 b = make_float4(T.x[j], T.y[j], T.z[j], T.w[j]);
+            int bin = 1, mf = 1, mr = 1;
+            if (tile_bins<F32>(C, P, pr, q, a, b, bin, mf, mr, rechecks)) {
+              const uint8_t fp = C.flags[pr], fq = C.flags[q];
+              const bool root_p = !(fp & FLAG_BUFFER), root_q = !(fq & FLAG_BUFFER);
+              const int rp = fp & FLAG_RANDOM, rq = fq & FLAG_RANDOM;
+              pairs += (root_p || root_q) ? 1 : 0;
+              const double prod = WEIGHTED ? C.w[pr] * C.w[q] : 0.0;
+              if (root_p) {
+                const int kh = (bin - 1) + P.nbins * (mf - 1) + nbm * (2 * rp + rq);
+                if (WHIST) {
+                  atomicAdd(&w_cnt[kh], 1u);
+                  if (WEIGHTED) fix_add(&w_lo[kh], &w_hi[kh], prod, fscale);
+                } else {
+                  atomicAdd(&g_cnt[kh], 1ull);
+                  if (WEIGHTED) fix_add(&g_fix[kh], &g_fix[nh + kh], prod, fscale);
+                }
+              }
+              if (root_q) {
+                const int kh = (bin - 1) + P.nbins * (mr - 1) + nbm * (2 * rq + rp);
+                if (WHIST) {
+                  atomicAdd(&w_cnt[kh], 1u);
+                  if (WEIGHTED) fix_add(&w_lo[kh], &w_hi[kh], prod, fscale);
+                } else {
+                  atomicAdd(&g_cnt[kh], 1ull);
+                  if (WEIGHTED) fix_add(&g_fix[kh], &g_fix[nh + kh], prod, fscale);
+                }
+              }
+            }
+          }
+        }
+        // a 32-bit count grows by at most 2 per binned pair
+        pending += (unsigned)tot;
+        if (pending > (1u << 30)) {
+          flush();
+          pending = 0u;
+        }
+        __syncwarp();
+      }
+    }
+  }
+  flush();
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    rechecks += __shfl_xor_sync(0xffffffffu, rechecks, o);
+    pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
+    cands += __shfl_xor_sync(0xffffffffu, cands, o);
+  }
+  if (lane == 0) {
+    if (rechecks) atomicAdd(&stats[0], rechecks);
+    if (cands) atomicAdd(&stats[1], cands);
+    if (pairs) atomicAdd(&stats[2], pairs);
+  }
+}
+
+}  // namespace
+
+size_t pair2_tile_smem_bytes(const PairParams& P, bool weighted) {
+  const size_t nh = (size_t)P.nbins * P.nmu * 4;
+  return nh * (weighted ? 20 : 4) * kTileWarps;
+}
+
+void launch_pair2_tile(const DevCatalog& C, const PairParams& P, bool weighted,
+                       unsigned long long* g_cnt, unsigned long long* g_fix, double fscale,
+                       unsigned long long* stats, int* work, cudaStream_t s) {
+  if (C.n <= 0) return;
+  size_t smem = pair2_tile_smem_bytes(P, weighted);
+  const bool whist = smem <= kMaxTileHistSmem;
+  if (!whist) smem = 0;
+  GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));
+  const int sub = C.grid.sub == 2 ? 2 : 1;
+#define GR_TILE_LAUNCH(F, W, H, S)                                                           \
+  do {                                                                                        \
+    auto k = pair2_tile_kernel<F, W, H, S>;                                                   \
+    GR_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
+                                     (int)smem));                                             \
+    int per_sm = 1;                                                                           \
+    GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTileThreads, smem)); \
+    int64_t blocks = (int64_t)std::max(1, per_sm) * sm_count();                               \
+    const int64_t need = (C.grid.ncell + kTileWarps - 1) / kTileWarps;                        \
+    if (blocks > need) blocks = std::max<int64_t>(1, need);                                   \
+    k<<<(unsigned)blocks, kTileThreads, smem, s>>>(C, P, g_cnt, g_fix, fscale, stats, work);  \
+  } while (0)
+#define GR_TILE_S(F, W, H)                                                                   \
+  do {                                                                                        \
+    if (sub == 2) GR_TILE_LAUNCH(F, W, H, 2); else GR_TILE_LAUNCH(F, W, H, 1);                \
+  } while (0)
+#define GR_TILE_H(F, W)                                                                      \
+  do {                                                                                        \
+    if (whist) GR_TILE_S(F, W, true); else GR_TILE_S(F, W, false);                            \
+  } while (0)
+  if (P.f32) {
+    if (weighted) GR_TILE_H(true, true); else GR_TILE_H(true, false);
+  } else {
+    if (weighted) GR_TILE_H(false, true); else GR_TILE_H(false, false);
+  }
+#undef GR_TILE_H
+#undef GR_TILE_S
+#undef GR_TILE_LAUNCH
+  GR_CHECK_LAUNCH();
+}
+
+}  // namespace gr

@@ -672,7 +672,7 @@ static void launch_tri3_part(const DevCatalog& C, const CSRView& G, const TriPar
     int per_sm = 0;                                                                           \
     GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nw * 32, smem));   \
     if (per_sm < 1) per_sm = 1;                                                               \
-    int64_t blocks = (int64_t)per_sm * 148;                                                   \
+    int64_t blocks = (int64_t)per_sm * sm_count();                                                   \
     const int64_t need = ((int64_t)C.n + nw * kChunk - 1) / (nw * kChunk);                    \
     if (blocks > need) blocks = need;                                                         \
     kfn<<<(unsigned)blocks, nw * 32, smem, s>>>(C, G, T, g_cnt, g_lim, stats, work, nullptr,  \
@@ -740,7 +740,7 @@ static void launch_adj3_part(const DevCatalog& C, const CSRView& G, const TriPar
   int per_sm = 0;
   GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, nw * 32, smem));
   if (per_sm < 1) per_sm = 1;
-  int64_t blocks = (int64_t)per_sm * 148;
+  int64_t blocks = (int64_t)per_sm * sm_count();
   const int64_t need = ((int64_t)C.n + nw * kChunk - 1) / (nw * kChunk);
   if (blocks > need) blocks = need;
   kfn<<<(unsigned)blocks, nw * 32, smem, s>>>(C, G, T, nullptr, nullptr, stats, work, cot2, cot3,

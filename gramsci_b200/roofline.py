@@ -70,6 +70,63 @@ def quad4_roofline(ctx, q_ms, pk, geometric):
             "bytes_per_launch": b, "ms_per_launch": ms, "peak_source": pk["source"]}
 
 
+def profile(kernel, workload):
+    """The committed ncu summary profiles/<kernel>_<workload>.json, or None."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+def issue_roofline(prof, units, ms, sm_mhz, n_sm):
+    """Instruction-issue ceiling of a kernel: warp instructions per work unit
+    from its committed ncu summary (warp_instructions / units of the profiled
+    launch) times the units of this launch, over the issue slots of the
+    launch (n_sm SMs x 4 schedulers x SM clock x duration).  None without a
+    profile or a clock reading."""
+    if not prof or not sm_mhz or not ms or "warp_instructions" not in prof or not prof.get("units"):
+        return None
+    per_unit = float(prof["warp_instructions"]) / float(prof["units"])
+    achieved = per_unit * units / (ms * 1e-3) / 1e9
+    peak = n_sm * 4 * sm_mhz * 1e6 / 1e9
+    return {"unit": "G warp instructions/s", "achieved": achieved, "peak": peak,
+            "frac": achieved / peak, "warp_inst_per_unit": per_unit,
+            "work_unit": prof.get("unit_name", "tuple"), "source": prof.get("file")}
+
+
+def atomic_roofline(prof, units, ms, sm_mhz, n_sm):
+    """Shared-memory atomic rate of a binning kernel: shared atomic
+    wavefronts per work unit from its ncu summary times this launch's units,
+    per second, against one shared-memory wavefront per SM per cycle (the
+    shared-memory pipe's peak)."""
+    if not prof or not sm_mhz or not ms or "shared_atomic_wavefronts" not in prof or not prof.get("units"):
+        return None
+    per_unit = float(prof["shared_atomic_wavefronts"]) / float(prof["units"])
+    rate = per_unit * units / (ms * 1e-3) / 1e9
+    peak = n_sm * sm_mhz * 1e6 / 1e9
+    return {"unit": "G shared atomic wavefronts/s", "achieved": rate, "peak": peak,
+            "frac": rate / peak, "wavefronts_per_unit": per_unit, "source": prof.get("file")}
+
+
+def graph_bytes(stats):
+    """Algorithmic bytes of the one-pass graph build (csr_fill_kernel): each
+    point's FP32 position read once (16 B) and its row start, length and
+    full degree written (16 B), and one 8-byte record written per upper
+    edge."""
+    return 32 * stats["n_points"] + 8 * stats["upper_edges"]
+
+
+def graph_roofline(stats, ms, pk, traffic):
+    b = graph_bytes(stats)
+    achieved = b / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": "csr_fill_kernel", "achieved": achieved,
+            "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
+            "traffic": traffic, "bytes_per_launch": b, "ms_per_launch": ms,
+            "peak_source": pk["source"]}
+
+
 def profiled_traffic(kernel, scale, workload="c2"):
     """DRAM bytes (read + write) per launch of `kernel` from the committed ncu
     summary profiles/<kernel>_<workload>.json, for the full-size workload

@@ -47,10 +47,14 @@ typedef struct gr_ctx gr_ctx;
 #define GR_OPT_TIMEOUT_MS 2 /* accepted (> 0) and stored; no kernel of this library waits on
                                another block, a flag or another device, so nothing uses it */
 #define GR_OPT_AUTOTUNE 3   /* 0: fixed kernels; 1: time the pair-sweep variants once per
-                               workload class and cache the choice (default); 2+v: force
-                               variant v (0 warp per cell, 1/2 block per cell of 128/256,
-                               3 warp per cell with queued binning, 4/5 block per cell of
-                               128/256 with queued binning) */
+                               workload class and cache the choice, and give dense
+                               catalogues (64 or more points per rmax-wide cell) cells of
+                               rmax/2 and the tile sweep (default); 2+v: force variant v
+                               (0 warp per cell, 1/2 block per cell of 128/256, 3 warp per
+                               cell with queued binning, 4/5 block per cell of 128/256 with
+                               queued binning, 6 the tile sweep, 7 the tile sweep on cells
+                               of rmax/2; 6 and 7 need the FP32 path and fall back to 0
+                               without it) */
 #define GR_OPT_KEEP_GRAPH 4 /* 0 (default): every count call builds the index and graph;
                                1: keep the graph of the last call and reuse it until the
                                catalogue, the bins or the precision change */
@@ -242,11 +246,15 @@ int gr_get_stats(gr_ctx* ctx, gr_stats* out);
  * live in one fixed device array inside the library (about 4.3 MB per GPU,
  * held until the process exits).  At most GR_NOALLOC_MAX_POINTS points and
  * nbins*nmu <= GR_NOALLOC_MAX_BINS; larger inputs return GR_E_CAPACITY and
- * run nothing.  Work is queued on `stream` (cudaStream_t, NULL = default
- * stream) on the current device; the outputs are ready when it completes.
- * The first call on a device looks up the array's device address, so make it
- * before any stream capture.  All calls share the array: calls whose work
- * overlaps on the GPU race and must be serialised by the caller. */
+ * run nothing.  Work runs on `stream` (cudaStream_t, NULL = default stream)
+ * on the current device.  Each call waits on `stream` once, part-way: the
+ * catalogue's bounding box is read back to size the cell grid; the rest of
+ * the work is queued without waiting and the outputs are ready when the
+ * stream reaches them.  Non-finite coordinates or weights return GR_E_ARG
+ * after that read-back.  The first call on a device (and CUDA context) looks
+ * up the array's device address, so make it before any stream capture.  All
+ * calls share the array: calls whose work overlaps on the GPU race and must
+ * be serialised by the caller. */
 #define GR_NOALLOC_MAX_POINTS 32768
 #define GR_NOALLOC_MAX_BINS 4096
 int gr_count_2pcf_noalloc(const double* d_xyz, const double* d_w, int64_t n_data, int64_t n_rand,

@@ -210,9 +210,45 @@ def test_pair_sweep_variants_agree(gpu_ctx, oracle, name, scale, nmu, weighted):
     gpu_ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], nmu)
     ref = oracle.Graph(cat.xyz, sp["rmin"], sp["rmax"], sp["nbins"], nmu).pcf2(w, cat.n_data)
     try:
-        for v in range(6):
+        # 0-5 on cells at least rmax wide, 6 the tile sweep on them, 7 the
+        # tile sweep on cells of rmax/2
+        for v in range(8):
             gpu_ctx.set_autotune(v)
             _check_sums(gpu_ctx.count_2pcf(), ref)
+    finally:
+        gpu_ctx.set_autotune("on")
+
+
+@pytest.mark.parametrize("variant", [6, 7])
+@pytest.mark.parametrize("case", ["buffers_mu", "coincident_rmin0", "far_origin_weighted"])
+def test_tile_sweep_edge_cases(gpu_ctx, oracle, variant, case):
+    """The tile sweeps (lanes over roots, packed FP32x2 membership tests,
+    approximate square roots inside the guard band) against the oracle on
+    dense cells: buffer points with line-of-sight bins, coincident points
+    with rmin = 0 (zero separations), and a catalogue far from the origin
+    with lognormal weights (large coordinates widen the guard band)."""
+    rng = np.random.default_rng(70 + variant)
+    n = 6000
+    nd = 2000
+    if case == "far_origin_weighted":
+        xyz = 1500.0 + rng.normal(0.0, 40.0, (n, 3))
+    else:
+        xyz = rng.normal(0.0, 25.0, (n, 3)) + np.array([300.0, -200.0, 100.0])
+    if case == "coincident_rmin0":
+        xyz[100:140] = xyz[100]          # 40 copies of one point
+        xyz[3000:3010] = xyz[2999]
+    w = catalogs.normalise(np.ones(n) if case != "far_origin_weighted"
+                           else rng.lognormal(0.0, 0.5, n), nd, n - nd)
+    buf = (rng.random(n) < 0.3).astype(np.int32) if case == "buffers_mu" else None
+    rmin = 0.0 if case == "coincident_rmin0" else 2.0
+    nmu = 7 if case == "buffers_mu" else 1
+    gpu_ctx.set_catalog(xyz, w, nd, buffer=buf)
+    gpu_ctx.set_bins(rmin, 20.0, 9, nmu)
+    ref = oracle.Graph(xyz, rmin, 20.0, 9, nmu).pcf2(w, nd, buffer=buf)
+    assert int(ref["counts"].sum()) > 100_000
+    try:
+        gpu_ctx.set_autotune(variant)
+        _check_sums(gpu_ctx.count_2pcf(), ref)
     finally:
         gpu_ctx.set_autotune("on")
 

@@ -28,7 +28,7 @@ def _worker(rank, world, port, out):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world,
                             timeout=datetime.timedelta(seconds=60))
-    cat, w, sp = bench.make_catalogue(0.001, bench.rank_seed(rank))
+    cat, w, sp = bench.make_catalogue(bench.WORKLOAD, 0.001, bench.rank_seed(rank))
     t = bench.reduce_over_ranks(10.0 + rank, "max", "cpu")
     c = bench.reduce_over_ranks(cat.n, "sum", "cpu")
     out[rank] = (t, c, cat.n, float(cat.xyz[0, 0]))
