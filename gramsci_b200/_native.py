@@ -82,6 +82,10 @@ SIGNATURES = {
     "gr_adjoint_2pcf": (ctypes.c_int, [_ctx, _vp, _vp, _vp]),
     "gr_set_regions": (ctypes.c_int, [_ctx, ctypes.c_int32]),
     "gr_count_2pcf_batched": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp]),
+    "gr_set_region_ids": (ctypes.c_int, [_ctx, _vp, ctypes.c_int32]),
+    "gr_set_mocks": (ctypes.c_int, [_ctx, ctypes.c_int32, _vp, _vp]),
+    "gr_count_2pcf_regions": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp]),
+    "gr_count_3pcf_batched": (ctypes.c_int, [_ctx, _vp, _vp, _vp, _vp]),
     "gr_regions_info": (ctypes.c_int, [_ctx, _vp, _vp]),
     "gr_regions_export": (ctypes.c_int, [_ctx, _vp, _vp, _vp]),
     "gr_adjoint_3pcf": (ctypes.c_int, [_ctx, _vp, _vp, _vp]),

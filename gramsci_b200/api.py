@@ -55,6 +55,8 @@ class Context:
         self.device = device
         self.nbins = self.nmu = None
         self.n = None
+        self._nsplit = 0
+        self.nregions = 0
         self._keep = None
 
     def close(self):
@@ -85,7 +87,9 @@ class Context:
 
     def set_catalog(self, xyz, w, n_data, buffer=None):
         """xyz (N,3) FP64, w (N,) signed normalised FP64 weights, galaxies
-        first (n_data of them), buffer (N,) 0/1 or None."""
+        first (n_data of them), buffer (N,) 0/1 or None.  Clears region ids
+        and mocks (they describe the points of a catalogue)."""
+        self.nregions = self._nsplit ** 3
         if _is_torch_cuda(xyz):
             import torch
 
@@ -126,7 +130,7 @@ class Context:
         int variant to force (0 warp per cell, 1/2 block per cell of 128/256
         threads, 3 warp per cell with queued binning, 4/5 block per cell of
         128/256 with queued binning, 6 the tile sweep, 7 the tile sweep on
-        cells of rmax/2; 6 and 7 need the FP32 path)."""
+        cells of rmax/2)."""
         v = {"off": 0, "on": 1}.get(mode, None)
         if v is None:
             v = 2 + int(mode)
@@ -186,6 +190,8 @@ class Context:
     def set_regions(self, nsplit):
         """Split the catalogue box into nsplit^3 regions with Rmax halos."""
         self._check(self._lib.gr_set_regions(self._h, int(nsplit)))
+        self._nsplit = int(nsplit)
+        self.nregions = self._nsplit ** 3
 
     def count_2pcf_batched(self):
         """2PCF of all regions in one launch (CUDA-graph replay after the
@@ -198,6 +204,52 @@ class Context:
                                                     _ptr(catsum)))
         return dict(N2=_fortran(N2, nb, nm), N3=_fortran(N3, nb, nm),
                     counts=_fortran(counts, nb, nm, 4), catsum=_fortran(catsum, nb, nm, 4))
+
+    def set_region_ids(self, region_of_point, nregions):
+        """Regions from a region id per point (e.g. jackknife regions): each
+        region's halo is the bounding box of its points grown by rmax."""
+        ids = np.ascontiguousarray(region_of_point, np.int32)
+        if ids.shape != (self.n,):
+            raise ValueError("one region id per catalogue point")
+        self._check(self._lib.gr_set_region_ids(self._h, _ptr(ids), int(nregions)))
+        self.nregions = int(nregions)
+
+    def set_mocks(self, n_data, n_rand):
+        """The catalogue is several independent mocks one after another (each
+        galaxies first, weights normalised within the mock); batched calls
+        count them all in one launch, never pairing two mocks."""
+        nd = np.ascontiguousarray(n_data, np.int64)
+        nr = np.ascontiguousarray(n_rand, np.int64)
+        if nd.shape != nr.shape or nd.ndim != 1:
+            raise ValueError("n_data and n_rand: one entry per mock")
+        self._check(self._lib.gr_set_mocks(self._h, int(nd.size), _ptr(nd), _ptr(nr)))
+        self.nregions = int(nd.size)
+
+    def count_2pcf_regions(self):
+        """2PCF of every region (or mock) separately, in one launch: N2, N3
+        (nbins, nmu, nregions), counts and catsum (nbins, nmu, 4, nregions)."""
+        nb, nm = self.nbins, self.nmu
+        R = self.nregions
+        N2, N3 = np.zeros(nb * nm * R), np.zeros(nb * nm * R)
+        counts = np.zeros(nb * nm * 4 * R, np.int64)
+        catsum = np.zeros(nb * nm * 4 * R)
+        self._check(self._lib.gr_count_2pcf_regions(self._h, _ptr(N2), _ptr(N3), _ptr(counts),
+                                                    _ptr(catsum)))
+        return dict(N2=_fortran(N2, nb, nm, R), N3=_fortran(N3, nb, nm, R),
+                    counts=_fortran(counts, nb, nm, 4, R), catsum=_fortran(catsum, nb, nm, 4, R))
+
+    def count_3pcf_batched(self):
+        """3PCF of all regions (or mocks) in one pass, summed; shapes as
+        count_3pcf."""
+        nb, nm = self.nbins, self.nmu
+        nc = ncfg3(nb)
+        N2, N3 = np.zeros(nc * nm), np.zeros(nc * nm)
+        cnt = np.zeros(nc * nm * 4, np.int64)
+        catsum = np.zeros(nc * nm * 4)
+        self._check(self._lib.gr_count_3pcf_batched(self._h, _ptr(N2), _ptr(N3), _ptr(cnt),
+                                                    _ptr(catsum)))
+        return dict(N2=_fortran(N2, nc, nm), N3=_fortran(N3, nc, nm),
+                    counts=_fortran(cnt, nc, nm, 4), catsum=_fortran(catsum, nc, nm, 4))
 
     def regions(self):
         """Region layout of the last batched call: list of (member catalogue

@@ -21,23 +21,6 @@ namespace {
 constexpr int kAdjWarps = 8;
 constexpr int kAdjThreads = kAdjWarps * 32;
 
-// Coefficient of the pair (p, q) in dL/dw: the cotangents of the bins the
-// pair lands in from each non-buffer end (cot3 only for random-random).
-__device__ __forceinline__ double pair_coef(const double* c2, const double* c3, int nbins, int b,
-                                            int mf, int mr, uint8_t fp, uint8_t fq) {
-  const bool rr = (fp & fq & FLAG_RANDOM) != 0;
-  double c = 0.0;
-  if (!(fp & FLAG_BUFFER)) {
-    const int k = (b - 1) + nbins * (mf - 1);
-    c += rr ? c2[k] + c3[k] : c2[k];
-  }
-  if (!(fq & FLAG_BUFFER)) {
-    const int k = (b - 1) + nbins * (mr - 1);
-    c += rr ? c2[k] + c3[k] : c2[k];
-  }
-  return c;
-}
-
 template <bool F32>
 __device__ __forceinline__ bool adj_edge(const DevCatalog& C, const PairParams& P, int p, int q,
                                          const float4& pi, const float4& pj, int& b, int& mf,

@@ -63,10 +63,12 @@ struct gr_ctx {
   DevBuf<int> work;
   DevBuf<double> cot, grad;              // adjoint inputs / output
   DevBuf<unsigned long long> gfix;       // adjoint fixed-point gradients (lo[n], hi[n])
-  // batched regions
+  // batched regions: 0 none, 1 nsplit^3 subcubes, 2 region ids, 3 mocks
+  int region_mode = 0;
   int nsplit = 0;
   RegionLayout regions;
   DevBuf<unsigned long long> bcnt, bfix, bstats;
+  DevBuf<unsigned long long> rcnt, rfix;  // per-region histograms
   DevBuf<int> bwork;
   bool batch_weighted = false;
   int batch_variant = 0;
@@ -305,19 +307,22 @@ int set_err(gr_ctx* c, int code, const std::string& m) {
 
 // Clears *flag unless all galaxy weights are equal and all random weights are
 // equal; writes max |w| over galaxies to wmax[0] and over randoms to wmax[1]
-// (as the bits of non-negative doubles).  Reduced per block first, so each
-// block makes at most three global updates.
+// (as the bits of non-negative doubles) and sets *nonfinite when a weight is
+// not finite (tested directly, not through the maxima).  Reduced per block
+// first, so each block makes at most four global updates.
 __global__ void uniform_check_kernel(const double* __restrict__ w, int64_t n_data, int64_t n,
-                                     unsigned char* flag, unsigned long long* wmax) {
+                                     unsigned char* flag, unsigned long long* wmax,
+                                     int* nonfinite) {
   __shared__ unsigned long long s_mg[32], s_mr[32];
   __shared__ int s_bad[32];
   unsigned long long mg = 0, mr = 0;
-  bool bad = false;
+  bool bad = false, nf = false;
   const double refg = n_data > 0 ? w[0] : 0.0;
   const double refr = n > n_data ? w[n_data] : 0.0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const double v = w[i];
+    nf = nf || !isfinite(v);
     const double ref = i < n_data ? refg : refr;
     bad = bad || __double_as_longlong(v) != __double_as_longlong(ref);
     const unsigned long long a = (unsigned long long)__double_as_longlong(fabs(v));
@@ -331,6 +336,7 @@ __global__ void uniform_check_kernel(const double* __restrict__ w, int64_t n_dat
     mr = u > mr ? u : mr;
   }
   bad = __any_sync(0xffffffffu, bad);
+  if (__any_sync(0xffffffffu, nf) && (threadIdx.x & 31) == 0) atomicOr(nonfinite, 1);
   const int wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   if ((threadIdx.x & 31) == 0) {
     s_mg[wid] = mg;
@@ -514,7 +520,8 @@ static int set_catalog_impl(gr_ctx* c, const double* xyz, const double* w, const
   c->n_rand = n_rand;
   // Uniform weights (all galaxies equal, all randoms equal) let the kernels
   // keep integer counts only; sums are then count x product.
-  // [0] uniform flag, [8] max |w| galaxies, [16] max |w| randoms, [24] fingerprint
+  // [0] uniform flag, [4] non-finite weight flag (int), [8] max |w| galaxies,
+  // [16] max |w| randoms, [24] fingerprint
   c->uniform_flag.reserve(32);
   unsigned char init[24] = {1};
   unsigned char out[24];
@@ -522,7 +529,8 @@ static int set_catalog_impl(gr_ctx* c, const double* xyz, const double* w, const
   unsigned long long* d_wmax = reinterpret_cast<unsigned long long*>(c->uniform_flag.p + 8);
   if (n > 0) {
     int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)2 * sm_count());
-    uniform_check_kernel<<<blocks, 256, 0, s>>>(c->w.p, n_data, n, c->uniform_flag.p, d_wmax);
+    uniform_check_kernel<<<blocks, 256, 0, s>>>(c->w.p, n_data, n, c->uniform_flag.p, d_wmax,
+                                                reinterpret_cast<int*>(c->uniform_flag.p + 4));
     GR_CHECK_LAUNCH();
   }
   GR_CUDA_TRY(cudaMemcpyAsync(out, c->uniform_flag.p, 24, cudaMemcpyDeviceToHost, s));
@@ -532,10 +540,19 @@ static int set_catalog_impl(gr_ctx* c, const double* xyz, const double* w, const
     GR_CUDA_TRY(cudaMemcpyAsync(&wr, c->w.p + n_data, sizeof(double), cudaMemcpyDeviceToHost, s));
   GR_CUDA_TRY(cudaStreamSynchronize(s));
   unsigned char flag = out[0];
+  int nonfinite = 0;
+  std::memcpy(&nonfinite, out + 4, 4);
+  if (nonfinite) {
+    c->cat_set = false;  // nothing may be counted on a half-set catalogue
+    return set_err(c, GR_E_ARG, "non-finite weights");
+  }
   std::memcpy(&c->wgmax, out + 8, 8);
   std::memcpy(&c->wrmax, out + 16, 8);
   c->wmax = std::max(c->wgmax, c->wrmax);
-  if (!std::isfinite(c->wmax)) return set_err(c, GR_E_ARG, "non-finite weights");
+  if (!std::isfinite(c->wmax)) {
+    c->cat_set = false;
+    return set_err(c, GR_E_ARG, "non-finite weights");
+  }
   c->uniform = flag != 0;
   c->w_gal = wg;
   c->w_ran = wr;
@@ -543,6 +560,12 @@ static int set_catalog_impl(gr_ctx* c, const double* xyz, const double* w, const
   c->csr_valid = false;
   c->graph_loaded = false;
   c->regions.valid = false;
+  // region ids and mocks describe the points of the previous catalogue
+  if (c->region_mode >= 2) {
+    c->regions.set_split();
+    c->regions.release_graph();
+    c->region_mode = c->nsplit > 0 ? 1 : 0;
+  }
   GR_API_END(c)
 }
 
@@ -582,6 +605,8 @@ int gr_set_option(gr_ctx* c, int32_t key, int64_t value) {
     if (c->precision != (int)value) {
       c->csr_valid = false;
       c->graph_loaded = false;
+      c->regions.valid = false;
+      c->regions.release_graph();
     }
     c->precision = (int)value;
   } else if (key == GR_OPT_KEEP_GRAPH) {
@@ -626,13 +651,11 @@ static int pick_pair2_variant(gr_ctx* c, const DevCatalog& C, bool weighted, dou
   if (C.grid.sub == 2) return kPairTile2;
   if (c->autotune == 0) return kPairWarpCell;
   if (c->autotune >= 2) {
-    int v = c->autotune - 2;
-    if (v == kPairTile2) v = kPairTile;
-    if (v == kPairTile && !c->P.f32) v = kPairWarpCell;
-    return v;
+    const int v = c->autotune - 2;
+    return v == kPairTile2 ? kPairTile : v;
   }
-  // the tile sweep runs on the FP32 path only
-  const int nvar = c->P.f32 ? kPairTile + 1 : kPairTile;
+  // the variants that read cells at least rmax wide
+  const int nvar = kPairTile + 1;
   const double per_cell = C.grid.ncell > 0 ? (double)C.n / (double)C.grid.ncell : 1.0;
   int dens = 0;
   while (dens < 20 && std::ldexp(1.0, dens + 1) <= per_cell) ++dens;
@@ -697,14 +720,11 @@ int gr_count_2pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
   c->stats.reserve(8);
   GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
   if (!reuse_graph(c)) {
-    // dense catalogues on the FP32 path: cells of rmax/2 and the tile sweep
+    // dense catalogues: cells of rmax/2 and the tile sweep
     int sub = 1;
-    if (c->precision == 0 && !c->logbins) {
-      if (c->autotune == 1) sub = 0;
-      if (c->autotune == 2 + kPairTile2) sub = 2;
-    }
+    if (c->autotune == 1) sub = 0;
+    if (c->autotune == 2 + kPairTile2) sub = 2;
     build_index(c, false, sub);
-    if (c->index.grid.sub == 2 && !c->P.f32) build_index(c, false, 1);
   }
   GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
   c->work.reserve(4);
@@ -1377,8 +1397,15 @@ static void finish_grad(gr_ctx* c, double gscale, double* grad_w, cudaEvent_t q0
 static int pick_adj2_layout(gr_ctx* c, const DevCatalog& C, const double* c2, const double* c3,
                             double gscale, unsigned long long* g_lo, unsigned long long* g_hi,
                             int* work, cudaStream_t s) {
+  // a grid of rmax/2 cells is read by the tile sweep only
+  if (C.grid.sub == 2) return kPairTile2;
   if (c->autotune == 0) return kPairWarpCell;
-  if (c->autotune >= 2) return c->autotune - 2;
+  if (c->autotune >= 2) {
+    const int v = c->autotune - 2;
+    if (v == kPairTile || v == kPairTile2) return kPairTile;
+    return v == kPairDense128 || v == kPairDenseQ128 ? kPairDense128
+           : v == kPairDense256 || v == kPairDenseQ256 ? kPairDense256 : kPairWarpCell;
+  }
   const double per_cell = C.grid.ncell > 0 ? (double)C.n / (double)C.grid.ncell : 1.0;
   int dens = 0;
   while (dens < 20 && std::ldexp(1.0, dens + 1) <= per_cell) ++dens;
@@ -1387,7 +1414,7 @@ static int pick_adj2_layout(gr_ctx* c, const DevCatalog& C, const double* c2, co
   int cb = 0;
   while (cb < 20 && ((int64_t)4 << (2 * cb)) <= C.grid.ncell) ++cb;
   char key[128];
-  std::snprintf(key, sizeof(key), "adj2v1|%s|dens%d|hist%d|cells%d", c->P.f32 ? "f32" : "f64", dens,
+  std::snprintf(key, sizeof(key), "adj2v2|%s|dens%d|hist%d|cells%d", c->P.f32 ? "f32" : "f64", dens,
                 hb, cb);
   Tuner& T = tuner();
   {
@@ -1396,16 +1423,24 @@ static int pick_adj2_layout(gr_ctx* c, const DevCatalog& C, const double* c2, co
     auto it = T.choice.find(key);
     if (it != T.choice.end()) return it->second;
   }
-  const int layouts[3] = {kPairWarpCell, kPairDense128, kPairDense256};
+  // the tile sweep accumulates into g_lo / g_hi: the caller zeroes them
+  // after the timing runs
+  const int layouts[4] = {kPairWarpCell, kPairDense128, kPairDense256, kPairTile};
+  c->stats.reserve(8);
+  auto run = [&](int v) {
+    if (layouts[v] == kPairTile)
+      launch_adj2_tile(C, c->P, c2, c3, gscale, g_lo, g_hi, c->stats.p, work, s);
+    else
+      launch_adj2(C, c->P, c2, c3, gscale, g_lo, g_hi, work, s, layouts[v]);
+  };
   ScopedEvents ev;
   cudaEvent_t a = ev.a, b = ev.b;
-  float t[3] = {1e30f, 1e30f, 1e30f};
-  for (int v = 0; v < 3; ++v)
-    launch_adj2(C, c->P, c2, c3, gscale, g_lo, g_hi, work, s, layouts[v]);
+  float t[4] = {1e30f, 1e30f, 1e30f, 1e30f};
+  for (int v = 0; v < 4; ++v) run(v);
   for (int round = 0; round < 3; ++round)
-    for (int v = 0; v < 3; ++v) {
+    for (int v = 0; v < 4; ++v) {
       GR_CUDA_TRY(cudaEventRecord(a, s));
-      launch_adj2(C, c->P, c2, c3, gscale, g_lo, g_hi, work, s, layouts[v]);
+      run(v);
       GR_CUDA_TRY(cudaEventRecord(b, s));
       GR_CUDA_TRY(cudaEventSynchronize(b));
       float ms = 0.f;
@@ -1413,7 +1448,7 @@ static int pick_adj2_layout(gr_ctx* c, const DevCatalog& C, const double* c2, co
       t[v] = std::min(t[v], ms);
     }
   int best = 0;
-  for (int v = 1; v < 3; ++v)
+  for (int v = 1; v < 4; ++v)
     if (t[v] < t[best]) best = v;
   std::lock_guard<std::mutex> lock(T.mu);
   T.choice[key] = layouts[best];
@@ -1430,24 +1465,44 @@ int gr_adjoint_2pcf(gr_ctx* c, const double* cot2, const double* cot3, double* g
   const int nbm = c->nbins * c->nmu;
   const int64_t n = c->n;
   const double cmax = max_abs(cot2, nbm) + max_abs(cot3, nbm);
-  const double gscale = fix_scale(2.0 * cmax * c->wmax);
   c->cot.reserve(2 * nbm);
   c->gfix.reserve(2 * n + 2);
   c->work.reserve(4);
+  c->stats.reserve(8);
   GR_CUDA_TRY(cudaMemcpyAsync(c->cot.p, cot2, sizeof(double) * nbm, cudaMemcpyHostToDevice, s));
   if (cot3)
     GR_CUDA_TRY(cudaMemcpyAsync(c->cot.p + nbm, cot3, sizeof(double) * nbm, cudaMemcpyHostToDevice, s));
+  else
+    GR_CUDA_TRY(cudaMemsetAsync(c->cot.p + nbm, 0, sizeof(double) * nbm, s));
   GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
-  if (!reuse_graph(c)) build_index(c);
+  if (!reuse_graph(c)) {
+    // dense catalogues: cells of rmax/2 and the tile sweep
+    int sub = 1;
+    if (c->autotune == 1) sub = 0;
+    if (c->autotune == 2 + kPairTile2) sub = 2;
+    build_index(c, false, sub);
+  }
   GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
-  GR_CUDA_TRY(cudaMemsetAsync(c->gfix.p, 0, sizeof(unsigned long long) * (2 * n + 2), s));
   std::memset(&c->st, 0, sizeof(c->st));
-  const double* dc3 = cot3 ? c->cot.p + nbm : nullptr;
-  const int variant = pick_adj2_layout(c, c->index.view(), c->cot.p, dc3, gscale, c->gfix.p,
+  const double* dc3 = c->cot.p + nbm;
+  // the tile sweep's per-warp 64-bit partials take up to 32 terms: 2^6 of
+  // headroom over the largest term (2 cotangents times a weight)
+  const double gscale_t = fix_scale(64.0 * 2.0 * cmax * c->wmax);
+  const double gscale_c = fix_scale(2.0 * cmax * c->wmax);
+  const int variant = pick_adj2_layout(c, c->index.view(), c->cot.p, dc3, gscale_t, c->gfix.p,
                                        c->gfix.p + n, c->work.p, s);
+  const bool tile = variant == kPairTile || variant == kPairTile2;
+  const double gscale = tile ? gscale_t : gscale_c;
   GR_CUDA_TRY(cudaEventRecord(c->ev[2], s));  // after any tuning runs
-  launch_adj2(c->index.view(), c->P, c->cot.p, dc3, gscale, c->gfix.p, c->gfix.p + n, c->work.p, s,
-              variant);
+  GR_CUDA_TRY(cudaMemsetAsync(c->gfix.p, 0, sizeof(unsigned long long) * (2 * n + 2), s));
+  if (tile) {
+    GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
+    launch_adj2_tile(c->index.view(), c->P, c->cot.p, dc3, gscale, c->gfix.p, c->gfix.p + n,
+                     c->stats.p, c->work.p, s);
+  } else {
+    launch_adj2(c->index.view(), c->P, c->cot.p, dc3, gscale, c->gfix.p, c->gfix.p + n, c->work.p,
+                s, variant);
+  }
   finish_grad(c, gscale, grad_w, c->ev[2]);
   c->st.ms_index = ev_ms(c->ev[0], c->ev[1]);
   c->st.ms_total = c->st.ms_index + c->st.ms_query;
@@ -1590,8 +1645,54 @@ int gr_set_regions(gr_ctx* c, int32_t nsplit) {
   GR_API_BEGIN(c)
   if (nsplit < 0 || nsplit > 64) return set_err(c, GR_E_ARG, "nsplit must be in 0..64");
   c->nsplit = nsplit;
-  c->regions.valid = false;
+  c->region_mode = nsplit > 0 ? 1 : 0;
+  c->regions.set_split();
+  c->regions.release_graph();
   GR_API_END(c)
+}
+
+int gr_set_region_ids(gr_ctx* c, const int32_t* region_of_point, int32_t nregions) {
+  GR_API_BEGIN(c)
+  if (!c->cat_set) return set_err(c, GR_E_ARG, "catalogue not set (gr_set_catalog)");
+  if (nregions < 1 || nregions > (1 << 20)) return set_err(c, GR_E_ARG, "nregions must be in 1..2^20");
+  if (c->n > 0 && !region_of_point) return set_err(c, GR_E_ARG, "null region ids");
+  c->regions.set_ids(region_of_point, c->n, nregions, c->stream());
+  c->region_mode = 2;
+  GR_API_END(c)
+}
+
+int gr_set_mocks(gr_ctx* c, int32_t nmocks, const int64_t* n_data, const int64_t* n_rand) {
+  GR_API_BEGIN(c)
+  if (!c->cat_set) return set_err(c, GR_E_ARG, "catalogue not set (gr_set_catalog)");
+  if (nmocks < 1 || nmocks > (1 << 20)) return set_err(c, GR_E_ARG, "nmocks must be in 1..2^20");
+  if (!n_data || !n_rand) return set_err(c, GR_E_ARG, "null mock sizes");
+  c->regions.set_mocks(n_data, n_rand, nmocks, c->n, c->stream());
+  c->region_mode = 3;
+  GR_API_END(c)
+}
+
+// The region layout of the current split, catalogue and binning, planned on
+// first use (pair parameters, weight mode, grid resolution).  rmax_cells:
+// the caller reads the layout with the rmax-wide cell kernels (graph
+// build), so a layout of rmax/2 cells is planned again.
+static void ensure_regions(gr_ctx* c, cudaStream_t s, bool rmax_cells) {
+  if (c->regions.valid && (!rmax_cells || c->regions.grid_sub == 1)) return;
+  // pair parameters from the catalogue's coordinate bound
+  c->index.build(c->xyz.p, c->w.p, nullptr, c->n, c->n_data, c->rmax, s);
+  make_pair_params(c->P, c->rmin, c->rmax, c->nbins, c->nmu, c->logbins, c->index.coord_max,
+                   c->precision == 1);
+  c->csr_valid = false;
+  // dense regions: cells of rmax/2 and the tile sweep
+  int sub = 1;
+  if (!rmax_cells) {
+    if (c->autotune == 1) sub = 0;
+    if (c->autotune == 2 + kPairTile2) sub = 2;
+  }
+  c->regions.plan(c->xyz.p, c->n, c->n_data, c->rmax, c->nsplit, s, sub, kDenseCellPoints);
+  // mocks carry their own galaxy / random split and normalisation: always
+  // the fixed-point sums
+  c->batch_weighted = !c->uniform || c->region_mode == 3;
+  c->batch_fscale = fix_scale(c->wmax * c->wmax);
 }
 
 // Device work of one batched call: region layout, histogram reset, pair sweep.
@@ -1605,10 +1706,36 @@ static void enqueue_batched(gr_ctx* c, cudaStream_t s) {
                c->bstats.p, c->bwork.p, s, c->batch_variant);
 }
 
+// 2PCF sums of one histogram set (nh counts and 2nh fixed-point words) into
+// the caller's arrays.
+static void pair_outputs(const gr_ctx* c, bool weighted, double fscale,
+                         const unsigned long long* hc, const unsigned long long* hf, double* N2,
+                         double* N3, int64_t* counts, double* catsum) {
+  const int nbm = c->nbins * c->nmu, nh = nbm * 4;
+  std::vector<double> hs(nh, 0.0);
+  if (weighted) {
+    for (int k = 0; k < nh; ++k) hs[k] = fix_value(hf[k], hf[nh + k], fscale);
+  } else {
+    for (int cat = 0; cat < 4; ++cat) {
+      const int nr = (cat >> 1) + (cat & 1);
+      const double prod = uniform_product(c->w_gal, c->w_ran, 2 - nr, nr);
+      for (int k = 0; k < nbm; ++k) hs[k + nbm * cat] = (double)hc[k + nbm * cat] * prod;
+    }
+  }
+  for (int k = 0; k < nbm; ++k) {
+    if (N2) N2[k] = ((hs[k] + hs[k + nbm]) + hs[k + 2 * nbm]) + hs[k + 3 * nbm];
+    if (N3) N3[k] = hs[k + 3 * nbm];
+  }
+  if (counts)
+    for (int k = 0; k < nh; ++k) counts[k] = (int64_t)hc[k];
+  if (catsum)
+    for (int k = 0; k < nh; ++k) catsum[k] = hs[k];
+}
+
 int gr_count_2pcf_batched(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* catsum) {
   GR_API_BEGIN(c)
   require_ready(c);
-  if (c->nsplit < 1) return set_err(c, GR_E_ARG, "regions not set (gr_set_regions)");
+  if (c->region_mode == 0) return set_err(c, GR_E_ARG, "regions not set (gr_set_regions, gr_set_region_ids or gr_set_mocks)");
   ensure_events(c);
   for (int k = 0; k < 2; ++k)
     if (!c->bev[k]) GR_CUDA_TRY(cudaEventCreateWithFlags(&c->bev[k], cudaEventDisableTiming));
@@ -1619,22 +1746,8 @@ int gr_count_2pcf_batched(gr_ctx* c, double* N2, double* N3, int64_t* counts, do
   GR_CUDA_TRY(cudaEventRecord(c->bev[0], us));
   GR_CUDA_TRY(cudaStreamWaitEvent(s, c->bev[0], 0));
   GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
-  bool replay = c->regions.valid && c->regions.exec;
-  if (!c->regions.valid) {
-    // pair parameters from the catalogue's coordinate bound
-    c->index.build(c->xyz.p, c->w.p, nullptr, c->n, c->n_data, c->rmax, s);
-    make_pair_params(c->P, c->rmin, c->rmax, c->nbins, c->nmu, c->logbins, c->index.coord_max,
-                     c->precision == 1);
-    // dense regions on the FP32 path: cells of rmax/2 and the tile sweep
-    int sub = 1;
-    if (c->P.f32) {
-      if (c->autotune == 1) sub = 0;
-      if (c->autotune == 2 + kPairTile2) sub = 2;
-    }
-    c->regions.plan(c->xyz.p, c->n, c->n_data, c->rmax, c->nsplit, s, sub, kDenseCellPoints);
-    c->csr_valid = false;
-    c->batch_weighted = !c->uniform;
-    c->batch_fscale = fix_scale(c->wmax * c->wmax);
+  ensure_regions(c, s, false);
+  if (!c->regions.exec) {
     c->bcnt.reserve(nh);
     c->bfix.reserve(2 * nh);
     c->bstats.reserve(8);
@@ -1660,12 +1773,10 @@ int gr_count_2pcf_batched(gr_ctx* c, double* N2, double* N3, int64_t* counts, do
     GR_CUDA_TRY(cudaStreamEndCapture(s, &c->regions.graph));
     GR_CUDA_TRY(cudaGraphInstantiate(&c->regions.exec, c->regions.graph, 0));
     GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
-    replay = true;
   }
-  if (replay) GR_CUDA_TRY(cudaGraphLaunch(c->regions.exec, s));
+  GR_CUDA_TRY(cudaGraphLaunch(c->regions.exec, s));
   GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
   std::vector<unsigned long long> hc(nh), hf(2 * nh, 0ull);
-  std::vector<double> hs(nh, 0.0);
   unsigned long long st[8];
   GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->bcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
   if (c->batch_weighted)
@@ -1674,25 +1785,9 @@ int gr_count_2pcf_batched(gr_ctx* c, double* N2, double* N3, int64_t* counts, do
   GR_CUDA_TRY(cudaEventRecord(c->bev[1], s));
   GR_CUDA_TRY(cudaStreamWaitEvent(us, c->bev[1], 0));
   GR_CUDA_TRY(cudaStreamSynchronize(s));
-  if (c->batch_weighted) {
-    for (int k = 0; k < nh; ++k) hs[k] = fix_value(hf[k], hf[nh + k], c->batch_fscale);
-  } else {
-    for (int cat = 0; cat < 4; ++cat) {
-      const int nr = (cat >> 1) + (cat & 1);
-      const double prod = uniform_product(c->w_gal, c->w_ran, 2 - nr, nr);
-      for (int k = 0; k < nbm; ++k) hs[k + nbm * cat] = (double)hc[k + nbm * cat] * prod;
-    }
-  }
+  pair_outputs(c, c->batch_weighted, c->batch_fscale, hc.data(), hf.data(), N2, N3, counts, catsum);
   int64_t rooted = 0;
   for (int k = 0; k < nh; ++k) rooted += (int64_t)hc[k];
-  for (int k = 0; k < nbm; ++k) {
-    if (N2) N2[k] = ((hs[k] + hs[k + nbm]) + hs[k + 2 * nbm]) + hs[k + 3 * nbm];
-    if (N3) N3[k] = hs[k + 3 * nbm];
-  }
-  if (counts)
-    for (int k = 0; k < nh; ++k) counts[k] = (int64_t)hc[k];
-  if (catsum)
-    for (int k = 0; k < nh; ++k) catsum[k] = hs[k];
   std::memset(&c->st, 0, sizeof(c->st));
   c->st.ms_query = ev_ms(c->ev[0], c->ev[1]);
   c->st.ms_total = c->st.ms_query;
@@ -1702,6 +1797,158 @@ int gr_count_2pcf_batched(gr_ctx* c, double* N2, double* N3, int64_t* counts, do
   c->st.fp64_rechecks = (int64_t)st[0];
   c->st.candidates = (int64_t)st[1];
   c->st.kernel_launches = 11;
+  GR_API_END(c)
+}
+
+int gr_count_2pcf_regions(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* catsum) {
+  GR_API_BEGIN(c)
+  require_ready(c);
+  if (c->region_mode == 0) return set_err(c, GR_E_ARG, "regions not set (gr_set_regions, gr_set_region_ids or gr_set_mocks)");
+  ensure_events(c);
+  cudaStream_t s = c->stream();
+  const int nbm = c->nbins * c->nmu, nh = nbm * 4;
+  GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
+  ensure_regions(c, s, false);
+  const int nreg = c->regions.nreg;
+  const size_t tot = (size_t)nreg * nh;
+  c->rcnt.reserve(tot);
+  c->rfix.reserve(2 * tot);
+  c->bstats.reserve(8);
+  c->bwork.reserve(4);
+  c->regions.enqueue_layout(c->xyz.p, c->w.p, s);
+  {
+    ZeroList z;
+    z.add(c->rcnt.p, sizeof(unsigned long long) * tot);
+    z.add(c->rfix.p, sizeof(unsigned long long) * 2 * tot);
+    z.add(c->bstats.p, sizeof(unsigned long long) * 8);
+    zero_async(z, s);
+  }
+  GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+  launch_pair2_tile(c->regions.view(), c->P, c->batch_weighted, c->rcnt.p, c->rfix.p,
+                    c->batch_fscale, c->bstats.p, c->bwork.p, s, true);
+  GR_CUDA_TRY(cudaEventRecord(c->ev[2], s));
+  std::vector<unsigned long long> hc(tot), hf(2 * tot, 0ull);
+  unsigned long long st[8];
+  GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->rcnt.p, sizeof(unsigned long long) * tot, cudaMemcpyDeviceToHost, s));
+  if (c->batch_weighted)
+    GR_CUDA_TRY(cudaMemcpyAsync(hf.data(), c->rfix.p, sizeof(unsigned long long) * 2 * tot, cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaMemcpyAsync(st, c->bstats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaStreamSynchronize(s));
+  int64_t rooted = 0;
+  for (int r = 0; r < nreg; ++r) {
+    const size_t o = (size_t)r * nh;
+    pair_outputs(c, c->batch_weighted, c->batch_fscale, hc.data() + o, hf.data() + 2 * o,
+                 N2 ? N2 + (size_t)r * nbm : nullptr, N3 ? N3 + (size_t)r * nbm : nullptr,
+                 counts ? counts + o : nullptr, catsum ? catsum + o : nullptr);
+  }
+  for (size_t k = 0; k < tot; ++k) rooted += (int64_t)hc[k];
+  std::memset(&c->st, 0, sizeof(c->st));
+  c->st.ms_index = ev_ms(c->ev[0], c->ev[1]);
+  c->st.ms_query = ev_ms(c->ev[1], c->ev[2]);
+  c->st.ms_total = ev_ms(c->ev[0], c->ev[2]);
+  c->st.n_points = c->regions.n_members;
+  c->st.tuples = (int64_t)st[2];
+  c->st.rooted = rooted;
+  c->st.fp64_rechecks = (int64_t)st[0];
+  c->st.candidates = (int64_t)st[1];
+  c->st.kernel_launches = 11;
+  GR_API_END(c)
+}
+
+int gr_count_3pcf_batched(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* catsum) {
+  GR_API_BEGIN(c)
+  require_ready(c);
+  if (c->region_mode == 0) return set_err(c, GR_E_ARG, "regions not set (gr_set_regions, gr_set_region_ids or gr_set_mocks)");
+  ensure_events(c);
+  cudaStream_t s = c->stream();
+  const int nmu = c->nmu;
+  const int ncfg = (int)(((int64_t)c->nbins * (c->nbins + 1) * (c->nbins + 2)) / 6);
+  const int nbin = ncfg * nmu, nh = nbin * 4;
+  GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
+  ensure_regions(c, s, true);
+  const bool weighted = c->batch_weighted;
+  // mocks carry no global galaxy / random split: one scale for every product
+  double fscale[4];
+  for (int nr = 0; nr < 4; ++nr)
+    fscale[nr] = c->region_mode == 3 ? fix_scale(c->wmax * c->wmax * c->wmax)
+                                     : fix_scale(std::pow(c->wgmax, 3 - nr) * std::pow(c->wrmax, nr));
+  c->hcnt.reserve(nh);
+  c->hfix.reserve(2 * nh);
+  c->stats.reserve(8);
+  c->work.reserve(4);
+  std::vector<uint8_t> nt;
+  normal_table(nmu, nt);
+  c->normal_dev.reserve(nt.size());
+  GR_CUDA_TRY(cudaMemcpyAsync(c->normal_dev.p, nt.data(), nt.size(), cudaMemcpyHostToDevice, s));
+  c->regions.enqueue_layout(c->xyz.p, c->w.p, s);
+  const DevCatalog RC = c->regions.view();
+  GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+  c->csr.build(RC, c->P, s);
+  c->csr_valid = false;  // the graph of the region members, not of the catalogue
+  GR_CUDA_TRY(cudaEventRecord(c->ev[2], s));
+  {
+    ZeroList z;
+    z.add(c->hcnt.p, sizeof(unsigned long long) * nh);
+    z.add(c->hfix.p, sizeof(unsigned long long) * 2 * nh);
+    z.add(c->stats.p, sizeof(unsigned long long) * 8);
+    zero_async(z, s);
+  }
+  TriParams T{};
+  T.nbins = c->nbins;
+  T.nmu = nmu;
+  T.ncfg = ncfg;
+  T.rsd = nmu >= 2;
+  T.equi = 0;
+  T.cap = round_cap(c->csr.max_deg, 32, 256);
+  T.normal = c->normal_dev.p;
+  make_rank_tables(T.rank, c->nbins, 3);
+  for (int nr = 0; nr < 4; ++nr) T.fscale[nr] = fscale[nr];
+  T.P = c->P;
+  T.geo = (c->clique_mode == 2 || (c->clique_mode == 0 &&
+           (!T.rsd || (double)c->csr.n_edges >= 24.0 * (double)std::max<int64_t>(1, RC.n)))) ? 1 : 0;
+  T.maxdeg = (int)std::min<int64_t>(c->csr.max_deg, 1 << 30);
+  T.long_geo = c->clique_mode != 1;
+  const int tri_launches = 1 + launch_tri3(RC, c->csr.view(), T, weighted, true, c->hcnt.p,
+                                           c->hfix.p, c->stats.p, c->work.p, s);
+  GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
+  std::vector<unsigned long long> hc(nh), hf(2 * nh, 0ull);
+  std::vector<double> hs(nh, 0.0);
+  unsigned long long st[8];
+  GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
+  if (weighted)
+    GR_CUDA_TRY(cudaMemcpyAsync(hf.data(), c->hfix.p, sizeof(unsigned long long) * 2 * nh, cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaStreamSynchronize(s));
+  if (weighted) {
+    for (int k = 0; k < nh; ++k) hs[k] = fix_value(hf[k], hf[nh + k], fscale[k / nbin]);
+  } else {
+    for (int nr = 0; nr < 4; ++nr) {
+      const double prod = uniform_product(c->w_gal, c->w_ran, 3 - nr, nr);
+      for (int k = 0; k < nbin; ++k) hs[k + nbin * nr] = (double)hc[k + nbin * nr] * prod;
+    }
+  }
+  for (int k = 0; k < nbin; ++k) {
+    if (N2) N2[k] = ((hs[k] + hs[k + nbin]) + hs[k + 2 * nbin]) + hs[k + 3 * nbin];
+    if (N3) N3[k] = -hs[k + 3 * nbin];
+  }
+  if (counts)
+    for (int k = 0; k < nh; ++k) counts[k] = (int64_t)hc[k];
+  if (catsum)
+    for (int k = 0; k < nh; ++k) catsum[k] = hs[k];
+  std::memset(&c->st, 0, sizeof(c->st));
+  c->st.ms_index = ev_ms(c->ev[0], c->ev[1]);
+  c->st.ms_graph = ev_ms(c->ev[1], c->ev[2]);
+  c->st.ms_query = ev_ms(c->ev[2], c->ev[3]);
+  c->st.ms_total = ev_ms(c->ev[0], c->ev[3]);
+  c->st.n_points = c->regions.n_members;
+  c->st.n_edges = 2 * c->csr.n_edges;
+  c->st.upper_edges = c->csr.n_edges;
+  c->st.tuples = (int64_t)st[0];
+  c->st.rooted = (int64_t)st[1];
+  c->st.probes = (int64_t)st[2];
+  c->st.fp64_rechecks = c->csr.rechecks;
+  c->st.candidates = c->csr.candidates;
+  c->st.kernel_launches = c->csr.launches + tri_launches + 9;
   GR_API_END(c)
 }
 

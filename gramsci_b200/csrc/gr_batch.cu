@@ -160,6 +160,83 @@ __global__ void b_member_kernel(const double* __restrict__ xyz, int n, int n_dat
   }
 }
 
+// Region boxes and sizes from a given region id per point.
+__global__ void b_region_box_ids_kernel(const double* __restrict__ xyz, int n,
+                                        const int* __restrict__ reg,
+                                        unsigned long long* __restrict__ box,
+                                        int* __restrict__ own_count) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int r = reg[i];
+    const double x = xyz[3 * (int64_t)i], y = xyz[3 * (int64_t)i + 1], z = xyz[3 * (int64_t)i + 2];
+    atomicMin(&box[6 * r + 0], bkey(x));
+    atomicMin(&box[6 * r + 1], bkey(y));
+    atomicMin(&box[6 * r + 2], bkey(z));
+    atomicMax(&box[6 * r + 3], bkey(x));
+    atomicMax(&box[6 * r + 4], bkey(y));
+    atomicMax(&box[6 * r + 5], bkey(z));
+    atomicAdd(&own_count[r], 1);
+  }
+}
+
+// Region r gains point i as a member (its own point, or a buffer copy).
+template <bool FILL>
+__device__ __forceinline__ void b_add_member(int r, int i, uint8_t fl, double x, double y, double z,
+                                             const RegionGeomDev& G, int* count, int* m_orig,
+                                             uint8_t* m_flag, int* m_key, int* m_slot,
+                                             int* cell_count) {
+  const int slot = atomicAdd(&count[r], 1);
+  if (!FILL) return;
+  const int m = G.mem_off[r] + slot;
+  m_orig[m] = i;
+  m_flag[m] = fl;
+  const GridParams g = G.grid[r];
+  const double v[3] = {x, y, z};
+  int c[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int q = (int)floor((v[d] - G.glo[3 * r + d]) * G.ginv[3 * r + d]);
+    const int nc = d == 0 ? g.nx : (d == 1 ? g.ny : g.nz);
+    c[d] = q < 0 ? 0 : (q >= nc ? nc - 1 : q);
+  }
+  const int key = G.cell_off[r] + (c[2] * g.ny + c[1]) * g.nx + c[0];
+  m_key[m] = key;
+  m_slot[m] = atomicAdd(&cell_count[key], 1);
+}
+
+// Members from a region id per point: every point joins its own region, and
+// (with a coarse grid) every other region whose halo contains it, as a
+// buffer point.  Without a coarse grid (mocks) regions have no halo.
+// Random flags from pflag when given, else from the galaxy/random split.
+template <bool FILL>
+__global__ void b_member_ids_kernel(const double* __restrict__ xyz, int n, int n_data,
+                                    const int* __restrict__ reg, const uint8_t* __restrict__ pflag,
+                                    RegionGeomDev G, CoarseDev CG, int* __restrict__ count,
+                                    int* __restrict__ m_orig, uint8_t* __restrict__ m_flag,
+                                    int* __restrict__ m_key, int* __restrict__ m_slot,
+                                    int* __restrict__ cell_count) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double x = xyz[3 * (int64_t)i], y = xyz[3 * (int64_t)i + 1], z = xyz[3 * (int64_t)i + 2];
+    const int own = reg[i];
+    const uint8_t rnd = pflag ? (uint8_t)(pflag[i] & FLAG_RANDOM) : (uint8_t)(i >= n_data ? FLAG_RANDOM : 0);
+    b_add_member<FILL>(own, i, rnd, x, y, z, G, count, m_orig, m_flag, m_key, m_slot, cell_count);
+    if (!CG.list) continue;
+    const double v[3] = {x, y, z};
+    int c[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int q = (int)floor((v[d] - CG.lo[d]) * CG.inv[d]);
+      c[d] = q < 0 ? 0 : (q >= CG.nc[d] ? CG.nc[d] - 1 : q);
+    }
+    const int cc = (c[2] * CG.nc[1] + c[1]) * CG.nc[0] + c[0];
+    for (int k = CG.off[cc]; k < CG.off[cc + 1]; ++k) {
+      const int r = CG.list[k];
+      if (r == own || !in_halo(G.halo + 6 * r, x, y, z)) continue;
+      b_add_member<FILL>(r, i, (uint8_t)(rnd | FLAG_BUFFER), x, y, z, G, count, m_orig, m_flag,
+                         m_key, m_slot, cell_count);
+    }
+  }
+}
+
 __global__ void b_scatter_kernel(int64_t m, const int* __restrict__ key, const int* __restrict__ slot,
                                  const int64_t* __restrict__ start, int* __restrict__ tmp) {
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m;
@@ -244,12 +321,16 @@ void RegionLayout::plan(const double* d_xyz, int64_t n_pts, int64_t n_data_pts, 
   n = n_pts;
   n_data = n_data_pts;
   rmax = rmax_;
-  ns = nsplit_;
-  nreg = ns * ns * ns;
+  if (mode == kRegionsSplit) {
+    ns = nsplit_;
+    nreg = ns * ns * ns;
+    sub.reserve(n + 1);
+  } else {
+    ns = 0;  // nreg and the region of every point were set by set_ids / set_mocks
+  }
   box_raw.reserve(6 * (size_t)nreg + 8);
   own_count.reserve(nreg);
   count.reserve(nreg);
-  sub.reserve(n + 1);
   // catalogue box
   {
     unsigned long long init[6] = {~0ull, ~0ull, ~0ull, 0, 0, 0};
@@ -264,21 +345,30 @@ void RegionLayout::plan(const double* d_xyz, int64_t n_pts, int64_t n_data_pts, 
   GR_CUDA_TRY(cudaStreamSynchronize(s));
   SplitGeom sg;
   sg.ns = ns;
+  double cat_lo[3], cat_hi[3];
   for (int d = 0; d < 3; ++d) {
     const double lo = n > 0 ? bkey_value(hb[d]) : 0.0, hi = n > 0 ? bkey_value(hb[3 + d]) : 0.0;
     if (!std::isfinite(lo) || !std::isfinite(hi)) throw Error{-1, "non-finite coordinates"};
+    cat_lo[d] = lo;
+    cat_hi[d] = hi;
     sg.lo[d] = lo;
     const double span = hi - lo;
     sg.inv_span[d] = span > 0 ? 1.0 / span : 0.0;
     // subcubes narrower than Rmax would let a halo reach beyond the
     // neighbouring subcubes
-    if (span > 0 && span / ns < rmax) throw Error{-1, "regions narrower than rmax; use a smaller split"};
+    if (mode == kRegionsSplit && span > 0 && span / ns < rmax)
+      throw Error{-1, "regions narrower than rmax; use a smaller split"};
   }
   b_init_box_kernel<<<nblocks(6 * (int64_t)nreg, 256), 256, 0, s>>>(box_raw.p, nreg);
   GR_CUDA_TRY(cudaMemsetAsync(own_count.p, 0, sizeof(int) * nreg, s));
-  if (n > 0)
-    b_region_box_kernel<<<nblocks(n, 256), 256, 0, s>>>(d_xyz, (int)n, sg, sub.p, box_raw.p,
-                                                        own_count.p);
+  if (n > 0) {
+    if (mode == kRegionsSplit)
+      b_region_box_kernel<<<nblocks(n, 256), 256, 0, s>>>(d_xyz, (int)n, sg, sub.p, box_raw.p,
+                                                          own_count.p);
+    else
+      b_region_box_ids_kernel<<<nblocks(n, 256), 256, 0, s>>>(d_xyz, (int)n, sub.p, box_raw.p,
+                                                              own_count.p);
+  }
   GR_CHECK_LAUNCH();
   std::vector<unsigned long long> hbox(6 * (size_t)nreg);
   std::vector<int> hown(nreg);
@@ -296,22 +386,75 @@ void RegionLayout::plan(const double* d_xyz, int64_t n_pts, int64_t n_data_pts, 
       }
       continue;
     }
+    // mocks have no halo: the region box bounds the mock's own grid
+    const double grow = mode == kRegionsMocks ? 0.0 : rmax;
     for (int d = 0; d < 3; ++d) {
-      h_halo[6 * r + d] = bkey_value(hbox[6 * r + d]) - rmax;
-      h_halo[6 * r + 3 + d] = bkey_value(hbox[6 * r + 3 + d]) + rmax;
+      h_halo[6 * r + d] = bkey_value(hbox[6 * r + d]) - grow;
+      h_halo[6 * r + 3 + d] = bkey_value(hbox[6 * r + 3 + d]) + grow;
     }
   }
   halo.reserve(6 * (size_t)nreg);
   GR_CUDA_TRY(cudaMemcpyAsync(halo.p, h_halo.data(), sizeof(double) * 6 * nreg, cudaMemcpyHostToDevice, s));
+  // region ids: a coarse grid over the catalogue listing, per cell, the
+  // regions whose halo reaches it (each point then tests only those)
+  ncoarse = 0;
+  if (mode == kRegionsIds) {
+    ncoarse = make_grid_geom(cat_lo, cat_hi, rmax, 64, (int64_t)1 << 18, coarse);
+    std::vector<int> cnt(ncoarse + 1, 0), lst;
+    auto cell_range = [&](int r, int d, int& a, int& b) {
+      const double lo = coarse.lo[d], inv = coarse.inv_cs[d];
+      const int nc = coarse.nc[d];
+      a = (int)std::floor((h_halo[6 * r + d] - lo) * inv);
+      b = (int)std::floor((h_halo[6 * r + 3 + d] - lo) * inv);
+      a = std::min(std::max(a, 0), nc - 1);
+      b = std::min(std::max(b, 0), nc - 1);
+    };
+    for (int pass = 0; pass < 2; ++pass) {
+      std::vector<int> fill;
+      if (pass == 1) {
+        for (int64_t c = 0; c < ncoarse; ++c) cnt[c + 1] += cnt[c];
+        lst.assign(cnt[ncoarse], 0);
+        fill.assign(cnt.begin(), cnt.end() - 1);
+      }
+      for (int r = 0; r < nreg; ++r) {
+        if (hown[r] == 0) continue;
+        int a[3], b[3];
+        for (int d = 0; d < 3; ++d) cell_range(r, d, a[d], b[d]);
+        for (int z = a[2]; z <= b[2]; ++z)
+          for (int y = a[1]; y <= b[1]; ++y)
+            for (int x = a[0]; x <= b[0]; ++x) {
+              const int64_t c = ((int64_t)z * coarse.nc[1] + y) * coarse.nc[0] + x;
+              if (pass == 0)
+                cnt[c + 1]++;
+              else
+                lst[fill[c]++] = r;
+            }
+      }
+    }
+    coarse_off.reserve(ncoarse + 1);
+    coarse_list.reserve(lst.size() + 1);
+    GR_CUDA_TRY(cudaMemcpyAsync(coarse_off.p, cnt.data(), sizeof(int) * (ncoarse + 1),
+                                cudaMemcpyHostToDevice, s));
+    if (!lst.empty())
+      GR_CUDA_TRY(cudaMemcpyAsync(coarse_list.p, lst.data(), sizeof(int) * lst.size(),
+                                  cudaMemcpyHostToDevice, s));
+    GR_CUDA_TRY(cudaStreamSynchronize(s));  // the host vectors must outlive the copies
+  }
   // member counts
   GR_CUDA_TRY(cudaMemsetAsync(count.p, 0, sizeof(int) * nreg, s));
   RegionGeomDev G{};
   G.halo = halo.p;
   G.ns = ns;
-  if (n > 0)
-    b_member_kernel<false><<<nblocks(n, 256), 256, 0, s>>>(d_xyz, (int)n, (int)n_data, sub.p, G,
-                                                           count.p, nullptr, nullptr, nullptr,
-                                                           nullptr, nullptr);
+  if (n > 0) {
+    if (mode == kRegionsSplit)
+      b_member_kernel<false><<<nblocks(n, 256), 256, 0, s>>>(d_xyz, (int)n, (int)n_data, sub.p, G,
+                                                             count.p, nullptr, nullptr, nullptr,
+                                                             nullptr, nullptr);
+    else
+      b_member_ids_kernel<false><<<nblocks(n, 256), 256, 0, s>>>(
+          d_xyz, (int)n, (int)n_data, sub.p, nullptr, G, coarse_dev(), count.p, nullptr, nullptr,
+          nullptr, nullptr, nullptr);
+  }
   GR_CHECK_LAUNCH();
   h_count.assign(nreg, 0);
   GR_CUDA_TRY(cudaMemcpyAsync(h_count.data(), count.p, sizeof(int) * nreg, cudaMemcpyDeviceToHost, s));
@@ -425,10 +568,16 @@ void RegionLayout::enqueue_layout(const double* d_xyz, const double* d_w, cudaSt
   G.ns = ns;
   GR_CUDA_TRY(cudaMemsetAsync(count.p, 0, sizeof(int) * nreg, s));
   GR_CUDA_TRY(cudaMemsetAsync(cell_count.p, 0, sizeof(int) * (ncell + 1), s));
-  if (n > 0)
-    b_member_kernel<true><<<nblocks(n, 256), 256, 0, s>>>(d_xyz, (int)n, (int)n_data, sub.p, G,
-                                                          count.p, m_orig.p, m_flag.p, m_key.p,
-                                                          m_slot.p, cell_count.p);
+  if (n > 0) {
+    if (mode == kRegionsSplit)
+      b_member_kernel<true><<<nblocks(n, 256), 256, 0, s>>>(d_xyz, (int)n, (int)n_data, sub.p, G,
+                                                            count.p, m_orig.p, m_flag.p, m_key.p,
+                                                            m_slot.p, cell_count.p);
+    else
+      b_member_ids_kernel<true><<<nblocks(n, 256), 256, 0, s>>>(
+          d_xyz, (int)n, (int)n_data, sub.p, mode == kRegionsMocks ? pflag.p : nullptr, G,
+          coarse_dev(), count.p, m_orig.p, m_flag.p, m_key.p, m_slot.p, cell_count.p);
+  }
   GR_CHECK_LAUNCH();
   scan_i32_to_i64(cell_count.p, cell_start64.p, ncell, s, scan_tmp);
   if (n_members > 0) {
@@ -442,6 +591,69 @@ void RegionLayout::enqueue_layout(const double* d_xyz, const double* d_w, cudaSt
   }
   b_narrow_kernel<<<nblocks(ncell + 1, 256), 256, 0, s>>>(cell_start64.p, cell_start.p, ncell + 1);
   GR_CHECK_LAUNCH();
+}
+
+CoarseDev RegionLayout::coarse_dev() const {
+  CoarseDev c{};
+  if (mode != kRegionsIds || ncoarse == 0) return c;  // list null: own region only
+  c.off = coarse_off.p;
+  c.list = coarse_list.p;
+  for (int d = 0; d < 3; ++d) {
+    c.lo[d] = coarse.lo[d];
+    c.inv[d] = coarse.inv_cs[d];
+    c.nc[d] = coarse.nc[d];
+  }
+  return c;
+}
+
+void RegionLayout::set_ids(const int* h_ids, int64_t n_pts, int nregions, cudaStream_t s) {
+  if (nregions < 1) throw Error{-1, "need at least one region"};
+  for (int64_t i = 0; i < n_pts; ++i)
+    if (h_ids[i] < 0 || h_ids[i] >= nregions) throw Error{-1, "region id out of range"};
+  release_graph();
+  sub.reserve(n_pts + 1);
+  if (n_pts > 0) {
+    GR_CUDA_TRY(cudaMemcpyAsync(sub.p, h_ids, sizeof(int) * n_pts, cudaMemcpyHostToDevice, s));
+    GR_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  mode = kRegionsIds;
+  nreg = nregions;
+  valid = false;
+}
+
+void RegionLayout::set_mocks(const int64_t* nd, const int64_t* nr, int nmocks, int64_t n_pts,
+                             cudaStream_t s) {
+  if (nmocks < 1) throw Error{-1, "need at least one mock"};
+  int64_t tot = 0;
+  for (int m = 0; m < nmocks; ++m) {
+    if (nd[m] < 0 || nr[m] < 0) throw Error{-1, "negative mock size"};
+    tot += nd[m] + nr[m];
+  }
+  if (tot != n_pts) throw Error{-1, "mock sizes do not add up to the catalogue"};
+  std::vector<int> ids(n_pts + 1);
+  std::vector<uint8_t> fl(n_pts + 1);
+  int64_t i = 0;
+  for (int m = 0; m < nmocks; ++m) {
+    for (int64_t k = 0; k < nd[m]; ++k, ++i) {
+      ids[i] = m;
+      fl[i] = 0;
+    }
+    for (int64_t k = 0; k < nr[m]; ++k, ++i) {
+      ids[i] = m;
+      fl[i] = FLAG_RANDOM;
+    }
+  }
+  release_graph();
+  sub.reserve(n_pts + 1);
+  pflag.reserve(n_pts + 1);
+  if (n_pts > 0) {
+    GR_CUDA_TRY(cudaMemcpyAsync(sub.p, ids.data(), sizeof(int) * n_pts, cudaMemcpyHostToDevice, s));
+    GR_CUDA_TRY(cudaMemcpyAsync(pflag.p, fl.data(), n_pts, cudaMemcpyHostToDevice, s));
+    GR_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  mode = kRegionsMocks;
+  nreg = nmocks;
+  valid = false;
 }
 
 DevCatalog RegionLayout::view() const {

@@ -7,8 +7,26 @@
 
 namespace gr {
 
+// Catalogue-wide coarse grid of candidate regions (region-id layouts): cell
+// c lists in list[off[c] .. off[c+1]) the regions whose halo reaches it; a
+// null list means no halos (every point belongs to its own region only).
+struct CoarseDev {
+  const int* off;
+  const int* list;
+  double lo[3], inv[3];
+  int nc[3];
+};
+
+// How the catalogue is split into regions.
+enum : int {
+  kRegionsSplit = 0,  // nsplit^3 equal subcubes of the bounding box, Rmax halos
+  kRegionsIds = 1,    // a region id per point (e.g. jackknife regions), Rmax halos
+  kRegionsMocks = 2   // independent catalogues one after another, no halos
+};
+
 struct RegionLayout {
   bool valid = false;
+  int mode = kRegionsSplit;
   int ns = 0, nreg = 0;
   int64_t n = 0, n_data = 0, n_members = 0, ncell = 0;
   double rmax = 0.0;
@@ -17,6 +35,14 @@ struct RegionLayout {
   std::vector<GridParams> h_grid;
   std::vector<int> h_count, h_cell_off;
   std::vector<int64_t> h_mem_off;
+  // ids / mocks: the region of every point (in `sub`) and, for mocks, the
+  // random flag of every point
+  DevBuf<uint8_t> pflag;
+  // ids: coarse grid over the catalogue; cell c lists the regions whose halo
+  // reaches it (coarse_off[c] .. coarse_off[c+1] in coarse_list)
+  GridGeom coarse{};
+  int64_t ncoarse = 0;
+  DevBuf<int> coarse_off, coarse_list;
   // device geometry
   DevBuf<unsigned long long> box_raw;
   DevBuf<int> own_count, count, sub, cell_off, mem_off, cell_region;
@@ -41,8 +67,19 @@ struct RegionLayout {
   int grid_sub = 1;
   void plan(const double* d_xyz, int64_t n, int64_t n_data, double rmax, int nsplit, cudaStream_t s,
             int sub_policy = 1, double dense_per_cell = 0.0);
+  // ids: region of every point (host array of n entries in [0, nregions));
+  // mocks: galaxies and randoms of each mock, the catalogue being the mocks
+  // one after another, each with its galaxies first.  Both replace the
+  // subcube split until set_split is called.
+  void set_ids(const int* h_ids, int64_t n, int nregions, cudaStream_t s);
+  void set_mocks(const int64_t* n_data, const int64_t* n_rand, int nmocks, int64_t n, cudaStream_t s);
+  void set_split() {
+    mode = kRegionsSplit;
+    valid = false;
+  }
   void enqueue_layout(const double* d_xyz, const double* d_w, cudaStream_t s);
   DevCatalog view() const;
+  CoarseDev coarse_dev() const;
 };
 
 }  // namespace gr

@@ -20,13 +20,17 @@ __device__ __forceinline__ unsigned long long dbl_key(double v) {
 }
 
 __global__ void bbox_kernel(const double* __restrict__ xyz, int64_t n, unsigned long long* out) {
-  // out[0..2] min keys, out[3..5] max keys, out[6] max |coord| key
+  // out[0..2] min keys, out[3..5] max keys, out[6] max |coord| key, out[7]
+  // set when a coordinate is not finite (tested directly: a NaN's key does
+  // not reliably survive the min / max reductions)
   unsigned long long mn[3] = {~0ull, ~0ull, ~0ull}, mx[3] = {0, 0, 0}, ab = 0;
+  bool bad = false;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       double v = xyz[3 * i + d];
+      bad = bad || !isfinite(v);
       unsigned long long k = dbl_key(v);
       mn[d] = k < mn[d] ? k : mn[d];
       mx[d] = k > mx[d] ? k : mx[d];
@@ -34,6 +38,7 @@ __global__ void bbox_kernel(const double* __restrict__ xyz, int64_t n, unsigned 
       ab = a > ab ? a : ab;
     }
   }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&out[7], 1ull);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
 #pragma unroll
@@ -79,14 +84,16 @@ __global__ void bbox_check_kernel(const unsigned long long* __restrict__ now,
   if (threadIdx.x == 0) {
     unsigned long long d = 0;
     for (int k = 0; k < 7; ++k) d |= now[k] ^ prev[k];
-    prev[7] = d != 0 ? 1ull : 0ull;
+    // a non-finite coordinate also sends the call to the build with waits,
+    // which reports it
+    prev[7] = (d != 0 || now[7] != 0) ? 1ull : 0ull;
   }
 }
 
 __global__ void init_bbox_kernel(unsigned long long* out) {
   int t = threadIdx.x;
   if (t < 3) out[t] = ~0ull;
-  if (t >= 3 && t < 7) out[t] = 0ull;
+  if (t >= 3 && t < 8) out[t] = 0ull;
 }
 
 __device__ __forceinline__ int cell_coord(double v, double lo, double inv_cs, int nc) {
@@ -200,18 +207,19 @@ void CellIndex::build(const double* d_xyz, const double* d_w, const int* d_buffe
     launches++;
   }
   GR_CHECK_LAUNCH();
-  unsigned long long h[7];
+  unsigned long long h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   speculated = speculate && !auto_sub && have_prev && prev_n == n && prev_rmax == rmax &&
                prev_sub == sub;
   if (speculated) {
-    std::memcpy(h, prev_raw, sizeof(h));
+    std::memcpy(h, prev_raw, sizeof(prev_raw));
     bbox_check_kernel<<<1, 32, 0, s>>>(bbox_raw.p, bbox_prev.p);
     launches++;
     GR_CHECK_LAUNCH();
   } else {
     GR_CUDA_TRY(cudaMemcpyAsync(h, bbox_raw.p, sizeof(h), cudaMemcpyDeviceToHost, s));
     GR_CUDA_TRY(cudaStreamSynchronize(s));
-    std::memcpy(prev_raw, h, sizeof(h));
+    if (h[7] != 0) throw Error{-1, "catalogue has non-finite coordinates"};
+    std::memcpy(prev_raw, h, sizeof(prev_raw));
     prev_n = n;
     prev_rmax = rmax;
     prev_sub = sub;

@@ -479,6 +479,25 @@ __device__ __forceinline__ void cell_grid(const DevCatalog& C, int cell, GridPar
 
 enum : uint8_t { FLAG_RANDOM = 1, FLAG_BUFFER = 2 };
 
+// 2PCF weight adjoint: coefficient of the pair (p, q) in dL/dw, the
+// cotangents of the bins the pair lands in from each non-buffer end (cot3
+// only for random-random pairs); the pair adds coef * w_q to dL/dw_p and
+// coef * w_p to dL/dw_q.
+__device__ __forceinline__ double pair_coef(const double* c2, const double* c3, int nbins, int b,
+                                            int mf, int mr, uint8_t fp, uint8_t fq) {
+  const bool rr = (fp & fq & FLAG_RANDOM) != 0;
+  double c = 0.0;
+  if (!(fp & FLAG_BUFFER)) {
+    const int k = (b - 1) + nbins * (mf - 1);
+    c += rr ? c2[k] + c3[k] : c2[k];
+  }
+  if (!(fq & FLAG_BUFFER)) {
+    const int k = (b - 1) + nbins * (mr - 1);
+    c += rr ? c2[k] + c3[k] : c2[k];
+  }
+  return c;
+}
+
 // ------------------------------------------------------- fixed-point sums --
 // Weighted sums are accumulated as signed 128-bit fixed-point integers with
 // 64-bit integer atomics: a product x becomes V = round(x * 2^e) (|V| < 2^63,

@@ -23,7 +23,7 @@ constexpr size_t kMaxHistSmem = 120 * 1024;
 // run with full warps.
 // kPairTile: the tile sweep (gr_tile.cu) on cells at least rmax wide;
 // kPairTile2: the same on cells at least rmax/2 wide (the only variant that
-// reads such grids).  The tile sweeps need the FP32 path (PairParams::f32).
+// reads such grids).
 enum {
   kPairWarpCell = 0,
   kPairDense128 = 1,
@@ -36,21 +36,25 @@ enum {
   kPairVariants = 8
 };
 // Points per rmax-wide cell from which the 2PCF sweeps use cells of rmax/2
-// and the tile sweep (FP32 path only).
+// and the tile sweep.
 constexpr double kDenseCellPoints = 64.0;
 size_t pair2_smem_bytes(const PairParams& P, bool weighted);
 
 // Tile sweep for dense cells (gr_tile.cu): warp per cell, lanes over 32
 // roots, candidates staged 32 at a time per warp and tested two per packed
-// FP32x2 instruction, hits binned from a per-warp queue; reads grids with
-// cells at least rmax wide (sub 1) or rmax/2 wide (sub 2).  Same inputs,
-// outputs and results as launch_pair2.  Histograms private to each warp in
-// shared memory when they need at most kMaxTileHistSmem bytes.
+// FP32x2 instruction (FP64 path: one per FP64 test), hits binned from a
+// per-warp queue; reads grids with cells at least rmax wide (sub 1) or rmax/2
+// wide (sub 2).  Same inputs, outputs and results as launch_pair2.
+// Histograms private to each warp in shared memory when they need at most
+// kMaxTileHistSmem bytes.  per_region (region layouts only): one histogram
+// per region, g_cnt nregions*nh and g_fix nregions*2*nh (region r's lo
+// words at 2*r*nh, hi words at 2*r*nh + nh), all zeroed.
 constexpr size_t kMaxTileHistSmem = 160 * 1024;
 size_t pair2_tile_smem_bytes(const PairParams& P, bool weighted);
 void launch_pair2_tile(const DevCatalog& C, const PairParams& P, bool weighted,
                        unsigned long long* g_cnt, unsigned long long* g_fix, double fscale,
-                       unsigned long long* stats, int* work, cudaStream_t s);
+                       unsigned long long* stats, int* work, cudaStream_t s,
+                       bool per_region = false);
 void launch_pair2(const DevCatalog& C, const PairParams& P, bool weighted,
                   unsigned long long* g_cnt, unsigned long long* g_fix, double fscale,
                   unsigned long long* stats, int* work, cudaStream_t s, int variant = kPairWarpCell);
@@ -92,6 +96,15 @@ void launch_adj2(const DevCatalog& C, const PairParams& P, const double* cot2, c
 int launch_adj3(const DevCatalog& C, const CSRView& G, const TriParams& T, const double* cot2,
                  const double* cot3, double gscale, unsigned long long* g_lo,
                  unsigned long long* g_hi, unsigned long long* stats, int* work, cudaStream_t s);
+// The same adjoint with the tile sweep (gr_tile.cu): half stencil, both ends
+// of every edge updated; g_lo / g_hi must be zeroed.  Per-warp 64-bit
+// partials take at most 32 terms each before they are merged, so gscale
+// needs 2^6 of headroom over the largest term: fix_scale(64 * term bound).
+// stats as launch_pair2 (zeroed).
+void launch_adj2_tile(const DevCatalog& C, const PairParams& P, const double* cot2,
+                      const double* cot3, double gscale, unsigned long long* g_lo,
+                      unsigned long long* g_hi, unsigned long long* stats, int* work,
+                      cudaStream_t s);
 void launch_grad_finish(int n, const int* orig, const unsigned long long* g_lo,
                         const unsigned long long* g_hi, double gscale, double* grad,
                         cudaStream_t s);

@@ -83,7 +83,8 @@ std::mutex g_symbol_mutex;
 std::vector<SymbolEntry> g_symbol_cache;
 
 // misc words: [0..2] min keys, [3..5] max keys, [6] max |coord| key,
-// [7] max |w| bits
+// [7] max |w| bits, [8] set when a coordinate or weight is not finite
+// (tested directly: a NaN's key does not reliably survive the reductions)
 __device__ __forceinline__ unsigned long long na_key(double v) {
   unsigned long long b = (unsigned long long)__double_as_longlong(v);
   return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
@@ -100,10 +101,13 @@ __global__ void na_bounds_kernel(const double* __restrict__ xyz, const double* _
   unsigned long long mn[3] = {~0ull, ~0ull, ~0ull}, mx[3] = {0, 0, 0}, ab = 0, wm = 0;
   const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
   if (i0 >= n) return;
+  bool bad = false;
   for (int i = i0; i < n; i += gridDim.x * blockDim.x) {
+    bad = bad || !isfinite(w[i]);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       const double v = xyz[3 * (int64_t)i + d];
+      bad = bad || !isfinite(v);
       const unsigned long long k = na_key(v);
       mn[d] = k < mn[d] ? k : mn[d];
       mx[d] = k > mx[d] ? k : mx[d];
@@ -120,6 +124,7 @@ __global__ void na_bounds_kernel(const double* __restrict__ xyz, const double* _
   }
   atomicMax(&misc[6], ab);
   atomicMax(&misc[7], wm);
+  if (bad) atomicOr(&misc[8], 1ull);
 }
 
 __global__ void na_assign_kernel(const double* __restrict__ xyz, int n, GridGeom g,
@@ -325,9 +330,10 @@ extern "C" int gr_count_2pcf_noalloc(const double* d_xyz, const double* d_w, int
     const int nsm = sm_count();
     if (ni > 0) na_bounds_kernel<<<std::min(nsm, (ni + 255) / 256), 256, 0, s>>>(d_xyz, d_w, ni, misc);
     GR_CHECK_LAUNCH();
-    unsigned long long h[8];
+    unsigned long long h[9];
     GR_CUDA_TRY(cudaMemcpyAsync(h, misc, sizeof(h), cudaMemcpyDeviceToHost, s));
     GR_CUDA_TRY(cudaStreamSynchronize(s));
+    if (h[8] != 0) return GR_E_ARG;  // a coordinate or weight is not finite
     double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
     double coord_max = 0.0, wmax = 0.0;
     if (ni > 0) {

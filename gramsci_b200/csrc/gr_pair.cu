@@ -642,7 +642,6 @@ void launch_pair2(const DevCatalog& C, const PairParams& P, bool weighted,
                   unsigned long long* stats, int* work, cudaStream_t s, int variant) {
   if (C.n <= 0) return;
   if (variant == kPairTile || variant == kPairTile2 || C.grid.sub == 2) {
-    if (!P.f32) throw Error{-1, "the tile pair sweep needs the FP32 path"};
     launch_pair2_tile(C, P, weighted, g_cnt, g_fix, fscale, stats, work, s);
     return;
   }

@@ -22,7 +22,13 @@
 // Histograms are private to each warp in shared memory when they fit (32-bit
 // counts, flushed to the global 64-bit counts before any could overflow, and
 // 128-bit fixed-point sums for weighted catalogues), else updated with
-// global atomics.
+// global atomics.  With per-region output (batched regions) each region has
+// its own histogram: a warp flushes its private copy into the region of its
+// cell whenever that region changes.
+//
+// The FP64 form (precision mode 1) stages the candidates' FP64 positions and
+// tests membership with the reference arithmetic; every hit is binned by the
+// exact FP64 predicate.
 #include "gr_kernels.cuh"
 
 namespace gr {
@@ -31,6 +37,10 @@ namespace {
 
 constexpr int kTileWarps = 8;
 constexpr int kTileThreads = kTileWarps * 32;
+// resident blocks per SM the register allocation is sized for
+#ifndef GR_TILE_MIN_BLOCKS
+#define GR_TILE_MIN_BLOCKS 2
+#endif
 constexpr int kTileQueue = 32 * 32;  // one tile's hits at most
 constexpr float kBufferPush = 1.0e30f;  // added to d2 of a pair of two buffer points
 
@@ -102,23 +112,50 @@ __device__ __forceinline__ bool tile_bins(const DevCatalog& C, const PairParams&
 struct TileWarp {
   float x[32], y[32], z[32], w[32];
   int q[32];
+  uint8_t fq[32], fr[32];  // flags of the tile's candidates and of the chunk's roots
+  double wq[32], wr[32];   // weights of the same (weighted sums and adjoint)
   float4 root[32];
   uint16_t queue[kTileQueue];
   int rb[16], rpre[16];  // candidate ranges of the current chunk: begin, prefix
+  // adjoint: signed 64-bit fixed-point gradient partials of the chunk's
+  // roots and of the tile's candidates (at most 32 terms each before they
+  // are merged into the 128-bit totals after every tile)
+  unsigned long long groot[32], gcand[32];
 };
 
+// Weight adjoint arguments (ADJ mode): cotangents of N2 / N3 (nbins*nmu
+// each, cot3 may be null) and the 128-bit gradient totals in label order.
+struct TileAdj {
+  const double* cot2;
+  const double* cot3;
+  double gscale;
+  unsigned long long* g_lo;
+  unsigned long long* g_hi;
+};
+// FP64 positions of the tile (FP64 form only)
+struct TileWarpD {
+  double x[32], y[32], z[32];
+};
+
+// F32: FP32 membership tests and binning with the guard band (else FP64).
 // WHIST: histograms private to each warp in shared memory (else global).
 // SUB: 1 (cells >= rmax, 5 ranges) or 2 (cells >= rmax/2, 13 ranges).
-template <bool F32, bool WEIGHTED, bool WHIST, int SUB>
-__global__ void __launch_bounds__(kTileThreads, 2)
+// PERREG: one histogram per region (C.cell_region), region r's counts at
+// g_cnt + r*nh and fixed-point words at g_fix + 2*r*nh.
+// ADJ: the 2PCF weight adjoint instead of histograms: each edge adds
+// coef * w_q to dL/dw_p and coef * w_p to dL/dw_q (pair_coef).
+template <bool F32, bool WEIGHTED, bool WHIST, int SUB, bool PERREG, bool ADJ>
+__global__ void __launch_bounds__(kTileThreads, GR_TILE_MIN_BLOCKS)
     pair2_tile_kernel(DevCatalog C, PairParams P, unsigned long long* __restrict__ g_cnt,
                       unsigned long long* __restrict__ g_fix, double fscale,
-                      unsigned long long* __restrict__ stats, int* __restrict__ work) {
+                      unsigned long long* __restrict__ stats, int* __restrict__ work, TileAdj A) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ TileWarp s_tw[kTileWarps];
+  __shared__ TileWarpD s_twd[F32 ? 1 : kTileWarps];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   TileWarp& T = s_tw[wib];
+  TileWarpD& TD = s_twd[F32 ? 0 : wib];
   const int nbm = P.nbins * P.nmu;
   const int nh = nbm * 4;
   // per-warp histograms: counts (32-bit), then fixed-point lo and hi words
@@ -136,22 +173,29 @@ __global__ void __launch_bounds__(kTileThreads, 2)
       }
     }
   }
+  if (ADJ) {
+    T.groot[lane] = 0ull;
+    T.gcand[lane] = 0ull;
+  }
   __syncwarp();
   const int ncell = (int)C.grid.ncell;
   constexpr int NR = SUB == 2 ? 13 : 5;
   unsigned long long rechecks = 0, cands = 0, pairs = 0;
   unsigned int pending = 0;  // edges drained since the last flush (warp-uniform)
+  int region = 0;            // region whose histogram the warp holds (PERREG)
+  unsigned long long* o_cnt = g_cnt;
+  unsigned long long* o_fix = g_fix;
 
   auto flush = [&]() {
     if (!WHIST) return;
     __syncwarp();
     for (int k = lane; k < nh; k += 32) {
       if (w_cnt[k]) {
-        atomicAdd(&g_cnt[k], (unsigned long long)w_cnt[k]);
+        atomicAdd(&o_cnt[k], (unsigned long long)w_cnt[k]);
         w_cnt[k] = 0u;
       }
       if (WEIGHTED && (w_lo[k] | w_hi[k])) {
-        fix_merge(&g_fix[k], &g_fix[nh + k], w_lo[k], w_hi[k]);
+        fix_merge(&o_fix[k], &o_fix[nh + k], w_lo[k], w_hi[k]);
         w_lo[k] = 0ull;
         w_hi[k] = 0ull;
       }
@@ -166,6 +210,15 @@ __global__ void __launch_bounds__(kTileThreads, 2)
     if (cell >= ncell) break;
     const int cb = C.cell_start[cell], ce = C.cell_start[cell + 1];
     if (cb == ce) continue;
+    if (PERREG) {
+      const int r = C.cell_region[cell];
+      if (r != region) {
+        flush();
+        region = r;
+        o_cnt = g_cnt + (size_t)r * nh;
+        o_fix = g_fix + (size_t)r * 2 * nh;
+      }
+    }
     GridParams g;
     const int* cs;
     int lkey;
@@ -199,12 +252,23 @@ __global__ void __launch_bounds__(kTileThreads, 2)
       }
       const int p = c0 + lane;
       const bool act = p < ce;
-      float4 pi = act ? C.pos4[p] : make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
+      // lanes without a root hold a NaN position: no candidate is ever a hit
+      float4 pi = make_float4(__int_as_float(0x7fc00000), 0.f, 0.f, 0.f);
+      double4 pd = make_double4(__longlong_as_double(0x7ff8000000000000ll), 0.0, 0.0, 0.0);
+      if (act) {
+        pi = C.pos4[p];
+        if (!F32) pd = C.posd[p];
+      }
       T.root[lane] = pi;
+      if (act) {
+        T.fr[lane] = C.flags[p];
+        if (WEIGHTED || ADJ) T.wr[lane] = C.w[p];
+      }
       const float pwb = (act && pi.w != 0.0f) ? kBufferPush : 0.0f;
       const float2 npx = make_float2(-pi.x, -pi.x), npy = make_float2(-pi.y, -pi.y),
                    npz = make_float2(-pi.z, -pi.z), pwb2 = make_float2(pwb, pwb);
       const float hi = P.rmax2_hi, lo = P.rmin2_lo;
+      const double pwbd = pwb;
       __syncwarp();
       int kr = 0;  // range of the tile's first candidate (warp-uniform)
       for (int t0 = 0; t0 < total; t0 += 32) {
@@ -222,16 +286,48 @@ __global__ void __launch_bounds__(kTileThreads, 2)
           T.z[lane] = c.z;
           T.w[lane] = c.w;
           T.q[lane] = q;
+          T.fq[lane] = C.flags[q];
+          if (WEIGHTED || ADJ) T.wq[lane] = C.w[q];
+          if (!F32) {
+            const double4 cd = C.posd[q];
+            TD.x[lane] = cd.x;
+            TD.y[lane] = cd.y;
+            TD.z[lane] = cd.z;
+          }
         } else {
           T.x[lane] = __int_as_float(0x7fc00000);  // NaN: never a hit
           T.y[lane] = 0.f;
           T.z[lane] = 0.f;
           T.w[lane] = 0.f;
           T.q[lane] = 0x7fffffff;
+          if (!F32) {
+            TD.x[lane] = __longlong_as_double(0x7ff8000000000000ll);
+            TD.y[lane] = 0.0;
+            TD.z[lane] = 0.0;
+          }
         }
         __syncwarp();
         unsigned m = 0u;
-        if (act) {
+        if (act && !F32) {
+          // the reference's squared separation, separate roundings
+#pragma unroll 8
+          for (int j = 0; j < 32; ++j) {
+            const double dx = __dsub_rn(TD.x[j], pd.x);
+            const double dy = __dsub_rn(TD.y[j], pd.y);
+            const double dz = __dsub_rn(TD.z[j], pd.z);
+            double sd = __dmul_rn(dx, dx);
+            sd = __dadd_rn(sd, __dmul_rn(dy, dy));
+            sd = __dadd_rn(sd, __dmul_rn(dz, dz));
+            sd = __fma_rn((double)T.w[j], pwbd, sd);
+            if (sd <= P.rmax2 && !(P.rmin > 0.0 && sd <= P.rmin2)) m |= 1u << j;
+          }
+          if (t0 == 0) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              if (T.q[j] <= p) m &= ~(1u << j);
+          }
+          cands += (unsigned long long)tn;
+        } else if (act) {
 #pragma unroll
           for (int j = 0; j < 32; j += 2) {
             const float2 cx = *reinterpret_cast<const float2*>(&T.x[j]);
@@ -281,20 +377,30 @@ __global__ void __launch_bounds__(kTileThreads, 2)
             const float4 a = T.root[r];
             const float4 b = make_float4(T.x[j], T.y[j], T.z[j], T.w[j]);
             int bin = 1, mf = 1, mr = 1;
-            if (tile_bins<F32>(C, P, pr, q, a, b, bin, mf, mr, rechecks)) {
-              const uint8_t fp = C.flags[pr], fq = C.flags[q];
+            if (ADJ) {
+              if (tile_bins<F32>(C, P, pr, q, a, b, bin, mf, mr, rechecks)) {
+                const uint8_t fp = T.fr[r], fq = T.fq[j];
+                pairs += (!(fp & FLAG_BUFFER) || !(fq & FLAG_BUFFER)) ? 1 : 0;
+                const double cf = pair_coef(A.cot2, A.cot3, P.nbins, bin, mf, mr, fp, fq);
+                if (cf != 0.0) {
+                  atomicAdd(&T.groot[r], (unsigned long long)__double2ll_rn(cf * T.wq[j] * A.gscale));
+                  atomicAdd(&T.gcand[j], (unsigned long long)__double2ll_rn(cf * T.wr[r] * A.gscale));
+                }
+              }
+            } else if (tile_bins<F32>(C, P, pr, q, a, b, bin, mf, mr, rechecks)) {
+              const uint8_t fp = T.fr[r], fq = T.fq[j];
               const bool root_p = !(fp & FLAG_BUFFER), root_q = !(fq & FLAG_BUFFER);
               const int rp = fp & FLAG_RANDOM, rq = fq & FLAG_RANDOM;
               pairs += (root_p || root_q) ? 1 : 0;
-              const double prod = WEIGHTED ? C.w[pr] * C.w[q] : 0.0;
+              const double prod = WEIGHTED ? T.wr[r] * T.wq[j] : 0.0;
               if (root_p) {
                 const int kh = (bin - 1) + P.nbins * (mf - 1) + nbm * (2 * rp + rq);
                 if (WHIST) {
                   atomicAdd(&w_cnt[kh], 1u);
                   if (WEIGHTED) fix_add(&w_lo[kh], &w_hi[kh], prod, fscale);
                 } else {
-                  atomicAdd(&g_cnt[kh], 1ull);
-                  if (WEIGHTED) fix_add(&g_fix[kh], &g_fix[nh + kh], prod, fscale);
+                  atomicAdd(&o_cnt[kh], 1ull);
+                  if (WEIGHTED) fix_add(&o_fix[kh], &o_fix[nh + kh], prod, fscale);
                 }
               }
               if (root_q) {
@@ -303,12 +409,22 @@ __global__ void __launch_bounds__(kTileThreads, 2)
                   atomicAdd(&w_cnt[kh], 1u);
                   if (WEIGHTED) fix_add(&w_lo[kh], &w_hi[kh], prod, fscale);
                 } else {
-                  atomicAdd(&g_cnt[kh], 1ull);
-                  if (WEIGHTED) fix_add(&g_fix[kh], &g_fix[nh + kh], prod, fscale);
+                  atomicAdd(&o_cnt[kh], 1ull);
+                  if (WEIGHTED) fix_add(&o_fix[kh], &o_fix[nh + kh], prod, fscale);
                 }
               }
             }
           }
+        }
+        if (ADJ) {
+          // merge the tile's gradient partials into the 128-bit totals
+          __syncwarp();
+          const long long vc = (long long)T.gcand[lane];
+          if (vc != 0) fix_add_int(&A.g_lo[T.q[lane]], &A.g_hi[T.q[lane]], vc);
+          T.gcand[lane] = 0ull;
+          const long long vr = (long long)T.groot[lane];
+          if (vr != 0) fix_add_int(&A.g_lo[c0 + lane], &A.g_hi[c0 + lane], vr);
+          T.groot[lane] = 0ull;
         }
         // a 32-bit count grows by at most 2 per binned pair
         pending += (unsigned)tot;
@@ -343,8 +459,9 @@ size_t pair2_tile_smem_bytes(const PairParams& P, bool weighted) {
 
 void launch_pair2_tile(const DevCatalog& C, const PairParams& P, bool weighted,
                        unsigned long long* g_cnt, unsigned long long* g_fix, double fscale,
-                       unsigned long long* stats, int* work, cudaStream_t s) {
+                       unsigned long long* stats, int* work, cudaStream_t s, bool per_region) {
   if (C.n <= 0) return;
+  if (per_region && !C.cell_region) throw Error{-1, "per-region output needs a region layout"};
   size_t smem = pair2_tile_smem_bytes(P, weighted);
   const bool whist = smem <= kMaxTileHistSmem;
   if (!whist) smem = 0;
@@ -352,7 +469,8 @@ void launch_pair2_tile(const DevCatalog& C, const PairParams& P, bool weighted,
   const int sub = C.grid.sub == 2 ? 2 : 1;
 #define GR_TILE_LAUNCH(F, W, H, S)                                                           \
   do {                                                                                        \
-    auto k = pair2_tile_kernel<F, W, H, S>;                                                   \
+    auto k = per_region ? pair2_tile_kernel<F, W, H, S, true, false>                         \
+                        : pair2_tile_kernel<F, W, H, S, false, false>;                        \
     GR_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
                                      (int)smem));                                             \
     int per_sm = 1;                                                                           \
@@ -360,7 +478,8 @@ void launch_pair2_tile(const DevCatalog& C, const PairParams& P, bool weighted,
     int64_t blocks = (int64_t)std::max(1, per_sm) * sm_count();                               \
     const int64_t need = (C.grid.ncell + kTileWarps - 1) / kTileWarps;                        \
     if (blocks > need) blocks = std::max<int64_t>(1, need);                                   \
-    k<<<(unsigned)blocks, kTileThreads, smem, s>>>(C, P, g_cnt, g_fix, fscale, stats, work);  \
+    k<<<(unsigned)blocks, kTileThreads, smem, s>>>(C, P, g_cnt, g_fix, fscale, stats, work,   \
+                                                   TileAdj{});                                \
   } while (0)
 #define GR_TILE_S(F, W, H)                                                                   \
   do {                                                                                        \
@@ -378,6 +497,33 @@ void launch_pair2_tile(const DevCatalog& C, const PairParams& P, bool weighted,
 #undef GR_TILE_H
 #undef GR_TILE_S
 #undef GR_TILE_LAUNCH
+  GR_CHECK_LAUNCH();
+}
+
+void launch_adj2_tile(const DevCatalog& C, const PairParams& P, const double* cot2,
+                      const double* cot3, double gscale, unsigned long long* g_lo,
+                      unsigned long long* g_hi, unsigned long long* stats, int* work,
+                      cudaStream_t s) {
+  if (C.n <= 0) return;
+  GR_CUDA_TRY(cudaMemsetAsync(work, 0, sizeof(int), s));
+  const TileAdj A{cot2, cot3, gscale, g_lo, g_hi};
+  const int sub = C.grid.sub == 2 ? 2 : 1;
+#define GR_ADJT_LAUNCH(F, S)                                                                  \
+  do {                                                                                        \
+    auto k = pair2_tile_kernel<F, true, false, S, false, true>;                               \
+    int per_sm = 1;                                                                           \
+    GR_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTileThreads, 0));  \
+    int64_t blocks = (int64_t)std::max(1, per_sm) * sm_count();                               \
+    const int64_t need = (C.grid.ncell + kTileWarps - 1) / kTileWarps;                        \
+    if (blocks > need) blocks = std::max<int64_t>(1, need);                                   \
+    k<<<(unsigned)blocks, kTileThreads, 0, s>>>(C, P, nullptr, nullptr, 1.0, stats, work, A); \
+  } while (0)
+  if (P.f32) {
+    if (sub == 2) GR_ADJT_LAUNCH(true, 2); else GR_ADJT_LAUNCH(true, 1);
+  } else {
+    if (sub == 2) GR_ADJT_LAUNCH(false, 2); else GR_ADJT_LAUNCH(false, 1);
+  }
+#undef GR_ADJT_LAUNCH
   GR_CHECK_LAUNCH();
 }
 

@@ -72,5 +72,32 @@ module gramsci_cuda
       real(c_double) :: N2(*), N3(*), catsum(*)
       integer(c_int64_t) :: counts(*)
     end function
+    integer(c_int) function gr_set_region_ids(ctx, region_of_point, nregions) &
+        bind(c, name="gr_set_region_ids")
+      import :: c_ptr, c_int, c_int32_t
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), intent(in) :: region_of_point(*)   ! 0-based region of every point
+      integer(c_int32_t), value :: nregions
+    end function
+    integer(c_int) function gr_set_mocks(ctx, nmocks, n_data, n_rand) bind(c, name="gr_set_mocks")
+      import :: c_ptr, c_int, c_int32_t, c_int64_t
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: nmocks
+      integer(c_int64_t), intent(in) :: n_data(*), n_rand(*)
+    end function
+    integer(c_int) function gr_count_2pcf_regions(ctx, N2, N3, counts, catsum) &
+        bind(c, name="gr_count_2pcf_regions")
+      import :: c_ptr, c_int, c_double, c_int64_t
+      type(c_ptr), value :: ctx
+      real(c_double) :: N2(*), N3(*), catsum(*)   ! (nbins, nmu, nregions) ...
+      integer(c_int64_t) :: counts(*)
+    end function
+    integer(c_int) function gr_count_3pcf_batched(ctx, N2, N3, counts, catsum) &
+        bind(c, name="gr_count_3pcf_batched")
+      import :: c_ptr, c_int, c_double, c_int64_t
+      type(c_ptr), value :: ctx
+      real(c_double) :: N2(*), N3(*), catsum(*)
+      integer(c_int64_t) :: counts(*)
+    end function
   end interface
 end module gramsci_cuda

@@ -53,8 +53,7 @@ typedef struct gr_ctx gr_ctx;
                                (0 warp per cell, 1/2 block per cell of 128/256, 3 warp per
                                cell with queued binning, 4/5 block per cell of 128/256 with
                                queued binning, 6 the tile sweep, 7 the tile sweep on cells
-                               of rmax/2; 6 and 7 need the FP32 path and fall back to 0
-                               without it) */
+                               of rmax/2) */
 #define GR_OPT_KEEP_GRAPH 4 /* 0 (default): every count call builds the index and graph;
                                1: keep the graph of the last call and reuse it until the
                                catalogue, the bins or the precision change */
@@ -202,6 +201,40 @@ int gr_graph_load(gr_ctx* ctx, const char* path);
  * is a buffer point), e.g. to run the regions one launch at a time. */
 int gr_set_regions(gr_ctx* ctx, int32_t nsplit);
 int gr_count_2pcf_batched(gr_ctx* ctx, double* N2, double* N3, int64_t* counts, double* catsum);
+
+/* Regions from a region id per point (jackknife regions, or any domain
+ * decomposition the caller made): region_of_point has one entry in
+ * [0, nregions) per catalogue point (host memory).  Region r's halo is the
+ * bounding box of its points grown by rmax (strict bounds), as in
+ * src/domain_decomposition.f90:39-80; points of other regions inside it are
+ * its buffer points.  Replaces the subcube split until gr_set_regions is
+ * called; gr_set_catalog clears it (the ids belong to the catalogue). */
+int gr_set_region_ids(gr_ctx* ctx, const int32_t* region_of_point, int32_t nregions);
+
+/* Independent catalogues (mocks) in one launch.  The catalogue given to
+ * gr_set_catalog is the mocks one after another, each with its galaxies
+ * first: mock m has n_data[m] galaxies then n_rand[m] randoms, with signed
+ * weights normalised within the mock (the reference's normalisation, one
+ * mock at a time; the catalogue's own n_data / n_rand split is not used).
+ * Each mock is a region without halo: pairs never join two mocks.  The
+ * batched calls then count every mock in one launch; gr_count_2pcf_regions
+ * gives each mock's histograms.  Cleared by gr_set_catalog. */
+int gr_set_mocks(gr_ctx* ctx, int32_t nmocks, const int64_t* n_data, const int64_t* n_rand);
+
+/* 2PCF of every region (or mock) separately, in one launch: the histograms
+ * each region's own run of the reference would write (its own points as
+ * roots, its buffer points as neighbours only).  Shapes as gr_count_2pcf
+ * with a last axis over the regions: N2, N3 (nbins, nmu, nregions), counts
+ * and catsum (nbins, nmu, 4, nregions).  Their sum over the regions is
+ * gr_count_2pcf_batched's result. */
+int gr_count_2pcf_regions(gr_ctx* ctx, double* N2, double* N3, int64_t* counts, double* catsum);
+
+/* 3PCF over all regions (or mocks) in one pass: the neighbour graph of every
+ * region's members built in one launch, every triangle rooted at each of
+ * its vertices that is a region's own point.  Outputs as gr_count_3pcf
+ * (summed over the regions; equal to gr_count_3pcf on the whole catalogue
+ * for a split into regions, the sum of the mocks' results for mocks). */
+int gr_count_3pcf_batched(gr_ctx* ctx, double* N2, double* N3, int64_t* counts, double* catsum);
 int gr_regions_info(gr_ctx* ctx, int32_t* nregions, int64_t* nmembers);
 int gr_regions_export(gr_ctx* ctx, int64_t* member_off, int32_t* member_orig,
                       int32_t* member_buffer);

@@ -115,3 +115,32 @@ def test_rows_longer_than_shared_capacity(oracle):
         ref = G.pcf3(w, n_data, buffer=buf)
     assert st["upper_edges"] > 0 and max(np.diff(G.csr()[0])) > 256
     _same(got, ref)
+
+
+@pytest.mark.parametrize("what", ["nan_coordinate", "inf_coordinate", "nan_weight", "inf_weight"])
+def test_non_finite_inputs_are_refused(what):
+    """A non-finite coordinate is refused by the count (the index build tests
+    every coordinate); a non-finite weight by gr_set_catalog.  After the
+    refusal the context counts a good catalogue as before."""
+    from gramsci_b200 import _native, api, catalogs
+
+    rng = np.random.default_rng(8)
+    xyz = rng.uniform(0.0, 100.0, (300, 3))
+    w = catalogs.normalise(np.ones(300), 150, 150)
+    bad_xyz, bad_w = xyz.copy(), w.copy()
+    if what == "nan_coordinate":
+        bad_xyz[40, 2] = np.nan
+    elif what == "inf_coordinate":
+        bad_xyz[200, 0] = -np.inf
+    elif what == "nan_weight":
+        bad_w[10] = np.nan
+    else:
+        bad_w[250] = np.inf
+    with api.Context(0) as ctx:
+        ctx.set_bins(1.0, 12.0, 4, 2)
+        with pytest.raises(_native.GramsciError) as e:
+            ctx.set_catalog(bad_xyz, bad_w, 150)
+            ctx.count_2pcf()
+        assert e.value.code == _native.GR_E_ARG
+        ctx.set_catalog(xyz, w, 150)
+        assert int(ctx.count_2pcf()["counts"].sum()) > 0
