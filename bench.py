@@ -620,13 +620,14 @@ def sub_quad(args, stream, flush):
     wl = catalogs.normalise(rng.lognormal(0.0, 0.3, cat.n), cat.n_data, cat.n_rand)
     ctx.set_catalog(xyz_d, torch.from_numpy(wl).cuda(), cat.n_data)
     fwd, adj = [], []
-    gotw = None
     for k in range(4):
-        gotw = ctx.count_4pcf()
+        # N2, N3, discN, discR as the reference computes them (no counts)
+        r = ctx.count_4pcf(counts=False)
         fwd.append(ctx.stats()["ms_query"])
-        cot = [rng.normal(size=gotw[x].shape) for x in ("N2", "N3", "discN", "discR")]
+        cot = [rng.normal(size=r[x].shape) for x in ("N2", "N3", "discN", "discR")]
         ctx.adjoint_4pcf(*cot)
         adj.append(ctx.stats()["ms_query"])
+    gotw = ctx.count_4pcf()  # with the counts, for the parity record
     ctx.close()
     rec = {"workload": f"{name}: Neyman-Scott 4PCF, {cat.n_data} galaxies + {cat.n_rand} randoms, "
                        f"box {cat.meta['box']:.0f}, rmin {sp['rmin']}, rmax {sp['rmax']}, "

@@ -169,22 +169,29 @@ class Context:
             out["counts"] = _fortran(cnt, nc, nm, 4)
         return out
 
-    def count_4pcf(self):
+    def count_4pcf(self, counts=True):
+        """N2, N3 (ncfg, nbins, nbins), discN, discR (ncfg, nbins, nbins, 6)
+        and the category sums; with counts=False the integer counts (not
+        part of the reference's output) are not kept, which spares the
+        weighted kernel one reduction per update."""
         nb = self.nbins
         nc = ncfg4(nb)
         nbin = nc * nb * nb
         N2, N3 = np.zeros(nbin), np.zeros(nbin)
         dN, dR = np.zeros(nbin * 6), np.zeros(nbin * 6)
-        counts = np.zeros(nbin * 5, np.int64)
+        cnt = np.zeros(nbin * 5, np.int64) if counts else None
         catsum = np.zeros(nbin * 5)
-        dcount = np.zeros(nbin * 24, np.int64)
+        dcount = np.zeros(nbin * 24, np.int64) if counts else None
         dsum = np.zeros(nbin * 24)
         self._check(self._lib.gr_count_4pcf(self._h, _ptr(N2), _ptr(N3), _ptr(dN), _ptr(dR),
-                                            _ptr(counts), _ptr(catsum), _ptr(dcount), _ptr(dsum)))
-        return dict(N2=_fortran(N2, nc, nb, nb), N3=_fortran(N3, nc, nb, nb),
-                    discN=_fortran(dN, nc, nb, nb, 6), discR=_fortran(dR, nc, nb, nb, 6),
-                    counts=_fortran(counts, nc, nb, nb, 5), catsum=_fortran(catsum, nc, nb, nb, 5),
-                    dcount=_fortran(dcount, nc, nb, nb, 6, 4), dsum=_fortran(dsum, nc, nb, nb, 6, 4))
+                                            _ptr(cnt), _ptr(catsum), _ptr(dcount), _ptr(dsum)))
+        out = dict(N2=_fortran(N2, nc, nb, nb), N3=_fortran(N3, nc, nb, nb),
+                   discN=_fortran(dN, nc, nb, nb, 6), discR=_fortran(dR, nc, nb, nb, 6),
+                   catsum=_fortran(catsum, nc, nb, nb, 5), dsum=_fortran(dsum, nc, nb, nb, 6, 4))
+        if counts:
+            out["counts"] = _fortran(cnt, nc, nb, nb, 5)
+            out["dcount"] = _fortran(dcount, nc, nb, nb, 6, 4)
+        return out
 
     # -- batched regions -------------------------------------------------
     def set_regions(self, nsplit):

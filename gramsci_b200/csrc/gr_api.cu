@@ -988,6 +988,10 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   Q.nbins = nb;
   Q.ncfg = ncfg;
   Q.tetra = tetra ? 1 : 0;
+  // integer counts are not part of the reference's output: kept when the
+  // caller asks for them (and always for unit weights, whose sums are
+  // count x product)
+  Q.counts = (!weighted || counts || dcount) ? 1 : 0;
   Q.cap = round_cap((int64_t)gst[2], 32, 1024);
   make_rank_tables(Q.rank, nb, 4);
   Q.P = c->P;
@@ -1964,21 +1968,30 @@ int gr_regions_export(gr_ctx* c, int64_t* member_off, int32_t* member_orig, int3
   GR_API_BEGIN(c)
   RegionLayout& L = c->regions;
   if (!L.valid) return set_err(c, GR_E_ARG, "no region layout (call gr_count_2pcf_batched)");
+  // the laid-out members (the last batched call's layout): region r owns
+  // the cells [cell_off[r], cell_off[r] + its cell count), its members the
+  // labels of those cells
   cudaStream_t s = c->own;
   const int64_t M = L.n_members;
-  std::vector<int> mo(M);
+  std::vector<int> mo(M), cs(L.ncell + 1);
   std::vector<uint8_t> mf(M);
   if (M > 0) {
-    GR_CUDA_TRY(cudaMemcpyAsync(mo.data(), L.m_orig.p, sizeof(int) * M, cudaMemcpyDeviceToHost, s));
-    GR_CUDA_TRY(cudaMemcpyAsync(mf.data(), L.m_flag.p, M, cudaMemcpyDeviceToHost, s));
+    GR_CUDA_TRY(cudaMemcpyAsync(mo.data(), L.orig.p, sizeof(int) * M, cudaMemcpyDeviceToHost, s));
+    GR_CUDA_TRY(cudaMemcpyAsync(mf.data(), L.flags.p, M, cudaMemcpyDeviceToHost, s));
   }
+  GR_CUDA_TRY(cudaMemcpyAsync(cs.data(), L.cell_start.p, sizeof(int) * (L.ncell + 1),
+                              cudaMemcpyDeviceToHost, s));
   GR_CUDA_TRY(cudaStreamSynchronize(s));
   // members of each region, ordered by catalogue index
   for (int r = 0; r < L.nreg; ++r) {
     const int64_t b = L.h_mem_off[r], e = L.h_mem_off[r + 1];
+    const int c0 = L.h_cell_off[r];
+    const int c1 = c0 + (int)L.h_grid[r].ncell;
+    const int lb = cs[c0], le = cs[c1];
+    if ((int64_t)(le - lb) != e - b) return set_err(c, GR_E_CUDA, "region layout is inconsistent");
     std::vector<std::pair<int, int>> v;
     v.reserve(e - b);
-    for (int64_t k = b; k < e; ++k) v.push_back({mo[k], (mf[k] & FLAG_BUFFER) ? 1 : 0});
+    for (int k = lb; k < le; ++k) v.push_back({mo[k], (mf[k] & FLAG_BUFFER) ? 1 : 0});
     std::sort(v.begin(), v.end());
     for (int64_t k = b; k < e; ++k) {
       if (member_orig) member_orig[k] = v[k - b].first;

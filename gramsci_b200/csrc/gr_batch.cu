@@ -98,66 +98,8 @@ __global__ void b_init_box_kernel(unsigned long long* box, int nreg) {
     box[k] = (k % 6) < 3 ? ~0ull : 0ull;
 }
 
-struct RegionGeomDev {
-  const double* halo;    // 6 per region: lo xyz, hi xyz (strict bounds)
-  const double* glo;     // 3 per region: grid origin
-  const double* ginv;    // 3 per region: inverse cell size
-  const GridParams* grid;
-  const int* cell_off;   // nreg + 1
-  const int* mem_off;    // nreg + 1
-  int ns;
-};
-
 __device__ __forceinline__ bool in_halo(const double* h, double x, double y, double z) {
   return x > h[0] && x < h[3] && y > h[1] && y < h[4] && z > h[2] && z < h[5];
-}
-
-// Visit the regions whose halo contains point i (its own subcube and the 26
-// around it; a halo reaches at most Rmax beyond its box, and a region's box
-// lies inside its subcube, so farther subcubes cannot qualify when the
-// subcubes are at least Rmax wide -- the host checks that).
-template <bool FILL>
-__global__ void b_member_kernel(const double* __restrict__ xyz, int n, int n_data,
-                                const int* __restrict__ sub, RegionGeomDev G,
-                                int* __restrict__ count, int* __restrict__ m_orig,
-                                uint8_t* __restrict__ m_flag, int* __restrict__ m_key,
-                                int* __restrict__ m_slot, int* __restrict__ cell_count) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const double x = xyz[3 * (int64_t)i], y = xyz[3 * (int64_t)i + 1], z = xyz[3 * (int64_t)i + 2];
-    const int own = sub[i];
-    const int sx = own % G.ns, sy = (own / G.ns) % G.ns, sz = own / (G.ns * G.ns);
-    for (int dz = -1; dz <= 1; ++dz) {
-      const int tz = sz + dz;
-      if (tz < 0 || tz >= G.ns) continue;
-      for (int dy = -1; dy <= 1; ++dy) {
-        const int ty = sy + dy;
-        if (ty < 0 || ty >= G.ns) continue;
-        for (int dx = -1; dx <= 1; ++dx) {
-          const int tx = sx + dx;
-          if (tx < 0 || tx >= G.ns) continue;
-          const int r = (tz * G.ns + ty) * G.ns + tx;
-          if (!in_halo(G.halo + 6 * r, x, y, z)) continue;
-          const int slot = atomicAdd(&count[r], 1);
-          if (!FILL) continue;
-          const int m = G.mem_off[r] + slot;
-          m_orig[m] = i;
-          m_flag[m] = (uint8_t)((r != own ? FLAG_BUFFER : 0) | (i >= n_data ? FLAG_RANDOM : 0));
-          const GridParams g = G.grid[r];
-          int c[3];
-          const double v[3] = {x, y, z};
-#pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            int q = (int)floor((v[d] - G.glo[3 * r + d]) * G.ginv[3 * r + d]);
-            const int nc = d == 0 ? g.nx : (d == 1 ? g.ny : g.nz);
-            c[d] = q < 0 ? 0 : (q >= nc ? nc - 1 : q);
-          }
-          const int key = G.cell_off[r] + (c[2] * g.ny + c[1]) * g.nx + c[0];
-          m_key[m] = key;
-          m_slot[m] = atomicAdd(&cell_count[key], 1);
-        }
-      }
-    }
-  }
 }
 
 // Region boxes and sizes from a given region id per point.
@@ -178,61 +120,98 @@ __global__ void b_region_box_ids_kernel(const double* __restrict__ xyz, int n,
   }
 }
 
-// Region r gains point i as a member (its own point, or a buffer copy).
-template <bool FILL>
-__device__ __forceinline__ void b_add_member(int r, int i, uint8_t fl, double x, double y, double z,
-                                             const RegionGeomDev& G, int* count, int* m_orig,
-                                             uint8_t* m_flag, int* m_key, int* m_slot,
-                                             int* cell_count) {
-  const int slot = atomicAdd(&count[r], 1);
-  if (!FILL) return;
-  const int m = G.mem_off[r] + slot;
-  m_orig[m] = i;
-  m_flag[m] = fl;
-  const GridParams g = G.grid[r];
+// Memberships of point i, f(region, buffer): every point belongs to its own
+// region, and in the halo layouts to every other region whose halo
+// contains it, as a buffer point.  Subcube split: the own subcube and the 26
+// around it (a halo reaches at most Rmax beyond its box, and a region's box
+// lies inside its subcube, so farther subcubes cannot qualify when the
+// subcubes are at least Rmax wide -- the host checks that).  Region ids: the
+// regions the coarse grid lists for the point's coarse cell.  Mocks: the own
+// region only (no halos).
+enum : int { kMemSplit = 0, kMemIds = 1, kMemMocks = 2 };
+
+template <int MODE, class F>
+__device__ __forceinline__ void for_each_membership(double x, double y, double z, int own,
+                                                    const RegionGeomDev& G, const CoarseDev& CG,
+                                                    F f) {
+  if (MODE == kMemSplit) {
+    const int sx = own % G.ns, sy = (own / G.ns) % G.ns, sz = own / (G.ns * G.ns);
+    for (int dz = -1; dz <= 1; ++dz) {
+      const int tz = sz + dz;
+      if (tz < 0 || tz >= G.ns) continue;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int ty = sy + dy;
+        if (ty < 0 || ty >= G.ns) continue;
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int tx = sx + dx;
+          if (tx < 0 || tx >= G.ns) continue;
+          const int r = (tz * G.ns + ty) * G.ns + tx;
+          if (in_halo(G.halo + 6 * r, x, y, z)) f(r, r != own);
+        }
+      }
+    }
+    return;
+  }
+  f(own, false);
+  if (MODE == kMemMocks) return;
   const double v[3] = {x, y, z};
   int c[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    const int q = (int)floor((v[d] - G.glo[3 * r + d]) * G.ginv[3 * r + d]);
-    const int nc = d == 0 ? g.nx : (d == 1 ? g.ny : g.nz);
-    c[d] = q < 0 ? 0 : (q >= nc ? nc - 1 : q);
+    const int q = (int)floor((v[d] - CG.lo[d]) * CG.inv[d]);
+    c[d] = q < 0 ? 0 : (q >= CG.nc[d] ? CG.nc[d] - 1 : q);
   }
-  const int key = G.cell_off[r] + (c[2] * g.ny + c[1]) * g.nx + c[0];
-  m_key[m] = key;
-  m_slot[m] = atomicAdd(&cell_count[key], 1);
+  const int cc = (c[2] * CG.nc[1] + c[1]) * CG.nc[0] + c[0];
+  for (int k = CG.off[cc]; k < CG.off[cc + 1]; ++k) {
+    const int r = CG.list[k];
+    if (r != own && in_halo(G.halo + 6 * r, x, y, z)) f(r, true);
+  }
 }
 
-// Members from a region id per point: every point joins its own region, and
-// (with a coarse grid) every other region whose halo contains it, as a
-// buffer point.  Without a coarse grid (mocks) regions have no halo.
-// Random flags from pflag when given, else from the galaxy/random split.
-template <bool FILL>
-__global__ void b_member_ids_kernel(const double* __restrict__ xyz, int n, int n_data,
-                                    const int* __restrict__ reg, const uint8_t* __restrict__ pflag,
-                                    RegionGeomDev G, CoarseDev CG, int* __restrict__ count,
-                                    int* __restrict__ m_orig, uint8_t* __restrict__ m_flag,
-                                    int* __restrict__ m_key, int* __restrict__ m_slot,
-                                    int* __restrict__ cell_count) {
+// Region members.  PASS 0 (planning): members per region (count).  PASS 1:
+// memberships per point (mcount).  PASS 2: the memberships of point i
+// written at moff[i] onward (an exclusive scan of PASS 1): catalogue index,
+// flags, cell key in the region's grid and slot in that cell.  Only the
+// per-cell slots use atomics (many cells, little contention); the members of
+// a region need no common counter.  Random flags from pflag when given,
+// else from the galaxy / random split.
+template <int PASS, int MODE>
+__global__ void b_members_kernel(const double* __restrict__ xyz, int n, int n_data,
+                                 const int* __restrict__ reg, const uint8_t* __restrict__ pflag,
+                                 RegionGeomDev G, CoarseDev CG, int* __restrict__ count,
+                                 int* __restrict__ mcount, const int64_t* __restrict__ moff,
+                                 int* __restrict__ m_orig, uint8_t* __restrict__ m_flag,
+                                 int* __restrict__ m_key, int* __restrict__ m_slot,
+                                 int* __restrict__ cell_count) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const double x = xyz[3 * (int64_t)i], y = xyz[3 * (int64_t)i + 1], z = xyz[3 * (int64_t)i + 2];
     const int own = reg[i];
     const uint8_t rnd = pflag ? (uint8_t)(pflag[i] & FLAG_RANDOM) : (uint8_t)(i >= n_data ? FLAG_RANDOM : 0);
-    b_add_member<FILL>(own, i, rnd, x, y, z, G, count, m_orig, m_flag, m_key, m_slot, cell_count);
-    if (!CG.list) continue;
-    const double v[3] = {x, y, z};
-    int c[3];
+    if (PASS == 0) {
+      for_each_membership<MODE>(x, y, z, own, G, CG, [&](int r, bool) { atomicAdd(&count[r], 1); });
+    } else if (PASS == 1) {
+      int c = 0;
+      for_each_membership<MODE>(x, y, z, own, G, CG, [&](int, bool) { ++c; });
+      mcount[i] = c;
+    } else {
+      int64_t m = moff[i];
+      for_each_membership<MODE>(x, y, z, own, G, CG, [&](int r, bool buf) {
+        m_orig[m] = i;
+        m_flag[m] = (uint8_t)(rnd | (buf ? FLAG_BUFFER : 0));
+        const GridParams g = G.grid[r];
+        const double v[3] = {x, y, z};
+        int c[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const int q = (int)floor((v[d] - CG.lo[d]) * CG.inv[d]);
-      c[d] = q < 0 ? 0 : (q >= CG.nc[d] ? CG.nc[d] - 1 : q);
-    }
-    const int cc = (c[2] * CG.nc[1] + c[1]) * CG.nc[0] + c[0];
-    for (int k = CG.off[cc]; k < CG.off[cc + 1]; ++k) {
-      const int r = CG.list[k];
-      if (r == own || !in_halo(G.halo + 6 * r, x, y, z)) continue;
-      b_add_member<FILL>(r, i, (uint8_t)(rnd | FLAG_BUFFER), x, y, z, G, count, m_orig, m_flag,
-                         m_key, m_slot, cell_count);
+        for (int d = 0; d < 3; ++d) {
+          const int q = (int)floor((v[d] - G.glo[3 * r + d]) * G.ginv[3 * r + d]);
+          const int nc = d == 0 ? g.nx : (d == 1 ? g.ny : g.nz);
+          c[d] = q < 0 ? 0 : (q >= nc ? nc - 1 : q);
+        }
+        const int key = G.cell_off[r] + (c[2] * g.ny + c[1]) * g.nx + c[0];
+        m_key[m] = key;
+        m_slot[m] = atomicAdd(&cell_count[key], 1);
+        ++m;
+      });
     }
   }
 }
@@ -445,16 +424,7 @@ void RegionLayout::plan(const double* d_xyz, int64_t n_pts, int64_t n_data_pts, 
   RegionGeomDev G{};
   G.halo = halo.p;
   G.ns = ns;
-  if (n > 0) {
-    if (mode == kRegionsSplit)
-      b_member_kernel<false><<<nblocks(n, 256), 256, 0, s>>>(d_xyz, (int)n, (int)n_data, sub.p, G,
-                                                             count.p, nullptr, nullptr, nullptr,
-                                                             nullptr, nullptr);
-    else
-      b_member_ids_kernel<false><<<nblocks(n, 256), 256, 0, s>>>(
-          d_xyz, (int)n, (int)n_data, sub.p, nullptr, G, coarse_dev(), count.p, nullptr, nullptr,
-          nullptr, nullptr, nullptr);
-  }
+  if (n > 0) launch_members(0, d_xyz, G, s);
   GR_CHECK_LAUNCH();
   h_count.assign(nreg, 0);
   GR_CUDA_TRY(cudaMemcpyAsync(h_count.data(), count.p, sizeof(int) * nreg, cudaMemcpyDeviceToHost, s));
@@ -523,20 +493,18 @@ void RegionLayout::plan(const double* d_xyz, int64_t n_pts, int64_t n_data_pts, 
   ginv.reserve(3 * (size_t)nreg);
   grid.reserve(nreg);
   cell_off.reserve(nreg + 1);
-  mem_off.reserve(nreg + 1);
   cell_region.reserve(ncell + 1);
-  std::vector<int> mo(nreg + 1);
-  for (int r = 0; r <= nreg; ++r) mo[r] = (int)h_mem_off[r];
   GR_CUDA_TRY(cudaMemcpyAsync(glo.p, h_glo.data(), sizeof(double) * 3 * nreg, cudaMemcpyHostToDevice, s));
   GR_CUDA_TRY(cudaMemcpyAsync(ginv.p, h_ginv.data(), sizeof(double) * 3 * nreg, cudaMemcpyHostToDevice, s));
   GR_CUDA_TRY(cudaMemcpyAsync(grid.p, h_grid.data(), sizeof(GridParams) * nreg, cudaMemcpyHostToDevice, s));
   GR_CUDA_TRY(cudaMemcpyAsync(cell_off.p, h_cell_off.data(), sizeof(int) * (nreg + 1), cudaMemcpyHostToDevice, s));
-  GR_CUDA_TRY(cudaMemcpyAsync(mem_off.p, mo.data(), sizeof(int) * (nreg + 1), cudaMemcpyHostToDevice, s));
   if (ncell > 0)
     GR_CUDA_TRY(cudaMemcpyAsync(cell_region.p, cell_region_h.data(), sizeof(int) * ncell,
                                 cudaMemcpyHostToDevice, s));
   // member and layout buffers
   const int64_t M = n_members;
+  mcount.reserve(n + 1);
+  moff.reserve(n + 1);
   m_orig.reserve(M + 1);
   m_flag.reserve(M + 1);
   m_key.reserve(M + 1);
@@ -564,19 +532,13 @@ void RegionLayout::enqueue_layout(const double* d_xyz, const double* d_w, cudaSt
   G.ginv = ginv.p;
   G.grid = grid.p;
   G.cell_off = cell_off.p;
-  G.mem_off = mem_off.p;
   G.ns = ns;
-  GR_CUDA_TRY(cudaMemsetAsync(count.p, 0, sizeof(int) * nreg, s));
   GR_CUDA_TRY(cudaMemsetAsync(cell_count.p, 0, sizeof(int) * (ncell + 1), s));
   if (n > 0) {
-    if (mode == kRegionsSplit)
-      b_member_kernel<true><<<nblocks(n, 256), 256, 0, s>>>(d_xyz, (int)n, (int)n_data, sub.p, G,
-                                                            count.p, m_orig.p, m_flag.p, m_key.p,
-                                                            m_slot.p, cell_count.p);
-    else
-      b_member_ids_kernel<true><<<nblocks(n, 256), 256, 0, s>>>(
-          d_xyz, (int)n, (int)n_data, sub.p, mode == kRegionsMocks ? pflag.p : nullptr, G,
-          coarse_dev(), count.p, m_orig.p, m_flag.p, m_key.p, m_slot.p, cell_count.p);
+    // memberships per point, their offsets, then the members themselves
+    launch_members(1, d_xyz, G, s);
+    scan_i32_to_i64(mcount.p, moff.p, n, s, scan_tmp);
+    launch_members(2, d_xyz, G, s);
   }
   GR_CHECK_LAUNCH();
   scan_i32_to_i64(cell_count.p, cell_start64.p, ncell, s, scan_tmp);
@@ -590,6 +552,29 @@ void RegionLayout::enqueue_layout(const double* d_xyz, const double* d_w, cudaSt
                                                             w.p, orig.p, flags.p, cell_key.p);
   }
   b_narrow_kernel<<<nblocks(ncell + 1, 256), 256, 0, s>>>(cell_start64.p, cell_start.p, ncell + 1);
+  GR_CHECK_LAUNCH();
+}
+
+void RegionLayout::launch_members(int pass, const double* d_xyz, const RegionGeomDev& G,
+                                  cudaStream_t s) {
+  const CoarseDev CG = coarse_dev();
+  const uint8_t* pf = mode == kRegionsMocks ? pflag.p : nullptr;
+  const int blocks = nblocks(n, 256);
+#define GR_MEM_LAUNCH(P, M)                                                                     \
+  b_members_kernel<P, M><<<blocks, 256, 0, s>>>(d_xyz, (int)n, (int)n_data, sub.p, pf, G, CG,    \
+                                                count.p, mcount.p, moff.p, m_orig.p, m_flag.p,   \
+                                                m_key.p, m_slot.p, cell_count.p)
+#define GR_MEM_MODE(P)                                                                          \
+  do {                                                                                          \
+    if (mode == kRegionsSplit) GR_MEM_LAUNCH(P, kMemSplit);                                     \
+    else if (mode == kRegionsIds) GR_MEM_LAUNCH(P, kMemIds);                                    \
+    else GR_MEM_LAUNCH(P, kMemMocks);                                                           \
+  } while (0)
+  if (pass == 0) GR_MEM_MODE(0);
+  else if (pass == 1) GR_MEM_MODE(1);
+  else GR_MEM_MODE(2);
+#undef GR_MEM_MODE
+#undef GR_MEM_LAUNCH
   GR_CHECK_LAUNCH();
 }
 

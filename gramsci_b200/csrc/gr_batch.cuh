@@ -17,6 +17,16 @@ struct CoarseDev {
   int nc[3];
 };
 
+// Region geometry read by the membership kernels.
+struct RegionGeomDev {
+  const double* halo;    // 6 per region: lo xyz, hi xyz (strict bounds)
+  const double* glo;     // 3 per region: grid origin
+  const double* ginv;    // 3 per region: inverse cell size
+  const GridParams* grid;
+  const int* cell_off;   // nreg + 1
+  int ns;                // subcubes per axis (subcube split)
+};
+
 // How the catalogue is split into regions.
 enum : int {
   kRegionsSplit = 0,  // nsplit^3 equal subcubes of the bounding box, Rmax halos
@@ -45,7 +55,9 @@ struct RegionLayout {
   DevBuf<int> coarse_off, coarse_list;
   // device geometry
   DevBuf<unsigned long long> box_raw;
-  DevBuf<int> own_count, count, sub, cell_off, mem_off, cell_region;
+  DevBuf<int> own_count, count, sub, cell_off, cell_region;
+  DevBuf<int> mcount;      // memberships of every point
+  DevBuf<int64_t> moff;    // their exclusive scan (where each point's members go)
   DevBuf<double> halo, glo, ginv;
   DevBuf<GridParams> grid;
   // members and layout
@@ -80,6 +92,9 @@ struct RegionLayout {
   void enqueue_layout(const double* d_xyz, const double* d_w, cudaStream_t s);
   DevCatalog view() const;
   CoarseDev coarse_dev() const;
+  // membership kernels (pass 0: members per region, 1: memberships per
+  // point, 2: the members)
+  void launch_members(int pass, const double* d_xyz, const RegionGeomDev& G, cudaStream_t s);
 };
 
 }  // namespace gr

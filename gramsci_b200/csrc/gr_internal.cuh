@@ -140,17 +140,21 @@ __device__ __forceinline__ bool edge_f64(const double4 pi, const double4 pj, con
 // FP32 classification.  Returns 0: certainly not an edge; 1: edge with the
 // bins written; 2: inside the guard band, re-evaluate with edge_f64.
 // NEED_BINS=false only decides membership (guards only at rmin and rmax).
+// The separation is d2 * rsqrtf(d2) and the cosine and its error bound use
+// __fdividef: make_pair_params sizes the guard band for these approximate
+// operations (d0 and eC), so outside the band the bins equal the FP64 ones.
 template <bool NEED_BINS>
 __device__ __forceinline__ int classify_f32(const float4 pi, const float4 pj, const PairParams& P,
                                             int& bin, int& muf, int& mur) {
-  float dx = pj.x - pi.x;
-  float dy = pj.y - pi.y;
-  float dz = pj.z - pi.z;
-  float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+  const float dx = pj.x - pi.x;
+  const float dy = pj.y - pi.y;
+  const float dz = pj.z - pi.z;
+  const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
   if (d2 >= P.rmax2_hi || d2 <= P.rmin2_lo) return 0;
-  float d = __fsqrt_rn(d2);
-  float t = (d - P.f_rmin) * P.f_inv_dr;
-  float tn = rintf(t);
+  // d2 = 0 (coincident points, rmin = 0): t = -rmin/dr, decided in FP64
+  const float d = d2 > 0.0f ? d2 * rsqrtf(d2) : 0.0f;
+  const float t = (d - P.f_rmin) * P.f_inv_dr;
+  const float tn = rintf(t);
   if (NEED_BINS) {
     if (fabsf(t - tn) < P.tguard) return 2;
   } else {
@@ -160,24 +164,26 @@ __device__ __forceinline__ int classify_f32(const float4 pi, const float4 pj, co
   if (!NEED_BINS) return 1;
   bin = (int)t + 1;
   if (P.rsd) {
-    float dd = d - P.d0;
-    float mx = 0.5f * (pi.x + pj.x);
-    float my = 0.5f * (pi.y + pj.y);
-    float mz = 0.5f * (pi.z + pj.z);
-    float mm = __fsqrt_rn(fmaf(mz, mz, fmaf(my, my, mx * mx)));
-    float mmm = mm - P.mB;
-    if (dd <= 0.0f || mmm <= 0.0f) return 2;
-    float dot = fmaf(mz, -dz, fmaf(my, -dy, mx * -dx));
-    float th = dot / (mm * d);
-    float eth = P.eA / dd + P.eB / mmm + P.eC;
-    float ug = eth * P.f_mu_scale + 8.0f * 5.96046448e-8f * P.f_nmu;
-    float u1 = (th + 1.0f) * P.f_mu_scale;
-    float u2 = (1.0f - th) * P.f_mu_scale;
-    float k1 = rintf(u1), k2 = rintf(u2);
+    const float dd = d - P.d0;
+    const float mx = 0.5f * (pi.x + pj.x);
+    const float my = 0.5f * (pi.y + pj.y);
+    const float mz = 0.5f * (pi.z + pj.z);
+    const float m2 = fmaf(mz, mz, fmaf(my, my, mx * mx));
+    const float mm = m2 * rsqrtf(m2);
+    const float mmm = mm - P.mB;
+    // __fdividef needs denominators of at least 2^-126
+    if (!(dd > 1e-30f) || !(mmm > 1e-30f) || !(m2 > 0.0f)) return 2;
+    const float dot = fmaf(mz, -dz, fmaf(my, -dy, mx * -dx));
+    const float th = __fdividef(dot, mm * d);
+    const float eth = __fdividef(P.eA, dd) + __fdividef(P.eB, mmm) + P.eC;
+    const float ug = eth * P.f_mu_scale + 8.0f * 5.96046448e-8f * P.f_nmu;
+    const float u1 = (th + 1.0f) * P.f_mu_scale;
+    const float u2 = (1.0f - th) * P.f_mu_scale;
+    const float k1 = rintf(u1), k2 = rintf(u2);
     if (k1 >= 1.0f && k1 <= P.f_nmu - 1.0f && fabsf(u1 - k1) < ug) return 2;
     if (k2 >= 1.0f && k2 <= P.f_nmu - 1.0f && fabsf(u2 - k2) < ug) return 2;
-    int a = (int)floorf(u1) + 1;
-    int b = (int)floorf(u2) + 1;
+    const int a = (int)floorf(u1) + 1;
+    const int b = (int)floorf(u2) + 1;
     muf = a < 1 ? 1 : (a > P.nmu ? P.nmu : a);
     mur = b < 1 ? 1 : (b > P.nmu ? P.nmu : b);
   } else {
@@ -219,7 +225,7 @@ __device__ __forceinline__ int edge_rbin(const double4* __restrict__ posd, const
     const float dy = pc.y - pa.y;
     const float dz = pc.z - pa.z;
     const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-    const float d = __fsqrt_rn(d2);
+    const float d = d2 > 0.0f ? d2 * rsqrtf(d2) : 0.0f;
     const float t = (d - P.f_rmin) * P.f_inv_dr;
     const float tn = rintf(t);
     if (fabsf(t - tn) >= P.tguard && t > 0.0f && t < (float)P.nbins) return (int)t + 1;

@@ -118,6 +118,7 @@ struct QuadParams {
   int geo;          // 1: edges among R+(p) by the geometric pair test (cap <= 256)
   int split;        // weighted sums as split limbs without returned values (fix_red);
                     // exact while every bin receives fewer than 2^32 updates
+  int counts;       // integer counts kept (always for unweighted catalogues)
 };
 
 // -tetra histograms (tetra = 1): g_cnt nbins*5, d_cnt nbins*30 (6 terms x 5

@@ -87,6 +87,7 @@ struct QuadCtx {
   unsigned long long *fix, *dfix;  // fixed-point (lo, hi) sums, hi at +5*nbin / +dhi
   int dhi;                          // disc entries on the device (hi offset in dfix)
   int split;                        // 1: sums as split limbs (fix_red), 0: carries (fix_add)
+  int counts;                       // 0: weighted sums only, no integer counts
   double fscale;  // scale of the 4-point products
   double dscale;  // scale of the pair products of the disconnected terms
   // adjoint: cotangents of N2, N3 (nbin each), discN, discR (6 nbin each)
@@ -105,12 +106,12 @@ __device__ __forceinline__ void qfix(const QuadCtx& X, unsigned long long* lo, u
 template <bool SHC>
 __device__ __forceinline__ void qcount(const QuadCtx& X, int k) {
   if (SHC) atomicAdd(&X.scnt[k], 1u);
-  else atomicAdd(&X.cnt[k], 1ull);
+  else if (X.counts) atomicAdd(&X.cnt[k], 1ull);
 }
 template <bool SHC>
 __device__ __forceinline__ void qdcount(const QuadCtx& X, int k) {
   if (SHC) atomicAdd(&X.sdcnt[k], 1u);
-  else atomicAdd(&X.dcnt[k], 1ull);
+  else if (X.counts) atomicAdd(&X.dcnt[k], 1ull);
 }
 
 // The four vertices of a clique: flags (with kFlagDeg4), catalogue ids and
@@ -444,6 +445,7 @@ __device__ __forceinline__ void quad_setup(QuadCtx& X, const QuadParams& Q, unsi
   X.dfix = d_fix;
   X.dhi = nd;
   X.split = Q.split;
+  X.counts = Q.counts;
   X.scnt = nullptr;
   X.sdcnt = nullptr;
   if (SHC) {
@@ -459,6 +461,113 @@ __device__ __forceinline__ void quad_setup(QuadCtx& X, const QuadParams& Q, unsi
   X.c3 = ADJ ? cot + X.nbin : nullptr;
   X.cN = ADJ ? cot + 2 * (size_t)X.nbin : nullptr;
   X.cR = ADJ ? cot + 8 * (size_t)X.nbin : nullptr;
+}
+
+// Weighted 4PCF contributions of the warp's cliques, flattened: every lane
+// first evaluates the four roots of its clique (act: the lane holds one)
+// without branching -- root validity, histogram index and the other three
+// vertices in catalogue-id order -- then the warp takes the valid (clique,
+// root) pairs 32 at a time, every lane updating one root's N2 / N3 sum and
+// its gated pair terms.  The compact per-clique loops diverge (a quarter of
+// the lanes active on average); here every lane is busy in both stages.
+// Products and histogram indices are those of quad_root_rt, so the sums are
+// identical.  Returns this lane's number of rooted contributions.
+__device__ __forceinline__ int quad_contrib_flat(const QuadCtx& X, const QVerts& V,
+                                                 const uint32_t m[6], bool act) {
+  const int lane = threadIdx.x & 31;
+  unsigned long long packed = 0;
+#pragma unroll
+  for (int e = 0; e < 6; ++e) packed |= (unsigned long long)meta_bin(m[e]) << (8 * e);
+  unsigned rndm = 0, flw = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    rndm |= (unsigned)(V.fl[k] & FLAG_RANDOM) << k;
+    flw |= (unsigned)V.fl[k] << (8 * k);
+  }
+  const unsigned perm = id_order(V);
+  // stage 1: the four roots of this lane's clique
+  unsigned vm = 0, rpk = 0;
+  int kk[4];
+#pragma unroll
+  for (int R = 0; R < 4; ++R) {
+    kk[R] = 0;
+    const unsigned fr = flw >> (8 * R);
+    int pos = 0;
+#pragma unroll
+    for (int i = 1; i < 4; ++i)
+      if ((int)((perm >> (2 * i)) & 3u) == R) pos = i;
+    const unsigned lowm = (1u << (2 * pos)) - 1u;
+    const unsigned oth = (perm & lowm) | ((perm >> (2 * pos + 2)) << (2 * pos));
+    const int u0 = (int)(oth & 3u), u1 = (int)((oth >> 2) & 3u), u2 = (int)((oth >> 4) & 3u);
+    const int b1 = qbin(packed, R, u0), b2 = qbin(packed, u0, u1), b3 = qbin(packed, u1, u2),
+              b4 = qbin(packed, R, u2);
+    const bool ok = act && !(fr & FLAG_BUFFER) && (fr & kFlagDeg4) && b1 <= b2 && b2 <= b3 &&
+                    b3 <= b4;
+    if (ok) {
+      const int nb2 = X.nbins + 2;
+      const int cfg = 1 + (X.F[b1] - X.F[1]) + (X.F[nb2 + b2] - X.F[nb2 + b1]) +
+                      (X.F[2 * nb2 + b3] - X.F[2 * nb2 + b2]) +
+                      (X.F[3 * nb2 + b4] - X.F[3 * nb2 + b3]);
+      const int d1 = qbin(packed, R, u1), d2 = qbin(packed, u0, u2);
+      kk[R] = (cfg - 1) + X.ncfg * ((d1 - 1) + X.nbins * (d2 - 1));
+      vm |= 1u << R;
+    }
+    rpk |= ((unsigned)R | ((unsigned)u0 << 2) | ((unsigned)u1 << 4) | ((unsigned)u2 << 6)) << (8 * R);
+  }
+  const int cnt = __popc(vm);
+  int incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  const int excl = incl - cnt;
+  const int nr_own = __popc(rndm);
+  // stage 2: item i belongs to the last lane whose exclusive offset is <= i
+  for (int i0 = 0; i0 < total; i0 += 32) {
+    const int i = i0 + lane;
+    int o = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+      const int c = o + step;
+      const int ex = __shfl_sync(0xffffffffu, excl, c & 31);
+      if (c < 32 && ex <= i) o = c;
+    }
+    const int oex = __shfl_sync(0xffffffffu, excl, o);
+    const unsigned ovm = __shfl_sync(0xffffffffu, vm, o);
+    const unsigned orp = __shfl_sync(0xffffffffu, rpk, o);
+    const unsigned ornd = __shfl_sync(0xffffffffu, rndm, o);
+    const int onr = __shfl_sync(0xffffffffu, nr_own, o);
+    int okk[4];
+    double ow[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      okk[k] = __shfl_sync(0xffffffffu, kk[k], o);
+      ow[k] = __shfl_sync(0xffffffffu, V.w[k], o);
+    }
+    if (i >= total) continue;
+    const int R = __fns(ovm, 0, i - oex + 1);
+    const int kr = R == 0 ? okk[0] : (R == 1 ? okk[1] : (R == 2 ? okk[2] : okk[3]));
+    const unsigned rp = (orp >> (8 * R)) & 0xffu;
+    const int u0 = (int)((rp >> 2) & 3u), u1 = (int)((rp >> 4) & 3u), u2 = (int)((rp >> 6) & 3u);
+    auto wsel = [&](int v) { return v == 0 ? ow[0] : (v == 1 ? ow[1] : (v == 2 ? ow[2] : ow[3])); };
+    qcount<false>(X, kr + X.nbin * onr);
+    qfix(X, &X.fix[kr + X.nbin * onr], &X.fix[kr + X.nbin * (onr + 5)],
+         ((wsel(R) * wsel(u0)) * wsel(u1)) * wsel(u2), X.fscale);
+#pragma unroll
+    for (int tt = 0; tt < 6; ++tt) {
+      const int ga = (int)((rp >> (2 * term_gate(tt))) & 3u);
+      if (!((ornd >> ga) & 1u)) continue;
+      const int u = (int)((rp >> (2 * term_pu(tt))) & 3u), vv = (int)((rp >> (2 * term_pv(tt))) & 3u);
+      const int npr = (int)((ornd >> u) & 1u) + (int)((ornd >> vv) & 1u);
+      const int kt = kr + X.nbin * tt;
+      qdcount<false>(X, kt + X.nbin * 6 * npr);
+      qfix(X, &X.dfix[kt + X.nbin * 6 * npr], &X.dfix[kt + X.nbin * 6 * npr + X.dhi],
+           wsel(u) * wsel(vv), X.dscale);
+    }
+  }
+  return cnt;
 }
 
 // One 4-clique (p, a, b, d) = vertices 0..3 with edge metas m: its
@@ -625,31 +734,53 @@ __global__ void __launch_bounds__((WEIGHTED || ADJ ? kQuadMaxWarps : kQuadMaxWar
       if (nx < 2) continue;
       const unsigned long long mpa_w = s_mo[x];
       int qn = 0;
-      // one queued clique: (p, a = row x, b = X entry z, d = row y_d)
-      auto drain_one = [&](int e) {
-        const unsigned long long qe = s_q[e];
-        const int z = (int)(qe & 0x3ffu), yd = (int)((qe >> 10) & 0x3ffu);
-        const uint32_t mbd = (uint32_t)(qe >> 32);
-        const int yb = s_xy[z];
-        const unsigned long long mpb_w = s_mo[yb], mpd_w = s_mo[yd];
+      // one queued clique: (p, a = row x, b = X entry z, d = row y_d), one
+      // per lane (act: the lane holds entry e).  The weighted 4PCF bins the
+      // warp's cliques together (quad_contrib_flat), so every lane takes
+      // part; a lane without a clique reads nothing and holds zero bins
+      // (no valid root).  Every other mode bins one clique per lane.
+      auto drain_one = [&](int e, bool act) {
+        constexpr bool FLAT = WEIGHTED && COMPACT && !ADJ && !SHC;
+        if (!act && !(FLAT && !X.tetra)) return;
         QVerts V;
-        V.fl[0] = fp;
-        V.fl[1] = (uint8_t)((uint32_t)mpa_w >> 24);
-        V.fl[2] = (uint8_t)((uint32_t)mpb_w >> 24);
-        V.fl[3] = (uint8_t)((uint32_t)mpd_w >> 24);
-        V.og[0] = op;
-        V.og[1] = (int)(mpa_w >> 32);
-        V.og[2] = (int)(mpb_w >> 32);
-        V.og[3] = (int)(mpd_w >> 32);
-        V.w[0] = wp;
-        V.w[1] = LW ? s_w[x] : 0.0;
-        V.w[2] = LW ? s_w[yb] : 0.0;
-        V.w[3] = LW ? s_w[yd] : 0.0;
-        // m: (p,a) (p,b) (p,d) (a,b) (a,d) (b,d)
-        const uint32_t m[6] = {(uint32_t)mpa_w & 0xffffffu, (uint32_t)mpb_w & 0xffffffu,
-                               (uint32_t)mpd_w & 0xffffffu, s_xm[z], s_xm[s_xz[yd]], mbd};
-        const int nroot =
-            quad_emit<WEIGHTED, SHC, ADJ, COMPACT>(X, V, m, gscale, racc, s_glo, s_ghi, x, yb, yd);
+        uint32_t m[6] = {0u, 0u, 0u, 0u, 0u, 0u};
+        int yb = 0, yd = 0;
+        V.fl[0] = V.fl[1] = V.fl[2] = V.fl[3] = 0;
+        V.og[0] = V.og[1] = V.og[2] = V.og[3] = 0;
+        V.w[0] = V.w[1] = V.w[2] = V.w[3] = 0.0;
+        if (act) {
+          const unsigned long long qe = s_q[e];
+          const int z = (int)(qe & 0x3ffu);
+          yd = (int)((qe >> 10) & 0x3ffu);
+          const uint32_t mbd = (uint32_t)(qe >> 32);
+          yb = s_xy[z];
+          const unsigned long long mpb_w = s_mo[yb], mpd_w = s_mo[yd];
+          V.fl[0] = fp;
+          V.fl[1] = (uint8_t)((uint32_t)mpa_w >> 24);
+          V.fl[2] = (uint8_t)((uint32_t)mpb_w >> 24);
+          V.fl[3] = (uint8_t)((uint32_t)mpd_w >> 24);
+          V.og[0] = op;
+          V.og[1] = (int)(mpa_w >> 32);
+          V.og[2] = (int)(mpb_w >> 32);
+          V.og[3] = (int)(mpd_w >> 32);
+          V.w[0] = wp;
+          V.w[1] = LW ? s_w[x] : 0.0;
+          V.w[2] = LW ? s_w[yb] : 0.0;
+          V.w[3] = LW ? s_w[yd] : 0.0;
+          // m: (p,a) (p,b) (p,d) (a,b) (a,d) (b,d)
+          m[0] = (uint32_t)mpa_w & 0xffffffu;
+          m[1] = (uint32_t)mpb_w & 0xffffffu;
+          m[2] = (uint32_t)mpd_w & 0xffffffu;
+          m[3] = s_xm[z];
+          m[4] = s_xm[s_xz[yd]];
+          m[5] = mbd;
+        }
+        int nroot;
+        if (FLAT && !X.tetra)
+          nroot = quad_contrib_flat(X, V, m, act);
+        else
+          nroot = quad_emit<WEIGHTED, SHC, ADJ, COMPACT>(X, V, m, gscale, racc, s_glo, s_ghi, x, yb,
+                                                         yd);
         quads += nroot > 0;
         rooted += nroot;
       };
@@ -703,7 +834,7 @@ __global__ void __launch_bounds__((WEIGHTED || ADJ ? kQuadMaxWarps : kQuadMaxWar
           qn += __popc(m);
           if (qn >= 32) {
             __syncwarp();
-            drain_one(qn - 32 + lane);
+            drain_one(qn - 32 + lane, true);
             qn -= 32;
             __syncwarp();
           }
@@ -711,7 +842,7 @@ __global__ void __launch_bounds__((WEIGHTED || ADJ ? kQuadMaxWarps : kQuadMaxWar
       }
       // the X data of this a are replaced next: drain what is left
       __syncwarp();
-      if (lane < qn) drain_one(lane);
+      if (qn > 0) drain_one(lane, lane < qn);
       __syncwarp();
     }
     if (ADJ) {

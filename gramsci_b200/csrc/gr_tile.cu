@@ -37,71 +37,27 @@ namespace {
 
 constexpr int kTileWarps = 8;
 constexpr int kTileThreads = kTileWarps * 32;
-// resident blocks per SM the register allocation is sized for
+// resident blocks per SM the register allocation is sized for: 3 (at most
+// 85 registers); the adjoint on cells of rmax/2 runs best at 4 (64
+// registers, no spills; measured on the 3M-point adjoint catalogue: 23.5
+// against 27.8 ms, while the forward sweep is faster at 3: 19.4 against
+// 20.4 ms)
 #ifndef GR_TILE_MIN_BLOCKS
-#define GR_TILE_MIN_BLOCKS 2
+#define GR_TILE_MIN_BLOCKS 3
 #endif
 constexpr int kTileQueue = 32 * 32;  // one tile's hits at most
 constexpr float kBufferPush = 1.0e30f;  // added to d2 of a pair of two buffer points
 
 // Exact bins of a pair that passed the outer membership bounds: FP32 with
-// the guard band (approximate square roots and divisions, whose errors the
-// band covers: see make_pair_params), FP64 reference arithmetic inside it.
+// the guard band (classify_f32), FP64 reference arithmetic inside it.
 // Returns false when the pair is not an edge.
 template <bool F32>
 __device__ __forceinline__ bool tile_bins(const DevCatalog& C, const PairParams& P, int p, int q,
                                           const float4 pi, const float4 pj, int& bin, int& muf,
                                           int& mur, unsigned long long& rechecks) {
   if (F32) {
-    const float dx = pj.x - pi.x;
-    const float dy = pj.y - pi.y;
-    const float dz = pj.z - pi.z;
-    const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-    int r = 1;
-    if (d2 >= P.rmax2_hi || d2 <= P.rmin2_lo) return false;
-    const float d = d2 > 0.0f ? d2 * rsqrtf(d2) : 0.0f;  // 0: t = -rmin, decided in FP64
-    const float t = (d - P.f_rmin) * P.f_inv_dr;
-    const float tn = rintf(t);
-    if (fabsf(t - tn) < P.tguard) {
-      r = 2;
-    } else if (t <= 0.0f || t >= (float)P.nbins) {
-      return false;
-    } else {
-      bin = (int)t + 1;
-      muf = 1;
-      mur = 1;
-      if (P.rsd) {
-        const float dd = d - P.d0;
-        const float mx = 0.5f * (pi.x + pj.x);
-        const float my = 0.5f * (pi.y + pj.y);
-        const float mz = 0.5f * (pi.z + pj.z);
-        const float m2 = fmaf(mz, mz, fmaf(my, my, mx * mx));
-        const float mm = m2 * rsqrtf(m2);
-        const float mmm = mm - P.mB;
-        // __fdividef needs denominators of at least 2^-126
-        if (!(dd > 1e-30f) || !(mmm > 1e-30f) || !(m2 > 0.0f)) {
-          r = 2;
-        } else {
-          const float dot = fmaf(mz, -dz, fmaf(my, -dy, mx * -dx));
-          const float th = __fdividef(dot, mm * d);
-          const float eth = __fdividef(P.eA, dd) + __fdividef(P.eB, mmm) + P.eC;
-          const float ug = eth * P.f_mu_scale + 8.0f * 5.96046448e-8f * P.f_nmu;
-          const float u1 = (th + 1.0f) * P.f_mu_scale;
-          const float u2 = (1.0f - th) * P.f_mu_scale;
-          const float k1 = rintf(u1), k2 = rintf(u2);
-          if ((k1 >= 1.0f && k1 <= P.f_nmu - 1.0f && fabsf(u1 - k1) < ug) ||
-              (k2 >= 1.0f && k2 <= P.f_nmu - 1.0f && fabsf(u2 - k2) < ug)) {
-            r = 2;
-          } else {
-            const int a = (int)floorf(u1) + 1;
-            const int b = (int)floorf(u2) + 1;
-            muf = a < 1 ? 1 : (a > P.nmu ? P.nmu : a);
-            mur = b < 1 ? 1 : (b > P.nmu ? P.nmu : b);
-          }
-        }
-      }
-    }
-    if (r == 1) return true;
+    const int r = classify_f32<true>(pi, pj, P, bin, muf, mur);
+    if (r != 2) return r == 1;
     rechecks++;
   }
   return edge_f64(C.posd[p], C.posd[q], P, bin, muf, mur);
@@ -145,7 +101,7 @@ struct TileWarpD {
 // ADJ: the 2PCF weight adjoint instead of histograms: each edge adds
 // coef * w_q to dL/dw_p and coef * w_p to dL/dw_q (pair_coef).
 template <bool F32, bool WEIGHTED, bool WHIST, int SUB, bool PERREG, bool ADJ>
-__global__ void __launch_bounds__(kTileThreads, GR_TILE_MIN_BLOCKS)
+__global__ void __launch_bounds__(kTileThreads, (ADJ && SUB == 2) ? 4 : GR_TILE_MIN_BLOCKS)
     pair2_tile_kernel(DevCatalog C, PairParams P, unsigned long long* __restrict__ g_cnt,
                       unsigned long long* __restrict__ g_fix, double fscale,
                       unsigned long long* __restrict__ stats, int* __restrict__ work, TileAdj A) {

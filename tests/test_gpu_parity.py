@@ -341,3 +341,18 @@ def test_3pcf_without_counts_and_skewed_weights(gpu_ctx, oracle):
     assert np.array_equal(full["N2"], lean["N2"]) and np.array_equal(full["N3"], lean["N3"])
     ref = oracle.Graph(xyz, sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"]).pcf3(w, nd)
     _check_sums(full, ref)
+
+
+def test_4pcf_weighted_sums_without_counts(gpu_ctx):
+    """Weighted 4PCF sums are the same whether or not the integer counts
+    (not part of the reference's output) are kept."""
+    cat, _, sp = _cat("c3_4pcf", 0.05)
+    w = catalogs.normalise(np.random.default_rng(4).lognormal(0, 0.3, cat.n), cat.n_data,
+                           cat.n_rand)
+    gpu_ctx.set_catalog(cat.xyz, w, cat.n_data)
+    gpu_ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
+    full = gpu_ctx.count_4pcf()
+    lean = gpu_ctx.count_4pcf(counts=False)
+    assert "counts" not in lean and int(full["counts"].sum()) > 0
+    for k in ("N2", "N3", "discN", "discR", "catsum", "dsum"):
+        assert np.array_equal(full[k], lean[k]), k
