@@ -664,7 +664,7 @@ def sub_batched(args, stream, flush):
     + guard-band kernels, and in the plain FP64 form."""
     import torch
 
-    from gramsci_b200 import api
+    from gramsci_b200 import api, roofline
 
     name = "c4_batched"
     cat, w, sp = make_catalogue(name, args.scale)
@@ -741,6 +741,16 @@ def sub_batched(args, stream, flush):
                                 "per_region_sum_f32": res["f32"][1],
                                 "per_region_sum_f64": res["f64"][1]},
            "clocks": ck.clocks}
+    # issue and shared-atomic ceilings of the tile sweep, from its ncu summary
+    # (10%-scale catalogue: the same density, so the same instructions per
+    # pair test), over the whole batched call's device time (layout kernels
+    # included: a lower bound for the sweep kernel alone)
+    prof = roofline.profile("pair2_tile_kernel", "c4")
+    n_sm = torch.cuda.get_device_properties(0).multi_processor_count
+    rf = {"kernel": "pair2_tile_kernel", "ms": tb, "ms_is": "whole batched call"}
+    rf["issue"] = roofline.issue_roofline(prof, st["candidates"], tb, ck.clocks.get("sm_mhz"), n_sm)
+    rf["atomics"] = roofline.atomic_roofline(prof, st["candidates"], tb, ck.clocks.get("sm_mhz"), n_sm)
+    rec["roofline"] = rf
     ctx.close()
     del reg_dev, xyz_d, w_d
     if not args.no_cpu_baseline:

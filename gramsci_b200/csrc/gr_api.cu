@@ -61,6 +61,7 @@ struct gr_ctx {
   double wgmax = 0.0, wrmax = 0.0;        // max |w| over galaxies / randoms
   DevBuf<unsigned char> uniform_flag;
   DevBuf<int> work;
+  DevBuf<int> qorder;                    // 4-clique root order (n) + its class counts
   DevBuf<double> cot, grad;              // adjoint inputs / output
   DevBuf<unsigned long long> gfix;       // adjoint fixed-point gradients (lo[n], hi[n])
   // batched regions: 0 none, 1 nsplit^3 subcubes, 2 region ids, 3 mocks
@@ -781,16 +782,31 @@ int gr_count_2pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
   GR_API_END(c)
 }
 
-// Third-edge test of the triangle kernel: the geometric pair test unless mu
-// bins are on and rows are short (mean upper degree below 24), where
-// re-binning every third edge costs more than the hash probes it saves
-// (measured: 3PCF catalogue with 5 mu bins and upper degree 13.7, 0.78 ms
-// geometric against 0.75 ms; without mu bins 0.56 against 0.64 ms; upper
-// degree 156, 197 against 250 ms with 5 mu bins).
-static int tri_geometric(const gr_ctx* c, int rsd) {
-  if (c->clique_mode != 0) return c->clique_mode == 2 ? 1 : 0;
-  if (!rsd) return 1;
-  return c->n > 0 && (double)c->csr.n_edges >= 24.0 * (double)c->n ? 1 : 0;
+// Longest-first root order of the current graph for the 4-clique kernels
+// (rows longer than the class cap share the first class).  Measured on the
+// 4PCF workload: unit weights 4.97 -> 4.34 ms, lognormal weighted sums 9.86
+// -> 8.23 ms, adjoint 12.9 -> 9.3 ms (the last roots of a block no longer
+// keep its other warps waiting at the final barrier, nor the launch waiting
+// on one heavy root).  The triangle kernel keeps label order: on the 3PCF
+// workload the order cost 0.04 ms (0.765 against 0.723 ms: the sort, and
+// neighbouring roots no longer sharing their rows in L1), and the 3M-point
+// adjoint catalogue gained nothing (398 against 396 ms, 852 against 849 ms).
+constexpr int kRootOrderLaunches = 3;  // kernels of order_roots_by_length
+static const int* root_order(gr_ctx* c, cudaStream_t s) {
+  const int cap = (int)std::min<int64_t>(std::max<int64_t>(c->csr.max_deg, 1024) + 1, 1 << 16);
+  c->qorder.reserve((size_t)c->n + cap + 1);
+  order_roots_by_length(c->csr.view(), (int)c->n, cap, c->qorder.p, c->qorder.p + c->n, s);
+  return c->qorder.p;
+}
+
+// Third-edge test of the triangle kernel: the geometric pair test unless the
+// hash probes are forced.  Measured: 3PCF catalogue with 5 mu bins and upper
+// degree 13.7, 0.743 ms geometric against 0.754 ms (the FP32 binning of the
+// re-tested third edges with approximate square root and division; 0.78
+// against 0.75 ms with correctly rounded ones); without mu bins 0.56
+// against 0.64 ms; upper degree 156, 197 against 250 ms with 5 mu bins.
+static int tri_geometric(const gr_ctx* c) {
+  return c->clique_mode == 1 ? 0 : 1;
 }
 
 static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* counts, double* catsum) {
@@ -854,7 +870,7 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
     make_rank_tables(T.rank, c->nbins, 3);
     for (int nr = 0; nr < 4; ++nr) T.fscale[nr] = fscale[nr];
     T.P = c->P;
-    T.geo = tri_geometric(c, T.rsd);
+    T.geo = tri_geometric(c);
     T.maxdeg = (int)std::min<int64_t>(c->csr.max_deg, 1 << 30);
     T.long_geo = c->clique_mode != 1;
     const CSRView G = c->csr.view();
@@ -936,11 +952,10 @@ int gr_count_equi(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
 // Edges among R+(p) in the 4-clique kernels: the geometric pair test (rows
 // up to 256 members) or hash probes of the members' rows.  Measured on the
 // 4PCF workload (upper degree 17.5): unit weights 5.0 ms geometric against
-// 7.0 ms, adjoint 13.0 against 15.3 ms, but lognormal weights 24.9 against
-// 22.8 ms, so weighted sums keep the hash probes.
-static int quad_geometric(const gr_ctx* c, int cap, int nbins, bool weighted_sums) {
-  if (cap > 256 || nbins > 255 || c->clique_mode == 1) return 0;
-  return c->clique_mode == 2 || !weighted_sums ? 1 : 0;
+// 6.3 ms, lognormal weighted sums 9.8 against 10.8 ms, adjoint 13.0 against
+// 15.3 ms.
+static int quad_geometric(const gr_ctx* c, int cap, int nbins) {
+  return (cap > 256 || nbins > 255 || c->clique_mode == 1) ? 0 : 1;
 }
 
 static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* discN, double* discR,
@@ -995,10 +1010,11 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   Q.cap = round_cap((int64_t)gst[2], 32, 1024);
   make_rank_tables(Q.rank, nb, 4);
   Q.P = c->P;
-  Q.geo = quad_geometric(c, Q.cap, nb, weighted);
+  Q.geo = quad_geometric(c, Q.cap, nb);
   const CSRView G = c->csr.view();
   cudaEvent_t q0 = c->ev[4];  // owned by the context
   GR_CUDA_TRY(cudaEventRecord(q0, s));
+  Q.order = root_order(c, s);
   c->work.reserve(4);
   std::vector<unsigned long long> hc(nh), dc(nd), hf, df;
   std::vector<double> hs(nh, 0.0), ds(nd, 0.0);
@@ -1095,7 +1111,7 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   c->st.upper_edges = c->csr.n_edges;
   c->st.fp64_rechecks = (int64_t)gst[0];
   c->st.candidates = (int64_t)gst[1];
-  c->st.kernel_launches = c->index.launches + c->csr.launches + 1;
+  c->st.kernel_launches = c->index.launches + c->csr.launches + 1 + (Q.order ? kRootOrderLaunches : 0);
   GR_API_END(c)
 }
 
@@ -1623,8 +1639,9 @@ int gr_adjoint_4pcf(gr_ctx* c, const double* cot2, const double* cot3, const dou
   Q.cap = round_cap(c->csr.max_deg, 32, 1024);
   make_rank_tables(Q.rank, nb, 4);
   Q.P = c->P;
-  Q.geo = quad_geometric(c, Q.cap, nb, false);
+  Q.geo = quad_geometric(c, Q.cap, nb);
   std::memset(&c->st, 0, sizeof(c->st));
+  Q.order = root_order(c, s);
   launch_adj4(c->index.view(), c->csr.view(), Q, c->cot.p, gscale, c->gfix.p, c->gfix.p + n,
               c->stats.p, c->work.p, s);
   unsigned long long st[8];
@@ -1640,7 +1657,8 @@ int gr_adjoint_4pcf(gr_ctx* c, const double* cot2, const double* cot3, const dou
   c->st.tuples = (int64_t)st[0];
   c->st.rooted = (int64_t)st[1];
   c->st.probes = (int64_t)st[2];
-  c->st.kernel_launches = (reuse ? 0 : c->index.launches + c->csr.launches) + 2;
+  c->st.kernel_launches =
+      (reuse ? 0 : c->index.launches + c->csr.launches) + 2 + (Q.order ? kRootOrderLaunches : 0);
   GR_API_END(c)
 }
 
@@ -1908,8 +1926,7 @@ int gr_count_3pcf_batched(gr_ctx* c, double* N2, double* N3, int64_t* counts, do
   make_rank_tables(T.rank, c->nbins, 3);
   for (int nr = 0; nr < 4; ++nr) T.fscale[nr] = fscale[nr];
   T.P = c->P;
-  T.geo = (c->clique_mode == 2 || (c->clique_mode == 0 &&
-           (!T.rsd || (double)c->csr.n_edges >= 24.0 * (double)std::max<int64_t>(1, RC.n)))) ? 1 : 0;
+  T.geo = tri_geometric(c);
   T.maxdeg = (int)std::min<int64_t>(c->csr.max_deg, 1 << 30);
   T.long_geo = c->clique_mode != 1;
   const int tri_launches = 1 + launch_tri3(RC, c->csr.view(), T, weighted, true, c->hcnt.p,

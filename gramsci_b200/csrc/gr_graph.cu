@@ -9,6 +9,8 @@
 // are visited in increasing label order and compacted with a warp ballot, so
 // rows come out sorted without a sort.  Each undirected edge is stored once,
 // in the row of its smaller label, with the bins seen from both ends.
+#include <algorithm>
+
 #include "gr_index.cuh"
 
 namespace gr {
@@ -359,6 +361,98 @@ void UpperCSR::compact(cudaStream_t s) {
     GR_CHECK_LAUNCH();
   }
   compacted = true;
+}
+
+namespace {
+
+// scratch[0..cap]: the number of roots per length class min(len, cap), then
+// the first slot of each class in longest-first order.  Privatised in shared
+// memory when the classes fit (smem_hist).
+__global__ void root_len_hist_kernel(const int* __restrict__ len, int n, int cap,
+                                     int* __restrict__ hist, bool smem_hist) {
+  extern __shared__ int s_hist[];
+  if (smem_hist) {
+    for (int b = threadIdx.x; b <= cap; b += blockDim.x) s_hist[b] = 0;
+    __syncthreads();
+  }
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    atomicAdd(smem_hist ? &s_hist[min(len[i], cap)] : &hist[min(len[i], cap)], 1);
+  if (smem_hist) {
+    __syncthreads();
+    for (int b = threadIdx.x; b <= cap; b += blockDim.x)
+      if (s_hist[b]) atomicAdd(&hist[b], s_hist[b]);
+  }
+}
+
+// exclusive scan in descending class order, one block: hist[b] = the number
+// of roots in the classes above b
+__global__ void root_len_scan_kernel(int* __restrict__ hist, int cap) {
+  __shared__ int s_warp[32];
+  __shared__ int s_carry;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  for (int j0 = 0; j0 <= cap; j0 += blockDim.x) {
+    const int j = j0 + threadIdx.x;
+    const int v = j <= cap ? hist[cap - j] : 0;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      int w = lane < nw ? s_warp[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      s_warp[lane] = w;
+    }
+    __syncthreads();
+    const int before = s_carry + (wid > 0 ? s_warp[wid - 1] : 0);
+    if (j <= cap) hist[cap - j] = before + x - v;
+    __syncthreads();
+    if (threadIdx.x == 0) s_carry += s_warp[nw - 1];
+    __syncthreads();
+  }
+}
+
+// one slot per root; lanes of a warp with the same class share one atomic
+__global__ void root_scatter_kernel(const int* __restrict__ len, int n, int cap,
+                                    int* __restrict__ off, int* __restrict__ order) {
+  const int lane = threadIdx.x & 31;
+  for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+    const int i = i0 + threadIdx.x;
+    const bool live = i < n;
+    const int b = live ? min(len[i], cap) : -1;
+    const unsigned grp = __match_any_sync(0xffffffffu, b);
+    const int leader = __ffs(grp) - 1;
+    int base = 0;
+    if (live && lane == leader) base = atomicAdd(&off[b], __popc(grp));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (live) order[base + __popc(grp & ((1u << lane) - 1u))] = i;
+  }
+}
+
+}  // namespace
+
+void order_roots_by_length(const CSRView& G, int n, int cap, int* order, int* scratch,
+                           cudaStream_t s) {
+  if (n <= 0) return;
+  GR_CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(int) * (size_t)(cap + 1), s));
+  const int blocks = (int)std::min<int64_t>(((int64_t)n + 255) / 256, 2 * (int64_t)sm_count());
+  const size_t hb = sizeof(int) * (size_t)(cap + 1);
+  const bool smem_hist = hb <= 32 * 1024;
+  root_len_hist_kernel<<<blocks, 256, smem_hist ? hb : 0, s>>>(G.len, n, cap, scratch, smem_hist);
+  GR_CHECK_LAUNCH();
+  root_len_scan_kernel<<<1, 1024, 0, s>>>(scratch, cap);
+  GR_CHECK_LAUNCH();
+  root_scatter_kernel<<<blocks, 256, 0, s>>>(G.len, n, cap, scratch, order);
+  GR_CHECK_LAUNCH();
 }
 
 }  // namespace gr

@@ -62,6 +62,13 @@ struct CSRView {
   const int* deg_full;
 };
 
+// Roots ordered by upper row length, longest first (lengths above cap share
+// the first class), into order[0..n): the counting kernels hand roots out in
+// this order so that the costliest start first and no warp ends a launch on
+// one of them.  scratch: cap + 1 device ints.
+void order_roots_by_length(const CSRView& G, int n, int cap, int* order, int* scratch,
+                           cudaStream_t s);
+
 struct UpperCSR {
   int64_t n = 0, n_edges = 0;  // n_edges counts upper (undirected) edges
   int64_t max_deg = 0;         // largest upper degree

@@ -119,6 +119,8 @@ struct QuadParams {
   int split;        // weighted sums as split limbs without returned values (fix_red);
                     // exact while every bin receives fewer than 2^32 updates
   int counts;       // integer counts kept (always for unweighted catalogues)
+  const int* order; // roots in the order the work counter hands them out
+                    // (order_roots_by_length), or null: label order
 };
 
 // -tetra histograms (tetra = 1): g_cnt nbins*5, d_cnt nbins*30 (6 terms x 5
@@ -133,7 +135,7 @@ struct QuadParams {
 // The outputs (g_cnt nh, g_fix 2 nh, d_cnt nd, d_fix 2 nd; fix arrays only
 // when weighted) must be zeroed; the last disc category (discR, equal to the
 // all-random one before it) is not written, nd covers the others.
-// shared_counts: unweighted counts in block-private 32-bit shared-memory
+// shared_counts: integer counts in block-private 32-bit shared-memory
 // counters (exact while the rooted total stays below 2^32; the caller
 // checks stats[1] and reruns without them otherwise).  Returns whether the
 // shared counters were used.
@@ -148,6 +150,5 @@ bool launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bo
 void launch_adj4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, const double* cot,
                  double gscale, unsigned long long* g_lo, unsigned long long* g_hi,
                  unsigned long long* stats, int* work, cudaStream_t s);
-
 
 }  // namespace gr

@@ -21,8 +21,11 @@
 //
 // A second kernel (quad4g_kernel, the geometric mode) finds the edges among
 // the members of R+(p) with the graph's own membership test on their
-// positions instead of probing the members' rows; it is used for unweighted
-// counts and the adjoint (rows up to 256 members).
+// positions instead of probing the members' rows; it is used whenever the
+// rows fit (up to 256 members).
+#include <algorithm>
+#include <type_traits>
+
 #include "gr_kernels.cuh"
 
 namespace gr {
@@ -31,6 +34,10 @@ namespace {
 
 constexpr int kQuadMaxWarps = 16;   // weighted / adjoint kernels (up to 128 registers)
 constexpr int kQuadMaxWarpsU = 24;  // unweighted kernels (up to 85 registers)
+#ifndef GR_QUADG_WEIGHTED_WARPS
+#define GR_QUADG_WEIGHTED_WARPS 16
+#endif
+constexpr int kQuadGWarpsW = GR_QUADG_WEIGHTED_WARPS;  // weighted geometric kernel
 constexpr size_t kQuadSmemLimit = 227 * 1024;
 constexpr int kQQueue = 96;         // hit queue entries per warp (< 32 left + 64 pushed)
 constexpr int kQMaxOffset = 1 << 22;  // hash entries: (label offset << 10) | position
@@ -472,6 +479,7 @@ __device__ __forceinline__ void quad_setup(QuadCtx& X, const QuadParams& Q, unsi
 // the lanes active on average); here every lane is busy in both stages.
 // Products and histogram indices are those of quad_root_rt, so the sums are
 // identical.  Returns this lane's number of rooted contributions.
+template <bool SHC>
 __device__ __forceinline__ int quad_contrib_flat(const QuadCtx& X, const QVerts& V,
                                                  const uint32_t m[6], bool act) {
   const int lane = threadIdx.x & 31;
@@ -552,7 +560,7 @@ __device__ __forceinline__ int quad_contrib_flat(const QuadCtx& X, const QVerts&
     const unsigned rp = (orp >> (8 * R)) & 0xffu;
     const int u0 = (int)((rp >> 2) & 3u), u1 = (int)((rp >> 4) & 3u), u2 = (int)((rp >> 6) & 3u);
     auto wsel = [&](int v) { return v == 0 ? ow[0] : (v == 1 ? ow[1] : (v == 2 ? ow[2] : ow[3])); };
-    qcount<false>(X, kr + X.nbin * onr);
+    qcount<SHC>(X, kr + X.nbin * onr);
     qfix(X, &X.fix[kr + X.nbin * onr], &X.fix[kr + X.nbin * (onr + 5)],
          ((wsel(R) * wsel(u0)) * wsel(u1)) * wsel(u2), X.fscale);
 #pragma unroll
@@ -562,7 +570,7 @@ __device__ __forceinline__ int quad_contrib_flat(const QuadCtx& X, const QVerts&
       const int u = (int)((rp >> (2 * term_pu(tt))) & 3u), vv = (int)((rp >> (2 * term_pv(tt))) & 3u);
       const int npr = (int)((ornd >> u) & 1u) + (int)((ornd >> vv) & 1u);
       const int kt = kr + X.nbin * tt;
-      qdcount<false>(X, kt + X.nbin * 6 * npr);
+      qdcount<SHC>(X, kt + X.nbin * 6 * npr);
       qfix(X, &X.dfix[kt + X.nbin * 6 * npr], &X.dfix[kt + X.nbin * 6 * npr + X.dhi],
            wsel(u) * wsel(vv), X.dscale);
     }
@@ -574,7 +582,7 @@ __device__ __forceinline__ int quad_contrib_flat(const QuadCtx& X, const QVerts&
 // contributions to the histograms, or (ADJ) its weight gradient: the root's
 // to racc, those of a, b, d to the per-neighbour accumulators at positions
 // ya, yb, yd.  Returns the number of rooted contributions.
-template <bool WEIGHTED, bool SHC, bool ADJ, bool COMPACT>
+template <bool WEIGHTED, bool SHC, bool ADJ, bool COMPACT, bool TETRA>
 __device__ __forceinline__ int quad_emit(const QuadCtx& X, const QVerts& V, const uint32_t m[6],
                                          double gscale, Fix128& racc, unsigned long long* s_glo,
                                          unsigned long long* s_ghi, int ya, int yb, int yd) {
@@ -589,19 +597,20 @@ __device__ __forceinline__ int quad_emit(const QuadCtx& X, const QVerts& V, cons
     }
     return nroot;
   }
-  return X.tetra ? tetra_contrib<WEIGHTED, SHC>(X, V, m)
-                 : (COMPACT ? quad_contrib_c<WEIGHTED, SHC>(X, V, m)
-                            : quad_contrib<WEIGHTED, SHC>(X, V, m));
+  if (TETRA) return tetra_contrib<WEIGHTED, SHC>(X, V, m);
+  return COMPACT ? quad_contrib_c<WEIGHTED, SHC>(X, V, m) : quad_contrib<WEIGHTED, SHC>(X, V, m);
 }
 
-// SHC: unweighted counts in block-private 32-bit shared-memory counters,
+// SHC: integer counts in block-private 32-bit shared-memory counters,
 // added to the global histograms at the end of the block.
 // ADJ: instead of the histograms, the weight gradient (g_lo / g_hi, label
 // order, scale gscale) of sum(c2 N2) + sum(c3 N3) + sum(cN discN) +
 // sum(cR discR), cot = [c2 | c3 | cN | cR].
 // COMPACT: the 4PCF contributions through quad_contrib_c (loops over roots
 // and terms) instead of the unrolled quad_contrib.
-template <bool WEIGHTED, bool SHC, bool ADJ, bool COMPACT>
+// TETRA: the -tetra counts (query_graph_tetrahedron) instead of the 4PCF;
+// a template argument so that each kernel holds the code of one form only.
+template <bool WEIGHTED, bool SHC, bool ADJ, bool COMPACT, bool TETRA>
 __global__ void __launch_bounds__((WEIGHTED || ADJ ? kQuadMaxWarps : kQuadMaxWarpsU) * 32) quad4_kernel(
     DevCatalog C, CSRView G, QuadParams Q, unsigned long long* __restrict__ g_cnt,
     unsigned long long* __restrict__ g_fix, unsigned long long* __restrict__ d_cnt,
@@ -658,11 +667,15 @@ __global__ void __launch_bounds__((WEIGHTED || ADJ ? kQuadMaxWarps : kQuadMaxWar
 
   for (;;) {
     int p = 0;
-    if (lane == 0) p = atomicAdd(work, 1);
+    if (lane == 0) {
+      p = atomicAdd(work, 1);
+      if (Q.order && p < C.n) p = Q.order[p];
+    }
     p = __shfl_sync(0xffffffffu, p, 0);
     if (p >= C.n) break;
     const int64_t b0 = G.start[p];
     const int k = G.len[p];
+    if (k < 3 && Q.order) break;  // longest rows first: every later root is as short
     if (k < 3 || k > cap) continue;  // rows longer than cap are rejected on the host
     if (rec_col(G.rec[b0 + k - 1]) - p >= kQMaxOffset) {
       if (lane == 0) atomicMax(&stats[3], 1ull);  // reported to the host
@@ -740,8 +753,8 @@ __global__ void __launch_bounds__((WEIGHTED || ADJ ? kQuadMaxWarps : kQuadMaxWar
       // part; a lane without a clique reads nothing and holds zero bins
       // (no valid root).  Every other mode bins one clique per lane.
       auto drain_one = [&](int e, bool act) {
-        constexpr bool FLAT = WEIGHTED && COMPACT && !ADJ && !SHC;
-        if (!act && !(FLAT && !X.tetra)) return;
+        constexpr bool FLAT = WEIGHTED && COMPACT && !ADJ && !TETRA;
+        if (!act && !FLAT) return;
         QVerts V;
         uint32_t m[6] = {0u, 0u, 0u, 0u, 0u, 0u};
         int yb = 0, yd = 0;
@@ -776,43 +789,59 @@ __global__ void __launch_bounds__((WEIGHTED || ADJ ? kQuadMaxWarps : kQuadMaxWar
           m[5] = mbd;
         }
         int nroot;
-        if (FLAT && !X.tetra)
-          nroot = quad_contrib_flat(X, V, m, act);
+        if (FLAT)
+          nroot = quad_contrib_flat<SHC>(X, V, m, act);
         else
-          nroot = quad_emit<WEIGHTED, SHC, ADJ, COMPACT>(X, V, m, gscale, racc, s_glo, s_ghi, x, yb,
-                                                         yd);
+          nroot = quad_emit<WEIGHTED, SHC, ADJ, COMPACT, TETRA>(X, V, m, gscale, racc, s_glo, s_ghi,
+                                                                x, yb, yd);
         quads += nroot > 0;
         rooted += nroot;
       };
-      // work items (b = X[z], d in R+(b)), X entries in batches of 32
-      for (int zb = 0; zb < nx; zb += 32) {
-        const int z = zb + lane;
-        int len = 0;
-        long long rs = 0;
-        if (z < nx) {
-          const int yb = s_xy[z];
-          len = s_len[yb];
-          rs = s_rs[yb];
-        }
-        const unsigned nz = __ballot_sync(0xffffffffu, len > 0);
-        const int nrows = __popc(nz);
-        const int src = lane < nrows ? (int)__fns(nz, 0, lane + 1) : 0;
-        // every lane takes part in each shuffle; the select comes after
-        const int slen = __shfl_sync(0xffffffffu, len, src);
-        const int clen = lane < nrows ? slen : 0;
-        const long long crs = __shfl_sync(0xffffffffu, rs, src);
-        const int cz = zb + src;
-        int incl = clen;
+      // Work items (b = X[z], d in R+(b)): X entries in batches of 32, the
+      // rows of a batch flattened over the lanes in windows of 32 items.
+      // One loop over the windows, with a last pass (fin) that drains the
+      // cliques still queued, so that the long binning code has one call
+      // site (the X data of this a are replaced next).
+      int zb = 0, tot = 0, t0 = 0, nrows = 0, incl = 0, excl = 0, cz = 0, done = 0;
+      long long crs = 0;
+      bool fin = false;
+      for (;;) {
+        while (!fin && t0 >= tot) {
+          if (zb >= nx) {
+            fin = true;
+            break;
+          }
+          // the next batch of X entries with their rows
+          const int z = zb + lane;
+          int len = 0;
+          long long rs = 0;
+          if (z < nx) {
+            const int yb = s_xy[z];
+            len = s_len[yb];
+            rs = s_rs[yb];
+          }
+          const unsigned nz = __ballot_sync(0xffffffffu, len > 0);
+          nrows = __popc(nz);
+          const int src = lane < nrows ? (int)__fns(nz, 0, lane + 1) : 0;
+          // every lane takes part in each shuffle; the select comes after
+          const int slen = __shfl_sync(0xffffffffu, len, src);
+          const int clen = lane < nrows ? slen : 0;
+          crs = __shfl_sync(0xffffffffu, rs, src);
+          cz = zb + src;
+          incl = clen;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int yv = __shfl_up_sync(0xffffffffu, incl, o);
-          if (lane >= o) incl += yv;
+          for (int o = 1; o < 32; o <<= 1) {
+            const int yv = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += yv;
+          }
+          tot = __shfl_sync(0xffffffffu, incl, 31);
+          excl = incl - clen;
+          if (lane == 0) probes += (unsigned long long)tot;
+          done = 0;  // compacted rows that ended before the window
+          t0 = 0;
+          zb += 32;
         }
-        const int tot = __shfl_sync(0xffffffffu, incl, 31);
-        const int excl = incl - clen;
-        if (lane == 0) probes += (unsigned long long)tot;
-        int done = 0;  // compacted rows that ended before the window
-        for (int t0 = 0; t0 < tot; t0 += 32) {
+        if (!fin) {
           const int last = incl - 1 - t0;
           const unsigned bit = (lane < nrows && last >= 0 && last < 32) ? (1u << last) : 0u;
           const unsigned ends = __reduce_or_sync(0xffffffffu, bit);
@@ -832,17 +861,17 @@ __global__ void __launch_bounds__((WEIGHTED || ADJ ? kQuadMaxWarps : kQuadMaxWar
             s_q[pos] = ((unsigned long long)rec_meta(rr) << 32) | (uint32_t)(oz | (yd << 10));
           }
           qn += __popc(m);
-          if (qn >= 32) {
-            __syncwarp();
-            drain_one(qn - 32 + lane, true);
-            qn -= 32;
-            __syncwarp();
-          }
+          t0 += 32;
         }
+        if (qn >= 32 || (fin && qn > 0)) {
+          const int nq = min(qn, 32);
+          __syncwarp();
+          drain_one(qn - nq + lane, lane < nq);
+          qn -= nq;
+          __syncwarp();
+        }
+        if (fin && qn == 0) break;
       }
-      // the X data of this a are replaced next: drain what is left
-      __syncwarp();
-      if (qn > 0) drain_one(lane, lane < qn);
       __syncwarp();
     }
     if (ADJ) {
@@ -919,8 +948,9 @@ __host__ __device__ inline QuadGLayout quadg_layout(int nbins, int cap, int nwar
   return L;
 }
 
-template <bool WEIGHTED, bool SHC, bool ADJ, bool COMPACT>
-__global__ void __launch_bounds__((WEIGHTED || ADJ ? kQuadMaxWarps : kQuadMaxWarpsU) * 32) quad4g_kernel(
+template <bool WEIGHTED, bool SHC, bool ADJ, bool COMPACT, bool TETRA>
+__global__ void __launch_bounds__((ADJ ? kQuadMaxWarps : (WEIGHTED ? kQuadGWarpsW : kQuadMaxWarpsU)) * 32)
+    quad4g_kernel(
     DevCatalog C, CSRView G, QuadParams Q, unsigned long long* __restrict__ g_cnt,
     unsigned long long* __restrict__ g_fix, unsigned long long* __restrict__ d_cnt,
     unsigned long long* __restrict__ d_fix, int nh, int nd, double fscale, double dscale,
@@ -951,11 +981,15 @@ __global__ void __launch_bounds__((WEIGHTED || ADJ ? kQuadMaxWarps : kQuadMaxWar
 
   for (;;) {
     int p = 0;
-    if (lane == 0) p = atomicAdd(work, 1);
+    if (lane == 0) {
+      p = atomicAdd(work, 1);
+      if (Q.order && p < C.n) p = Q.order[p];
+    }
     p = __shfl_sync(0xffffffffu, p, 0);
     if (p >= C.n) break;
     const int64_t b0 = G.start[p];
     const int k = G.len[p];
+    if (k < 3 && Q.order) break;  // longest rows first: every later root is as short
     if (k < 3 || k > Q.cap) continue;  // rows longer than cap are rejected on the host
     const uint8_t fp = C.flags[p] | (G.deg_full[p] > 3 ? kFlagDeg4 : 0);
     const int op = C.orig[p];
@@ -1003,33 +1037,54 @@ __global__ void __launch_bounds__((WEIGHTED || ADJ ? kQuadMaxWarps : kQuadMaxWar
     }
     __syncwarp();
     int qn = 0, en = 0;
-    // one queued clique: (p, a = member x, b = member y, d = member z)
-    auto drain_one = [&](int e) {
-      const uint32_t qe = s_q[e];
-      const int x = (int)(qe & 0xffu), y = (int)((qe >> 8) & 0xffu), z = (int)((qe >> 16) & 0xffu);
-      const int bxy = (int)(qe >> 24);
-      const int bxz = edge_rbin(C.posd, P, s_col[x], s_col[z], s_pos[x], s_pos[z]);
-      const int byz = edge_rbin(C.posd, P, s_col[y], s_col[z], s_pos[y], s_pos[z]);
-      const unsigned long long ma = s_mo[x], mb = s_mo[y], md = s_mo[z];
+    // one queued clique: (p, a = member x, b = member y, d = member z), one
+    // per lane (act: the lane holds entry e).  The weighted 4PCF bins the
+    // warp's cliques together (quad_contrib_flat): every lane takes part, a
+    // lane without a clique reads nothing and holds no valid root.
+    auto drain_one = [&](int e, bool act) {
+      constexpr bool FLAT = WEIGHTED && COMPACT && !ADJ && !TETRA;
+      if (!act && !FLAT) return;
       QVerts V;
-      V.fl[0] = fp;
-      V.fl[1] = (uint8_t)((uint32_t)ma >> 24);
-      V.fl[2] = (uint8_t)((uint32_t)mb >> 24);
-      V.fl[3] = (uint8_t)((uint32_t)md >> 24);
-      V.og[0] = op;
-      V.og[1] = (int)(ma >> 32);
-      V.og[2] = (int)(mb >> 32);
-      V.og[3] = (int)(md >> 32);
-      V.w[0] = wp;
-      V.w[1] = LW ? s_w[x] : 0.0;
-      V.w[2] = LW ? s_w[y] : 0.0;
-      V.w[3] = LW ? s_w[z] : 0.0;
-      // m: (p,a) (p,b) (p,d) (a,b) (a,d) (b,d)
-      const uint32_t m[6] = {(uint32_t)ma & 0xffffffu, (uint32_t)mb & 0xffffffu,
-                             (uint32_t)md & 0xffffffu, pack_meta(bxy, 1, 1), pack_meta(bxz, 1, 1),
-                             pack_meta(byz, 1, 1)};
-      const int nroot =
-          quad_emit<WEIGHTED, SHC, ADJ, COMPACT>(X, V, m, gscale, racc, s_glo, s_ghi, x, y, z);
+      uint32_t m[6] = {0u, 0u, 0u, 0u, 0u, 0u};
+      int x = 0, y = 0, z = 0;
+      V.fl[0] = V.fl[1] = V.fl[2] = V.fl[3] = 0;
+      V.og[0] = V.og[1] = V.og[2] = V.og[3] = 0;
+      V.w[0] = V.w[1] = V.w[2] = V.w[3] = 0.0;
+      if (act) {
+        const uint32_t qe = s_q[e];
+        x = (int)(qe & 0xffu);
+        y = (int)((qe >> 8) & 0xffu);
+        z = (int)((qe >> 16) & 0xffu);
+        const int bxy = (int)(qe >> 24);
+        const int bxz = edge_rbin(C.posd, P, s_col[x], s_col[z], s_pos[x], s_pos[z]);
+        const int byz = edge_rbin(C.posd, P, s_col[y], s_col[z], s_pos[y], s_pos[z]);
+        const unsigned long long ma = s_mo[x], mb = s_mo[y], md = s_mo[z];
+        V.fl[0] = fp;
+        V.fl[1] = (uint8_t)((uint32_t)ma >> 24);
+        V.fl[2] = (uint8_t)((uint32_t)mb >> 24);
+        V.fl[3] = (uint8_t)((uint32_t)md >> 24);
+        V.og[0] = op;
+        V.og[1] = (int)(ma >> 32);
+        V.og[2] = (int)(mb >> 32);
+        V.og[3] = (int)(md >> 32);
+        V.w[0] = wp;
+        V.w[1] = LW ? s_w[x] : 0.0;
+        V.w[2] = LW ? s_w[y] : 0.0;
+        V.w[3] = LW ? s_w[z] : 0.0;
+        // m: (p,a) (p,b) (p,d) (a,b) (a,d) (b,d)
+        m[0] = (uint32_t)ma & 0xffffffu;
+        m[1] = (uint32_t)mb & 0xffffffu;
+        m[2] = (uint32_t)md & 0xffffffu;
+        m[3] = pack_meta(bxy, 1, 1);
+        m[4] = pack_meta(bxz, 1, 1);
+        m[5] = pack_meta(byz, 1, 1);
+      }
+      int nroot;
+      if (FLAT)
+        nroot = quad_contrib_flat<SHC>(X, V, m, act);
+      else
+        nroot = quad_emit<WEIGHTED, SHC, ADJ, COMPACT, TETRA>(X, V, m, gscale, racc, s_glo, s_ghi,
+                                                              x, y, z);
       quads += nroot > 0;
       rooted += nroot;
     };
@@ -1065,7 +1120,7 @@ __global__ void __launch_bounds__((WEIGHTED || ADJ ? kQuadMaxWarps : kQuadMaxWar
         if (qn >= 32 || (fin && hm == 0u && qn > 0)) {
           const int nq = min(qn, 32);
           __syncwarp();
-          if (lane < nq) drain_one(qn - nq + lane);
+          drain_one(qn - nq + lane, lane < nq);
           qn -= nq;
           __syncwarp();
         }
@@ -1172,41 +1227,45 @@ bool launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bo
                   bool shared_counts, unsigned long long* stats, int* work, cudaStream_t s) {
   if (C.n <= 0) return false;
   const bool geo = Q.geo != 0;
-  const int maxw = weighted ? kQuadMaxWarps : kQuadMaxWarpsU;
+  const int maxw = weighted ? (geo ? kQuadGWarpsW : kQuadMaxWarps) : kQuadMaxWarpsU;
   auto warps = [&](int ncounts, int mw) {
     return geo ? quadg_warps(Q.nbins, Q.cap, ncounts, false, weighted, mw)
                : quad4_warps(Q.nbins, Q.cap, ncounts, false, mw);
   };
-  // block-private counters for unweighted catalogues when they leave room
-  // for at least 8 warps
+  // integer counts in block-private counters when they leave room for at
+  // least 8 warps (weighted sums without counts need none)
   const int ncnt = nh + nd;
-  if (weighted || warps(ncnt, kQuadMaxWarps) < 8) shared_counts = false;
+  if ((weighted && !Q.counts) || warps(ncnt, kQuadMaxWarps) < 8) shared_counts = false;
   const int nc = shared_counts ? ncnt : 0;
   const int nw = warps(nc, maxw);
   const size_t smem = geo ? quadg_layout(Q.nbins, Q.cap, nw, nc, false, weighted).total
                           : quad_layout(Q.nbins, Q.cap, nw, nc).total;
   // weighted: the compact contribution code (the unrolled form of its long
   // fixed-point updates overflows the instruction cache); unweighted: unrolled
-#define GR_QUAD_LAUNCH(KERNEL)                                                                  \
-  do {                                                                                          \
-    if (weighted)                                                                               \
-      launch_quad_grid(KERNEL<true, false, false, true>, nw, smem, C.n, work, s, C, G, Q, g_cnt, \
-                       g_fix, d_cnt, d_fix, nh, nd, fscale, dscale, stats, nullptr, 1.0,        \
-                       nullptr, nullptr);                                                       \
-    else if (shared_counts)                                                                     \
-      launch_quad_grid(KERNEL<false, true, false, false>, nw, smem, C.n, work, s, C, G, Q,       \
-                       g_cnt, g_fix, d_cnt, d_fix, nh, nd, fscale, dscale, stats, nullptr, 1.0, \
-                       nullptr, nullptr);                                                       \
-    else                                                                                        \
-      launch_quad_grid(KERNEL<false, false, false, false>, nw, smem, C.n, work, s, C, G, Q,      \
-                       g_cnt, g_fix, d_cnt, d_fix, nh, nd, fscale, dscale, stats, nullptr, 1.0, \
-                       nullptr, nullptr);                                                       \
-  } while (0)
+  auto go = [&](auto kfn) {
+    launch_quad_grid(kfn, nw, smem, C.n, work, s, C, G, Q, g_cnt, g_fix, d_cnt, d_fix, nh, nd,
+                     fscale, dscale, stats, nullptr, 1.0, nullptr, nullptr);
+  };
+  auto pick = [&](auto geo_t, auto tetra_t) {
+    constexpr bool GEO = decltype(geo_t)::value, TT = decltype(tetra_t)::value;
+    if constexpr (GEO) {
+      if (weighted && shared_counts) go(quad4g_kernel<true, true, false, true, TT>);
+      else if (weighted) go(quad4g_kernel<true, false, false, true, TT>);
+      else if (shared_counts) go(quad4g_kernel<false, true, false, false, TT>);
+      else go(quad4g_kernel<false, false, false, false, TT>);
+    } else {
+      if (weighted && shared_counts) go(quad4_kernel<true, true, false, true, TT>);
+      else if (weighted) go(quad4_kernel<true, false, false, true, TT>);
+      else if (shared_counts) go(quad4_kernel<false, true, false, false, TT>);
+      else go(quad4_kernel<false, false, false, false, TT>);
+    }
+  };
+  using T1 = std::true_type;
+  using T0 = std::false_type;
   if (geo)
-    GR_QUAD_LAUNCH(quad4g_kernel);
+    Q.tetra ? pick(T1{}, T1{}) : pick(T1{}, T0{});
   else
-    GR_QUAD_LAUNCH(quad4_kernel);
-#undef GR_QUAD_LAUNCH
+    Q.tetra ? pick(T0{}, T1{}) : pick(T0{}, T0{});
   return shared_counts;
 }
 
@@ -1217,13 +1276,13 @@ void launch_adj4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, con
   if (Q.geo) {
     const int nw = quadg_warps(Q.nbins, Q.cap, 0, true, true, kQuadMaxWarps);
     const size_t smem = quadg_layout(Q.nbins, Q.cap, nw, 0, true, true).total;
-    launch_quad_grid(quad4g_kernel<false, false, true, true>, nw, smem, C.n, work, s, C, G, Q,
+    launch_quad_grid(quad4g_kernel<false, false, true, true, false>, nw, smem, C.n, work, s, C, G, Q,
                      nullptr, nullptr, nullptr, nullptr, 0, 0, 1.0, 1.0, stats, cot, gscale, g_lo,
                      g_hi);
   } else {
     const int nw = quad4_warps(Q.nbins, Q.cap, 0, true);
     const size_t smem = quad_layout(Q.nbins, Q.cap, nw, 0, true).total;
-    launch_quad_grid(quad4_kernel<false, false, true, true>, nw, smem, C.n, work, s, C, G, Q,
+    launch_quad_grid(quad4_kernel<false, false, true, true, false>, nw, smem, C.n, work, s, C, G, Q,
                      nullptr, nullptr, nullptr, nullptr, 0, 0, 1.0, 1.0, stats, cot, gscale, g_lo,
                      g_hi);
   }

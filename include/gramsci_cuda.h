@@ -58,9 +58,10 @@ typedef struct gr_ctx gr_ctx;
                                1: keep the graph of the last call and reuse it until the
                                catalogue, the bins or the precision change */
 #define GR_OPT_CLIQUE_MODE 5 /* how the 3PCF / 4PCF kernels find the edges among a root's
-                               larger-label neighbours: 0 automatic (default), 1 hash probes
-                               of the neighbours' rows, 2 the graph's membership test on the
-                               pairs of neighbours.  4PCF: mode 2 takes rows up to 256
+                               larger-label neighbours: 0 automatic (default: mode 2 wherever
+                               the rows allow it), 1 hash probes of the neighbours' rows, 2
+                               the graph's membership test on the pairs of neighbours.
+                               4PCF: mode 2 takes rows up to 256
                                neighbours (longer rows use 1).  3PCF: rows longer than 256
                                neighbours take a second launch in mode 2 (up to 1024, then a
                                global-memory path) unless mode 1 is forced.  Results are
