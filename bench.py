@@ -614,6 +614,11 @@ def sub_quad(args, stream, flush):
     pk = roofline.peaks()
     rf = roofline.quad4_roofline(ctx, q_ms, pk, geometric=True)
     rf["traffic"] = roofline.profiled_traffic("quad4g_kernel", args.scale, "c3")
+    # issue ceiling: warp instructions per 4-clique from the committed ncu summary
+    prof = roofline.profile("quad4g_kernel", "c3") if args.scale == 1.0 else None
+    n_sm = torch.cuda.get_device_properties(0).multi_processor_count
+    rf["issue"] = roofline.issue_roofline(prof, st["tuples"], rf["ms_per_launch"],
+                                          ck.clocks.get("sm_mhz"), n_sm)
     # lognormal weights (automatic kernel choice): weighted sums and adjoint
     ctx.set_clique_mode("auto")
     rng = np.random.default_rng(5)

@@ -55,12 +55,14 @@ struct gr_ctx {
   bool graph_loaded = false;  // graph read by gr_graph_load
   PairParams P{};
   DevBuf<uint8_t> normal_dev;
+  int normal_nmu = 0;                     // nmu of the table in normal_dev (0: none)
   DevBuf<unsigned long long> hcnt, dcnt, stats;
   DevBuf<unsigned long long> hfix, dfix;  // fixed-point sums (lo words, then hi words)
   double wmax = 0.0;                      // max |w| over the catalogue
   double wgmax = 0.0, wrmax = 0.0;        // max |w| over galaxies / randoms
   DevBuf<unsigned char> uniform_flag;
   DevBuf<int> work;
+  HostBuf<unsigned long long> stage;     // pinned read-back of a call's results
   DevBuf<int> qorder;                    // 4-clique root order (n) + its class counts
   DevBuf<double> cot, grad;              // adjoint inputs / output
   DevBuf<unsigned long long> gfix;       // adjoint fixed-point gradients (lo[n], hi[n])
@@ -232,6 +234,17 @@ void normal_table(int nmu, std::vector<uint8_t>& out) {
       }
       out[(size_t)(a - 1) + (size_t)nmu * (b - 1)] = (uint8_t)m;
     }
+}
+
+// The find_normal table of nmu on the device, uploaded when nmu changes.
+static void ensure_normal(gr_ctx* c, int nmu, cudaStream_t s) {
+  if (c->normal_nmu == nmu && c->normal_dev.p) return;
+  std::vector<uint8_t> nt;
+  normal_table(nmu, nt);
+  c->normal_dev.reserve(nt.size());
+  GR_CUDA_TRY(cudaMemcpyAsync(c->normal_dev.p, nt.data(), nt.size(), cudaMemcpyHostToDevice, s));
+  GR_CUDA_TRY(cudaStreamSynchronize(s));  // nt is pageable and goes out of scope
+  c->normal_nmu = nmu;
 }
 
 // ------------------------------------------------------------------ autotune --
@@ -524,8 +537,12 @@ static int set_catalog_impl(gr_ctx* c, const double* xyz, const double* w, const
   // [0] uniform flag, [4] non-finite weight flag (int), [8] max |w| galaxies,
   // [16] max |w| randoms, [24] fingerprint
   c->uniform_flag.reserve(32);
-  unsigned char init[24] = {1};
-  unsigned char out[24];
+  // pinned stage: [0..3) the 24 bytes below, [3] first galaxy weight,
+  // [4] first random weight
+  c->stage.reserve(8);
+  unsigned char* init = reinterpret_cast<unsigned char*>(c->stage.p);
+  std::memset(init, 0, 24);
+  init[0] = 1;
   GR_CUDA_TRY(cudaMemcpyAsync(c->uniform_flag.p, init, 24, cudaMemcpyHostToDevice, s));
   unsigned long long* d_wmax = reinterpret_cast<unsigned long long*>(c->uniform_flag.p + 8);
   if (n > 0) {
@@ -534,12 +551,17 @@ static int set_catalog_impl(gr_ctx* c, const double* xyz, const double* w, const
                                                 reinterpret_cast<int*>(c->uniform_flag.p + 4));
     GR_CHECK_LAUNCH();
   }
+  // the read-back lands in the stage after the upload above has read it
+  unsigned char* out = reinterpret_cast<unsigned char*>(c->stage.p);
+  double* wgr = reinterpret_cast<double*>(c->stage.p + 3);
+  wgr[0] = 0.0;
+  wgr[1] = 0.0;
   GR_CUDA_TRY(cudaMemcpyAsync(out, c->uniform_flag.p, 24, cudaMemcpyDeviceToHost, s));
-  double wg = 0.0, wr = 0.0;
-  if (n_data > 0) GR_CUDA_TRY(cudaMemcpyAsync(&wg, c->w.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (n_data > 0) GR_CUDA_TRY(cudaMemcpyAsync(&wgr[0], c->w.p, sizeof(double), cudaMemcpyDeviceToHost, s));
   if (n_rand > 0)
-    GR_CUDA_TRY(cudaMemcpyAsync(&wr, c->w.p + n_data, sizeof(double), cudaMemcpyDeviceToHost, s));
+    GR_CUDA_TRY(cudaMemcpyAsync(&wgr[1], c->w.p + n_data, sizeof(double), cudaMemcpyDeviceToHost, s));
   GR_CUDA_TRY(cudaStreamSynchronize(s));
+  const double wg = wgr[0], wr = wgr[1];
   unsigned char flag = out[0];
   int nonfinite = 0;
   std::memcpy(&nonfinite, out + 4, 4);
@@ -739,13 +761,16 @@ int gr_count_2pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
   launch_pair2(c->index.view(), c->P, weighted, c->hcnt.p, c->hfix.p, fscale, c->stats.p,
                c->work.p, s, variant);
   GR_CUDA_TRY(cudaEventRecord(c->ev[2], s));
-  std::vector<unsigned long long> hc(nh), hf(2 * nh, 0ull);
+  // read-back in the pinned stage: counts (nh), fixed-point sums (2 nh), stats (8)
+  c->stage.reserve(3 * (size_t)nh + 8);
+  unsigned long long* hc = c->stage.p;
+  unsigned long long* hf = hc + nh;
+  unsigned long long* st = hf + 2 * (size_t)nh;
   std::vector<double> hs(nh, 0.0);
-  unsigned long long st[8];
-  GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaMemcpyAsync(hc, c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
   if (weighted)
-    GR_CUDA_TRY(cudaMemcpyAsync(hf.data(), c->hfix.p, sizeof(unsigned long long) * 2 * nh, cudaMemcpyDeviceToHost, s));
-  GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
+    GR_CUDA_TRY(cudaMemcpyAsync(hf, c->hfix.p, sizeof(unsigned long long) * 2 * nh, cudaMemcpyDeviceToHost, s));
+  GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(unsigned long long) * 8, cudaMemcpyDeviceToHost, s));
   GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
   GR_CUDA_TRY(cudaStreamSynchronize(s));
   if (weighted)
@@ -825,10 +850,7 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
   c->hcnt.reserve(nh);
   c->hfix.reserve(2 * nh);
   c->stats.reserve(8);
-  std::vector<uint8_t> nt;
-  normal_table(nmu, nt);
-  c->normal_dev.reserve(nt.size());
-  GR_CUDA_TRY(cudaMemcpyAsync(c->normal_dev.p, nt.data(), nt.size(), cudaMemcpyHostToDevice, s));
+  ensure_normal(c, nmu, s);
   const bool reuse = reuse_graph(c);
   // A rebuild of a catalogue seen before runs without waiting on the host:
   // the grid is taken from the last bounding box, the graph is filled in the
@@ -839,9 +861,16 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
   // read with the results, and the call is then repeated with waits.
   const bool can_spec =
       !reuse && c->index.have_prev && (c->cat_gen == c->spec_gen || c->spec_new_ok);
-  std::vector<unsigned long long> hc(nh, 0ull), hf(2 * nh, 0ull);
+  // read-back layout in the pinned stage: counts (nh), fixed-point sums
+  // (2 nh), kernel stats (8), graph control (4) and stats (3), bbox flag (1)
+  c->stage.reserve(3 * (size_t)nh + 16);
+  unsigned long long* hc = c->stage.p;
+  unsigned long long* hf = hc + nh;
+  unsigned long long* st = hf + 2 * (size_t)nh;
+  unsigned long long* gctl = st + 8;
+  unsigned long long* gsts = gctl + 4;
+  unsigned long long* gflag = gsts + 3;
   std::vector<double> hs(nh, 0.0);
-  unsigned long long st[8];
   cudaEvent_t q0 = c->ev[4];  // owned by the context
   c->work.reserve(4);
   int tri_launches = 0;
@@ -879,21 +908,21 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
                                    c->hfix.p, c->stats.p, c->work.p, s);  // + the zero fill
     GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
     if (want_counts)
-      GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
+      GR_CUDA_TRY(cudaMemcpyAsync(hc, c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
     if (weighted)
-      GR_CUDA_TRY(cudaMemcpyAsync(hf.data(), c->hfix.p, sizeof(unsigned long long) * 2 * nh, cudaMemcpyDeviceToHost, s));
-    GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
-    unsigned long long gctl[4] = {0, 0, 0, 0}, gsts[3] = {0, 0, 0}, gflag = 0;
+      GR_CUDA_TRY(cudaMemcpyAsync(hf, c->hfix.p, sizeof(unsigned long long) * 2 * nh, cudaMemcpyDeviceToHost, s));
+    GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(unsigned long long) * 8, cudaMemcpyDeviceToHost, s));
+    std::memset(gctl, 0, sizeof(unsigned long long) * 8);
     if (spec) {
-      GR_CUDA_TRY(cudaMemcpyAsync(gctl, c->csr.ctl.p, sizeof(gctl), cudaMemcpyDeviceToHost, s));
-      GR_CUDA_TRY(cudaMemcpyAsync(gsts, c->csr.stats.p, sizeof(gsts), cudaMemcpyDeviceToHost, s));
+      GR_CUDA_TRY(cudaMemcpyAsync(gctl, c->csr.ctl.p, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost, s));
+      GR_CUDA_TRY(cudaMemcpyAsync(gsts, c->csr.stats.p, sizeof(unsigned long long) * 3, cudaMemcpyDeviceToHost, s));
       if (c->index.speculated)
-        GR_CUDA_TRY(cudaMemcpyAsync(&gflag, c->index.mismatch_flag(), sizeof(gflag),
+        GR_CUDA_TRY(cudaMemcpyAsync(gflag, c->index.mismatch_flag(), sizeof(unsigned long long),
                                     cudaMemcpyDeviceToHost, s));
     }
     GR_CUDA_TRY(cudaStreamSynchronize(s));
     if (spec) {
-      if (gflag != 0 || gctl[1] == 1) {  // repeat with waits
+      if (*gflag != 0 || gctl[1] == 1) {  // repeat with waits
         if (c->cat_gen != c->spec_gen) c->spec_new_ok = false;
         continue;
       }
@@ -1545,14 +1574,11 @@ int gr_adjoint_3pcf(gr_ctx* c, const double* cot2, const double* cot3, double* g
   // 2^10 below the per-term bound: the kernel sums up to 1023 terms of one
   // root per neighbour in signed 64 bits before the 128-bit totals
   const double gscale = fix_scale(3.0 * cmax * c->wmax * c->wmax * 1024.0);
-  std::vector<uint8_t> nt;
-  normal_table(nmu, nt);
-  c->normal_dev.reserve(nt.size());
+  ensure_normal(c, nmu, s);
   c->cot.reserve(2 * nc);
   c->gfix.reserve(2 * n + 2);
   c->work.reserve(4);
   c->stats.reserve(8);
-  GR_CUDA_TRY(cudaMemcpyAsync(c->normal_dev.p, nt.data(), nt.size(), cudaMemcpyHostToDevice, s));
   GR_CUDA_TRY(cudaMemcpyAsync(c->cot.p, cot2, sizeof(double) * nc, cudaMemcpyHostToDevice, s));
   if (cot3)
     GR_CUDA_TRY(cudaMemcpyAsync(c->cot.p + nc, cot3, sizeof(double) * nc, cudaMemcpyHostToDevice, s));
@@ -1898,10 +1924,7 @@ int gr_count_3pcf_batched(gr_ctx* c, double* N2, double* N3, int64_t* counts, do
   c->hfix.reserve(2 * nh);
   c->stats.reserve(8);
   c->work.reserve(4);
-  std::vector<uint8_t> nt;
-  normal_table(nmu, nt);
-  c->normal_dev.reserve(nt.size());
-  GR_CUDA_TRY(cudaMemcpyAsync(c->normal_dev.p, nt.data(), nt.size(), cudaMemcpyHostToDevice, s));
+  ensure_normal(c, nmu, s);
   c->regions.enqueue_layout(c->xyz.p, c->w.p, s);
   const DevCatalog RC = c->regions.view();
   GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));

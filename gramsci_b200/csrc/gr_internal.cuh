@@ -52,6 +52,31 @@ struct DevBuf {
   }
 };
 
+// Pinned host memory for the results a call reads back: copies into it are
+// asynchronous, so one stream synchronisation covers all of them (a copy
+// into pageable memory blocks the host once per copy).
+template <typename T>
+struct HostBuf {
+  T* p = nullptr;
+  size_t n = 0;  // capacity in elements
+  HostBuf() = default;
+  HostBuf(const HostBuf&) = delete;
+  HostBuf& operator=(const HostBuf&) = delete;
+  ~HostBuf() { release(); }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    n = 0;
+  }
+  void reserve(size_t count) {
+    if (count <= n && p) return;
+    release();
+    size_t c = count > 0 ? count : 1;
+    GR_CUDA_TRY(cudaMallocHost(&p, c * sizeof(T)));
+    n = c;
+  }
+};
+
 // ------------------------------------------------------------ pair predicate --
 // Everything a kernel needs to decide whether (i, j) is an edge of the
 // reference graph and which radial / mu bins it falls in.
