@@ -189,28 +189,33 @@ __device__ __forceinline__ int classify_f32(const float4 pi, const float4 pj, co
   if (!NEED_BINS) return 1;
   bin = (int)t + 1;
   if (P.rsd) {
+    // s = pi + pj is twice the midpoint m: the factors of 2 cancel in the
+    // cosine th = m.(-d) / (|m| d) and are exact, so th is as with m
     const float dd = d - P.d0;
-    const float mx = 0.5f * (pi.x + pj.x);
-    const float my = 0.5f * (pi.y + pj.y);
-    const float mz = 0.5f * (pi.z + pj.z);
-    const float m2 = fmaf(mz, mz, fmaf(my, my, mx * mx));
-    const float mm = m2 * rsqrtf(m2);
-    const float mmm = mm - P.mB;
+    const float sx = pi.x + pj.x;
+    const float sy = pi.y + pj.y;
+    const float sz = pi.z + pj.z;
+    const float s2 = fmaf(sz, sz, fmaf(sy, sy, sx * sx));
+    const float sn = s2 * rsqrtf(s2);
+    const float mmm = fmaf(0.5f, sn, -P.mB);  // |m| - mB
+    // one bound for both error terms: eA/dd + eB/mmm <= (eA + eB)/min(dd, mmm);
     // __fdividef needs denominators of at least 2^-126
-    if (!(dd > 1e-30f) || !(mmm > 1e-30f) || !(m2 > 0.0f)) return 2;
-    const float dot = fmaf(mz, -dz, fmaf(my, -dy, mx * -dx));
-    const float th = __fdividef(dot, mm * d);
-    const float eth = __fdividef(P.eA, dd) + __fdividef(P.eB, mmm) + P.eC;
+    const float den = fminf(dd, mmm);
+    if (!(den > 1e-30f) || !(s2 > 0.0f)) return 2;
+    const float dot = fmaf(sz, -dz, fmaf(sy, -dy, sx * -dx));
+    const float th = __fdividef(dot, sn * d);
+    const float eth = __fdividef(P.eA + P.eB, den) + P.eC;
     const float ug = eth * P.f_mu_scale + 8.0f * 5.96046448e-8f * P.f_nmu;
+    // mu bins of th (root p) and of -th (root q): u2 = (1 - th) nmu/2 is
+    // nmu - u1, so the interior bin edges of u2 are those of u1 mirrored
+    // and one guard test covers both; outside it the bin of -th is
+    // nmu + 1 - (bin of th), also at the clamped ends th = -1 and 1
     const float u1 = (th + 1.0f) * P.f_mu_scale;
-    const float u2 = (1.0f - th) * P.f_mu_scale;
-    const float k1 = rintf(u1), k2 = rintf(u2);
+    const float k1 = rintf(u1);
     if (k1 >= 1.0f && k1 <= P.f_nmu - 1.0f && fabsf(u1 - k1) < ug) return 2;
-    if (k2 >= 1.0f && k2 <= P.f_nmu - 1.0f && fabsf(u2 - k2) < ug) return 2;
     const int a = (int)floorf(u1) + 1;
-    const int b = (int)floorf(u2) + 1;
     muf = a < 1 ? 1 : (a > P.nmu ? P.nmu : a);
-    mur = b < 1 ? 1 : (b > P.nmu ? P.nmu : b);
+    mur = P.nmu + 1 - muf;
   } else {
     muf = 1;
     mur = 1;
