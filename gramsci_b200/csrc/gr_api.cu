@@ -63,6 +63,7 @@ struct gr_ctx {
   DevBuf<unsigned char> uniform_flag;
   DevBuf<int> work;
   HostBuf<unsigned long long> stage;     // pinned read-back of a call's results
+  DevBuf<double> hval;                   // fixed-point sums converted on the device
   DevBuf<int> qorder;                    // 4-clique root order (n) + its class counts
   DevBuf<double> cot, grad;              // adjoint inputs / output
   DevBuf<unsigned long long> gfix;       // adjoint fixed-point gradients (lo[n], hi[n])
@@ -318,6 +319,46 @@ int set_err(gr_ctx* c, int code, const std::string& m) {
     return set_err((ctx), GR_E_CUDA, "unknown error"); \
   }                                                \
   return GR_OK;
+
+// The 128-bit fixed-point sums of a histogram in FP64, on the device: value
+// k of (lo[k], hi[k]) times inv_scale[k / per] (inverses of powers of two,
+// so one rounding, as the host's fix_value).  split: (lo, hi) are the split
+// limbs of fix_red, worth hi * 2^32 + lo (fix_split_value).  The host then
+// reads n doubles instead of 2n words and converts nothing.
+__global__ void fix_convert_kernel(const unsigned long long* __restrict__ lo,
+                                   const unsigned long long* __restrict__ hi, int64_t n,
+                                   int64_t per, double4 inv_scale, int split,
+                                   double* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = i / per;
+    const double is = c == 0 ? inv_scale.x : (c == 1 ? inv_scale.y : (c == 2 ? inv_scale.z : inv_scale.w));
+    unsigned long long l = lo[i], h = hi[i];
+    if (split) {
+      // (signed h) << 32 as 128 bits, plus l
+      const long long hs = (long long)h;
+      const unsigned long long L = (unsigned long long)hs << 32;
+      unsigned long long H = (unsigned long long)(hs >> 32);
+      const unsigned long long L2 = L + l;
+      H += L2 < L ? 1ull : 0ull;
+      l = L2;
+      h = H;
+    }
+    out[i] = fix_to_double(l, h, is);
+  }
+}
+
+// Queue fix_convert_kernel: n values from (lo, lo + hi_off), categories of
+// `per` values with scales sc[0..3].
+static void enqueue_fix_convert(const unsigned long long* lo, int64_t hi_off, int64_t n,
+                                int64_t per, const double sc[4], bool split, double* out,
+                                cudaStream_t s) {
+  if (n <= 0) return;
+  const double4 inv = make_double4(1.0 / sc[0], 1.0 / sc[1], 1.0 / sc[2], 1.0 / sc[3]);
+  const int blocks = (int)std::min<int64_t>((n + 255) / 256, 2 * (int64_t)sm_count());
+  fix_convert_kernel<<<blocks, 256, 0, s>>>(lo, lo + hi_off, n, per, inv, split ? 1 : 0, out);
+  GR_CHECK_LAUNCH();
+}
 
 // Clears *flag unless all galaxy weights are equal and all random weights are
 // equal; writes max |w| over galaxies to wmax[0] and over randoms to wmax[1]
@@ -861,12 +902,14 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
   // read with the results, and the call is then repeated with waits.
   const bool can_spec =
       !reuse && c->index.have_prev && (c->cat_gen == c->spec_gen || c->spec_new_ok);
-  // read-back layout in the pinned stage: counts (nh), fixed-point sums
-  // (2 nh), kernel stats (8), graph control (4) and stats (3), bbox flag (1)
-  c->stage.reserve(3 * (size_t)nh + 16);
+  // read-back layout in the pinned stage: counts (nh), the sums converted
+  // on the device (nh doubles), kernel stats (8), graph control (4) and
+  // stats (3), bbox flag (1)
+  c->stage.reserve(2 * (size_t)nh + 16);
+  c->hval.reserve(nh);
   unsigned long long* hc = c->stage.p;
-  unsigned long long* hf = hc + nh;
-  unsigned long long* st = hf + 2 * (size_t)nh;
+  double* hv = reinterpret_cast<double*>(hc + nh);
+  unsigned long long* st = hc + 2 * (size_t)nh;
   unsigned long long* gctl = st + 8;
   unsigned long long* gsts = gctl + 4;
   unsigned long long* gflag = gsts + 3;
@@ -909,8 +952,10 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
     GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
     if (want_counts)
       GR_CUDA_TRY(cudaMemcpyAsync(hc, c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
-    if (weighted)
-      GR_CUDA_TRY(cudaMemcpyAsync(hf, c->hfix.p, sizeof(unsigned long long) * 2 * nh, cudaMemcpyDeviceToHost, s));
+    if (weighted) {
+      enqueue_fix_convert(c->hfix.p, nh, nh, nbin, fscale, false, c->hval.p, s);
+      GR_CUDA_TRY(cudaMemcpyAsync(hv, c->hval.p, sizeof(double) * nh, cudaMemcpyDeviceToHost, s));
+    }
     GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(unsigned long long) * 8, cudaMemcpyDeviceToHost, s));
     std::memset(gctl, 0, sizeof(unsigned long long) * 8);
     if (spec) {
@@ -937,7 +982,7 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
                                      (unsigned long long)c->csr.candidates,
                                      (unsigned long long)c->csr.max_deg};
   if (weighted)
-    for (int k = 0; k < nh; ++k) hs[k] = fix_value(hf[k], hf[nh + k], fscale[k / nbin]);
+    for (int k = 0; k < nh; ++k) hs[k] = hv[k];
   if (!weighted) {
     for (int nr = 0; nr < 4; ++nr) {
       double prod = uniform_product(c->w_gal, c->w_ran, 3 - nr, nr);
@@ -966,7 +1011,8 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
   c->st.upper_edges = c->csr.n_edges;
   c->st.fp64_rechecks = (int64_t)gst[0];
   c->st.candidates = (int64_t)gst[1];
-  c->st.kernel_launches = (reuse ? 0 : c->index.launches + c->csr.launches) + tri_launches;
+  c->st.kernel_launches =
+      (reuse ? 0 : c->index.launches + c->csr.launches) + tri_launches + (weighted ? 1 : 0);
   GR_API_END(c)
 }
 
@@ -1045,9 +1091,16 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   GR_CUDA_TRY(cudaEventRecord(q0, s));
   Q.order = root_order(c, s);
   c->work.reserve(4);
-  std::vector<unsigned long long> hc(nh), dc(nd), hf, df;
+  std::vector<unsigned long long> hc(nh), dc(nd);
   std::vector<double> hs(nh, 0.0), ds(nd, 0.0);
-  unsigned long long st[8];
+  // read-back in the pinned stage: counts (nh, ndv), the sums converted on
+  // the device (nh, ndv doubles), kernel stats (8)
+  c->stage.reserve(2 * ((size_t)nh + ndv) + 8);
+  c->hval.reserve((size_t)nh + ndv);
+  unsigned long long* sc = c->stage.p;
+  unsigned long long* sd = sc + nh;
+  double* sv = reinterpret_cast<double*>(sd + ndv);
+  unsigned long long* st = sd + ndv + nh + ndv;
   // First attempt: unweighted counts in block-private 32-bit counters, and
   // weighted sums as split limbs added without returned values (fix_red).
   // Both are exact while every bin receives fewer than 2^32 updates, which
@@ -1070,26 +1123,32 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
                                      c->dcnt.p, c->dfix.p, nh, ndv, fscale, dscale, attempt == 0,
                                      c->stats.p, c->work.p, s);
     GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
-    GR_CUDA_TRY(cudaMemcpyAsync(hc.data(), c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
-    GR_CUDA_TRY(cudaMemcpyAsync(dc.data(), c->dcnt.p, sizeof(unsigned long long) * ndv, cudaMemcpyDeviceToHost, s));
-    if (weighted) {
-      hf.resize(2 * (size_t)nh);
-      df.resize(2 * (size_t)ndv);
-      GR_CUDA_TRY(cudaMemcpyAsync(hf.data(), c->hfix.p, sizeof(unsigned long long) * 2 * nh, cudaMemcpyDeviceToHost, s));
-      GR_CUDA_TRY(cudaMemcpyAsync(df.data(), c->dfix.p, sizeof(unsigned long long) * 2 * ndv, cudaMemcpyDeviceToHost, s));
+    if (Q.counts) {
+      GR_CUDA_TRY(cudaMemcpyAsync(sc, c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
+      GR_CUDA_TRY(cudaMemcpyAsync(sd, c->dcnt.p, sizeof(unsigned long long) * ndv, cudaMemcpyDeviceToHost, s));
     }
-    GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s));
+    if (weighted) {
+      const double fs[4] = {fscale, fscale, fscale, fscale};
+      const double ds4[4] = {dscale, dscale, dscale, dscale};
+      enqueue_fix_convert(c->hfix.p, nh, nh, nh, fs, Q.split != 0, c->hval.p, s);
+      enqueue_fix_convert(c->dfix.p, ndv, ndv, ndv, ds4, Q.split != 0, c->hval.p + nh, s);
+      GR_CUDA_TRY(cudaMemcpyAsync(sv, c->hval.p, sizeof(double) * ((size_t)nh + ndv), cudaMemcpyDeviceToHost, s));
+    }
+    GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(unsigned long long) * 8, cudaMemcpyDeviceToHost, s));
     GR_CUDA_TRY(cudaStreamSynchronize(s));
     if (!(shared || Q.split) || st[1] < (1ull << 32)) break;
+  }
+  if (Q.counts) {
+    std::memcpy(hc.data(), sc, sizeof(unsigned long long) * nh);
+    std::memcpy(dc.data(), sd, sizeof(unsigned long long) * ndv);
   }
   if (st[3] != 0)
     return set_err(c, GR_E_CAPACITY, "4PCF: label offsets within a row exceed the hash key range");
   // discR category = the all-random category before it
   for (int k = 0; k < nbin * 6; ++k) dc[(size_t)ndv + k] = dc[(size_t)ndv - nbin * 6 + k];
   if (weighted) {
-    auto val = Q.split ? fix_split_value : fix_value;
-    for (int k = 0; k < nh; ++k) hs[k] = val(hf[k], hf[(size_t)nh + k], fscale);
-    for (int k = 0; k < ndv; ++k) ds[k] = val(df[k], df[(size_t)ndv + k], dscale);
+    std::memcpy(hs.data(), sv, sizeof(double) * nh);
+    std::memcpy(ds.data(), sv + nh, sizeof(double) * ndv);
     for (int k = 0; k < nbin * 6; ++k) ds[(size_t)ndv + k] = ds[(size_t)ndv - nbin * 6 + k];
   }
   if (!weighted) {
@@ -1140,7 +1199,8 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   c->st.upper_edges = c->csr.n_edges;
   c->st.fp64_rechecks = (int64_t)gst[0];
   c->st.candidates = (int64_t)gst[1];
-  c->st.kernel_launches = c->index.launches + c->csr.launches + 1 + (Q.order ? kRootOrderLaunches : 0);
+  c->st.kernel_launches = c->index.launches + c->csr.launches + 1 + (Q.order ? kRootOrderLaunches : 0) +
+                          (weighted ? 2 : 0);
   GR_API_END(c)
 }
 
