@@ -858,10 +858,16 @@ int gr_count_2pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
 // neighbouring roots no longer sharing their rows in L1), and the 3M-point
 // adjoint catalogue gained nothing (398 against 396 ms, 852 against 849 ms).
 constexpr int kRootOrderLaunches = 3;  // kernels of order_roots_by_length
-static const int* root_order(gr_ctx* c, cudaStream_t s) {
+static const int* root_order(gr_ctx* c, cudaStream_t s, const int** above = nullptr,
+                             int* nclass = nullptr) {
   const int cap = (int)std::min<int64_t>(std::max<int64_t>(c->csr.max_deg, 1024) + 1, 1 << 16);
   c->qorder.reserve((size_t)c->n + cap + 1);
-  order_roots_by_length(c->csr.view(), (int)c->n, cap, c->qorder.p, c->qorder.p + c->n, s);
+  int* scratch = c->qorder.p + c->n;
+  order_roots_by_length(c->csr.view(), (int)c->n, cap, c->qorder.p, scratch, s);
+  // after the ordering, scratch[b] holds the number of roots in the classes
+  // above b (classes 0..cap)
+  if (above) *above = scratch;
+  if (nclass) *nclass = cap + 1;
   return c->qorder.p;
 }
 
@@ -1089,7 +1095,7 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   const CSRView G = c->csr.view();
   cudaEvent_t q0 = c->ev[4];  // owned by the context
   GR_CUDA_TRY(cudaEventRecord(q0, s));
-  Q.order = root_order(c, s);
+  Q.order = root_order(c, s, &Q.above, &Q.nclass);
   c->work.reserve(4);
   std::vector<unsigned long long> hc(nh), dc(nd);
   std::vector<double> hs(nh, 0.0), ds(nd, 0.0);
@@ -1727,7 +1733,7 @@ int gr_adjoint_4pcf(gr_ctx* c, const double* cot2, const double* cot3, const dou
   Q.P = c->P;
   Q.geo = quad_geometric(c, Q.cap, nb);
   std::memset(&c->st, 0, sizeof(c->st));
-  Q.order = root_order(c, s);
+  Q.order = root_order(c, s, &Q.above, &Q.nclass);
   launch_adj4(c->index.view(), c->csr.view(), Q, c->cot.p, gscale, c->gfix.p, c->gfix.p + n,
               c->stats.p, c->work.p, s);
   unsigned long long st[8];

@@ -121,6 +121,9 @@ struct QuadParams {
   int counts;       // integer counts kept (always for unweighted catalogues)
   const int* order; // roots in the order the work counter hands them out
                     // (order_roots_by_length), or null: label order
+  const int* above;  // with order: above[b] = the number of roots whose row
+                     // length class (min(length, nclass - 1)) exceeds b, or null
+  int nclass;
 };
 
 // -tetra histograms (tetra = 1): g_cnt nbins*5, d_cnt nbins*30 (6 terms x 5

@@ -42,6 +42,49 @@ constexpr size_t kQuadSmemLimit = 227 * 1024;
 constexpr int kQQueue = 96;         // hit queue entries per warp (< 32 left + 64 pushed)
 constexpr int kQMaxOffset = 1 << 22;  // hash entries: (label offset << 10) | position
 constexpr uint8_t kFlagDeg4 = 4;    // staged flag: full row length > 3 (a reference root)
+// The longest rows (a root's cost grows with the cube of its row length) are
+// handed out as kSplitParts work items each, every item staging the root in
+// full and taking every kSplitParts-th share of its cliques: a heavy root on
+// one warp otherwise ends the launch alone (measured on the 4PCF workload:
+// one SM busy for 8.0M cycles while the others were done after 5.1M).  The
+// split roots are the longest ones, at least kSplitRow long, few enough that
+// their items fill at most an eighth of the launch's warps.
+constexpr int kSplitRow = 32;
+constexpr int kSplitParts = 8;
+
+// The root and part of work item `item` (QuadParams::order / nheavy).
+// Items [0, nheavy * parts) are the parts of the heavy roots, then one item
+// per remaining root.  Returns false past the last root.
+__device__ __forceinline__ bool quad_item(const QuadParams& Q, int n, int item, int nh, int parts,
+                                          int& p, int& part) {
+  int slot;
+  part = 0;
+  if (item < nh * parts) {
+    slot = item / parts;
+    part = item - slot * parts;
+  } else {
+    slot = nh + (item - nh * parts);
+  }
+  if (slot >= n) return false;
+  p = Q.order ? Q.order[slot] : slot;
+  return true;
+}
+__device__ __forceinline__ int quad_split_parts(const QuadParams& Q, int& nh) {
+  nh = 0;
+  if (!Q.order || !Q.above || Q.nclass <= kSplitRow) return 1;
+  const int limit = (int)gridDim.x * (int)(blockDim.x >> 5) / (8 * kSplitParts);
+  // above[] does not increase with b: the smallest b >= kSplitRow - 1 with
+  // above[b] <= limit
+  int lo = kSplitRow - 1, hi = Q.nclass - 1;
+  if (Q.above[hi] > limit) return 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (Q.above[mid] <= limit) hi = mid;
+    else lo = mid + 1;
+  }
+  nh = Q.above[lo];
+  return nh > 0 ? kSplitParts : 1;
+}
 
 __host__ __device__ inline size_t qalign8(size_t x) { return (x + 7) & ~(size_t)7; }
 
@@ -665,14 +708,15 @@ __global__ void __launch_bounds__((WEIGHTED || ADJ ? kQuadMaxWarps : kQuadMaxWar
     return hit ? (int)(e & 0x3ffu) : -1;
   };
 
+  int nheavy;
+  const int parts = quad_split_parts(Q, nheavy);
   for (;;) {
-    int p = 0;
-    if (lane == 0) {
-      p = atomicAdd(work, 1);
-      if (Q.order && p < C.n) p = Q.order[p];
-    }
-    p = __shfl_sync(0xffffffffu, p, 0);
-    if (p >= C.n) break;
+    int item = 0;
+    if (lane == 0) item = atomicAdd(work, 1);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    int p, part;
+    if (!quad_item(Q, C.n, item, nheavy, parts, p, part)) break;
+    const int nparts = item < nheavy * parts ? parts : 1;
     const int64_t b0 = G.start[p];
     const int k = G.len[p];
     if (k < 3 && Q.order) break;  // longest rows first: every later root is as short
@@ -718,7 +762,7 @@ __global__ void __launch_bounds__((WEIGHTED || ADJ ? kQuadMaxWarps : kQuadMaxWar
     }
     __syncwarp();
     const int nwords = (k + 31) >> 5;
-    for (int x = 0; x < k - 2; ++x) {
+    for (int x = part; x < k - 2; x += nparts) {  // a split root: every nparts-th a
       // X = R+(a) ∩ R+(p) beyond position x, listed in label order and
       // marked in the bitmask
       for (int wd = lane; wd < nwords; wd += 32) s_bits[wd] = 0u;
@@ -979,14 +1023,15 @@ __global__ void __launch_bounds__((ADJ ? kQuadMaxWarps : (WEIGHTED ? kQuadGWarps
   uint32_t* s_eq = reinterpret_cast<uint32_t*>(wb + L.o_eq);
   unsigned long long quads = 0, rooted = 0, probes = 0;
 
+  int nheavy;
+  const int parts = quad_split_parts(Q, nheavy);
   for (;;) {
-    int p = 0;
-    if (lane == 0) {
-      p = atomicAdd(work, 1);
-      if (Q.order && p < C.n) p = Q.order[p];
-    }
-    p = __shfl_sync(0xffffffffu, p, 0);
-    if (p >= C.n) break;
+    int item = 0;
+    if (lane == 0) item = atomicAdd(work, 1);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    int p, part;
+    if (!quad_item(Q, C.n, item, nheavy, parts, p, part)) break;
+    const int nparts = item < nheavy * parts ? parts : 1;
     const int64_t b0 = G.start[p];
     const int k = G.len[p];
     if (k < 3 && Q.order) break;  // longest rows first: every later root is as short
@@ -1015,7 +1060,7 @@ __global__ void __launch_bounds__((ADJ ? kQuadMaxWarps : (WEIGHTED ? kQuadGWarps
     // pass 1: adjacency among the members of R+(p)
     const int npair = k * (k - 1) / 2;
     const int k2m1 = 2 * k - 1;
-    if (lane == 0) probes += (unsigned long long)npair;
+    if (lane == 0 && part == 0) probes += (unsigned long long)npair;  // once per root
     auto pair_of = [&](int t, int& x, int& y) {
       // x: the largest row with x (2k - 1 - x) / 2 <= t pairs before it
       const float disc = (float)(k2m1 * k2m1) - 8.0f * (float)t;
@@ -1128,8 +1173,9 @@ __global__ void __launch_bounds__((ADJ ? kQuadMaxWarps : (WEIGHTED ? kQuadGWarps
       }
     };
     // pass 2: the edges in pair order, 32 at a time, then what is queued
+    // (a split root: every nparts-th chunk of 32 pairs)
     for (int t0 = 0;; t0 += 32) {
-      if (t0 < npair) {
+      if (t0 < npair && ((t0 >> 5) % nparts) == part) {
         const int t = t0 + lane;
         bool edge = false;
         int x = 0, y = 0;
