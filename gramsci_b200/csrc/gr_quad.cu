@@ -520,11 +520,16 @@ __device__ __forceinline__ void quad_setup(QuadCtx& X, const QuadParams& Q, unsi
 // root) pairs 32 at a time, every lane updating one root's N2 / N3 sum and
 // its gated pair terms.  The compact per-clique loops diverge (a quarter of
 // the lanes active on average); here every lane is busy in both stages.
-// Products and histogram indices are those of quad_root_rt, so the sums are
-// identical.  Returns this lane's number of rooted contributions.
+// The pairs are ordered by root index, then lane: one ballot per root index
+// gives each pair's lane with no search, and the vertex weights are read
+// from the staged weights (s_w at the positions packed 10 bits each in vpos
+// for vertices 1..3; vertex 0 is the warp's root, weight wp).  Products and
+// histogram indices are those of quad_root_rt, so the sums are identical.
+// Returns this lane's number of rooted contributions.
 template <bool SHC>
 __device__ __forceinline__ int quad_contrib_flat(const QuadCtx& X, const QVerts& V,
-                                                 const uint32_t m[6], bool act) {
+                                                 const uint32_t m[6], bool act, unsigned vpos,
+                                                 const double* s_w, double wp) {
   const int lane = threadIdx.x & 31;
   unsigned long long packed = 0;
 #pragma unroll
@@ -565,44 +570,35 @@ __device__ __forceinline__ int quad_contrib_flat(const QuadCtx& X, const QVerts&
     }
     rpk |= ((unsigned)R | ((unsigned)u0 << 2) | ((unsigned)u1 << 4) | ((unsigned)u2 << 6)) << (8 * R);
   }
-  const int cnt = __popc(vm);
-  int incl = cnt;
+  // stage 2: pairs (root index R, lane) in that order
+  unsigned mr[4];
+  int c0, c1, c2, total;
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int v = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += v;
-  }
-  const int total = __shfl_sync(0xffffffffu, incl, 31);
-  const int excl = incl - cnt;
-  const int nr_own = __popc(rndm);
-  // stage 2: item i belongs to the last lane whose exclusive offset is <= i
+  for (int R = 0; R < 4; ++R) mr[R] = __ballot_sync(0xffffffffu, (vm >> R) & 1u);
+  c0 = __popc(mr[0]);
+  c1 = c0 + __popc(mr[1]);
+  c2 = c1 + __popc(mr[2]);
+  total = c2 + __popc(mr[3]);
   for (int i0 = 0; i0 < total; i0 += 32) {
     const int i = i0 + lane;
-    int o = 0;
-#pragma unroll
-    for (int step = 16; step > 0; step >>= 1) {
-      const int c = o + step;
-      const int ex = __shfl_sync(0xffffffffu, excl, c & 31);
-      if (c < 32 && ex <= i) o = c;
-    }
-    const int oex = __shfl_sync(0xffffffffu, excl, o);
-    const unsigned ovm = __shfl_sync(0xffffffffu, vm, o);
+    const int R = i < c0 ? 0 : (i < c1 ? 1 : (i < c2 ? 2 : 3));
+    const int base = R == 0 ? 0 : (R == 1 ? c0 : (R == 2 ? c1 : c2));
+    const unsigned mR = R == 0 ? mr[0] : (R == 1 ? mr[1] : (R == 2 ? mr[2] : mr[3]));
+    const int o = i < total ? (int)__fns(mR, 0, i - base + 1) : 0;
+    // every lane takes part in each shuffle; the select comes after
     const unsigned orp = __shfl_sync(0xffffffffu, rpk, o);
     const unsigned ornd = __shfl_sync(0xffffffffu, rndm, o);
-    const int onr = __shfl_sync(0xffffffffu, nr_own, o);
-    int okk[4];
-    double ow[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      okk[k] = __shfl_sync(0xffffffffu, kk[k], o);
-      ow[k] = __shfl_sync(0xffffffffu, V.w[k], o);
-    }
+    const unsigned opos = __shfl_sync(0xffffffffu, vpos, o);
+    const int k0 = __shfl_sync(0xffffffffu, kk[0], o), k1 = __shfl_sync(0xffffffffu, kk[1], o),
+              k2 = __shfl_sync(0xffffffffu, kk[2], o), k3 = __shfl_sync(0xffffffffu, kk[3], o);
     if (i >= total) continue;
-    const int R = __fns(ovm, 0, i - oex + 1);
-    const int kr = R == 0 ? okk[0] : (R == 1 ? okk[1] : (R == 2 ? okk[2] : okk[3]));
+    const int kr = R == 0 ? k0 : (R == 1 ? k1 : (R == 2 ? k2 : k3));
+    const int onr = __popc(ornd);
     const unsigned rp = (orp >> (8 * R)) & 0xffu;
     const int u0 = (int)((rp >> 2) & 3u), u1 = (int)((rp >> 4) & 3u), u2 = (int)((rp >> 6) & 3u);
-    auto wsel = [&](int v) { return v == 0 ? ow[0] : (v == 1 ? ow[1] : (v == 2 ? ow[2] : ow[3])); };
+    const double w1 = s_w[opos & 0x3ffu], w2 = s_w[(opos >> 10) & 0x3ffu],
+                 w3 = s_w[(opos >> 20) & 0x3ffu];
+    auto wsel = [&](int v) { return v == 0 ? wp : (v == 1 ? w1 : (v == 2 ? w2 : w3)); };
     qcount<SHC>(X, kr + X.nbin * onr);
     qfix(X, &X.fix[kr + X.nbin * onr], &X.fix[kr + X.nbin * (onr + 5)],
          ((wsel(R) * wsel(u0)) * wsel(u1)) * wsel(u2), X.fscale);
@@ -618,7 +614,7 @@ __device__ __forceinline__ int quad_contrib_flat(const QuadCtx& X, const QVerts&
            wsel(u) * wsel(vv), X.dscale);
     }
   }
-  return cnt;
+  return __popc(vm);
 }
 
 // One 4-clique (p, a, b, d) = vertices 0..3 with edge metas m: its
@@ -834,7 +830,9 @@ __global__ void __launch_bounds__((WEIGHTED || ADJ ? kQuadMaxWarps : kQuadMaxWar
         }
         int nroot;
         if (FLAT)
-          nroot = quad_contrib_flat<SHC>(X, V, m, act);
+          nroot = quad_contrib_flat<SHC>(X, V, m, act,
+                                         (unsigned)x | ((unsigned)yb << 10) | ((unsigned)yd << 20),
+                                         s_w, wp);
         else
           nroot = quad_emit<WEIGHTED, SHC, ADJ, COMPACT, TETRA>(X, V, m, gscale, racc, s_glo, s_ghi,
                                                                 x, yb, yd);
@@ -1126,7 +1124,9 @@ __global__ void __launch_bounds__((ADJ ? kQuadMaxWarps : (WEIGHTED ? kQuadGWarps
       }
       int nroot;
       if (FLAT)
-        nroot = quad_contrib_flat<SHC>(X, V, m, act);
+        nroot = quad_contrib_flat<SHC>(X, V, m, act,
+                                       (unsigned)x | ((unsigned)y << 10) | ((unsigned)z << 20), s_w,
+                                       wp);
       else
         nroot = quad_emit<WEIGHTED, SHC, ADJ, COMPACT, TETRA>(X, V, m, gscale, racc, s_glo, s_ghi,
                                                               x, y, z);
