@@ -348,6 +348,7 @@ def e2e_loop(ctx, cat, w, count, stream, flush, steps):
 
     timed(call, 2, stream, flush)
     ms = timed(call, steps, stream, flush)
+    e2e_loop.spread = [float(np.min(ms)), float(np.median(ms)), float(np.max(ms))]
     return float(np.mean(ms)), out["r"]
 
 
@@ -463,6 +464,7 @@ def run_ours(args):
                   "phase_ms": {"index": st["ms_index"], "graph": st["ms_graph"],
                                "query": st["ms_query"]}},
         "e2e": {"value": e2e_value, "unit": "tuples/s", "h2d_bytes_per_step": h2d,
+                "ms_per_step": e2e_t, "ms_min_median_max": e2e_loop.spread,
                 "d2h_bytes_per_step": d2h},
         "roofline": rf,
         "graph_roofline": grf,
