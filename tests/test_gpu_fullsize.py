@@ -9,7 +9,9 @@ compare the CUDA library with the CPU oracle on the same inputs:
 * the plain 2PCF (70,000 points) and the clustered 3PCF with line-of-sight
   bins (400,000 points), in full;
 * the 4PCF on the dense clustered set (120,000 points), unit and lognormal
-  weights, with the disconnected pair terms;
+  weights, with the disconnected pair terms, and its two 4-clique kernels
+  (hash probes and the geometric pair test, heaviest roots split over
+  several work items) giving identical results and gradients;
 * four seeded regions of the batched catalogue (12M points, 125 regions with
   60 Mpc/h buffers), each region's members counted alone, and the per-region
   counts of all 125 regions summed against the one-launch batched count;
@@ -190,3 +192,33 @@ def test_full_c5_gradients_local(oracle, order):
             # the largest gradient, as in the other adjoint tests
             assert abs(grad[k] - g_orc) <= RTOL * gmax, (k, grad[k], g_orc)
             assert abs(grad[k] - fd) <= 1e-8 * max(abs(fd), 1e-300), (k, grad[k], fd)
+
+
+def test_full_c3_clique_modes_identical():
+    """The hash-probe and the geometric 4-clique kernels at full size, where
+    the roots are taken longest row first and the heaviest rows are split
+    over several work items: identical counts, sums and weight gradients,
+    unit and lognormal weights."""
+    cat, w, sp = _cat("c3_4pcf")
+    rng = np.random.default_rng(34)
+    wl = catalogs.normalise(rng.lognormal(0.0, 0.3, cat.n), cat.n_data, cat.n_rand)
+    out, grads = {}, {}
+    with api.Context(0) as ctx:
+        ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
+        for wname, ww in (("unit", w), ("lognormal", wl)):
+            ctx.set_catalog(cat.xyz, ww, cat.n_data)
+            for mode in ("hash", "geometric"):
+                ctx.set_clique_mode(mode)
+                r = ctx.count_4pcf()
+                out[(wname, mode)] = r
+                if wname == "lognormal":
+                    cot = [np.random.default_rng(35).normal(size=r[k].shape)
+                           for k in ("N2", "N3", "discN", "discR")]
+                    grads[mode] = ctx.adjoint_4pcf(*cot)
+    for wname in ("unit", "lognormal"):
+        a, b = out[(wname, "hash")], out[(wname, "geometric")]
+        assert set(a) == set(b)
+        for k in a:
+            assert np.array_equal(a[k], b[k]), (wname, k)
+    assert int(out[("unit", "geometric")]["counts"].sum()) > 50_000_000
+    assert np.array_equal(grads["hash"], grads["geometric"])

@@ -2,9 +2,11 @@
 takes the grid of the last bounding box and fills the graph in the scratch
 area as it is, and a device flag sends the call round again with waits when
 the bounding box changed or the scratch area was too small.  Every case is
-checked against the oracle: repeated counts of one catalogue, a denser
-catalogue with the same bounding box (scratch too small), and a catalogue
-with another bounding box (grid changed)."""
+checked against the oracle: repeated counts of one catalogue, another
+catalogue of the same size and bounding box (the captured rebuild of the
+previous call replayed), a denser catalogue with the same bounding box
+(scratch too small), and a catalogue with another bounding box (grid
+changed)."""
 import numpy as np
 import pytest
 
@@ -37,10 +39,14 @@ def test_repeats_and_scratch_overflow(oracle):
     rng = np.random.default_rng(31)
     box = 300.0
     a = _with_corners(rng, rng.uniform(0.0, box, (2992, 3)), box)
+    a2 = _with_corners(rng, rng.uniform(0.0, box, (2992, 3)), box)  # same box and size
     b = _with_corners(rng, rng.uniform(100.0, 200.0, (2992, 3)), box)  # same box, dense
     with api.Context(0) as ctx:
         ctx.set_bins(RMIN, RMAX, NBINS, NMU)
         _check(ctx, oracle, a, 1000, rng)
+        # other points, same configuration: the captured rebuild of the
+        # previous call is replayed
+        _check(ctx, oracle, a2, 1000, rng)
         _check(ctx, oracle, b, 1000, rng)
         _check(ctx, oracle, a, 1000, rng)
 
