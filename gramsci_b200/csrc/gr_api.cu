@@ -84,6 +84,7 @@ struct gr_ctx {
   DevBuf<double> hval;                   // fixed-point sums converted on the device
   DevBuf<int> qorder;                    // 4-clique root order (n) + its class counts
   SpecGraph spec_graph;                  // captured speculative rebuild (count_tri)
+  SpecGraph spec_index;                  // captured speculative index (gr_count_2pcf)
   DevBuf<double> cot, grad;              // adjoint inputs / output
   DevBuf<unsigned long long> gfix;       // adjoint fixed-point gradients (lo[n], hi[n])
   // batched regions: 0 none, 1 nsplit^3 subcubes, 2 region ids, 3 mocks
@@ -523,6 +524,124 @@ double uniform_product(double wg, double wr, int ng, int nr) {
 
 }  // namespace
 
+// Everything the speculative index and graph phases read from the host:
+// the catalogue's device pointers and sizes, the binning and precision, the
+// previous bounding box, and every buffer's address and capacity.
+static std::vector<unsigned long long> spec_key(const gr_ctx* c) {
+  std::vector<unsigned long long> k;
+  auto add = [&](auto v) {
+    unsigned long long u = 0;
+    std::memcpy(&u, &v, std::min(sizeof(v), sizeof(u)));
+    k.push_back(u);
+  };
+  auto buf = [&](const auto& b) {
+    add(b.p);
+    add(b.n);
+  };
+  add(c->xyz.p);
+  add(c->w.p);
+  add(c->has_buffer ? c->buffer.p : nullptr);
+  add(c->n);
+  add(c->n_data);
+  add(c->rmin);
+  add(c->rmax);
+  add(c->nbins);
+  add(c->nmu);
+  add(c->logbins);
+  add(c->precision);
+  const CellIndex& I = c->index;
+  add(I.have_prev);
+  add(I.prev_n);
+  add(I.prev_rmax);
+  add(I.prev_sub);
+  for (int i = 0; i < 7; ++i) add(I.prev_raw[i]);
+  buf(I.bbox_raw);
+  buf(I.bbox_prev);
+  buf(I.cell_count);
+  buf(I.key_orig);
+  buf(I.slot);
+  buf(I.tmp_perm);
+  buf(I.perm);
+  buf(I.cell_start);
+  buf(I.orig);
+  buf(I.cell_key);
+  buf(I.cell_start64);
+  buf(I.scan_tmp);
+  buf(I.pos4);
+  buf(I.posd);
+  buf(I.w);
+  buf(I.flags);
+  const UpperCSR& G = c->csr;
+  buf(G.deg_up);
+  buf(G.deg_full);
+  buf(G.work);
+  buf(G.scan_tmp);
+  buf(G.rstart);
+  buf(G.cbound);
+  buf(G.cbase);
+  buf(G.scratch);
+  buf(G.stats);
+  buf(G.ctl);
+  return k;
+}
+
+// Capture the speculative index and graph phases of the current
+// configuration (the call has just run them with success) on the context's
+// own stream.  A capture that fails leaves no graph: the next call runs the
+// phases eagerly.
+static std::vector<unsigned long long> spec_key(const gr_ctx* c, int sub, bool with_csr) {
+  std::vector<unsigned long long> k = spec_key(c);
+  k.push_back((unsigned long long)sub);
+  k.push_back(with_csr ? 1ull : 0ull);
+  return k;
+}
+
+// Capture the speculative index phase (grid choice `sub`) and, with_csr, the
+// graph phase of the current configuration into G (the call has just run
+// them with success) on the context's own stream.  A capture that fails
+// leaves no graph: the next call runs the phases eagerly.
+static void capture_spec_graph(gr_ctx* c, SpecGraph& G, int sub, bool with_csr) {
+  G.release();
+  // the configuration as this call leaves it (a successful speculative build
+  // changes none of it; buffers it grew have their new addresses)
+  const std::vector<unsigned long long> key = spec_key(c, sub, with_csr);
+  cudaStream_t user = c->user;
+  c->user = nullptr;  // build_index / build_csr enqueue on c->stream()
+  cudaStream_t s = c->own;
+  cudaGraph_t g[2] = {nullptr, nullptr};
+  cudaGraphExec_t e[2] = {nullptr, nullptr};
+  bool ok = true;
+  const int phases = with_csr ? 2 : 1;
+  for (int phase = 0; phase < phases && ok; ++phase) {
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      ok = false;
+      break;
+    }
+    try {
+      if (phase == 0)
+        build_index(c, true, sub);
+      else
+        build_csr(c, true);
+    } catch (...) {
+      ok = false;
+    }
+    if (cudaStreamEndCapture(s, &g[phase]) != cudaSuccess || !g[phase]) ok = false;
+    if (ok && cudaGraphInstantiate(&e[phase], g[phase], 0) != cudaSuccess) ok = false;
+  }
+  for (int k = 0; k < 2; ++k)
+    if (g[k]) cudaGraphDestroy(g[k]);
+  c->user = user;
+  cudaGetLastError();  // a failed capture leaves nothing behind
+  if (!ok || !c->index.speculated || spec_key(c, sub, with_csr) != key) {
+    for (int k = 0; k < 2; ++k)
+      if (e[k]) cudaGraphExecDestroy(e[k]);
+    return;
+  }
+  G.idx = e[0];
+  G.csr = e[1];
+  G.key = key;
+}
+
 extern "C" {
 
 const char* gr_version(void) { return "gramsci_b200 0.1 (sm_100a)"; }
@@ -557,6 +676,7 @@ int gr_destroy(gr_ctx* c) {
     if (c->bev[k]) cudaEventDestroy(c->bev[k]);
   c->regions.release_graph();
   c->spec_graph.release();
+  c->spec_index.release();
   if (c->own) cudaStreamDestroy(c->own);
   delete c;
   return GR_OK;
@@ -802,38 +922,73 @@ int gr_count_2pcf(gr_ctx* c, double* N2, double* N3, int64_t* counts, double* ca
   c->hcnt.reserve(nh);
   c->hfix.reserve(2 * nh);
   c->stats.reserve(8);
-  GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
-  if (!reuse_graph(c)) {
-    // dense catalogues: cells of rmax/2 and the tile sweep
-    int sub = 1;
-    if (c->autotune == 1) sub = 0;
-    if (c->autotune == 2 + kPairTile2) sub = 2;
-    build_index(c, false, sub);
-  }
-  GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
-  c->work.reserve(4);
-  const int variant = pick_pair2_variant(c, c->index.view(), weighted, fscale, c->hcnt.p,
-                                         c->hfix.p, c->stats.p, c->work.p, s);
-  c->last_variant = variant;
-  GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
-  GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nh, s));
-  GR_CUDA_TRY(cudaMemsetAsync(c->hfix.p, 0, sizeof(unsigned long long) * 2 * nh, s));
-  GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
-  launch_pair2(c->index.view(), c->P, weighted, c->hcnt.p, c->hfix.p, fscale, c->stats.p,
-               c->work.p, s, variant);
-  GR_CUDA_TRY(cudaEventRecord(c->ev[2], s));
-  // read-back in the pinned stage: counts (nh), fixed-point sums (2 nh), stats (8)
-  c->stage.reserve(3 * (size_t)nh + 8);
+  // read-back in the pinned stage: counts (nh), fixed-point sums (2 nh),
+  // stats (8), the speculative grid's bounding-box flag (1)
+  c->stage.reserve(3 * (size_t)nh + 9);
   unsigned long long* hc = c->stage.p;
   unsigned long long* hf = hc + nh;
   unsigned long long* st = hf + 2 * (size_t)nh;
+  unsigned long long* gflag = st + 8;
   std::vector<double> hs(nh, 0.0);
-  GR_CUDA_TRY(cudaMemcpyAsync(hc, c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
-  if (weighted)
-    GR_CUDA_TRY(cudaMemcpyAsync(hf, c->hfix.p, sizeof(unsigned long long) * 2 * nh, cudaMemcpyDeviceToHost, s));
-  GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(unsigned long long) * 8, cudaMemcpyDeviceToHost, s));
-  GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
-  GR_CUDA_TRY(cudaStreamSynchronize(s));
+  // dense catalogues: cells of rmax/2 and the tile sweep
+  int sub = 1;
+  if (c->autotune == 1) sub = 0;
+  if (c->autotune == 2 + kPairTile2) sub = 2;
+  // A catalogue seen before (or a new one while that has worked) is indexed
+  // on the grid of the last bounding box without waiting for the new one;
+  // a device flag read with the histograms repeats the call with waits when
+  // the box changed (as for the 3PCF).
+  const bool reuse = reuse_graph(c);
+  const bool can_spec =
+      !reuse && c->index.have_prev && (c->cat_gen == c->spec_gen || c->spec_new_ok);
+  int variant = 0;
+  bool replayed = false;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    const bool spec = can_spec && attempt == 0;
+    replayed = spec && c->spec_index.idx && spec_key(c, sub, false) == c->spec_index.key;
+    GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
+    if (!reuse) {
+      if (replayed) {
+        // the host state of the last identical build stands
+        GR_CUDA_TRY(cudaGraphLaunch(c->spec_index.idx, s));
+        c->csr_valid = false;
+      } else {
+        build_index(c, spec, sub);
+      }
+    }
+    GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+    c->work.reserve(4);
+    variant = pick_pair2_variant(c, c->index.view(), weighted, fscale, c->hcnt.p, c->hfix.p,
+                                 c->stats.p, c->work.p, s);
+    c->last_variant = variant;
+    GR_CUDA_TRY(cudaEventRecord(c->ev[1], s));
+    GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nh, s));
+    GR_CUDA_TRY(cudaMemsetAsync(c->hfix.p, 0, sizeof(unsigned long long) * 2 * nh, s));
+    GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
+    launch_pair2(c->index.view(), c->P, weighted, c->hcnt.p, c->hfix.p, fscale, c->stats.p,
+                 c->work.p, s, variant);
+    GR_CUDA_TRY(cudaEventRecord(c->ev[2], s));
+    GR_CUDA_TRY(cudaMemcpyAsync(hc, c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
+    if (weighted)
+      GR_CUDA_TRY(cudaMemcpyAsync(hf, c->hfix.p, sizeof(unsigned long long) * 2 * nh, cudaMemcpyDeviceToHost, s));
+    GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(unsigned long long) * 8, cudaMemcpyDeviceToHost, s));
+    *gflag = 0;
+    const bool speculated = spec && c->index.speculated;
+    if (speculated)
+      GR_CUDA_TRY(cudaMemcpyAsync(gflag, c->index.mismatch_flag(), sizeof(unsigned long long),
+                                  cudaMemcpyDeviceToHost, s));
+    GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
+    GR_CUDA_TRY(cudaStreamSynchronize(s));
+    if (speculated && *gflag != 0) {  // the bounding box changed: repeat with waits
+      if (c->cat_gen != c->spec_gen) c->spec_new_ok = false;
+      continue;
+    }
+    // a speculative index that held: kept as a graph for the next call of
+    // the same configuration
+    if (speculated && !replayed) capture_spec_graph(c, c->spec_index, sub, false);
+    break;
+  }
+  if (!reuse) c->spec_gen = c->cat_gen;
   if (weighted)
     for (int k = 0; k < nh; ++k) hs[k] = fix_value(hf[k], hf[nh + k], fscale);
   if (!weighted) {
@@ -901,112 +1056,6 @@ static int tri_geometric(const gr_ctx* c) {
   return c->clique_mode == 1 ? 0 : 1;
 }
 
-// Everything the speculative index and graph phases read from the host:
-// the catalogue's device pointers and sizes, the binning and precision, the
-// previous bounding box, and every buffer's address and capacity.
-static std::vector<unsigned long long> spec_key(const gr_ctx* c) {
-  std::vector<unsigned long long> k;
-  auto add = [&](auto v) {
-    unsigned long long u = 0;
-    std::memcpy(&u, &v, std::min(sizeof(v), sizeof(u)));
-    k.push_back(u);
-  };
-  auto buf = [&](const auto& b) {
-    add(b.p);
-    add(b.n);
-  };
-  add(c->xyz.p);
-  add(c->w.p);
-  add(c->has_buffer ? c->buffer.p : nullptr);
-  add(c->n);
-  add(c->n_data);
-  add(c->rmin);
-  add(c->rmax);
-  add(c->nbins);
-  add(c->nmu);
-  add(c->logbins);
-  add(c->precision);
-  const CellIndex& I = c->index;
-  add(I.have_prev);
-  add(I.prev_n);
-  add(I.prev_rmax);
-  add(I.prev_sub);
-  for (int i = 0; i < 7; ++i) add(I.prev_raw[i]);
-  buf(I.bbox_raw);
-  buf(I.bbox_prev);
-  buf(I.cell_count);
-  buf(I.key_orig);
-  buf(I.slot);
-  buf(I.tmp_perm);
-  buf(I.perm);
-  buf(I.cell_start);
-  buf(I.orig);
-  buf(I.cell_key);
-  buf(I.cell_start64);
-  buf(I.scan_tmp);
-  buf(I.pos4);
-  buf(I.posd);
-  buf(I.w);
-  buf(I.flags);
-  const UpperCSR& G = c->csr;
-  buf(G.deg_up);
-  buf(G.deg_full);
-  buf(G.work);
-  buf(G.scan_tmp);
-  buf(G.rstart);
-  buf(G.cbound);
-  buf(G.cbase);
-  buf(G.scratch);
-  buf(G.stats);
-  buf(G.ctl);
-  return k;
-}
-
-// Capture the speculative index and graph phases of the current
-// configuration (the call has just run them with success) on the context's
-// own stream.  A capture that fails leaves no graph: the next call runs the
-// phases eagerly.
-static void capture_spec_graph(gr_ctx* c) {
-  c->spec_graph.release();
-  // the configuration as this call leaves it (a successful speculative build
-  // changes none of it; buffers it grew have their new addresses)
-  const std::vector<unsigned long long> key = spec_key(c);
-  cudaStream_t user = c->user;
-  c->user = nullptr;  // build_index / build_csr enqueue on c->stream()
-  cudaStream_t s = c->own;
-  cudaGraph_t g[2] = {nullptr, nullptr};
-  cudaGraphExec_t e[2] = {nullptr, nullptr};
-  bool ok = true;
-  for (int phase = 0; phase < 2 && ok; ++phase) {
-    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
-      ok = false;
-      break;
-    }
-    try {
-      if (phase == 0)
-        build_index(c, true);
-      else
-        build_csr(c, true);
-    } catch (...) {
-      ok = false;
-    }
-    if (cudaStreamEndCapture(s, &g[phase]) != cudaSuccess || !g[phase]) ok = false;
-    if (ok && cudaGraphInstantiate(&e[phase], g[phase], 0) != cudaSuccess) ok = false;
-  }
-  for (int k = 0; k < 2; ++k)
-    if (g[k]) cudaGraphDestroy(g[k]);
-  c->user = user;
-  cudaGetLastError();  // a failed capture leaves nothing behind
-  if (!ok || !c->index.speculated || spec_key(c) != key) {
-    for (int k = 0; k < 2; ++k)
-      if (e[k]) cudaGraphExecDestroy(e[k]);
-    return;
-  }
-  c->spec_graph.idx = e[0];
-  c->spec_graph.csr = e[1];
-  c->spec_graph.key = key;
-}
-
 static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* counts, double* catsum) {
   GR_API_BEGIN(c)
   require_ready(c);
@@ -1055,8 +1104,8 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
     const bool spec = can_spec && attempt == 0;
     bool replay = false;
     if (spec) {
-      key = spec_key(c);
-      replay = c->spec_graph.idx && key == c->spec_graph.key;
+      key = spec_key(c, 1, true);
+      replay = c->spec_graph.idx && c->spec_graph.csr && key == c->spec_graph.key;
     }
     replayed = replay;
     GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
@@ -1131,7 +1180,7 @@ static int count_tri(gr_ctx* c, bool equi, double* N2, double* N3, int64_t* coun
       // a speculative build that needed no second pass: keep it as graphs
       // for the next call of the same configuration
       if (!replayed) {
-        capture_spec_graph(c);
+        capture_spec_graph(c, c->spec_graph, 1, true);
         c->csr_valid = true;
         c->csr.settle(gctl, gsts);
       }

@@ -208,8 +208,10 @@ void CellIndex::build(const double* d_xyz, const double* d_w, const int* d_buffe
   }
   GR_CHECK_LAUNCH();
   unsigned long long h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  speculated = speculate && !auto_sub && have_prev && prev_n == n && prev_rmax == rmax &&
-               prev_sub == sub;
+  // an automatic choice of sub decides from the bounding box, so it speculates
+  // on the previous build's box like the grid does
+  speculated = speculate && have_prev && prev_n == n && prev_rmax == rmax &&
+               prev_auto == auto_sub && prev_sub == sub;
   if (speculated) {
     std::memcpy(h, prev_raw, sizeof(prev_raw));
     bbox_check_kernel<<<1, 32, 0, s>>>(bbox_raw.p, bbox_prev.p);
@@ -223,6 +225,7 @@ void CellIndex::build(const double* d_xyz, const double* d_w, const int* d_buffe
     prev_n = n;
     prev_rmax = rmax;
     prev_sub = sub;
+    prev_auto = auto_sub;
     have_prev = true;
     GR_CUDA_TRY(cudaMemcpyAsync(bbox_prev.p, prev_raw, sizeof(prev_raw), cudaMemcpyHostToDevice, s));
     GR_CUDA_TRY(cudaMemsetAsync(bbox_prev.p + 7, 0, sizeof(unsigned long long), s));

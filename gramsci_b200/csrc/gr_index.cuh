@@ -27,6 +27,7 @@ struct CellIndex {
   int64_t prev_n = -1;
   double prev_rmax = 0.0;
   int prev_sub = 0;
+  bool prev_auto = false;  // the previous build chose sub itself
   unsigned long long prev_raw[7] = {0, 0, 0, 0, 0, 0, 0};
   DevBuf<unsigned long long> bbox_prev;  // previous raw bounding box [0..6], mismatch flag [7]
   DevBuf<int> cell_count, key_orig, slot, tmp_perm, perm, cell_start, orig, cell_key;

@@ -1,4 +1,4 @@
-"""Rebuilds without host waits (3PCF): a count of a catalogue seen before
+"""Rebuilds without host waits (3PCF and 2PCF): a count of a catalogue seen before
 takes the grid of the last bounding box and fills the graph in the scratch
 area as it is, and a device flag sends the call round again with waits when
 the bounding box changed or the scratch area was too small.  Every case is
@@ -60,3 +60,32 @@ def test_changed_bounding_box(oracle):
         _check(ctx, oracle, a, 1000, rng)
         _check(ctx, oracle, c, 1000, rng)
         _check(ctx, oracle, a, 1000, rng)
+
+
+def _check2(ctx, oracle, xyz, n_data, rng):
+    n = len(xyz)
+    w = catalogs.normalise(rng.lognormal(0, 0.3, n), n_data, n - n_data)
+    ctx.set_catalog(xyz, w, n_data)
+    ref = oracle.Graph(xyz, RMIN, RMAX, NBINS, NMU).pcf2(w, n_data)
+    for _ in range(2):
+        got = ctx.count_2pcf()
+        assert np.array_equal(got["counts"], ref["counts"])
+        scale = np.abs(ref["catsum"]).max()
+        assert np.all(np.abs(got["catsum"] - ref["catsum"]) <= 1e-12 * scale)
+    assert int(ref["counts"].sum()) > 0
+
+
+def test_2pcf_rebuilds(oracle):
+    """The 2PCF takes the grid of the last bounding box too: repeats, another
+    catalogue of the same size and box (the captured index replayed), a
+    changed box, on a sparse grid and on a dense one (cells of rmax/2)."""
+    rng = np.random.default_rng(33)
+    a = _with_corners(rng, rng.uniform(0.0, 300.0, (2992, 3)), 300.0)
+    a2 = _with_corners(rng, rng.uniform(0.0, 300.0, (2992, 3)), 300.0)
+    c = rng.uniform(0.0, 360.0, (3000, 3))
+    d = _with_corners(rng, rng.uniform(0.0, 150.0, (19992, 3)), 150.0)
+    d2 = _with_corners(rng, rng.uniform(0.0, 150.0, (19992, 3)), 150.0)
+    with api.Context(0) as ctx:
+        ctx.set_bins(RMIN, RMAX, NBINS, NMU)
+        for xyz in (a, a2, c, a, d, d2, d):
+            _check2(ctx, oracle, xyz, len(xyz) // 3, rng)
