@@ -96,7 +96,12 @@ int gr_destroy(gr_ctx* ctx);
 const char* gr_last_error(const gr_ctx* ctx);
 
 /* Use a caller-owned CUDA stream (cudaStream_t passed as void*); NULL
- * restores the context's own stream. */
+ * restores the context's own stream.  Count calls wait on the stream for
+ * their results, so they cannot be captured into a caller's CUDA graph.
+ * Internally, a 2PCF or 3PCF count of a catalogue of the same size, box and
+ * binning as the previous one replays that call's index (and graph)
+ * phases as a CUDA graph the library captured on the context's own stream;
+ * the replay is launched on the stream in use. */
 int gr_set_stream(gr_ctx* ctx, void* stream);
 
 /* Catalogue.  Replaces read_files_2's result (src/gramsci.F90:1364-1396):
