@@ -460,6 +460,7 @@ def run_ours(args):
         "data": "synthetic (seeded Neyman-Scott galaxies + uniform randoms)",
         "config": c2_config(cat, sp, args.scale, world, st["tuples"], st["rooted"], st["n_edges"]),
         "stats": {"precision": args.precision, "fp64_rechecks": st["fp64_rechecks"],
+                  "fp64_recheck_fraction": st["fp64_rechecks"] / max(1, st["candidates"]),
                   "upper_edges": st["upper_edges"], "probes": st["probes"],
                   "phase_ms": {"index": st["ms_index"], "graph": st["ms_graph"],
                                "query": st["ms_query"]}},
@@ -530,7 +531,7 @@ def sub_pcf2(args, stream, flush):
     the CPU restatement."""
     import torch
 
-    from gramsci_b200 import api
+    from gramsci_b200 import api, roofline
 
     name = "c1_2pcf"
     cat, w, sp = make_catalogue(name, args.scale)
@@ -555,7 +556,13 @@ def sub_pcf2(args, stream, flush):
            "e2e": {"value": pairs / (e2e_ms / 1e3), "unit": "pairs/s",
                    "h2d_bytes_per_step": int(cat.xyz.nbytes + w.nbytes),
                    "d2h_bytes_per_step": int(sum(v.nbytes for v in got.values()))},
-           "clocks": ck.clocks, "phase_ms": {"index": st["ms_index"], "query": st["ms_query"]}}
+           "clocks": ck.clocks, "phase_ms": {"index": st["ms_index"], "query": st["ms_query"]},
+           "fp64_recheck_fraction": st["fp64_rechecks"] / max(1, st["candidates"])}
+    # the pair sweep's FP32 arithmetic over its own device time
+    rec["roofline"] = {"kernel": "pair sweep", "ms": st["ms_query"],
+                       "fp32": roofline.fp32_binning_roofline(
+                           int(got["counts"].sum()), sp["nmu"], st["ms_query"], ck.clocks.get("sm_mhz"),
+                           torch.cuda.get_device_properties(0).multi_processor_count)}
     ctx.close()
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -757,7 +764,10 @@ def sub_batched(args, stream, flush):
     rf = {"kernel": "pair2_tile_kernel", "ms": tb, "ms_is": "whole batched call"}
     rf["issue"] = roofline.issue_roofline(prof, st["candidates"], tb, ck.clocks.get("sm_mhz"), n_sm)
     rf["atomics"] = roofline.atomic_roofline(prof, st["candidates"], tb, ck.clocks.get("sm_mhz"), n_sm)
+    rf["fp32"] = roofline.fp32_binning_roofline(rec["rooted"], sp["nmu"], tb, ck.clocks.get("sm_mhz"),
+                                                n_sm)
     rec["roofline"] = rf
+    rec["fp64_recheck_fraction"] = st["fp64_rechecks"] / max(1, st["candidates"])
     ctx.close()
     del reg_dev, xyz_d, w_d
     if not args.no_cpu_baseline:

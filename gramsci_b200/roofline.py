@@ -140,3 +140,20 @@ def profiled_traffic(kernel, scale, workload="c2"):
         return float(d["dram_bytes_read"]) + float(d["dram_bytes_write"])
     except Exception:
         return None
+
+
+def fp32_binning_roofline(binned_directed_pairs, nmu, ms, sm_mhz, n_sm):
+    """FP32 arithmetic of 2PCF binning against the chip's nominal FP32 rate:
+    per binned directed pair 11 operations without mu bins (3 subtractions,
+    5 for the squared separation, a square root, 2 for the bin) and 27 with
+    them (16 more for the midpoint, dot product, norms and reciprocal square
+    root), an FMA counted as 2; the peak is 128 FP32 lanes x 2 per SM per
+    cycle at the sampled SM clock.  Candidate pairs outside the range are
+    not credited.  None without a clock reading."""
+    if not sm_mhz or not ms:
+        return None
+    f = 11 if nmu <= 1 else 27
+    achieved = binned_directed_pairs * f / (ms * 1e-3) / 1e12
+    peak = n_sm * 128 * 2 * sm_mhz * 1e6 / 1e12
+    return {"unit": "TFLOP/s", "achieved": achieved, "peak": peak, "frac": achieved / peak,
+            "flop_per_binned_pair": f, "peak_kind": "nominal FP32 FMA rate at the sampled clock"}

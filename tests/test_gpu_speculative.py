@@ -89,3 +89,30 @@ def test_2pcf_rebuilds(oracle):
         ctx.set_bins(RMIN, RMAX, NBINS, NMU)
         for xyz in (a, a2, c, a, d, d2, d):
             _check2(ctx, oracle, xyz, len(xyz) // 3, rng)
+
+
+def test_mixed_calls_keep_their_rebuilds_apart(oracle):
+    """2PCF and 3PCF counts, bin and precision changes interleaved on one
+    context (each kind keeps its own captured rebuild, keyed by what it
+    reads): every result against the oracle."""
+    rng = np.random.default_rng(34)
+    a = _with_corners(rng, rng.uniform(0.0, 300.0, (2992, 3)), 300.0)
+    b = _with_corners(rng, rng.uniform(0.0, 300.0, (2992, 3)), 300.0)
+    n_data = 1000
+    with api.Context(0) as ctx:
+        for xyz, bins, prec in ((a, (RMIN, RMAX, NBINS, NMU), "f32"),
+                                (b, (RMIN, RMAX, NBINS, NMU), "f32"),
+                                (b, (4.0, 20.0, 6, 3), "f32"),
+                                (a, (4.0, 20.0, 6, 3), "f64"),
+                                (a, (RMIN, RMAX, NBINS, NMU), "f32")):
+            ctx.set_precision(prec)
+            ctx.set_bins(*bins)
+            w = catalogs.normalise(rng.lognormal(0, 0.3, len(xyz)), n_data, len(xyz) - n_data)
+            ctx.set_catalog(xyz, w, n_data)
+            G = oracle.Graph(xyz, *bins)
+            ref2, ref3 = G.pcf2(w, n_data), G.pcf3(w, n_data)
+            for _ in range(2):
+                for got, ref in ((ctx.count_3pcf(), ref3), (ctx.count_2pcf(), ref2)):
+                    assert np.array_equal(got["counts"], ref["counts"])
+                    scale = np.abs(ref["catsum"]).max()
+                    assert np.all(np.abs(got["catsum"] - ref["catsum"]) <= 1e-12 * scale)

@@ -83,3 +83,15 @@ def test_profiled_traffic_from_committed_summary(kernel, workload):
     # the summaries hold full-size captures only
     assert roofline.profiled_traffic(kernel, 0.5, workload) is None
     assert roofline.profiled_traffic(kernel, 1.0, "nonexistent") is None
+
+
+def test_fp32_binning_roofline():
+    from gramsci_b200 import roofline
+    # 1e9 binned directed pairs with mu bins in 1 ms on 148 SMs at 1965 MHz
+    r = roofline.fp32_binning_roofline(1e9, 10, 1.0, 1965.0, 148)
+    assert r["flop_per_binned_pair"] == 27
+    assert abs(r["achieved"] - 27.0) < 1e-9
+    assert abs(r["peak"] - 148 * 256 * 1.965e9 / 1e12) < 1e-9
+    assert abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-12
+    assert roofline.fp32_binning_roofline(1e9, 1, 1.0, 1965.0, 148)["flop_per_binned_pair"] == 11
+    assert roofline.fp32_binning_roofline(1e9, 1, 1.0, None, 148) is None
