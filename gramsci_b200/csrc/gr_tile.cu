@@ -224,6 +224,13 @@ __global__ void __launch_bounds__(kTileThreads, (ADJ && SUB == 2) ? 4 : GR_TILE_
       const float2 npx = make_float2(-pi.x, -pi.x), npy = make_float2(-pi.y, -pi.y),
                    npz = make_float2(-pi.z, -pi.z), pwb2 = make_float2(pwb, pwb);
       const float hi = P.rmax2_hi, lo = P.rmin2_lo;
+      // one compare per candidate: |d2 - mid| < half, widened by far more
+      // than the subtraction's rounding (2^-24 of rmax2_hi), accepts every
+      // d2 in (lo, hi); the few pairs just outside the band that it also
+      // accepts are rejected by the exact classification of the binning
+      const float midv = 0.5f * (hi + lo);
+      const float halfv = __int_as_float(__float_as_int(0.5f * (hi - lo) + 1e-6f * fabsf(hi)) + 4);
+      const float2 nmid2 = make_float2(-midv, -midv);
       const double pwbd = pwb;
       __syncwarp();
       int kr = 0;  // range of the tile's first candidate (warp-uniform)
@@ -297,8 +304,9 @@ __global__ void __launch_bounds__(kTileThreads, (ADJ && SUB == 2) ? 4 : GR_TILE_
             d2 = __ffma2_rn(dy, dy, d2);
             d2 = __ffma2_rn(dz, dz, d2);
             d2 = __ffma2_rn(cw, pwb2, d2);
-            if (d2.x < hi && d2.x > lo) m |= 1u << j;
-            if (d2.y < hi && d2.y > lo) m |= 2u << j;
+            const float2 dm = __fadd2_rn(d2, nmid2);
+            if (fabsf(dm.x) < halfv) m |= 1u << j;
+            if (fabsf(dm.y) < halfv) m |= 2u << j;
           }
           // the first tile holds own-cell candidates with labels at or
           // below some lanes' roots
