@@ -316,12 +316,8 @@ __device__ __forceinline__ int quad_contrib(const QuadCtx& X, const QVerts& V, c
          quad_root<WEIGHTED, SHC, 2>(X, V, packed, rndm, nr) + quad_root<WEIGHTED, SHC, 3>(X, V, packed, rndm, nr);
 }
 
-// Compact form of quad_contrib: the four roots and the six terms are loops
-// that are not unrolled, so the code of the (long) weighted updates appears
-// once; the clique's id order, flags and roles are packed into registers
-// (two bits per vertex index, eight per flag byte) so that runtime indices
-// need no local memory.
-// Vertex indices 0..3 in ascending catalogue id, two bits each.
+// Vertex indices 0..3 in ascending catalogue id, two bits each (the
+// register sorting network the flattened drain and the gradient use).
 __device__ __forceinline__ unsigned id_order(const QVerts& V) {
   int g0 = V.og[0], g1 = V.og[1], g2 = V.og[2], g3 = V.og[3];
   unsigned a0 = 0, a1 = 1, a2 = 2, a3 = 3;
@@ -339,68 +335,6 @@ __device__ __forceinline__ unsigned id_order(const QVerts& V) {
   return a0 | (a1 << 2) | (a2 << 4) | (a3 << 6);
 }
 
-template <bool WEIGHTED, bool SHC>
-__device__ __forceinline__ int quad_root_rt(const QuadCtx& X, const QVerts& V,
-                                            unsigned long long packed, unsigned rndm, int nr,
-                                            int R, unsigned perm, unsigned flw) {
-  const unsigned fr = flw >> (8 * R);
-  if (fr & FLAG_BUFFER) return 0;
-  if (!(fr & kFlagDeg4)) return 0;
-  // the other three in id order: drop R's field from the id order
-  int pos = 0;
-#pragma unroll
-  for (int i = 1; i < 4; ++i)
-    if ((int)((perm >> (2 * i)) & 3u) == R) pos = i;
-  const unsigned lowm = (1u << (2 * pos)) - 1u;
-  const unsigned oth = (perm & lowm) | ((perm >> (2 * pos + 2)) << (2 * pos));
-  const int u0 = (int)(oth & 3u), u1 = (int)((oth >> 2) & 3u), u2 = (int)((oth >> 4) & 3u);
-  const int b1 = qbin(packed, R, u0), b2 = qbin(packed, u0, u1), b3 = qbin(packed, u1, u2),
-            b4 = qbin(packed, R, u2);
-  if (!(b1 <= b2 && b2 <= b3 && b3 <= b4)) return 0;
-  const int nb2 = X.nbins + 2;
-  const int cfg = 1 + (X.F[b1] - X.F[1]) + (X.F[nb2 + b2] - X.F[nb2 + b1]) +
-                  (X.F[2 * nb2 + b3] - X.F[2 * nb2 + b2]) + (X.F[3 * nb2 + b4] - X.F[3 * nb2 + b3]);
-  const int d1 = qbin(packed, R, u1), d2 = qbin(packed, u0, u2);
-  const int kk = (cfg - 1) + X.ncfg * ((d1 - 1) + X.nbins * (d2 - 1));
-  qcount<SHC>(X, kk + X.nbin * nr);
-  if (WEIGHTED)
-    qfix(X, &X.fix[kk + X.nbin * nr], &X.fix[kk + X.nbin * (nr + 5)],
-            ((qsel(R, V) * qsel(u0, V)) * qsel(u1, V)) * qsel(u2, V), X.fscale);
-  const unsigned rp = (unsigned)R | ((unsigned)u0 << 2) | ((unsigned)u1 << 4) | ((unsigned)u2 << 6);
-#pragma unroll 1
-  for (int tt = 0; tt < 6; ++tt) {
-    const int ga = (int)((rp >> (2 * term_gate(tt))) & 3u);
-    if (!((rndm >> ga) & 1u)) continue;
-    const int u = (int)((rp >> (2 * term_pu(tt))) & 3u), vv = (int)((rp >> (2 * term_pv(tt))) & 3u);
-    const int npr = (int)((rndm >> u) & 1u) + (int)((rndm >> vv) & 1u);
-    const int kt = kk + X.nbin * tt;
-    qdcount<SHC>(X, kt + X.nbin * 6 * npr);
-    if (WEIGHTED)
-      qfix(X, &X.dfix[kt + X.nbin * 6 * npr], &X.dfix[kt + X.nbin * 6 * npr + X.dhi],
-              qsel(u, V) * qsel(vv, V), X.dscale);
-  }
-  return 1;
-}
-
-template <bool WEIGHTED, bool SHC>
-__device__ __forceinline__ int quad_contrib_c(const QuadCtx& X, const QVerts& V, const uint32_t m[6]) {
-  unsigned long long packed = 0;
-#pragma unroll
-  for (int e = 0; e < 6; ++e) packed |= (unsigned long long)meta_bin(m[e]) << (8 * e);
-  unsigned rndm = 0, flw = 0;
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    rndm |= (unsigned)(V.fl[k] & FLAG_RANDOM) << k;
-    flw |= (unsigned)V.fl[k] << (8 * k);
-  }
-  const int nr = __popc(rndm);
-  const unsigned perm = id_order(V);
-  int n = 0;
-#pragma unroll 1
-  for (int R = 0; R < 4; ++R) n += quad_root_rt<WEIGHTED, SHC>(X, V, packed, rndm, nr, R, perm, flw);
-  return n;
-}
-
 // Gradient of the cotangent-weighted sums with respect to the four vertex
 // weights of one clique (g[v] = d/dw_v, vertices as in quad_contrib).  The
 // sums are multilinear: a 4-product contributes its cotangent times the
@@ -408,7 +342,8 @@ __device__ __forceinline__ int quad_contrib_c(const QuadCtx& X, const QVerts& V,
 // partner's weight.  The valid roots' cotangents are gathered into one
 // 4-product coefficient c4 and one coefficient per clique edge D[e] (edges
 // 0 (0,1) 1 (0,2) 2 (0,3) 3 (1,2) 4 (1,3) 5 (2,3)); the roots are a loop
-// that is not unrolled, as in quad_contrib_c.
+// that is not unrolled (fully unrolled, the gradient code overflowed the
+// instruction cache).
 __device__ __forceinline__ int quad_grad_c(const QuadCtx& X, const QVerts& V, const uint32_t m[6],
                                            double g[4]) {
   unsigned long long packed = 0;
@@ -524,7 +459,7 @@ __device__ __forceinline__ void quad_setup(QuadCtx& X, const QuadParams& Q, unsi
 // gives each pair's lane with no search, and the vertex weights are read
 // from the staged weights (s_w at the positions packed 10 bits each in vpos
 // for vertices 1..3; vertex 0 is the warp's root, weight wp).  Products and
-// histogram indices are those of quad_root_rt, so the sums are identical.
+// histogram indices are those of quad_root.
 // Returns this lane's number of rooted contributions.
 template <bool SHC>
 __device__ __forceinline__ int quad_contrib_flat(const QuadCtx& X, const QVerts& V,
@@ -625,7 +560,7 @@ template <bool WEIGHTED, bool SHC, bool ADJ, bool COMPACT, bool TETRA>
 __device__ __forceinline__ int quad_emit(const QuadCtx& X, const QVerts& V, const uint32_t m[6],
                                          double gscale, Fix128& racc, unsigned long long* s_glo,
                                          unsigned long long* s_ghi, int ya, int yb, int yd) {
-  if (ADJ) {
+  if constexpr (ADJ) {
     double g[4];
     const int nroot = quad_grad_c(X, V, m, g);
     if (nroot) {
@@ -635,9 +570,12 @@ __device__ __forceinline__ int quad_emit(const QuadCtx& X, const QVerts& V, cons
       fix_add(&s_glo[yd], &s_ghi[yd], g[3], gscale);
     }
     return nroot;
+  } else if constexpr (TETRA) {
+    return tetra_contrib<WEIGHTED, SHC>(X, V, m);
+  } else {
+    static_assert(!(WEIGHTED && COMPACT), "weighted 4PCF sums take the flattened drain");
+    return quad_contrib<WEIGHTED, SHC>(X, V, m);
   }
-  if (TETRA) return tetra_contrib<WEIGHTED, SHC>(X, V, m);
-  return COMPACT ? quad_contrib_c<WEIGHTED, SHC>(X, V, m) : quad_contrib<WEIGHTED, SHC>(X, V, m);
 }
 
 // SHC: integer counts in block-private 32-bit shared-memory counters,
@@ -645,8 +583,8 @@ __device__ __forceinline__ int quad_emit(const QuadCtx& X, const QVerts& V, cons
 // ADJ: instead of the histograms, the weight gradient (g_lo / g_hi, label
 // order, scale gscale) of sum(c2 N2) + sum(c3 N3) + sum(cN discN) +
 // sum(cR discR), cot = [c2 | c3 | cN | cR].
-// COMPACT: the 4PCF contributions through quad_contrib_c (loops over roots
-// and terms) instead of the unrolled quad_contrib.
+// COMPACT: the weighted 4PCF sums through the flattened drain
+// (quad_contrib_flat) instead of the unrolled per-clique quad_contrib.
 // TETRA: the -tetra counts (query_graph_tetrahedron) instead of the 4PCF;
 // a template argument so that each kernel holds the code of one form only.
 template <bool WEIGHTED, bool SHC, bool ADJ, bool COMPACT, bool TETRA>
@@ -829,7 +767,7 @@ __global__ void __launch_bounds__((WEIGHTED || ADJ ? kQuadMaxWarps : kQuadMaxWar
           m[5] = mbd;
         }
         int nroot;
-        if (FLAT)
+        if constexpr (FLAT)
           nroot = quad_contrib_flat<SHC>(X, V, m, act,
                                          (unsigned)x | ((unsigned)yb << 10) | ((unsigned)yd << 20),
                                          s_w, wp);
@@ -1123,7 +1061,7 @@ __global__ void __launch_bounds__((ADJ ? kQuadMaxWarps : (WEIGHTED ? kQuadGWarps
         m[5] = pack_meta(byz, 1, 1);
       }
       int nroot;
-      if (FLAT)
+      if constexpr (FLAT)
         nroot = quad_contrib_flat<SHC>(X, V, m, act,
                                        (unsigned)x | ((unsigned)y << 10) | ((unsigned)z << 20), s_w,
                                        wp);
