@@ -223,6 +223,16 @@ __device__ __forceinline__ int classify_f32(const float4 pi, const float4 pj, co
   return 1;
 }
 
+// Square root for the inversion of the triangular pair index of k members
+// (x = floor((2k - 1 - sqrt((2k - 1)^2 - 8t)) / 2), followed by one
+// adjustment each way): disc * rsqrtf(disc), within about 3e-7 relative of
+// the root.  The adjustments absorb an estimate off by one; checked on the
+// CPU for every pair of every k up to 1024 with the root perturbed by
+// 4e-7 either way.
+__device__ __forceinline__ float pair_index_sqrt(float disc) {
+  return disc > 0.0f ? disc * rsqrtf(disc) : 0.0f;
+}
+
 // Both points of a pair are buffer points (pos4.w = 1 marks them): the pair
 // has no root and adds nothing to any 2PCF histogram or gradient, so the
 // pair sweeps skip it before testing it.  (The neighbour graph keeps such

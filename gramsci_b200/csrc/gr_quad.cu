@@ -48,7 +48,9 @@ constexpr uint8_t kFlagDeg4 = 4;    // staged flag: full row length > 3 (a refer
 // one warp otherwise ends the launch alone (measured on the 4PCF workload:
 // one SM busy for 8.0M cycles while the others were done after 5.1M).  The
 // split roots are the longest ones, at least kSplitRow long, few enough that
-// their items fill at most an eighth of the launch's warps.
+// their items fill at most a quarter of the launch's warps (measured on the
+// 4PCF workload, unit weights: 2.98 ms at an eighth, 2.64 ms at a quarter,
+// 2.62 ms at a half; 16 items per root: 3.01 ms).
 constexpr int kSplitRow = 32;
 constexpr int kSplitParts = 8;
 
@@ -72,7 +74,7 @@ __device__ __forceinline__ bool quad_item(const QuadParams& Q, int n, int item, 
 __device__ __forceinline__ int quad_split_parts(const QuadParams& Q, int& nh) {
   nh = 0;
   if (!Q.order || !Q.above || Q.nclass <= kSplitRow) return 1;
-  const int limit = (int)gridDim.x * (int)(blockDim.x >> 5) / (8 * kSplitParts);
+  const int limit = (int)gridDim.x * (int)(blockDim.x >> 5) / (4 * kSplitParts);
   // above[] does not increase with b: the smallest b >= kSplitRow - 1 with
   // above[b] <= limit
   int lo = kSplitRow - 1, hi = Q.nclass - 1;
@@ -1000,7 +1002,7 @@ __global__ void __launch_bounds__((ADJ ? kQuadMaxWarps : (WEIGHTED ? kQuadGWarps
     auto pair_of = [&](int t, int& x, int& y) {
       // x: the largest row with x (2k - 1 - x) / 2 <= t pairs before it
       const float disc = (float)(k2m1 * k2m1) - 8.0f * (float)t;
-      x = (int)(0.5f * ((float)k2m1 - sqrtf(fmaxf(disc, 0.0f))));
+      x = (int)(0.5f * ((float)k2m1 - pair_index_sqrt(disc)));
       x = max(0, min(x, k - 2));
       if ((x + 1) * (k2m1 - x - 1) / 2 <= t) ++x;
       if (x * (k2m1 - x) / 2 > t) --x;

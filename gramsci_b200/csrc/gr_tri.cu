@@ -430,7 +430,7 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
             if (t < npair) {
               // x: the largest row with x (2k - 1 - x) / 2 <= t pairs before it
               const float disc = (float)(k2m1 * k2m1) - 8.0f * (float)t;
-              x = (int)(0.5f * ((float)k2m1 - sqrtf(fmaxf(disc, 0.0f))));
+              x = (int)(0.5f * ((float)k2m1 - pair_index_sqrt(disc)));
               x = max(0, min(x, k - 2));
               if ((x + 1) * (k2m1 - x - 1) / 2 <= t) ++x;
               if (x * (k2m1 - x) / 2 > t) --x;
