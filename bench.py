@@ -49,6 +49,7 @@ import subprocess
 import sys
 import threading
 import time
+import types
 
 import numpy as np
 
@@ -71,6 +72,10 @@ def parse(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-sub-records", action="store_true",
                     help="headline line only (no pcf2 / quad / batched / adjoint sub-records)")
+    ap.add_argument("--shard", action="store_true",
+                    help="one catalogue over the ranks: slabs with Rmax halos and one all-reduce "
+                         "of the histograms per step (strong scaling); default: one independent "
+                         "mock per rank (weak scaling)")
     ap.add_argument("--workload", default="c2_3pcf",
                     choices=["c2_3pcf", "c1_2pcf", "c3_4pcf", "c4_batched", "c5_adjoint"],
                     help="c2_3pcf is the headline line; the others print one sub-record alone")
@@ -108,8 +113,10 @@ def make_catalogue(name, scale, seed=None):
     return cat, w, catalogs.WORKLOADS[name]
 
 
-def c2_config(cat, sp, scale, world, triangles, rooted, edges):
+def c2_config(cat, sp, scale, world, triangles, rooted, edges, parallelism=None):
     """The headline line's config: the same keys and values in both arms."""
+    if parallelism is None:
+        parallelism = f"replicas{world}" if world > 1 else "single"
     return {
         "workload": f"{WORKLOAD}: Neyman-Scott 3PCF, {cat.n_data} galaxies + {cat.n_rand} randoms, "
                     f"box {cat.meta['box']:.0f}, rmin {sp['rmin']}, rmax {sp['rmax']}, "
@@ -117,7 +124,7 @@ def c2_config(cat, sp, scale, world, triangles, rooted, edges):
         "n_points": int(cat.n),
         "scale": scale,
         "l2": L2_NOTE,
-        "parallelism": f"replicas{world}" if world > 1 else "single",
+        "parallelism": parallelism,
         "triangles_per_step": int(triangles),
         "rooted_per_step": int(rooted),
         "edges": int(edges),
@@ -332,17 +339,20 @@ def timed(fn, steps, stream, flush=None):
     return ms
 
 
-def e2e_loop(ctx, cat, w, count, stream, flush, steps):
-    """End to end through the C ABI: pinned host catalogue -> device, the
-    count, results read back; the first two calls are warm-up."""
+def e2e_loop(ctx, cat, w, count, stream, flush, steps, buffer=None):
+    """End to end through the C ABI: pinned host catalogue (and buffer
+    flags, when given) -> device, the count, results read back; the first
+    two calls are warm-up."""
     import torch
 
     xyz_h = torch.from_numpy(cat.xyz).pin_memory()
     w_h = torch.from_numpy(w).pin_memory()
+    b_h = None if buffer is None else torch.from_numpy(np.ascontiguousarray(buffer, np.int32)).pin_memory()
     out = {}
 
     def call():
-        ctx._check(ctx._lib.gr_set_catalog(ctx._h, xyz_h.data_ptr(), w_h.data_ptr(), None,
+        ctx._check(ctx._lib.gr_set_catalog(ctx._h, xyz_h.data_ptr(), w_h.data_ptr(),
+                                           None if b_h is None else b_h.data_ptr(),
                                            cat.n_data, cat.n_rand))
         out["r"] = count()
 
@@ -887,10 +897,139 @@ def run_sub(args, fn):
     return 0
 
 
+def run_shard(args):
+    """The headline workload as ONE catalogue over the ranks
+    (gramsci_b200/shard.py): every rank holds the whole catalogue, counts the
+    slab of roots it owns with the slab's Rmax halo as buffer points, and one
+    all-reduce (NCCL, sum) of the histograms per step gives every rank the
+    whole catalogue's counts.  A step is the rank's count plus the
+    all-reduce; the tuples are the whole catalogue's distinct triangles
+    (counted once on rank 0 before the timed region), so the work is fixed as
+    the ranks grow (strong scaling)."""
+    import torch
+
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    device = local if world > 1 else 0
+    torch.cuda.set_device(device)
+    dv = f"cuda:{device}"
+    from gramsci_b200 import api, roofline, shard
+
+    cat, w, sp = make_catalogue(WORKLOAD, args.scale)  # the same catalogue on every rank
+    stream = torch.cuda.current_stream()
+    ctx = api.Context(device)
+    ctx.set_stream(stream)
+    ctx.set_precision(args.precision)
+    ctx.set_bins(sp["rmin"], sp["rmax"], sp["nbins"], sp["nmu"])
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dv)
+    full, full_st = None, None
+    if rank == 0:
+        ctx.set_catalog(torch.from_numpy(cat.xyz).to(dv), torch.from_numpy(w).to(dv), cat.n_data)
+        full = ctx.count_3pcf()
+        full_st = ctx.stats()
+    sx, sw, snd, sb, idx = shard.shard(cat.xyz, w, cat.n_data, rank, world, sp["rmax"])
+    xyz_d = torch.from_numpy(sx).to(dv)
+    w_d = torch.from_numpy(sw).to(dv)
+    b_d = torch.from_numpy(sb).to(dv)
+    ctx.set_catalog(xyz_d, w_d, snd, buffer=b_d)
+
+    def step(counts=False):
+        out = ctx.count_3pcf(counts=counts)
+        if world > 1:
+            shard.allreduce_counts(out, device=dv)
+        return out
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    sampler = ClockSampler(device)
+    sampler.start()
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    t_region0 = time.monotonic()
+    ev = [(_ev(), _ev()) for _ in range(args.steps)]
+    q_ms, launches, out = [], 0, None
+    for k in range(args.steps):
+        flush.zero_()
+        ev[k][0].record(stream)
+        out = step()
+        ev[k][1].record(stream)
+        st = ctx.stats()
+        q_ms.append(st["ms_query"])
+        launches += st["kernel_launches"]
+    torch.cuda.synchronize()
+    t_region1 = time.monotonic()
+    barrier()
+    clocks = sampler.stop(t_region0, t_region1)
+    total_ms = float(sum(a.elapsed_time(b) for a, b in ev))
+    t_max = reduce_over_ranks(total_ms, "max", dv) if world > 1 else total_ms
+    # end to end: the rank's shard (coordinates, weights, buffer flags) from
+    # pinned host memory, the count, the all-reduce, the histograms back
+    shard_cat = types.SimpleNamespace(xyz=sx, n_data=snd, n_rand=int(sx.shape[0]) - snd)
+    e2e_t, _ = e2e_loop(ctx, shard_cat, sw, step, stream, flush, max(3, min(args.steps, 20)),
+                        buffer=sb)
+    if world > 1:
+        e2e_t = reduce_over_ranks(e2e_t, "max", dv)
+    # parity: the sharded counts (with the integer counts) against rank 0's
+    # call on the whole catalogue; every rank takes this step
+    chk = step(counts=True)
+    pk = roofline.peaks()
+    rf = roofline.tri3_roofline(ctx, q_ms, pk)
+    rf["of"] = "rank 0's slab"
+    line = None
+    if rank == 0:
+        tri = int(full_st["tuples"])
+        value = tri * args.steps / (t_max / 1e3)
+        nh = out["catsum"].size
+        line = {
+            "metric": METRIC, "value": value, "unit": "tuples/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32+f64", "data": "synthetic (seeded Neyman-Scott galaxies + uniform randoms)",
+            "config": c2_config(cat, sp, args.scale, world, tri, full_st["rooted"],
+                                full_st["n_edges"], parallelism=f"slabs{world}"),
+            "e2e": {"value": tri / (e2e_t / 1e3), "unit": "tuples/s", "ms_per_step": e2e_t,
+                    "h2d_bytes_per_step": int(sx.nbytes + sw.nbytes + sb.nbytes),
+                    "d2h_bytes_per_step": int(nh * 8 * 2 + 8 * 8),
+                    "ms_min_median_max": e2e_loop.spread},
+            "roofline": rf,
+            "clocks": clocks,
+            "gpu_launches": launches,
+            "device": device_info(),
+            "shard": {"points": int(sx.shape[0]), "roots": int(np.count_nonzero(sb == 0)),
+                      "catalogue_points": int(cat.n), "collective": "all_reduce(sum) per step"
+                      if world > 1 else "none"},
+            "parity": {"against": "one call on the whole catalogue on rank 0",
+                       "counts_exact": bool(np.array_equal(chk["counts"], full["counts"])),
+                       "max_rel_catsum": float(np.max(np.abs(chk["catsum"] - full["catsum"]) /
+                                                      np.maximum(np.abs(full["catsum"]), 1e-300)))},
+        }
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.shard and args.workload == "c2_3pcf":
+        return run_shard(args)
     subs = {"c1_2pcf": sub_pcf2, "c3_4pcf": sub_quad, "c4_batched": sub_batched,
             "c5_adjoint": sub_adjoint}
     if args.workload in subs:
