@@ -233,6 +233,23 @@ __device__ __forceinline__ float pair_index_sqrt(float disc) {
   return disc > 0.0f ? disc * rsqrtf(disc) : 0.0f;
 }
 
+// Row x of pair t (0 <= t < k(k-1)/2, k2m1 = 2k - 1) with no adjustment, exact
+// for k <= kPairRowExact.  There disc = (2k-1)^2 - 8t is an integer in
+// [9, 511^2], exact in FP32; the root from pair_index_sqrt is within 2.5 ulp
+// (rsqrtf's 2 ulp and the product's rounding), 1.6e-4 absolute, and
+// u = (2k - 1 - root) / 2 comes out within 1.1e-4 of its true value.  The
+// true u is an integer or a half-integer when disc is a square, and otherwise
+// at least 4.8e-4 from every integer (a root of a non-square below 512^2 is
+// at least 1/1024 from every integer).  Adding 2.5e-4 before truncating
+// therefore gives floor(u) in every case.  Beyond kPairRowExact the result
+// is within one row and the caller adjusts it.  Checked on the CPU for every
+// pair of every k up to kPairRowExact with the root 3 ulp off either way.
+constexpr int kPairRowExact = 256;
+__device__ __forceinline__ int pair_row_biased(int k2m1, int t) {
+  const float disc = (float)(k2m1 * k2m1) - 8.0f * (float)t;
+  return (int)(0.5f * ((float)k2m1 - pair_index_sqrt(disc)) + 2.5e-4f);
+}
+
 // Both points of a pair are buffer points (pos4.w = 1 marks them): the pair
 // has no root and adds nothing to any 2PCF histogram or gradient, so the
 // pair sweeps skip it before testing it.  (The neighbour graph keeps such

@@ -1001,12 +1001,14 @@ __global__ void __launch_bounds__((ADJ ? kQuadMaxWarps : (WEIGHTED ? kQuadGWarps
     if (lane == 0 && part == 0) probes += (unsigned long long)npair;  // once per root
     auto pair_of = [&](int t, int& x, int& y) {
       // x: the largest row with x (2k - 1 - x) / 2 <= t pairs before it
-      const float disc = (float)(k2m1 * k2m1) - 8.0f * (float)t;
-      x = (int)(0.5f * ((float)k2m1 - pair_index_sqrt(disc)));
-      x = max(0, min(x, k - 2));
-      if ((x + 1) * (k2m1 - x - 1) / 2 <= t) ++x;
-      if (x * (k2m1 - x) / 2 > t) --x;
-      y = t - x * (k2m1 - x) / 2 + x + 1;
+      // (exact up to kPairRowExact members, else one adjustment each way)
+      x = pair_row_biased(k2m1, t);
+      if (k > kPairRowExact) {
+        x = max(0, min(x, k - 2));
+        if ((x + 1) * (k2m1 - x - 1) / 2 <= t) ++x;
+        if (x * (k2m1 - x) / 2 > t) --x;
+      }
+      y = t - (int)((unsigned)(x * (k2m1 - x)) >> 1) + x + 1;
     };
     for (int t = lane; t < npair; t += 32) {
       int x, y;

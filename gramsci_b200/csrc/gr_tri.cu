@@ -429,12 +429,14 @@ __global__ void __launch_bounds__(kTriMaxWarps * 32) tri3_kernel(DevCatalog C, C
             int x = 0, y = 0;
             if (t < npair) {
               // x: the largest row with x (2k - 1 - x) / 2 <= t pairs before it
-              const float disc = (float)(k2m1 * k2m1) - 8.0f * (float)t;
-              x = (int)(0.5f * ((float)k2m1 - pair_index_sqrt(disc)));
-              x = max(0, min(x, k - 2));
-              if ((x + 1) * (k2m1 - x - 1) / 2 <= t) ++x;
-              if (x * (k2m1 - x) / 2 > t) --x;
-              y = t - x * (k2m1 - x) / 2 + x + 1;
+              // (exact up to kPairRowExact members, else one adjustment each way)
+              x = pair_row_biased(k2m1, t);
+              if (k > kPairRowExact) {
+                x = max(0, min(x, k - 2));
+                if ((x + 1) * (k2m1 - x - 1) / 2 <= t) ++x;
+                if (x * (k2m1 - x) / 2 > t) --x;
+              }
+              y = t - (int)((unsigned)(x * (k2m1 - x)) >> 1) + x + 1;
               int r = T.P.f32 ? member_f32(s_pos[x], s_pos[y], T.P) : 2;
               if (r == 2) {
                 int b, mf, mr;
