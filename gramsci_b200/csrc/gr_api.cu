@@ -1260,9 +1260,13 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   // copied here instead of accumulated on the device
   const int nh = nbin * 5, nd = nbin * 6 * ndc, ndv = nbin * 6 * (ndc - 1);
   const bool weighted = !c->uniform;
+  // unit-weight 4PCF: the kernels fill the pattern histogram (kQuadPatterns
+  // x nbin counts), expanded here into the N2 / N3 and disconnected-term counts
+  const bool patterns = !weighted && !tetra;
+  const int nhk = patterns ? nbin * kQuadPatterns : nh, ndk = patterns ? 0 : ndv;
   const double fscale = fix_scale(c->wmax * c->wmax * c->wmax * c->wmax);
   const double dscale = fix_scale(tetra ? c->wmax * c->wmax * c->wmax : c->wmax * c->wmax);
-  c->hcnt.reserve(nh);
+  c->hcnt.reserve(std::max(nh, nhk));
   c->hfix.reserve(2 * nh);
   c->dcnt.reserve(ndv);
   c->dfix.reserve(2 * ndv);
@@ -1276,8 +1280,8 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   const unsigned long long gst[3] = {(unsigned long long)c->csr.rechecks,
                                      (unsigned long long)c->csr.candidates,
                                      (unsigned long long)c->csr.max_deg};
-  GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nh, s));
-  GR_CUDA_TRY(cudaMemsetAsync(c->dcnt.p, 0, sizeof(unsigned long long) * ndv, s));
+  GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nhk, s));
+  if (ndk) GR_CUDA_TRY(cudaMemsetAsync(c->dcnt.p, 0, sizeof(unsigned long long) * ndk, s));
   if (weighted) {
     GR_CUDA_TRY(cudaMemsetAsync(c->hfix.p, 0, sizeof(unsigned long long) * 2 * nh, s));
     GR_CUDA_TRY(cudaMemsetAsync(c->dfix.p, 0, sizeof(unsigned long long) * 2 * ndv, s));
@@ -1304,8 +1308,9 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   c->work.reserve(4);
   std::vector<unsigned long long> hc(nh), dc(nd);
   std::vector<double> hs(nh, 0.0), ds(nd, 0.0);
-  // read-back in the pinned stage: counts (nh, ndv), the sums converted on
-  // the device (nh, ndv doubles), kernel stats (8)
+  // read-back in the pinned stage: counts (nh, ndv; or the nhk pattern
+  // counts, fewer), the sums converted on the device (nh, ndv doubles),
+  // kernel stats (8)
   c->stage.reserve(2 * ((size_t)nh + ndv) + 8);
   c->hval.reserve((size_t)nh + ndv);
   unsigned long long* sc = c->stage.p;
@@ -1320,8 +1325,8 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   // launch is repeated with 64-bit counters and carried 128-bit sums.
   for (int attempt = 0; attempt < 2; ++attempt) {
     if (attempt > 0) {
-      GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nh, s));
-      GR_CUDA_TRY(cudaMemsetAsync(c->dcnt.p, 0, sizeof(unsigned long long) * ndv, s));
+      GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nhk, s));
+      if (ndk) GR_CUDA_TRY(cudaMemsetAsync(c->dcnt.p, 0, sizeof(unsigned long long) * ndk, s));
       if (weighted) {
         GR_CUDA_TRY(cudaMemsetAsync(c->hfix.p, 0, sizeof(unsigned long long) * 2 * nh, s));
         GR_CUDA_TRY(cudaMemsetAsync(c->dfix.p, 0, sizeof(unsigned long long) * 2 * ndv, s));
@@ -1331,12 +1336,13 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
     }
     Q.split = (weighted && attempt == 0) ? 1 : 0;
     const bool shared = launch_quad4(c->index.view(), G, Q, weighted, c->hcnt.p, c->hfix.p,
-                                     c->dcnt.p, c->dfix.p, nh, ndv, fscale, dscale, attempt == 0,
+                                     c->dcnt.p, c->dfix.p, nhk, ndk, fscale, dscale, attempt == 0,
                                      c->stats.p, c->work.p, s);
     GR_CUDA_TRY(cudaEventRecord(c->ev[3], s));
     if (Q.counts) {
-      GR_CUDA_TRY(cudaMemcpyAsync(sc, c->hcnt.p, sizeof(unsigned long long) * nh, cudaMemcpyDeviceToHost, s));
-      GR_CUDA_TRY(cudaMemcpyAsync(sd, c->dcnt.p, sizeof(unsigned long long) * ndv, cudaMemcpyDeviceToHost, s));
+      GR_CUDA_TRY(cudaMemcpyAsync(sc, c->hcnt.p, sizeof(unsigned long long) * nhk, cudaMemcpyDeviceToHost, s));
+      if (ndk)
+        GR_CUDA_TRY(cudaMemcpyAsync(sd, c->dcnt.p, sizeof(unsigned long long) * ndk, cudaMemcpyDeviceToHost, s));
     }
     if (weighted) {
       const double fs[4] = {fscale, fscale, fscale, fscale};
@@ -1349,7 +1355,9 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
     GR_CUDA_TRY(cudaStreamSynchronize(s));
     if (!(shared || Q.split) || st[1] < (1ull << 32)) break;
   }
-  if (Q.counts) {
+  if (patterns) {
+    quad_expand_patterns(sc, nbin, hc.data(), dc.data());
+  } else if (Q.counts) {
     std::memcpy(hc.data(), sc, sizeof(unsigned long long) * nh);
     std::memcpy(dc.data(), sd, sizeof(unsigned long long) * ndv);
   }

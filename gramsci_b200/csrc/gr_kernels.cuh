@@ -146,6 +146,17 @@ bool launch_quad4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, bo
                   unsigned long long* g_cnt, unsigned long long* g_fix, unsigned long long* d_cnt,
                   unsigned long long* d_fix, int nh, int nd, double fscale, double dscale,
                   bool shared_counts, unsigned long long* stats, int* work, cudaStream_t s);
+// Unit-weight 4PCF (tetra = 0, not weighted): the kernels count each rooted
+// clique once at (histogram index kk, pattern), pattern = the randomness of
+// the root and of the other three vertices in catalogue-id order (bits 0..3);
+// g_cnt then holds kQuadPatterns * nbin entries (nh = that, nd = 0).
+// quad_expand_patterns forms from them the N2 / N3 counts hc (5 * nbin, by
+// number of randoms) and the disconnected-term counts dc (6 * 3 * nbin: term,
+// randoms in the pair; a term counts when its gating role is random), as the
+// kernels otherwise accumulate them.
+constexpr int kQuadPatterns = 16;
+void quad_expand_patterns(const unsigned long long* H, int nbin, unsigned long long* hc,
+                          unsigned long long* dc);
 // 4PCF adjoint: gradient of sum(cot2 N2) + sum(cot3 N3) + sum(cotN discN)
 // + sum(cotR discR), cot = [cot2 nbin | cot3 nbin | cotN 6 nbin | cotR 6 nbin]
 // (nbin = ncfg nbins^2), into g_lo / g_hi (label order, zeroed) at scale

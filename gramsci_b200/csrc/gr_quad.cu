@@ -276,13 +276,23 @@ __device__ __forceinline__ int quad_root_index(const QuadCtx& X, const QVerts& V
   return (cfg - 1) + X.ncfg * ((d1 - 1) + X.nbins * (d2 - 1));
 }
 
-// N2 / N3 and the six disconnected terms of root R.
+// N2 / N3 and the six disconnected terms of root R.  Unit weights: one
+// count at (histogram index, randomness of the four roles) instead, the
+// pattern histogram from which quad_expand_patterns forms the N2 / N3 and
+// disconnected-term counts (which roles are random decides the category of
+// each and which terms are gated in).
 template <bool WEIGHTED, bool SHC, int R>
 __device__ __forceinline__ int quad_root(const QuadCtx& X, const QVerts& V, unsigned long long packed,
                                          unsigned rndm, int nr) {
   int u0, u1, u2;
   const int kk = quad_root_index<R>(X, V, packed, u0, u1, u2);
   if (kk < 0) return 0;
+  if constexpr (!WEIGHTED) {
+    const unsigned pat = ((rndm >> R) & 1u) | (((rndm >> u0) & 1u) << 1) |
+                         (((rndm >> u1) & 1u) << 2) | (((rndm >> u2) & 1u) << 3);
+    qcount<SHC>(X, kk + X.nbin * (int)pat);
+    return 1;
+  }
   qcount<SHC>(X, kk + X.nbin * nr);
   if (WEIGHTED)
     qfix(X, &X.fix[kk + X.nbin * nr], &X.fix[kk + X.nbin * (nr + 5)],
@@ -1273,6 +1283,25 @@ void launch_adj4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, con
     launch_quad_grid(quad4_kernel<false, false, true, true, false>, nw, smem, C.n, work, s, C, G, Q,
                      nullptr, nullptr, nullptr, nullptr, 0, 0, 1.0, 1.0, stats, cot, gscale, g_lo,
                      g_hi);
+  }
+}
+
+void quad_expand_patterns(const unsigned long long* H, int nbin, unsigned long long* hc,
+                          unsigned long long* dc) {
+  std::fill(hc, hc + (size_t)nbin * 5, 0ull);
+  std::fill(dc, dc + (size_t)nbin * 6 * 3, 0ull);
+  for (int pat = 0; pat < kQuadPatterns; ++pat) {
+    const int nr = __builtin_popcount((unsigned)pat);
+    for (int k = 0; k < nbin; ++k) {
+      const unsigned long long v = H[k + (size_t)nbin * pat];
+      if (!v) continue;
+      hc[k + (size_t)nbin * nr] += v;
+      for (int tt = 0; tt < 6; ++tt) {
+        if (!((pat >> term_gate(tt)) & 1)) continue;
+        const int npr = ((pat >> term_pu(tt)) & 1) + ((pat >> term_pv(tt)) & 1);
+        dc[k + (size_t)nbin * tt + (size_t)nbin * 6 * npr] += v;
+      }
+    }
   }
 }
 
