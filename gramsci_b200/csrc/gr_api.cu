@@ -347,13 +347,13 @@ int set_err(gr_ctx* c, int code, const std::string& m) {
 // reads n doubles instead of 2n words and converts nothing.
 __global__ void fix_convert_kernel(const unsigned long long* __restrict__ lo,
                                    const unsigned long long* __restrict__ hi, int64_t n,
-                                   int64_t per, double4 inv_scale, int split,
+                                   int64_t per, double4 inv_scale, int split, int stride,
                                    double* __restrict__ out) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t c = i / per;
     const double is = c == 0 ? inv_scale.x : (c == 1 ? inv_scale.y : (c == 2 ? inv_scale.z : inv_scale.w));
-    unsigned long long l = lo[i], h = hi[i];
+    unsigned long long l = lo[i * stride], h = hi[i * stride];
     if (split) {
       // (signed h) << 32 as 128 bits, plus l
       const long long hs = (long long)h;
@@ -368,15 +368,16 @@ __global__ void fix_convert_kernel(const unsigned long long* __restrict__ lo,
   }
 }
 
-// Queue fix_convert_kernel: n values from (lo, lo + hi_off), categories of
-// `per` values with scales sc[0..3].
+// Queue fix_convert_kernel: n values from (lo, lo + hi_off) entries of
+// `stride` words each, categories of `per` values with scales sc[0..3].
 static void enqueue_fix_convert(const unsigned long long* lo, int64_t hi_off, int64_t n,
                                 int64_t per, const double sc[4], bool split, double* out,
-                                cudaStream_t s) {
+                                cudaStream_t s, int stride = 1) {
   if (n <= 0) return;
   const double4 inv = make_double4(1.0 / sc[0], 1.0 / sc[1], 1.0 / sc[2], 1.0 / sc[3]);
   const int blocks = (int)std::min<int64_t>((n + 255) / 256, 2 * (int64_t)sm_count());
-  fix_convert_kernel<<<blocks, 256, 0, s>>>(lo, lo + hi_off, n, per, inv, split ? 1 : 0, out);
+  fix_convert_kernel<<<blocks, 256, 0, s>>>(lo, lo + hi_off * stride, n, per, inv, split ? 1 : 0,
+                                            stride, out);
   GR_CHECK_LAUNCH();
 }
 
@@ -1267,9 +1268,9 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   const double fscale = fix_scale(c->wmax * c->wmax * c->wmax * c->wmax);
   const double dscale = fix_scale(tetra ? c->wmax * c->wmax * c->wmax : c->wmax * c->wmax);
   c->hcnt.reserve(std::max(nh, nhk));
-  c->hfix.reserve(2 * nh);
+  c->hfix.reserve((size_t)2 * nh * kFixStride);
   c->dcnt.reserve(ndv);
-  c->dfix.reserve(2 * ndv);
+  c->dfix.reserve((size_t)2 * ndv * kFixStride);
   c->stats.reserve(8);
   const bool reuse = reuse_graph(c);
   GR_CUDA_TRY(cudaEventRecord(c->ev[0], s));
@@ -1283,8 +1284,8 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
   GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nhk, s));
   if (ndk) GR_CUDA_TRY(cudaMemsetAsync(c->dcnt.p, 0, sizeof(unsigned long long) * ndk, s));
   if (weighted) {
-    GR_CUDA_TRY(cudaMemsetAsync(c->hfix.p, 0, sizeof(unsigned long long) * 2 * nh, s));
-    GR_CUDA_TRY(cudaMemsetAsync(c->dfix.p, 0, sizeof(unsigned long long) * 2 * ndv, s));
+    GR_CUDA_TRY(cudaMemsetAsync(c->hfix.p, 0, sizeof(unsigned long long) * 2 * nh * kFixStride, s));
+    GR_CUDA_TRY(cudaMemsetAsync(c->dfix.p, 0, sizeof(unsigned long long) * 2 * ndv * kFixStride, s));
   }
   GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
   if ((int64_t)gst[2] > 1024)
@@ -1328,8 +1329,8 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
       GR_CUDA_TRY(cudaMemsetAsync(c->hcnt.p, 0, sizeof(unsigned long long) * nhk, s));
       if (ndk) GR_CUDA_TRY(cudaMemsetAsync(c->dcnt.p, 0, sizeof(unsigned long long) * ndk, s));
       if (weighted) {
-        GR_CUDA_TRY(cudaMemsetAsync(c->hfix.p, 0, sizeof(unsigned long long) * 2 * nh, s));
-        GR_CUDA_TRY(cudaMemsetAsync(c->dfix.p, 0, sizeof(unsigned long long) * 2 * ndv, s));
+        GR_CUDA_TRY(cudaMemsetAsync(c->hfix.p, 0, sizeof(unsigned long long) * 2 * nh * kFixStride, s));
+        GR_CUDA_TRY(cudaMemsetAsync(c->dfix.p, 0, sizeof(unsigned long long) * 2 * ndv * kFixStride, s));
       }
       GR_CUDA_TRY(cudaMemsetAsync(c->stats.p, 0, sizeof(unsigned long long) * 8, s));
       GR_CUDA_TRY(cudaEventRecord(q0, s));
@@ -1347,8 +1348,8 @@ static int count_quad(gr_ctx* c, bool tetra, double* N2, double* N3, double* dis
     if (weighted) {
       const double fs[4] = {fscale, fscale, fscale, fscale};
       const double ds4[4] = {dscale, dscale, dscale, dscale};
-      enqueue_fix_convert(c->hfix.p, nh, nh, nh, fs, Q.split != 0, c->hval.p, s);
-      enqueue_fix_convert(c->dfix.p, ndv, ndv, ndv, ds4, Q.split != 0, c->hval.p + nh, s);
+      enqueue_fix_convert(c->hfix.p, nh, nh, nh, fs, Q.split != 0, c->hval.p, s, kFixStride);
+      enqueue_fix_convert(c->dfix.p, ndv, ndv, ndv, ds4, Q.split != 0, c->hval.p + nh, s, kFixStride);
       GR_CUDA_TRY(cudaMemcpyAsync(sv, c->hval.p, sizeof(double) * ((size_t)nh + ndv), cudaMemcpyDeviceToHost, s));
     }
     GR_CUDA_TRY(cudaMemcpyAsync(st, c->stats.p, sizeof(unsigned long long) * 8, cudaMemcpyDeviceToHost, s));

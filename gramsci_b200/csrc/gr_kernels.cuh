@@ -109,6 +109,13 @@ void launch_grad_finish(int n, const int* orig, const unsigned long long* g_lo,
                         const unsigned long long* g_hi, double gscale, double* grad,
                         cudaStream_t s);
 
+// 8-byte words per entry of the 4PCF kernels' global fixed-point sums
+// (g_fix, d_fix): 16, one 128-byte line per entry.
+#ifndef GR_FIX_STRIDE
+#define GR_FIX_STRIDE 16
+#endif
+constexpr int kFixStride = GR_FIX_STRIDE;
+
 struct QuadParams {
   int nbins, ncfg;
   int tetra;  // -tetra: only 4-cliques with six equal bins (histograms by bin)
@@ -135,8 +142,8 @@ struct QuadParams {
 // incidences, [2] probes, [3] set when a root's label offsets exceed the
 // hash key range (the host reports it).  work: one device int, the dynamic
 // root counter (reset by the launch).
-// The outputs (g_cnt nh, g_fix 2 nh, d_cnt nd, d_fix 2 nd; fix arrays only
-// when weighted) must be zeroed; the last disc category (discR, equal to the
+// The outputs (g_cnt nh, g_fix 2 nh, d_cnt nd, d_fix 2 nd entries, the fix
+// arrays kFixStride words per entry and only when weighted) must be zeroed; the last disc category (discR, equal to the
 // all-random one before it) is not written, nd covers the others.
 // shared_counts: integer counts in block-private 32-bit shared-memory
 // counters (exact while the rooted total stays below 2^32; the caller
