@@ -35,9 +35,14 @@ namespace {
 constexpr int kQuadMaxWarps = 16;   // weighted / adjoint kernels (up to 128 registers)
 constexpr int kQuadMaxWarpsU = 24;  // unweighted kernels (up to 85 registers)
 #ifndef GR_QUADG_WEIGHTED_WARPS
-#define GR_QUADG_WEIGHTED_WARPS 16
+#define GR_QUADG_WEIGHTED_WARPS 24
 #endif
-constexpr int kQuadGWarpsW = GR_QUADG_WEIGHTED_WARPS;  // weighted geometric kernel
+// Weighted geometric kernel: 24 warps (at most 85 registers, a few bytes
+// spilled) measured 4.47 ms on the 4PCF workload against 4.64 ms at 20 and
+// 5.04 ms at 16 (106 registers) once its sums had a line per bin; before
+// that the reductions, not the warps, bounded it.  (The high limb in the
+// low limb's line instead of a line of its own: 4.58 ms.)
+constexpr int kQuadGWarpsW = GR_QUADG_WEIGHTED_WARPS;
 constexpr size_t kQuadSmemLimit = 227 * 1024;
 constexpr int kQQueue = 96;         // hit queue entries per warp (< 32 left + 64 pushed)
 constexpr int kQMaxOffset = 1 << 22;  // hash entries: (label offset << 10) | position
