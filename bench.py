@@ -477,8 +477,8 @@ def run_ours(args):
         "e2e": {"value": e2e_value, "unit": "tuples/s", "h2d_bytes_per_step": h2d,
                 "ms_per_step": e2e_t, "ms_min_median_max": e2e_loop.spread,
                 "d2h_bytes_per_step": d2h},
-        "roofline": rf,
-        "graph_roofline": grf,
+        "roofline": roofline.mark_binding(rf),
+        "graph_roofline": roofline.mark_binding(grf),
         "clocks": clocks,
         "gpu_launches": launches,
         "device": dev,
@@ -569,10 +569,11 @@ def sub_pcf2(args, stream, flush):
            "clocks": ck.clocks, "phase_ms": {"index": st["ms_index"], "query": st["ms_query"]},
            "fp64_recheck_fraction": st["fp64_rechecks"] / max(1, st["candidates"])}
     # the pair sweep's FP32 arithmetic over its own device time
-    rec["roofline"] = {"kernel": "pair sweep", "ms": st["ms_query"],
-                       "fp32": roofline.fp32_binning_roofline(
-                           int(got["counts"].sum()), sp["nmu"], st["ms_query"], ck.clocks.get("sm_mhz"),
-                           torch.cuda.get_device_properties(0).multi_processor_count)}
+    rec["roofline"] = roofline.mark_binding(
+        {"kernel": "pair sweep", "ms": st["ms_query"],
+         "fp32": roofline.fp32_binning_roofline(
+             int(got["counts"].sum()), sp["nmu"], st["ms_query"], ck.clocks.get("sm_mhz"),
+             torch.cuda.get_device_properties(0).multi_processor_count)})
     ctx.close()
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -663,7 +664,7 @@ def sub_quad(args, stream, flush):
            "e2e": {"value": st["rooted"] / (e2e_ms / 1e3), "unit": "tuples/s",
                    "h2d_bytes_per_step": int(cat.xyz.nbytes + w.nbytes),
                    "d2h_bytes_per_step": int(sum(v.nbytes for v in out.values()) + 64)},
-           "roofline": rf, "clocks": ck.clocks, "gpu_launches": launches,
+           "roofline": roofline.mark_binding(rf), "clocks": ck.clocks, "gpu_launches": launches,
            "lognormal_weights": {"forward_query_ms": float(np.median(fwd[1:])),
                                  "adjoint_ms": float(np.median(adj[1:])),
                                  "adjoint_over_forward": float(np.median(adj[1:]) / np.median(fwd[1:])),
@@ -776,7 +777,7 @@ def sub_batched(args, stream, flush):
     rf["atomics"] = roofline.atomic_roofline(prof, st["candidates"], tb, ck.clocks.get("sm_mhz"), n_sm)
     rf["fp32"] = roofline.fp32_binning_roofline(rec["rooted"], sp["nmu"], tb, ck.clocks.get("sm_mhz"),
                                                 n_sm)
-    rec["roofline"] = rf
+    rec["roofline"] = roofline.mark_binding(rf)
     rec["fp64_recheck_fraction"] = st["fp64_rechecks"] / max(1, st["candidates"])
     ctx.close()
     del reg_dev, xyz_d, w_d

@@ -157,3 +157,23 @@ def fp32_binning_roofline(binned_directed_pairs, nmu, ms, sm_mhz, n_sm):
     peak = n_sm * 128 * 2 * sm_mhz * 1e6 / 1e12
     return {"unit": "TFLOP/s", "achieved": achieved, "peak": peak, "frac": achieved / peak,
             "flop_per_binned_pair": f, "peak_kind": "nominal FP32 FMA rate at the sampled clock"}
+
+
+def mark_binding(rf):
+    """Name the ceiling that binds a kernel: of its fractions (the top-level
+    one, against HBM, and those of its `issue`, `atomics` and `fp32`
+    entries) the largest, as rf["binding"] with rf["binding_frac"].  A
+    kernel far below its HBM ceiling but near its issue ceiling is
+    issue-bound, and the line says so.  Returns rf."""
+    fr = {}
+    if isinstance(rf.get("frac"), (int, float)):
+        fr[rf.get("bound", "hbm")] = float(rf["frac"])
+    for k in ("issue", "atomics", "fp32"):
+        v = rf.get(k)
+        if isinstance(v, dict) and isinstance(v.get("frac"), (int, float)):
+            fr[k] = float(v["frac"])
+    if fr:
+        b = max(fr, key=fr.get)
+        rf["binding"] = b
+        rf["binding_frac"] = fr[b]
+    return rf

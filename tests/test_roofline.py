@@ -95,3 +95,17 @@ def test_fp32_binning_roofline():
     assert abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-12
     assert roofline.fp32_binning_roofline(1e9, 1, 1.0, 1965.0, 148)["flop_per_binned_pair"] == 11
     assert roofline.fp32_binning_roofline(1e9, 1, 1.0, None, 148) is None
+
+
+def test_mark_binding_names_the_largest_fraction():
+    from gramsci_b200 import roofline
+
+    rf = {"bound": "hbm", "frac": 0.25, "issue": {"frac": 0.75}, "atomics": {"frac": 0.16}}
+    roofline.mark_binding(rf)
+    assert rf["binding"] == "issue" and rf["binding_frac"] == 0.75
+    rf = {"kernel": "pair sweep", "fp32": {"frac": 0.07}, "issue": None}
+    roofline.mark_binding(rf)
+    assert rf["binding"] == "fp32"
+    rf = {"bound": "hbm", "frac": 0.9, "issue": {"frac": 0.5}}
+    assert roofline.mark_binding(rf)["binding"] == "hbm"
+    assert "binding" not in roofline.mark_binding({"kernel": "x", "fp32": None})
