@@ -562,7 +562,6 @@ static std::vector<unsigned long long> spec_key(const gr_ctx* c) {
   buf(I.key_orig);
   buf(I.slot);
   buf(I.tmp_perm);
-  buf(I.perm);
   buf(I.cell_start);
   buf(I.orig);
   buf(I.cell_key);

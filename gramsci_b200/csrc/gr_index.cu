@@ -126,49 +126,43 @@ __global__ void cell_scatter_kernel(int64_t n, const int* __restrict__ key,
     tmp_perm[start[key[i]] + slot[i]] = (int)i;
 }
 
-// One warp per cell: rank each member by original index (O(c^2/32)).
-__global__ void cell_order_kernel(int64_t ncell, const int64_t* __restrict__ start,
-                                  const int* __restrict__ tmp_perm, int* __restrict__ perm) {
-  int lane = threadIdx.x & 31;
-  int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-  int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+// One warp per cell: rank each member by its catalogue index (O(c^2/32)),
+// so that within a cell points keep their catalogue order, and write the
+// member's data at its place in the cell-ordered layout (the scattered
+// reads of the catalogue happen here, once per point).
+__global__ void cell_order_gather_kernel(int64_t ncell, const int64_t* __restrict__ start,
+                                         const int* __restrict__ tmp_perm,
+                                         const double* __restrict__ xyz,
+                                         const double* __restrict__ w,
+                                         const int* __restrict__ buffer, int64_t n_data,
+                                         float4* __restrict__ pos4, double4* __restrict__ posd,
+                                         double* __restrict__ wl, int* __restrict__ orig,
+                                         uint8_t* __restrict__ flags, int* __restrict__ cell_key) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t c = warp; c < ncell; c += nwarps) {
-    int64_t b = start[c], e = start[c + 1];
-    int cnt = (int)(e - b);
-    if (cnt == 1) {
-      if (lane == 0) perm[b] = tmp_perm[b];
-      continue;
-    }
+    const int64_t b = start[c], e = start[c + 1];
+    const int cnt = (int)(e - b);
     for (int k = lane; k < cnt; k += 32) {
-      int v = tmp_perm[b + k];
+      const int i = tmp_perm[b + k];
       int r = 0;
-      for (int j = 0; j < cnt; ++j) r += tmp_perm[b + j] < v;
-      perm[b + r] = v;
+      for (int j = 0; j < cnt; ++j) r += tmp_perm[b + j] < i;
+      const int64_t p = b + r;
+      const double x = xyz[3 * (int64_t)i + 0], y = xyz[3 * (int64_t)i + 1],
+                   z = xyz[3 * (int64_t)i + 2];
+      const double wi = w[i];
+      uint8_t f = (i >= n_data) ? FLAG_RANDOM : 0;
+      if (buffer && buffer[i] == 1) f |= FLAG_BUFFER;
+      // the fourth component marks buffer points (pair sweeps skip pairs of two)
+      pos4[p] = make_float4(__double2float_rn(x), __double2float_rn(y), __double2float_rn(z),
+                            (f & FLAG_BUFFER) ? 1.0f : 0.0f);
+      posd[p] = make_double4(x, y, z, wi);
+      wl[p] = wi;
+      orig[p] = i;
+      flags[p] = f;
+      cell_key[p] = (int)c;
     }
-  }
-}
-
-__global__ void gather_kernel(int64_t n, const int* __restrict__ perm,
-                              const double* __restrict__ xyz, const double* __restrict__ w,
-                              const int* __restrict__ buffer, const int* __restrict__ key_orig,
-                              int64_t n_data, float4* __restrict__ pos4, double4* __restrict__ posd,
-                              double* __restrict__ wl, int* __restrict__ orig,
-                              uint8_t* __restrict__ flags, int* __restrict__ cell_key) {
-  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n;
-       p += (int64_t)gridDim.x * blockDim.x) {
-    int i = perm[p];
-    double x = xyz[3 * (int64_t)i + 0], y = xyz[3 * (int64_t)i + 1], z = xyz[3 * (int64_t)i + 2];
-    double wi = w[i];
-    uint8_t f = (i >= n_data) ? FLAG_RANDOM : 0;
-    if (buffer && buffer[i] == 1) f |= FLAG_BUFFER;
-    // the fourth component marks buffer points (pair sweeps skip pairs of two)
-    pos4[p] = make_float4(__double2float_rn(x), __double2float_rn(y), __double2float_rn(z),
-                          (f & FLAG_BUFFER) ? 1.0f : 0.0f);
-    posd[p] = make_double4(x, y, z, wi);
-    wl[p] = wi;
-    orig[p] = i;
-    flags[p] = f;
-    cell_key[p] = key_orig[i];
   }
 }
 
@@ -258,7 +252,6 @@ void CellIndex::build(const double* d_xyz, const double* d_w, const int* d_buffe
   key_orig.reserve(n);
   slot.reserve(n);
   tmp_perm.reserve(n);
-  perm.reserve(n);
   cell_start64.reserve(total + 1);
   cell_start.reserve(total + 1);
   pos4.reserve(n);
@@ -275,20 +268,18 @@ void CellIndex::build(const double* d_xyz, const double* d_w, const int* d_buffe
     launches++;
   }
   GR_CHECK_LAUNCH();
-  scan_i32_to_i64(cell_count.p, cell_start64.p, total, s, scan_tmp);
+  // cell starts as 64-bit offsets and, in the same pass, the 32-bit copy
+  // the kernels read
+  scan_i32_to_i64(cell_count.p, cell_start64.p, total, s, scan_tmp, cell_start.p);
   launches += 3;
   if (n > 0) {
     cell_scatter_kernel<<<blocks_for(n, 256), 256, 0, s>>>(n, key_orig.p, slot.p, cell_start64.p,
                                                           tmp_perm.p);
-    cell_order_kernel<<<blocks_for(total * 32, 256), 256, 0, s>>>(total, cell_start64.p,
-                                                                  tmp_perm.p, perm.p);
-    gather_kernel<<<blocks_for(n, 256), 256, 0, s>>>(n, perm.p, d_xyz, d_w, d_buffer, key_orig.p,
-                                                     n_data, pos4.p, posd.p, w.p, orig.p,
-                                                     flags.p, cell_key.p);
-    launches += 3;
+    cell_order_gather_kernel<<<blocks_for(total * 32, 256), 256, 0, s>>>(
+        total, cell_start64.p, tmp_perm.p, d_xyz, d_w, d_buffer, n_data, pos4.p, posd.p, w.p,
+        orig.p, flags.p, cell_key.p);
+    launches += 2;
   }
-  narrow_kernel_launch(cell_start64.p, cell_start.p, total + 1, s);
-  launches++;
   GR_CHECK_LAUNCH();
 }
 
@@ -333,18 +324,6 @@ int64_t make_grid_geom(const double lo[3], const double hi[3], double rmax, int 
     total = (int64_t)g.nc[0] * g.nc[1] * g.nc[2];
   }
   return total;
-}
-
-namespace {
-__global__ void narrow_kernel(const int64_t* __restrict__ in, int* __restrict__ out, int64_t n) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x)
-    out[i] = (int)in[i];
-}
-}  // namespace
-
-void narrow_kernel_launch(const int64_t* in, int* out, int64_t n, cudaStream_t s) {
-  narrow_kernel<<<blocks_for(n, 256), 256, 0, s>>>(in, out, n);
 }
 
 DevCatalog CellIndex::view() const {
@@ -414,7 +393,7 @@ __global__ void scan_tile_sums(const T* __restrict__ in, int64_t n, int64_t* __r
 
 template <typename T>
 __global__ void scan_tile_apply(const T* __restrict__ in, int64_t n, const int64_t* __restrict__ offs,
-                                int64_t* __restrict__ out) {
+                                int64_t* __restrict__ out, int* __restrict__ out32) {
   __shared__ int64_t warp_tot[32];
   int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
   int64_t v[kScanItems];
@@ -428,23 +407,32 @@ __global__ void scan_tile_apply(const T* __restrict__ in, int64_t n, const int64
   int64_t ex = block_exclusive_scan<T>(s, warp_tot, total) + (offs ? offs[blockIdx.x] : 0);
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k) {
-    if (base + k < n) out[base + k] = ex;
+    if (base + k < n) {
+      out[base + k] = ex;
+      if (out32) out32[base + k] = (int)ex;
+    }
     ex += v[k];
   }
   // the last element of the whole array writes the grand total at out[n]
-  if (base <= n - 1 && n - 1 < base + kScanItems) out[n] = ex;
+  if (base <= n - 1 && n - 1 < base + kScanItems) {
+    out[n] = ex;
+    if (out32) out32[n] = (int)ex;
+  }
 }
 
+// Exclusive scan of in[0, n) into out[0, n] (out[n] = the total); out32,
+// when given, receives the same values as 32-bit integers.
 template <typename T>
 void scan_impl(const T* in, int64_t* out, int64_t n, cudaStream_t s, DevBuf<int64_t>& tmp,
-               size_t tmp_off) {
+               size_t tmp_off, int* out32 = nullptr) {
   if (n <= 0) {
     GR_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(int64_t), s));
+    if (out32) GR_CUDA_TRY(cudaMemsetAsync(out32, 0, sizeof(int), s));
     return;
   }
   int64_t tiles = (n + kScanTile - 1) / kScanTile;
   if (tiles == 1) {
-    scan_tile_apply<T><<<1, kScanThreads, 0, s>>>(in, n, nullptr, out);
+    scan_tile_apply<T><<<1, kScanThreads, 0, s>>>(in, n, nullptr, out, out32);
     GR_CHECK_LAUNCH();
     return;
   }
@@ -453,7 +441,7 @@ void scan_impl(const T* in, int64_t* out, int64_t n, cudaStream_t s, DevBuf<int6
   scan_tile_sums<T><<<(unsigned)tiles, kScanThreads, 0, s>>>(in, n, sums);
   GR_CHECK_LAUNCH();
   scan_impl<int64_t>(sums, offs, tiles, s, tmp, tmp_off + 2 * tiles + 1);
-  scan_tile_apply<T><<<(unsigned)tiles, kScanThreads, 0, s>>>(in, n, offs, out);
+  scan_tile_apply<T><<<(unsigned)tiles, kScanThreads, 0, s>>>(in, n, offs, out, out32);
   GR_CHECK_LAUNCH();
 }
 
@@ -510,10 +498,11 @@ void scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s, DevBuf
   scan_impl<int64_t>(in, out, n, s, tmp, 0);
 }
 
-void scan_i32_to_i64(const int* in, int64_t* out, int64_t n, cudaStream_t s, DevBuf<int64_t>& tmp) {
+void scan_i32_to_i64(const int* in, int64_t* out, int64_t n, cudaStream_t s, DevBuf<int64_t>& tmp,
+                     int* out32) {
   size_t need = scan_tmp_need(n);
   if (tmp.n < need) tmp.reserve(need);
-  scan_impl<int>(in, out, n, s, tmp, 0);
+  scan_impl<int>(in, out, n, s, tmp, 0, out32);
 }
 
 }  // namespace gr

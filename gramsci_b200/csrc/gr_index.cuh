@@ -30,7 +30,7 @@ struct CellIndex {
   bool prev_auto = false;  // the previous build chose sub itself
   unsigned long long prev_raw[7] = {0, 0, 0, 0, 0, 0, 0};
   DevBuf<unsigned long long> bbox_prev;  // previous raw bounding box [0..6], mismatch flag [7]
-  DevBuf<int> cell_count, key_orig, slot, tmp_perm, perm, cell_start, orig, cell_key;
+  DevBuf<int> cell_count, key_orig, slot, tmp_perm, cell_start, orig, cell_key;
   DevBuf<int64_t> cell_start64, scan_tmp;
   DevBuf<float4> pos4;
   DevBuf<double4> posd;
@@ -48,7 +48,6 @@ struct CellIndex {
   DevCatalog view() const;
 };
 
-void narrow_kernel_launch(const int64_t* in, int* out, int64_t n, cudaStream_t s);
 
 // Upper adjacency: row p lists the neighbours q > p (internal labels) of the
 // (rmin, rmax) graph in increasing label order, with packed bin / mu

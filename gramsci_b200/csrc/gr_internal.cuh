@@ -703,7 +703,9 @@ struct ZeroList {
 void zero_async(const ZeroList& z, cudaStream_t s);
 
 // Exclusive scan of n int32 values into n+1 int64 values (out[n] = total).
-void scan_i32_to_i64(const int* in, int64_t* out, int64_t n, cudaStream_t s, DevBuf<int64_t>& tmp);
+// out32 (optional): the scan also as 32-bit integers (values below 2^31)
+void scan_i32_to_i64(const int* in, int64_t* out, int64_t n, cudaStream_t s, DevBuf<int64_t>& tmp,
+                     int* out32 = nullptr);
 void scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s, DevBuf<int64_t>& tmp);
 
 }  // namespace gr
