@@ -43,6 +43,10 @@ constexpr int kQuadMaxWarpsU = 24;  // unweighted kernels (up to 85 registers)
 // that the reductions, not the warps, bounded it.  (The high limb in the
 // low limb's line instead of a line of its own: 4.58 ms.)
 constexpr int kQuadGWarpsW = GR_QUADG_WEIGHTED_WARPS;
+// Geometric adjoint kernel: 24 warps (at most 85 registers, ~50 bytes
+// spilled) measured 6.13 ms on the 4PCF workload against 6.67 ms at 20 and
+// 7.27 ms at 16 (116 registers), identical gradients.
+constexpr int kQuadGWarpsA = 24;
 constexpr size_t kQuadSmemLimit = 227 * 1024;
 constexpr int kQQueue = 96;         // hit queue entries per warp (< 32 left + 64 pushed)
 constexpr int kQMaxOffset = 1 << 22;  // hash entries: (label offset << 10) | position
@@ -956,7 +960,7 @@ __host__ __device__ inline QuadGLayout quadg_layout(int nbins, int cap, int nwar
 }
 
 template <bool WEIGHTED, bool SHC, bool ADJ, bool COMPACT, bool TETRA>
-__global__ void __launch_bounds__((ADJ ? kQuadMaxWarps : (WEIGHTED ? kQuadGWarpsW : kQuadMaxWarpsU)) * 32)
+__global__ void __launch_bounds__((ADJ ? kQuadGWarpsA : (WEIGHTED ? kQuadGWarpsW : kQuadMaxWarpsU)) * 32)
     quad4g_kernel(
     DevCatalog C, CSRView G, QuadParams Q, unsigned long long* __restrict__ g_cnt,
     unsigned long long* __restrict__ g_fix, unsigned long long* __restrict__ d_cnt,
@@ -1287,7 +1291,7 @@ void launch_adj4(const DevCatalog& C, const CSRView& G, const QuadParams& Q, con
                  unsigned long long* stats, int* work, cudaStream_t s) {
   if (C.n <= 0) return;
   if (Q.geo) {
-    const int nw = quadg_warps(Q.nbins, Q.cap, 0, true, true, kQuadMaxWarps);
+    const int nw = quadg_warps(Q.nbins, Q.cap, 0, true, true, kQuadGWarpsA);
     const size_t smem = quadg_layout(Q.nbins, Q.cap, nw, 0, true, true).total;
     launch_quad_grid(quad4g_kernel<false, false, true, true, false>, nw, smem, C.n, work, s, C, G, Q,
                      nullptr, nullptr, nullptr, nullptr, 0, 0, 1.0, 1.0, stats, cot, gscale, g_lo,
