@@ -38,9 +38,10 @@ constexpr int kQuadMaxWarpsU = 24;  // unweighted kernels (up to 85 registers)
 #define GR_QUADG_WEIGHTED_WARPS 24
 #endif
 // Weighted geometric kernel: 24 warps (at most 85 registers, a few bytes
-// spilled) measured 4.47 ms on the 4PCF workload against 4.64 ms at 20 and
-// 5.04 ms at 16 (106 registers) once its sums had a line per bin; before
-// that the reductions, not the warps, bounded it.  (The high limb in the
+// spilled) measured 4.47 ms on the 4PCF workload against 4.64 ms at 20,
+// 5.04 ms at 16 (106 registers), 4.84 ms at 28 and 5.29 ms at 32 (spills)
+// once its sums had a line per bin; before that the reductions, not the
+// warps, bounded it.  (The high limb in the
 // low limb's line instead of a line of its own: 4.58 ms.)
 constexpr int kQuadGWarpsW = GR_QUADG_WEIGHTED_WARPS;
 // Geometric adjoint kernel: 24 warps (at most 85 registers, ~50 bytes
